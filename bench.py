@@ -1,0 +1,436 @@
+#!/usr/bin/env python
+"""Benchmark of the lceqcd Monte Carlo hot path on B200.
+
+Metric: site-updates/s of the heatbath + overrelaxation sweep (the sweep of
+f/main.f:38-41: ahiggs2, ahiggs3, agauge, reunitarisation), whole job, on the
+single-chain mixed-precision workload: 64^3, beta = 12, x = 0.09, y = 0.3, hot
+start, FP32 fields with FP64 reunitarisation and FP64 sums, measurements on
+every sweep.  A step is one sweep; L2 is flushed (256 MB write) between timed
+steps.  Inputs are synthetic (hot start), there is no dataset.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl reference] [--no-extras]
+
+N > 1 runs N independent replica chains, one per GPU (the path does not
+shard; no collective on the data path), launched by torch.distributed.run.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import re
+import signal
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+L_MAIN = (64, 64, 64)
+COUP = dict(beta=12.0, x=0.09, y=0.3)
+METRIC = "site-updates/s (HB+OR sweep)"
+UNIT = "site-updates/s"
+# algorithmic HBM bytes per lattice site (FP32 fields): one link pass
+# (eo, mu) moves 68 B*V, one Higgs pass 66 B*V, the sweep 672 B*V.
+B_LINK, B_HIGGS, B_SWEEP = 68, 66, 672
+FALLBACK_HBM_GBS = 6650.0
+
+
+def vol(L):
+    return L[0] * L[1] * L[2]
+
+
+def peaks():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    try:
+        d = json.load(open(p))
+        return float(d["hbm_gbs"]), "measured"
+    except Exception:
+        return FALLBACK_HBM_GBS, "fallback"
+
+
+def profile_traffic():
+    """dram bytes per launch of the link kernel from the committed ncu summary."""
+    p = os.path.join(ROOT, "profiles", "link_kernel_64cubed.txt")
+    try:
+        m = re.search(r"dram_bytes_per_launch\s*=\s*([0-9.eE+]+)", open(p).read())
+        return float(m.group(1)) if m else None
+    except OSError:
+        return None
+
+
+class Clocks:
+    """nvidia-smi sampling of SM clock and throttle reasons during a region."""
+
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.hw_slowdown,"
+         "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+         "clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, local_rank: int):
+        vis = os.environ.get("CUDA_VISIBLE_DEVICES", "")
+        ids = [v for v in vis.split(",") if v.strip()]
+        self.index = ids[local_rank] if local_rank < len(ids) else str(local_rank)
+        self.proc = None
+        self.path = None
+
+    def start(self):
+        try:
+            fd, self.path = tempfile.mkstemp(suffix=".csv")
+            os.close(fd)
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--id={self.index}", f"--query-gpu={self.Q}", "--format=csv,noheader,nounits",
+                 "-lms", "200"], stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
+        except Exception:
+            self.proc = None
+
+    def stop(self):
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": [], "note": "nvidia-smi unavailable"}
+        time.sleep(0.25)
+        self.proc.send_signal(signal.SIGTERM)
+        try:
+            self.proc.wait(timeout=5)
+        except Exception:
+            self.proc.kill()
+        sm, smax, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in open(self.path):
+            f = [x.strip() for x in line.split(",")]
+            if len(f) < 8:
+                continue
+            try:
+                sm.append(float(f[1]))
+                smax.append(float(f[2]))
+            except ValueError:
+                continue
+            for n, v in zip(names, f[4:8]):
+                if v.lower().startswith("active"):
+                    reasons.add(n)
+        os.unlink(self.path)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(smax) if smax else None,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def dist_setup():
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if world > 1:
+        import datetime
+        import torch
+        import torch.distributed as dist
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
+    return rank, world, local
+
+
+def barrier(world):
+    if world > 1:
+        import torch.distributed as dist
+        dist.barrier()
+
+
+def max_over_ranks(v: float, world: int) -> float:
+    if world == 1:
+        return v
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([v], dtype=torch.float64, device="cuda")
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+# ---------------------------------------------------------------------- GPU arm
+def timed_sweeps(lat, K, flush=True):
+    """K sweeps, each bracketed by CUDA events on the context stream; L2
+    flushed between steps (outside the events).  Returns total device ms."""
+    tot = 0.0
+    for _ in range(K):
+        if flush:
+            lat.flush_l2()
+        lat.timer_start()
+        lat.sweeps(1, 1)
+        tot += lat.timer_stop()
+    return tot
+
+
+def kernel_profile(lat, reps=10):
+    """Per-pass durations (events between kernels) of the sweep, averaged."""
+    acc = None
+    for _ in range(reps):
+        lat.flush_l2()
+        lat.synchronize()
+        ms = lat.profile_sweep(1)
+        acc = ms if acc is None else acc + ms
+    return acc / reps
+
+
+def cpu_baseline(L, budget_s=20.0, warm=1):
+    """The oracle (FP32 restatement of the reference, OpenMP over sites in a
+    parity pass) on the host cores, time-bounded sample of the workload."""
+    import numpy as np
+    from oracle.oracle import Oracle, hot_config
+    threads = os.cpu_count() or 1
+    u, a = hot_config(L, seed=3, dtype=np.float32)
+    o = Oracle(L, COUP["beta"], COUP["x"], COUP["y"], bits=32, threads=threads)
+    o.set_fields(u, a)
+    o.set_philox(3, 0)
+    for _ in range(warm):
+        o.sweep(1)
+    n, t0 = 0, time.perf_counter()
+    while True:
+        o.sweep(1)
+        n += 1
+        el = time.perf_counter() - t0
+        if el > budget_s or n >= 10000:
+            break
+    return vol(L) * n / el, threads, n, el
+
+
+def extras(args, peak):
+    """Bounded secondary measurements (rank 0, N = 1)."""
+    import numpy as np
+    from lceqcd_b200 import Ensemble, Lattice, Params
+    out = {}
+    for L in ((128, 128, 128), (256, 256, 256)):
+        key = f"sweep_{L[0]}cubed"
+        try:
+            lat = Lattice(L, **COUP, precision="f32", seed=11)
+            lat.init_hot(12)
+            lat.sweeps(3, 0)
+            timed_sweeps(lat, 3)
+            K = 20 if L[0] <= 128 else 10
+            ms = timed_sweeps(lat, K)
+            prof = kernel_profile(lat, reps=3)
+            link = float(np.mean(prof[4:10])) if len(prof) >= 10 else None
+            sps = vol(L) * K / (ms / 1e3)
+            out[key] = {"site_updates_per_s": sps, "ms_per_sweep": ms / K,
+                        "sweep_hbm_gbs": sps * B_SWEEP / 1e9, "sweep_frac_of_measured_hbm": sps * B_SWEEP / 1e9 / peak,
+                        "link_kernel_ms": link,
+                        "link_kernel_frac_of_measured_hbm": (B_LINK * vol(L) / (link / 1e3) / 1e9 / peak) if link else None}
+            lat.close()
+        except Exception as e:  # a secondary number must not take the headline down
+            out[key] = {"error": repr(e)[:300]}
+    # Landau gauge fixing of thermalised 128^3 configurations to theta < 1e-10
+    try:
+        L = (128, 128, 128)
+        lat = Lattice(L, **COUP, precision="f32", seed=21, lam=1.7, limit_or=1e-10)
+        lat.init_hot(22)
+        lat.sweeps(200, 0)
+        res = []
+        for _ in range(2):
+            lat.sweeps(10, 0)
+            lat.synchronize()
+            t0 = time.perf_counter()
+            th, it = lat.landau_gauge(max_iters=100000)
+            res.append((time.perf_counter() - t0, it, th, lat.gauge_functional()))
+        out["gauge_fix_128cubed"] = {
+            "s_per_config": statistics.mean(r[0] for r in res), "iterations": [r[1] for r in res],
+            "theta": [r[2] for r in res], "functional": [r[3] for r in res], "limit": 1e-10,
+            "gf_hbm_gbs": statistics.mean(216 * vol(L) * r[1] / r[0] / 1e9 for r in res)}
+        lat.close()
+    except Exception as e:
+        out["gauge_fix_128cubed"] = {"error": repr(e)[:300]}
+    # batched ensemble: 96 chains (32 each of 16^3, 32^3, 48^3) over the
+    # coupling grid, against the same chains run one context at a time
+    try:
+        grid = [(b, y, x) for b in (6.0, 9.0, 12.0, 16.0) for y in (0.1, 0.3, 0.5) for x in (0.08, 0.1)]
+        specs = []
+        for i in range(96):
+            b, y, x = grid[i % 24]
+            n = (16, 32, 48)[i // 32]
+            specs.append(Params(L=(n, n, n), beta=b, x=x, y=y, seed=i + 1))
+        sites = sum(vol(s.L) for s in specs)
+        ens = Ensemble(specs)
+        ens.init_hot(5)
+        ens.sweeps(5, 0)
+        timed_sweeps(ens, 3)
+        K = 20
+        ms_b = timed_sweeps(ens, K)
+        ens.close()
+        plain = {}
+        for prec in ("f64", "f32"):
+            tot = 0.0
+            for s in specs:
+                g = Lattice(s.L, beta=s.beta, x=s.x, y=s.y, seed=s.seed, precision=prec)
+                g.init_hot(s.seed)
+                g.sweeps(2, 1)
+                g.synchronize()
+                t = timed_sweeps(g, 3, flush=False) / 3
+                tot += t
+                g.close()
+            plain[prec] = sites / (tot / 1e3)
+        bat = sites * K / (ms_b / 1e3)
+        out["batched_96_chains"] = {"site_updates_per_s": bat, "plain_f64_site_updates_per_s": plain["f64"],
+                                    "plain_f32_site_updates_per_s": plain["f32"],
+                                    "speedup_vs_plain_f64": bat / plain["f64"], "speedup_vs_plain_f32": bat / plain["f32"],
+                                    "sites": sites}
+    except Exception as e:
+        out["batched_96_chains"] = {"error": repr(e)[:300]}
+    return out
+
+
+def run_gpu(args):
+    import numpy as np
+    from lceqcd_b200 import Lattice
+    rank, world, local = dist_setup()
+    peak, peak_src = peaks()
+    V = vol(L_MAIN)
+    lat = Lattice(L_MAIN, **COUP, precision="f32", seed=1000 + rank, device=local)
+    lat.init_hot(2000 + rank)
+    lat.sweeps(20, 0)
+    timed_sweeps(lat, max(args.warmup, 3))
+    lat.synchronize()
+    barrier(world)
+    clk = Clocks(local)
+    clk.start()
+    wall0 = time.perf_counter()
+    ms = timed_sweeps(lat, args.steps)
+    lat.synchronize()
+    wall = time.perf_counter() - wall0
+    barrier(world)
+    clocks = clk.stop()
+    ms_max = max_over_ranks(ms, world)
+    value = world * V * args.steps / (ms_max / 1e3)
+    launches = args.steps * (11 + 1)  # 10 pass kernels + finalize per sweep, 1 L2 flush per step
+
+    # roofline of the dominant kernel (link update, 6 of the 10 passes)
+    prof = kernel_profile(lat, reps=10)
+    link_ms = float(np.mean(prof[4:10]))
+    higgs_ms = float(np.mean(prof[0:4]))
+    achieved = B_LINK * V / (link_ms / 1e3) / 1e9
+    traffic = profile_traffic()
+
+    # end to end through the C ABI with pinned host buffers: upload the fields,
+    # one measured sweep with the scalars read back, download the fields
+    import torch
+    nh = V // 2
+    hu = torch.empty((3, 2, nh, 4), dtype=torch.float32, pin_memory=True).numpy()
+    ha = torch.empty((2, nh, 3), dtype=torch.float32, pin_memory=True).numpy()
+    u0, a0 = lat.download()
+    hu[...] = u0
+    ha[...] = a0
+    Ke = max(5, min(args.steps, 50))
+    for _ in range(2):
+        lat.upload(hu, ha)
+        lat.sweep(1)
+        lat.download_into(hu, ha)
+    barrier(world)
+    e2e_ms = 0.0
+    for _ in range(Ke):
+        lat.flush_l2()
+        lat.timer_start()
+        lat.upload(hu, ha)
+        lat.sweep(1)
+        lat.download_into(hu, ha)
+        e2e_ms += lat.timer_stop()
+    e2e_ms = max_over_ranks(e2e_ms, world)
+    e2e_val = world * V * Ke / (e2e_ms / 1e3)
+    h2d = hu.nbytes + ha.nbytes
+    d2h = hu.nbytes + ha.nbytes + 13 * 8
+
+    line = {
+        "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": ms_max / args.steps, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+        "data": "synthetic (hot start: Haar links, A0 ~ N(0,1))",
+        "config": {"workload": "single chain 64^3, beta=12, x=0.09, y=0.3, hot start; FP32 fields, FP64 "
+                               "reunitarisation and sums; sweep = ahiggs2+ahiggs3+agauge (+fused renorm), "
+                               "measurements every sweep",
+                   "L": list(L_MAIN), "sites": V, "l2": "flushed between timed steps (256 MB write)",
+                   "parallelism": f"replicas x{world}" if world > 1 else "single GPU",
+                   "wall_s_timed_region": wall},
+        "e2e": {"value": e2e_val, "unit": UNIT, "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
+                "note": "lce_upload(host fields) + lce_sweep(meas read back) + lce_download(host fields) per step"},
+        "gpu_launches": launches,
+        "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
+                     "traffic": traffic, "kernel": "link_kernel (agauge pass, one parity x one mu)",
+                     "algorithmic_bytes_per_launch": B_LINK * V, "avg_launch_ms": link_ms,
+                     "peak_source": f"{peak_src} (MEASURED_PEAKS.json hbm_gbs)" if peak_src == "measured" else "fallback",
+                     "higgs_kernel_frac": B_HIGGS * V / (higgs_ms / 1e3) / 1e9 / peak,
+                     "sweep_frac": value / world * B_SWEEP / 1e9 / peak},
+        "clocks": clocks,
+    }
+    if rank == 0 and world == 1:
+        try:
+            v, cores, n, el = cpu_baseline(L_MAIN, budget_s=args.cpu_budget)
+            line["cpu_baseline"] = {"value": v, "unit": UNIT, "cores": cores, "kind": "port",
+                                    "sample": f"{n} full 64^3 sweeps ({el:.1f} s) of the FP32 oracle restatement "
+                                              f"of the reference (OpenMP over sites, {cores} threads)"}
+        except Exception as e:
+            line["cpu_baseline"] = {"value": None, "unit": UNIT, "cores": 0, "kind": "port", "sample": repr(e)[:200]}
+        if args.extras:
+            line["secondary"] = extras(args, peak)
+    lat.close()
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    if world > 1:
+        import torch.distributed as dist
+        dist.destroy_process_group()
+
+
+# ---------------------------------------------------------------- reference arm
+def run_reference(args):
+    """The reference's CPU implementation of the path: the Fortran/MPI
+    reference cannot be compiled in this image (no gfortran, no MPI), so this
+    times the oracle port (FP32 restatement, OpenMP) on the host cores, on
+    the same 64^3 workload; one step = one sweep."""
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    if rank != 0:
+        return
+    import numpy as np
+    from oracle.oracle import Oracle, hot_config
+    threads = os.cpu_count() or 1
+    u, a = hot_config(L_MAIN, seed=3, dtype=np.float32)
+    o = Oracle(L_MAIN, COUP["beta"], COUP["x"], COUP["y"], bits=32, threads=threads)
+    o.set_fields(u, a)
+    o.set_philox(3, 0)
+    t0 = time.perf_counter()
+    o.sweep(1)
+    t1 = time.perf_counter() - t0
+    budget = 150.0
+    W = min(args.warmup, max(1, int(20 / max(t1, 1e-3))))
+    for _ in range(W):
+        o.sweep(1)
+    K = min(args.steps, max(1, int(budget / max(t1, 1e-3))))
+    t0 = time.perf_counter()
+    for _ in range(K):
+        o.sweep(1)
+    el = time.perf_counter() - t0
+    v = vol(L_MAIN) * K / el
+    line = {"metric": METRIC, "value": v, "unit": UNIT, "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": el / K * 1e3, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "dtype": "f32", "data": "synthetic (hot start)", "impl": "reference",
+            "config": {"workload": "single chain 64^3, beta=12, x=0.09, y=0.3, hot start; FP32; reference sweep "
+                                   "composition", "L": list(L_MAIN), "sites": vol(L_MAIN)},
+            "cpu_baseline": {"value": v, "unit": UNIT, "cores": threads, "kind": "port",
+                             "sample": f"{K} of {args.steps} steps timed (bounded to ~{budget:.0f} s), each a full "
+                                       "64^3 sweep of the FP32 oracle restatement (the Fortran reference has no "
+                                       "compiler in this image)"},
+            "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=100)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", default="lceqcd_b200", choices=["lceqcd_b200", "reference"])
+    ap.add_argument("--no-extras", dest="extras", action="store_false")
+    ap.add_argument("--cpu-budget", type=float, default=15.0)
+    args = ap.parse_args()
+    if args.warmup < 3:
+        args.warmup = 3
+    if args.impl == "reference":
+        run_reference(args)
+    else:
+        run_gpu(args)
+
+
+if __name__ == "__main__":
+    main()

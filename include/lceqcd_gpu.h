@@ -1,0 +1,220 @@
+/*
+ * lceqcd_gpu.h -- C ABI of the B200 (sm_100a) Monte Carlo hot path for the
+ * 3D SU(2) + adjoint Higgs (A0) lattice code derek-teaney/lceqcd.
+ *
+ * Every entry point is extern "C", takes plain pointers and sizes, and
+ * returns an int status (LCE_OK = 0, negative = error; see lce_strerror).
+ * A Fortran driver binds these with ISO_C_BINDING; the C++ driver
+ * (lceqcd_b200/driver/lce_main.cpp) and the Python mirror
+ * (lceqcd_b200/lattice.py) call them directly.
+ *
+ * The reference exposes no plugin API: the boundary replaced here is the set
+ * of Fortran subroutines that f/main.f:21-78 calls inside its sweep loop, and
+ * the COMMON blocks they share (f/INCLUDE/gaugefield.inc:35-36,
+ * f/INCLUDE/measurement.inc:228-233).  Each declaration below names the
+ * reference routine it replaces.
+ *
+ * Host field layout ("reference order"), matching the COMMON arrays
+ * COMPLEX u(2, maxarray, 0:1, 3) and REAL a(3, maxarray, 0:1):
+ *   u[((mu*2 + eo)*ld + site)*4 + c], c = (Re a, Im a, Re b, Im b) of the first
+ *       row (a, b) of U = {{a, b}, {-b*, a*}};  mu = 0..2, eo = 0..1
+ *   a[(eo*ld + site)*3 + k],  A = a_k sigma_k
+ * with site in the half-row order of f/adresses.f and ld >= L1*L2*L3/2 the
+ * leading site dimension (maxarray for the Fortran COMMON blocks).
+ *
+ * Threading: one host thread per context.  All work of a context is queued
+ * on its CUDA stream; calls that return values to host memory synchronise
+ * that stream.
+ */
+#ifndef LCEQCD_GPU_H
+#define LCEQCD_GPU_H
+
+#include <stddef.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+#if defined(__GNUC__)
+#pragma GCC visibility push(default)
+#endif
+
+#define LCE_ABI_VERSION 1
+
+/* status codes */
+#define LCE_OK 0
+#define LCE_ERR_INVALID (-1)        /* bad argument or lattice shape */
+#define LCE_ERR_CUDA (-2)           /* CUDA runtime error (lce_last_error) */
+#define LCE_ERR_GF_NOT_CONVERGED (-3)  /* gauge fixing hit max_iters */
+#define LCE_ERR_STREAM (-4)         /* validation uniform stream exhausted */
+#define LCE_ERR_NAN (-5)            /* non-finite value in a reduction */
+#define LCE_ERR_NOMEM (-6)          /* device allocation failed */
+#define LCE_ERR_UNSUPPORTED (-7)    /* call not valid for this context */
+
+/* precision of the device fields */
+#define LCE_PREC_F32 0  /* FP32 fields; FP64 reunitarisation, sums, theta */
+#define LCE_PREC_F64 1  /* FP64 everywhere (validation / plain path) */
+
+/* uniform sources */
+#define LCE_RNG_PHILOX 0  /* counter-based Philox4x32-10, per (seed, pass, site) */
+#define LCE_RNG_STREAM 1  /* host-supplied uniforms in the reference's order */
+
+/* gauge-fixing angle evaluation.  The reference takes theta = acos(Re Omega),
+ * which cannot resolve rotations below ~sqrt(eps) (~3e-4 rad in FP32, ~1e-8 in
+ * FP64), so the iteration stalls near theta ~ 1e-7 (FP32) or 1e-14 (FP64).
+ * ATAN2 takes the same angle as atan2(|vector part|, scalar part) of w, which
+ * is accurate for small angles; it is the default. */
+#define LCE_GF_ACOS 0
+#define LCE_GF_ATAN2 1
+
+/* field selectors for upload/download */
+#define LCE_FIELDS 0        /* u, a        (COMMON /linkvar/ u, a) */
+#define LCE_FIELDS_FIXED 1  /* u_f, a_f    (COMMON /linkvar/ u_f, a_f) */
+
+typedef struct lce_ctx lce_ctx;
+
+/* Input parameters: the hot-path subset of the reference's inputfile
+ * (f/paraminit.f:325-344) plus build-only knobs. */
+typedef struct lce_params {
+  int L[3];              /* global lattice extents (even)            inputfile line 1 */
+  double beta, x, y;     /* couplings                                  lines 8-10 */
+  double lambda;         /* gauge-fixing overrelaxation parameter      line 11 */
+  double alpha;          /* z-link weight of the gauge functional      line 12 */
+  double limit_or;       /* stopping value of theta                    line 13 */
+  int imode;             /* Higgs heatbath mode 0/1                    line 20 */
+  int precision;         /* LCE_PREC_F32 | LCE_PREC_F64 */
+  int rng;               /* LCE_RNG_PHILOX | LCE_RNG_STREAM */
+  unsigned long long seed;  /* Philox key */
+  int device;            /* CUDA device ordinal */
+  int n_link_or;         /* link overrelaxation hits per lce_sweep (0: reference composition) */
+  int n_higgs_metro;     /* ahiggs1 calls per lce_sweep (0: reference composition) */
+  double delta0;         /* initial ahiggs1 step */
+  int gf_angle;          /* gauge-fixing rotation angle: LCE_GF_ACOS (the
+                            reference, f/or_gauge_fixing1.f:174) or LCE_GF_ATAN2 */
+} lce_params;
+
+/* Measured quantities: /aver_loc/ (plaq0, a0kin, a02, a04, a0f) and the
+ * acceptances of f/INCLUDE/measurement.inc, in FP64. */
+typedef struct lce_meas {
+  double plaq;        /* agauge plaquette against the pre-update staple, /(12V) */
+  double akin;        /* sum a.F / (6V) of the last Higgs update */
+  double a2;          /* <A^2> of the last Higgs update */
+  double a4;          /* <A^4> of the last Higgs update */
+  double acc_gauge;   /* agauge accept (KP rate x Metropolis rate / 4) */
+  double acc_hb;      /* ahiggs2 accept */
+  double acc_or;      /* ahiggs3 accept */
+  double acc_metro;   /* ahiggs1 accept */
+  double acc_link_or; /* link overrelaxation accept */
+  double delta;       /* current ahiggs1 step */
+  double af[3];       /* meas2a: average of A_f */
+} lce_meas;
+
+/* ---- library ---- */
+const char* lce_version(void);
+const char* lce_strerror(int status);
+/* last CUDA/validation error message of a context (or of the last failed create) */
+const char* lce_last_error(lce_ctx* ctx);
+void lce_default_params(lce_params* p);
+/* f/paraminit.f:393-396: beta_a, beta_2, beta_4 from beta, x, y (FP64) */
+int lce_couplings(const lce_params* p, double out[3]);
+/* f/adresses.f:91-337 neighbour tables (single rank, periodic), 0-based:
+ * t[(eo*3 + mu)*nh + site]; computed by the same index arithmetic the kernels use */
+int lce_geometry_tables(int L1, int L2, int L3, int* siteup, int* sitedn);
+
+/* ---- context (replaces f/initialize.f:23-53 state set-up for the hot path) ---- */
+lce_ctx* lce_create(const lce_params* p);
+/* many independent chains (uneven volumes and couplings) in one context;
+ * every update call advances all chains together */
+lce_ctx* lce_create_batch(const lce_params* p, int nchains);
+void lce_destroy(lce_ctx* ctx);
+int lce_nchains(lce_ctx* ctx);
+int lce_set_stream(lce_ctx* ctx, void* cuda_stream); /* NULL: the context's own stream */
+int lce_synchronize(lce_ctx* ctx);
+
+/* ---- fields (COMMON /linkvar/ mirrors; f/confget.f / f/confsave.f boundary) ---- */
+int lce_upload(lce_ctx* ctx, int chain, int which, const float* u, const float* a, long ld);
+int lce_upload_f64(lce_ctx* ctx, int chain, int which, const double* u, const double* a, long ld);
+int lce_download(lce_ctx* ctx, int chain, int which, float* u, float* a, long ld);
+int lce_download_f64(lce_ctx* ctx, int chain, int which, double* u, double* a, long ld);
+/* f/confget.f unitconf (:295-307): U = 1, A = (0, 0, a3) on every chain */
+int lce_init_unit(lce_ctx* ctx, double a3);
+/* hot start: Haar links (normalised 4-Gaussians), A components ~ N(0,1) */
+int lce_init_hot(lce_ctx* ctx, unsigned long long seed);
+
+/* ---- random numbers ---- */
+/* validation mode (LCE_RNG_STREAM, single chain): uniforms consumed in the
+ * reference's order, 29*V per reference sweep (f/heat_kpi.f, f/gauss.f,
+ * f/agauge.f, f/ahiggs2.f, f/ahiggs3.f draw order) */
+int lce_set_rng_stream(lce_ctx* ctx, const double* uniforms, size_t n);
+int lce_get_rng_position(lce_ctx* ctx, unsigned long long* pass_ctr, unsigned long long* stream_pos);
+int lce_set_rng_position(lce_ctx* ctx, unsigned long long pass_ctr, unsigned long long stream_pos);
+
+/* ---- Monte Carlo updates (accept may be NULL: no synchronisation) ---- */
+/* f/ahiggs1.f:7-127 Metropolis; *delta is adapted as the reference does */
+int lce_ahiggs1(lce_ctx* ctx, float* delta, int measflag, float* accept);
+/* f/ahiggs2.f:124-267 heatbath (with f/a_force.f, f/gauss.f) */
+int lce_ahiggs2(lce_ctx* ctx, int measflag, float* accept);
+/* f/ahiggs3.f:283-424 overrelaxation */
+int lce_ahiggs3(lce_ctx* ctx, int measflag, float* accept);
+/* f/agauge.f:7-205 with f/staples.f, f/heat_kpi.f */
+int lce_agauge(lce_ctx* ctx, int measflag, float* accept);
+/* link overrelaxation with the agauge Metropolis test (no reference counterpart) */
+int lce_link_or(lce_ctx* ctx, int measflag, float* accept);
+/* f/renorm.f:205-236 */
+int lce_renorm(lce_ctx* ctx);
+/* f/main.f:38-41: ahiggs2, ahiggs3, [ahiggs1 x n_higgs_metro], agauge,
+ * [link OR x n_link_or], reunitarisation fused into the link writers; one
+ * CUDA graph per measflag.  m (chain 0) may be NULL: no synchronisation. */
+int lce_sweep(lce_ctx* ctx, int measflag, lce_meas* m);
+/* nsweeps graph replays without synchronisation */
+int lce_sweeps(lce_ctx* ctx, int nsweeps, int measflag);
+/* f/meas1.f inputs: the last measured quantities of a chain */
+int lce_get_meas(lce_ctx* ctx, int chain, lce_meas* m);
+int lce_get_meas_batch(lce_ctx* ctx, lce_meas* m /* [nchains] */);
+
+/* ---- gauge fixing (f/landau_gauge.f:281-338, f/or_gauge_fixing1.f) ---- */
+/* copy U,A -> U_f,A_f, iterate overrelaxed gauge fixing until theta <= limit_or.
+ * max_iters <= 0 means no cap (the reference has none).  Returns
+ * LCE_ERR_GF_NOT_CONVERGED when the cap ends the loop. */
+int lce_landau_gauge(lce_ctx* ctx, int chain, double* theta, int* iters, int max_iters);
+/* iterate on the current U_f,A_f without the copy (warm starts, continuation) */
+int lce_gauge_fix_continue(lce_ctx* ctx, int chain, double* theta, int* iters, int max_iters);
+/* gauge functional (1/((2+alpha)V)) sum_x,mu c_mu Re a of U_f */
+int lce_gauge_functional(lce_ctx* ctx, int chain, double* value);
+/* theta of the current U_f (odd sites, FP64), without updating */
+int lce_theta(lce_ctx* ctx, int chain, double* theta);
+
+/* ---- measurements ---- */
+/* f/correlator.f:11-186 (z-slice correlators of A_f and U_f, all z) and
+ * f/meas2a.f:168-178 (average of A_f); any output may be NULL */
+int lce_correlator(lce_ctx* ctx, int chain, double* corr_a, double* corr_u, double* corr_3,
+                   double af[3]);
+/* f/polyakov.f:202-315: slice means of cos(4|A|), their correlator, mean^2 */
+int lce_polyakov(lce_ctx* ctx, int chain, double* slice, double* corr, double* mean2);
+/* f/scalarcorr.f:331-440: slice means of |A|^2, their correlator, mean */
+int lce_scalarcorr(lce_ctx* ctx, int chain, double* slice, double* corr, double* mean);
+/* average plaquette 1/2 Re Tr of the current U (all 3V plaquettes) */
+int lce_plaquette(lce_ctx* ctx, int chain, double* plaq);
+
+/* ---- validation entry points (FP64 outputs) ---- */
+/* staple V(x) of f/staples.f for (eo, mu): out[site*4 + c] */
+int lce_debug_staple(lce_ctx* ctx, int eo, int mu, double* out);
+/* Higgs force F(x) of f/a_force.f for parity eo: out[site*3 + k] */
+int lce_debug_force(lce_ctx* ctx, int eo, double* out);
+
+/* ---- timing ---- */
+/* write a device buffer larger than L2 (126 MB) on the context stream */
+int lce_flush_l2(lce_ctx* ctx);
+/* run one sweep with a CUDA event between kernels; ms[i] = duration of pass
+ * i (10 passes for the reference composition); returns the pass count */
+int lce_profile_sweep(lce_ctx* ctx, int measflag, float* ms, int max_passes);
+/* events on the context stream */
+int lce_timer_start(lce_ctx* ctx);
+int lce_timer_stop(lce_ctx* ctx, float* ms);
+
+#if defined(__GNUC__)
+#pragma GCC visibility pop
+#endif
+#ifdef __cplusplus
+}
+#endif
+#endif /* LCEQCD_GPU_H */

@@ -1,0 +1,1004 @@
+// lce_capi.cu -- the extern "C" boundary (include/lceqcd_gpu.h).
+//
+// A context owns one CUDA stream, one device allocation holding the fields of
+// all its chains, a chain table, the device-resident run state (RNG pass
+// counter, validation-stream position, status bits, per-chain gauge-fixing
+// state) and FP64 partial-sum buffers.  Update routines are queued as one
+// kernel per parity pass followed by one finalize kernel; lce_sweep captures
+// its whole pass sequence once per measflag into a CUDA graph and replays it.
+// The RNG counters live on the device, so a replayed graph draws fresh
+// numbers every time.
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <map>
+#include <string>
+#include <vector>
+
+#include "lce_internal.hpp"
+
+using namespace lce;
+
+namespace {
+
+thread_local std::string g_create_error;
+
+struct Pass {
+  unsigned char kind;
+  int eo, mu;
+  bool end;  // last pass of its routine
+};
+
+}  // namespace
+
+struct lce_ctx {
+  int device = 0;
+  int prec = LCE_PREC_F32;
+  int rng = LCE_RNG_PHILOX;
+  int nchains = 0;
+  int n_link_or = 0, n_higgs_metro = 0;
+  std::vector<lce_params> params;
+  std::vector<ChainDev> ch;
+  std::vector<int> blk;  // prefix of blocks per pass
+  int max_nh = 0, max_L3 = 0;
+  ChainDev* ch_d = nullptr;
+  int* blk_d = nullptr;
+  CtxState* st_d = nullptr;
+  ChainState* cst_d = nullptr;
+  lce_meas* meas_d = nullptr;
+  double* part_d = nullptr;
+  int part_slots = 0;
+  size_t slot_stride = 0;
+  double* totals_d = nullptr;
+  double* scratch_d = nullptr;
+  size_t scratch_n = 0;
+  void* fields_d = nullptr;
+  double* stream_d = nullptr;
+  size_t stream_n = 0;
+  void* staging_d = nullptr;
+  size_t staging_bytes = 0;
+  void* flush_d = nullptr;
+  size_t flush_bytes = 0;
+  cudaStream_t own = nullptr, stream = nullptr;
+  cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+  cudaGraphExec_t sweep_exec[2] = {nullptr, nullptr};
+  std::map<std::pair<int, int>, cudaGraphExec_t> gf_exec;
+  std::string err;
+};
+
+namespace {
+
+int fail(lce_ctx* c, int code, const std::string& msg) {
+  if (c) c->err = msg;
+  else g_create_error = msg;
+  return code;
+}
+
+int cuda_fail(lce_ctx* c, cudaError_t e, const char* where) {
+  return fail(c, LCE_ERR_CUDA, std::string(where) + ": " + cudaGetErrorString(e));
+}
+
+#define CK(call)                                          \
+  do {                                                    \
+    cudaError_t e_ = (call);                              \
+    if (e_ != cudaSuccess) return cuda_fail(c, e_, #call); \
+  } while (0)
+
+size_t link_bytes(int prec) { return prec == LCE_PREC_F64 ? 32 : 16; }
+size_t real_bytes(int prec) { return prec == LCE_PREC_F64 ? 8 : 4; }
+size_t align256(size_t n) { return (n + 255) & ~(size_t)255; }
+
+// f/paraminit.f:287-290 and :393-396, in the precision of the fields
+template <typename T>
+void couplings_t(double beta, double x, double y, double out[3]) {
+  const T pi = (T)2.0 * (T)std::acos((T)0.0);
+  const T sigma = (T)3.1759114;
+  const T b = (T)beta, xx = (T)x, yy = (T)y;
+  const T beta_a = b;
+  const T beta_2 = beta_a * ((T)3 + (T)8 * yy / (b * b) - sigma * ((T)4 + (T)5 * xx) / ((T)2 * pi * b) -
+                             (((T)20 * xx - (T)10 * (xx * xx)) * ((T)std::log((T)1.5 * b) + (T)0.09) + (T)8.7 +
+                              (T)11.6 * xx) /
+                                 (((T)2 * (pi * pi)) * (b * b)));
+  out[0] = beta_a;
+  out[1] = beta_2;
+  out[2] = xx * b;
+}
+
+bool valid_params(const lce_params& p, std::string& why) {
+  for (int i = 0; i < 3; ++i)
+    if (p.L[i] < 2 || (p.L[i] & 1)) {
+      why = "lattice extents must be even and >= 2";
+      return false;
+    }
+  double v = (double)p.L[0] * p.L[1] * p.L[2];
+  if (v / 2 > 1.0e9) {
+    why = "lattice too large for 32-bit site indices";
+    return false;
+  }
+  if (p.precision != LCE_PREC_F32 && p.precision != LCE_PREC_F64) {
+    why = "precision must be LCE_PREC_F32 or LCE_PREC_F64";
+    return false;
+  }
+  if (p.rng != LCE_RNG_PHILOX && p.rng != LCE_RNG_STREAM) {
+    why = "rng must be LCE_RNG_PHILOX or LCE_RNG_STREAM";
+    return false;
+  }
+  if (!(p.beta > 0)) {
+    why = "beta must be positive";
+    return false;
+  }
+  if (p.imode != 0 && p.imode != 1) {
+    why = "imode must be 0 or 1";
+    return false;
+  }
+  if (p.gf_angle != LCE_GF_ACOS && p.gf_angle != LCE_GF_ATAN2) {
+    why = "gf_angle must be LCE_GF_ACOS or LCE_GF_ATAN2";
+    return false;
+  }
+  if (!(p.lambda > 0) || !(p.alpha >= 0)) {
+    why = "lambda must be positive and alpha non-negative";
+    return false;
+  }
+  if (p.n_link_or < 0 || p.n_higgs_metro < 0 || 4 + 6 + 2 * p.n_higgs_metro + 6 * p.n_link_or > kMaxSlots) {
+    why = "too many extra update passes per sweep";
+    return false;
+  }
+  return true;
+}
+
+int status_check(lce_ctx* c) {
+  CtxState st;
+  CK(cudaMemcpyAsync(&st, c->st_d, sizeof(st), cudaMemcpyDeviceToHost, c->stream));
+  CK(cudaStreamSynchronize(c->stream));
+  if (st.status) {
+    unsigned int z = 0;
+    CK(cudaMemcpy(&c->st_d->status, &z, sizeof(z), cudaMemcpyHostToDevice));
+    if (st.status & kStatusStreamExhausted) return fail(c, LCE_ERR_STREAM, "validation uniform stream exhausted");
+    return fail(c, LCE_ERR_NAN, "non-finite value in a measurement reduction");
+  }
+  return LCE_OK;
+}
+
+int nslots_of(unsigned char kind) {
+  switch (kind) {
+    case kHiggsHB: return 7;
+    case kHiggsOR: return 1;
+    case kHiggsMetro: return 4;
+    case kLinkHB: return 7;
+    default: return 1;
+  }
+}
+
+void expand(unsigned char kind, std::vector<Pass>& out) {
+  if (kind <= kHiggsMetro) {
+    out.push_back({kind, 0, 0, false});
+    out.push_back({kind, 1, 0, true});
+  } else {
+    for (int eo = 0; eo < 2; ++eo)
+      for (int mu = 0; mu < 3; ++mu) out.push_back({kind, eo, mu, eo == 1 && mu == 2});
+  }
+}
+
+// Queue the passes of the given routines and one finalize kernel.
+// events: optional array receiving an event record after every pass.
+int enqueue(lce_ctx* c, const std::vector<unsigned char>& routines, int measflag, bool fuse_renorm,
+            cudaEvent_t* events = nullptr) {
+  std::vector<Pass> passes;
+  for (unsigned char r : routines) expand(r, passes);
+  FinalizeArgs f;
+  std::memset(&f, 0, sizeof(f));
+  f.chains = c->ch_d;
+  f.blk_begin = c->blk_d;
+  f.st = c->st_d;
+  f.cst = c->cst_d;
+  f.meas = c->meas_d;
+  f.part = c->part_d;
+  f.slot_stride = c->slot_stride;
+  f.totals = c->totals_d;
+  f.nchains = c->nchains;
+  f.single = c->prec == LCE_PREC_F32;
+  const int nblocks = c->blk.back();
+  unsigned long long soff = 0;
+  int slot = 0;
+  for (size_t i = 0; i < passes.size(); ++i) {
+    const Pass& ps = passes[i];
+    const bool reduce = measflag == 1 || ps.kind == kHiggsMetro;
+    if (reduce && slot >= c->part_slots) return fail(c, LCE_ERR_INVALID, "too many reduction slots");
+    PassArgs a;
+    a.chains = c->ch_d;
+    a.blk_begin = c->blk_d;
+    a.st = c->st_d;
+    a.cst = c->cst_d;
+    a.part = reduce ? c->part_d + (size_t)slot * c->slot_stride : nullptr;
+    a.stream = c->rng == LCE_RNG_STREAM ? c->stream_d : nullptr;
+    a.stream_n = c->stream_n;
+    a.stream_off = soff;
+    a.pass_off = (unsigned int)i;
+    a.nchains = c->nchains;
+    a.eo = ps.eo;
+    a.fuse_renorm = fuse_renorm ? 1 : 0;
+    if (ps.kind <= kHiggsMetro) {
+      if (c->prec == LCE_PREC_F64) launch_higgs<double>(ps.kind, a, nblocks, c->stream);
+      else launch_higgs<float>(ps.kind, a, nblocks, c->stream);
+    } else {
+      const int mode = ps.kind == kLinkHB ? 0 : 1;
+      if (c->prec == LCE_PREC_F64) launch_link<double>(mode, ps.mu, a, nblocks, c->stream);
+      else launch_link<float>(mode, ps.mu, a, nblocks, c->stream);
+    }
+    if (events) CK(cudaEventRecord(events[i], c->stream));
+    if (reduce) {
+      f.kinds[slot] = (unsigned char)(ps.kind | (ps.end ? kKindEnd : 0));
+      ++slot;
+    }
+    if (c->nchains == 1) soff += (unsigned long long)nslots_of(ps.kind) * c->ch[0].nh;
+  }
+  f.nslots = slot;
+  f.npasses = (unsigned int)passes.size();
+  f.nstream = c->rng == LCE_RNG_STREAM ? soff : 0;
+  launch_finalize(f, c->stream);
+  CK(cudaGetLastError());
+  return LCE_OK;
+}
+
+std::vector<unsigned char> sweep_routines(const lce_ctx* c) {
+  std::vector<unsigned char> r = {kHiggsHB, kHiggsOR};
+  for (int i = 0; i < c->n_higgs_metro; ++i) r.push_back(kHiggsMetro);
+  r.push_back(kLinkHB);
+  for (int i = 0; i < c->n_link_or; ++i) r.push_back(kLinkOR);
+  return r;
+}
+
+int routine_call(lce_ctx* c, unsigned char kind, int measflag, float* accept, bool renorm) {
+  int rc = enqueue(c, {kind}, measflag, renorm);
+  if (rc) return rc;
+  if (!accept) return LCE_OK;
+  rc = status_check(c);
+  if (rc) return rc;
+  lce_meas m;
+  CK(cudaMemcpy(&m, c->meas_d, sizeof(m), cudaMemcpyDeviceToHost));
+  switch (kind) {
+    case kHiggsHB: *accept = (float)m.acc_hb; break;
+    case kHiggsOR: *accept = (float)m.acc_or; break;
+    case kHiggsMetro: *accept = (float)m.acc_metro; break;
+    case kLinkHB: *accept = (float)m.acc_gauge; break;
+    default: *accept = (float)m.acc_link_or; break;
+  }
+  return LCE_OK;
+}
+
+int ensure_staging(lce_ctx* c, size_t bytes) {
+  if (c->staging_bytes >= bytes) return LCE_OK;
+  if (c->staging_d) CK(cudaFree(c->staging_d));
+  c->staging_d = nullptr;
+  c->staging_bytes = 0;
+  CK(cudaMalloc(&c->staging_d, bytes));
+  c->staging_bytes = bytes;
+  return LCE_OK;
+}
+
+void* field_ptr(const ChainDev& ch, int which, bool links) {
+  if (which == LCE_FIELDS) return links ? ch.u : ch.a;
+  return links ? ch.uf : ch.af;
+}
+
+template <typename Rin>
+int upload_t(lce_ctx* c, int chain, int which, const Rin* u, const Rin* a, long ld) {
+  if (chain < 0 || chain >= c->nchains || (which != LCE_FIELDS && which != LCE_FIELDS_FIXED))
+    return fail(c, LCE_ERR_INVALID, "upload: bad chain or field selector");
+  const ChainDev& ch = c->ch[chain];
+  if (ld < ch.nh) return fail(c, LCE_ERR_INVALID, "upload: ld smaller than L1*L2*L3/2");
+  const int nh = ch.nh;
+  if (u) {
+    void* dst = field_ptr(ch, which, true);
+    const bool direct = (sizeof(Rin) == real_bytes(c->prec));
+    if (direct) {
+      CK(cudaMemcpy2DAsync(dst, (size_t)nh * 4 * sizeof(Rin), u, (size_t)ld * 4 * sizeof(Rin),
+                           (size_t)nh * 4 * sizeof(Rin), 6, cudaMemcpyHostToDevice, c->stream));
+    } else {
+      int rc = ensure_staging(c, (size_t)6 * c->max_nh * 4 * sizeof(double));
+      if (rc) return rc;
+      CK(cudaMemcpy2DAsync(c->staging_d, (size_t)nh * 4 * sizeof(Rin), u, (size_t)ld * 4 * sizeof(Rin),
+                           (size_t)nh * 4 * sizeof(Rin), 6, cudaMemcpyHostToDevice, c->stream));
+      if (c->prec == LCE_PREC_F64) launch_links_in<Rin, double>((const Rin*)c->staging_d, dst, nh, c->stream);
+      else launch_links_in<Rin, float>((const Rin*)c->staging_d, dst, nh, c->stream);
+    }
+  }
+  if (a) {
+    void* dst = field_ptr(ch, which, false);
+    int rc = ensure_staging(c, (size_t)6 * c->max_nh * 4 * sizeof(double));
+    if (rc) return rc;
+    CK(cudaMemcpy2DAsync(c->staging_d, (size_t)nh * 3 * sizeof(Rin), a, (size_t)ld * 3 * sizeof(Rin),
+                         (size_t)nh * 3 * sizeof(Rin), 2, cudaMemcpyHostToDevice, c->stream));
+    if (c->prec == LCE_PREC_F64) launch_higgs_in<Rin, double>((const Rin*)c->staging_d, dst, nh, c->stream);
+    else launch_higgs_in<Rin, float>((const Rin*)c->staging_d, dst, nh, c->stream);
+  }
+  CK(cudaGetLastError());
+  CK(cudaStreamSynchronize(c->stream));
+  return LCE_OK;
+}
+
+template <typename Rout>
+int download_t(lce_ctx* c, int chain, int which, Rout* u, Rout* a, long ld) {
+  if (chain < 0 || chain >= c->nchains || (which != LCE_FIELDS && which != LCE_FIELDS_FIXED))
+    return fail(c, LCE_ERR_INVALID, "download: bad chain or field selector");
+  const ChainDev& ch = c->ch[chain];
+  if (ld < ch.nh) return fail(c, LCE_ERR_INVALID, "download: ld smaller than L1*L2*L3/2");
+  const int nh = ch.nh;
+  if (u) {
+    const void* src = field_ptr(ch, which, true);
+    if (sizeof(Rout) == real_bytes(c->prec)) {
+      CK(cudaMemcpy2DAsync(u, (size_t)ld * 4 * sizeof(Rout), src, (size_t)nh * 4 * sizeof(Rout),
+                           (size_t)nh * 4 * sizeof(Rout), 6, cudaMemcpyDeviceToHost, c->stream));
+    } else {
+      int rc = ensure_staging(c, (size_t)6 * c->max_nh * 4 * sizeof(double));
+      if (rc) return rc;
+      if (c->prec == LCE_PREC_F64) launch_links_out<double, Rout>(src, (Rout*)c->staging_d, nh, c->stream);
+      else launch_links_out<float, Rout>(src, (Rout*)c->staging_d, nh, c->stream);
+      CK(cudaMemcpy2DAsync(u, (size_t)ld * 4 * sizeof(Rout), c->staging_d, (size_t)nh * 4 * sizeof(Rout),
+                           (size_t)nh * 4 * sizeof(Rout), 6, cudaMemcpyDeviceToHost, c->stream));
+    }
+  }
+  if (a) {
+    const void* src = field_ptr(ch, which, false);
+    int rc = ensure_staging(c, (size_t)6 * c->max_nh * 4 * sizeof(double));
+    if (rc) return rc;
+    if (c->prec == LCE_PREC_F64) launch_higgs_out<double, Rout>(src, (Rout*)c->staging_d, nh, c->stream);
+    else launch_higgs_out<float, Rout>(src, (Rout*)c->staging_d, nh, c->stream);
+    CK(cudaMemcpy2DAsync(a, (size_t)ld * 3 * sizeof(Rout), c->staging_d, (size_t)nh * 3 * sizeof(Rout),
+                         (size_t)nh * 3 * sizeof(Rout), 2, cudaMemcpyDeviceToHost, c->stream));
+  }
+  CK(cudaGetLastError());
+  CK(cudaStreamSynchronize(c->stream));
+  return LCE_OK;
+}
+
+int set_device(lce_ctx* c) {
+  CK(cudaSetDevice(c->device));
+  return LCE_OK;
+}
+
+lce_ctx* create_impl(const lce_params* p, int n) {
+  g_create_error.clear();
+  if (!p || n < 1) {
+    fail(nullptr, LCE_ERR_INVALID, "create: null params or no chains");
+    return nullptr;
+  }
+  for (int i = 0; i < n; ++i) {
+    std::string why;
+    if (!valid_params(p[i], why)) {
+      fail(nullptr, LCE_ERR_INVALID, "create: chain " + std::to_string(i) + ": " + why);
+      return nullptr;
+    }
+    if (p[i].precision != p[0].precision || p[i].rng != p[0].rng || p[i].device != p[0].device ||
+        p[i].n_link_or != p[0].n_link_or || p[i].n_higgs_metro != p[0].n_higgs_metro) {
+      fail(nullptr, LCE_ERR_INVALID, "create: chains of a batch must share precision, rng, device and composition");
+      return nullptr;
+    }
+  }
+  if (n > 1 && p[0].rng == LCE_RNG_STREAM) {
+    fail(nullptr, LCE_ERR_UNSUPPORTED, "create: validation streams need a single-chain context");
+    return nullptr;
+  }
+  lce_ctx* c = new lce_ctx();
+  c->device = p[0].device;
+  c->prec = p[0].precision;
+  c->rng = p[0].rng;
+  c->nchains = n;
+  c->n_link_or = p[0].n_link_or;
+  c->n_higgs_metro = p[0].n_higgs_metro;
+  c->params.assign(p, p + n);
+  auto bail = [&](cudaError_t e, const char* where) -> lce_ctx* {
+    g_create_error = std::string(where) + ": " + cudaGetErrorString(e);
+    lce_destroy(c);
+    return nullptr;
+  };
+  cudaError_t e = cudaSetDevice(c->device);
+  if (e != cudaSuccess) return bail(e, "cudaSetDevice");
+  e = cudaStreamCreateWithFlags(&c->own, cudaStreamNonBlocking);
+  if (e != cudaSuccess) return bail(e, "cudaStreamCreate");
+  c->stream = c->own;
+  if ((e = cudaEventCreate(&c->ev0)) != cudaSuccess) return bail(e, "cudaEventCreate");
+  if ((e = cudaEventCreate(&c->ev1)) != cudaSuccess) return bail(e, "cudaEventCreate");
+
+  // chain table and field layout
+  const size_t lb = link_bytes(c->prec), rb = real_bytes(c->prec);
+  size_t off = 0;
+  std::vector<size_t> offs;
+  c->blk.assign(1, 0);
+  for (int i = 0; i < n; ++i) {
+    ChainDev d;
+    std::memset(&d, 0, sizeof(d));
+    d.L1 = p[i].L[0];
+    d.L2 = p[i].L[1];
+    d.L3 = p[i].L[2];
+    d.hx = d.L1 / 2;
+    d.nxy = d.L1 * d.L2 / 2;
+    d.nh = d.nxy * d.L3;
+    d.dhx = make_fastdiv((uint32_t)d.hx);
+    d.dnxy = make_fastdiv((uint32_t)d.nxy);
+    double cp[3];
+    lce_couplings(&p[i], cp);
+    if (c->prec == LCE_PREC_F32) {
+      d.beta = (float)p[i].beta;
+      d.lambda = (float)p[i].lambda;
+      d.alpha = (float)p[i].alpha;
+      d.limit_or = (float)p[i].limit_or;
+    } else {
+      d.beta = p[i].beta;
+      d.lambda = p[i].lambda;
+      d.alpha = p[i].alpha;
+      d.limit_or = p[i].limit_or;
+    }
+    d.beta_a = cp[0];
+    d.beta_2 = cp[1];
+    d.beta_4 = cp[2];
+    d.imode = p[i].imode;
+    d.gf_angle = p[i].gf_angle;
+    d.key0 = (uint32_t)p[i].seed;
+    d.key1 = (uint32_t)(p[i].seed >> 32);
+    offs.push_back(off);
+    off += 2 * (align256((size_t)6 * d.nh * lb) + align256((size_t)6 * d.nh * rb));
+    c->ch.push_back(d);
+    c->blk.push_back(c->blk.back() + ceil_div(d.nh, kBlock));
+    c->max_nh = std::max(c->max_nh, d.nh);
+    c->max_L3 = std::max(c->max_L3, d.L3);
+  }
+  if ((e = cudaMalloc(&c->fields_d, off)) != cudaSuccess) return bail(e, "cudaMalloc(fields)");
+  for (int i = 0; i < n; ++i) {
+    char* b = (char*)c->fields_d + offs[i];
+    ChainDev& d = c->ch[i];
+    const size_t ul = align256((size_t)6 * d.nh * lb), al = align256((size_t)6 * d.nh * rb);
+    d.u = b;
+    d.a = b + ul;
+    d.uf = b + ul + al;
+    d.af = b + 2 * ul + al;
+  }
+  if ((e = cudaMemset(c->fields_d, 0, off)) != cudaSuccess) return bail(e, "cudaMemset(fields)");
+  if ((e = cudaMalloc(&c->ch_d, sizeof(ChainDev) * n)) != cudaSuccess) return bail(e, "cudaMalloc(chains)");
+  if ((e = cudaMemcpy(c->ch_d, c->ch.data(), sizeof(ChainDev) * n, cudaMemcpyHostToDevice)) != cudaSuccess)
+    return bail(e, "cudaMemcpy(chains)");
+  if ((e = cudaMalloc(&c->blk_d, sizeof(int) * (n + 1))) != cudaSuccess) return bail(e, "cudaMalloc(blk)");
+  if ((e = cudaMemcpy(c->blk_d, c->blk.data(), sizeof(int) * (n + 1), cudaMemcpyHostToDevice)) != cudaSuccess)
+    return bail(e, "cudaMemcpy(blk)");
+  if ((e = cudaMalloc(&c->st_d, sizeof(CtxState))) != cudaSuccess) return bail(e, "cudaMalloc(state)");
+  if ((e = cudaMemset(c->st_d, 0, sizeof(CtxState))) != cudaSuccess) return bail(e, "cudaMemset(state)");
+  if ((e = cudaMalloc(&c->cst_d, sizeof(ChainState) * n)) != cudaSuccess) return bail(e, "cudaMalloc(cstate)");
+  {
+    std::vector<ChainState> cs(n);
+    for (int i = 0; i < n; ++i) {
+      std::memset(&cs[i], 0, sizeof(ChainState));
+      cs[i].delta = p[i].delta0;
+    }
+    if ((e = cudaMemcpy(c->cst_d, cs.data(), sizeof(ChainState) * n, cudaMemcpyHostToDevice)) != cudaSuccess)
+      return bail(e, "cudaMemcpy(cstate)");
+  }
+  if ((e = cudaMalloc(&c->meas_d, sizeof(lce_meas) * n)) != cudaSuccess) return bail(e, "cudaMalloc(meas)");
+  if ((e = cudaMemset(c->meas_d, 0, sizeof(lce_meas) * n)) != cudaSuccess) return bail(e, "cudaMemset(meas)");
+  c->part_slots = std::max(6, 4 + 6 + 2 * c->n_higgs_metro + 6 * c->n_link_or);
+  c->slot_stride = (size_t)c->blk.back() * kNQ;
+  if ((e = cudaMalloc(&c->part_d, sizeof(double) * c->slot_stride * c->part_slots)) != cudaSuccess)
+    return bail(e, "cudaMalloc(partials)");
+  if ((e = cudaMalloc(&c->totals_d, sizeof(double) * (size_t)n * kMaxSlots * kNQ)) != cudaSuccess)
+    return bail(e, "cudaMalloc(totals)");
+  c->scratch_n = (size_t)2 * ceil_div(2L * c->max_nh, 256) + (size_t)32 * c->max_L3 + 64;
+  if ((e = cudaMalloc(&c->scratch_d, sizeof(double) * c->scratch_n)) != cudaSuccess)
+    return bail(e, "cudaMalloc(scratch)");
+  if (c->max_L3 * 14 * sizeof(double) > 48 * 1024) {
+    // correlator kernel stages the slice sums in shared memory
+    if (c->max_L3 * 14 * sizeof(double) > 200 * 1024) {
+      g_create_error = "create: L3 too large for the correlator kernel";
+      lce_destroy(c);
+      return nullptr;
+    }
+  }
+  return c;
+}
+
+int get_slices(lce_ctx* c, int chain, double*& out) {
+  const ChainDev& ch = c->ch[chain];
+  double* slices = c->scratch_d;
+  out = c->scratch_d + (size_t)14 * ch.L3;
+  if (c->prec == LCE_PREC_F64) launch_slice_sums<double>(c->ch_d + chain, ch.L3, slices, c->stream);
+  else launch_slice_sums<float>(c->ch_d + chain, ch.L3, slices, c->stream);
+  launch_correlators(slices, ch.L1, ch.L2, ch.L3, out, c->stream);
+  CK(cudaGetLastError());
+  return LCE_OK;
+}
+
+int gf_loop(lce_ctx* c, int chain, double* theta, int* iters, int max_iters) {
+  const ChainDev& ch = c->ch[chain];
+  // bounded on the device in every case; no cap requested means 10^6
+  const int cap = max_iters > 0 ? max_iters : 1000000;
+  ChainState cs;
+  CK(cudaMemcpyAsync(&cs, c->cst_d + chain, sizeof(cs), cudaMemcpyDeviceToHost, c->stream));
+  CK(cudaStreamSynchronize(c->stream));
+  cs.gf_done = 0;
+  cs.gf_iters = 0;
+  cs.gf_cap = cap;
+  cs.gf_theta = 1.0e4;
+  CK(cudaMemcpyAsync(c->cst_d + chain, &cs, sizeof(cs), cudaMemcpyHostToDevice, c->stream));
+  CK(cudaStreamSynchronize(c->stream));
+  double* part = c->scratch_d;
+  int batch = 8;
+  while (true) {
+    auto key = std::make_pair(chain, batch);
+    auto it = c->gf_exec.find(key);
+    if (it == c->gf_exec.end()) {
+      cudaGraph_t g;
+      CK(cudaStreamBeginCapture(c->stream, cudaStreamCaptureModeThreadLocal));
+      for (int k = 0; k < batch; ++k) {
+        if (c->prec == LCE_PREC_F64)
+          launch_gf_iteration<double>(c->ch_d + chain, c->cst_d + chain, chain, part, ch.nh, c->stream);
+        else
+          launch_gf_iteration<float>(c->ch_d + chain, c->cst_d + chain, chain, part, ch.nh, c->stream);
+      }
+      CK(cudaStreamEndCapture(c->stream, &g));
+      cudaGraphExec_t ex;
+      cudaError_t e = cudaGraphInstantiate(&ex, g, 0);
+      cudaGraphDestroy(g);
+      if (e != cudaSuccess) return cuda_fail(c, e, "cudaGraphInstantiate(gauge fixing)");
+      it = c->gf_exec.emplace(key, ex).first;
+    }
+    CK(cudaGraphLaunch(it->second, c->stream));
+    CK(cudaMemcpyAsync(&cs, c->cst_d + chain, sizeof(cs), cudaMemcpyDeviceToHost, c->stream));
+    CK(cudaStreamSynchronize(c->stream));
+    if (cs.gf_done) break;
+    if (batch < 256) batch *= 2;
+  }
+  if (theta) *theta = cs.gf_theta;
+  if (iters) *iters = cs.gf_iters;
+  if (!std::isfinite(cs.gf_theta)) return fail(c, LCE_ERR_NAN, "gauge fixing: theta is not finite");
+  if (cs.gf_theta > ch.limit_or) return fail(c, LCE_ERR_GF_NOT_CONVERGED, "gauge fixing: iteration cap reached");
+  return LCE_OK;
+}
+
+}  // namespace
+
+// ====================================================================== C ABI
+extern "C" {
+
+const char* lce_version(void) { return "lceqcd_b200 1.0 (sm_100a)"; }
+
+const char* lce_strerror(int s) {
+  switch (s) {
+    case LCE_OK: return "ok";
+    case LCE_ERR_INVALID: return "invalid argument";
+    case LCE_ERR_CUDA: return "CUDA error";
+    case LCE_ERR_GF_NOT_CONVERGED: return "gauge fixing did not converge";
+    case LCE_ERR_STREAM: return "validation uniform stream exhausted";
+    case LCE_ERR_NAN: return "non-finite value";
+    case LCE_ERR_NOMEM: return "out of device memory";
+    case LCE_ERR_UNSUPPORTED: return "unsupported for this context";
+    default: return "unknown status";
+  }
+}
+
+const char* lce_last_error(lce_ctx* c) { return c ? c->err.c_str() : g_create_error.c_str(); }
+
+void lce_default_params(lce_params* p) {
+  std::memset(p, 0, sizeof(*p));
+  p->L[0] = p->L[1] = p->L[2] = 16;
+  p->beta = 9.0;
+  p->x = 0.1;
+  p->y = 0.5;
+  p->lambda = 1.8;
+  p->alpha = 1.0;
+  p->limit_or = 1.0e-9;
+  p->imode = 0;
+  p->precision = LCE_PREC_F32;
+  p->rng = LCE_RNG_PHILOX;
+  p->seed = 12345;
+  p->device = 0;
+  p->delta0 = 1.0;
+  p->gf_angle = LCE_GF_ATAN2;
+}
+
+int lce_couplings(const lce_params* p, double out[3]) {
+  if (!p || !out) return LCE_ERR_INVALID;
+  if (p->precision == LCE_PREC_F32) couplings_t<float>(p->beta, p->x, p->y, out);
+  else couplings_t<double>(p->beta, p->x, p->y, out);
+  return LCE_OK;
+}
+
+int lce_geometry_tables(int L1, int L2, int L3, int* siteup, int* sitedn) {
+  if (L1 < 2 || L2 < 2 || L3 < 2 || (L1 | L2 | L3) & 1 || !siteup || !sitedn) return LCE_ERR_INVALID;
+  const int hx = L1 / 2, nxy = L1 * L2 / 2, nh = nxy * L3;
+  const FastDiv dhx = make_fastdiv(hx), dnxy = make_fastdiv(nxy);
+  const int L[3] = {L1, L2, L3};
+  for (int eo = 0; eo < 2; ++eo)
+    for (int s = 0; s < nh; ++s) {
+      Coord X = site_coord(eo, s, hx, nxy, dhx, dnxy);
+      for (int mu = 0; mu < 3; ++mu) {
+        int cu[3] = {X.x, X.y, X.z}, cd[3] = {X.x, X.y, X.z};
+        cu[mu] = wrap(cu[mu] + 1, L[mu]);
+        cd[mu] = wrap(cd[mu] - 1, L[mu]);
+        siteup[((size_t)eo * 3 + mu) * nh + s] = site_index(cu[0], cu[1], cu[2], hx, nxy);
+        sitedn[((size_t)eo * 3 + mu) * nh + s] = site_index(cd[0], cd[1], cd[2], hx, nxy);
+      }
+    }
+  return LCE_OK;
+}
+
+lce_ctx* lce_create(const lce_params* p) { return create_impl(p, 1); }
+lce_ctx* lce_create_batch(const lce_params* p, int nchains) { return create_impl(p, nchains); }
+
+void lce_destroy(lce_ctx* c) {
+  if (!c) return;
+  cudaSetDevice(c->device);
+  if (c->stream) cudaStreamSynchronize(c->stream);
+  for (int i = 0; i < 2; ++i)
+    if (c->sweep_exec[i]) cudaGraphExecDestroy(c->sweep_exec[i]);
+  for (auto& kv : c->gf_exec) cudaGraphExecDestroy(kv.second);
+  void* ptrs[] = {c->ch_d, c->blk_d, c->st_d, c->cst_d, c->meas_d, c->part_d, c->totals_d,
+                  c->scratch_d, c->fields_d, c->stream_d, c->staging_d, c->flush_d};
+  for (void* q : ptrs)
+    if (q) cudaFree(q);
+  if (c->ev0) cudaEventDestroy(c->ev0);
+  if (c->ev1) cudaEventDestroy(c->ev1);
+  if (c->own) cudaStreamDestroy(c->own);
+  delete c;
+}
+
+int lce_nchains(lce_ctx* c) { return c ? c->nchains : LCE_ERR_INVALID; }
+
+int lce_set_stream(lce_ctx* c, void* s) {
+  if (!c) return LCE_ERR_INVALID;
+  c->stream = s ? (cudaStream_t)s : c->own;
+  return LCE_OK;
+}
+
+int lce_synchronize(lce_ctx* c) {
+  if (!c) return LCE_ERR_INVALID;
+  CK(cudaStreamSynchronize(c->stream));
+  return status_check(c);
+}
+
+int lce_upload(lce_ctx* c, int chain, int which, const float* u, const float* a, long ld) {
+  if (!c) return LCE_ERR_INVALID;
+  return upload_t<float>(c, chain, which, u, a, ld);
+}
+int lce_upload_f64(lce_ctx* c, int chain, int which, const double* u, const double* a, long ld) {
+  if (!c) return LCE_ERR_INVALID;
+  return upload_t<double>(c, chain, which, u, a, ld);
+}
+int lce_download(lce_ctx* c, int chain, int which, float* u, float* a, long ld) {
+  if (!c) return LCE_ERR_INVALID;
+  return download_t<float>(c, chain, which, u, a, ld);
+}
+int lce_download_f64(lce_ctx* c, int chain, int which, double* u, double* a, long ld) {
+  if (!c) return LCE_ERR_INVALID;
+  return download_t<double>(c, chain, which, u, a, ld);
+}
+
+int lce_init_unit(lce_ctx* c, double a3) {
+  if (!c) return LCE_ERR_INVALID;
+  for (int i = 0; i < c->nchains; ++i) {
+    if (c->prec == LCE_PREC_F64) launch_init_unit<double>(c->ch[i].u, c->ch[i].a, c->ch[i].nh, a3, c->stream);
+    else launch_init_unit<float>(c->ch[i].u, c->ch[i].a, c->ch[i].nh, a3, c->stream);
+  }
+  CK(cudaGetLastError());
+  return LCE_OK;
+}
+
+int lce_init_hot(lce_ctx* c, unsigned long long seed) {
+  if (!c) return LCE_ERR_INVALID;
+  for (int i = 0; i < c->nchains; ++i) {
+    const unsigned long long k = seed + 0x9E3779B97F4A7C15ull * (unsigned long long)i;
+    const uint32_t k0 = (uint32_t)k, k1 = (uint32_t)(k >> 32);
+    if (c->prec == LCE_PREC_F64) launch_init_hot<double>(c->ch[i].u, c->ch[i].a, c->ch[i].nh, k0, k1, c->stream);
+    else launch_init_hot<float>(c->ch[i].u, c->ch[i].a, c->ch[i].nh, k0, k1, c->stream);
+  }
+  CK(cudaGetLastError());
+  return LCE_OK;
+}
+
+int lce_set_rng_stream(lce_ctx* c, const double* u, size_t n) {
+  if (!c || (!u && n)) return LCE_ERR_INVALID;
+  if (c->rng != LCE_RNG_STREAM) return fail(c, LCE_ERR_UNSUPPORTED, "context was not created with LCE_RNG_STREAM");
+  CK(cudaStreamSynchronize(c->stream));
+  if (c->stream_d) CK(cudaFree(c->stream_d));
+  c->stream_d = nullptr;
+  c->stream_n = 0;
+  if (n) {
+    CK(cudaMalloc(&c->stream_d, n * sizeof(double)));
+    CK(cudaMemcpy(c->stream_d, u, n * sizeof(double), cudaMemcpyHostToDevice));
+  }
+  c->stream_n = n;
+  // graphs captured the old stream pointer
+  for (int i = 0; i < 2; ++i)
+    if (c->sweep_exec[i]) {
+      cudaGraphExecDestroy(c->sweep_exec[i]);
+      c->sweep_exec[i] = nullptr;
+    }
+  unsigned long long z = 0;
+  CK(cudaMemcpy(&c->st_d->stream_pos, &z, sizeof(z), cudaMemcpyHostToDevice));
+  return LCE_OK;
+}
+
+int lce_get_rng_position(lce_ctx* c, unsigned long long* pass_ctr, unsigned long long* stream_pos) {
+  if (!c) return LCE_ERR_INVALID;
+  CtxState st;
+  CK(cudaMemcpyAsync(&st, c->st_d, sizeof(st), cudaMemcpyDeviceToHost, c->stream));
+  CK(cudaStreamSynchronize(c->stream));
+  if (pass_ctr) *pass_ctr = st.pass_ctr;
+  if (stream_pos) *stream_pos = st.stream_pos;
+  return LCE_OK;
+}
+
+int lce_set_rng_position(lce_ctx* c, unsigned long long pass_ctr, unsigned long long stream_pos) {
+  if (!c) return LCE_ERR_INVALID;
+  CK(cudaStreamSynchronize(c->stream));
+  CK(cudaMemcpy(&c->st_d->pass_ctr, &pass_ctr, sizeof(pass_ctr), cudaMemcpyHostToDevice));
+  CK(cudaMemcpy(&c->st_d->stream_pos, &stream_pos, sizeof(stream_pos), cudaMemcpyHostToDevice));
+  return LCE_OK;
+}
+
+int lce_ahiggs1(lce_ctx* c, float* delta, int measflag, float* accept) {
+  if (!c) return LCE_ERR_INVALID;
+  if (delta) {
+    // the step lives on the device; the caller's value is the one to use
+    CK(cudaStreamSynchronize(c->stream));
+    for (int i = 0; i < c->nchains; ++i) {
+      double d = *delta;
+      CK(cudaMemcpy(&c->cst_d[i].delta, &d, sizeof(d), cudaMemcpyHostToDevice));
+    }
+  }
+  float acc = 0;
+  int rc = routine_call(c, kHiggsMetro, measflag, (accept || delta) ? &acc : nullptr, false);
+  if (rc) return rc;
+  if (accept) *accept = acc;
+  if (delta) {
+    double d;
+    CK(cudaMemcpy(&d, &c->cst_d[0].delta, sizeof(d), cudaMemcpyDeviceToHost));
+    *delta = (float)d;
+  }
+  return LCE_OK;
+}
+
+int lce_ahiggs2(lce_ctx* c, int measflag, float* accept) {
+  return c ? routine_call(c, kHiggsHB, measflag, accept, false) : LCE_ERR_INVALID;
+}
+int lce_ahiggs3(lce_ctx* c, int measflag, float* accept) {
+  return c ? routine_call(c, kHiggsOR, measflag, accept, false) : LCE_ERR_INVALID;
+}
+int lce_agauge(lce_ctx* c, int measflag, float* accept) {
+  return c ? routine_call(c, kLinkHB, measflag, accept, false) : LCE_ERR_INVALID;
+}
+int lce_link_or(lce_ctx* c, int measflag, float* accept) {
+  return c ? routine_call(c, kLinkOR, measflag, accept, false) : LCE_ERR_INVALID;
+}
+
+int lce_renorm(lce_ctx* c) {
+  if (!c) return LCE_ERR_INVALID;
+  for (int i = 0; i < c->nchains; ++i) {
+    if (c->prec == LCE_PREC_F64) launch_renorm<double>(c->ch[i].u, (size_t)6 * c->ch[i].nh, c->stream);
+    else launch_renorm<float>(c->ch[i].u, (size_t)6 * c->ch[i].nh, c->stream);
+  }
+  CK(cudaGetLastError());
+  return LCE_OK;
+}
+
+int lce_sweeps(lce_ctx* c, int nsweeps, int measflag) {
+  if (!c || nsweeps < 0) return LCE_ERR_INVALID;
+  const int mf = measflag == 1 ? 1 : 0;
+  if (!c->sweep_exec[mf]) {
+    cudaGraph_t g;
+    CK(cudaStreamBeginCapture(c->stream, cudaStreamCaptureModeThreadLocal));
+    int rc = enqueue(c, sweep_routines(c), mf, true);
+    cudaError_t e = cudaStreamEndCapture(c->stream, &g);
+    if (rc) {
+      if (e == cudaSuccess) cudaGraphDestroy(g);
+      return rc;
+    }
+    if (e != cudaSuccess) return cuda_fail(c, e, "cudaStreamEndCapture(sweep)");
+    e = cudaGraphInstantiate(&c->sweep_exec[mf], g, 0);
+    cudaGraphDestroy(g);
+    if (e != cudaSuccess) return cuda_fail(c, e, "cudaGraphInstantiate(sweep)");
+  }
+  for (int i = 0; i < nsweeps; ++i) CK(cudaGraphLaunch(c->sweep_exec[mf], c->stream));
+  return LCE_OK;
+}
+
+int lce_sweep(lce_ctx* c, int measflag, lce_meas* m) {
+  int rc = lce_sweeps(c, 1, measflag);
+  if (rc || !m) return rc;
+  return lce_get_meas(c, 0, m);
+}
+
+int lce_get_meas(lce_ctx* c, int chain, lce_meas* m) {
+  if (!c || !m || chain < 0 || chain >= c->nchains) return LCE_ERR_INVALID;
+  CK(cudaMemcpyAsync(m, c->meas_d + chain, sizeof(*m), cudaMemcpyDeviceToHost, c->stream));
+  int rc = status_check(c);
+  if (rc) return rc;
+  return LCE_OK;
+}
+
+int lce_get_meas_batch(lce_ctx* c, lce_meas* m) {
+  if (!c || !m) return LCE_ERR_INVALID;
+  CK(cudaMemcpyAsync(m, c->meas_d, sizeof(lce_meas) * c->nchains, cudaMemcpyDeviceToHost, c->stream));
+  return status_check(c);
+}
+
+int lce_landau_gauge(lce_ctx* c, int chain, double* theta, int* iters, int max_iters) {
+  if (!c || chain < 0 || chain >= c->nchains) return LCE_ERR_INVALID;
+  const ChainDev& ch = c->ch[chain];
+  // f/landau_gauge.f:308-324 copy u -> u_f, a -> a_f
+  const size_t ub = (size_t)6 * ch.nh * link_bytes(c->prec), ab = (size_t)6 * ch.nh * real_bytes(c->prec);
+  CK(cudaMemcpyAsync(ch.uf, ch.u, ub, cudaMemcpyDeviceToDevice, c->stream));
+  CK(cudaMemcpyAsync(ch.af, ch.a, ab, cudaMemcpyDeviceToDevice, c->stream));
+  return gf_loop(c, chain, theta, iters, max_iters);
+}
+
+int lce_gauge_fix_continue(lce_ctx* c, int chain, double* theta, int* iters, int max_iters) {
+  if (!c || chain < 0 || chain >= c->nchains) return LCE_ERR_INVALID;
+  return gf_loop(c, chain, theta, iters, max_iters);
+}
+
+int lce_gauge_functional(lce_ctx* c, int chain, double* value) {
+  if (!c || !value || chain < 0 || chain >= c->nchains) return LCE_ERR_INVALID;
+  const ChainDev& ch = c->ch[chain];
+  const int nb = ceil_div(2L * ch.nh, 256);
+  double* part = c->scratch_d;
+  double* out = c->scratch_d + nb;
+  if (c->prec == LCE_PREC_F64) launch_functional<double>(c->ch_d + chain, part, ch.nh, c->stream);
+  else launch_functional<float>(c->ch_d + chain, part, ch.nh, c->stream);
+  launch_sum_partials(part, nb, 1, out, c->stream);
+  CK(cudaGetLastError());
+  double s;
+  CK(cudaMemcpyAsync(&s, out, sizeof(s), cudaMemcpyDeviceToHost, c->stream));
+  CK(cudaStreamSynchronize(c->stream));
+  *value = s / ((2.0 + ch.alpha) * 2.0 * ch.nh);
+  return LCE_OK;
+}
+
+int lce_theta(lce_ctx* c, int chain, double* theta) {
+  if (!c || !theta || chain < 0 || chain >= c->nchains) return LCE_ERR_INVALID;
+  const ChainDev& ch = c->ch[chain];
+  const int nb = ceil_div(ch.nh, kBlock);
+  double* part = c->scratch_d;
+  double* out = c->scratch_d + nb;
+  if (c->prec == LCE_PREC_F64) launch_gf_theta<double>(c->ch_d + chain, part, ch.nh, c->stream);
+  else launch_gf_theta<float>(c->ch_d + chain, part, ch.nh, c->stream);
+  launch_sum_partials(part, nb, 1, out, c->stream);
+  CK(cudaGetLastError());
+  double s;
+  CK(cudaMemcpyAsync(&s, out, sizeof(s), cudaMemcpyDeviceToHost, c->stream));
+  CK(cudaStreamSynchronize(c->stream));
+  *theta = s / ch.nh;
+  return LCE_OK;
+}
+
+int lce_correlator(lce_ctx* c, int chain, double* corr_a, double* corr_u, double* corr_3, double af[3]) {
+  if (!c || chain < 0 || chain >= c->nchains) return LCE_ERR_INVALID;
+  const int L3 = c->ch[chain].L3;
+  double* out;
+  int rc = get_slices(c, chain, out);
+  if (rc) return rc;
+  std::vector<double> h((size_t)7 * L3 + 5);
+  CK(cudaMemcpyAsync(h.data(), out, h.size() * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+  CK(cudaStreamSynchronize(c->stream));
+  if (corr_a) std::memcpy(corr_a, h.data(), L3 * sizeof(double));
+  if (corr_u) std::memcpy(corr_u, h.data() + L3, L3 * sizeof(double));
+  if (corr_3) std::memcpy(corr_3, h.data() + 2 * L3, L3 * sizeof(double));
+  if (af) std::memcpy(af, h.data() + 7 * L3, 3 * sizeof(double));
+  return LCE_OK;
+}
+
+int lce_polyakov(lce_ctx* c, int chain, double* slice, double* corr, double* mean2) {
+  if (!c || chain < 0 || chain >= c->nchains) return LCE_ERR_INVALID;
+  const int L3 = c->ch[chain].L3;
+  double* out;
+  int rc = get_slices(c, chain, out);
+  if (rc) return rc;
+  std::vector<double> h((size_t)7 * L3 + 5);
+  CK(cudaMemcpyAsync(h.data(), out, h.size() * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+  CK(cudaStreamSynchronize(c->stream));
+  if (slice) std::memcpy(slice, h.data() + 3 * L3, L3 * sizeof(double));
+  if (corr) std::memcpy(corr, h.data() + 4 * L3, L3 * sizeof(double));
+  if (mean2) *mean2 = h[7 * L3 + 3];
+  return LCE_OK;
+}
+
+int lce_scalarcorr(lce_ctx* c, int chain, double* slice, double* corr, double* mean) {
+  if (!c || chain < 0 || chain >= c->nchains) return LCE_ERR_INVALID;
+  const int L3 = c->ch[chain].L3;
+  double* out;
+  int rc = get_slices(c, chain, out);
+  if (rc) return rc;
+  std::vector<double> h((size_t)7 * L3 + 5);
+  CK(cudaMemcpyAsync(h.data(), out, h.size() * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+  CK(cudaStreamSynchronize(c->stream));
+  if (slice) std::memcpy(slice, h.data() + 5 * L3, L3 * sizeof(double));
+  if (corr) std::memcpy(corr, h.data() + 6 * L3, L3 * sizeof(double));
+  if (mean) *mean = h[7 * L3 + 4];
+  return LCE_OK;
+}
+
+int lce_plaquette(lce_ctx* c, int chain, double* plaq) {
+  if (!c || !plaq || chain < 0 || chain >= c->nchains) return LCE_ERR_INVALID;
+  const ChainDev& ch = c->ch[chain];
+  const int nb = ceil_div(2L * ch.nh, 256);
+  double* part = c->scratch_d;
+  double* out = c->scratch_d + nb;
+  if (c->prec == LCE_PREC_F64) launch_plaquette<double>(c->ch_d + chain, part, ch.nh, c->stream);
+  else launch_plaquette<float>(c->ch_d + chain, part, ch.nh, c->stream);
+  launch_sum_partials(part, nb, 1, out, c->stream);
+  CK(cudaGetLastError());
+  double s;
+  CK(cudaMemcpyAsync(&s, out, sizeof(s), cudaMemcpyDeviceToHost, c->stream));
+  CK(cudaStreamSynchronize(c->stream));
+  *plaq = s / (3.0 * 2.0 * ch.nh);
+  return LCE_OK;
+}
+
+int lce_debug_staple(lce_ctx* c, int eo, int mu, double* out) {
+  if (!c || !out || eo < 0 || eo > 1 || mu < 0 || mu > 2) return LCE_ERR_INVALID;
+  const int nh = c->ch[0].nh;
+  int rc = ensure_staging(c, (size_t)nh * 4 * sizeof(double));
+  if (rc) return rc;
+  if (c->prec == LCE_PREC_F64) launch_debug_staple<double>(c->ch_d, eo, mu, (double*)c->staging_d, nh, c->stream);
+  else launch_debug_staple<float>(c->ch_d, eo, mu, (double*)c->staging_d, nh, c->stream);
+  CK(cudaGetLastError());
+  CK(cudaMemcpyAsync(out, c->staging_d, (size_t)nh * 4 * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+  CK(cudaStreamSynchronize(c->stream));
+  return LCE_OK;
+}
+
+int lce_debug_force(lce_ctx* c, int eo, double* out) {
+  if (!c || !out || eo < 0 || eo > 1) return LCE_ERR_INVALID;
+  const int nh = c->ch[0].nh;
+  int rc = ensure_staging(c, (size_t)nh * 3 * sizeof(double));
+  if (rc) return rc;
+  if (c->prec == LCE_PREC_F64) launch_debug_force<double>(c->ch_d, eo, (double*)c->staging_d, nh, c->stream);
+  else launch_debug_force<float>(c->ch_d, eo, (double*)c->staging_d, nh, c->stream);
+  CK(cudaGetLastError());
+  CK(cudaMemcpyAsync(out, c->staging_d, (size_t)nh * 3 * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+  CK(cudaStreamSynchronize(c->stream));
+  return LCE_OK;
+}
+
+int lce_flush_l2(lce_ctx* c) {
+  if (!c) return LCE_ERR_INVALID;
+  if (!c->flush_d) {
+    c->flush_bytes = (size_t)256 << 20;
+    CK(cudaMalloc(&c->flush_d, c->flush_bytes));
+  }
+  launch_flush(c->flush_d, c->flush_bytes, c->stream);
+  CK(cudaGetLastError());
+  return LCE_OK;
+}
+
+int lce_profile_sweep(lce_ctx* c, int measflag, float* ms, int max_passes) {
+  if (!c || !ms) return LCE_ERR_INVALID;
+  std::vector<unsigned char> r = sweep_routines(c);
+  std::vector<Pass> passes;
+  for (unsigned char k : r) expand(k, passes);
+  const int np = (int)passes.size();
+  std::vector<cudaEvent_t> ev(np + 1);
+  for (auto& e : ev) CK(cudaEventCreate(&e));
+  CK(cudaEventRecord(ev[0], c->stream));
+  int rc = enqueue(c, r, measflag == 1 ? 1 : 0, true, ev.data() + 1);
+  if (rc == LCE_OK) {
+    CK(cudaStreamSynchronize(c->stream));
+    for (int i = 0; i < np && i < max_passes; ++i) CK(cudaEventElapsedTime(&ms[i], ev[i], ev[i + 1]));
+  }
+  for (auto& e : ev) cudaEventDestroy(e);
+  return rc ? rc : np;
+}
+
+int lce_timer_start(lce_ctx* c) {
+  if (!c) return LCE_ERR_INVALID;
+  CK(cudaEventRecord(c->ev0, c->stream));
+  return LCE_OK;
+}
+
+int lce_timer_stop(lce_ctx* c, float* ms) {
+  if (!c || !ms) return LCE_ERR_INVALID;
+  CK(cudaEventRecord(c->ev1, c->stream));
+  CK(cudaEventSynchronize(c->ev1));
+  CK(cudaEventElapsedTime(ms, c->ev0, c->ev1));
+  return LCE_OK;
+}
+
+}  // extern "C"

@@ -1,0 +1,222 @@
+// lce_gaugefix.cu -- overrelaxed Landau gauge fixing on the device.
+//
+// One iteration of f/or_gauge_fixing1.f:52-337 is two half-steps (eo = 0, 1).
+// A half-step kernel gives one thread per site x of parity eo; the thread
+//   * gathers w(x) = sum_mu c_mu [U_mu(x) + U_mu(x-mu)^+] (c_3 = alpha),
+//   * on eo = 1 adds theta(x) = (Im w_a)^2 + |w_b|^2 to an FP64 partial sum,
+//   * builds Omega = w/|w|, overrelaxes its angle by lambda,
+//   * writes A_f(x) -> Omega A_f Omega^+, U_mu(x) -> Omega U_mu(x) and
+//     U_mu(x-mu) -> U_mu(x-mu) Omega^+.
+// Every link touched in a half-step belongs to exactly one thread, so the
+// update is race free.  All links are rewritten in the eo = 1 half-step, so
+// reunitarising there is exactly f/u_f_renorm.f after the iteration
+// (f/landau_gauge.f:329-334).  A one-block check kernel sums the partials in a
+// fixed order, counts the iteration and raises a device flag when theta <=
+// limit_or (or the cap is reached); later kernels of a captured batch of
+// iterations see the flag and return at once, so the host reads the state
+// only once per batch.
+#include <algorithm>
+
+#include "lce_internal.hpp"
+
+namespace lce {
+
+template <typename R>
+__device__ __forceinline__ su2<R> ldUf(const ChainDev& ch, int mu, int p, int s) {
+  return LinkIO<R>::ld_cg(ch.uf, ((size_t)(mu * 2 + p)) * ch.nh + s);
+}
+
+template <int MU>
+__device__ __forceinline__ int nbr_dn(const ChainDev& ch, Coord X) {
+  int x = X.x, y = X.y, z = X.z;
+  if (MU == 0) x = wrap(x - 1, ch.L1);
+  if (MU == 1) y = wrap(y - 1, ch.L2);
+  if (MU == 2) z = wrap(z - 1, ch.L3);
+  return site_index(x, y, z, ch.hx, ch.nxy);
+}
+
+// w sums in FP64: t1 = sum_mu c_mu U_mu(x), t2 = sum_mu c_mu U_mu(x-mu)
+// (f/or_gauge_fixing1.f:97-142)
+template <typename R>
+__device__ __forceinline__ void gf_sums(const ChainDev& ch, const su2<R> (&um)[3], const su2<R> (&ud)[3],
+                                        su2<double>& t1, su2<double>& t2) {
+  const double al = ch.alpha;
+  t1 = su2<double>{{0, 0}, {0, 0}};
+  t2 = t1;
+#pragma unroll
+  for (int mu = 0; mu < 2; ++mu) {
+    t1.a = t1.a + mk<double>(um[mu].a.re, um[mu].a.im);
+    t1.b = t1.b + mk<double>(um[mu].b.re, um[mu].b.im);
+  }
+  t1.a = t1.a + mk<double>(al * um[2].a.re, al * um[2].a.im);
+  t1.b = t1.b + mk<double>(al * um[2].b.re, al * um[2].b.im);
+#pragma unroll
+  for (int mu = 0; mu < 2; ++mu) {
+    t2.a = t2.a + mk<double>(ud[mu].a.re, ud[mu].a.im);
+    t2.b = t2.b + mk<double>(ud[mu].b.re, ud[mu].b.im);
+  }
+  t2.a = t2.a + mk<double>(al * ud[2].a.re, al * ud[2].a.im);
+  t2.b = t2.b + mk<double>(al * ud[2].b.re, al * ud[2].b.im);
+}
+
+template <typename R>
+__global__ void __launch_bounds__(kBlock) gf_half_kernel(const ChainDev* chp, const ChainState* cst, int eo,
+                                                         double* part) {
+  if (cst->gf_done) return;
+  const ChainDev& ch = *chp;
+  const int s = blockIdx.x * kBlock + threadIdx.x;
+  const int oe = 1 - eo, nh = ch.nh;
+  double th[1] = {0.0};
+  if (s < nh) {
+    const Coord X = site_coord(eo, s, ch.hx, ch.nxy, ch.dhx, ch.dnxy);
+    const int xm[3] = {nbr_dn<0>(ch, X), nbr_dn<1>(ch, X), nbr_dn<2>(ch, X)};
+    su2<R> um[3], ud[3];
+#pragma unroll
+    for (int mu = 0; mu < 3; ++mu) {
+      um[mu] = ldUf<R>(ch, mu, eo, s);
+      ud[mu] = ldUf<R>(ch, mu, oe, xm[mu]);
+    }
+    su2<double> t1, t2;
+    gf_sums<R>(ch, um, ud, t1, t2);
+    // (:145-146) w = first row of sum [U + U^+(x-mu)]
+    const cpx<double> w1 = t1.a + cj(t2.a), w2 = t1.b - t2.b;
+    if (eo == 1) {
+      // (:153-158)
+      const double d = t1.a.im - t2.a.im;
+      th[0] = d * d + (w2.re * w2.re + w2.im * w2.im);
+    }
+    // (:162-184) Omega = w/|w| with its angle overrelaxed by lambda
+    su2<R> o{{(R)w1.re, (R)w1.im}, {(R)w2.re, (R)w2.im}};
+    const R sk = sqrt(norm2(o));
+    o = su2<R>{{o.a.re / sk, o.a.im / sk}, {o.b.re / sk, o.b.im / sk}};
+    const R lam = (R)ch.lambda;
+    if (ch.gf_angle == LCE_GF_ACOS) {
+      // the reference's angle acos(Re Omega), clamped to the domain
+      const R ca = o.a.re > (R)1 ? (R)1 : (o.a.re < (R)-1 ? (R)-1 : o.a.re);
+      const R tht = acos(ca);
+      if (tht != (R)0) {
+        const R tho = lam * tht;
+        const R q1 = cos(tho);
+        const R q2 = sin(tho) / sin(tht) * o.a.im;
+        const R f = -sin(tho) / sin(tht);
+        o.a = mk<R>(q1, -q2);
+        o.b = mk<R>(f * o.b.re, f * o.b.im);
+      }
+    } else {
+      // same rotation, angle atan2(|vector part|, scalar part) of w: accurate
+      // for the small angles that decide convergence below theta ~ 1e-7
+      const double svd = sqrt(w1.im * w1.im + w2.re * w2.re + w2.im * w2.im);
+      if (svd != 0.0) {
+        const R sv = (R)svd;
+        const R tho = lam * atan2(sv, (R)w1.re);
+        R sn, cs;
+        sincos(tho, &sn, &cs);
+        const R f = sn / sv;
+        o.a = mk<R>(cs, -f * (R)w1.im);
+        o.b = mk<R>(-f * (R)w2.re, -f * (R)w2.im);
+      }
+    }
+    // (:243-252) A_f(x) -> Omega (iA) Omega^+
+    R* Af = reinterpret_cast<R*>(ch.af);
+    const R a1 = Af[((size_t)(eo * 3 + 0)) * nh + s], a2 = Af[((size_t)(eo * 3 + 1)) * nh + s],
+            a3 = Af[((size_t)(eo * 3 + 2)) * nh + s];
+    const su2<R> ta = nn(o, ad(a1, a2, a3, o));
+    Af[((size_t)(eo * 3 + 0)) * nh + s] = ta.b.im;
+    Af[((size_t)(eo * 3 + 1)) * nh + s] = ta.b.re;
+    Af[((size_t)(eo * 3 + 2)) * nh + s] = ta.a.im;
+    // (:256-324) links at both ends; renormalise on the eo = 1 half-step
+#pragma unroll
+    for (int mu = 0; mu < 3; ++mu) {
+      su2<R> a = nn(o, um[mu]);
+      su2<R> b = nd(ud[mu], o);
+      if (eo == 1) {
+        a = unitarise64(a);
+        b = unitarise64(b);
+      }
+      LinkIO<R>::st(ch.uf, ((size_t)(mu * 2 + eo)) * nh + s, a);
+      LinkIO<R>::st(ch.uf, ((size_t)(mu * 2 + oe)) * nh + xm[mu], b);
+    }
+  }
+  if (eo == 1) block_reduce_store<1>(th, part + blockIdx.x);
+}
+
+// sum the theta partials in block order, count the iteration, test convergence
+__global__ void __launch_bounds__(1024) gf_check_kernel(const ChainDev* chp, ChainState* cst, const double* part,
+                                                        int nblocks) {
+  if (cst->gf_done) return;
+  double v[1] = {0.0};
+  for (int b = threadIdx.x; b < nblocks; b += blockDim.x) v[0] += part[b];
+  __shared__ double tot;
+  block_reduce_store<1>(v, &tot);
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    const double theta = tot / chp->nh;
+    const int it = cst->gf_iters + 1;
+    cst->gf_iters = it;
+    cst->gf_theta = theta;
+    if (!(theta > chp->limit_or) || (cst->gf_cap > 0 && it >= cst->gf_cap)) cst->gf_done = 1;
+  }
+}
+
+// theta of the current U_f without updating (odd sites)
+template <typename R>
+__global__ void __launch_bounds__(kBlock) gf_theta_kernel(const ChainDev* chp, double* part) {
+  const ChainDev& ch = *chp;
+  const int s = blockIdx.x * kBlock + threadIdx.x;
+  double th[1] = {0.0};
+  if (s < ch.nh) {
+    const Coord X = site_coord(1, s, ch.hx, ch.nxy, ch.dhx, ch.dnxy);
+    const int xm[3] = {nbr_dn<0>(ch, X), nbr_dn<1>(ch, X), nbr_dn<2>(ch, X)};
+    su2<R> um[3], ud[3];
+#pragma unroll
+    for (int mu = 0; mu < 3; ++mu) {
+      um[mu] = ldUf<R>(ch, mu, 1, s);
+      ud[mu] = ldUf<R>(ch, mu, 0, xm[mu]);
+    }
+    su2<double> t1, t2;
+    gf_sums<R>(ch, um, ud, t1, t2);
+    const cpx<double> w2 = t1.b - t2.b;
+    const double d = t1.a.im - t2.a.im;
+    th[0] = d * d + (w2.re * w2.re + w2.im * w2.im);
+  }
+  block_reduce_store<1>(th, part + blockIdx.x);
+}
+
+template <int NQ>
+__global__ void __launch_bounds__(1024) sum_partials_kernel(const double* part, int nblocks, double* out) {
+  double v[NQ];
+#pragma unroll
+  for (int q = 0; q < NQ; ++q) v[q] = 0.0;
+  for (int b = threadIdx.x; b < nblocks; b += blockDim.x) {
+#pragma unroll
+    for (int q = 0; q < NQ; ++q) v[q] += part[(size_t)b * NQ + q];
+  }
+  block_reduce_store<NQ>(v, out);
+}
+
+template <typename R>
+void launch_gf_iteration(const ChainDev* ch, ChainState* cst, int chain, double* part, int nh, cudaStream_t s) {
+  (void)chain;
+  const int nb = ceil_div(nh, kBlock);
+  gf_half_kernel<R><<<nb, kBlock, 0, s>>>(ch, cst, 0, part);
+  gf_half_kernel<R><<<nb, kBlock, 0, s>>>(ch, cst, 1, part);
+  gf_check_kernel<<<1, 1024, 0, s>>>(ch, cst, part, nb);
+}
+
+template <typename R>
+void launch_gf_theta(const ChainDev* ch, double* part, int nh, cudaStream_t s) {
+  gf_theta_kernel<R><<<ceil_div(nh, kBlock), kBlock, 0, s>>>(ch, part);
+}
+
+void launch_sum_partials(const double* part, int nblocks, int nq, double* out, cudaStream_t s) {
+  if (nq == 1) sum_partials_kernel<1><<<1, 1024, 0, s>>>(part, nblocks, out);
+  else if (nq == 2) sum_partials_kernel<2><<<1, 1024, 0, s>>>(part, nblocks, out);
+  else sum_partials_kernel<4><<<1, 1024, 0, s>>>(part, nblocks, out);
+}
+
+template void launch_gf_iteration<float>(const ChainDev*, ChainState*, int, double*, int, cudaStream_t);
+template void launch_gf_iteration<double>(const ChainDev*, ChainState*, int, double*, int, cudaStream_t);
+template void launch_gf_theta<float>(const ChainDev*, double*, int, cudaStream_t);
+template void launch_gf_theta<double>(const ChainDev*, double*, int, cudaStream_t);
+
+}  // namespace lce

@@ -1,0 +1,154 @@
+// lce_internal.hpp -- descriptors shared by the kernels and the C-ABI layer.
+//
+// Device layout of one chain (all planes 256-byte aligned, one allocation):
+//   U   [mu 0..2][parity 0..1][site 0..nh-1]  links, float4 or 2 x double2
+//   A   [parity][k 0..2][site]                adjoint Higgs, SoA planes
+//   U_f, A_f                                  gauge-fixed copies, same layout
+// "parity" is the reference's eo index; sites inside a parity are in the
+// half-row order of f/adresses.f.
+#pragma once
+
+#include <cstddef>
+#include <cstdint>
+#include <string>
+#include <vector>
+
+#include "lce_common.cuh"
+#include "../../include/lceqcd_gpu.h"
+
+namespace lce {
+
+constexpr int kBlock = 256;      // threads per block of the update kernels
+constexpr int kNQ = 4;           // doubles of partial sums per block
+constexpr int kMaxSlots = 64;    // reduction slots per finalize
+
+// pass kinds (one kernel launch over one parity)
+enum PassKind : unsigned char {
+  kHiggsHB = 0,     // ahiggs2
+  kHiggsOR = 1,     // ahiggs3
+  kHiggsMetro = 2,  // ahiggs1
+  kLinkHB = 3,      // agauge
+  kLinkOR = 4,      // link overrelaxation (no reference counterpart)
+  kKindEnd = 0x80,  // flag: last slot of one routine
+};
+
+struct ChainDev {
+  int L1, L2, L3, hx, nxy, nh;
+  FastDiv dhx, dnxy;
+  double beta, beta_a, beta_2, beta_4, lambda, alpha, limit_or;
+  int imode;
+  int gf_angle;
+  uint32_t key0, key1;
+  void* u;
+  void* a;
+  void* uf;
+  void* af;
+};
+
+// mutable state shared by the chains of one context
+struct CtxState {
+  unsigned long long pass_ctr;    // Philox pass counter
+  unsigned long long stream_pos;  // validation-stream position
+  unsigned int status;            // LCE_STATUS_* bits
+  unsigned int ticket;            // last-block ticket of the finalize kernel
+};
+
+// per-chain mutable state
+struct ChainState {
+  double delta;      // ahiggs1 step
+  double gf_theta;   // last theta of the gauge fixing
+  int gf_done;       // converged (or capped)
+  int gf_iters;      // iterations done
+  int gf_cap;        // iteration cap (<= 0: none)
+  int gf_pad;
+  unsigned int ticket;
+  unsigned int pad2;
+};
+
+// device status bits
+enum : unsigned int {
+  kStatusStreamExhausted = 1u,
+  kStatusNaN = 2u,
+};
+
+struct PassArgs {
+  const ChainDev* chains;
+  const int* blk_begin;   // nchains + 1 prefix of block counts
+  CtxState* st;
+  ChainState* cst;
+  double* part;           // [block][kNQ] for this slot, or null
+  const double* stream;   // validation stream (device) or null for Philox
+  unsigned long long stream_n;
+  unsigned long long stream_off;  // relative to st->stream_pos
+  unsigned int pass_off;          // relative to st->pass_ctr
+  int nchains;
+  int eo;
+  int fuse_renorm;
+};
+
+struct FinalizeArgs {
+  const ChainDev* chains;
+  const int* blk_begin;
+  CtxState* st;
+  ChainState* cst;
+  lce_meas* meas;         // [nchains]
+  const double* part;     // slot i at part + i * slot_stride
+  size_t slot_stride;
+  double* totals;         // [nchains][kMaxSlots][kNQ]
+  int nchains;
+  int nslots;
+  unsigned int npasses;           // advance of st->pass_ctr
+  unsigned long long nstream;     // advance of st->stream_pos
+  int single;                     // FP32 arithmetic for the ahiggs1 step update
+  unsigned char kinds[kMaxSlots];
+};
+
+// ---- launchers (lce_update.cu)
+template <typename R>
+void launch_higgs(int mode, const PassArgs& a, int nblocks, cudaStream_t s);
+template <typename R>
+void launch_link(int mode, int mu, const PassArgs& a, int nblocks, cudaStream_t s);
+void launch_finalize(const FinalizeArgs& f, cudaStream_t s);
+template <typename R>
+void launch_renorm(void* u, size_t nlinks, cudaStream_t s);
+template <typename R>
+void launch_debug_staple(const ChainDev* ch, int eo, int mu, double* out, int nh, cudaStream_t s);
+template <typename R>
+void launch_debug_force(const ChainDev* ch, int eo, double* out, int nh, cudaStream_t s);
+
+// ---- field conversion (lce_fields.cu)
+// reference order u[mu][eo][site(ld)][4], a[eo][site(ld)][3]  <->  device planes
+template <typename Rin, typename R>
+void launch_links_in(const Rin* src, void* dst, int nh, cudaStream_t s);
+template <typename R, typename Rout>
+void launch_links_out(const void* src, Rout* dst, int nh, cudaStream_t s);
+template <typename Rin, typename R>
+void launch_higgs_in(const Rin* src, void* dst, int nh, cudaStream_t s);
+template <typename R, typename Rout>
+void launch_higgs_out(const void* src, Rout* dst, int nh, cudaStream_t s);
+template <typename R>
+void launch_init_unit(void* u, void* a, int nh, double a3, cudaStream_t s);
+template <typename R>
+void launch_init_hot(void* u, void* a, int nh, uint32_t k0, uint32_t k1, cudaStream_t s);
+void launch_flush(void* buf, size_t bytes, cudaStream_t s);
+
+// ---- gauge fixing (lce_gaugefix.cu)
+template <typename R>
+void launch_gf_iteration(const ChainDev* ch, ChainState* cst, int chain, double* part, int nh,
+                         cudaStream_t s);
+template <typename R>
+void launch_gf_theta(const ChainDev* ch, double* part, int nh, cudaStream_t s);
+void launch_sum_partials(const double* part, int nblocks, int nq, double* out, cudaStream_t s);
+
+// ---- measurements (lce_meas.cu)
+template <typename R>
+void launch_slice_sums(const ChainDev* ch, int L3, double* slices, cudaStream_t s);
+void launch_correlators(const double* slices, int L1, int L2, int L3, double* out, cudaStream_t s);
+template <typename R>
+void launch_plaquette(const ChainDev* ch, double* part, int nh, cudaStream_t s);
+template <typename R>
+void launch_functional(const ChainDev* ch, double* part, int nh, cudaStream_t s);
+
+inline int ceil_div(long a, long b) { return (int)((a + b - 1) / b); }
+
+}  // namespace lce

@@ -1,0 +1,502 @@
+// lce_update.cu -- checkerboard Monte Carlo update kernels.
+//
+// One kernel launch per (routine, parity[, mu]) pass, one thread per site.
+// Each kernel fuses what the reference does as a chain of whole-lattice array
+// passes (multall*, halo exchanges, temporaries): neighbour gathers, the SU(2)
+// algebra, the random proposal, the accept/reject and the FP64 partial sums
+// of the measurements, so every field element is read from HBM once per pass.
+//
+//   higgs_kernel<R, MODE>   f/a_force.f + f/ahiggs2.f (MODE 0, heatbath),
+//                           f/ahiggs3.f (MODE 1, overrelaxation),
+//                           f/ahiggs1.f (MODE 2, Metropolis)
+//   link_kernel<R, MU, OR>  f/staples.f + f/agauge.f + f/heat_kpi.f (OR = 0);
+//                           link overrelaxation (OR = 1, no reference)
+//   finalize_kernel         deterministic FP64 reduction of the per-block
+//                           partials into /aver_loc/-style results (f/meas1.f)
+//
+// Random numbers: Philox4x32-10 keyed by the chain seed with counter
+// (site, call, pass), or, in validation mode, the host-supplied stream indexed
+// in the reference's consumption order (slot layouts in lce_common.cuh).
+#include <algorithm>
+
+#include "lce_internal.hpp"
+
+namespace lce {
+
+// The reference evaluates cos(tpi*u) and sin(tpi*u) with tpi = 2 acos(-1)
+// (f/heat_kpi.f:250, f/gauss.f:185); here cospi(2u) / sinpi(2u), the same
+// functions of u without rounding 2 pi u first.
+__device__ __forceinline__ float cospi(float x) { return cospif(x); }
+__device__ __forceinline__ double cospi(double x) { return ::cospi(x); }
+__device__ __forceinline__ void sincospi(float x, float* s, float* c) { sincospif(x, s, c); }
+__device__ __forceinline__ void sincospi(double x, double* s, double* c) { ::sincospi(x, s, c); }
+
+__device__ __forceinline__ int find_chain(const int* blk_begin, int n, int b) {
+  int lo = 0, hi = n - 1;
+  while (lo < hi) {
+    int mid = (lo + hi + 1) >> 1;
+    if (__ldg(blk_begin + mid) <= b) lo = mid;
+    else hi = mid - 1;
+  }
+  return lo;
+}
+
+template <typename R>
+__device__ __forceinline__ R ldA(const R* A, int nh, int p, int k, int s) {
+  return __ldg(A + ((size_t)(p * 3 + k)) * nh + s);
+}
+
+// neighbour of X one step along mu (d = +1 / -1), index inside its parity
+template <int MU>
+__device__ __forceinline__ int nbr(const ChainDev& ch, Coord X, int d) {
+  int x = X.x, y = X.y, z = X.z;
+  if (MU == 0) x = wrap(x + d, ch.L1);
+  if (MU == 1) y = wrap(y + d, ch.L2);
+  if (MU == 2) z = wrap(z + d, ch.L3);
+  return site_index(x, y, z, ch.hx, ch.nxy);
+}
+// two steps: +d1 along M1 and +d2 along M2 (M1 != M2)
+template <int M1, int M2>
+__device__ __forceinline__ int nbr2(const ChainDev& ch, Coord X, int d1, int d2) {
+  int x = X.x, y = X.y, z = X.z;
+  if (M1 == 0) x = wrap(x + d1, ch.L1);
+  if (M1 == 1) y = wrap(y + d1, ch.L2);
+  if (M1 == 2) z = wrap(z + d1, ch.L3);
+  if (M2 == 0) x = wrap(x + d2, ch.L1);
+  if (M2 == 1) y = wrap(y + d2, ch.L2);
+  if (M2 == 2) z = wrap(z + d2, ch.L3);
+  return site_index(x, y, z, ch.hx, ch.nxy);
+}
+
+template <typename R>
+__device__ __forceinline__ su2<R> ldU(const ChainDev& ch, int mu, int p, int s) {
+  return LinkIO<R>::ld(ch.u, ((size_t)(mu * 2 + p)) * ch.nh + s);
+}
+
+// f/staples.f:259-415: for each nu != mu (ascending),
+//   upper  = U_nu(x+mu) [U_mu(x+nu)^+ U_nu(x)^+]          (NN of DD)
+//   lower  = U_nu(x-nu+mu)^+ [U_mu(x-nu)^+ U_nu(x-nu)]    (DN of DN)
+//   V      = (V + upper) + lower
+template <typename R, int MU, int NU>
+__device__ __forceinline__ void staple_add(const ChainDev& ch, int eo, Coord X, int s, su2<R>& V) {
+  const int oe = 1 - eo;
+  const int xpmu = nbr<MU>(ch, X, +1), xpnu = nbr<NU>(ch, X, +1), xmnu = nbr<NU>(ch, X, -1);
+  const int xmnupmu = nbr2<NU, MU>(ch, X, -1, +1);
+  su2<R> up1 = dd(ldU<R>(ch, MU, oe, xpnu), ldU<R>(ch, NU, eo, s));
+  su2<R> up2 = nn(ldU<R>(ch, NU, oe, xpmu), up1);
+  su2<R> bt1 = dn(ldU<R>(ch, MU, oe, xmnu), ldU<R>(ch, NU, oe, xmnu));
+  su2<R> bt2 = dn(ldU<R>(ch, NU, eo, xmnupmu), bt1);
+  V.a = (V.a + up2.a) + bt2.a;
+  V.b = (V.b + up2.b) + bt2.b;
+}
+
+template <typename R, int MU>
+__device__ __forceinline__ su2<R> staple(const ChainDev& ch, int eo, Coord X, int s) {
+  su2<R> V{{(R)0, (R)0}, {(R)0, (R)0}};
+  if (MU == 0) {
+    staple_add<R, 0, 1>(ch, eo, X, s, V);
+    staple_add<R, 0, 2>(ch, eo, X, s, V);
+  } else if (MU == 1) {
+    staple_add<R, 1, 0>(ch, eo, X, s, V);
+    staple_add<R, 1, 2>(ch, eo, X, s, V);
+  } else {
+    staple_add<R, 2, 0>(ch, eo, X, s, V);
+    staple_add<R, 2, 1>(ch, eo, X, s, V);
+  }
+  return V;
+}
+
+// f/a_force.f:54-110: F = sum_mu [U(x)(iA(x+mu))U(x)^+ + U(x-mu)^+(iA(x-mu))U(x-mu)],
+// components F3 = Im(.)_a, F2 = Re(.)_b, F1 = Im(.)_b
+template <typename R, int MU>
+__device__ __forceinline__ void force_add(const ChainDev& ch, int eo, Coord X, int s, R& f1, R& f2,
+                                          R& f3) {
+  const int oe = 1 - eo, nh = ch.nh;
+  const R* A = reinterpret_cast<const R*>(ch.a);
+  const int xp = nbr<MU>(ch, X, +1), xm = nbr<MU>(ch, X, -1);
+  su2<R> ux = ldU<R>(ch, MU, eo, s);
+  su2<R> ud = ldU<R>(ch, MU, oe, xm);
+  su2<R> t1 = nn(ux, ad(ldA(A, nh, oe, 0, xp), ldA(A, nh, oe, 1, xp), ldA(A, nh, oe, 2, xp), ux));
+  su2<R> tb = dn(ud, an(ldA(A, nh, oe, 0, xm), ldA(A, nh, oe, 1, xm), ldA(A, nh, oe, 2, xm), ud));
+  f3 = f3 + (t1.a.im + tb.a.im);
+  f2 = f2 + (t1.b.re + tb.b.re);
+  f1 = f1 + (t1.b.im + tb.b.im);
+}
+
+template <typename R>
+__device__ __forceinline__ void higgs_force(const ChainDev& ch, int eo, Coord X, int s, R& f1, R& f2,
+                                            R& f3) {
+  f1 = f2 = f3 = (R)0;
+  force_add<R, 0>(ch, eo, X, s, f1, f2, f3);
+  force_add<R, 1>(ch, eo, X, s, f1, f2, f3);
+  force_add<R, 2>(ch, eo, X, s, f1, f2, f3);
+}
+
+// Set up the uniform source of this pass.  Returns false (and flags the
+// context) when the validation stream cannot cover the pass.
+template <typename R, int N>
+__device__ __forceinline__ bool setup_uniforms(const PassArgs& p, const ChainDev& ch, int s, int layout,
+                                               Uniforms<R, N>& U) {
+  if (p.stream) {
+    unsigned long long base = p.st->stream_pos + p.stream_off;
+    if (base + (unsigned long long)N * ch.nh > p.stream_n) {
+      if (s == 0) atomicOr(&p.st->status, kStatusStreamExhausted);
+      return false;
+    }
+    U.fill_stream(p.stream + base, ch.nh, layout, s);
+  } else {
+    U.fill_philox(ch.key0, ch.key1, p.st->pass_ctr + p.pass_off, s);
+  }
+  return true;
+}
+
+// ------------------------------------------------------------------ Higgs
+template <typename R, int MODE>
+__global__ void __launch_bounds__(kBlock) higgs_kernel(PassArgs p) {
+  const int c = p.nchains > 1 ? find_chain(p.blk_begin, p.nchains, blockIdx.x) : 0;
+  const ChainDev& ch = p.chains[c];
+  const int s = (blockIdx.x - __ldg(p.blk_begin + c)) * kBlock + threadIdx.x;
+  const int eo = p.eo, nh = ch.nh;
+  double q[kNQ] = {0.0, 0.0, 0.0, 0.0};
+  if (s < nh) {
+    constexpr int NS = MODE == 0 ? 7 : (MODE == 1 ? 1 : 4);
+    const int layout = MODE == 2 ? kTriple : kPlanar;
+    Uniforms<R, NS> Un;
+    if (setup_uniforms<R, NS>(p, ch, s, layout, Un)) {
+      Coord X = site_coord(eo, s, ch.hx, ch.nxy, ch.dhx, ch.dnxy);
+      R f[3];
+      higgs_force<R>(ch, eo, X, s, f[0], f[1], f[2]);
+      R* A = reinterpret_cast<R*>(ch.a);
+      R ao[3], an_[3];
+#pragma unroll
+      for (int k = 0; k < 3; ++k) ao[k] = A[((size_t)(eo * 3 + k)) * nh + s];
+      const R beta_a = (R)ch.beta_a, beta_2 = (R)ch.beta_2, beta_4 = (R)ch.beta_4;
+      R alph = (R)0, sf_o = (R)0, sf_n = (R)0;
+      if constexpr (MODE == 0 || MODE == 1) {
+        // f/ahiggs2.f:169-194 width / cxval / alph
+        R width, cxval;
+        if (ch.imode == 1) {
+          R conf2 = (R)0;
+#pragma unroll
+          for (int i = 0; i < 3; ++i) conf2 = conf2 + beta_a * (f[i] * f[i]);
+          R qq = beta_2 + beta_4 * conf2;
+          alph = (beta_4 * conf2) / ((R)2 * (qq * qq));
+          width = beta_2 + alph;
+          cxval = (R)1 / (R)2 / width;
+        } else {
+          width = beta_2;
+          cxval = (R)1 / beta_2 / (R)2;
+        }
+        if constexpr (MODE == 0) {
+          // f/gauss.f:186-197: X = sqrt(-ln(W1)/R) cos(2 pi W2); f/ahiggs2.f:204-208
+          const R rr = (R)1 / width;
+#pragma unroll
+          for (int i = 0; i < 3; ++i) {
+            R w1 = -(R)1 * rr * log(Un.v[2 * i]);
+            R g = sqrt(w1) * cospi((R)2 * Un.v[2 * i + 1]);
+            an_[i] = g + beta_a * f[i] * cxval;
+          }
+        } else {
+          // f/ahiggs3.f:359-363
+#pragma unroll
+          for (int i = 0; i < 3; ++i) an_[i] = -ao[i] + (R)2 * beta_a * f[i] * cxval;
+        }
+      } else {
+        // f/ahiggs1.f:51-56 box proposal
+        const R delta = (R)p.cst[c].delta;
+#pragma unroll
+        for (int i = 0; i < 3; ++i) an_[i] = ao[i] + (Un.v[i] - (R)0.5) * delta;
+      }
+      R rho_o = (R)0, rho_n = (R)0;
+#pragma unroll
+      for (int i = 0; i < 3; ++i) {
+        if (MODE == 2) {
+          sf_o = sf_o + ao[i] * f[i];
+          sf_n = sf_n + an_[i] * f[i];
+        }
+        rho_o = rho_o + ao[i] * ao[i];
+        rho_n = rho_n + an_[i] * an_[i];
+      }
+      R boltz;
+      if (MODE == 2) {
+        // f/ahiggs1.f:77-78
+        boltz = exp(-beta_a * (sf_o - sf_n) + beta_2 * (rho_o - rho_n) +
+                    beta_4 * (rho_o * rho_o - rho_n * rho_n));
+      } else {
+        // f/ahiggs2.f:225-226
+        boltz = exp(-alph * (rho_o - rho_n) + beta_4 * (rho_o * rho_o - rho_n * rho_n));
+      }
+      constexpr int acc_slot = MODE == 0 ? 6 : (MODE == 1 ? 0 : 3);
+      if (boltz >= Un.v[acc_slot]) {
+#pragma unroll
+        for (int k = 0; k < 3; ++k) {
+          A[((size_t)(eo * 3 + k)) * nh + s] = an_[k];
+          ao[k] = an_[k];
+        }
+        rho_o = rho_n;
+        sf_o = sf_n;
+        q[0] = 1.0;
+      }
+      if (p.part) {
+        q[1] = (double)rho_o;
+        q[2] = (double)rho_o * (double)rho_o;
+        if (MODE == 2) q[3] = (double)sf_o;
+        else q[3] = (double)ao[0] * f[0] + (double)ao[1] * f[1] + (double)ao[2] * f[2];
+      }
+    }
+  }
+  if (p.part) block_reduce_store<kNQ>(q, p.part + (size_t)blockIdx.x * kNQ);
+}
+
+// ------------------------------------------------------------------ links
+template <typename R, int MU, int OR>
+__global__ void __launch_bounds__(kBlock) link_kernel(PassArgs p) {
+  const int c = p.nchains > 1 ? find_chain(p.blk_begin, p.nchains, blockIdx.x) : 0;
+  const ChainDev& ch = p.chains[c];
+  const int s = (blockIdx.x - __ldg(p.blk_begin + c)) * kBlock + threadIdx.x;
+  const int eo = p.eo, oe = 1 - eo, nh = ch.nh;
+  double q[kNQ] = {0.0, 0.0, 0.0, 0.0};
+  if (s < nh) {
+    Uniforms<R, OR ? 1 : 7> Un;
+    if (setup_uniforms<R, OR ? 1 : 7>(p, ch, s, OR ? kPlanar : kTriple, Un)) {
+      Coord X = site_coord(eo, s, ch.hx, ch.nxy, ch.dhx, ch.dnxy);
+      const su2<R> V = staple<R, MU>(ch, eo, X, s);
+      const size_t li = ((size_t)(MU * 2 + eo)) * nh + s;
+      const su2<R> uo = LinkIO<R>::ld(ch.u, li);
+      // f/agauge.f:71-84: normalised staple, 1/(beta |V|), 1/2 Re Tr(U Vhat)
+      R t1 = (R)1 / sqrt(norm2(V));
+      const su2<R> vh{{t1 * V.a.re, t1 * V.a.im}, {t1 * V.b.re, t1 * V.b.im}};
+      su2<R> hn;
+      if constexpr (!OR) {
+        t1 = t1 / (R)ch.beta;
+        const R t2 = (uo.a * vh.a - uo.b * cj(vh.b)).re;
+        // f/heat_kpi.f:254-319 single-trial Kennedy-Pendleton
+        R a1 = Un.v[0], a2 = Un.v[1], a3 = Un.v[2];
+        if (a1 == (R)0) a1 = (R)0.0000033;
+        if (a2 == (R)0) a2 = (R)0.0000066;
+        const R cc = cospi((R)2 * a3);
+        R a0 = -(log(a1) + log(a2) * (cc * cc)) * t1;
+        const R r4 = Un.v[3];
+        const bool lacc = r4 * r4 <= ((R)1 - (R)0.5 * a0);
+        a0 = lacc ? (R)1 - a0 : t2;
+        q[0] = lacc ? 1.0 : 0.0;
+        R b1 = (R)1 - a0 * a0;
+        b1 = b1 >= (R)0 ? sqrt(b1) : (R)0;
+        const R b2 = (R)2 * (Un.v[4] - (R)0.5);
+        su2<R> Xk;
+        Xk.a = mk<R>(a0, b1 * b2);
+        R q0 = (R)1 - b2 * b2;
+        q0 = q0 >= (R)0 ? b1 * sqrt(q0) : (R)0;
+        R sph, cph;
+        sincospi((R)2 * Un.v[5], &sph, &cph);
+        Xk.b = mk<R>(q0 * sph, q0 * cph);
+        hn = nd(Xk, vh);  // f/agauge.f:98-99
+      } else {
+        // overrelaxation U' = (Vhat U Vhat)^+ leaves Re Tr(U V) unchanged
+        const su2<R> w = nn(nn(vh, uo), vh);
+        hn = su2<R>{cj(w.a), -w.b};
+      }
+      // f/agauge.f:126-174 hopping term beta_a Re[(iA(x) U)(iA(x+mu) U^+)]_11 and accept
+      const R* A = reinterpret_cast<const R*>(ch.a);
+      const int xp = nbr<MU>(ch, X, +1);
+      const R x1 = ldA(A, nh, eo, 0, s), x2 = ldA(A, nh, eo, 1, s), x3 = ldA(A, nh, eo, 2, s);
+      const R y1 = ldA(A, nh, oe, 0, xp), y2 = ldA(A, nh, oe, 1, xp), y3 = ldA(A, nh, oe, 2, xp);
+      const R beta_a = (R)ch.beta_a;
+      const R sa_old = beta_a * nn(an(x1, x2, x3, uo), ad(y1, y2, y3, uo)).a.re;
+      const R sa_new = beta_a * nn(an(x1, x2, x3, hn), ad(y1, y2, y3, hn)).a.re;
+      su2<R> un = uo;
+      if (exp(sa_old - sa_new) >= Un.v[OR ? 0 : 6]) {
+        un = hn;
+        LinkIO<R>::st(ch.u, li, p.fuse_renorm ? unitarise64(hn) : hn);
+        q[OR ? 0 : 1] = 1.0;
+      }
+      // f/agauge.f:179-185 plaquette against the staple
+      if (!OR && p.part) q[2] = (double)nn(un, V).a.re;
+    }
+  }
+  if (p.part) block_reduce_store<kNQ>(q, p.part + (size_t)blockIdx.x * kNQ);
+}
+
+// ------------------------------------------------------------------ finalize
+// grid = nchains * nslots blocks (+ at least one); block (c, i) sums the
+// partials of chain c in slot i in a fixed order; the last block combines
+// them per chain in the reference's normalisations and advances the RNG.
+__global__ void __launch_bounds__(256) finalize_kernel(FinalizeArgs f) {
+  const int nwork = f.nchains * f.nslots;
+  if ((int)blockIdx.x < nwork) {
+    const int c = blockIdx.x / f.nslots, i = blockIdx.x % f.nslots;
+    const int b0 = f.blk_begin[c], b1 = f.blk_begin[c + 1];
+    const double* part = f.part + (size_t)i * f.slot_stride;
+    double v[kNQ] = {0.0, 0.0, 0.0, 0.0};
+    for (int b = b0 + threadIdx.x; b < b1; b += blockDim.x) {
+#pragma unroll
+      for (int q = 0; q < kNQ; ++q) v[q] += part[(size_t)b * kNQ + q];
+    }
+    block_reduce_store<kNQ>(v, f.totals + ((size_t)c * kMaxSlots + i) * kNQ);
+  }
+  __shared__ bool last;
+  __threadfence();
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    unsigned int t = atomicAdd(&f.st->ticket, 1u);
+    last = (t == gridDim.x - 1);
+  }
+  __syncthreads();
+  if (!last) return;
+  __threadfence();
+  for (int c = threadIdx.x; c < f.nchains; c += blockDim.x) {
+    const ChainDev& ch = f.chains[c];
+    const double V = 2.0 * ch.nh;
+    lce_meas& m = f.meas[c];
+    double h[kNQ] = {0, 0, 0, 0}, l[kNQ] = {0, 0, 0, 0};
+    for (int i = 0; i < f.nslots; ++i) {
+      const volatile double* t = f.totals + ((size_t)c * kMaxSlots + i) * kNQ;
+      const int kind = f.kinds[i] & 0x7f;
+      const bool end = (f.kinds[i] & kKindEnd) != 0;
+      if (!isfinite(t[0]) || !isfinite(t[1]) || !isfinite(t[2]) || !isfinite(t[3]))
+        atomicOr(&f.st->status, kStatusNaN);
+      if (kind <= kHiggsMetro) {
+        for (int q = 0; q < kNQ; ++q) h[q] += t[q];
+        if (end) {
+          // f/ahiggs2.f:259-264 (same in ahiggs1/3)
+          m.a2 = h[1] / V;
+          m.a4 = h[2] / V;
+          m.akin = h[3] / (6.0 * V);
+          const double acc = h[0] / V;
+          if (kind == kHiggsHB) m.acc_hb = acc;
+          if (kind == kHiggsOR) m.acc_or = acc;
+          if (kind == kHiggsMetro) {
+            // f/ahiggs1.f:113-123 step adaptation, in the build's precision
+            if (f.single) {
+              float a = (float)h[0] / (float)V, d = (float)f.cst[c].delta;
+              if (fabsf(a - 0.5f) > 0.1f) d = (a > 0.5f) ? 1.1131241f * d : 0.8989669f * d;
+              m.acc_metro = a;
+              f.cst[c].delta = d;
+            } else {
+              double d = f.cst[c].delta;
+              if (fabs(acc - 0.5) > 0.1) d = (acc > 0.5) ? 1.1131241 * d : 0.8989669 * d;
+              m.acc_metro = acc;
+              f.cst[c].delta = d;
+            }
+            m.delta = f.cst[c].delta;
+          }
+          h[0] = h[1] = h[2] = h[3] = 0;
+        }
+      } else if (kind == kLinkHB) {
+        for (int q = 0; q < kNQ; ++q) l[q] += t[q];
+        if (end) {
+          // f/agauge.f:195-200
+          m.plaq = l[2] / (12.0 * V);
+          m.acc_gauge = (l[0] / (3.0 * V)) * (l[1] / (12.0 * V));
+          l[0] = l[1] = l[2] = l[3] = 0;
+        }
+      } else if (kind == kLinkOR) {
+        for (int q = 0; q < kNQ; ++q) l[q] += t[q];
+        if (end) {
+          m.acc_link_or = l[0] / (3.0 * V);
+          l[0] = l[1] = l[2] = l[3] = 0;
+        }
+      }
+    }
+    m.delta = f.cst[c].delta;
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    f.st->pass_ctr += f.npasses;
+    f.st->stream_pos += f.nstream;
+    f.st->ticket = 0;
+  }
+}
+
+// ------------------------------------------------------------------ renorm
+// f/renorm.f:223-233, in FP64 arithmetic for FP32 links
+template <typename R>
+__global__ void renorm_kernel(void* u, size_t n) {
+  for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x)
+    LinkIO<R>::st(u, i, unitarise64(LinkIO<R>::ld_cg(u, i)));
+}
+
+// ------------------------------------------------------------------ debug
+template <typename R, int MU>
+__global__ void debug_staple_kernel(const ChainDev* chp, int eo, double* out) {
+  const ChainDev& ch = *chp;
+  const int s = blockIdx.x * blockDim.x + threadIdx.x;
+  if (s >= ch.nh) return;
+  Coord X = site_coord(eo, s, ch.hx, ch.nxy, ch.dhx, ch.dnxy);
+  su2<R> V = staple<R, MU>(ch, eo, X, s);
+  out[(size_t)s * 4 + 0] = V.a.re;
+  out[(size_t)s * 4 + 1] = V.a.im;
+  out[(size_t)s * 4 + 2] = V.b.re;
+  out[(size_t)s * 4 + 3] = V.b.im;
+}
+
+template <typename R>
+__global__ void debug_force_kernel(const ChainDev* chp, int eo, double* out) {
+  const ChainDev& ch = *chp;
+  const int s = blockIdx.x * blockDim.x + threadIdx.x;
+  if (s >= ch.nh) return;
+  Coord X = site_coord(eo, s, ch.hx, ch.nxy, ch.dhx, ch.dnxy);
+  R f1, f2, f3;
+  higgs_force<R>(ch, eo, X, s, f1, f2, f3);
+  out[(size_t)s * 3 + 0] = f1;
+  out[(size_t)s * 3 + 1] = f2;
+  out[(size_t)s * 3 + 2] = f3;
+}
+
+// ------------------------------------------------------------------ launchers
+template <typename R>
+void launch_higgs(int mode, const PassArgs& a, int nblocks, cudaStream_t s) {
+  if (mode == 0) higgs_kernel<R, 0><<<nblocks, kBlock, 0, s>>>(a);
+  else if (mode == 1) higgs_kernel<R, 1><<<nblocks, kBlock, 0, s>>>(a);
+  else higgs_kernel<R, 2><<<nblocks, kBlock, 0, s>>>(a);
+}
+
+template <typename R>
+void launch_link(int mode, int mu, const PassArgs& a, int nblocks, cudaStream_t s) {
+  if (mode == 0) {
+    if (mu == 0) link_kernel<R, 0, 0><<<nblocks, kBlock, 0, s>>>(a);
+    else if (mu == 1) link_kernel<R, 1, 0><<<nblocks, kBlock, 0, s>>>(a);
+    else link_kernel<R, 2, 0><<<nblocks, kBlock, 0, s>>>(a);
+  } else {
+    if (mu == 0) link_kernel<R, 0, 1><<<nblocks, kBlock, 0, s>>>(a);
+    else if (mu == 1) link_kernel<R, 1, 1><<<nblocks, kBlock, 0, s>>>(a);
+    else link_kernel<R, 2, 1><<<nblocks, kBlock, 0, s>>>(a);
+  }
+}
+
+void launch_finalize(const FinalizeArgs& f, cudaStream_t s) {
+  int grid = f.nchains * f.nslots;
+  if (grid < 1) grid = 1;
+  finalize_kernel<<<grid, 256, 0, s>>>(f);
+}
+
+template <typename R>
+void launch_renorm(void* u, size_t nlinks, cudaStream_t s) {
+  int grid = (int)std::min<size_t>((nlinks + 255) / 256, 148 * 16);
+  renorm_kernel<R><<<grid, 256, 0, s>>>(u, nlinks);
+}
+
+template <typename R>
+void launch_debug_staple(const ChainDev* ch, int eo, int mu, double* out, int nh, cudaStream_t s) {
+  int grid = ceil_div(nh, 128);
+  if (mu == 0) debug_staple_kernel<R, 0><<<grid, 128, 0, s>>>(ch, eo, out);
+  else if (mu == 1) debug_staple_kernel<R, 1><<<grid, 128, 0, s>>>(ch, eo, out);
+  else debug_staple_kernel<R, 2><<<grid, 128, 0, s>>>(ch, eo, out);
+}
+
+template <typename R>
+void launch_debug_force(const ChainDev* ch, int eo, double* out, int nh, cudaStream_t s) {
+  debug_force_kernel<R><<<ceil_div(nh, 128), 128, 0, s>>>(ch, eo, out);
+}
+
+#define LCE_INST(R)                                                                          \
+  template void launch_higgs<R>(int, const PassArgs&, int, cudaStream_t);                  \
+  template void launch_link<R>(int, int, const PassArgs&, int, cudaStream_t);              \
+  template void launch_renorm<R>(void*, size_t, cudaStream_t);                             \
+  template void launch_debug_staple<R>(const ChainDev*, int, int, double*, int, cudaStream_t); \
+  template void launch_debug_force<R>(const ChainDev*, int, double*, int, cudaStream_t);
+LCE_INST(float)
+LCE_INST(double)
+#undef LCE_INST
+
+}  // namespace lce

@@ -1,0 +1,343 @@
+"""Python mirror of the reference's hot-path interface, over the C ABI.
+
+`Lattice` exposes the subroutines f/main.f calls inside its sweep loop under
+their reference names and argument meanings:
+
+    ahiggs2(measflag) -> accept            f/ahiggs2.f:124
+    ahiggs3(measflag) -> accept            f/ahiggs3.f:283
+    ahiggs1(delta, measflag) -> (accept, delta)   f/ahiggs1.f:7
+    agauge(measflag) -> accept             f/agauge.f:7
+    renorm()                               f/renorm.f:205
+    landau_gauge() -> (da1, iter_or1)      f/landau_gauge.f:281
+    meas1() -> dict(plaq, akin, a2, a4)    f/meas1.f:7 (the reduced values)
+    meas2() -> af(3)                       f/meas2a.f:138
+    correlator() -> corr_a, corr_u, corr_3 f/correlator.f:11
+    polyakov(), scalarcorr()               f/polyakov.f:202, f/scalarcorr.f:331
+
+Errors raise LceError (the reference calls abort()).  Fields move in the
+reference's array order: u[mu, eo, site, 4] = (Re a, Im a, Re b, Im b) of the
+link's first row, a[eo, site, 3].
+"""
+from __future__ import annotations
+
+import ctypes as C
+from dataclasses import dataclass, field
+
+import numpy as np
+
+from . import _lib
+from ._lib import LceMeas, LceParams, check, load
+
+PREC = {"f32": _lib.LCE_PREC_F32, "f64": _lib.LCE_PREC_F64}
+RNG = {"philox": _lib.LCE_RNG_PHILOX, "stream": _lib.LCE_RNG_STREAM}
+
+
+def _ptr(a: np.ndarray):
+    assert a.flags["C_CONTIGUOUS"]
+    return C.c_void_p(a.ctypes.data)
+
+
+@dataclass
+class Params:
+    L: tuple = (16, 16, 16)
+    beta: float = 9.0
+    x: float = 0.1
+    y: float = 0.5
+    lam: float = 1.8
+    alpha: float = 1.0
+    limit_or: float = 1e-9
+    imode: int = 0
+    precision: str = "f32"
+    rng: str = "philox"
+    seed: int = 12345
+    device: int = 0
+    n_link_or: int = 0
+    n_higgs_metro: int = 0
+    delta0: float = 1.0
+    gf_angle: str = "atan2"
+
+    def to_c(self) -> LceParams:
+        p = LceParams()
+        load().lce_default_params(C.byref(p))
+        for i in range(3):
+            p.L[i] = int(self.L[i])
+        p.beta, p.x, p.y = float(self.beta), float(self.x), float(self.y)
+        p.lambda_, p.alpha, p.limit_or = float(self.lam), float(self.alpha), float(self.limit_or)
+        p.imode = int(self.imode)
+        p.precision = PREC[self.precision]
+        p.rng = RNG[self.rng]
+        p.seed = int(self.seed)
+        p.device = int(self.device)
+        p.n_link_or = int(self.n_link_or)
+        p.n_higgs_metro = int(self.n_higgs_metro)
+        p.delta0 = float(self.delta0)
+        p.gf_angle = {"acos": _lib.LCE_GF_ACOS, "atan2": _lib.LCE_GF_ATAN2}[self.gf_angle]
+        return p
+
+
+def couplings(beta: float, x: float, y: float, precision: str = "f64"):
+    """beta_a, beta_2, beta_4 of f/paraminit.f:393-396."""
+    p = Params(beta=beta, x=x, y=y, precision=precision).to_c()
+    out = np.zeros(3)
+    check(load().lce_couplings(C.byref(p), _ptr(out)))
+    return tuple(out)
+
+
+def geometry_tables(L):
+    """siteup/sitedn of f/adresses.f (0-based), [eo, mu, site]."""
+    nh = L[0] * L[1] * L[2] // 2
+    up = np.zeros((2, 3, nh), np.int32)
+    dn = np.zeros((2, 3, nh), np.int32)
+    check(load().lce_geometry_tables(int(L[0]), int(L[1]), int(L[2]), _ptr(up), _ptr(dn)))
+    return up, dn
+
+
+class _Context:
+    def __init__(self, params_list):
+        self.lib = load()
+        self.params = list(params_list)
+        arr = (LceParams * len(self.params))(*[p.to_c() for p in self.params])
+        if len(self.params) == 1:
+            h = self.lib.lce_create(arr)
+        else:
+            h = self.lib.lce_create_batch(arr, len(self.params))
+        if not h:
+            raise _lib.LceError(_lib.LCE_ERR_INVALID, "lce_create: " + self.lib.lce_last_error(None).decode())
+        self.h = C.c_void_p(h)
+        self.dtype = np.float64 if self.params[0].precision == "f64" else np.float32
+
+    def close(self):
+        if getattr(self, "h", None):
+            self.lib.lce_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        self.close()
+
+    def _ck(self, rc):
+        return check(rc, self.h)
+
+    # ---- fields
+    def nh(self, chain: int = 0) -> int:
+        L = self.params[chain].L
+        return L[0] * L[1] * L[2] // 2
+
+    def upload(self, u=None, a=None, which: int = 0, chain: int = 0):
+        nh = self.nh(chain)
+        f64 = (u is not None and np.asarray(u).dtype == np.float64) or \
+              (a is not None and np.asarray(a).dtype == np.float64)
+        dt = np.float64 if f64 else np.float32
+        uu = None if u is None else np.ascontiguousarray(u, dt).reshape(3, 2, nh, 4)
+        aa = None if a is None else np.ascontiguousarray(a, dt).reshape(2, nh, 3)
+        fn = self.lib.lce_upload_f64 if f64 else self.lib.lce_upload
+        self._ck(fn(self.h, chain, which, None if uu is None else _ptr(uu), None if aa is None else _ptr(aa), nh))
+
+    def download(self, which: int = 0, chain: int = 0, dtype=None):
+        nh = self.nh(chain)
+        dt = dtype or self.dtype
+        u = np.zeros((3, 2, nh, 4), dt)
+        a = np.zeros((2, nh, 3), dt)
+        fn = self.lib.lce_download_f64 if dt == np.float64 else self.lib.lce_download
+        self._ck(fn(self.h, chain, which, _ptr(u), _ptr(a), nh))
+        return u, a
+
+    def download_into(self, u: np.ndarray, a: np.ndarray, which: int = 0, chain: int = 0):
+        """Download into caller-owned (e.g. pinned) arrays of the reference layout."""
+        nh = self.nh(chain)
+        assert u.dtype == a.dtype and u.size == 24 * nh and a.size == 6 * nh
+        fn = self.lib.lce_download_f64 if u.dtype == np.float64 else self.lib.lce_download
+        self._ck(fn(self.h, chain, which, _ptr(u), _ptr(a), nh))
+
+    def init_unit(self, a3: float = 1.0):
+        self._ck(self.lib.lce_init_unit(self.h, float(a3)))
+
+    def init_hot(self, seed: int):
+        self._ck(self.lib.lce_init_hot(self.h, int(seed)))
+
+    # ---- random numbers
+    def set_rng_stream(self, u: np.ndarray):
+        self._stream = np.ascontiguousarray(u, np.float64)
+        self._ck(self.lib.lce_set_rng_stream(self.h, _ptr(self._stream), self._stream.size))
+
+    def rng_position(self):
+        a, b = C.c_ulonglong(), C.c_ulonglong()
+        self._ck(self.lib.lce_get_rng_position(self.h, C.byref(a), C.byref(b)))
+        return a.value, b.value
+
+    def set_rng_position(self, pass_ctr: int, stream_pos: int = 0):
+        self._ck(self.lib.lce_set_rng_position(self.h, pass_ctr, stream_pos))
+
+    # ---- updates (reference names)
+    def ahiggs1(self, delta: float, measflag: int = 1):
+        d, acc = C.c_float(delta), C.c_float()
+        self._ck(self.lib.lce_ahiggs1(self.h, C.byref(d), measflag, C.byref(acc)))
+        return acc.value, d.value
+
+    def ahiggs2(self, measflag: int = 1) -> float:
+        acc = C.c_float()
+        self._ck(self.lib.lce_ahiggs2(self.h, measflag, C.byref(acc)))
+        return acc.value
+
+    def ahiggs3(self, measflag: int = 1) -> float:
+        acc = C.c_float()
+        self._ck(self.lib.lce_ahiggs3(self.h, measflag, C.byref(acc)))
+        return acc.value
+
+    def agauge(self, measflag: int = 1) -> float:
+        acc = C.c_float()
+        self._ck(self.lib.lce_agauge(self.h, measflag, C.byref(acc)))
+        return acc.value
+
+    def link_or(self, measflag: int = 1) -> float:
+        acc = C.c_float()
+        self._ck(self.lib.lce_link_or(self.h, measflag, C.byref(acc)))
+        return acc.value
+
+    def renorm(self):
+        self._ck(self.lib.lce_renorm(self.h))
+
+    def sweep(self, measflag: int = 1) -> dict:
+        m = LceMeas()
+        self._ck(self.lib.lce_sweep(self.h, measflag, C.byref(m)))
+        return m.as_dict()
+
+    def sweeps(self, n: int, measflag: int = 0):
+        self._ck(self.lib.lce_sweeps(self.h, int(n), measflag))
+
+    def meas1(self, chain: int = 0) -> dict:
+        m = LceMeas()
+        self._ck(self.lib.lce_get_meas(self.h, chain, C.byref(m)))
+        return m.as_dict()
+
+    def meas_batch(self) -> list:
+        m = (LceMeas * len(self.params))()
+        self._ck(self.lib.lce_get_meas_batch(self.h, m))
+        return [x.as_dict() for x in m]
+
+    def synchronize(self):
+        self._ck(self.lib.lce_synchronize(self.h))
+
+    # ---- gauge fixing and measurements
+    def landau_gauge(self, max_iters: int = 0, chain: int = 0):
+        th, it = C.c_double(), C.c_int()
+        self._ck(self.lib.lce_landau_gauge(self.h, chain, C.byref(th), C.byref(it), int(max_iters)))
+        return th.value, it.value
+
+    def gauge_fix_continue(self, max_iters: int = 0, chain: int = 0):
+        th, it = C.c_double(), C.c_int()
+        self._ck(self.lib.lce_gauge_fix_continue(self.h, chain, C.byref(th), C.byref(it), int(max_iters)))
+        return th.value, it.value
+
+    def gauge_functional(self, chain: int = 0) -> float:
+        v = C.c_double()
+        self._ck(self.lib.lce_gauge_functional(self.h, chain, C.byref(v)))
+        return v.value
+
+    def theta(self, chain: int = 0) -> float:
+        v = C.c_double()
+        self._ck(self.lib.lce_theta(self.h, chain, C.byref(v)))
+        return v.value
+
+    def correlator(self, chain: int = 0):
+        L3 = self.params[chain].L[2]
+        ca, cu, c3, af = np.zeros(L3), np.zeros(L3), np.zeros(L3), np.zeros(3)
+        self._ck(self.lib.lce_correlator(self.h, chain, _ptr(ca), _ptr(cu), _ptr(c3), _ptr(af)))
+        return ca, cu, c3, af
+
+    def meas2(self, chain: int = 0):
+        return self.correlator(chain)[3]
+
+    def polyakov(self, chain: int = 0):
+        L3 = self.params[chain].L[2]
+        sl, co, m = np.zeros(L3), np.zeros(L3), C.c_double()
+        self._ck(self.lib.lce_polyakov(self.h, chain, _ptr(sl), _ptr(co), C.byref(m)))
+        return sl, co, m.value
+
+    def scalarcorr(self, chain: int = 0):
+        L3 = self.params[chain].L[2]
+        sl, co, m = np.zeros(L3), np.zeros(L3), C.c_double()
+        self._ck(self.lib.lce_scalarcorr(self.h, chain, _ptr(sl), _ptr(co), C.byref(m)))
+        return sl, co, m.value
+
+    def plaquette(self, chain: int = 0) -> float:
+        v = C.c_double()
+        self._ck(self.lib.lce_plaquette(self.h, chain, C.byref(v)))
+        return v.value
+
+    def debug_staple(self, eo: int, mu: int) -> np.ndarray:
+        out = np.zeros((self.nh(), 4))
+        self._ck(self.lib.lce_debug_staple(self.h, eo, mu, _ptr(out)))
+        return out
+
+    def debug_force(self, eo: int) -> np.ndarray:
+        out = np.zeros((self.nh(), 3))
+        self._ck(self.lib.lce_debug_force(self.h, eo, _ptr(out)))
+        return out
+
+    # ---- timing
+    def flush_l2(self):
+        self._ck(self.lib.lce_flush_l2(self.h))
+
+    def profile_sweep(self, measflag: int = 0, max_passes: int = 64):
+        ms = np.zeros(max_passes, np.float32)
+        n = self._ck(self.lib.lce_profile_sweep(self.h, measflag, _ptr(ms), max_passes))
+        return ms[:n].astype(np.float64)
+
+    def timer_start(self):
+        self._ck(self.lib.lce_timer_start(self.h))
+
+    def timer_stop(self) -> float:
+        ms = C.c_float()
+        self._ck(self.lib.lce_timer_stop(self.h, C.byref(ms)))
+        return ms.value
+
+
+class Lattice(_Context):
+    """One chain on one GPU (the drop-in for the reference's single lattice)."""
+
+    def __init__(self, L=(16, 16, 16), beta=9.0, x=0.1, y=0.5, **kw):
+        super().__init__([Params(L=tuple(L), beta=beta, x=x, y=y, **kw)])
+
+
+class Ensemble(_Context):
+    """Many independent chains (uneven volumes and couplings) advanced together."""
+
+    def __init__(self, params_list):
+        super().__init__(params_list)
+
+
+# ------------------------------------------------------------------ inputfile
+INPUTFILE_KEYS = [
+    ("n_lattice", 3, int), ("dimproc", 3, int), ("nproc", 1, int), ("init", 1, int), ("rand", 1, int),
+    ("save", 1, int), ("confstart", 1, int), ("beta", 1, float), ("x", 1, float), ("y", 1, float),
+    ("lambda", 1, float), ("alpha", 1, float), ("limit_or", 1, float), ("limit_it", 1, float),
+    ("inorm", 1, int), ("nsweep_flag", 1, int), ("ntime", 1, int), ("nsweep", 1, int), ("imeas", 1, int),
+    ("imode", 1, int),
+]
+
+
+def read_inputfile(path: str) -> dict:
+    """The 20-line positional inputfile of f/paraminit.f:325-344 (list-directed
+    reads: the leading values of each line, the rest is a comment).  Raises
+    ValueError where the reference would abort()."""
+    with open(path) as f:
+        lines = f.read().splitlines()
+    if len(lines) < len(INPUTFILE_KEYS):
+        raise ValueError(f"inputfile {path}: {len(lines)} lines, need {len(INPUTFILE_KEYS)}")
+    out = {}
+    for (key, n, typ), line in zip(INPUTFILE_KEYS, lines):
+        tok = line.replace(",", " ").split()
+        try:
+            vals = [typ(float(t)) if typ is int else float(t.replace("d", "e").replace("D", "E"))
+                    for t in tok[:n]]
+        except ValueError as e:
+            raise ValueError(f"inputfile {path}: bad value for {key}: {line!r}") from e
+        if len(vals) < n:
+            raise ValueError(f"inputfile {path}: missing value for {key}")
+        out[key] = vals if n > 1 else vals[0]
+    return out
+
+
+def params_from_inputfile(cfg: dict, **kw) -> Params:
+    return Params(L=tuple(cfg["n_lattice"]), beta=cfg["beta"], x=cfg["x"], y=cfg["y"], lam=cfg["lambda"],
+                  alpha=cfg["alpha"], limit_or=cfg["limit_or"], imode=cfg["imode"], **kw)

@@ -1,0 +1,308 @@
+"""GPU parity tests: the CUDA path through the C ABI against the CPU oracle.
+
+FP64 validation mode consumes the host-supplied RANLUX stream in the
+reference's consumption order (29*V uniforms per sweep) and must reproduce
+the oracle to 1e-12 relative (the tolerance stated for the plain FP64 path);
+the FP32 production path is compared with the FP32 oracle drawing the same
+Philox stream, within single-precision tolerance.
+"""
+import numpy as np
+import pytest
+
+from oracle.oracle import Oracle, hot_config, random_gauge_transform, reference_stream, uniforms_per_sweep
+
+pytestmark = pytest.mark.gpu
+lce = pytest.importorskip("lceqcd_b200")
+from lceqcd_b200 import Ensemble, LceError, Lattice, Params  # noqa: E402
+
+TOL64 = 1e-12
+LATS = [(4, 4, 4), (4, 6, 8), (6, 4, 2), (2, 2, 2), (8, 8, 8)]
+COUP = dict(beta=9.0, x=0.1, y=0.45)
+
+
+def rel_err(a, b):
+    a, b = np.asarray(a, np.float64), np.asarray(b, np.float64)
+    return float(np.max(np.abs(a - b)) / max(1.0, np.max(np.abs(b))))
+
+
+def pair(L, seed=1, rng="stream", precision="f64", **kw):
+    u, a = hot_config(L, seed=seed)
+    o = Oracle(L, COUP["beta"], COUP["x"], COUP["y"], lam=kw.get("lam", 1.8), alpha=kw.get("alpha", 1.0),
+               limit_or=kw.get("limit_or", 1e-9), imode=kw.get("imode", 0))
+    o.set_fields(u, a)
+    g = Lattice(L, **COUP, precision=precision, rng=rng, **kw)
+    g.upload(u, a)
+    return o, g, u, a
+
+
+@pytest.mark.parametrize("L", LATS)
+def test_staple_and_force(L):
+    o, g, _, _ = pair(L, seed=3)
+    for eo in range(2):
+        for mu in range(3):
+            o.staples(eo, mu)
+            assert rel_err(g.debug_staple(eo, mu), o.staple()[mu, eo]) < TOL64
+        o.a_force(eo)
+        assert rel_err(g.debug_force(eo), o.force()) < TOL64
+
+
+@pytest.mark.parametrize("L", LATS)
+@pytest.mark.parametrize("imode", [0, 1])
+def test_routines_fp64_stream(L, imode):
+    """ahiggs2, ahiggs3, agauge, renorm called one by one (f/main.f:38-41)."""
+    o, g, _, _ = pair(L, seed=5, imode=imode)
+    stream = reference_stream(uniforms_per_sweep(L) + 7, seed=314159)
+    o.set_stream(stream)
+    g.set_rng_stream(stream)
+    for name in ("ahiggs2", "ahiggs3", "agauge"):
+        ao = getattr(o, name)(1)
+        ag = getattr(g, name)(1)
+        assert abs(ao - ag) < 1e-6, name  # accept rates are returned as REAL
+        uo, a_o = o.get_fields()
+        ug, a_g = g.download(dtype=np.float64)
+        assert rel_err(a_g, a_o) < TOL64, name
+        assert rel_err(ug, uo) < TOL64, name
+        mo, mg = o.meas(), g.meas1()
+        for k in ("plaq", "akin", "a2", "a4") if name == "agauge" else ("akin", "a2", "a4"):
+            assert abs(mo[k] - mg[k]) <= TOL64 * max(1, abs(mo[k])), (name, k)
+    o.renorm()
+    g.renorm()
+    assert rel_err(g.download(dtype=np.float64)[0], o.get_fields()[0]) < TOL64
+    assert g.rng_position()[1] == o.stream_pos() == uniforms_per_sweep(L)
+
+
+@pytest.mark.parametrize("L", [(4, 4, 4), (6, 4, 8)])
+def test_fused_sweeps_fp64_stream(L):
+    """lce_sweep (CUDA graph, reunitarisation fused into the link writer)
+    against three reference sweeps."""
+    o, g, _, _ = pair(L, seed=7)
+    stream = reference_stream(3 * uniforms_per_sweep(L), seed=27182)
+    o.set_stream(stream)
+    g.set_rng_stream(stream)
+    for _ in range(3):
+        mo = o.sweep(1)
+        mg = g.sweep(1)
+        for k in ("plaq", "akin", "a2", "a4", "acc_gauge", "acc_hb", "acc_or"):
+            assert abs(mo[k] - mg[k]) <= 1e-11 * max(1, abs(mo[k])), k
+    uo, ao = o.get_fields()
+    ug, ag = g.download(dtype=np.float64)
+    assert rel_err(ug, uo) < 1e-11 and rel_err(ag, ao) < 1e-11
+    with pytest.raises(LceError) as e:  # the stream is used up
+        g.sweep(1)
+    assert e.value.code == lce._lib.LCE_ERR_STREAM
+
+
+@pytest.mark.parametrize("L", [(4, 4, 4), (8, 6, 4)])
+def test_philox_stream_matches_oracle(L):
+    """The device Philox4x32-10 counters (site, call, pass) equal the oracle's."""
+    o, g, _, _ = pair(L, seed=9, rng="philox")
+    o.set_philox(12345, 0)
+    for _ in range(2):
+        o.sweep(1)
+        g.sweep(1)
+    assert g.rng_position()[0] == o.pass_ctr() == 20
+    assert rel_err(g.download(dtype=np.float64)[0], o.get_fields()[0]) < 1e-11
+
+
+def test_ahiggs1_and_link_or_fp64():
+    L = (4, 6, 4)
+    o, g, _, _ = pair(L, seed=11)
+    stream = reference_stream(10 * 2 * 4 * 48 + 6 * 48 * 2, seed=99)
+    o.set_stream(stream)
+    g.set_rng_stream(stream)
+    for d0 in (0.8, 5.0, 0.05):
+        ao, do = o.ahiggs1(d0, 1)
+        ag, dg = g.ahiggs1(d0, 1)
+        assert abs(ao - ag) < 1e-6 and abs(do - dg) < 1e-6 * d0
+        assert rel_err(g.download(dtype=np.float64)[1], o.get_fields()[1]) < TOL64
+    ao, ag = o.link_or(1), g.link_or(1)
+    assert abs(ao - ag) < 1e-6
+    assert rel_err(g.download(dtype=np.float64)[0], o.get_fields()[0]) < TOL64
+
+
+@pytest.mark.parametrize("angle", ["acos", "atan2"])
+@pytest.mark.parametrize("L", [(4, 4, 4), (6, 4, 8)])
+def test_gauge_fixing_iterations_fp64(L, angle):
+    o, g, _, _ = pair(L, seed=13, lam=1.7, alpha=0.9, limit_or=1e-30, gf_angle=angle)
+    o.set_gf_angle(0 if angle == "acos" else 1)
+    o.landau_copy()
+    done = 0
+    for k in (1, 4, 20):
+        for _ in range(k):
+            da1 = o.or_gauge_fixing()
+            o.u_f_renorm()
+        done += k
+        # restart from U on the GPU and run `done` iterations
+        with pytest.raises(LceError) as e:
+            g.landau_gauge(max_iters=done)
+        assert e.value.code == lce._lib.LCE_ERR_GF_NOT_CONVERGED
+        uf, af = g.download(which=1, dtype=np.float64)
+        uo, ao = o.get_fields(which=1)
+        assert rel_err(uf, uo) < 1e-11 and rel_err(af, ao) < 1e-11
+        assert abs(g.theta() - o.theta_direct()) <= 1e-10 * o.theta_direct() + 1e-20
+        assert abs(g.gauge_functional() - o.gauge_functional()) < 1e-12
+
+
+@pytest.mark.parametrize("angle,limit", [("acos", 1e-8), ("atan2", 1e-12)])
+def test_gauge_fixing_convergence_fp64(angle, limit):
+    L = (6, 6, 6)
+    o, g, _, _ = pair(L, seed=17, lam=1.7, limit_or=limit, gf_angle=angle)
+    o.set_gf_angle(0 if angle == "acos" else 1)
+    da_o, it_o = o.landau_gauge(max_iters=20000)
+    da_g, it_g = g.landau_gauge()
+    assert it_o == it_g and da_g <= limit
+    assert abs(da_o - da_g) <= 1e-9 * da_o
+    ca, cu, c3 = o.correlator()
+    ga, gu, g3, af = g.correlator()
+    for x, y in ((ca, ga), (cu, gu), (c3, g3)):
+        assert rel_err(y, x) < 1e-10
+    np.testing.assert_allclose(af, o.meas2(), rtol=1e-9, atol=1e-13)
+
+
+@pytest.mark.parametrize("L", [(4, 4, 6), (8, 4, 4)])
+def test_measurements_fp64(L):
+    o, g, u, a = pair(L, seed=19)
+    o.landau_copy()
+    g.upload(u, a, which=1)
+    ca, cu, c3 = o.correlator()
+    ga, gu, g3, af = g.correlator()
+    for x, y in ((ca, ga), (cu, gu), (c3, g3)):
+        assert rel_err(y, x) < TOL64
+    assert rel_err(af, o.meas2()) < TOL64
+    for f in ("polyakov", "scalarcorr"):
+        so, co, mo = getattr(o, f)()
+        sg, cg, mg = getattr(g, f)()
+        assert rel_err(sg, so) < TOL64 and rel_err(cg, co) < TOL64 and abs(mo - mg) < TOL64 * max(1, abs(mo))
+    assert abs(g.plaquette() - o.plaquette()) < TOL64
+    assert abs(g.gauge_functional() - o.gauge_functional()) < TOL64
+    assert abs(g.theta() - o.theta_direct()) < TOL64 * max(1, o.theta_direct())
+
+
+def test_testconf_correlators_on_gpu():
+    L = (4, 4, 6)
+    o = Oracle(L, 9.0, 0.1, 0.45)
+    o.testconf()
+    o.landau_copy()
+    u, a = o.get_fields()
+    g = Lattice(L, **COUP, precision="f64")
+    g.upload(u, a, which=1)
+    for x, y in zip(o.correlator(), g.correlator()[:3]):
+        assert rel_err(y, x) < TOL64
+
+
+def test_fp32_production_tracks_fp32_oracle():
+    """Same Philox stream, FP32 arithmetic on both sides: the bulk of the sites
+    agree to single precision after two sweeps (a few accept decisions near
+    threshold may differ) and the measured scalars agree closely."""
+    L = (8, 8, 8)
+    u, a = hot_config(L, seed=21, dtype=np.float32)
+    o = Oracle(L, 12.0, 0.09, 0.3, bits=32)
+    o.set_fields(u, a)
+    o.set_philox(777, 0)
+    g = Lattice(L, beta=12.0, x=0.09, y=0.3, precision="f32", seed=777)
+    g.upload(u, a)
+    for _ in range(2):
+        mo = o.sweep(1)
+        mg = g.sweep(1)
+    for k in ("plaq", "a2", "akin"):
+        assert abs(mo[k] - mg[k]) < 2e-3 * max(1, abs(mo[k])), k
+    ug, ag = g.download()
+    uo, ao = o.get_fields()
+    close = np.abs(ug.astype(np.float64) - uo).max(axis=-1) < 1e-4
+    assert close.mean() > 0.97
+
+
+def test_batch_equals_single_chains():
+    """A batched context of uneven chains reproduces each chain run alone, bit
+    for bit (per-chain Philox keys, per-chain reductions)."""
+    specs = [Params(L=(4, 4, 4), beta=9.0, x=0.1, y=0.45, seed=1),
+             Params(L=(6, 4, 8), beta=12.0, x=0.09, y=0.3, seed=2),
+             Params(L=(8, 8, 8), beta=16.0, x=0.08, y=0.2, seed=3, imode=1)]
+    ens = Ensemble(specs)
+    ens.init_hot(42)
+    starts = [ens.download(chain=i) for i in range(3)]
+    for _ in range(3):
+        ens.sweep(1)
+    mb = ens.meas_batch()
+    for i, sp in enumerate(specs):
+        g = Lattice(sp.L, beta=sp.beta, x=sp.x, y=sp.y, seed=sp.seed, imode=sp.imode)
+        g.upload(*starts[i])
+        for _ in range(3):
+            ms = g.sweep(1)
+        ub, ab = ens.download(chain=i)
+        us, as_ = g.download()
+        np.testing.assert_array_equal(ub, us)
+        np.testing.assert_array_equal(ab, as_)
+        for k in ("plaq", "a2", "acc_gauge"):
+            assert mb[i][k] == ms[k]
+
+
+@pytest.mark.parametrize("precision", ["f32", "f64"])
+def test_upload_download_roundtrip(precision):
+    L = (6, 4, 4)
+    u, a = hot_config(L, seed=23)
+    g = Lattice(L, **COUP, precision=precision)
+    for dt in (np.float32, np.float64):
+        g.upload(u.astype(dt), a.astype(dt))
+        for which in (0, 1):
+            if which == 1:
+                g.upload(u.astype(dt), a.astype(dt), which=1)
+            uu, aa = g.download(which=which, dtype=np.float64)
+            tol = 1e-7 if (precision == "f32" or dt == np.float32) else 0
+            np.testing.assert_allclose(uu, u, atol=tol)
+            np.testing.assert_allclose(aa, a, atol=tol)
+
+
+def test_hot_and_unit_starts():
+    L = (16, 16, 16)
+    g = Lattice(L, **COUP)
+    g.init_unit(0.0)
+    assert abs(g.plaquette() - 1.0) < 1e-12
+    u, a = g.download(dtype=np.float64)
+    assert np.all(u[..., 0] == 1) and np.all(a == 0)
+    g.init_hot(5)
+    u, a = g.download(dtype=np.float64)
+    np.testing.assert_allclose(np.linalg.norm(u, axis=-1), 1, atol=1e-6)
+    # Haar measure: each quaternion component has mean 0 and variance 1/4
+    assert abs(u.mean()) < 5e-3 and abs(u.var() - 0.25) < 5e-3
+    assert abs(a.mean()) < 1e-2 and abs(a.var() - 1.0) < 2e-2
+    assert abs(g.plaquette()) < 1e-2
+
+
+def test_error_paths():
+    L = (4, 4, 4)
+    with pytest.raises(LceError):
+        Lattice((4, 4, 5), **COUP)
+    g = Lattice(L, **COUP, precision="f64", rng="stream")
+    g.init_unit(1.0)
+    g.set_rng_stream(np.full(10, 0.5))
+    with pytest.raises(LceError) as e:
+        g.ahiggs2(1)
+    assert e.value.code == lce._lib.LCE_ERR_STREAM
+    # a non-finite field shows up as LCE_ERR_NAN in the measured sums
+    u, a = hot_config(L, seed=1)
+    a[0, 3, 1] = np.nan
+    h = Lattice(L, **COUP, precision="f64")
+    h.upload(u, a)
+    with pytest.raises(LceError) as e:
+        h.sweep(1)
+    assert e.value.code == lce._lib.LCE_ERR_NAN
+    # the gauge-fixing cap returns a status instead of spinning
+    k = Lattice(L, **COUP, precision="f64", limit_or=1e-40)
+    k.init_hot(3)
+    with pytest.raises(LceError) as e:
+        k.landau_gauge(max_iters=3)
+    assert e.value.code == lce._lib.LCE_ERR_GF_NOT_CONVERGED
+
+
+def test_gauge_invariant_measurements_on_gpu():
+    L = (8, 8, 8)
+    u, a = hot_config(L, seed=29)
+    ug, ag = random_gauge_transform(u, a, L, seed=31)
+    g1 = Lattice(L, **COUP, precision="f64")
+    g2 = Lattice(L, **COUP, precision="f64")
+    g1.upload(u, a)
+    g2.upload(ug, ag)
+    assert abs(g1.plaquette() - g2.plaquette()) < 1e-12
+    assert rel_err(g1.scalarcorr()[0], g2.scalarcorr()[0]) < 1e-12
+    assert rel_err(g1.polyakov()[0], g2.polyakov()[0]) < 1e-12
