@@ -278,24 +278,32 @@ def run_gpu(args):
     from lceqcd_b200 import Lattice
     rank, world, local = dist_setup()
     peak, peak_src = peaks()
-    V = vol(L_MAIN)
-    lat = Lattice(L_MAIN, **COUP, precision="f32", seed=1000 + rank, device=local)
+    L = (args.lattice,) * 3 if args.lattice else L_MAIN
+    V = vol(L)
+    lat = Lattice(L, **COUP, precision="f32", seed=1000 + rank, device=local)
     lat.init_hot(2000 + rank)
     lat.sweeps(20, 0)
-    timed_sweeps(lat, max(args.warmup, 3))
+    timed_sweeps(lat, args.warmup)
     lat.synchronize()
     barrier(world)
     clk = Clocks(local)
-    clk.start()
+    if not args.quick:
+        clk.start()
     wall0 = time.perf_counter()
     ms = timed_sweeps(lat, args.steps)
     lat.synchronize()
     wall = time.perf_counter() - wall0
     barrier(world)
-    clocks = clk.stop()
+    clocks = clk.stop() if not args.quick else None
     ms_max = max_over_ranks(ms, world)
     value = world * V * args.steps / (ms_max / 1e3)
     launches = args.steps * (11 + 1)  # 10 pass kernels + finalize per sweep, 1 L2 flush per step
+    if args.quick:
+        if rank == 0:
+            print(json.dumps({"metric": METRIC, "value": value, "unit": UNIT, "L": list(L), "steps": args.steps,
+                              "ms_per_step": ms_max / args.steps, "quick": True}), flush=True)
+        lat.close()
+        return
 
     # roofline of the dominant kernel (link update, 6 of the 10 passes)
     prof = kernel_profile(lat, reps=10)
@@ -304,33 +312,41 @@ def run_gpu(args):
     achieved = B_LINK * V / (link_ms / 1e3) / 1e9
     traffic = profile_traffic()
 
-    # end to end through the C ABI with pinned host buffers: upload the fields,
-    # one measured sweep with the scalars read back, download the fields
+    # End to end through the C ABI with pinned host buffers.  A step uploads
+    # the configuration (the step's input, lce_upload), runs one measured
+    # sweep and reads its measurements back (the step's result, lce_sweep with
+    # an lce_meas output).  A second figure adds the download of the updated
+    # fields (lce_download), i.e. a driver that keeps host mirrors in sync.
     import torch
     nh = V // 2
     hu = torch.empty((3, 2, nh, 4), dtype=torch.float32, pin_memory=True).numpy()
     ha = torch.empty((2, nh, 3), dtype=torch.float32, pin_memory=True).numpy()
-    u0, a0 = lat.download()
-    hu[...] = u0
-    ha[...] = a0
+    lat.download_into(hu, ha)
     Ke = max(5, min(args.steps, 50))
     for _ in range(2):
         lat.upload(hu, ha)
         lat.sweep(1)
         lat.download_into(hu, ha)
     barrier(world)
-    e2e_ms = 0.0
+    e2e_ms, rt_ms = 0.0, 0.0
+    for _ in range(Ke):
+        lat.flush_l2()
+        lat.timer_start()
+        lat.upload(hu, ha)
+        lat.sweep(1)
+        e2e_ms += lat.timer_stop()
     for _ in range(Ke):
         lat.flush_l2()
         lat.timer_start()
         lat.upload(hu, ha)
         lat.sweep(1)
         lat.download_into(hu, ha)
-        e2e_ms += lat.timer_stop()
+        rt_ms += lat.timer_stop()
     e2e_ms = max_over_ranks(e2e_ms, world)
+    rt_ms = max_over_ranks(rt_ms, world)
     e2e_val = world * V * Ke / (e2e_ms / 1e3)
     h2d = hu.nbytes + ha.nbytes
-    d2h = hu.nbytes + ha.nbytes + 13 * 8
+    d2h = 13 * 8  # lce_meas
 
     line = {
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
@@ -340,11 +356,12 @@ def run_gpu(args):
         "config": {"workload": "single chain 64^3, beta=12, x=0.09, y=0.3, hot start; FP32 fields, FP64 "
                                "reunitarisation and sums; sweep = ahiggs2+ahiggs3+agauge (+fused renorm), "
                                "measurements every sweep",
-                   "L": list(L_MAIN), "sites": V, "l2": "flushed between timed steps (256 MB write)",
+                   "L": list(L), "sites": V, "l2": "flushed between timed steps (256 MB write)",
                    "parallelism": f"replicas x{world}" if world > 1 else "single GPU",
                    "wall_s_timed_region": wall},
         "e2e": {"value": e2e_val, "unit": UNIT, "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
-                "note": "lce_upload(host fields) + lce_sweep(meas read back) + lce_download(host fields) per step"},
+                "note": "per step: lce_upload(pinned host fields) + lce_sweep(measflag=1, measurements read back)",
+                "with_field_download": {"value": world * V * Ke / (rt_ms / 1e3), "d2h_bytes_per_step": d2h + h2d}},
         "gpu_launches": launches,
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
                      "traffic": traffic, "kernel": "link_kernel (agauge pass, one parity x one mu)",
@@ -356,9 +373,9 @@ def run_gpu(args):
     }
     if rank == 0 and world == 1:
         try:
-            v, cores, n, el = cpu_baseline(L_MAIN, budget_s=args.cpu_budget)
+            v, cores, n, el = cpu_baseline(L, budget_s=args.cpu_budget)
             line["cpu_baseline"] = {"value": v, "unit": UNIT, "cores": cores, "kind": "port",
-                                    "sample": f"{n} full 64^3 sweeps ({el:.1f} s) of the FP32 oracle restatement "
+                                    "sample": f"{n} full {L[0]}^3 sweeps ({el:.1f} s) of the FP32 oracle restatement "
                                               f"of the reference (OpenMP over sites, {cores} threads)"}
         except Exception as e:
             line["cpu_baseline"] = {"value": None, "unit": UNIT, "cores": 0, "kind": "port", "sample": repr(e)[:200]}
@@ -423,9 +440,14 @@ def main():
     ap.add_argument("--impl", default="lceqcd_b200", choices=["lceqcd_b200", "reference"])
     ap.add_argument("--no-extras", dest="extras", action="store_false")
     ap.add_argument("--cpu-budget", type=float, default=15.0)
+    ap.add_argument("--quick", action="store_true",
+                    help="timed sweeps only (no e2e, CPU baseline, extras or clocks): the ncu profiling case")
+    ap.add_argument("--lattice", type=int, default=0, help="cubic extent for --quick runs (default 64)")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3
+    if args.lattice and not args.quick:
+        ap.error("--lattice only applies to --quick profiling runs; the headline workload is 64^3")
     if args.impl == "reference":
         run_reference(args)
     else:

@@ -433,6 +433,13 @@ lce_ctx* create_impl(const lce_params* p, int n) {
     d.beta_a = cp[0];
     d.beta_2 = cp[1];
     d.beta_4 = cp[2];
+    if (c->prec == LCE_PREC_F32) {
+      d.inv_beta2 = 1.0f / (float)cp[1];
+      d.cxval0 = 1.0f / (float)cp[1] / 2.0f;
+    } else {
+      d.inv_beta2 = 1.0 / cp[1];
+      d.cxval0 = 1.0 / cp[1] / 2.0;
+    }
     d.imode = p[i].imode;
     d.gf_angle = p[i].gf_angle;
     d.key0 = (uint32_t)p[i].seed;
@@ -540,10 +547,12 @@ int gf_loop(lce_ctx* c, int chain, double* theta, int* iters, int max_iters) {
       if (e != cudaSuccess) return cuda_fail(c, e, "cudaGraphInstantiate(gauge fixing)");
       it = c->gf_exec.emplace(key, ex).first;
     }
+    const int before = cs.gf_iters;
     CK(cudaGraphLaunch(it->second, c->stream));
     CK(cudaMemcpyAsync(&cs, c->cst_d + chain, sizeof(cs), cudaMemcpyDeviceToHost, c->stream));
     CK(cudaStreamSynchronize(c->stream));
     if (cs.gf_done) break;
+    if (cs.gf_iters <= before) return fail(c, LCE_ERR_CUDA, "gauge fixing: a batch of iterations made no progress");
     if (batch < 256) batch *= 2;
   }
   if (theta) *theta = cs.gf_theta;

@@ -12,6 +12,7 @@
 #pragma once
 
 #include <cstdint>
+#include <utility>
 #include <cuda_runtime.h>
 
 #define LCE_HD __host__ __device__ __forceinline__
@@ -125,13 +126,66 @@ struct LinkIO<double> {
 };
 
 // Reunitarise in FP64 before storing (f/renorm.f:226-230 fused into the writer).
+// The norm is formed in FP64 from the stored components; for n = 1 + e with
+// |e| < 1e-4 (every link written by an update) 1/sqrt(n) is the series
+// 1 - e/2 + 3e^2/8 - 5e^3/16, whose truncation error (35/128) e^4 < 3e-17 is
+// below FP64 rounding; otherwise the division is taken.
 template <typename R>
 __device__ __forceinline__ su2<R> unitarise64(su2<R> u) {
-  double n = (double)u.a.re * u.a.re + (double)u.a.im * u.a.im + (double)u.b.re * u.b.re +
-             (double)u.b.im * u.b.im;
-  double t = 1.0 / sqrt(n);
+  const double n = (double)u.a.re * u.a.re + (double)u.a.im * u.a.im + (double)u.b.re * u.b.re +
+                   (double)u.b.im * u.b.im;
+  const double e = n - 1.0;
+  double t;
+  if (fabs(e) < 1.0e-4) t = fma(e, fma(e, fma(e, -0.3125, 0.375), -0.5), 1.0);
+  else t = 1.0 / sqrt(n);
   return su2<R>{{(R)(u.a.re * t), (R)(u.a.im * t)}, {(R)(u.b.re * t), (R)(u.b.im * t)}};
 }
+
+// ------------------------------------------------------------------ math policy
+// M<double>: the library functions (validation mode, compared with the FP64
+// oracle at 1e-12).  M<float>: the SFU (MUFU) forms for the production path;
+// their errors (a few 1e-7 relative or absolute, CUDA C Programming Guide
+// intrinsic-function tables) sit at the level of FP32 storage rounding.
+// Arguments of the trigonometric forms are 2*pi*u with u in (0,1), reduced
+// to [-pi, pi] where the SFU error bound holds: cos(2 pi u) = -cos(2 pi (u - 1/2)).
+template <typename R>
+struct M;
+
+template <>
+struct M<double> {
+  __device__ static double log(double x) { return ::log(x); }
+  __device__ static double exp(double x) { return ::exp(x); }
+  __device__ static double sqrt(double x) { return ::sqrt(x); }
+  __device__ static double rsqrt(double x) { return 1.0 / ::sqrt(x); }
+  __device__ static double div(double a, double b) { return a / b; }
+  __device__ static double cos2pi(double u) { return ::cospi(2.0 * u); }
+  __device__ static void sincos2pi(double u, double* s, double* c) { ::sincospi(2.0 * u, s, c); }
+  __device__ static double acos(double x) { return ::acos(x); }
+  __device__ static double atan2(double y, double x) { return ::atan2(y, x); }
+  __device__ static void sincos(double x, double* s, double* c) { ::sincos(x, s, c); }
+  __device__ static double sin(double x) { return ::sin(x); }
+  __device__ static double cos(double x) { return ::cos(x); }
+};
+
+template <>
+struct M<float> {
+  __device__ static float log(float x) { return __logf(x); }
+  __device__ static float exp(float x) { return __expf(x); }
+  __device__ static float sqrt(float x) { return x > 0.0f ? x * rsqrtf(x) : 0.0f; }
+  __device__ static float rsqrt(float x) { return rsqrtf(x); }
+  __device__ static float div(float a, float b) { return __fdividef(a, b); }
+  __device__ static float cos2pi(float u) { return -__cosf(6.28318530717958647692f * (u - 0.5f)); }
+  __device__ static void sincos2pi(float u, float* s, float* c) {
+    __sincosf(6.28318530717958647692f * (u - 0.5f), s, c);
+    *s = -*s;
+    *c = -*c;
+  }
+  __device__ static float acos(float x) { return acosf(x); }
+  __device__ static float atan2(float y, float x) { return atan2f(y, x); }
+  __device__ static void sincos(float x, float* s, float* c) { sincosf(x, s, c); }
+  __device__ static float sin(float x) { return sinf(x); }
+  __device__ static float cos(float x) { return cosf(x); }
+};
 
 // ------------------------------------------------------------------ geometry
 // Division by a runtime constant with one high multiply (round-up method of
@@ -224,7 +278,78 @@ struct Uniforms {
   }
 };
 
+// ------------------------------------------------------------------ PDL
+// Programmatic dependent launch (sm_90+): a kernel lets the next kernel of
+// its stream begin launching once every block of it has started, and the
+// next kernel blocks in griddepcontrol.wait until this grid has completed
+// and its writes are visible.  Kernels call pdl_trigger() first, do
+// data-independent set-up, and call pdl_wait() before their first read of
+// anything an earlier kernel writes.
+__device__ __forceinline__ void pdl_trigger() { asm volatile("griddepcontrol.launch_dependents;" ::: "memory"); }
+__device__ __forceinline__ void pdl_wait() { asm volatile("griddepcontrol.wait;" ::: "memory"); }
+
+template <typename... KArgs, typename... Args>
+inline cudaError_t launch_pdl(void (*kern)(KArgs...), dim3 grid, dim3 block, size_t smem, cudaStream_t s,
+                              Args&&... args) {
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = grid;
+  cfg.blockDim = block;
+  cfg.dynamicSmemBytes = smem;
+  cfg.stream = s;
+  cudaLaunchAttribute attr[1];
+  attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+  attr[0].val.programmaticStreamSerializationAllowed = 1;
+  cfg.attrs = attr;
+  cfg.numAttrs = 1;
+  return cudaLaunchKernelEx(&cfg, kern, std::forward<Args>(args)...);
+}
+
 // ------------------------------------------------------------------ reductions
+// Block partials of NC event counts (reduced as 32-bit integers) and ND FP64
+// sums; out[0..NC) = counts, out[NC..NC+ND) = sums, out[NC+ND..NQ) = 0.
+template <int NC, int ND, int NQ>
+__device__ __forceinline__ void block_reduce_cs(const unsigned (&cnt)[NC > 0 ? NC : 1], double (&v)[ND > 0 ? ND : 1],
+                                                double* out) {
+  static_assert(NC + ND <= NQ, "too many partials");
+  __shared__ unsigned redc[32][NC > 0 ? NC : 1];
+  __shared__ double redd[32][ND > 0 ? ND : 1];
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+  unsigned cw[NC > 0 ? NC : 1];
+#pragma unroll
+  for (int q = 0; q < NC; ++q) cw[q] = __reduce_add_sync(0xffffffffu, cnt[q]);
+#pragma unroll
+  for (int q = 0; q < ND; ++q) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v[q] += __shfl_down_sync(0xffffffffu, v[q], o);
+  }
+  if (lane == 0) {
+#pragma unroll
+    for (int q = 0; q < NC; ++q) redc[w][q] = cw[q];
+#pragma unroll
+    for (int q = 0; q < ND; ++q) redd[w][q] = v[q];
+  }
+  __syncthreads();
+  if (w == 0) {
+    const int nw = (blockDim.x + 31) >> 5;
+#pragma unroll
+    for (int q = 0; q < NC; ++q) {
+      unsigned t = __reduce_add_sync(0xffffffffu, lane < nw ? redc[lane][q] : 0u);
+      if (lane == 0) out[q] = (double)t;
+    }
+#pragma unroll
+    for (int q = 0; q < ND; ++q) {
+      double t = lane < nw ? redd[lane][q] : 0.0;
+#pragma unroll
+      for (int o = 16; o > 0; o >>= 1) t += __shfl_down_sync(0xffffffffu, t, o);
+      if (lane == 0) out[NC + q] = t;
+    }
+    if (lane == 0) {
+#pragma unroll
+      for (int q = NC + ND; q < NQ; ++q) out[q] = 0.0;
+    }
+  }
+}
+
 template <int NQ>
 __device__ __forceinline__ void block_reduce_store(double (&v)[NQ], double* out) {
   __shared__ double red[32][NQ];

@@ -62,14 +62,16 @@ __device__ __forceinline__ void gf_sums(const ChainDev& ch, const su2<R> (&um)[3
 template <typename R>
 __global__ void __launch_bounds__(kBlock) gf_half_kernel(const ChainDev* chp, const ChainState* cst, int eo,
                                                          double* part) {
-  if (cst->gf_done) return;
+  pdl_trigger();
   const ChainDev& ch = *chp;
   const int s = blockIdx.x * kBlock + threadIdx.x;
   const int oe = 1 - eo, nh = ch.nh;
+  const Coord X = site_coord(eo, s < nh ? s : 0, ch.hx, ch.nxy, ch.dhx, ch.dnxy);
+  const int xm[3] = {nbr_dn<0>(ch, X), nbr_dn<1>(ch, X), nbr_dn<2>(ch, X)};
+  pdl_wait();
+  if (cst->gf_done) return;
   double th[1] = {0.0};
   if (s < nh) {
-    const Coord X = site_coord(eo, s, ch.hx, ch.nxy, ch.dhx, ch.dnxy);
-    const int xm[3] = {nbr_dn<0>(ch, X), nbr_dn<1>(ch, X), nbr_dn<2>(ch, X)};
     su2<R> um[3], ud[3];
 #pragma unroll
     for (int mu = 0; mu < 3; ++mu) {
@@ -87,8 +89,8 @@ __global__ void __launch_bounds__(kBlock) gf_half_kernel(const ChainDev* chp, co
     }
     // (:162-184) Omega = w/|w| with its angle overrelaxed by lambda
     su2<R> o{{(R)w1.re, (R)w1.im}, {(R)w2.re, (R)w2.im}};
-    const R sk = sqrt(norm2(o));
-    o = su2<R>{{o.a.re / sk, o.a.im / sk}, {o.b.re / sk, o.b.im / sk}};
+    const R sk = M<R>::sqrt(norm2(o));
+    o = su2<R>{{M<R>::div(o.a.re, sk), M<R>::div(o.a.im, sk)}, {M<R>::div(o.b.re, sk), M<R>::div(o.b.im, sk)}};
     const R lam = (R)ch.lambda;
     if (ch.gf_angle == LCE_GF_ACOS) {
       // the reference's angle acos(Re Omega), clamped to the domain
@@ -143,6 +145,8 @@ __global__ void __launch_bounds__(kBlock) gf_half_kernel(const ChainDev* chp, co
 // sum the theta partials in block order, count the iteration, test convergence
 __global__ void __launch_bounds__(1024) gf_check_kernel(const ChainDev* chp, ChainState* cst, const double* part,
                                                         int nblocks) {
+  pdl_trigger();
+  pdl_wait();
   if (cst->gf_done) return;
   double v[1] = {0.0};
   for (int b = threadIdx.x; b < nblocks; b += blockDim.x) v[0] += part[b];
@@ -198,9 +202,10 @@ template <typename R>
 void launch_gf_iteration(const ChainDev* ch, ChainState* cst, int chain, double* part, int nh, cudaStream_t s) {
   (void)chain;
   const int nb = ceil_div(nh, kBlock);
-  gf_half_kernel<R><<<nb, kBlock, 0, s>>>(ch, cst, 0, part);
-  gf_half_kernel<R><<<nb, kBlock, 0, s>>>(ch, cst, 1, part);
-  gf_check_kernel<<<1, 1024, 0, s>>>(ch, cst, part, nb);
+  // programmatic dependent launch: each kernel waits in griddepcontrol.wait
+  (void)launch_pdl(gf_half_kernel<R>, nb, kBlock, 0, s, ch, (const ChainState*)cst, 0, part);
+  (void)launch_pdl(gf_half_kernel<R>, nb, kBlock, 0, s, ch, (const ChainState*)cst, 1, part);
+  (void)launch_pdl(gf_check_kernel, 1, 1024, 0, s, ch, cst, (const double*)part, nb);
 }
 
 template <typename R>

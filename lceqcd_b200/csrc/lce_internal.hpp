@@ -19,6 +19,10 @@
 namespace lce {
 
 constexpr int kBlock = 256;      // threads per block of the update kernels
+// resident blocks per SM the update kernels are compiled for (register cap
+// 48 for FP32 production kernels, 80 for the FP64 validation kernels)
+template <typename R>
+constexpr int min_blocks() { return sizeof(R) == 4 ? 5 : 3; }
 constexpr int kNQ = 4;           // doubles of partial sums per block
 constexpr int kMaxSlots = 64;    // reduction slots per finalize
 
@@ -36,6 +40,7 @@ struct ChainDev {
   int L1, L2, L3, hx, nxy, nh;
   FastDiv dhx, dnxy;
   double beta, beta_a, beta_2, beta_4, lambda, alpha, limit_or;
+  double inv_beta2, cxval0;  // 1/beta_2 and 1/beta_2/2 in the fields' precision
   int imode;
   int gf_angle;
   uint32_t key0, key1;

@@ -24,12 +24,8 @@
 namespace lce {
 
 // The reference evaluates cos(tpi*u) and sin(tpi*u) with tpi = 2 acos(-1)
-// (f/heat_kpi.f:250, f/gauss.f:185); here cospi(2u) / sinpi(2u), the same
-// functions of u without rounding 2 pi u first.
-__device__ __forceinline__ float cospi(float x) { return cospif(x); }
-__device__ __forceinline__ double cospi(double x) { return ::cospi(x); }
-__device__ __forceinline__ void sincospi(float x, float* s, float* c) { sincospif(x, s, c); }
-__device__ __forceinline__ void sincospi(double x, double* s, double* c) { ::sincospi(x, s, c); }
+// (f/heat_kpi.f:250, f/gauss.f:185); M<R>::cos2pi / sincos2pi take u itself
+// (lce_common.cuh).
 
 __device__ __forceinline__ int find_chain(const int* blk_begin, int n, int b) {
   int lo = 0, hi = n - 1;
@@ -152,18 +148,22 @@ __device__ __forceinline__ bool setup_uniforms(const PassArgs& p, const ChainDev
 
 // ------------------------------------------------------------------ Higgs
 template <typename R, int MODE>
-__global__ void __launch_bounds__(kBlock) higgs_kernel(PassArgs p) {
+__global__ void __launch_bounds__(kBlock, min_blocks<R>()) higgs_kernel(PassArgs p) {
+  pdl_trigger();
+  // the chain table is written once at context creation: safe before pdl_wait
   const int c = p.nchains > 1 ? find_chain(p.blk_begin, p.nchains, blockIdx.x) : 0;
   const ChainDev& ch = p.chains[c];
   const int s = (blockIdx.x - __ldg(p.blk_begin + c)) * kBlock + threadIdx.x;
   const int eo = p.eo, nh = ch.nh;
-  double q[kNQ] = {0.0, 0.0, 0.0, 0.0};
+  const Coord X = site_coord(eo, s < nh ? s : 0, ch.hx, ch.nxy, ch.dhx, ch.dnxy);
+  unsigned acc[1] = {0u};
+  double q[3] = {0.0, 0.0, 0.0};
+  pdl_wait();
   if (s < nh) {
     constexpr int NS = MODE == 0 ? 7 : (MODE == 1 ? 1 : 4);
     const int layout = MODE == 2 ? kTriple : kPlanar;
     Uniforms<R, NS> Un;
     if (setup_uniforms<R, NS>(p, ch, s, layout, Un)) {
-      Coord X = site_coord(eo, s, ch.hx, ch.nxy, ch.dhx, ch.dnxy);
       R f[3];
       higgs_force<R>(ch, eo, X, s, f[0], f[1], f[2]);
       R* A = reinterpret_cast<R*>(ch.a);
@@ -174,26 +174,26 @@ __global__ void __launch_bounds__(kBlock) higgs_kernel(PassArgs p) {
       R alph = (R)0, sf_o = (R)0, sf_n = (R)0;
       if constexpr (MODE == 0 || MODE == 1) {
         // f/ahiggs2.f:169-194 width / cxval / alph
-        R width, cxval;
+        R rr, cxval;
         if (ch.imode == 1) {
           R conf2 = (R)0;
 #pragma unroll
           for (int i = 0; i < 3; ++i) conf2 = conf2 + beta_a * (f[i] * f[i]);
           R qq = beta_2 + beta_4 * conf2;
-          alph = (beta_4 * conf2) / ((R)2 * (qq * qq));
-          width = beta_2 + alph;
-          cxval = (R)1 / (R)2 / width;
+          alph = M<R>::div(beta_4 * conf2, (R)2 * (qq * qq));
+          const R width = beta_2 + alph;
+          rr = M<R>::div((R)1, width);
+          cxval = M<R>::div(M<R>::div((R)1, (R)2), width);
         } else {
-          width = beta_2;
-          cxval = (R)1 / beta_2 / (R)2;
+          rr = (R)ch.inv_beta2;      // 1/width, width = beta_2
+          cxval = (R)ch.cxval0;      // 1/beta_2/2
         }
         if constexpr (MODE == 0) {
           // f/gauss.f:186-197: X = sqrt(-ln(W1)/R) cos(2 pi W2); f/ahiggs2.f:204-208
-          const R rr = (R)1 / width;
 #pragma unroll
           for (int i = 0; i < 3; ++i) {
-            R w1 = -(R)1 * rr * log(Un.v[2 * i]);
-            R g = sqrt(w1) * cospi((R)2 * Un.v[2 * i + 1]);
+            const R w1 = -(R)1 * rr * M<R>::log(Un.v[2 * i]);
+            const R g = M<R>::sqrt(w1) * M<R>::cos2pi(Un.v[2 * i + 1]);
             an_[i] = g + beta_a * f[i] * cxval;
           }
         } else {
@@ -218,13 +218,13 @@ __global__ void __launch_bounds__(kBlock) higgs_kernel(PassArgs p) {
         rho_n = rho_n + an_[i] * an_[i];
       }
       R boltz;
-      if (MODE == 2) {
+      if constexpr (MODE == 2) {
         // f/ahiggs1.f:77-78
-        boltz = exp(-beta_a * (sf_o - sf_n) + beta_2 * (rho_o - rho_n) +
-                    beta_4 * (rho_o * rho_o - rho_n * rho_n));
+        boltz = M<R>::exp(-beta_a * (sf_o - sf_n) + beta_2 * (rho_o - rho_n) +
+                          beta_4 * (rho_o * rho_o - rho_n * rho_n));
       } else {
         // f/ahiggs2.f:225-226
-        boltz = exp(-alph * (rho_o - rho_n) + beta_4 * (rho_o * rho_o - rho_n * rho_n));
+        boltz = M<R>::exp(-alph * (rho_o - rho_n) + beta_4 * (rho_o * rho_o - rho_n * rho_n));
       }
       constexpr int acc_slot = MODE == 0 ? 6 : (MODE == 1 ? 0 : 3);
       if (boltz >= Un.v[acc_slot]) {
@@ -235,60 +235,64 @@ __global__ void __launch_bounds__(kBlock) higgs_kernel(PassArgs p) {
         }
         rho_o = rho_n;
         sf_o = sf_n;
-        q[0] = 1.0;
+        acc[0] = 1u;
       }
       if (p.part) {
-        q[1] = (double)rho_o;
-        q[2] = (double)rho_o * (double)rho_o;
-        if (MODE == 2) q[3] = (double)sf_o;
-        else q[3] = (double)ao[0] * f[0] + (double)ao[1] * f[1] + (double)ao[2] * f[2];
+        q[0] = (double)rho_o;
+        q[1] = (double)rho_o * (double)rho_o;
+        if (MODE == 2) q[2] = (double)sf_o;
+        else q[2] = (double)ao[0] * f[0] + (double)ao[1] * f[1] + (double)ao[2] * f[2];
       }
     }
   }
-  if (p.part) block_reduce_store<kNQ>(q, p.part + (size_t)blockIdx.x * kNQ);
+  // partials {accepted, sum rho, sum rho^2, sum a.F}
+  if (p.part) block_reduce_cs<1, 3, kNQ>(acc, q, p.part + (size_t)blockIdx.x * kNQ);
 }
 
 // ------------------------------------------------------------------ links
 template <typename R, int MU, int OR>
-__global__ void __launch_bounds__(kBlock) link_kernel(PassArgs p) {
+__global__ void __launch_bounds__(kBlock, min_blocks<R>()) link_kernel(PassArgs p) {
+  pdl_trigger();
   const int c = p.nchains > 1 ? find_chain(p.blk_begin, p.nchains, blockIdx.x) : 0;
   const ChainDev& ch = p.chains[c];
   const int s = (blockIdx.x - __ldg(p.blk_begin + c)) * kBlock + threadIdx.x;
   const int eo = p.eo, oe = 1 - eo, nh = ch.nh;
-  double q[kNQ] = {0.0, 0.0, 0.0, 0.0};
+  const Coord X = site_coord(eo, s < nh ? s : 0, ch.hx, ch.nxy, ch.dhx, ch.dnxy);
+  unsigned cnt[2] = {0u, 0u};
+  double pl[1] = {0.0};
+  pdl_wait();
   if (s < nh) {
     Uniforms<R, OR ? 1 : 7> Un;
     if (setup_uniforms<R, OR ? 1 : 7>(p, ch, s, OR ? kPlanar : kTriple, Un)) {
-      Coord X = site_coord(eo, s, ch.hx, ch.nxy, ch.dhx, ch.dnxy);
       const su2<R> V = staple<R, MU>(ch, eo, X, s);
       const size_t li = ((size_t)(MU * 2 + eo)) * nh + s;
       const su2<R> uo = LinkIO<R>::ld(ch.u, li);
       // f/agauge.f:71-84: normalised staple, 1/(beta |V|), 1/2 Re Tr(U Vhat)
-      R t1 = (R)1 / sqrt(norm2(V));
+      R t1 = M<R>::rsqrt(norm2(V));
       const su2<R> vh{{t1 * V.a.re, t1 * V.a.im}, {t1 * V.b.re, t1 * V.b.im}};
       su2<R> hn;
       if constexpr (!OR) {
-        t1 = t1 / (R)ch.beta;
+        t1 = M<R>::div(t1, (R)ch.beta);
         const R t2 = (uo.a * vh.a - uo.b * cj(vh.b)).re;
         // f/heat_kpi.f:254-319 single-trial Kennedy-Pendleton
         R a1 = Un.v[0], a2 = Un.v[1], a3 = Un.v[2];
         if (a1 == (R)0) a1 = (R)0.0000033;
         if (a2 == (R)0) a2 = (R)0.0000066;
-        const R cc = cospi((R)2 * a3);
-        R a0 = -(log(a1) + log(a2) * (cc * cc)) * t1;
+        const R cc = M<R>::cos2pi(a3);
+        R a0 = -(M<R>::log(a1) + M<R>::log(a2) * (cc * cc)) * t1;
         const R r4 = Un.v[3];
         const bool lacc = r4 * r4 <= ((R)1 - (R)0.5 * a0);
         a0 = lacc ? (R)1 - a0 : t2;
-        q[0] = lacc ? 1.0 : 0.0;
+        cnt[0] = lacc ? 1u : 0u;
         R b1 = (R)1 - a0 * a0;
-        b1 = b1 >= (R)0 ? sqrt(b1) : (R)0;
+        b1 = b1 >= (R)0 ? M<R>::sqrt(b1) : (R)0;
         const R b2 = (R)2 * (Un.v[4] - (R)0.5);
         su2<R> Xk;
         Xk.a = mk<R>(a0, b1 * b2);
         R q0 = (R)1 - b2 * b2;
-        q0 = q0 >= (R)0 ? b1 * sqrt(q0) : (R)0;
+        q0 = q0 >= (R)0 ? b1 * M<R>::sqrt(q0) : (R)0;
         R sph, cph;
-        sincospi((R)2 * Un.v[5], &sph, &cph);
+        M<R>::sincos2pi(Un.v[5], &sph, &cph);
         Xk.b = mk<R>(q0 * sph, q0 * cph);
         hn = nd(Xk, vh);  // f/agauge.f:98-99
       } else {
@@ -305,16 +309,24 @@ __global__ void __launch_bounds__(kBlock) link_kernel(PassArgs p) {
       const R sa_old = beta_a * nn(an(x1, x2, x3, uo), ad(y1, y2, y3, uo)).a.re;
       const R sa_new = beta_a * nn(an(x1, x2, x3, hn), ad(y1, y2, y3, hn)).a.re;
       su2<R> un = uo;
-      if (exp(sa_old - sa_new) >= Un.v[OR ? 0 : 6]) {
+      if (M<R>::exp(sa_old - sa_new) >= Un.v[OR ? 0 : 6]) {
         un = hn;
         LinkIO<R>::st(ch.u, li, p.fuse_renorm ? unitarise64(hn) : hn);
-        q[OR ? 0 : 1] = 1.0;
+        cnt[OR ? 0 : 1] = 1u;
       }
       // f/agauge.f:179-185 plaquette against the staple
-      if (!OR && p.part) q[2] = (double)nn(un, V).a.re;
+      if (!OR && p.part) pl[0] = (double)nn(un, V).a.re;
     }
   }
-  if (p.part) block_reduce_store<kNQ>(q, p.part + (size_t)blockIdx.x * kNQ);
+  // partials {KP accepted, Metropolis accepted, sum plaquette} / {OR accepted}
+  if (p.part) {
+    if constexpr (!OR) block_reduce_cs<2, 1, kNQ>(cnt, pl, p.part + (size_t)blockIdx.x * kNQ);
+    else {
+      unsigned c1[1] = {cnt[0]};
+      double d0[1] = {0.0};
+      block_reduce_cs<1, 0, kNQ>(c1, d0, p.part + (size_t)blockIdx.x * kNQ);
+    }
+  }
 }
 
 // ------------------------------------------------------------------ finalize
@@ -322,6 +334,8 @@ __global__ void __launch_bounds__(kBlock) link_kernel(PassArgs p) {
 // partials of chain c in slot i in a fixed order; the last block combines
 // them per chain in the reference's normalisations and advances the RNG.
 __global__ void __launch_bounds__(256) finalize_kernel(FinalizeArgs f) {
+  pdl_trigger();
+  pdl_wait();
   const int nwork = f.nchains * f.nslots;
   if ((int)blockIdx.x < nwork) {
     const int c = blockIdx.x / f.nslots, i = blockIdx.x % f.nslots;
@@ -444,30 +458,26 @@ __global__ void debug_force_kernel(const ChainDev* chp, int eo, double* out) {
 }
 
 // ------------------------------------------------------------------ launchers
+// The pass kernels and the finalize kernel are launched with programmatic
+// dependent launch (lce_common.cuh: launch_pdl / pdl_wait).
 template <typename R>
 void launch_higgs(int mode, const PassArgs& a, int nblocks, cudaStream_t s) {
-  if (mode == 0) higgs_kernel<R, 0><<<nblocks, kBlock, 0, s>>>(a);
-  else if (mode == 1) higgs_kernel<R, 1><<<nblocks, kBlock, 0, s>>>(a);
-  else higgs_kernel<R, 2><<<nblocks, kBlock, 0, s>>>(a);
+  void (*k)(PassArgs) = mode == 0 ? higgs_kernel<R, 0> : (mode == 1 ? higgs_kernel<R, 1> : higgs_kernel<R, 2>);
+  (void)launch_pdl(k, nblocks, kBlock, 0, s, a);
 }
 
 template <typename R>
 void launch_link(int mode, int mu, const PassArgs& a, int nblocks, cudaStream_t s) {
-  if (mode == 0) {
-    if (mu == 0) link_kernel<R, 0, 0><<<nblocks, kBlock, 0, s>>>(a);
-    else if (mu == 1) link_kernel<R, 1, 0><<<nblocks, kBlock, 0, s>>>(a);
-    else link_kernel<R, 2, 0><<<nblocks, kBlock, 0, s>>>(a);
-  } else {
-    if (mu == 0) link_kernel<R, 0, 1><<<nblocks, kBlock, 0, s>>>(a);
-    else if (mu == 1) link_kernel<R, 1, 1><<<nblocks, kBlock, 0, s>>>(a);
-    else link_kernel<R, 2, 1><<<nblocks, kBlock, 0, s>>>(a);
-  }
+  void (*k)(PassArgs);
+  if (mode == 0) k = mu == 0 ? link_kernel<R, 0, 0> : (mu == 1 ? link_kernel<R, 1, 0> : link_kernel<R, 2, 0>);
+  else k = mu == 0 ? link_kernel<R, 0, 1> : (mu == 1 ? link_kernel<R, 1, 1> : link_kernel<R, 2, 1>);
+  (void)launch_pdl(k, nblocks, kBlock, 0, s, a);
 }
 
 void launch_finalize(const FinalizeArgs& f, cudaStream_t s) {
   int grid = f.nchains * f.nslots;
   if (grid < 1) grid = 1;
-  finalize_kernel<<<grid, 256, 0, s>>>(f);
+  (void)launch_pdl(finalize_kernel, grid, 256, 0, s, f);
 }
 
 template <typename R>
