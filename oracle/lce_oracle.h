@@ -24,10 +24,12 @@
  *   RANLUX           f/luxury.f (pinned to the expected output in f/luxtst.f:392-466)
  *   configurations   f/confget.f unitconf/randomconf/testconf
  *
- * Parity pinning: RANLUX is pinned to the reference's own known-answer block.
- * Every other routine has no golden vector in the reference; those are pinned
- * by derived known answers (unit configuration, gauge invariance, testconf
- * closed forms, distribution tests) in tests/.
+ * Parity status: RANLUX is pinned to the reference's own known-answer block.
+ * The Monte Carlo routines are "parity unpinned": the reference ships no
+ * golden vectors for them and cannot be compiled here (Fortran + MPI, no
+ * Fortran compiler in the image), so the restatement is checked only by
+ * derived known answers (unit configuration, gauge invariance/covariance,
+ * testconf closed forms, stream-consumption counts) in tests/.
  *
  * Build: FP64 (default) or FP32 (-DLCE_ORACLE_F32).  Measurement sums are
  * accumulated in double in both modes.
