@@ -211,6 +211,23 @@ int lce_profile_sweep(lce_ctx* ctx, int measflag, float* ms, int max_passes);
 int lce_timer_start(lce_ctx* ctx);
 int lce_timer_stop(lce_ctx* ctx, float* ms);
 
+/* ---- allocation-free measurement ----
+ * No counterpart in the reference.  For callers that cannot let this library
+ * allocate device memory -- a driver whose GPU memory belongs to another
+ * allocator (a caching allocator or a CUDA Fortran pool) or a fixed budget,
+ * or code between asynchronous launches where cudaMalloc/cudaFree could
+ * synchronise the device.  Average plaquette (1/2 Re Tr, all 3V plaquettes)
+ * of a caller-owned FP32 link field u (device memory, reference order, leading
+ * dimension ld >= V/2, 16-byte aligned), written to *plaq (device memory) on
+ * `stream` (a cudaStream_t; NULL = default stream).  No host synchronisation.
+ * Allocates nothing: the per-block scratch is a fixed 512 KiB __device__
+ * array held by every GPU that loads the library; lattices larger than
+ * 16,777,216 sites (256^3) are rejected with LCE_ERR_INVALID.  The first call
+ * on a device looks up the array's address (make it before any stream
+ * capture).  All calls share the array: calls whose kernels overlap on the GPU
+ * race and must be serialised by the caller. */
+int lce_plaquette_noalloc(const float* u, long ld, int L1, int L2, int L3, double* plaq, void* stream);
+
 #if defined(__GNUC__)
 #pragma GCC visibility pop
 #endif

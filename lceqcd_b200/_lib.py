@@ -105,6 +105,7 @@ SIGNATURES = {
     "lce_profile_sweep": (I, [P, I, P, I]),
     "lce_timer_start": (I, [P]),
     "lce_timer_stop": (I, [P, P]),
+    "lce_plaquette_noalloc": (I, [P, C.c_long, I, I, I, P, P]),
 }
 
 _lib = None

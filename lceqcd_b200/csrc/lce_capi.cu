@@ -32,6 +32,8 @@ struct Pass {
 
 }  // namespace
 
+void lce::set_thread_error(const std::string& msg) { g_create_error = msg; }
+
 struct lce_ctx {
   int device = 0;
   int prec = LCE_PREC_F32;

@@ -156,4 +156,7 @@ void launch_functional(const ChainDev* ch, double* part, int nh, cudaStream_t s)
 
 inline int ceil_div(long a, long b) { return (int)((a + b - 1) / b); }
 
+// message returned by lce_last_error(NULL) on this host thread
+void set_thread_error(const std::string& msg);
+
 }  // namespace lce
