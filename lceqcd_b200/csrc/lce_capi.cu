@@ -972,8 +972,8 @@ int lce_debug_force(lce_ctx* c, int eo, double* out) {
 int lce_flush_l2(lce_ctx* c) {
   if (!c) return LCE_ERR_INVALID;
   if (!c->flush_d) {
-    c->flush_bytes = (size_t)256 << 20;
-    CK(cudaMalloc(&c->flush_d, c->flush_bytes));
+    c->flush_bytes = (size_t)256 << 20;  // written; a second 256 MB half is read
+    CK(cudaMalloc(&c->flush_d, 2 * c->flush_bytes));
   }
   launch_flush(c->flush_d, c->flush_bytes, c->stream);
   CK(cudaGetLastError());
