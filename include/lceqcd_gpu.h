@@ -66,6 +66,13 @@ extern "C" {
 #define LCE_GF_ACOS 0
 #define LCE_GF_ATAN2 1
 
+/* execution form of lce_sweep(s): one kernel per parity pass chained in a
+ * CUDA graph, or one cooperative persistent kernel per sweep that loops over
+ * the (chain, tile) work list of every pass with a grid barrier in between */
+#define LCE_SWEEP_AUTO 0
+#define LCE_SWEEP_PASSES 1
+#define LCE_SWEEP_PERSISTENT 2
+
 /* field selectors for upload/download */
 #define LCE_FIELDS 0        /* u, a        (COMMON /linkvar/ u, a) */
 #define LCE_FIELDS_FIXED 1  /* u_f, a_f    (COMMON /linkvar/ u_f, a_f) */
@@ -90,6 +97,9 @@ typedef struct lce_params {
   double delta0;         /* initial ahiggs1 step */
   int gf_angle;          /* gauge-fixing rotation angle: LCE_GF_ACOS (the
                             reference, f/or_gauge_fixing1.f:174) or LCE_GF_ATAN2 */
+  int sweep_mode;        /* LCE_SWEEP_AUTO (time both forms on the first sweeps
+                            and keep the faster), LCE_SWEEP_PASSES or
+                            LCE_SWEEP_PERSISTENT */
 } lce_params;
 
 /* Measured quantities: /aver_loc/ (plaq0, a0kin, a02, a04, a0f) and the
@@ -165,8 +175,12 @@ int lce_renorm(lce_ctx* ctx);
  * [link OR x n_link_or], reunitarisation fused into the link writers; one
  * CUDA graph per measflag.  m (chain 0) may be NULL: no synchronisation. */
 int lce_sweep(lce_ctx* ctx, int measflag, lce_meas* m);
-/* nsweeps graph replays without synchronisation */
+/* nsweeps graph replays without synchronisation (with LCE_SWEEP_AUTO the first
+ * sweeps of a context alternate the two forms under CUDA events -- every one
+ * of them a real sweep -- and the faster form is kept) */
 int lce_sweeps(lce_ctx* ctx, int nsweeps, int measflag);
+/* the form lce_sweeps uses now (LCE_SWEEP_AUTO while still undecided) */
+int lce_get_sweep_mode(lce_ctx* ctx);
 /* f/meas1.f inputs: the last measured quantities of a chain */
 int lce_get_meas(lce_ctx* ctx, int chain, lce_meas* m);
 int lce_get_meas_batch(lce_ctx* ctx, lce_meas* m /* [nchains] */);

@@ -27,6 +27,9 @@ LCE_RNG_PHILOX = 0
 LCE_RNG_STREAM = 1
 LCE_GF_ACOS = 0
 LCE_GF_ATAN2 = 1
+LCE_SWEEP_AUTO = 0
+LCE_SWEEP_PASSES = 1
+LCE_SWEEP_PERSISTENT = 2
 LCE_FIELDS = 0
 LCE_FIELDS_FIXED = 1
 
@@ -39,7 +42,7 @@ class LceParams(C.Structure):
         ("imode", C.c_int), ("precision", C.c_int), ("rng", C.c_int),
         ("seed", C.c_ulonglong), ("device", C.c_int),
         ("n_link_or", C.c_int), ("n_higgs_metro", C.c_int),
-        ("delta0", C.c_double), ("gf_angle", C.c_int),
+        ("delta0", C.c_double), ("gf_angle", C.c_int), ("sweep_mode", C.c_int),
     ]
 
 
@@ -89,6 +92,7 @@ SIGNATURES = {
     "lce_renorm": (I, [P]),
     "lce_sweep": (I, [P, I, P]),
     "lce_sweeps": (I, [P, I, I]),
+    "lce_get_sweep_mode": (I, [P]),
     "lce_get_meas": (I, [P, I, P]),
     "lce_get_meas_batch": (I, [P, P]),
     "lce_landau_gauge": (I, [P, I, P, P, I]),

@@ -64,7 +64,13 @@ struct lce_ctx {
   size_t flush_bytes = 0;
   cudaStream_t own = nullptr, stream = nullptr;
   cudaEvent_t ev0 = nullptr, ev1 = nullptr;
-  cudaGraphExec_t sweep_exec[2] = {nullptr, nullptr};
+  cudaGraphExec_t sweep_exec[2] = {nullptr, nullptr};     // per-pass kernels, per measflag
+  cudaGraphExec_t persist_exec[2] = {nullptr, nullptr};   // persistent kernel, per measflag
+  GridBar* bar_d = nullptr;
+  int persist_grid = 0;
+  int sweep_mode = LCE_SWEEP_AUTO;   // requested
+  int mode = LCE_SWEEP_AUTO;         // in use (AUTO while tuning)
+  std::vector<float> tune_ms[2];     // autotune samples per form
   std::map<std::pair<int, int>, cudaGraphExec_t> gf_exec;
   std::string err;
 };
@@ -134,6 +140,10 @@ bool valid_params(const lce_params& p, std::string& why) {
     why = "imode must be 0 or 1";
     return false;
   }
+  if (p.sweep_mode < LCE_SWEEP_AUTO || p.sweep_mode > LCE_SWEEP_PERSISTENT) {
+    why = "sweep_mode must be LCE_SWEEP_AUTO, LCE_SWEEP_PASSES or LCE_SWEEP_PERSISTENT";
+    return false;
+  }
   if (p.gf_angle != LCE_GF_ACOS && p.gf_angle != LCE_GF_ATAN2) {
     why = "gf_angle must be LCE_GF_ACOS or LCE_GF_ATAN2";
     return false;
@@ -157,6 +167,11 @@ int status_check(lce_ctx* c) {
     unsigned int z = 0;
     CK(cudaMemcpy(&c->st_d->status, &z, sizeof(z), cudaMemcpyHostToDevice));
     if (st.status & kStatusStreamExhausted) return fail(c, LCE_ERR_STREAM, "validation uniform stream exhausted");
+    if (st.status & kStatusBarrierTimeout) {
+      // leave the barrier in a clean state for the next launch
+      CK(cudaMemset(c->bar_d, 0, sizeof(GridBar)));
+      return fail(c, LCE_ERR_CUDA, "persistent sweep: a grid barrier timed out");
+    }
     return fail(c, LCE_ERR_NAN, "non-finite value in a measurement reduction");
   }
   return LCE_OK;
@@ -240,6 +255,102 @@ int enqueue(lce_ctx* c, const std::vector<unsigned char>& routines, int measflag
   f.nstream = c->rng == LCE_RNG_STREAM ? soff : 0;
   launch_finalize(f, c->stream);
   CK(cudaGetLastError());
+  return LCE_OK;
+}
+
+std::vector<unsigned char> sweep_routines(const lce_ctx* c);
+
+// Queue the passes of the given routines as one cooperative persistent kernel
+// (plan of passes, reduction slots and stream offsets as in enqueue).
+template <typename R>
+int enqueue_persistent(lce_ctx* c, const std::vector<unsigned char>& routines, int measflag, bool fuse_renorm) {
+  std::vector<Pass> passes;
+  for (unsigned char r : routines) expand(r, passes);
+  if ((int)passes.size() > kMaxSlots) return fail(c, LCE_ERR_INVALID, "too many passes for one persistent sweep");
+  PersistArgs a;
+  std::memset(&a, 0, sizeof(a));
+  PassArgs& b = a.base;
+  b.chains = c->ch_d;
+  b.blk_begin = c->blk_d;
+  b.st = c->st_d;
+  b.cst = c->cst_d;
+  b.stream = c->rng == LCE_RNG_STREAM ? c->stream_d : nullptr;
+  b.stream_n = c->stream_n;
+  b.nchains = c->nchains;
+  b.fuse_renorm = fuse_renorm ? 1 : 0;
+  FinalizeArgs& f = a.fin;
+  f.chains = c->ch_d;
+  f.blk_begin = c->blk_d;
+  f.st = c->st_d;
+  f.cst = c->cst_d;
+  f.meas = c->meas_d;
+  f.part = c->part_d;
+  f.slot_stride = c->slot_stride;
+  f.totals = c->totals_d;
+  f.nchains = c->nchains;
+  f.single = c->prec == LCE_PREC_F32;
+  unsigned long long soff = 0;
+  int slot = 0;
+  for (size_t i = 0; i < passes.size(); ++i) {
+    const Pass& ps = passes[i];
+    const bool reduce = measflag == 1 || ps.kind == kHiggsMetro;
+    if (reduce && slot >= c->part_slots) return fail(c, LCE_ERR_INVALID, "too many reduction slots");
+    a.plan[i] = PlanEntry{ps.kind, (unsigned char)ps.eo, (unsigned char)ps.mu,
+                          reduce ? (unsigned char)slot : kNoSlot};
+    a.stream_off[i] = soff;
+    if (reduce) {
+      f.kinds[slot] = (unsigned char)(ps.kind | (ps.end ? kKindEnd : 0));
+      ++slot;
+    }
+    if (c->nchains == 1) soff += (unsigned long long)nslots_of(ps.kind) * c->ch[0].nh;
+  }
+  f.nslots = slot;
+  f.npasses = (unsigned int)passes.size();
+  f.nstream = c->rng == LCE_RNG_STREAM ? soff : 0;
+  a.bar = c->bar_d;
+  a.ntiles = c->blk.back();
+  a.npasses = (int)passes.size();
+  const int grid = std::max(1, std::min(c->persist_grid, a.ntiles));
+  CK(launch_persistent<R>(a, grid, c->stream));
+  return LCE_OK;
+}
+
+constexpr size_t kTuneSamples = 3;
+
+// The instantiated graph of one sweep in the given form (built once per
+// form and measflag).  The persistent form falls back to the per-pass form
+// under LCE_SWEEP_AUTO if it cannot be captured on this device.
+int sweep_graph(lce_ctx* c, int form, int mf, cudaGraphExec_t* out) {
+  cudaGraphExec_t* slot = form == LCE_SWEEP_PERSISTENT ? &c->persist_exec[mf] : &c->sweep_exec[mf];
+  if (!*slot) {
+    cudaGraph_t g;
+    CK(cudaStreamBeginCapture(c->stream, cudaStreamCaptureModeThreadLocal));
+    int rc;
+    if (form == LCE_SWEEP_PERSISTENT)
+      rc = c->prec == LCE_PREC_F64 ? enqueue_persistent<double>(c, sweep_routines(c), mf, true)
+                                   : enqueue_persistent<float>(c, sweep_routines(c), mf, true);
+    else
+      rc = enqueue(c, sweep_routines(c), mf, true);
+    const cudaError_t ec = cudaStreamEndCapture(c->stream, &g);
+    cudaError_t ei = cudaSuccess;
+    if (ec == cudaSuccess) {
+      if (rc == LCE_OK) ei = cudaGraphInstantiate(slot, g, 0);
+      cudaGraphDestroy(g);
+    }
+    if (rc) return rc;
+    const cudaError_t e = ec != cudaSuccess ? ec : ei;
+    if (e != cudaSuccess) {
+      *slot = nullptr;
+      cudaGetLastError();
+      if (form == LCE_SWEEP_PERSISTENT && c->sweep_mode == LCE_SWEEP_AUTO) {
+        c->err = std::string("persistent sweep unavailable: ") + cudaGetErrorString(e);
+        c->mode = LCE_SWEEP_PASSES;
+        return sweep_graph(c, LCE_SWEEP_PASSES, mf, out);
+      }
+      return cuda_fail(c, e, "sweep graph capture");
+    }
+  }
+  *out = *slot;
   return LCE_OK;
 }
 
@@ -483,6 +594,19 @@ lce_ctx* create_impl(const lce_params* p, int n) {
       return bail(e, "cudaMemcpy(cstate)");
   }
   if ((e = cudaMalloc(&c->meas_d, sizeof(lce_meas) * n)) != cudaSuccess) return bail(e, "cudaMalloc(meas)");
+  if ((e = cudaMalloc(&c->bar_d, sizeof(GridBar))) != cudaSuccess) return bail(e, "cudaMalloc(barrier)");
+  if ((e = cudaMemset(c->bar_d, 0, sizeof(GridBar))) != cudaSuccess) return bail(e, "cudaMemset(barrier)");
+  c->sweep_mode = p[0].sweep_mode;
+  c->mode = p[0].sweep_mode;
+  c->persist_grid = c->prec == LCE_PREC_F64 ? persistent_grid<double>() : persistent_grid<float>();
+  if (c->persist_grid <= 0) {
+    if (c->sweep_mode == LCE_SWEEP_PERSISTENT) {
+      g_create_error = "create: the persistent sweep kernel cannot be made resident on this device";
+      lce_destroy(c);
+      return nullptr;
+    }
+    c->mode = LCE_SWEEP_PASSES;
+  }
   if ((e = cudaMemset(c->meas_d, 0, sizeof(lce_meas) * n)) != cudaSuccess) return bail(e, "cudaMemset(meas)");
   c->part_slots = std::max(6, 4 + 6 + 2 * c->n_higgs_metro + 6 * c->n_link_or);
   c->slot_stride = (size_t)c->blk.back() * kNQ;
@@ -603,6 +727,7 @@ void lce_default_params(lce_params* p) {
   p->device = 0;
   p->delta0 = 1.0;
   p->gf_angle = LCE_GF_ATAN2;
+  p->sweep_mode = LCE_SWEEP_AUTO;
 }
 
 int lce_couplings(const lce_params* p, double out[3]) {
@@ -638,11 +763,13 @@ void lce_destroy(lce_ctx* c) {
   if (!c) return;
   cudaSetDevice(c->device);
   if (c->stream) cudaStreamSynchronize(c->stream);
-  for (int i = 0; i < 2; ++i)
+  for (int i = 0; i < 2; ++i) {
     if (c->sweep_exec[i]) cudaGraphExecDestroy(c->sweep_exec[i]);
+    if (c->persist_exec[i]) cudaGraphExecDestroy(c->persist_exec[i]);
+  }
   for (auto& kv : c->gf_exec) cudaGraphExecDestroy(kv.second);
   void* ptrs[] = {c->ch_d, c->blk_d, c->st_d, c->cst_d, c->meas_d, c->part_d, c->totals_d,
-                  c->scratch_d, c->fields_d, c->stream_d, c->staging_d, c->flush_d};
+                  c->scratch_d, c->fields_d, c->stream_d, c->staging_d, c->flush_d, c->bar_d};
   for (void* q : ptrs)
     if (q) cudaFree(q);
   if (c->ev0) cudaEventDestroy(c->ev0);
@@ -717,11 +844,16 @@ int lce_set_rng_stream(lce_ctx* c, const double* u, size_t n) {
   }
   c->stream_n = n;
   // graphs captured the old stream pointer
-  for (int i = 0; i < 2; ++i)
+  for (int i = 0; i < 2; ++i) {
     if (c->sweep_exec[i]) {
       cudaGraphExecDestroy(c->sweep_exec[i]);
       c->sweep_exec[i] = nullptr;
     }
+    if (c->persist_exec[i]) {
+      cudaGraphExecDestroy(c->persist_exec[i]);
+      c->persist_exec[i] = nullptr;
+    }
+  }
   unsigned long long z = 0;
   CK(cudaMemcpy(&c->st_d->stream_pos, &z, sizeof(z), cudaMemcpyHostToDevice));
   return LCE_OK;
@@ -793,23 +925,43 @@ int lce_renorm(lce_ctx* c) {
 int lce_sweeps(lce_ctx* c, int nsweeps, int measflag) {
   if (!c || nsweeps < 0) return LCE_ERR_INVALID;
   const int mf = measflag == 1 ? 1 : 0;
-  if (!c->sweep_exec[mf]) {
-    cudaGraph_t g;
-    CK(cudaStreamBeginCapture(c->stream, cudaStreamCaptureModeThreadLocal));
-    int rc = enqueue(c, sweep_routines(c), mf, true);
-    cudaError_t e = cudaStreamEndCapture(c->stream, &g);
-    if (rc) {
-      if (e == cudaSuccess) cudaGraphDestroy(g);
-      return rc;
+  int done = 0;
+  // autotune: alternate the two forms on real sweeps, one timed sweep at a
+  // time, until each has kTuneSamples samples; then keep the faster.
+  while (c->mode == LCE_SWEEP_AUTO && done < nsweeps) {
+    const int form = (c->tune_ms[0].size() <= c->tune_ms[1].size()) ? 0 : 1;
+    cudaGraphExec_t ex;
+    int rc = sweep_graph(c, form == 0 ? LCE_SWEEP_PASSES : LCE_SWEEP_PERSISTENT, mf, &ex);
+    if (rc) return rc;
+    CK(cudaEventRecord(c->ev0, c->stream));
+    CK(cudaGraphLaunch(ex, c->stream));
+    CK(cudaEventRecord(c->ev1, c->stream));
+    CK(cudaEventSynchronize(c->ev1));
+    float ms = 0;
+    CK(cudaEventElapsedTime(&ms, c->ev0, c->ev1));
+    c->tune_ms[form].push_back(ms);
+    ++done;
+    if (c->tune_ms[0].size() >= kTuneSamples + 1 && c->tune_ms[1].size() >= kTuneSamples + 1) {
+      // drop each form's first (instantiation-cold) sample, compare medians
+      float med[2];
+      for (int f = 0; f < 2; ++f) {
+        std::vector<float> v(c->tune_ms[f].begin() + 1, c->tune_ms[f].end());
+        std::sort(v.begin(), v.end());
+        med[f] = v[v.size() / 2];
+      }
+      c->mode = med[1] < med[0] ? LCE_SWEEP_PERSISTENT : LCE_SWEEP_PASSES;
     }
-    if (e != cudaSuccess) return cuda_fail(c, e, "cudaStreamEndCapture(sweep)");
-    e = cudaGraphInstantiate(&c->sweep_exec[mf], g, 0);
-    cudaGraphDestroy(g);
-    if (e != cudaSuccess) return cuda_fail(c, e, "cudaGraphInstantiate(sweep)");
   }
-  for (int i = 0; i < nsweeps; ++i) CK(cudaGraphLaunch(c->sweep_exec[mf], c->stream));
+  if (done < nsweeps) {
+    cudaGraphExec_t ex;
+    int rc = sweep_graph(c, c->mode, mf, &ex);
+    if (rc) return rc;
+    for (int i = done; i < nsweeps; ++i) CK(cudaGraphLaunch(ex, c->stream));
+  }
   return LCE_OK;
 }
+
+int lce_get_sweep_mode(lce_ctx* c) { return c ? c->mode : LCE_ERR_INVALID; }
 
 int lce_sweep(lce_ctx* c, int measflag, lce_meas* m) {
   int rc = lce_sweeps(c, 1, measflag);

@@ -99,8 +99,7 @@ struct LinkIO<float> {
   __device__ static su2<float> ld_cg(const void* base, size_t i) {
     float4 v = __ldcg(reinterpret_cast<const float4*>(base) + i);
     return su2<float>{{v.x, v.y}, {v.z, v.w}};
-  }
-  __device__ static void st(void* base, size_t i, su2<float> u) {
+  }  __device__ static void st(void* base, size_t i, su2<float> u) {
     reinterpret_cast<float4*>(base)[i] = make_float4(u.a.re, u.a.im, u.b.re, u.b.im);
   }
 };
@@ -314,6 +313,7 @@ __device__ __forceinline__ void block_reduce_cs(const unsigned (&cnt)[NC > 0 ? N
   __shared__ unsigned redc[32][NC > 0 ? NC : 1];
   __shared__ double redd[32][ND > 0 ? ND : 1];
   const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+  __syncthreads();  // a previous call's readers are done with the shared slots
   unsigned cw[NC > 0 ? NC : 1];
 #pragma unroll
   for (int q = 0; q < NC; ++q) cw[q] = __reduce_add_sync(0xffffffffu, cnt[q]);

@@ -74,6 +74,22 @@ struct ChainState {
 enum : unsigned int {
   kStatusStreamExhausted = 1u,
   kStatusNaN = 2u,
+  kStatusBarrierTimeout = 4u,
+};
+
+// grid barrier of the persistent sweep kernel (zeroed at context creation)
+struct GridBar {
+  unsigned count;  // arrivals, only ever incremented (wraps; compared as a difference)
+  unsigned base;   // count at the start of the next launch
+};
+// polls of a grid barrier before the kernel gives up (>= 20 ns sleep each: >= 1.3 s)
+constexpr unsigned kBarrierSpinLimit = 1u << 26;
+constexpr int kPersistMinBlocks = 4;  // register cap 64 for the all-pass kernel
+constexpr unsigned char kNoSlot = 0xff;
+
+// one pass of a planned sweep
+struct PlanEntry {
+  unsigned char kind, eo, mu, slot;  // slot: reduction slot or kNoSlot
 };
 
 struct PassArgs {
@@ -108,7 +124,21 @@ struct FinalizeArgs {
   unsigned char kinds[kMaxSlots];
 };
 
+struct PersistArgs {
+  PassArgs base;          // per-pass fields (eo, part, offsets) are filled in the kernel
+  FinalizeArgs fin;
+  GridBar* bar;
+  int ntiles;             // tiles per pass (all chains)
+  int npasses;
+  PlanEntry plan[kMaxSlots];
+  unsigned long long stream_off[kMaxSlots];
+};
+
 // ---- launchers (lce_update.cu)
+template <typename R>
+int persistent_grid();  // co-resident blocks of the persistent kernel on this device
+template <typename R>
+cudaError_t launch_persistent(const PersistArgs& a, int grid, cudaStream_t s);
 template <typename R>
 void launch_higgs(int mode, const PassArgs& a, int nblocks, cudaStream_t s);
 template <typename R>

@@ -1,18 +1,27 @@
 // lce_update.cu -- checkerboard Monte Carlo update kernels.
 //
-// One kernel launch per (routine, parity[, mu]) pass, one thread per site.
-// Each kernel fuses what the reference does as a chain of whole-lattice array
-// passes (multall*, halo exchanges, temporaries): neighbour gathers, the SU(2)
-// algebra, the random proposal, the accept/reject and the FP64 partial sums
-// of the measurements, so every field element is read from HBM once per pass.
+// One pass = one routine over one parity (and one mu for links), one thread
+// per site, sites grouped in tiles of kBlock consecutive sites of one chain.
+// The per-tile bodies fuse what the reference does as a chain of whole-lattice
+// array passes (multall*, halo exchanges, temporaries): neighbour gathers, the
+// SU(2) algebra, the random proposal, the accept/reject and the FP64 partial
+// sums of the measurements, so every field element is read from HBM once per
+// pass.
 //
-//   higgs_kernel<R, MODE>   f/a_force.f + f/ahiggs2.f (MODE 0, heatbath),
-//                           f/ahiggs3.f (MODE 1, overrelaxation),
-//                           f/ahiggs1.f (MODE 2, Metropolis)
-//   link_kernel<R, MU, OR>  f/staples.f + f/agauge.f + f/heat_kpi.f (OR = 0);
-//                           link overrelaxation (OR = 1, no reference)
-//   finalize_kernel         deterministic FP64 reduction of the per-block
-//                           partials into /aver_loc/-style results (f/meas1.f)
+//   higgs_tile<R, MODE>    f/a_force.f + f/ahiggs2.f (MODE 0, heatbath),
+//                          f/ahiggs3.f (MODE 1, overrelaxation),
+//                          f/ahiggs1.f (MODE 2, Metropolis)
+//   link_tile<R, MU, OR>   f/staples.f + f/agauge.f + f/heat_kpi.f (OR = 0);
+//                          link overrelaxation (OR = 1, no reference)
+//   finalize_sum/combine   deterministic FP64 reduction of the per-tile
+//                          partials into /aver_loc/-style results (f/meas1.f)
+//
+// Two execution forms share these bodies:
+//   * one kernel per pass (higgs_kernel, link_kernel, finalize_kernel),
+//     chained with programmatic dependent launch and captured in a graph;
+//   * sweep_persistent_kernel: one cooperative launch per sweep whose blocks
+//     loop over the tile work list of every pass, with a bounded grid barrier
+//     between passes (no kernel boundaries inside the sweep).
 //
 // Random numbers: Philox4x32-10 keyed by the chain seed with counter
 // (site, call, pass), or, in validation mode, the host-supplied stream indexed
@@ -37,9 +46,17 @@ __device__ __forceinline__ int find_chain(const int* blk_begin, int n, int b) {
   return lo;
 }
 
-template <typename R>
+// Field loads.  NC = true: the read-only (non-coherent) path, valid when no
+// earlier writer runs in the same kernel (the per-pass form).  NC = false:
+// L2 loads (ld.global.cg) for the persistent form, where fields written by
+// other blocks before a grid barrier are read after it.  Ordinary cached
+// loads are not enough there: measured on B200, lines an SM's L1 fetched
+// before the barrier were still served after it (the persistent sweep then
+// differs from the per-pass sweep), so L1 is bypassed.
+template <typename R, bool NC = true>
 __device__ __forceinline__ R ldA(const R* A, int nh, int p, int k, int s) {
-  return __ldg(A + ((size_t)(p * 3 + k)) * nh + s);
+  const R* q = A + ((size_t)(p * 3 + k)) * nh + s;
+  return NC ? __ldg(q) : __ldcg(q);
 }
 
 // neighbour of X one step along mu (d = +1 / -1), index inside its parity
@@ -64,68 +81,69 @@ __device__ __forceinline__ int nbr2(const ChainDev& ch, Coord X, int d1, int d2)
   return site_index(x, y, z, ch.hx, ch.nxy);
 }
 
-template <typename R>
+template <typename R, bool NC = true>
 __device__ __forceinline__ su2<R> ldU(const ChainDev& ch, int mu, int p, int s) {
-  return LinkIO<R>::ld(ch.u, ((size_t)(mu * 2 + p)) * ch.nh + s);
+  const size_t i = ((size_t)(mu * 2 + p)) * ch.nh + s;
+  return NC ? LinkIO<R>::ld(ch.u, i) : LinkIO<R>::ld_cg(ch.u, i);
 }
 
 // f/staples.f:259-415: for each nu != mu (ascending),
 //   upper  = U_nu(x+mu) [U_mu(x+nu)^+ U_nu(x)^+]          (NN of DD)
 //   lower  = U_nu(x-nu+mu)^+ [U_mu(x-nu)^+ U_nu(x-nu)]    (DN of DN)
 //   V      = (V + upper) + lower
-template <typename R, int MU, int NU>
+template <typename R, int MU, int NU, bool NC>
 __device__ __forceinline__ void staple_add(const ChainDev& ch, int eo, Coord X, int s, su2<R>& V) {
   const int oe = 1 - eo;
   const int xpmu = nbr<MU>(ch, X, +1), xpnu = nbr<NU>(ch, X, +1), xmnu = nbr<NU>(ch, X, -1);
   const int xmnupmu = nbr2<NU, MU>(ch, X, -1, +1);
-  su2<R> up1 = dd(ldU<R>(ch, MU, oe, xpnu), ldU<R>(ch, NU, eo, s));
-  su2<R> up2 = nn(ldU<R>(ch, NU, oe, xpmu), up1);
-  su2<R> bt1 = dn(ldU<R>(ch, MU, oe, xmnu), ldU<R>(ch, NU, oe, xmnu));
-  su2<R> bt2 = dn(ldU<R>(ch, NU, eo, xmnupmu), bt1);
+  su2<R> up1 = dd(ldU<R, NC>(ch, MU, oe, xpnu), ldU<R, NC>(ch, NU, eo, s));
+  su2<R> up2 = nn(ldU<R, NC>(ch, NU, oe, xpmu), up1);
+  su2<R> bt1 = dn(ldU<R, NC>(ch, MU, oe, xmnu), ldU<R, NC>(ch, NU, oe, xmnu));
+  su2<R> bt2 = dn(ldU<R, NC>(ch, NU, eo, xmnupmu), bt1);
   V.a = (V.a + up2.a) + bt2.a;
   V.b = (V.b + up2.b) + bt2.b;
 }
 
-template <typename R, int MU>
+template <typename R, int MU, bool NC = true>
 __device__ __forceinline__ su2<R> staple(const ChainDev& ch, int eo, Coord X, int s) {
   su2<R> V{{(R)0, (R)0}, {(R)0, (R)0}};
   if (MU == 0) {
-    staple_add<R, 0, 1>(ch, eo, X, s, V);
-    staple_add<R, 0, 2>(ch, eo, X, s, V);
+    staple_add<R, 0, 1, NC>(ch, eo, X, s, V);
+    staple_add<R, 0, 2, NC>(ch, eo, X, s, V);
   } else if (MU == 1) {
-    staple_add<R, 1, 0>(ch, eo, X, s, V);
-    staple_add<R, 1, 2>(ch, eo, X, s, V);
+    staple_add<R, 1, 0, NC>(ch, eo, X, s, V);
+    staple_add<R, 1, 2, NC>(ch, eo, X, s, V);
   } else {
-    staple_add<R, 2, 0>(ch, eo, X, s, V);
-    staple_add<R, 2, 1>(ch, eo, X, s, V);
+    staple_add<R, 2, 0, NC>(ch, eo, X, s, V);
+    staple_add<R, 2, 1, NC>(ch, eo, X, s, V);
   }
   return V;
 }
 
 // f/a_force.f:54-110: F = sum_mu [U(x)(iA(x+mu))U(x)^+ + U(x-mu)^+(iA(x-mu))U(x-mu)],
 // components F3 = Im(.)_a, F2 = Re(.)_b, F1 = Im(.)_b
-template <typename R, int MU>
+template <typename R, int MU, bool NC>
 __device__ __forceinline__ void force_add(const ChainDev& ch, int eo, Coord X, int s, R& f1, R& f2,
                                           R& f3) {
   const int oe = 1 - eo, nh = ch.nh;
   const R* A = reinterpret_cast<const R*>(ch.a);
   const int xp = nbr<MU>(ch, X, +1), xm = nbr<MU>(ch, X, -1);
-  su2<R> ux = ldU<R>(ch, MU, eo, s);
-  su2<R> ud = ldU<R>(ch, MU, oe, xm);
-  su2<R> t1 = nn(ux, ad(ldA(A, nh, oe, 0, xp), ldA(A, nh, oe, 1, xp), ldA(A, nh, oe, 2, xp), ux));
-  su2<R> tb = dn(ud, an(ldA(A, nh, oe, 0, xm), ldA(A, nh, oe, 1, xm), ldA(A, nh, oe, 2, xm), ud));
+  su2<R> ux = ldU<R, NC>(ch, MU, eo, s);
+  su2<R> ud = ldU<R, NC>(ch, MU, oe, xm);
+  su2<R> t1 = nn(ux, ad(ldA<R, NC>(A, nh, oe, 0, xp), ldA<R, NC>(A, nh, oe, 1, xp), ldA<R, NC>(A, nh, oe, 2, xp), ux));
+  su2<R> tb = dn(ud, an(ldA<R, NC>(A, nh, oe, 0, xm), ldA<R, NC>(A, nh, oe, 1, xm), ldA<R, NC>(A, nh, oe, 2, xm), ud));
   f3 = f3 + (t1.a.im + tb.a.im);
   f2 = f2 + (t1.b.re + tb.b.re);
   f1 = f1 + (t1.b.im + tb.b.im);
 }
 
-template <typename R>
+template <typename R, bool NC = true>
 __device__ __forceinline__ void higgs_force(const ChainDev& ch, int eo, Coord X, int s, R& f1, R& f2,
                                             R& f3) {
   f1 = f2 = f3 = (R)0;
-  force_add<R, 0>(ch, eo, X, s, f1, f2, f3);
-  force_add<R, 1>(ch, eo, X, s, f1, f2, f3);
-  force_add<R, 2>(ch, eo, X, s, f1, f2, f3);
+  force_add<R, 0, NC>(ch, eo, X, s, f1, f2, f3);
+  force_add<R, 1, NC>(ch, eo, X, s, f1, f2, f3);
+  force_add<R, 2, NC>(ch, eo, X, s, f1, f2, f3);
 }
 
 // Set up the uniform source of this pass.  Returns false (and flags the
@@ -147,29 +165,31 @@ __device__ __forceinline__ bool setup_uniforms(const PassArgs& p, const ChainDev
 }
 
 // ------------------------------------------------------------------ Higgs
-template <typename R, int MODE>
-__global__ void __launch_bounds__(kBlock, min_blocks<R>()) higgs_kernel(PassArgs p) {
-  pdl_trigger();
+// One tile (kBlock consecutive sites of one chain) of a Higgs pass.  PDL:
+// trigger dependents and wait for the previous kernel (per-pass form only).
+template <typename R, int MODE, bool PDL>
+__device__ __forceinline__ void higgs_tile(const PassArgs& p, int tile) {
+  if (PDL) pdl_trigger();
   // the chain table is written once at context creation: safe before pdl_wait
-  const int c = p.nchains > 1 ? find_chain(p.blk_begin, p.nchains, blockIdx.x) : 0;
+  const int c = p.nchains > 1 ? find_chain(p.blk_begin, p.nchains, tile) : 0;
   const ChainDev& ch = p.chains[c];
-  const int s = (blockIdx.x - __ldg(p.blk_begin + c)) * kBlock + threadIdx.x;
+  const int s = (tile - __ldg(p.blk_begin + c)) * kBlock + threadIdx.x;
   const int eo = p.eo, nh = ch.nh;
   const Coord X = site_coord(eo, s < nh ? s : 0, ch.hx, ch.nxy, ch.dhx, ch.dnxy);
   unsigned acc[1] = {0u};
   double q[3] = {0.0, 0.0, 0.0};
-  pdl_wait();
+  if (PDL) pdl_wait();
   if (s < nh) {
     constexpr int NS = MODE == 0 ? 7 : (MODE == 1 ? 1 : 4);
     const int layout = MODE == 2 ? kTriple : kPlanar;
     Uniforms<R, NS> Un;
     if (setup_uniforms<R, NS>(p, ch, s, layout, Un)) {
       R f[3];
-      higgs_force<R>(ch, eo, X, s, f[0], f[1], f[2]);
+      higgs_force<R, PDL>(ch, eo, X, s, f[0], f[1], f[2]);
       R* A = reinterpret_cast<R*>(ch.a);
       R ao[3], an_[3];
 #pragma unroll
-      for (int k = 0; k < 3; ++k) ao[k] = A[((size_t)(eo * 3 + k)) * nh + s];
+      for (int k = 0; k < 3; ++k) ao[k] = PDL ? A[((size_t)(eo * 3 + k)) * nh + s] : __ldcg(A + ((size_t)(eo * 3 + k)) * nh + s);
       const R beta_a = (R)ch.beta_a, beta_2 = (R)ch.beta_2, beta_4 = (R)ch.beta_4;
       R alph = (R)0, sf_o = (R)0, sf_n = (R)0;
       if constexpr (MODE == 0 || MODE == 1) {
@@ -246,27 +266,27 @@ __global__ void __launch_bounds__(kBlock, min_blocks<R>()) higgs_kernel(PassArgs
     }
   }
   // partials {accepted, sum rho, sum rho^2, sum a.F}
-  if (p.part) block_reduce_cs<1, 3, kNQ>(acc, q, p.part + (size_t)blockIdx.x * kNQ);
+  if (p.part) block_reduce_cs<1, 3, kNQ>(acc, q, p.part + (size_t)tile * kNQ);
 }
 
 // ------------------------------------------------------------------ links
-template <typename R, int MU, int OR>
-__global__ void __launch_bounds__(kBlock, min_blocks<R>()) link_kernel(PassArgs p) {
-  pdl_trigger();
-  const int c = p.nchains > 1 ? find_chain(p.blk_begin, p.nchains, blockIdx.x) : 0;
+template <typename R, int MU, int OR, bool PDL>
+__device__ __forceinline__ void link_tile(const PassArgs& p, int tile) {
+  if (PDL) pdl_trigger();
+  const int c = p.nchains > 1 ? find_chain(p.blk_begin, p.nchains, tile) : 0;
   const ChainDev& ch = p.chains[c];
-  const int s = (blockIdx.x - __ldg(p.blk_begin + c)) * kBlock + threadIdx.x;
+  const int s = (tile - __ldg(p.blk_begin + c)) * kBlock + threadIdx.x;
   const int eo = p.eo, oe = 1 - eo, nh = ch.nh;
   const Coord X = site_coord(eo, s < nh ? s : 0, ch.hx, ch.nxy, ch.dhx, ch.dnxy);
   unsigned cnt[2] = {0u, 0u};
   double pl[1] = {0.0};
-  pdl_wait();
+  if (PDL) pdl_wait();
   if (s < nh) {
     Uniforms<R, OR ? 1 : 7> Un;
     if (setup_uniforms<R, OR ? 1 : 7>(p, ch, s, OR ? kPlanar : kTriple, Un)) {
-      const su2<R> V = staple<R, MU>(ch, eo, X, s);
+      const su2<R> V = staple<R, MU, PDL>(ch, eo, X, s);
       const size_t li = ((size_t)(MU * 2 + eo)) * nh + s;
-      const su2<R> uo = LinkIO<R>::ld(ch.u, li);
+      const su2<R> uo = PDL ? LinkIO<R>::ld(ch.u, li) : LinkIO<R>::ld_cg(ch.u, li);
       // f/agauge.f:71-84: normalised staple, 1/(beta |V|), 1/2 Re Tr(U Vhat)
       R t1 = M<R>::rsqrt(norm2(V));
       const su2<R> vh{{t1 * V.a.re, t1 * V.a.im}, {t1 * V.b.re, t1 * V.b.im}};
@@ -303,8 +323,8 @@ __global__ void __launch_bounds__(kBlock, min_blocks<R>()) link_kernel(PassArgs 
       // f/agauge.f:126-174 hopping term beta_a Re[(iA(x) U)(iA(x+mu) U^+)]_11 and accept
       const R* A = reinterpret_cast<const R*>(ch.a);
       const int xp = nbr<MU>(ch, X, +1);
-      const R x1 = ldA(A, nh, eo, 0, s), x2 = ldA(A, nh, eo, 1, s), x3 = ldA(A, nh, eo, 2, s);
-      const R y1 = ldA(A, nh, oe, 0, xp), y2 = ldA(A, nh, oe, 1, xp), y3 = ldA(A, nh, oe, 2, xp);
+      const R x1 = ldA<R, PDL>(A, nh, eo, 0, s), x2 = ldA<R, PDL>(A, nh, eo, 1, s), x3 = ldA<R, PDL>(A, nh, eo, 2, s);
+      const R y1 = ldA<R, PDL>(A, nh, oe, 0, xp), y2 = ldA<R, PDL>(A, nh, oe, 1, xp), y3 = ldA<R, PDL>(A, nh, oe, 2, xp);
       const R beta_a = (R)ch.beta_a;
       const R sa_old = beta_a * nn(an(x1, x2, x3, uo), ad(y1, y2, y3, uo)).a.re;
       const R sa_new = beta_a * nn(an(x1, x2, x3, hn), ad(y1, y2, y3, hn)).a.re;
@@ -320,44 +340,44 @@ __global__ void __launch_bounds__(kBlock, min_blocks<R>()) link_kernel(PassArgs 
   }
   // partials {KP accepted, Metropolis accepted, sum plaquette} / {OR accepted}
   if (p.part) {
-    if constexpr (!OR) block_reduce_cs<2, 1, kNQ>(cnt, pl, p.part + (size_t)blockIdx.x * kNQ);
+    if constexpr (!OR) block_reduce_cs<2, 1, kNQ>(cnt, pl, p.part + (size_t)tile * kNQ);
     else {
       unsigned c1[1] = {cnt[0]};
       double d0[1] = {0.0};
-      block_reduce_cs<1, 0, kNQ>(c1, d0, p.part + (size_t)blockIdx.x * kNQ);
+      block_reduce_cs<1, 0, kNQ>(c1, d0, p.part + (size_t)tile * kNQ);
     }
   }
 }
 
+template <typename R, int MODE>
+__global__ void __launch_bounds__(kBlock, min_blocks<R>()) higgs_kernel(PassArgs p) {
+  higgs_tile<R, MODE, true>(p, blockIdx.x);
+}
+
+template <typename R, int MU, int OR>
+__global__ void __launch_bounds__(kBlock, min_blocks<R>()) link_kernel(PassArgs p) {
+  link_tile<R, MU, OR, true>(p, blockIdx.x);
+}
+
 // ------------------------------------------------------------------ finalize
-// grid = nchains * nslots blocks (+ at least one); block (c, i) sums the
-// partials of chain c in slot i in a fixed order; the last block combines
-// them per chain in the reference's normalisations and advances the RNG.
-__global__ void __launch_bounds__(256) finalize_kernel(FinalizeArgs f) {
-  pdl_trigger();
-  pdl_wait();
-  const int nwork = f.nchains * f.nslots;
-  if ((int)blockIdx.x < nwork) {
-    const int c = blockIdx.x / f.nslots, i = blockIdx.x % f.nslots;
-    const int b0 = f.blk_begin[c], b1 = f.blk_begin[c + 1];
-    const double* part = f.part + (size_t)i * f.slot_stride;
-    double v[kNQ] = {0.0, 0.0, 0.0, 0.0};
-    for (int b = b0 + threadIdx.x; b < b1; b += blockDim.x) {
+// Work item w = (chain c, slot i): sum the partials of chain c in slot i in a
+// fixed order into totals[c][i].
+__device__ __forceinline__ void finalize_sum(const FinalizeArgs& f, int w) {
+  const int c = w / f.nslots, i = w % f.nslots;
+  const int b0 = f.blk_begin[c], b1 = f.blk_begin[c + 1];
+  const double* part = f.part + (size_t)i * f.slot_stride;
+  double v[kNQ] = {0.0, 0.0, 0.0, 0.0};
+  for (int b = b0 + threadIdx.x; b < b1; b += blockDim.x) {
 #pragma unroll
-      for (int q = 0; q < kNQ; ++q) v[q] += part[(size_t)b * kNQ + q];
-    }
-    block_reduce_store<kNQ>(v, f.totals + ((size_t)c * kMaxSlots + i) * kNQ);
-  }
-  __shared__ bool last;
-  __threadfence();
-  __syncthreads();
-  if (threadIdx.x == 0) {
-    unsigned int t = atomicAdd(&f.st->ticket, 1u);
-    last = (t == gridDim.x - 1);
+    for (int q = 0; q < kNQ; ++q) v[q] += __ldcg(part + (size_t)b * kNQ + q);
   }
   __syncthreads();
-  if (!last) return;
-  __threadfence();
+  block_reduce_store<kNQ>(v, f.totals + ((size_t)c * kMaxSlots + i) * kNQ);
+}
+
+// Per chain, in slot order, the reference's normalisations; then advance the
+// RNG counters.  Run by one block after every finalize_sum has completed.
+__device__ __forceinline__ void finalize_combine(const FinalizeArgs& f) {
   for (int c = threadIdx.x; c < f.nchains; c += blockDim.x) {
     const ChainDev& ch = f.chains[c];
     const double V = 2.0 * ch.nh;
@@ -418,7 +438,121 @@ __global__ void __launch_bounds__(256) finalize_kernel(FinalizeArgs f) {
   if (threadIdx.x == 0) {
     f.st->pass_ctr += f.npasses;
     f.st->stream_pos += f.nstream;
-    f.st->ticket = 0;
+  }
+}
+
+// grid = nchains * nslots blocks (at least one); the last block to finish its
+// sum combines.
+__global__ void __launch_bounds__(256) finalize_kernel(FinalizeArgs f) {
+  pdl_trigger();
+  pdl_wait();
+  if ((int)blockIdx.x < f.nchains * f.nslots) finalize_sum(f, blockIdx.x);
+  __shared__ bool last;
+  __threadfence();
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    unsigned int t = atomicAdd(&f.st->ticket, 1u);
+    last = (t == gridDim.x - 1);
+  }
+  __syncthreads();
+  if (!last) return;
+  __threadfence();
+  finalize_combine(f);
+  if (threadIdx.x == 0) f.st->ticket = 0;
+}
+
+// ------------------------------------------------------------------ persistent sweep
+// Grid barrier for a cooperative launch (every block resident).  The arrival
+// counter only grows: barrier k of a launch waits for count >= base +
+// (k+1)*nblocks, where base (the count when the launch began) is stored in
+// device memory by block 0 at the end of the previous launch.  Thread 0 of
+// each block makes the block's writes visible (acq_rel fence after the block
+// barrier), arrives with a non-returning release add, and polls the count
+// with acquire loads and a bounded number of short sleeps.  On timeout the
+// block records the status bit and the kernel returns instead of spinning on.
+__device__ __forceinline__ void fence_acq_rel_gpu() { asm volatile("fence.acq_rel.gpu;" ::: "memory"); }
+__device__ __forceinline__ void red_release_add(unsigned* p, unsigned v) {
+  asm volatile("red.release.gpu.global.add.u32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
+}
+__device__ __forceinline__ unsigned ld_acquire(const unsigned* p) {
+  unsigned v;
+  asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+  return v;
+}
+
+__device__ __forceinline__ bool grid_sync(GridBar* bar, unsigned nblocks, unsigned& target, unsigned* status) {
+  __shared__ int s_ok;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    int ok = 1;
+    fence_acq_rel_gpu();
+    red_release_add(&bar->count, 1u);
+    target += nblocks;
+    unsigned spins = 0;
+    while ((int)(ld_acquire(&bar->count) - target) < 0) {
+      if (++spins > kBarrierSpinLimit) {
+        ok = 0;
+        atomicOr(status, kStatusBarrierTimeout);
+        break;
+      }
+      __nanosleep(20);
+    }
+    fence_acq_rel_gpu();
+    s_ok = ok;
+  }
+  __syncthreads();
+  return s_ok != 0;
+}
+
+template <typename R>
+__device__ __forceinline__ void persistent_pass(const PersistArgs& a, const PassArgs& p, const PlanEntry& e) {
+  const int nt = a.ntiles;
+  switch (e.kind) {
+    case kHiggsHB:
+      for (int t = blockIdx.x; t < nt; t += gridDim.x) higgs_tile<R, 0, false>(p, t);
+      break;
+    case kHiggsOR:
+      for (int t = blockIdx.x; t < nt; t += gridDim.x) higgs_tile<R, 1, false>(p, t);
+      break;
+    case kHiggsMetro:
+      for (int t = blockIdx.x; t < nt; t += gridDim.x) higgs_tile<R, 2, false>(p, t);
+      break;
+    case kLinkHB:
+      if (e.mu == 0) for (int t = blockIdx.x; t < nt; t += gridDim.x) link_tile<R, 0, 0, false>(p, t);
+      else if (e.mu == 1) for (int t = blockIdx.x; t < nt; t += gridDim.x) link_tile<R, 1, 0, false>(p, t);
+      else for (int t = blockIdx.x; t < nt; t += gridDim.x) link_tile<R, 2, 0, false>(p, t);
+      break;
+    default:
+      if (e.mu == 0) for (int t = blockIdx.x; t < nt; t += gridDim.x) link_tile<R, 0, 1, false>(p, t);
+      else if (e.mu == 1) for (int t = blockIdx.x; t < nt; t += gridDim.x) link_tile<R, 1, 1, false>(p, t);
+      else for (int t = blockIdx.x; t < nt; t += gridDim.x) link_tile<R, 2, 1, false>(p, t);
+      break;
+  }
+}
+
+// One sweep: every pass over the (chain, tile) work list, a grid barrier
+// between passes, then the finalize reduction -- a single cooperative launch.
+template <typename R>
+__global__ void __launch_bounds__(kBlock, kPersistMinBlocks) sweep_persistent_kernel(PersistArgs a) {
+  // only thread 0 of each block tracks the barrier target
+  unsigned target = 0;
+  if (threadIdx.x == 0) target = *(volatile unsigned*)&a.bar->base;
+  PassArgs p = a.base;
+  for (int i = 0; i < a.npasses; ++i) {
+    const PlanEntry e = a.plan[i];
+    p.eo = e.eo;
+    p.pass_off = (unsigned)i;
+    p.stream_off = a.stream_off[i];
+    p.part = e.slot == kNoSlot ? nullptr : const_cast<double*>(a.fin.part) + (size_t)e.slot * a.fin.slot_stride;
+    persistent_pass<R>(a, p, e);
+    if (!grid_sync(a.bar, gridDim.x, target, &a.base.st->status)) return;
+  }
+  for (int w = blockIdx.x; w < a.fin.nchains * a.fin.nslots; w += gridDim.x) finalize_sum(a.fin, w);
+  if (!grid_sync(a.bar, gridDim.x, target, &a.base.st->status)) return;
+  if (blockIdx.x == 0) {
+    finalize_combine(a.fin);
+    // every block has passed the last barrier: record where the count stands
+    if (threadIdx.x == 0) *(volatile unsigned*)&a.bar->base = target;
   }
 }
 
@@ -481,6 +615,30 @@ void launch_finalize(const FinalizeArgs& f, cudaStream_t s) {
 }
 
 template <typename R>
+int persistent_grid() {
+  int dev = 0, nsm = 0, per = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess) return 0;
+  if (cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess) return 0;
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, sweep_persistent_kernel<R>, kBlock, 0) != cudaSuccess)
+    return 0;
+  return per * nsm;
+}
+
+template <typename R>
+cudaError_t launch_persistent(const PersistArgs& a, int grid, cudaStream_t s) {
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = grid;
+  cfg.blockDim = kBlock;
+  cfg.stream = s;
+  cudaLaunchAttribute attr[1];
+  attr[0].id = cudaLaunchAttributeCooperative;
+  attr[0].val.cooperative = 1;
+  cfg.attrs = attr;
+  cfg.numAttrs = 1;
+  return cudaLaunchKernelEx(&cfg, sweep_persistent_kernel<R>, a);
+}
+
+template <typename R>
 void launch_renorm(void* u, size_t nlinks, cudaStream_t s) {
   int grid = (int)std::min<size_t>((nlinks + 255) / 256, 148 * 16);
   renorm_kernel<R><<<grid, 256, 0, s>>>(u, nlinks);
@@ -502,6 +660,8 @@ void launch_debug_force(const ChainDev* ch, int eo, double* out, int nh, cudaStr
 #define LCE_INST(R)                                                                          \
   template void launch_higgs<R>(int, const PassArgs&, int, cudaStream_t);                  \
   template void launch_link<R>(int, int, const PassArgs&, int, cudaStream_t);              \
+  template int persistent_grid<R>();                                                         \
+  template cudaError_t launch_persistent<R>(const PersistArgs&, int, cudaStream_t);          \
   template void launch_renorm<R>(void*, size_t, cudaStream_t);                             \
   template void launch_debug_staple<R>(const ChainDev*, int, int, double*, int, cudaStream_t); \
   template void launch_debug_force<R>(const ChainDev*, int, double*, int, cudaStream_t);

@@ -30,6 +30,8 @@ from ._lib import LceMeas, LceParams, check, load
 
 PREC = {"f32": _lib.LCE_PREC_F32, "f64": _lib.LCE_PREC_F64}
 RNG = {"philox": _lib.LCE_RNG_PHILOX, "stream": _lib.LCE_RNG_STREAM}
+SWEEP_MODES = {"auto": _lib.LCE_SWEEP_AUTO, "passes": _lib.LCE_SWEEP_PASSES,
+               "persistent": _lib.LCE_SWEEP_PERSISTENT}
 
 
 def _ptr(a: np.ndarray):
@@ -55,6 +57,7 @@ class Params:
     n_higgs_metro: int = 0
     delta0: float = 1.0
     gf_angle: str = "atan2"
+    sweep_mode: str = "auto"
 
     def to_c(self) -> LceParams:
         p = LceParams()
@@ -72,6 +75,7 @@ class Params:
         p.n_higgs_metro = int(self.n_higgs_metro)
         p.delta0 = float(self.delta0)
         p.gf_angle = {"acos": _lib.LCE_GF_ACOS, "atan2": _lib.LCE_GF_ATAN2}[self.gf_angle]
+        p.sweep_mode = SWEEP_MODES[self.sweep_mode]
         return p
 
 
@@ -203,6 +207,10 @@ class _Context:
 
     def sweeps(self, n: int, measflag: int = 0):
         self._ck(self.lib.lce_sweeps(self.h, int(n), measflag))
+
+    def sweep_mode(self) -> str:
+        m = self._ck(self.lib.lce_get_sweep_mode(self.h))
+        return {v: k for k, v in SWEEP_MODES.items()}[m]
 
     def meas1(self, chain: int = 0) -> dict:
         m = LceMeas()

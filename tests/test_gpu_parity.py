@@ -237,6 +237,58 @@ def test_batch_equals_single_chains():
             assert mb[i][k] == ms[k]
 
 
+@pytest.mark.parametrize("L", [(4, 4, 4), (16, 16, 16), (32, 16, 24)])
+def test_persistent_sweep_equals_pass_kernels(L):
+    """The cooperative persistent sweep kernel (one launch per sweep, grid
+    barriers between passes) reproduces the per-pass kernel graph bit for bit."""
+    res = []
+    for mode in ("passes", "persistent"):
+        g = Lattice(L, beta=12.0, x=0.09, y=0.3, seed=99, sweep_mode=mode)
+        g.init_hot(7)
+        for mf in (1, 0, 1):
+            g.sweeps(2, mf)
+        m = g.meas1()
+        assert g.sweep_mode() == mode
+        res.append((g.download(), m, g.rng_position()))
+    (u0, a0), m0, r0 = res[0]
+    (u1, a1), m1, r1 = res[1]
+    np.testing.assert_array_equal(u0, u1)
+    np.testing.assert_array_equal(a0, a1)
+    assert m0 == m1 and r0 == r1
+
+
+def test_persistent_batch_and_autotune():
+    # a batch shares one sweep composition: here with a link-OR hit and ahiggs1
+    specs = [Params(L=(16, 16, 16), beta=6.0, x=0.1, y=0.1, seed=5, n_link_or=1, n_higgs_metro=1),
+             Params(L=(8, 12, 6), beta=16.0, x=0.08, y=0.5, seed=6, n_link_or=1, n_higgs_metro=1, imode=1)]
+    outs = []
+    for mode in ("passes", "persistent", "auto"):
+        ens = Ensemble([Params(**{**s.__dict__, "sweep_mode": mode}) for s in specs])
+        ens.init_hot(3)
+        ens.sweeps(12, 1)
+        if mode == "auto":
+            assert ens.sweep_mode() in ("passes", "persistent")
+        outs.append(([ens.download(chain=i) for i in range(2)], ens.meas_batch()))
+    for o in outs[1:]:
+        for i in range(2):
+            np.testing.assert_array_equal(o[0][i][0], outs[0][0][i][0])
+            np.testing.assert_array_equal(o[0][i][1], outs[0][0][i][1])
+        assert o[1] == outs[0][1]
+
+
+def test_persistent_fp64_stream_matches_oracle():
+    L = (6, 4, 8)
+    o, g, _, _ = pair(L, seed=33, sweep_mode="persistent")
+    stream = reference_stream(2 * uniforms_per_sweep(L), seed=4711)
+    o.set_stream(stream)
+    g.set_rng_stream(stream)
+    for _ in range(2):
+        mo, mg = o.sweep(1), g.sweep(1)
+        for k in ("plaq", "akin", "a2", "a4", "acc_gauge", "acc_hb", "acc_or"):
+            assert abs(mo[k] - mg[k]) <= 1e-11 * max(1, abs(mo[k])), k
+    assert rel_err(g.download(dtype=np.float64)[0], o.get_fields()[0]) < 1e-11
+
+
 @pytest.mark.parametrize("precision", ["f32", "f64"])
 def test_upload_download_roundtrip(precision):
     L = (6, 4, 4)
