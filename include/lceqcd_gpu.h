@@ -137,6 +137,8 @@ lce_ctx* lce_create(const lce_params* p);
 lce_ctx* lce_create_batch(const lce_params* p, int nchains);
 void lce_destroy(lce_ctx* ctx);
 int lce_nchains(lce_ctx* ctx);
+/* lattice extents of a chain */
+int lce_get_extents(lce_ctx* ctx, int chain, int L[3]);
 int lce_set_stream(lce_ctx* ctx, void* cuda_stream); /* NULL: the context's own stream */
 int lce_synchronize(lce_ctx* ctx);
 
@@ -149,6 +151,21 @@ int lce_download_f64(lce_ctx* ctx, int chain, int which, double* u, double* a, l
 int lce_init_unit(lce_ctx* ctx, double a3);
 /* hot start: Haar links (normalised 4-Gaussians), A components ~ N(0,1) */
 int lce_init_hot(lce_ctx* ctx, unsigned long long seed);
+
+/* ---- configuration files (f/confsave.f:18-258, f/confget.f oldconf :318-526) ----
+ * Direct-access unformatted records, single precision: links one record per
+ * (mu, eo, z), Higgs one per (eo, z), each one global xy slice in half-row
+ * order, record lengths u_rl = 16*2*L1*L2/2 and a_rl = 8*3*L1*L2/2 bytes as the
+ * reference declares them (payload first, zero padding).  lce_confsave also
+ * writes "<u_path>.rng" (Philox pass counter); lce_confget restores it when
+ * present, so a resumed chain continues its random stream. */
+int lce_confsave(lce_ctx* ctx, int chain, const char* u_path, const char* a_path);
+int lce_confget(lce_ctx* ctx, int chain, const char* u_path, const char* a_path);
+/* f/measinit.f file names: "<prefix>_sLL_beBBBBB_xXXXXX_yYYYYY_uNNNNNN" with
+ * BBBBB = nint(1000 beta), XXXXX = nint(10000 x), YYYYY = nint(10000 y); the
+ * reference's lower-case "_be" / "_u" form is used for saving too */
+int lce_conf_filename(char* buf, size_t n, const char* prefix, int L3, double beta, double x, double y,
+                      int number);
 
 /* ---- random numbers ---- */
 /* validation mode (LCE_RNG_STREAM, single chain): uniforms consumed in the

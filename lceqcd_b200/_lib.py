@@ -73,6 +73,10 @@ SIGNATURES = {
     "lce_create_batch": (P, [P, I]),
     "lce_destroy": (None, [P]),
     "lce_nchains": (I, [P]),
+    "lce_get_extents": (I, [P, I, P]),
+    "lce_confsave": (I, [P, I, C.c_char_p, C.c_char_p]),
+    "lce_confget": (I, [P, I, C.c_char_p, C.c_char_p]),
+    "lce_conf_filename": (I, [C.c_char_p, C.c_size_t, C.c_char_p, I, D, D, D, I]),
     "lce_set_stream": (I, [P, P]),
     "lce_synchronize": (I, [P]),
     "lce_upload": (I, [P, I, I, P, P, C.c_long]),

@@ -780,6 +780,14 @@ void lce_destroy(lce_ctx* c) {
 
 int lce_nchains(lce_ctx* c) { return c ? c->nchains : LCE_ERR_INVALID; }
 
+int lce_get_extents(lce_ctx* c, int chain, int L[3]) {
+  if (!c || !L || chain < 0 || chain >= c->nchains) return LCE_ERR_INVALID;
+  L[0] = c->ch[chain].L1;
+  L[1] = c->ch[chain].L2;
+  L[2] = c->ch[chain].L3;
+  return LCE_OK;
+}
+
 int lce_set_stream(lce_ctx* c, void* s) {
   if (!c) return LCE_ERR_INVALID;
   c->stream = s ? (cudaStream_t)s : c->own;

@@ -87,6 +87,14 @@ def couplings(beta: float, x: float, y: float, precision: str = "f64"):
     return tuple(out)
 
 
+def conf_filename(prefix: str, L3: int, beta: float, x: float, y: float, number: int) -> str:
+    """f/measinit.f names, e.g. conf_filename('action', 16, 9.0, 0.1, 0.45, 0)."""
+    buf = C.create_string_buffer(256)
+    check(load().lce_conf_filename(buf, 256, prefix.encode(), int(L3), float(beta), float(x), float(y),
+                                   int(number)))
+    return buf.value.decode()
+
+
 def geometry_tables(L):
     """siteup/sitedn of f/adresses.f (0-based), [eo, mu, site]."""
     nh = L[0] * L[1] * L[2] // 2
@@ -151,6 +159,19 @@ class _Context:
         assert u.dtype == a.dtype and u.size == 24 * nh and a.size == 6 * nh
         fn = self.lib.lce_download_f64 if u.dtype == np.float64 else self.lib.lce_download
         self._ck(fn(self.h, chain, which, _ptr(u), _ptr(a), nh))
+
+    def extents(self, chain: int = 0):
+        L = (C.c_int * 3)()
+        self._ck(self.lib.lce_get_extents(self.h, chain, L))
+        return tuple(L)
+
+    def confsave(self, u_path: str, a_path: str, chain: int = 0):
+        """f/confsave.f format (+ '<u_path>.rng' with the Philox position)."""
+        self._ck(self.lib.lce_confsave(self.h, chain, u_path.encode(), a_path.encode()))
+
+    def confget(self, u_path: str, a_path: str, chain: int = 0):
+        """f/confget.f oldconf format; restores the Philox position if the sidecar exists."""
+        self._ck(self.lib.lce_confget(self.h, chain, u_path.encode(), a_path.encode()))
 
     def init_unit(self, a3: float = 1.0):
         self._ck(self.lib.lce_init_unit(self.h, float(a3)))
