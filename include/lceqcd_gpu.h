@@ -209,6 +209,24 @@ int lce_get_meas_batch(lce_ctx* ctx, lce_meas* m /* [nchains] */);
 int lce_landau_gauge(lce_ctx* ctx, int chain, double* theta, int* iters, int max_iters);
 /* iterate on the current U_f,A_f without the copy (warm starts, continuation) */
 int lce_gauge_fix_continue(lce_ctx* ctx, int chain, double* theta, int* iters, int max_iters);
+/* Gauge fixing that also tracks the accumulated transform G, with
+ * U_f(x,mu) = G(x) U(x,mu) G(x+mu)^+ and A_f = G A G^+ throughout (no
+ * reference counterpart: the reference keeps no transform).  start:
+ *   LCE_GF_START_IDENTITY   G = 1 (the reference's start, f/landau_gauge.f:308-324)
+ *   LCE_GF_START_TRANSFORM  start from the context's current G (warm start:
+ *                           the previous measurement's converged transform,
+ *                           a transform set by lce_set_transform, or one
+ *                           predicted by lce_net_predict)
+ * theta_start (may be NULL) receives theta of the starting U_f. */
+#define LCE_GF_START_IDENTITY 0
+#define LCE_GF_START_TRANSFORM 1
+int lce_landau_gauge_from(lce_ctx* ctx, int chain, int start, double* theta_start, double* theta, int* iters,
+                          int max_iters);
+/* U_f, A_f := (U, A) transformed by the current G */
+int lce_apply_transform(lce_ctx* ctx, int chain);
+/* the transform field G: g[(eo*ld + site)*4 + c], SU(2) first rows like the links */
+int lce_set_transform(lce_ctx* ctx, int chain, const float* g, long ld);
+int lce_get_transform(lce_ctx* ctx, int chain, float* g, long ld);
 /* gauge functional (1/((2+alpha)V)) sum_x,mu c_mu Re a of U_f */
 int lce_gauge_functional(lce_ctx* ctx, int chain, double* value);
 /* theta of the current U_f (odd sites, FP64), without updating */

@@ -32,6 +32,8 @@ LCE_SWEEP_PASSES = 1
 LCE_SWEEP_PERSISTENT = 2
 LCE_FIELDS = 0
 LCE_FIELDS_FIXED = 1
+LCE_GF_START_IDENTITY = 0
+LCE_GF_START_TRANSFORM = 1
 
 
 class LceParams(C.Structure):
@@ -101,6 +103,10 @@ SIGNATURES = {
     "lce_get_meas_batch": (I, [P, P]),
     "lce_landau_gauge": (I, [P, I, P, P, I]),
     "lce_gauge_fix_continue": (I, [P, I, P, P, I]),
+    "lce_landau_gauge_from": (I, [P, I, I, P, P, P, I]),
+    "lce_apply_transform": (I, [P, I]),
+    "lce_set_transform": (I, [P, I, P, C.c_long]),
+    "lce_get_transform": (I, [P, I, P, C.c_long]),
     "lce_gauge_functional": (I, [P, I, P]),
     "lce_theta": (I, [P, I, P]),
     "lce_correlator": (I, [P, I, P, P, P, P]),

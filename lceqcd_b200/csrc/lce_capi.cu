@@ -558,7 +558,7 @@ lce_ctx* create_impl(const lce_params* p, int n) {
     d.key0 = (uint32_t)p[i].seed;
     d.key1 = (uint32_t)(p[i].seed >> 32);
     offs.push_back(off);
-    off += 2 * (align256((size_t)6 * d.nh * lb) + align256((size_t)6 * d.nh * rb));
+    off += 2 * (align256((size_t)6 * d.nh * lb) + align256((size_t)6 * d.nh * rb)) + align256((size_t)2 * d.nh * lb);
     c->ch.push_back(d);
     c->blk.push_back(c->blk.back() + ceil_div(d.nh, kBlock));
     c->max_nh = std::max(c->max_nh, d.nh);
@@ -573,6 +573,7 @@ lce_ctx* create_impl(const lce_params* p, int n) {
     d.a = b + ul;
     d.uf = b + ul + al;
     d.af = b + 2 * ul + al;
+    d.g = b + 2 * ul + 2 * al;
   }
   if ((e = cudaMemset(c->fields_d, 0, off)) != cudaSuccess) return bail(e, "cudaMemset(fields)");
   if ((e = cudaMalloc(&c->ch_d, sizeof(ChainDev) * n)) != cudaSuccess) return bail(e, "cudaMalloc(chains)");
@@ -639,7 +640,7 @@ int get_slices(lce_ctx* c, int chain, double*& out) {
   return LCE_OK;
 }
 
-int gf_loop(lce_ctx* c, int chain, double* theta, int* iters, int max_iters) {
+int gf_loop(lce_ctx* c, int chain, double* theta, int* iters, int max_iters, int track = 0) {
   const ChainDev& ch = c->ch[chain];
   // bounded on the device in every case; no cap requested means 10^6
   const int cap = max_iters > 0 ? max_iters : 1000000;
@@ -655,16 +656,16 @@ int gf_loop(lce_ctx* c, int chain, double* theta, int* iters, int max_iters) {
   double* part = c->scratch_d;
   int batch = 8;
   while (true) {
-    auto key = std::make_pair(chain, batch);
+    auto key = std::make_pair(chain, 2 * batch + (track ? 1 : 0));
     auto it = c->gf_exec.find(key);
     if (it == c->gf_exec.end()) {
       cudaGraph_t g;
       CK(cudaStreamBeginCapture(c->stream, cudaStreamCaptureModeThreadLocal));
       for (int k = 0; k < batch; ++k) {
         if (c->prec == LCE_PREC_F64)
-          launch_gf_iteration<double>(c->ch_d + chain, c->cst_d + chain, chain, part, ch.nh, c->stream);
+          launch_gf_iteration<double>(c->ch_d + chain, c->cst_d + chain, track, part, ch.nh, c->stream);
         else
-          launch_gf_iteration<float>(c->ch_d + chain, c->cst_d + chain, chain, part, ch.nh, c->stream);
+          launch_gf_iteration<float>(c->ch_d + chain, c->cst_d + chain, track, part, ch.nh, c->stream);
       }
       CK(cudaStreamEndCapture(c->stream, &g));
       cudaGraphExec_t ex;
@@ -1004,6 +1005,72 @@ int lce_landau_gauge(lce_ctx* c, int chain, double* theta, int* iters, int max_i
 int lce_gauge_fix_continue(lce_ctx* c, int chain, double* theta, int* iters, int max_iters) {
   if (!c || chain < 0 || chain >= c->nchains) return LCE_ERR_INVALID;
   return gf_loop(c, chain, theta, iters, max_iters);
+}
+
+int lce_apply_transform(lce_ctx* c, int chain) {
+  if (!c || chain < 0 || chain >= c->nchains) return LCE_ERR_INVALID;
+  if (c->prec == LCE_PREC_F64) launch_gauge_apply<double>(c->ch_d + chain, c->ch[chain].nh, c->stream);
+  else launch_gauge_apply<float>(c->ch_d + chain, c->ch[chain].nh, c->stream);
+  CK(cudaGetLastError());
+  return LCE_OK;
+}
+
+int lce_landau_gauge_from(lce_ctx* c, int chain, int start, double* theta_start, double* theta, int* iters,
+                          int max_iters) {
+  if (!c || chain < 0 || chain >= c->nchains) return LCE_ERR_INVALID;
+  const ChainDev& ch = c->ch[chain];
+  if (start == LCE_GF_START_IDENTITY) {
+    if (c->prec == LCE_PREC_F64) launch_transform_identity<double>(ch.g, ch.nh, c->stream);
+    else launch_transform_identity<float>(ch.g, ch.nh, c->stream);
+    const size_t ub = (size_t)6 * ch.nh * link_bytes(c->prec), ab = (size_t)6 * ch.nh * real_bytes(c->prec);
+    CK(cudaMemcpyAsync(ch.uf, ch.u, ub, cudaMemcpyDeviceToDevice, c->stream));
+    CK(cudaMemcpyAsync(ch.af, ch.a, ab, cudaMemcpyDeviceToDevice, c->stream));
+  } else if (start == LCE_GF_START_TRANSFORM) {
+    int rc = lce_apply_transform(c, chain);
+    if (rc) return rc;
+  } else {
+    return fail(c, LCE_ERR_INVALID, "landau_gauge_from: unknown start");
+  }
+  if (theta_start) {
+    int rc = lce_theta(c, chain, theta_start);
+    if (rc) return rc;
+  }
+  return gf_loop(c, chain, theta, iters, max_iters, 1);
+}
+
+int lce_set_transform(lce_ctx* c, int chain, const float* g, long ld) {
+  if (!c || !g || chain < 0 || chain >= c->nchains || ld < c->ch[chain].nh) return LCE_ERR_INVALID;
+  const ChainDev& ch = c->ch[chain];
+  const int nh = ch.nh;
+  if (c->prec == LCE_PREC_F32) {
+    CK(cudaMemcpy2DAsync(ch.g, (size_t)nh * 16, g, (size_t)ld * 16, (size_t)nh * 16, 2, cudaMemcpyHostToDevice,
+                         c->stream));
+  } else {
+    std::vector<double> h((size_t)2 * nh * 4);
+    for (int eo = 0; eo < 2; ++eo)
+      for (long i = 0; i < (long)nh * 4; ++i) h[(size_t)eo * nh * 4 + i] = g[(size_t)eo * ld * 4 + i];
+    CK(cudaMemcpyAsync(ch.g, h.data(), h.size() * sizeof(double), cudaMemcpyHostToDevice, c->stream));
+  }
+  CK(cudaStreamSynchronize(c->stream));
+  return LCE_OK;
+}
+
+int lce_get_transform(lce_ctx* c, int chain, float* g, long ld) {
+  if (!c || !g || chain < 0 || chain >= c->nchains || ld < c->ch[chain].nh) return LCE_ERR_INVALID;
+  const ChainDev& ch = c->ch[chain];
+  const int nh = ch.nh;
+  if (c->prec == LCE_PREC_F32) {
+    CK(cudaMemcpy2DAsync(g, (size_t)ld * 16, ch.g, (size_t)nh * 16, (size_t)nh * 16, 2, cudaMemcpyDeviceToHost,
+                         c->stream));
+    CK(cudaStreamSynchronize(c->stream));
+  } else {
+    std::vector<double> h((size_t)2 * nh * 4);
+    CK(cudaMemcpyAsync(h.data(), ch.g, h.size() * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+    CK(cudaStreamSynchronize(c->stream));
+    for (int eo = 0; eo < 2; ++eo)
+      for (long i = 0; i < (long)nh * 4; ++i) g[(size_t)eo * ld * 4 + i] = (float)h[(size_t)eo * nh * 4 + i];
+  }
+  return LCE_OK;
 }
 
 int lce_gauge_functional(lce_ctx* c, int chain, double* value) {

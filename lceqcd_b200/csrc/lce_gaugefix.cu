@@ -59,9 +59,11 @@ __device__ __forceinline__ void gf_sums(const ChainDev& ch, const su2<R> (&um)[3
   t2.b = t2.b + mk<double>(al * ud[2].b.re, al * ud[2].b.im);
 }
 
+// track != 0: also accumulate the gauge transform, G(x) -> Omega(x) G(x), so
+// that U_f(x,mu) = G(x) U(x,mu) G(x+mu)^+ holds throughout
 template <typename R>
 __global__ void __launch_bounds__(kBlock) gf_half_kernel(const ChainDev* chp, const ChainState* cst, int eo,
-                                                         double* part) {
+                                                         double* part, int track) {
   pdl_trigger();
   const ChainDev& ch = *chp;
   const int s = blockIdx.x * kBlock + threadIdx.x;
@@ -138,8 +140,47 @@ __global__ void __launch_bounds__(kBlock) gf_half_kernel(const ChainDev* chp, co
       LinkIO<R>::st(ch.uf, ((size_t)(mu * 2 + eo)) * nh + s, a);
       LinkIO<R>::st(ch.uf, ((size_t)(mu * 2 + oe)) * nh + xm[mu], b);
     }
+    if (track) {
+      const size_t gi = (size_t)eo * nh + s;
+      LinkIO<R>::st(ch.g, gi, unitarise64(nn(o, LinkIO<R>::ld_cg(ch.g, gi))));
+    }
   }
   if (eo == 1) block_reduce_store<1>(th, part + blockIdx.x);
+}
+
+// U_f(x,mu) = G(x) U(x,mu) G(x+mu)^+ and A_f(x) -> G(x) A(x) G(x)^+, one
+// thread per site of both parities
+template <typename R>
+__global__ void __launch_bounds__(kBlock) gauge_apply_kernel(const ChainDev* chp) {
+  const ChainDev& ch = *chp;
+  const int i = blockIdx.x * kBlock + threadIdx.x;
+  if (i >= 2 * ch.nh) return;
+  const int eo = i >= ch.nh ? 1 : 0, oe = 1 - eo, s = i - eo * ch.nh, nh = ch.nh;
+  const Coord X = site_coord(eo, s, ch.hx, ch.nxy, ch.dhx, ch.dnxy);
+  const su2<R> gx = LinkIO<R>::ld(ch.g, (size_t)eo * nh + s);
+  const int L[3] = {ch.L1, ch.L2, ch.L3};
+#pragma unroll
+  for (int mu = 0; mu < 3; ++mu) {
+    int c[3] = {X.x, X.y, X.z};
+    c[mu] = wrap(c[mu] + 1, L[mu]);
+    const int sp = site_index(c[0], c[1], c[2], ch.hx, ch.nxy);
+    const su2<R> gp = LinkIO<R>::ld(ch.g, (size_t)oe * nh + sp);
+    const size_t li = ((size_t)(mu * 2 + eo)) * nh + s;
+    LinkIO<R>::st(ch.uf, li, unitarise64(nd(nn(gx, LinkIO<R>::ld(ch.u, li)), gp)));
+  }
+  const R* A = reinterpret_cast<const R*>(ch.a);
+  R* Af = reinterpret_cast<R*>(ch.af);
+  const su2<R> t = nn(gx, ad(A[((size_t)(eo * 3 + 0)) * nh + s], A[((size_t)(eo * 3 + 1)) * nh + s],
+                             A[((size_t)(eo * 3 + 2)) * nh + s], gx));
+  Af[((size_t)(eo * 3 + 0)) * nh + s] = t.b.im;
+  Af[((size_t)(eo * 3 + 1)) * nh + s] = t.b.re;
+  Af[((size_t)(eo * 3 + 2)) * nh + s] = t.a.im;
+}
+
+template <typename R>
+__global__ void transform_identity_kernel(void* g, size_t n) {
+  for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x)
+    LinkIO<R>::st(g, i, su2<R>{{(R)1, (R)0}, {(R)0, (R)0}});
 }
 
 // sum the theta partials in block order, count the iteration, test convergence
@@ -199,14 +240,28 @@ __global__ void __launch_bounds__(1024) sum_partials_kernel(const double* part, 
 }
 
 template <typename R>
-void launch_gf_iteration(const ChainDev* ch, ChainState* cst, int chain, double* part, int nh, cudaStream_t s) {
-  (void)chain;
+void launch_gf_iteration(const ChainDev* ch, ChainState* cst, int track, double* part, int nh, cudaStream_t s) {
   const int nb = ceil_div(nh, kBlock);
   // programmatic dependent launch: each kernel waits in griddepcontrol.wait
-  (void)launch_pdl(gf_half_kernel<R>, nb, kBlock, 0, s, ch, (const ChainState*)cst, 0, part);
-  (void)launch_pdl(gf_half_kernel<R>, nb, kBlock, 0, s, ch, (const ChainState*)cst, 1, part);
+  (void)launch_pdl(gf_half_kernel<R>, nb, kBlock, 0, s, ch, (const ChainState*)cst, 0, part, track);
+  (void)launch_pdl(gf_half_kernel<R>, nb, kBlock, 0, s, ch, (const ChainState*)cst, 1, part, track);
   (void)launch_pdl(gf_check_kernel, 1, 1024, 0, s, ch, cst, (const double*)part, nb);
 }
+
+template <typename R>
+void launch_gauge_apply(const ChainDev* ch, int nh, cudaStream_t s) {
+  gauge_apply_kernel<R><<<ceil_div(2L * nh, kBlock), kBlock, 0, s>>>(ch);
+}
+
+template <typename R>
+void launch_transform_identity(void* g, int nh, cudaStream_t s) {
+  transform_identity_kernel<R><<<ceil_div(2L * nh, 256), 256, 0, s>>>(g, (size_t)2 * nh);
+}
+
+template void launch_gauge_apply<float>(const ChainDev*, int, cudaStream_t);
+template void launch_gauge_apply<double>(const ChainDev*, int, cudaStream_t);
+template void launch_transform_identity<float>(void*, int, cudaStream_t);
+template void launch_transform_identity<double>(void*, int, cudaStream_t);
 
 template <typename R>
 void launch_gf_theta(const ChainDev* ch, double* part, int nh, cudaStream_t s) {

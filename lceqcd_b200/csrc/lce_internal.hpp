@@ -48,6 +48,7 @@ struct ChainDev {
   void* a;
   void* uf;
   void* af;
+  void* g;   // gauge transform of the last tracked gauge fixing, [parity][site]
 };
 
 // mutable state shared by the chains of one context
@@ -169,8 +170,12 @@ void launch_flush(void* buf, size_t bytes, cudaStream_t s);
 
 // ---- gauge fixing (lce_gaugefix.cu)
 template <typename R>
-void launch_gf_iteration(const ChainDev* ch, ChainState* cst, int chain, double* part, int nh,
+void launch_gf_iteration(const ChainDev* ch, ChainState* cst, int track, double* part, int nh,
                          cudaStream_t s);
+template <typename R>
+void launch_gauge_apply(const ChainDev* ch, int nh, cudaStream_t s);
+template <typename R>
+void launch_transform_identity(void* g, int nh, cudaStream_t s);
 template <typename R>
 void launch_gf_theta(const ChainDev* ch, double* part, int nh, cudaStream_t s);
 void launch_sum_partials(const double* part, int nblocks, int nq, double* out, cudaStream_t s);

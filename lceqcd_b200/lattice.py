@@ -257,6 +257,27 @@ class _Context:
         self._ck(self.lib.lce_gauge_fix_continue(self.h, chain, C.byref(th), C.byref(it), int(max_iters)))
         return th.value, it.value
 
+    def landau_gauge_from(self, start: str = "identity", max_iters: int = 0, chain: int = 0):
+        """Gauge fixing tracking the transform G; start 'identity' or 'transform'
+        (the current G).  Returns (theta_start, theta, iterations)."""
+        ts, th, it = C.c_double(), C.c_double(), C.c_int()
+        code = {"identity": _lib.LCE_GF_START_IDENTITY, "transform": _lib.LCE_GF_START_TRANSFORM}[start]
+        self._ck(self.lib.lce_landau_gauge_from(self.h, chain, code, C.byref(ts), C.byref(th), C.byref(it),
+                                                int(max_iters)))
+        return ts.value, th.value, it.value
+
+    def apply_transform(self, chain: int = 0):
+        self._ck(self.lib.lce_apply_transform(self.h, chain))
+
+    def get_transform(self, chain: int = 0) -> np.ndarray:
+        g = np.zeros((2, self.nh(chain), 4), np.float32)
+        self._ck(self.lib.lce_get_transform(self.h, chain, _ptr(g), self.nh(chain)))
+        return g
+
+    def set_transform(self, g: np.ndarray, chain: int = 0):
+        gg = np.ascontiguousarray(g, np.float32).reshape(2, self.nh(chain), 4)
+        self._ck(self.lib.lce_set_transform(self.h, chain, _ptr(gg), self.nh(chain)))
+
     def gauge_functional(self, chain: int = 0) -> float:
         v = C.c_double()
         self._ck(self.lib.lce_gauge_functional(self.h, chain, C.byref(v)))

@@ -159,6 +159,34 @@ def test_gauge_fixing_convergence_fp64(angle, limit):
     np.testing.assert_allclose(af, o.meas2(), rtol=1e-9, atol=1e-13)
 
 
+@pytest.mark.parametrize("precision,tol", [("f64", 1e-12), ("f32", 2e-5)])
+def test_tracked_transform_reproduces_fixed_fields(precision, tol):
+    """With transform tracking, U_f = G U G^+ and A_f = G A G^+ at every step:
+    re-applying the final G to (U, A) gives the gauge-fixed fields, and a
+    restart from G is converged at once."""
+    L = (8, 6, 4)
+    g = Lattice(L, **COUP, precision=precision, lam=1.7, limit_or=1e-11)
+    g.init_hot(5)
+    th0, th, it = g.landau_gauge_from("identity")
+    assert th <= 1e-11 and it > 5 and th0 > th
+    uf, af = g.download(which=1, dtype=np.float64)
+    # identity start tracks the same iteration as the plain gauge fixing
+    h = Lattice(L, **COUP, precision=precision, lam=1.7, limit_or=1e-11)
+    h.upload(*g.download(dtype=np.float64))
+    h.landau_gauge()
+    np.testing.assert_allclose(h.download(which=1, dtype=np.float64)[0], uf, atol=tol)
+    g.apply_transform()
+    u2, a2 = g.download(which=1, dtype=np.float64)
+    np.testing.assert_allclose(u2, uf, atol=100 * tol)
+    np.testing.assert_allclose(a2, af, atol=100 * tol * max(1, np.abs(af).max()))
+    ts, th2, it2 = g.landau_gauge_from("transform")
+    assert ts <= 1e-10 and it2 <= 2
+    gt = g.get_transform()
+    np.testing.assert_allclose(np.linalg.norm(gt, axis=-1), 1.0, atol=1e-6)
+    g.set_transform(gt)
+    np.testing.assert_array_equal(g.get_transform(), gt)
+
+
 @pytest.mark.parametrize("L", [(4, 4, 6), (8, 4, 4)])
 def test_measurements_fp64(L):
     o, g, u, a = pair(L, seed=19)
