@@ -215,8 +215,7 @@ int lce_gauge_fix_continue(lce_ctx* ctx, int chain, double* theta, int* iters, i
  *   LCE_GF_START_IDENTITY   G = 1 (the reference's start, f/landau_gauge.f:308-324)
  *   LCE_GF_START_TRANSFORM  start from the context's current G (warm start:
  *                           the previous measurement's converged transform,
- *                           a transform set by lce_set_transform, or one
- *                           predicted by lce_net_predict)
+ *                           a transform set by lce_set_transform)
  * theta_start (may be NULL) receives theta of the starting U_f. */
 #define LCE_GF_START_IDENTITY 0
 #define LCE_GF_START_TRANSFORM 1
@@ -276,6 +275,53 @@ int lce_timer_stop(lce_ctx* ctx, float* ms);
  * capture).  All calls share the array: calls whose kernels overlap on the GPU
  * race and must be serialised by the caller. */
 int lce_plaquette_noalloc(const float* u, long ld, int L1, int L2, int L3, double* plaq, void* stream);
+
+/* ---- learned warm start for Landau gauge fixing (no reference counterpart;
+ * the reference always starts f/landau_gauge.f from G = 1).
+ * A 4-layer, 16-channel, 3x3x3 periodic convolutional network (BF16 weights
+ * and activations, FP32 accumulation on the tensor cores) maps the
+ * configuration in the gauge of the previous converged transform G_prev
+ * (12 link components of U_f and 3 of A_f per site) to a unit quaternion
+ * Omega(x); the warm start is G = Omega G_prev.  The network is trained on
+ * the device from pairs recorded by lce_landau_gauge_warm (target: the
+ * converged G_new G_prev^+; loss 1 - Omega . target per site, Adam).
+ * Nothing about the gauge-fixed result depends on the network: the plain
+ * overrelaxed iteration runs to the same theta <= limit_or from whichever
+ * start is taken.  A network object is not thread-safe. */
+typedef struct lce_net lce_net;
+lce_net* lce_net_create(int device, unsigned long long seed);  /* untrained: Omega = 1 */
+void lce_net_destroy(lce_net* net);
+int lce_net_num_params(lce_net* net);
+/* parameters, FP32 master copy: per layer [27][16 out][16 in] weights then 16 biases */
+int lce_net_get_params(lce_net* net, float* w);
+int lce_net_set_params(lce_net* net, const float* w);
+int lce_net_save(lce_net* net, const char* path);
+int lce_net_load(lce_net* net, const char* path);
+/* forward + loss + gradient on caller data, no update: feat [2][V/2][16]
+ * (parity-split site order, rounded to BF16), target [2][V/2][4]; out
+ * [2][V/2][4] (raw network output) and grad [nparam] may be NULL */
+int lce_net_eval(lce_net* net, int L1, int L2, int L3, const float* feat, const float* target, float* out,
+                 float* grad, double* loss);
+int lce_net_num_pairs(lce_net* net);
+int lce_net_clear_pairs(lce_net* net);
+/* `epochs` Adam passes over the recorded pairs; *mean_loss = last epoch's */
+int lce_net_train(lce_net* net, int epochs, double lr, double* mean_loss);
+
+/* Tracked gauge fixing of `chain` from a warm start.  Candidates: the
+ * identity (0), the previous transform G_prev held by the context (1), and,
+ * with LCE_WARM_NET, the network's Omega G_prev (2).  With LCE_WARM_JUDGE
+ * every candidate's gauge functional is evaluated (functional[0..2], NaN for
+ * one not evaluated) and the start with the largest is taken -- the fallback
+ * to the plain start when the prediction is worse; otherwise the network's
+ * start (LCE_WARM_NET) or G_prev.  LCE_WARM_RECORD stores the pair
+ * (configuration in G_prev gauge, G_new G_prev^+) for lce_net_train after
+ * convergence.  net may be NULL when neither NET nor RECORD is set. */
+#define LCE_WARM_NET 1
+#define LCE_WARM_JUDGE 2
+#define LCE_WARM_RECORD 4
+#define LCE_GF_START_NET 2
+int lce_landau_gauge_warm(lce_ctx* ctx, int chain, lce_net* net, int flags, int* start_used, double functional[3],
+                          double* theta, int* iters, int max_iters);
 
 #if defined(__GNUC__)
 #pragma GCC visibility pop

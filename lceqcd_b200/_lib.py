@@ -34,6 +34,10 @@ LCE_FIELDS = 0
 LCE_FIELDS_FIXED = 1
 LCE_GF_START_IDENTITY = 0
 LCE_GF_START_TRANSFORM = 1
+LCE_GF_START_NET = 2
+LCE_WARM_NET = 1
+LCE_WARM_JUDGE = 2
+LCE_WARM_RECORD = 4
 
 
 class LceParams(C.Structure):
@@ -120,6 +124,18 @@ SIGNATURES = {
     "lce_timer_start": (I, [P]),
     "lce_timer_stop": (I, [P, P]),
     "lce_plaquette_noalloc": (I, [P, C.c_long, I, I, I, P, P]),
+    "lce_net_create": (P, [I, C.c_ulonglong]),
+    "lce_net_destroy": (None, [P]),
+    "lce_net_num_params": (I, [P]),
+    "lce_net_get_params": (I, [P, P]),
+    "lce_net_set_params": (I, [P, P]),
+    "lce_net_save": (I, [P, C.c_char_p]),
+    "lce_net_load": (I, [P, C.c_char_p]),
+    "lce_net_eval": (I, [P, I, I, I, P, P, P, P, P]),
+    "lce_net_num_pairs": (I, [P]),
+    "lce_net_clear_pairs": (I, [P]),
+    "lce_net_train": (I, [P, I, D, P]),
+    "lce_landau_gauge_warm": (I, [P, I, P, I, P, P, P, P, I]),
 }
 
 _lib = None

@@ -62,6 +62,7 @@ struct lce_ctx {
   size_t staging_bytes = 0;
   void* flush_d = nullptr;
   size_t flush_bytes = 0;
+  void* gsave_d = nullptr;  // G_prev during a warm-started gauge fixing
   cudaStream_t own = nullptr, stream = nullptr;
   cudaEvent_t ev0 = nullptr, ev1 = nullptr;
   cudaGraphExec_t sweep_exec[2] = {nullptr, nullptr};     // per-pass kernels, per measflag
@@ -770,7 +771,8 @@ void lce_destroy(lce_ctx* c) {
   }
   for (auto& kv : c->gf_exec) cudaGraphExecDestroy(kv.second);
   void* ptrs[] = {c->ch_d, c->blk_d, c->st_d, c->cst_d, c->meas_d, c->part_d, c->totals_d,
-                  c->scratch_d, c->fields_d, c->stream_d, c->staging_d, c->flush_d, c->bar_d};
+                  c->scratch_d, c->fields_d, c->stream_d, c->staging_d, c->flush_d, c->bar_d,
+                  c->gsave_d};
   for (void* q : ptrs)
     if (q) cudaFree(q);
   if (c->ev0) cudaEventDestroy(c->ev0);
@@ -1036,6 +1038,72 @@ int lce_landau_gauge_from(lce_ctx* c, int chain, int start, double* theta_start,
     if (rc) return rc;
   }
   return gf_loop(c, chain, theta, iters, max_iters, 1);
+}
+
+int lce_landau_gauge_warm(lce_ctx* c, int chain, lce_net* net, int flags, int* start_used, double functional[3],
+                          double* theta, int* iters, int max_iters) {
+  if (!c || chain < 0 || chain >= c->nchains || (flags & ~(LCE_WARM_NET | LCE_WARM_JUDGE | LCE_WARM_RECORD)))
+    return LCE_ERR_INVALID;
+  const bool use_net = flags & LCE_WARM_NET, judge = flags & LCE_WARM_JUDGE, record = flags & LCE_WARM_RECORD;
+  if ((use_net || record) && !net) return fail(c, LCE_ERR_INVALID, "landau_gauge_warm: no network given");
+  if (net && net_device(net) != c->device) return fail(c, LCE_ERR_INVALID, "landau_gauge_warm: network on another device");
+  const ChainDev& ch = c->ch[chain];
+  const bool f64 = c->prec == LCE_PREC_F64;
+  const size_t gb = (size_t)2 * ch.nh * link_bytes(c->prec);
+  if (!c->gsave_d) CK(cudaMalloc(&c->gsave_d, (size_t)2 * c->max_nh * link_bytes(c->prec)));
+  double F[3] = {NAN, NAN, NAN};
+  int rc;
+  // candidate 1: G_prev
+  CK(cudaMemcpyAsync(c->gsave_d, ch.g, gb, cudaMemcpyDeviceToDevice, c->stream));
+  if ((rc = lce_apply_transform(c, chain))) return rc;
+  if (judge && (rc = lce_gauge_functional(c, chain, &F[1]))) return rc;
+  if (use_net || record) {
+    if ((rc = net_features(net, c->ch_d + chain, ch, f64, c->stream))) return fail(c, rc, "network features");
+  }
+  // candidate 2: Omega G_prev
+  if (use_net) {
+    net_predict(net, ch, c->stream);
+    if (judge) {
+      if ((rc = net_compose(net, ch, c->gsave_d, f64, c->stream))) return fail(c, rc, "network compose");
+      if ((rc = lce_apply_transform(c, chain))) return rc;
+      if ((rc = lce_gauge_functional(c, chain, &F[2]))) return rc;
+    }
+  }
+  // candidate 0: the identity, the reference's start
+  if (judge) {
+    const size_t ub = (size_t)6 * ch.nh * link_bytes(c->prec), ab = (size_t)6 * ch.nh * real_bytes(c->prec);
+    CK(cudaMemcpyAsync(ch.uf, ch.u, ub, cudaMemcpyDeviceToDevice, c->stream));
+    CK(cudaMemcpyAsync(ch.af, ch.a, ab, cudaMemcpyDeviceToDevice, c->stream));
+    if ((rc = lce_gauge_functional(c, chain, &F[0]))) return rc;
+  }
+  int pick = use_net ? LCE_GF_START_NET : LCE_GF_START_TRANSFORM;
+  if (judge) {
+    pick = LCE_GF_START_IDENTITY;
+    if (F[1] > F[pick]) pick = LCE_GF_START_TRANSFORM;
+    if (use_net && F[2] > F[pick]) pick = LCE_GF_START_NET;
+  }
+  if (pick == LCE_GF_START_IDENTITY) {
+    // U_f, A_f already hold U, A
+    if (f64) launch_transform_identity<double>(ch.g, ch.nh, c->stream);
+    else launch_transform_identity<float>(ch.g, ch.nh, c->stream);
+  } else {
+    if (pick == LCE_GF_START_TRANSFORM) {
+      CK(cudaMemcpyAsync(ch.g, c->gsave_d, gb, cudaMemcpyDeviceToDevice, c->stream));
+    } else if ((rc = net_compose(net, ch, c->gsave_d, f64, c->stream))) {
+      return fail(c, rc, "network compose");
+    }
+    if ((rc = lce_apply_transform(c, chain))) return rc;
+  }
+  CK(cudaGetLastError());
+  if (start_used) *start_used = pick;
+  if (functional)
+    for (int k = 0; k < 3; ++k) functional[k] = F[k];
+  rc = gf_loop(c, chain, theta, iters, max_iters, 1);
+  if (rc == LCE_OK && record) {
+    if ((rc = net_record(net, ch, c->gsave_d, f64, c->stream))) return fail(c, rc, "record training pair");
+    CK(cudaStreamSynchronize(c->stream));
+  }
+  return rc;
 }
 
 int lce_set_transform(lce_ctx* c, int chain, const float* g, long ld) {

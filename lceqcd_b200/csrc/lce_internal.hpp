@@ -191,6 +191,16 @@ void launch_functional(const ChainDev* ch, double* part, int nh, cudaStream_t s)
 
 inline int ceil_div(long a, long b) { return (int)((a + b - 1) / b); }
 
+// ---- learned warm start (lce_net.cu); all work on stream s
+int net_device(lce_net* n);
+// network input from the chain's U_f, A_f
+int net_features(lce_net* n, const ChainDev* chd, const ChainDev& ch, bool f64, cudaStream_t s);
+void net_predict(lce_net* n, const ChainDev& ch, cudaStream_t s);
+// ch.g = Omega G_prev from the last prediction
+int net_compose(lce_net* n, const ChainDev& ch, const void* gprev, bool f64, cudaStream_t s);
+// record (last features, ch.g G_prev^+) as a training pair
+int net_record(lce_net* n, const ChainDev& ch, const void* gprev, bool f64, cudaStream_t s);
+
 // message returned by lce_last_error(NULL) on this host thread
 void set_thread_error(const std::string& msg);
 

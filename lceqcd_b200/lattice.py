@@ -266,6 +266,21 @@ class _Context:
                                                 int(max_iters)))
         return ts.value, th.value, it.value
 
+    def landau_gauge_warm(self, net=None, use_net: bool = True, judge: bool = True, record: bool = False,
+                          max_iters: int = 0, chain: int = 0):
+        """Tracked gauge fixing from a warm start (the previous transform, or the
+        network's correction of it; with judge the start of largest gauge
+        functional among identity / previous / network).  Returns
+        (start, functionals[3], theta, iterations); start is 'identity',
+        'transform' or 'net'."""
+        flags = ((_lib.LCE_WARM_NET if (use_net and net is not None) else 0) |
+                 (_lib.LCE_WARM_JUDGE if judge else 0) | (_lib.LCE_WARM_RECORD if record else 0))
+        su, th, it = C.c_int(), C.c_double(), C.c_int()
+        F = (C.c_double * 3)()
+        self._ck(self.lib.lce_landau_gauge_warm(self.h, chain, net.h if net is not None else None, flags,
+                                                C.byref(su), F, C.byref(th), C.byref(it), int(max_iters)))
+        return ["identity", "transform", "net"][su.value], list(F), th.value, it.value
+
     def apply_transform(self, chain: int = 0):
         self._ck(self.lib.lce_apply_transform(self.h, chain))
 
@@ -340,6 +355,72 @@ class _Context:
         ms = C.c_float()
         self._ck(self.lib.lce_timer_stop(self.h, C.byref(ms)))
         return ms.value
+
+
+class GaugeNet:
+    """The warm-start network of lce_landau_gauge_warm (4 layers, 16 channels,
+    3x3x3 periodic kernels, BF16 on the tensor cores; no reference
+    counterpart).  Parameters per layer: weights [27][16 out][16 in], then 16
+    biases; offset k = 9 (dx+1) + 3 (dy+1) + (dz+1)."""
+
+    LAYERS, CHANNELS, OFFSETS, OUT = 4, 16, 27, 4
+
+    def __init__(self, device: int = 0, seed: int = 1):
+        self.lib = load()
+        h = self.lib.lce_net_create(int(device), int(seed))
+        if not h:
+            raise _lib.LceError(_lib.LCE_ERR_CUDA, "lce_net_create: " + self.lib.lce_last_error(None).decode())
+        self.h = C.c_void_p(h)
+        self.nparam = self.lib.lce_net_num_params(self.h)
+
+    def close(self):
+        if getattr(self, "h", None):
+            self.lib.lce_net_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        self.close()
+
+    def params(self) -> np.ndarray:
+        w = np.empty(self.nparam, np.float32)
+        check(self.lib.lce_net_get_params(self.h, _ptr(w)))
+        return w
+
+    def set_params(self, w: np.ndarray):
+        w = np.ascontiguousarray(w, np.float32)
+        assert w.size == self.nparam
+        check(self.lib.lce_net_set_params(self.h, _ptr(w)))
+
+    def save(self, path: str):
+        check(self.lib.lce_net_save(self.h, path.encode()))
+
+    def load(self, path: str):
+        check(self.lib.lce_net_load(self.h, path.encode()))
+
+    def eval(self, L, feat: np.ndarray, target: np.ndarray):
+        """(raw output [V][4], gradient [nparam], loss) on caller data in the
+        parity-split site order: feat [V][16], target [V][4]."""
+        feat = np.ascontiguousarray(feat, np.float32)
+        target = np.ascontiguousarray(target, np.float32)
+        V = L[0] * L[1] * L[2]
+        assert feat.shape == (V, 16) and target.shape == (V, 4)
+        out = np.empty((V, 4), np.float32)
+        grad = np.empty(self.nparam, np.float32)
+        loss = C.c_double()
+        check(self.lib.lce_net_eval(self.h, int(L[0]), int(L[1]), int(L[2]), _ptr(feat), _ptr(target), _ptr(out),
+                                    _ptr(grad), C.byref(loss)))
+        return out, grad, loss.value
+
+    def num_pairs(self) -> int:
+        return check(self.lib.lce_net_num_pairs(self.h))
+
+    def clear_pairs(self):
+        check(self.lib.lce_net_clear_pairs(self.h))
+
+    def train(self, epochs: int = 1, lr: float = 1e-3) -> float:
+        loss = C.c_double()
+        check(self.lib.lce_net_train(self.h, int(epochs), float(lr), C.byref(loss)))
+        return loss.value
 
 
 class Lattice(_Context):

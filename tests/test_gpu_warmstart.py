@@ -1,0 +1,143 @@
+"""Learned warm start for Landau gauge fixing: the CUDA network against its FP64
+numpy restatement (forward, loss, gradient), parameter I/O, on-device
+training, the judge's fallback, and the warm-started gauge fixing itself."""
+import numpy as np
+import pytest
+
+import net_reference as NR
+
+pytestmark = pytest.mark.gpu
+
+
+def _params(seed, scale=0.25):
+    rng = np.random.default_rng(seed)
+    w = rng.standard_normal(NR.NPARAM) * scale
+    for l in range(NR.LAYERS):
+        w[l * NR.PL + NR.WL:(l + 1) * NR.PL] = rng.standard_normal(16) * 0.1
+    last = (NR.LAYERS - 1) * NR.PL
+    w[last:last + NR.WL].reshape(27, 16, 16)[:, NR.OUT:, :] = 0.0
+    w[last + NR.WL + NR.OUT:] = 0.0
+    return w.astype(np.float32)
+
+
+def _problem(L, seed):
+    rng = np.random.default_rng(seed)
+    V = L[0] * L[1] * L[2]
+    feat = rng.uniform(-1, 1, (V, 16)).astype(np.float32)
+    feat[:, 15] = 0.0
+    t = rng.standard_normal((V, 4))
+    t /= np.linalg.norm(t, axis=1, keepdims=True)
+    return feat, t.astype(np.float32)
+
+
+@pytest.mark.parametrize("L", [(4, 4, 6), (8, 6, 4), (6, 10, 8)])
+def test_forward_loss_gradient_match_fp64_reference(L):
+    from lceqcd_b200 import GaugeNet
+    net = GaugeNet(seed=1)
+    w = _params(11)
+    net.set_params(w)
+    feat, t = _problem(L, 12)
+    out, grad, loss = net.eval(L, feat, t)
+    o_ref, l_ref, g_ref = NR.forward_backward(w.astype(np.float64), feat, t, L, bf16_path=True)
+    # BF16 activations: an FP32-vs-FP64 accumulation difference can move a
+    # hidden value across a BF16 rounding boundary (2^-8 relative), so the
+    # tolerances are a few BF16 ulps of the scale, not FP32 ones
+    assert np.max(np.abs(out - o_ref)) <= 2e-2 * np.max(np.abs(o_ref))
+    assert abs(loss - l_ref) <= 1e-3 * abs(l_ref) + 1e-6
+    for l in range(NR.LAYERS):
+        sl = slice(l * NR.PL, (l + 1) * NR.PL)
+        gr, gg = g_ref[sl], grad[sl].astype(np.float64)
+        rel = np.linalg.norm(gg - gr) / np.linalg.norm(gr)
+        assert rel <= 2e-2, (l, rel)
+
+
+def test_untrained_network_is_identity_and_params_roundtrip(tmp_path):
+    from lceqcd_b200 import GaugeNet
+    net = GaugeNet(seed=7)
+    L = (4, 4, 4)
+    feat, t = _problem(L, 1)
+    out, _, _ = net.eval(L, feat, t)
+    assert np.array_equal(out, np.tile(np.float32([1, 0, 0, 0]), (64, 1)))
+    w = _params(3)
+    net.set_params(w)
+    assert np.array_equal(net.params(), w)
+    p = str(tmp_path / "net.bin")
+    net.save(p)
+    other = GaugeNet(seed=9)
+    other.load(p)
+    assert np.array_equal(other.params(), w)
+    a, ga, la = net.eval(L, feat, t)
+    b, gb, lb = other.eval(L, feat, t)
+    assert np.array_equal(a, b) and np.array_equal(ga, gb) and la == lb
+
+
+def test_training_fits_a_local_rotation():
+    """Targets that are a fixed local function of the inputs are learnable:
+    Adam on the device lowers the loss well below its starting value."""
+    from lceqcd_b200 import GaugeNet, Lattice
+    g = Lattice((8, 8, 8), beta=12.0, x=0.09, y=0.3, lam=1.7, limit_or=1e-10, seed=5)
+    g.init_hot(2)
+    g.sweeps(20, 0)
+    net = GaugeNet(seed=2)
+    g.landau_gauge_from("identity")
+    for _ in range(4):
+        g.sweeps(2, 0)
+        g.landau_gauge_warm(net, use_net=False, judge=False, record=True)
+    assert net.num_pairs() == 4
+    first = net.train(1, lr=2e-3)
+    last = net.train(60, lr=2e-3)
+    assert np.isfinite(last) and last < 0.8 * first, (first, last)
+    net.clear_pairs()
+    assert net.num_pairs() == 0
+
+
+@pytest.mark.parametrize("precision,tol", [("f64", 1e-9), ("f32", 2e-3)])
+def test_warm_start_fixes_to_the_same_condition_and_tracks_the_transform(precision, tol):
+    from lceqcd_b200 import GaugeNet, Lattice
+    g = Lattice((8, 8, 12), beta=12.0, x=0.09, y=0.3, lam=1.7, limit_or=1e-11, seed=9, precision=precision)
+    g.init_hot(3)
+    g.sweeps(30, 0)
+    net = GaugeNet(seed=4)
+    g.landau_gauge_from("identity")
+    for _ in range(3):
+        g.sweeps(3, 0)
+        start, F, th, it = g.landau_gauge_warm(net, use_net=True, judge=True)
+        assert th <= 1e-11 and it > 0
+        assert start in ("identity", "transform", "net")
+        assert all(np.isfinite(F))
+        # U_f is the tracked transform applied to U
+        uf, af = g.download(which=1, dtype=np.float64)
+        g.apply_transform()
+        uf2, af2 = g.download(which=1, dtype=np.float64)
+        assert np.max(np.abs(uf - uf2)) < tol
+        assert np.max(np.abs(af - af2)) < tol * max(1.0, np.abs(af).max())
+
+
+def test_judge_falls_back_when_the_prediction_is_worse():
+    from lceqcd_b200 import GaugeNet, Lattice
+    g = Lattice((8, 8, 8), beta=12.0, x=0.09, y=0.3, lam=1.7, limit_or=1e-10, seed=6)
+    g.init_hot(1)
+    g.sweeps(20, 0)
+    g.landau_gauge_from("identity")
+    g.sweeps(2, 0)
+    net = GaugeNet(seed=3)
+    w = _params(5, scale=2.0)  # a network whose rotations are large and random
+    net.set_params(w)
+    G = g.get_transform()
+    start, F, th, it = g.landau_gauge_warm(net, use_net=True, judge=True)
+    assert F[2] < F[1] and start != "net"
+    assert th <= 1e-10
+    # without the judge the bad prediction is taken, and still converges
+    g.set_transform(G)
+    start2, F2, th2, it2 = g.landau_gauge_warm(net, use_net=True, judge=False)
+    assert start2 == "net" and np.isnan(F2[0]) and th2 <= 1e-10
+
+
+def test_warm_start_needs_a_network_for_net_or_record():
+    from lceqcd_b200 import Lattice, LceError
+    from lceqcd_b200 import _lib
+    g = Lattice((4, 4, 4), seed=1)
+    g.init_unit()
+    for flags in (_lib.LCE_WARM_NET, _lib.LCE_WARM_RECORD, 8):
+        with pytest.raises(LceError):
+            g._ck(g.lib.lce_landau_gauge_warm(g.h, 0, None, flags, None, None, None, None, 0))
