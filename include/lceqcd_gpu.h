@@ -38,7 +38,7 @@ extern "C" {
 #pragma GCC visibility push(default)
 #endif
 
-#define LCE_ABI_VERSION 1
+#define LCE_ABI_VERSION 2
 
 /* status codes */
 #define LCE_OK 0
@@ -100,6 +100,10 @@ typedef struct lce_params {
   int sweep_mode;        /* LCE_SWEEP_AUTO (time both forms on the first sweeps
                             and keep the faster), LCE_SWEEP_PASSES or
                             LCE_SWEEP_PERSISTENT */
+  int agauge_hits;       /* link update of lce_sweep: 1 = f/agauge.f (default;
+                            0 is read as 1), 3 = f/agauge1.f (three heatbath +
+                            Metropolis hits per link) -- the reference selects
+                            one of the two files at build time */
 } lce_params;
 
 /* Measured quantities: /aver_loc/ (plaq0, a0kin, a02, a04, a0f) and the
@@ -184,6 +188,10 @@ int lce_ahiggs2(lce_ctx* ctx, int measflag, float* accept);
 int lce_ahiggs3(lce_ctx* ctx, int measflag, float* accept);
 /* f/agauge.f:7-205 with f/staples.f, f/heat_kpi.f */
 int lce_agauge(lce_ctx* ctx, int measflag, float* accept);
+/* f/agauge1.f:7-235: the 3-hit link update (staple once per (parity, mu),
+ * then three heatbath + Metropolis hits of 7 uniforms per site each; the
+ * acceptance divides the Metropolis count by the hits, :226-231) */
+int lce_agauge1(lce_ctx* ctx, int measflag, float* accept);
 /* link overrelaxation with the agauge Metropolis test (no reference counterpart) */
 int lce_link_or(lce_ctx* ctx, int measflag, float* accept);
 /* f/renorm.f:205-236 */
@@ -221,6 +229,25 @@ int lce_gauge_fix_continue(lce_ctx* ctx, int chain, double* theta, int* iters, i
 #define LCE_GF_START_TRANSFORM 1
 int lce_landau_gauge_from(lce_ctx* ctx, int chain, int start, double* theta_start, double* theta, int* iters,
                           int max_iters);
+/* Fourier-accelerated Landau gauge fixing (no reference counterpart; Davies
+ * et al., Phys. Rev. D 37 (1988) 1581).  Each step rotates every site by
+ * g = exp(-i omega.sigma), omega = step * F^-1[F[Delta]/p^2], Delta the
+ * divergence of the gauge field (the vector part whose square is theta) and
+ * p^2 the lattice Laplacian with the functional's weights (1, 1, alpha), so
+ * that long wavelengths relax as fast as short ones.  From `start` (as in
+ * lce_landau_gauge_from; G is tracked) it iterates until theta <=
+ * theta_switch (<= 0: limit_or); if that is above limit_or the plain
+ * overrelaxed iteration continues to theta <= limit_or -- the stopping
+ * criterion of lce_landau_gauge either way.  step <= 0 selects 1 (a Newton
+ * step near the Landau gauge); a step that doubles theta is shortened by 0.7
+ * on the device.  Extents must be powers of two up to 512, else
+ * LCE_ERR_UNSUPPORTED.  max_iters caps both phases together. */
+int lce_landau_gauge_fourier(lce_ctx* ctx, int chain, int start, double step, double theta_switch, double* theta,
+                             int* iters_fourier, int* iters_plain, int max_iters);
+/* one preconditioned direction omega [2][V/2][3] (components a3, Re b, Im b
+ * of the vector part, parity-split order) from the current U_f; nothing is
+ * updated (test hook for the FFT path) */
+int lce_debug_fourier_step(lce_ctx* ctx, int chain, double step, double* omega);
 /* U_f, A_f := (U, A) transformed by the current G */
 int lce_apply_transform(lce_ctx* ctx, int chain);
 /* the transform field G: g[(eo*ld + site)*4 + c], SU(2) first rows like the links */
@@ -315,10 +342,14 @@ int lce_net_train(lce_net* net, int epochs, double lr, double* mean_loss);
  * to the plain start when the prediction is worse; otherwise the network's
  * start (LCE_WARM_NET) or G_prev.  LCE_WARM_RECORD stores the pair
  * (configuration in G_prev gauge, G_new G_prev^+) for lce_net_train after
- * convergence.  net may be NULL when neither NET nor RECORD is set. */
+ * convergence.  LCE_WARM_FOURIER iterates from the chosen start with the
+ * Fourier-accelerated step of lce_landau_gauge_fourier instead of the plain
+ * overrelaxation (power-of-two extents).  net may be NULL when neither NET
+ * nor RECORD is set. */
 #define LCE_WARM_NET 1
 #define LCE_WARM_JUDGE 2
 #define LCE_WARM_RECORD 4
+#define LCE_WARM_FOURIER 8
 #define LCE_GF_START_NET 2
 int lce_landau_gauge_warm(lce_ctx* ctx, int chain, lce_net* net, int flags, int* start_used, double functional[3],
                           double* theta, int* iters, int max_iters);

@@ -38,6 +38,7 @@ LCE_GF_START_NET = 2
 LCE_WARM_NET = 1
 LCE_WARM_JUDGE = 2
 LCE_WARM_RECORD = 4
+LCE_WARM_FOURIER = 8
 
 
 class LceParams(C.Structure):
@@ -49,6 +50,7 @@ class LceParams(C.Structure):
         ("seed", C.c_ulonglong), ("device", C.c_int),
         ("n_link_or", C.c_int), ("n_higgs_metro", C.c_int),
         ("delta0", C.c_double), ("gf_angle", C.c_int), ("sweep_mode", C.c_int),
+        ("agauge_hits", C.c_int),
     ]
 
 
@@ -98,6 +100,7 @@ SIGNATURES = {
     "lce_ahiggs2": (I, [P, I, P]),
     "lce_ahiggs3": (I, [P, I, P]),
     "lce_agauge": (I, [P, I, P]),
+    "lce_agauge1": (I, [P, I, P]),
     "lce_link_or": (I, [P, I, P]),
     "lce_renorm": (I, [P]),
     "lce_sweep": (I, [P, I, P]),
@@ -109,6 +112,8 @@ SIGNATURES = {
     "lce_gauge_fix_continue": (I, [P, I, P, P, I]),
     "lce_landau_gauge_from": (I, [P, I, I, P, P, P, I]),
     "lce_apply_transform": (I, [P, I]),
+    "lce_landau_gauge_fourier": (I, [P, I, I, D, D, P, P, P, I]),
+    "lce_debug_fourier_step": (I, [P, I, D, P]),
     "lce_set_transform": (I, [P, I, P, C.c_long]),
     "lce_get_transform": (I, [P, I, P, C.c_long]),
     "lce_gauge_functional": (I, [P, I, P]),

@@ -40,6 +40,7 @@ struct lce_ctx {
   int rng = LCE_RNG_PHILOX;
   int nchains = 0;
   int n_link_or = 0, n_higgs_metro = 0;
+  int agauge_hits = 1;  // 1: f/agauge.f, 3: f/agauge1.f in lce_sweep
   std::vector<lce_params> params;
   std::vector<ChainDev> ch;
   std::vector<int> blk;  // prefix of blocks per pass
@@ -63,6 +64,9 @@ struct lce_ctx {
   void* flush_d = nullptr;
   size_t flush_bytes = 0;
   void* gsave_d = nullptr;  // G_prev during a warm-started gauge fixing
+  void* fa_d = nullptr;     // Fourier-accelerated fixing: FFT fields and the step transform
+  size_t fa_bytes = 0;
+  std::map<std::pair<int, int>, cudaGraphExec_t> fa_exec;
   cudaStream_t own = nullptr, stream = nullptr;
   cudaEvent_t ev0 = nullptr, ev1 = nullptr;
   cudaGraphExec_t sweep_exec[2] = {nullptr, nullptr};     // per-pass kernels, per measflag
@@ -153,6 +157,10 @@ bool valid_params(const lce_params& p, std::string& why) {
     why = "lambda must be positive and alpha non-negative";
     return false;
   }
+  if (p.agauge_hits != 0 && p.agauge_hits != 1 && p.agauge_hits != 3) {
+    why = "agauge_hits must be 1 (f/agauge.f) or 3 (f/agauge1.f)";
+    return false;
+  }
   if (p.n_link_or < 0 || p.n_higgs_metro < 0 || 4 + 6 + 2 * p.n_higgs_metro + 6 * p.n_link_or > kMaxSlots) {
     why = "too many extra update passes per sweep";
     return false;
@@ -184,9 +192,13 @@ int nslots_of(unsigned char kind) {
     case kHiggsOR: return 1;
     case kHiggsMetro: return 4;
     case kLinkHB: return 7;
+    case kLinkHB3: return 21;
     default: return 1;
   }
 }
+
+// Philox passes a pass kind consumes (one per hit)
+int philox_passes(unsigned char kind) { return kind == kLinkHB3 ? 3 : 1; }
 
 void expand(unsigned char kind, std::vector<Pass>& out) {
   if (kind <= kHiggsMetro) {
@@ -218,6 +230,7 @@ int enqueue(lce_ctx* c, const std::vector<unsigned char>& routines, int measflag
   f.single = c->prec == LCE_PREC_F32;
   const int nblocks = c->blk.back();
   unsigned long long soff = 0;
+  unsigned int poff = 0;
   int slot = 0;
   for (size_t i = 0; i < passes.size(); ++i) {
     const Pass& ps = passes[i];
@@ -232,7 +245,7 @@ int enqueue(lce_ctx* c, const std::vector<unsigned char>& routines, int measflag
     a.stream = c->rng == LCE_RNG_STREAM ? c->stream_d : nullptr;
     a.stream_n = c->stream_n;
     a.stream_off = soff;
-    a.pass_off = (unsigned int)i;
+    a.pass_off = poff;
     a.nchains = c->nchains;
     a.eo = ps.eo;
     a.fuse_renorm = fuse_renorm ? 1 : 0;
@@ -240,7 +253,7 @@ int enqueue(lce_ctx* c, const std::vector<unsigned char>& routines, int measflag
       if (c->prec == LCE_PREC_F64) launch_higgs<double>(ps.kind, a, nblocks, c->stream);
       else launch_higgs<float>(ps.kind, a, nblocks, c->stream);
     } else {
-      const int mode = ps.kind == kLinkHB ? 0 : 1;
+      const int mode = ps.kind == kLinkHB ? 0 : (ps.kind == kLinkOR ? 1 : 2);
       if (c->prec == LCE_PREC_F64) launch_link<double>(mode, ps.mu, a, nblocks, c->stream);
       else launch_link<float>(mode, ps.mu, a, nblocks, c->stream);
     }
@@ -250,9 +263,10 @@ int enqueue(lce_ctx* c, const std::vector<unsigned char>& routines, int measflag
       ++slot;
     }
     if (c->nchains == 1) soff += (unsigned long long)nslots_of(ps.kind) * c->ch[0].nh;
+    poff += philox_passes(ps.kind);
   }
   f.nslots = slot;
-  f.npasses = (unsigned int)passes.size();
+  f.npasses = poff;
   f.nstream = c->rng == LCE_RNG_STREAM ? soff : 0;
   launch_finalize(f, c->stream);
   CK(cudaGetLastError());
@@ -291,11 +305,14 @@ int enqueue_persistent(lce_ctx* c, const std::vector<unsigned char>& routines, i
   f.nchains = c->nchains;
   f.single = c->prec == LCE_PREC_F32;
   unsigned long long soff = 0;
+  unsigned int poff = 0;
   int slot = 0;
   for (size_t i = 0; i < passes.size(); ++i) {
     const Pass& ps = passes[i];
     const bool reduce = measflag == 1 || ps.kind == kHiggsMetro;
     if (reduce && slot >= c->part_slots) return fail(c, LCE_ERR_INVALID, "too many reduction slots");
+    a.pass_off[i] = (unsigned short)poff;
+    poff += philox_passes(ps.kind);
     a.plan[i] = PlanEntry{ps.kind, (unsigned char)ps.eo, (unsigned char)ps.mu,
                           reduce ? (unsigned char)slot : kNoSlot};
     a.stream_off[i] = soff;
@@ -306,7 +323,7 @@ int enqueue_persistent(lce_ctx* c, const std::vector<unsigned char>& routines, i
     if (c->nchains == 1) soff += (unsigned long long)nslots_of(ps.kind) * c->ch[0].nh;
   }
   f.nslots = slot;
-  f.npasses = (unsigned int)passes.size();
+  f.npasses = poff;
   f.nstream = c->rng == LCE_RNG_STREAM ? soff : 0;
   a.bar = c->bar_d;
   a.ntiles = c->blk.back();
@@ -358,7 +375,7 @@ int sweep_graph(lce_ctx* c, int form, int mf, cudaGraphExec_t* out) {
 std::vector<unsigned char> sweep_routines(const lce_ctx* c) {
   std::vector<unsigned char> r = {kHiggsHB, kHiggsOR};
   for (int i = 0; i < c->n_higgs_metro; ++i) r.push_back(kHiggsMetro);
-  r.push_back(kLinkHB);
+  r.push_back(c->agauge_hits == 3 ? kLinkHB3 : kLinkHB);
   for (int i = 0; i < c->n_link_or; ++i) r.push_back(kLinkOR);
   return r;
 }
@@ -376,6 +393,7 @@ int routine_call(lce_ctx* c, unsigned char kind, int measflag, float* accept, bo
     case kHiggsOR: *accept = (float)m.acc_or; break;
     case kHiggsMetro: *accept = (float)m.acc_metro; break;
     case kLinkHB: *accept = (float)m.acc_gauge; break;
+    case kLinkHB3: *accept = (float)m.acc_gauge; break;
     default: *accept = (float)m.acc_link_or; break;
   }
   return LCE_OK;
@@ -485,7 +503,8 @@ lce_ctx* create_impl(const lce_params* p, int n) {
       return nullptr;
     }
     if (p[i].precision != p[0].precision || p[i].rng != p[0].rng || p[i].device != p[0].device ||
-        p[i].n_link_or != p[0].n_link_or || p[i].n_higgs_metro != p[0].n_higgs_metro) {
+        p[i].n_link_or != p[0].n_link_or || p[i].n_higgs_metro != p[0].n_higgs_metro ||
+        p[i].agauge_hits != p[0].agauge_hits) {
       fail(nullptr, LCE_ERR_INVALID, "create: chains of a batch must share precision, rng, device and composition");
       return nullptr;
     }
@@ -501,6 +520,7 @@ lce_ctx* create_impl(const lce_params* p, int n) {
   c->nchains = n;
   c->n_link_or = p[0].n_link_or;
   c->n_higgs_metro = p[0].n_higgs_metro;
+  c->agauge_hits = p[0].agauge_hits == 3 ? 3 : 1;
   c->params.assign(p, p + n);
   auto bail = [&](cudaError_t e, const char* where) -> lce_ctx* {
     g_create_error = std::string(where) + ": " + cudaGetErrorString(e);
@@ -690,6 +710,72 @@ int gf_loop(lce_ctx* c, int chain, double* theta, int* iters, int max_iters, int
   return LCE_OK;
 }
 
+int fa_buffers(lce_ctx* c, const ChainDev& ch) {
+  const size_t need = fa_buffer_bytes(ch);
+  if (c->fa_bytes >= need) return LCE_OK;
+  if (c->fa_d) CK(cudaFree(c->fa_d));
+  c->fa_d = nullptr;
+  c->fa_bytes = 0;
+  if (cudaMalloc(&c->fa_d, need) != cudaSuccess) return fail(c, LCE_ERR_NOMEM, "Fourier-accelerated fixing buffers");
+  c->fa_bytes = need;
+  return LCE_OK;
+}
+
+// Fourier-accelerated iterations on U_f (tracking G) until theta <= limit or
+// the cap; same graph batching and progress guard as gf_loop
+int fa_loop(lce_ctx* c, int chain, double step, double limit, double* theta, int* iters, int cap) {
+  const ChainDev& ch = c->ch[chain];
+  int rc = fa_buffers(c, ch);
+  if (rc) return rc;
+  ChainState cs;
+  CK(cudaMemcpyAsync(&cs, c->cst_d + chain, sizeof(cs), cudaMemcpyDeviceToHost, c->stream));
+  CK(cudaStreamSynchronize(c->stream));
+  cs.gf_done = 0;
+  cs.gf_iters = 0;
+  cs.gf_cap = cap;
+  cs.gf_theta = 1.0e4;
+  cs.gf_limit = limit;
+  cs.gf_step = step;
+  CK(cudaMemcpyAsync(c->cst_d + chain, &cs, sizeof(cs), cudaMemcpyHostToDevice, c->stream));
+  CK(cudaStreamSynchronize(c->stream));
+  double* part = c->scratch_d;
+  int batch = 4;
+  while (true) {
+    auto key = std::make_pair(chain, batch);
+    auto it = c->fa_exec.find(key);
+    if (it == c->fa_exec.end()) {
+      cudaGraph_t g;
+      CK(cudaStreamBeginCapture(c->stream, cudaStreamCaptureModeThreadLocal));
+      for (int k = 0; k < batch; ++k) {
+        if (c->prec == LCE_PREC_F64)
+          launch_fa_iteration<double>(c->ch_d + chain, ch, c->cst_d + chain, step, c->fa_d, part, nullptr, 1, true,
+                                      true, c->stream);
+        else
+          launch_fa_iteration<float>(c->ch_d + chain, ch, c->cst_d + chain, step, c->fa_d, part, nullptr, 1, true,
+                                     true, c->stream);
+      }
+      CK(cudaStreamEndCapture(c->stream, &g));
+      cudaGraphExec_t ex;
+      cudaError_t e = cudaGraphInstantiate(&ex, g, 0);
+      cudaGraphDestroy(g);
+      if (e != cudaSuccess) return cuda_fail(c, e, "cudaGraphInstantiate(Fourier-accelerated fixing)");
+      it = c->fa_exec.emplace(key, ex).first;
+    }
+    const int before = cs.gf_iters;
+    CK(cudaGraphLaunch(it->second, c->stream));
+    CK(cudaMemcpyAsync(&cs, c->cst_d + chain, sizeof(cs), cudaMemcpyDeviceToHost, c->stream));
+    CK(cudaStreamSynchronize(c->stream));
+    if (cs.gf_done) break;
+    if (cs.gf_iters <= before)
+      return fail(c, LCE_ERR_CUDA, "Fourier-accelerated fixing: a batch of iterations made no progress");
+    if (batch < 64) batch *= 2;
+  }
+  if (theta) *theta = cs.gf_theta;
+  if (iters) *iters = cs.gf_iters;
+  if (!std::isfinite(cs.gf_theta)) return fail(c, LCE_ERR_NAN, "Fourier-accelerated fixing: theta is not finite");
+  return LCE_OK;
+}
+
 }  // namespace
 
 // ====================================================================== C ABI
@@ -730,6 +816,7 @@ void lce_default_params(lce_params* p) {
   p->delta0 = 1.0;
   p->gf_angle = LCE_GF_ATAN2;
   p->sweep_mode = LCE_SWEEP_AUTO;
+  p->agauge_hits = 1;
 }
 
 int lce_couplings(const lce_params* p, double out[3]) {
@@ -770,9 +857,10 @@ void lce_destroy(lce_ctx* c) {
     if (c->persist_exec[i]) cudaGraphExecDestroy(c->persist_exec[i]);
   }
   for (auto& kv : c->gf_exec) cudaGraphExecDestroy(kv.second);
+  for (auto& kv : c->fa_exec) cudaGraphExecDestroy(kv.second);
   void* ptrs[] = {c->ch_d, c->blk_d, c->st_d, c->cst_d, c->meas_d, c->part_d, c->totals_d,
                   c->scratch_d, c->fields_d, c->stream_d, c->staging_d, c->flush_d, c->bar_d,
-                  c->gsave_d};
+                  c->gsave_d, c->fa_d};
   for (void* q : ptrs)
     if (q) cudaFree(q);
   if (c->ev0) cudaEventDestroy(c->ev0);
@@ -919,6 +1007,9 @@ int lce_ahiggs3(lce_ctx* c, int measflag, float* accept) {
 int lce_agauge(lce_ctx* c, int measflag, float* accept) {
   return c ? routine_call(c, kLinkHB, measflag, accept, false) : LCE_ERR_INVALID;
 }
+int lce_agauge1(lce_ctx* c, int measflag, float* accept) {
+  return c ? routine_call(c, kLinkHB3, measflag, accept, false) : LCE_ERR_INVALID;
+}
 int lce_link_or(lce_ctx* c, int measflag, float* accept) {
   return c ? routine_call(c, kLinkOR, measflag, accept, false) : LCE_ERR_INVALID;
 }
@@ -1042,13 +1133,17 @@ int lce_landau_gauge_from(lce_ctx* c, int chain, int start, double* theta_start,
 
 int lce_landau_gauge_warm(lce_ctx* c, int chain, lce_net* net, int flags, int* start_used, double functional[3],
                           double* theta, int* iters, int max_iters) {
-  if (!c || chain < 0 || chain >= c->nchains || (flags & ~(LCE_WARM_NET | LCE_WARM_JUDGE | LCE_WARM_RECORD)))
+  if (!c || chain < 0 || chain >= c->nchains ||
+      (flags & ~(LCE_WARM_NET | LCE_WARM_JUDGE | LCE_WARM_RECORD | LCE_WARM_FOURIER)))
     return LCE_ERR_INVALID;
   const bool use_net = flags & LCE_WARM_NET, judge = flags & LCE_WARM_JUDGE, record = flags & LCE_WARM_RECORD;
   if ((use_net || record) && !net) return fail(c, LCE_ERR_INVALID, "landau_gauge_warm: no network given");
   if (net && net_device(net) != c->device) return fail(c, LCE_ERR_INVALID, "landau_gauge_warm: network on another device");
   const ChainDev& ch = c->ch[chain];
   const bool f64 = c->prec == LCE_PREC_F64;
+  const bool fourier = flags & LCE_WARM_FOURIER;
+  if (fourier && !fa_supported(ch))
+    return fail(c, LCE_ERR_UNSUPPORTED, "Fourier-accelerated fixing needs power-of-two extents");
   const size_t gb = (size_t)2 * ch.nh * link_bytes(c->prec);
   if (!c->gsave_d) CK(cudaMalloc(&c->gsave_d, (size_t)2 * c->max_nh * link_bytes(c->prec)));
   double F[3] = {NAN, NAN, NAN};
@@ -1098,12 +1193,80 @@ int lce_landau_gauge_warm(lce_ctx* c, int chain, lce_net* net, int flags, int* s
   if (start_used) *start_used = pick;
   if (functional)
     for (int k = 0; k < 3; ++k) functional[k] = F[k];
-  rc = gf_loop(c, chain, theta, iters, max_iters, 1);
+  if (fourier) {
+    const int cap = max_iters > 0 ? max_iters : 1000000;
+    double th = 0.0;
+    int it = 0;
+    rc = fa_loop(c, chain, 1.0, ch.limit_or, &th, &it, cap);
+    if (theta) *theta = th;
+    if (iters) *iters = it;
+    if (rc == LCE_OK && th > ch.limit_or) rc = fail(c, LCE_ERR_GF_NOT_CONVERGED, "gauge fixing: iteration cap reached");
+  } else {
+    rc = gf_loop(c, chain, theta, iters, max_iters, 1);
+  }
   if (rc == LCE_OK && record) {
     if ((rc = net_record(net, ch, c->gsave_d, f64, c->stream))) return fail(c, rc, "record training pair");
     CK(cudaStreamSynchronize(c->stream));
   }
   return rc;
+}
+
+int lce_landau_gauge_fourier(lce_ctx* c, int chain, int start, double step, double theta_switch, double* theta,
+                             int* iters_fourier, int* iters_plain, int max_iters) {
+  if (!c || chain < 0 || chain >= c->nchains) return LCE_ERR_INVALID;
+  const ChainDev& ch = c->ch[chain];
+  if (!fa_supported(ch)) return fail(c, LCE_ERR_UNSUPPORTED, "Fourier-accelerated fixing needs power-of-two extents");
+  if (!(step > 0.0)) step = 1.0;
+  if (!(theta_switch > 0.0)) theta_switch = ch.limit_or;
+  if (start == LCE_GF_START_IDENTITY) {
+    if (c->prec == LCE_PREC_F64) launch_transform_identity<double>(ch.g, ch.nh, c->stream);
+    else launch_transform_identity<float>(ch.g, ch.nh, c->stream);
+    const size_t ub = (size_t)6 * ch.nh * link_bytes(c->prec), ab = (size_t)6 * ch.nh * real_bytes(c->prec);
+    CK(cudaMemcpyAsync(ch.uf, ch.u, ub, cudaMemcpyDeviceToDevice, c->stream));
+    CK(cudaMemcpyAsync(ch.af, ch.a, ab, cudaMemcpyDeviceToDevice, c->stream));
+  } else if (start == LCE_GF_START_TRANSFORM) {
+    int rc = lce_apply_transform(c, chain);
+    if (rc) return rc;
+  } else {
+    return fail(c, LCE_ERR_INVALID, "landau_gauge_fourier: unknown start");
+  }
+  const int cap = max_iters > 0 ? max_iters : 1000000;
+  double th_fa = 0.0;
+  int it_fa = 0, it_or = 0;
+  int rc = fa_loop(c, chain, step, theta_switch, &th_fa, &it_fa, cap);
+  if (iters_fourier) *iters_fourier = it_fa;
+  if (iters_plain) *iters_plain = 0;
+  if (theta) *theta = th_fa;
+  if (rc) return rc;
+  if (th_fa <= ch.limit_or) return LCE_OK;
+  if (it_fa >= cap) return fail(c, LCE_ERR_GF_NOT_CONVERGED, "Fourier-accelerated fixing: iteration cap reached");
+  // the plain overrelaxed iteration from theta_switch to limit_or
+  rc = gf_loop(c, chain, theta, &it_or, cap - it_fa, 1);
+  if (iters_plain) *iters_plain = it_or;
+  return rc;
+}
+
+int lce_debug_fourier_step(lce_ctx* c, int chain, double step, double* omega) {
+  if (!c || !omega || chain < 0 || chain >= c->nchains) return LCE_ERR_INVALID;
+  const ChainDev& ch = c->ch[chain];
+  if (!fa_supported(ch)) return fail(c, LCE_ERR_UNSUPPORTED, "power-of-two extents needed");
+  int rc = fa_buffers(c, ch);
+  if (rc) return rc;
+  double* om = nullptr;
+  const size_t ob = sizeof(double) * 3 * 2 * (size_t)ch.nh;
+  CK(cudaMalloc(&om, ob));
+  if (c->prec == LCE_PREC_F64)
+    launch_fa_iteration<double>(c->ch_d + chain, ch, nullptr, step, c->fa_d, c->scratch_d, om, 0, false, false,
+                                c->stream);
+  else
+    launch_fa_iteration<float>(c->ch_d + chain, ch, nullptr, step, c->fa_d, c->scratch_d, om, 0, false, false,
+                               c->stream);
+  cudaError_t e = cudaGetLastError();
+  if (e == cudaSuccess) e = cudaMemcpyAsync(omega, om, ob, cudaMemcpyDeviceToHost, c->stream);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(c->stream);
+  cudaFree(om);
+  if (e != cudaSuccess) return cuda_fail(c, e, "debug_fourier_step");
+  return LCE_OK;
 }
 
 int lce_set_transform(lce_ctx* c, int chain, const float* g, long ld) {

@@ -20,9 +20,13 @@ namespace lce {
 
 constexpr int kBlock = 256;      // threads per block of the update kernels
 // resident blocks per SM the update kernels are compiled for (register cap
-// 48 for FP32 production kernels, 80 for the FP64 validation kernels)
+// 64 for FP32 production kernels, 80 for the FP64 validation kernels).  FP32:
+// 4 blocks of 256 (64 registers) keep a 64^3 parity pass (131,072 sites) in one
+// wave on 148 SMs and let the compiler issue the staple loads together; timed
+// on a B200 it beats 5 (48 registers, spills), 3 (80) and 2 (92) blocks at
+// every volume from 64^3 to 256^3 (by 17% at 64^3, 3-6% at 128^3-256^3).
 template <typename R>
-constexpr int min_blocks() { return sizeof(R) == 4 ? 5 : 3; }
+constexpr int min_blocks() { return sizeof(R) == 4 ? 4 : 3; }
 constexpr int kNQ = 4;           // doubles of partial sums per block
 constexpr int kMaxSlots = 64;    // reduction slots per finalize
 
@@ -33,6 +37,7 @@ enum PassKind : unsigned char {
   kHiggsMetro = 2,  // ahiggs1
   kLinkHB = 3,      // agauge
   kLinkOR = 4,      // link overrelaxation (no reference counterpart)
+  kLinkHB3 = 5,     // agauge of f/agauge1.f: three heatbath + Metropolis hits
   kKindEnd = 0x80,  // flag: last slot of one routine
 };
 
@@ -69,6 +74,8 @@ struct ChainState {
   int gf_pad;
   unsigned int ticket;
   unsigned int pad2;
+  double gf_limit;   // Fourier-accelerated fixing: theta to stop at
+  double gf_step;    // Fourier-accelerated fixing: step gamma
 };
 
 // device status bits
@@ -133,6 +140,7 @@ struct PersistArgs {
   int npasses;
   PlanEntry plan[kMaxSlots];
   unsigned long long stream_off[kMaxSlots];
+  unsigned short pass_off[kMaxSlots];  // Philox pass of each plan entry (3-hit passes take 3)
 };
 
 // ---- launchers (lce_update.cu)
@@ -176,6 +184,15 @@ template <typename R>
 void launch_gauge_apply(const ChainDev* ch, int nh, cudaStream_t s);
 template <typename R>
 void launch_transform_identity(void* g, int nh, cudaStream_t s);
+
+// ---- Fourier-accelerated gauge fixing (lce_fourier.cu)
+bool fa_supported(const ChainDev& ch);
+size_t fa_buffer_bytes(const ChainDev& ch);
+// one iteration; cst NULL (debug): never done, step gamma instead of the chain state's
+template <typename R>
+void launch_fa_iteration(const ChainDev* chd, const ChainDev& ch, ChainState* cst, double gamma, void* buf,
+                         double* part, double* omega_out, int track, bool with_check, bool with_apply,
+                         cudaStream_t s);
 template <typename R>
 void launch_gf_theta(const ChainDev* ch, double* part, int nh, cudaStream_t s);
 void launch_sum_partials(const double* part, int nblocks, int nq, double* out, cudaStream_t s);

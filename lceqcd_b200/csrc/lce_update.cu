@@ -146,20 +146,21 @@ __device__ __forceinline__ void higgs_force(const ChainDev& ch, int eo, Coord X,
   force_add<R, 2, NC>(ch, eo, X, s, f1, f2, f3);
 }
 
-// Set up the uniform source of this pass.  Returns false (and flags the
-// context) when the validation stream cannot cover the pass.
+// Set up the uniform source of this pass (of hit `hit` of a multi-hit pass:
+// the next N*nh stream values, the next Philox pass).  Returns false (and
+// flags the context) when the validation stream cannot cover the pass.
 template <typename R, int N>
 __device__ __forceinline__ bool setup_uniforms(const PassArgs& p, const ChainDev& ch, int s, int layout,
-                                               Uniforms<R, N>& U) {
+                                               Uniforms<R, N>& U, int hit = 0) {
   if (p.stream) {
-    unsigned long long base = p.st->stream_pos + p.stream_off;
+    unsigned long long base = p.st->stream_pos + p.stream_off + (unsigned long long)hit * N * ch.nh;
     if (base + (unsigned long long)N * ch.nh > p.stream_n) {
       if (s == 0) atomicOr(&p.st->status, kStatusStreamExhausted);
       return false;
     }
     U.fill_stream(p.stream + base, ch.nh, layout, s);
   } else {
-    U.fill_philox(ch.key0, ch.key1, p.st->pass_ctr + p.pass_off, s);
+    U.fill_philox(ch.key0, ch.key1, p.st->pass_ctr + p.pass_off + hit, s);
   }
   return true;
 }
@@ -270,7 +271,10 @@ __device__ __forceinline__ void higgs_tile(const PassArgs& p, int tile) {
 }
 
 // ------------------------------------------------------------------ links
-template <typename R, int MU, int OR, bool PDL>
+// NHIT = 3 is f/agauge1.f: the staple is built once and the heatbath +
+// Metropolis hit is repeated on the updated link, each hit with its own
+// uniforms (f/agauge1.f:95-198).
+template <typename R, int MU, int OR, bool PDL, int NHIT = 1>
 __device__ __forceinline__ void link_tile(const PassArgs& p, int tile) {
   if (PDL) pdl_trigger();
   const int c = p.nchains > 1 ? find_chain(p.blk_begin, p.nchains, tile) : 0;
@@ -286,56 +290,61 @@ __device__ __forceinline__ void link_tile(const PassArgs& p, int tile) {
     if (setup_uniforms<R, OR ? 1 : 7>(p, ch, s, OR ? kPlanar : kTriple, Un)) {
       const su2<R> V = staple<R, MU, PDL>(ch, eo, X, s);
       const size_t li = ((size_t)(MU * 2 + eo)) * nh + s;
-      const su2<R> uo = PDL ? LinkIO<R>::ld(ch.u, li) : LinkIO<R>::ld_cg(ch.u, li);
+      su2<R> uo = PDL ? LinkIO<R>::ld(ch.u, li) : LinkIO<R>::ld_cg(ch.u, li);
       // f/agauge.f:71-84: normalised staple, 1/(beta |V|), 1/2 Re Tr(U Vhat)
-      R t1 = M<R>::rsqrt(norm2(V));
-      const su2<R> vh{{t1 * V.a.re, t1 * V.a.im}, {t1 * V.b.re, t1 * V.b.im}};
-      su2<R> hn;
-      if constexpr (!OR) {
-        t1 = M<R>::div(t1, (R)ch.beta);
-        const R t2 = (uo.a * vh.a - uo.b * cj(vh.b)).re;
-        // f/heat_kpi.f:254-319 single-trial Kennedy-Pendleton
-        R a1 = Un.v[0], a2 = Un.v[1], a3 = Un.v[2];
-        if (a1 == (R)0) a1 = (R)0.0000033;
-        if (a2 == (R)0) a2 = (R)0.0000066;
-        const R cc = M<R>::cos2pi(a3);
-        R a0 = -(M<R>::log(a1) + M<R>::log(a2) * (cc * cc)) * t1;
-        const R r4 = Un.v[3];
-        const bool lacc = r4 * r4 <= ((R)1 - (R)0.5 * a0);
-        a0 = lacc ? (R)1 - a0 : t2;
-        cnt[0] = lacc ? 1u : 0u;
-        R b1 = (R)1 - a0 * a0;
-        b1 = b1 >= (R)0 ? M<R>::sqrt(b1) : (R)0;
-        const R b2 = (R)2 * (Un.v[4] - (R)0.5);
-        su2<R> Xk;
-        Xk.a = mk<R>(a0, b1 * b2);
-        R q0 = (R)1 - b2 * b2;
-        q0 = q0 >= (R)0 ? b1 * M<R>::sqrt(q0) : (R)0;
-        R sph, cph;
-        M<R>::sincos2pi(Un.v[5], &sph, &cph);
-        Xk.b = mk<R>(q0 * sph, q0 * cph);
-        hn = nd(Xk, vh);  // f/agauge.f:98-99
-      } else {
-        // overrelaxation U' = (Vhat U Vhat)^+ leaves Re Tr(U V) unchanged
-        const su2<R> w = nn(nn(vh, uo), vh);
-        hn = su2<R>{cj(w.a), -w.b};
-      }
+      const R tn = M<R>::rsqrt(norm2(V));
+      const su2<R> vh{{tn * V.a.re, tn * V.a.im}, {tn * V.b.re, tn * V.b.im}};
       // f/agauge.f:126-174 hopping term beta_a Re[(iA(x) U)(iA(x+mu) U^+)]_11 and accept
       const R* A = reinterpret_cast<const R*>(ch.a);
       const int xp = nbr<MU>(ch, X, +1);
       const R x1 = ldA<R, PDL>(A, nh, eo, 0, s), x2 = ldA<R, PDL>(A, nh, eo, 1, s), x3 = ldA<R, PDL>(A, nh, eo, 2, s);
       const R y1 = ldA<R, PDL>(A, nh, oe, 0, xp), y2 = ldA<R, PDL>(A, nh, oe, 1, xp), y3 = ldA<R, PDL>(A, nh, oe, 2, xp);
       const R beta_a = (R)ch.beta_a;
-      const R sa_old = beta_a * nn(an(x1, x2, x3, uo), ad(y1, y2, y3, uo)).a.re;
-      const R sa_new = beta_a * nn(an(x1, x2, x3, hn), ad(y1, y2, y3, hn)).a.re;
-      su2<R> un = uo;
-      if (M<R>::exp(sa_old - sa_new) >= Un.v[OR ? 0 : 6]) {
-        un = hn;
-        LinkIO<R>::st(ch.u, li, p.fuse_renorm ? unitarise64(hn) : hn);
-        cnt[OR ? 0 : 1] = 1u;
+      bool changed = false;
+#pragma unroll 1
+      for (int hit = 0; hit < NHIT; ++hit) {
+        if (hit > 0 && !setup_uniforms<R, OR ? 1 : 7>(p, ch, s, OR ? kPlanar : kTriple, Un, hit)) break;
+        su2<R> hn;
+        if constexpr (!OR) {
+          const R t1 = M<R>::div(tn, (R)ch.beta);
+          const R t2 = (uo.a * vh.a - uo.b * cj(vh.b)).re;
+          // f/heat_kpi.f:254-319 single-trial Kennedy-Pendleton
+          R a1 = Un.v[0], a2 = Un.v[1], a3 = Un.v[2];
+          if (a1 == (R)0) a1 = (R)0.0000033;
+          if (a2 == (R)0) a2 = (R)0.0000066;
+          const R cc = M<R>::cos2pi(a3);
+          R a0 = -(M<R>::log(a1) + M<R>::log(a2) * (cc * cc)) * t1;
+          const R r4 = Un.v[3];
+          const bool lacc = r4 * r4 <= ((R)1 - (R)0.5 * a0);
+          a0 = lacc ? (R)1 - a0 : t2;
+          cnt[0] += lacc ? 1u : 0u;
+          R b1 = (R)1 - a0 * a0;
+          b1 = b1 >= (R)0 ? M<R>::sqrt(b1) : (R)0;
+          const R b2 = (R)2 * (Un.v[4] - (R)0.5);
+          su2<R> Xk;
+          Xk.a = mk<R>(a0, b1 * b2);
+          R q0 = (R)1 - b2 * b2;
+          q0 = q0 >= (R)0 ? b1 * M<R>::sqrt(q0) : (R)0;
+          R sph, cph;
+          M<R>::sincos2pi(Un.v[5], &sph, &cph);
+          Xk.b = mk<R>(q0 * sph, q0 * cph);
+          hn = nd(Xk, vh);  // f/agauge.f:98-99
+        } else {
+          // overrelaxation U' = (Vhat U Vhat)^+ leaves Re Tr(U V) unchanged
+          const su2<R> w = nn(nn(vh, uo), vh);
+          hn = su2<R>{cj(w.a), -w.b};
+        }
+        const R sa_old = beta_a * nn(an(x1, x2, x3, uo), ad(y1, y2, y3, uo)).a.re;
+        const R sa_new = beta_a * nn(an(x1, x2, x3, hn), ad(y1, y2, y3, hn)).a.re;
+        if (M<R>::exp(sa_old - sa_new) >= Un.v[OR ? 0 : 6]) {
+          uo = hn;
+          changed = true;
+          cnt[OR ? 0 : 1] += 1u;
+        }
       }
+      if (changed) LinkIO<R>::st(ch.u, li, p.fuse_renorm ? unitarise64(uo) : uo);
       // f/agauge.f:179-185 plaquette against the staple
-      if (!OR && p.part) pl[0] = (double)nn(un, V).a.re;
+      if (!OR && p.part) pl[0] = (double)nn(uo, V).a.re;
     }
   }
   // partials {KP accepted, Metropolis accepted, sum plaquette} / {OR accepted}
@@ -357,6 +366,12 @@ __global__ void __launch_bounds__(kBlock, min_blocks<R>()) higgs_kernel(PassArgs
 template <typename R, int MU, int OR>
 __global__ void __launch_bounds__(kBlock, min_blocks<R>()) link_kernel(PassArgs p) {
   link_tile<R, MU, OR, true>(p, blockIdx.x);
+}
+
+// f/agauge1.f (3 hits)
+template <typename R, int MU>
+__global__ void __launch_bounds__(kBlock, min_blocks<R>()) link3_kernel(PassArgs p) {
+  link_tile<R, MU, 0, true, 3>(p, blockIdx.x);
 }
 
 // ------------------------------------------------------------------ finalize
@@ -422,6 +437,14 @@ __device__ __forceinline__ void finalize_combine(const FinalizeArgs& f) {
           // f/agauge.f:195-200
           m.plaq = l[2] / (12.0 * V);
           m.acc_gauge = (l[0] / (3.0 * V)) * (l[1] / (12.0 * V));
+          l[0] = l[1] = l[2] = l[3] = 0;
+        }
+      } else if (kind == kLinkHB3) {
+        for (int q = 0; q < kNQ; ++q) l[q] += t[q];
+        if (end) {
+          // f/agauge1.f:226-231: the Metropolis count is divided by the 3 hits
+          m.plaq = l[2] / (12.0 * V);
+          m.acc_gauge = (l[0] / (3.0 * V)) * (l[1] / (12.0 * V) / 3.0);
           l[0] = l[1] = l[2] = l[3] = 0;
         }
       } else if (kind == kLinkOR) {
@@ -522,6 +545,11 @@ __device__ __forceinline__ void persistent_pass(const PersistArgs& a, const Pass
       else if (e.mu == 1) for (int t = blockIdx.x; t < nt; t += gridDim.x) link_tile<R, 1, 0, false>(p, t);
       else for (int t = blockIdx.x; t < nt; t += gridDim.x) link_tile<R, 2, 0, false>(p, t);
       break;
+    case kLinkHB3:
+      if (e.mu == 0) for (int t = blockIdx.x; t < nt; t += gridDim.x) link_tile<R, 0, 0, false, 3>(p, t);
+      else if (e.mu == 1) for (int t = blockIdx.x; t < nt; t += gridDim.x) link_tile<R, 1, 0, false, 3>(p, t);
+      else for (int t = blockIdx.x; t < nt; t += gridDim.x) link_tile<R, 2, 0, false, 3>(p, t);
+      break;
     default:
       if (e.mu == 0) for (int t = blockIdx.x; t < nt; t += gridDim.x) link_tile<R, 0, 1, false>(p, t);
       else if (e.mu == 1) for (int t = blockIdx.x; t < nt; t += gridDim.x) link_tile<R, 1, 1, false>(p, t);
@@ -541,7 +569,7 @@ __global__ void __launch_bounds__(kBlock, kPersistMinBlocks) sweep_persistent_ke
   for (int i = 0; i < a.npasses; ++i) {
     const PlanEntry e = a.plan[i];
     p.eo = e.eo;
-    p.pass_off = (unsigned)i;
+    p.pass_off = a.pass_off[i];
     p.stream_off = a.stream_off[i];
     p.part = e.slot == kNoSlot ? nullptr : const_cast<double*>(a.fin.part) + (size_t)e.slot * a.fin.slot_stride;
     persistent_pass<R>(a, p, e);
@@ -604,7 +632,8 @@ template <typename R>
 void launch_link(int mode, int mu, const PassArgs& a, int nblocks, cudaStream_t s) {
   void (*k)(PassArgs);
   if (mode == 0) k = mu == 0 ? link_kernel<R, 0, 0> : (mu == 1 ? link_kernel<R, 1, 0> : link_kernel<R, 2, 0>);
-  else k = mu == 0 ? link_kernel<R, 0, 1> : (mu == 1 ? link_kernel<R, 1, 1> : link_kernel<R, 2, 1>);
+  else if (mode == 1) k = mu == 0 ? link_kernel<R, 0, 1> : (mu == 1 ? link_kernel<R, 1, 1> : link_kernel<R, 2, 1>);
+  else k = mu == 0 ? link3_kernel<R, 0> : (mu == 1 ? link3_kernel<R, 1> : link3_kernel<R, 2>);
   (void)launch_pdl(k, nblocks, kBlock, 0, s, a);
 }
 

@@ -10,7 +10,15 @@
 //
 //   lce_main [--input FILE] [--dir DIR] [--precision f32|f64] [--seed N]
 //            [--corr-flag 1|2|3] [--therm N] [--max-gf-iters N]
-//            [--gf-angle acos|atan2] [--device N]
+//            [--gf-angle acos|atan2] [--device N] [--agauge-hits 1|3]
+//            [--gauge-fix plain|warm|fourier]
+//
+// --agauge-hits 3 runs the 3-hit link update of f/agauge1.f (the reference
+// picks agauge.f or agauge1.f at build time).  --gauge-fix: plain is
+// f/landau_gauge.f (copy, overrelaxation from G = 1); warm starts every
+// measurement after the first from the previous converged transform; fourier
+// uses the Fourier-accelerated iteration (power-of-two extents) from that warm
+// start.  All three stop at theta <= limit_or.
 //
 // Deviations: init = 0 is a Haar hot start on the device (the reference's
 // randomconf is not Haar distributed, f/confget.f:115-149); the per-site
@@ -166,6 +174,8 @@ std::string header(const Input& in) {
 int main(int argc, char** argv) {
   std::string input = "inputfile", dir = ".";
   int prec = LCE_PREC_F32, corr_flag = 1, therm = 100, device = 0, max_gf = 0, gf_angle = LCE_GF_ATAN2;
+  int agauge_hits = 1;
+  std::string gauge_fix = "plain";
   unsigned long long seed = 314159;
   for (int i = 1; i < argc; ++i) {
     std::string a = argv[i];
@@ -182,6 +192,8 @@ int main(int argc, char** argv) {
     else if (a == "--device") device = std::atoi(next().c_str());
     else if (a == "--max-gf-iters") max_gf = std::atoi(next().c_str());
     else if (a == "--gf-angle") gf_angle = next() == "acos" ? LCE_GF_ACOS : LCE_GF_ATAN2;
+    else if (a == "--agauge-hits") agauge_hits = std::atoi(next().c_str());
+    else if (a == "--gauge-fix") gauge_fix = next();
     else die("unknown option %s", a.c_str());
   }
   const Input in = read_input(input);
@@ -204,6 +216,8 @@ int main(int argc, char** argv) {
   p.seed = seed;
   p.device = device;
   p.gf_angle = gf_angle;
+  p.agauge_hits = agauge_hits;
+  if (gauge_fix != "plain" && gauge_fix != "warm" && gauge_fix != "fourier") die("unknown --gauge-fix %s", gauge_fix.c_str());
   lce_ctx* ctx = lce_create(&p);
   if (!ctx) die("lce_create: %s", lce_last_error(nullptr));
 
@@ -295,7 +309,17 @@ int main(int argc, char** argv) {
     if (corr_flag == 1 || corr_flag == 3) {
       double theta = 0;
       int iters = 0;
-      const int rc = lce_landau_gauge(ctx, 0, &theta, &iters, max_gf);
+      int rc;
+      const int start = meas > 1 ? LCE_GF_START_TRANSFORM : LCE_GF_START_IDENTITY;
+      if (gauge_fix == "warm") {
+        rc = lce_landau_gauge_from(ctx, 0, start, nullptr, &theta, &iters, max_gf);
+      } else if (gauge_fix == "fourier") {
+        int it_plain = 0;
+        rc = lce_landau_gauge_fourier(ctx, 0, start, 0.0, 0.0, &theta, &iters, &it_plain, max_gf);
+        iters += it_plain;
+      } else {
+        rc = lce_landau_gauge(ctx, 0, &theta, &iters, max_gf);
+      }
       if (rc == LCE_ERR_GF_NOT_CONVERGED)
         std::fprintf(stderr, "lce_main: gauge fixing stopped at the cap (theta %g after %d iterations)\n", theta, iters);
       else

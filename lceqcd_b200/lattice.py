@@ -58,6 +58,7 @@ class Params:
     delta0: float = 1.0
     gf_angle: str = "atan2"
     sweep_mode: str = "auto"
+    agauge_hits: int = 1
 
     def to_c(self) -> LceParams:
         p = LceParams()
@@ -76,6 +77,7 @@ class Params:
         p.delta0 = float(self.delta0)
         p.gf_angle = {"acos": _lib.LCE_GF_ACOS, "atan2": _lib.LCE_GF_ATAN2}[self.gf_angle]
         p.sweep_mode = SWEEP_MODES[self.sweep_mode]
+        p.agauge_hits = int(self.agauge_hits)
         return p
 
 
@@ -213,6 +215,12 @@ class _Context:
         self._ck(self.lib.lce_agauge(self.h, measflag, C.byref(acc)))
         return acc.value
 
+    def agauge1(self, measflag: int = 1) -> float:
+        """f/agauge1.f: the 3-hit link update."""
+        acc = C.c_float()
+        self._ck(self.lib.lce_agauge1(self.h, measflag, C.byref(acc)))
+        return acc.value
+
     def link_or(self, measflag: int = 1) -> float:
         acc = C.c_float()
         self._ck(self.lib.lce_link_or(self.h, measflag, C.byref(acc)))
@@ -267,19 +275,36 @@ class _Context:
         return ts.value, th.value, it.value
 
     def landau_gauge_warm(self, net=None, use_net: bool = True, judge: bool = True, record: bool = False,
-                          max_iters: int = 0, chain: int = 0):
+                          fourier: bool = False, max_iters: int = 0, chain: int = 0):
         """Tracked gauge fixing from a warm start (the previous transform, or the
         network's correction of it; with judge the start of largest gauge
         functional among identity / previous / network).  Returns
         (start, functionals[3], theta, iterations); start is 'identity',
         'transform' or 'net'."""
         flags = ((_lib.LCE_WARM_NET if (use_net and net is not None) else 0) |
-                 (_lib.LCE_WARM_JUDGE if judge else 0) | (_lib.LCE_WARM_RECORD if record else 0))
+                 (_lib.LCE_WARM_JUDGE if judge else 0) | (_lib.LCE_WARM_RECORD if record else 0) |
+                 (_lib.LCE_WARM_FOURIER if fourier else 0))
         su, th, it = C.c_int(), C.c_double(), C.c_int()
         F = (C.c_double * 3)()
         self._ck(self.lib.lce_landau_gauge_warm(self.h, chain, net.h if net is not None else None, flags,
                                                 C.byref(su), F, C.byref(th), C.byref(it), int(max_iters)))
         return ["identity", "transform", "net"][su.value], list(F), th.value, it.value
+
+    def landau_gauge_fourier(self, start: str = "identity", step: float = 1.0, theta_switch: float = 0.0,
+                             max_iters: int = 0, chain: int = 0):
+        """Fourier-accelerated gauge fixing (tracking G) to theta_switch, then the
+        plain iteration to limit_or.  Returns (theta, fourier_iters, plain_iters)."""
+        th, itf, itp = C.c_double(), C.c_int(), C.c_int()
+        code = {"identity": _lib.LCE_GF_START_IDENTITY, "transform": _lib.LCE_GF_START_TRANSFORM}[start]
+        self._ck(self.lib.lce_landau_gauge_fourier(self.h, chain, code, float(step), float(theta_switch),
+                                                   C.byref(th), C.byref(itf), C.byref(itp), int(max_iters)))
+        return th.value, itf.value, itp.value
+
+    def debug_fourier_step(self, step: float = 1.0, chain: int = 0) -> np.ndarray:
+        """Preconditioned direction omega [2][V/2][3] (a3, Re b, Im b) of the current U_f."""
+        om = np.zeros((2, self.nh(chain), 3), np.float64)
+        self._ck(self.lib.lce_debug_fourier_step(self.h, chain, float(step), _ptr(om)))
+        return om
 
     def apply_transform(self, chain: int = 0):
         self._ck(self.lib.lce_apply_transform(self.h, chain))

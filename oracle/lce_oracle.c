@@ -477,9 +477,11 @@ int lco_staples(lco_ctx *c, int eo, int mu) {
 }
 
 /* ------------------------------------------------------------------ */
-/* link update  f/agauge.f:49-200 with f/heat_kpi.f:9-101              */
+/* link update  f/agauge.f:49-200 with f/heat_kpi.f:9-101; nhit = 3 is  */
+/* f/agauge1.f:58-231 (staple once per pass, then three heatbath +      */
+/* Metropolis hits, each drawing its own 7 uniforms per site)           */
 /* ------------------------------------------------------------------ */
-int lco_agauge(lco_ctx *c, int measflag, lco_real *accept_out) {
+static int agauge_hits(lco_ctx *c, int measflag, int nhit, lco_real *accept_out) {
   const int nh = c->nh;
   const real tpi = (real)2.0 * (real)acos((real)-1.0);
   double kp_acc = 0, acc1 = 0, plaq = 0;
@@ -488,61 +490,66 @@ int lco_agauge(lco_ctx *c, int measflag, lco_real *accept_out) {
     const int oe = 1 - eo;
     for (int mu = 0; mu < 3; ++mu) {
       lco_staples(c, eo, mu);
-      if (draw_pass(c, 7, LAY_TRIPLE)) return -1;
       double pass_kp = 0, pass_acc = 0, pass_plaq = 0;
-#pragma omp parallel for num_threads(c->nthreads) schedule(static) reduction(+ : pass_kp, pass_acc, pass_plaq)
-      for (int s = 0; s < nh; ++s) {
-        /* 2) normalise the staple (:71-84) */
-        const real *vp = c->v + UIDX(c, mu, eo, s);
-        su2 vv = ld_su2(vp);
-        real t1 = vv.a.re * vv.a.re + vv.a.im * vv.a.im + vv.b.re * vv.b.re + vv.b.im * vv.b.im;
-        t1 = (real)1.0 / (real)sqrt(t1);
-        su2 vh = {{t1 * vv.a.re, t1 * vv.a.im}, {t1 * vv.b.re, t1 * vv.b.im}};
-        t1 = t1 / c->beta;
-        su2 uo = ld_su2(c->u + UIDX(c, mu, eo, s));
-        real t2 = csub(cmul(uo.a, vh.a), cmul(uo.b, cconj(vh.b))).re;
-        /* 3) heat_kpi (f/heat_kpi.f:33-98) */
-        real a1 = UNI(c, LAY_TRIPLE, 0, s), a2 = UNI(c, LAY_TRIPLE, 1, s), a3 = UNI(c, LAY_TRIPLE, 2, s);
-        if (a1 == (real)0.0) a1 = (real)0.0000033;
-        if (a2 == (real)0.0) a2 = (real)0.0000066;
-        real cc = (real)cos(tpi * a3);
-        real a0 = -((real)log(a1) + (real)log(a2) * (cc * cc)) * t1;
-        real r4 = UNI(c, LAY_TRIPLE, 3, s);
-        int lacc = (r4 * r4 <= ((real)1.0 - (real)0.5 * a0));
-        if (lacc) a0 = (real)1.0 - a0;
-        else a0 = t2;
-        pass_kp += lacc;
-        real b1 = (real)1.0 - a0 * a0;
-        b1 = (b1 >= (real)0.0) ? (real)sqrt(b1) : (real)0.0;
-        real b2 = (real)2.0 * (UNI(c, LAY_TRIPLE, 4, s) - (real)0.5);
-        real b3 = b1 * b2;
-        su2 X;
-        X.a = cmk(a0, b3);
-        real q0 = (real)1.0 - b2 * b2;
-        q0 = (q0 >= (real)0.0) ? b1 * (real)sqrt(q0) : (real)0.0;
-        real ph = tpi * UNI(c, LAY_TRIPLE, 5, s);
-        real q1 = q0 * (real)cos(ph);
-        real q2 = q0 * (real)sin(ph);
-        X.b = cmk(q2, q1);
-        /* 4) proposal h = X * Vhat^+ (:98-104) */
-        su2 hn = mul_nd(X, vh);
-        /* hopping term, old and new (:126-159) */
-        const real *ax = c->a + AIDX(c, eo, s);
-        const real *axm = c->a + AIDX(c, oe, UP(c, eo, mu, s));
-        su2 o1 = mul_an(ax, uo), n1 = mul_an(ax, hn);
-        su2 o3 = mul_ad(axm, uo), n3 = mul_ad(axm, hn);
-        real sa_old = c->beta_a * mul_nn(o1, o3).a.re;
-        real sa_new = c->beta_a * mul_nn(n1, n3).a.re;
-        /* accept (:167-174) */
-        real rx = UNI(c, LAY_TRIPLE, 6, s);
-        su2 un = uo;
-        if ((real)exp(sa_old - sa_new) >= rx) {
-          un = hn;
-          st_su2(c->u + UIDX(c, mu, eo, s), hn);
-          pass_acc += 1.0;
+      for (int hit = 0; hit < nhit; ++hit) {
+        if (draw_pass(c, 7, LAY_TRIPLE)) return -1;
+#pragma omp parallel for num_threads(c->nthreads) schedule(static) reduction(+ : pass_kp, pass_acc)
+        for (int s = 0; s < nh; ++s) {
+          /* 2) normalise the staple (f/agauge.f:71-84, f/agauge1.f:72-85) */
+          const real *vp = c->v + UIDX(c, mu, eo, s);
+          su2 vv = ld_su2(vp);
+          real t1 = vv.a.re * vv.a.re + vv.a.im * vv.a.im + vv.b.re * vv.b.re + vv.b.im * vv.b.im;
+          t1 = (real)1.0 / (real)sqrt(t1);
+          su2 vh = {{t1 * vv.a.re, t1 * vv.a.im}, {t1 * vv.b.re, t1 * vv.b.im}};
+          t1 = t1 / c->beta;
+          /* the current link: updated by an earlier hit (f/agauge1.f:100-103) */
+          su2 uo = ld_su2(c->u + UIDX(c, mu, eo, s));
+          real t2 = csub(cmul(uo.a, vh.a), cmul(uo.b, cconj(vh.b))).re;
+          /* 3) heat_kpi (f/heat_kpi.f:33-98) */
+          real a1 = UNI(c, LAY_TRIPLE, 0, s), a2 = UNI(c, LAY_TRIPLE, 1, s), a3 = UNI(c, LAY_TRIPLE, 2, s);
+          if (a1 == (real)0.0) a1 = (real)0.0000033;
+          if (a2 == (real)0.0) a2 = (real)0.0000066;
+          real cc = (real)cos(tpi * a3);
+          real a0 = -((real)log(a1) + (real)log(a2) * (cc * cc)) * t1;
+          real r4 = UNI(c, LAY_TRIPLE, 3, s);
+          int lacc = (r4 * r4 <= ((real)1.0 - (real)0.5 * a0));
+          if (lacc) a0 = (real)1.0 - a0;
+          else a0 = t2;
+          pass_kp += lacc;
+          real b1 = (real)1.0 - a0 * a0;
+          b1 = (b1 >= (real)0.0) ? (real)sqrt(b1) : (real)0.0;
+          real b2 = (real)2.0 * (UNI(c, LAY_TRIPLE, 4, s) - (real)0.5);
+          real b3 = b1 * b2;
+          su2 X;
+          X.a = cmk(a0, b3);
+          real q0 = (real)1.0 - b2 * b2;
+          q0 = (q0 >= (real)0.0) ? b1 * (real)sqrt(q0) : (real)0.0;
+          real ph = tpi * UNI(c, LAY_TRIPLE, 5, s);
+          real q1 = q0 * (real)cos(ph);
+          real q2 = q0 * (real)sin(ph);
+          X.b = cmk(q2, q1);
+          /* 4) proposal h = X * Vhat^+ (f/agauge.f:98-104) */
+          su2 hn = mul_nd(X, vh);
+          /* hopping term, old and new (:126-159) */
+          const real *ax = c->a + AIDX(c, eo, s);
+          const real *axm = c->a + AIDX(c, oe, UP(c, eo, mu, s));
+          su2 o1 = mul_an(ax, uo), n1 = mul_an(ax, hn);
+          su2 o3 = mul_ad(axm, uo), n3 = mul_ad(axm, hn);
+          real sa_old = c->beta_a * mul_nn(o1, o3).a.re;
+          real sa_new = c->beta_a * mul_nn(n1, n3).a.re;
+          /* accept (:167-174) */
+          real rx = UNI(c, LAY_TRIPLE, 6, s);
+          if ((real)exp(sa_old - sa_new) >= rx) {
+            st_su2(c->u + UIDX(c, mu, eo, s), hn);
+            pass_acc += 1.0;
+          }
         }
-        /* plaquette against the staple (:179-185) */
-        if (measflag == 1) pass_plaq += mul_nn(un, vv).a.re;
+      }
+      /* plaquette against the staple, after the hits (f/agauge.f:179-185, f/agauge1.f:207-214) */
+      if (measflag == 1) {
+#pragma omp parallel for num_threads(c->nthreads) schedule(static) reduction(+ : pass_plaq)
+        for (int s = 0; s < nh; ++s)
+          pass_plaq += mul_nn(ld_su2(c->u + UIDX(c, mu, eo, s)), ld_su2(c->v + UIDX(c, mu, eo, s))).a.re;
       }
       kp_acc += pass_kp;
       acc1 += pass_acc;
@@ -551,15 +558,20 @@ int lco_agauge(lco_ctx *c, int measflag, lco_real *accept_out) {
   }
   double accept = kp_acc;
   if (measflag == 1) {
+    /* f/agauge.f:195-200; f/agauge1.f:226-231 divides acc1 by nhit too */
     c->plaq0 = plaq / (12.0 * c->vol);
     accept = accept / (3.0 * c->vol);
-    acc1 = acc1 / (12.0 * c->vol);
+    acc1 = acc1 / (12.0 * c->vol) / nhit;
     accept = accept * acc1;
   }
   c->acc_gauge = accept;
   if (accept_out) *accept_out = (real)accept;
   return 0;
 }
+
+int lco_agauge(lco_ctx *c, int measflag, lco_real *accept_out) { return agauge_hits(c, measflag, 1, accept_out); }
+
+int lco_agauge1(lco_ctx *c, int measflag, lco_real *accept_out) { return agauge_hits(c, measflag, 3, accept_out); }
 
 /* Link overrelaxation (no reference counterpart; the reference has no link
  * OR).  Proposal U' = Vhat^+ U^+ Vhat^+ keeps Re Tr(U V) fixed; the hopping

@@ -114,6 +114,9 @@ int  lco_ahiggs1(lco_ctx *c, lco_real *delta, int measflag, lco_real *accept);
 int  lco_ahiggs2(lco_ctx *c, int measflag, lco_real *accept);
 int  lco_ahiggs3(lco_ctx *c, int measflag, lco_real *accept);
 int  lco_agauge(lco_ctx *c, int measflag, lco_real *accept);
+/* f/agauge1.f: the 3-hit form (staple once per pass, three heatbath +
+ * Metropolis hits of 7 uniforms per site each) */
+int  lco_agauge1(lco_ctx *c, int measflag, lco_real *accept);
 int  lco_link_or(lco_ctx *c, int measflag, lco_real *accept);
 void lco_renorm(lco_ctx *c);
 int  lco_sweep(lco_ctx *c, int measflag, lco_meas *m);   /* main.f:38-41 order */

@@ -75,6 +75,7 @@ def _lib(bits: int) -> C.CDLL:
         "lco_ahiggs2": (C.c_int, [P, C.c_int, P]),
         "lco_ahiggs3": (C.c_int, [P, C.c_int, P]),
         "lco_agauge": (C.c_int, [P, C.c_int, P]),
+        "lco_agauge1": (C.c_int, [P, C.c_int, P]),
         "lco_link_or": (C.c_int, [P, C.c_int, P]),
         "lco_renorm": (None, [P]),
         "lco_sweep": (C.c_int, [P, C.c_int, P]),
@@ -290,6 +291,12 @@ class Oracle:
     def agauge(self, measflag: int = 1) -> float:
         acc = self._acc()
         self._check(self.lib.lco_agauge(self.h, measflag, C.byref(acc)))
+        return acc.value
+
+    def agauge1(self, measflag: int = 1) -> float:
+        """f/agauge1.f: 3-hit link update."""
+        acc = self._acc()
+        self._check(self.lib.lco_agauge1(self.h, measflag, C.byref(acc)))
         return acc.value
 
     def link_or(self, measflag: int = 1) -> float:
