@@ -256,6 +256,38 @@ def extras(args, peak):
         lat.close()
     except Exception as e:
         out["gauge_fix_128cubed"] = {"error": repr(e)[:300]}
+    # the full production pipeline at 256^3 (beta = 16, x = 0.08, y = 0.2): a
+    # sweep is ahiggs2, ahiggs3, one ahiggs1, the agauge heatbath and 4 link
+    # overrelaxation hits; a measurement every 20 sweeps is a warm-started
+    # Fourier-accelerated Landau gauge fixing to theta < 1e-10 and the
+    # correlators.  Timed: 20 sweeps + 1 measurement, after thermalisation and a
+    # first gauge fixing from G = 1; the 2000-sweep run is projected from them.
+    try:
+        L = (256, 256, 256)
+        lat = Lattice(L, beta=16.0, x=0.08, y=0.2, precision="f32", seed=31, lam=1.7, limit_or=1e-10,
+                      n_link_or=4, n_higgs_metro=1)
+        lat.init_hot(32)
+        lat.sweeps(20, 0)
+        lat.landau_gauge_fourier("identity")
+        lat.synchronize()
+        t0 = time.perf_counter()
+        lat.sweeps(19, 0)
+        lat.sweep(1)
+        lat.synchronize()
+        t1 = time.perf_counter()
+        th, itf, itp = lat.landau_gauge_fourier("transform")
+        lat.correlator()
+        lat.synchronize()
+        t2 = time.perf_counter()
+        ms_sweep = (t1 - t0) / 20 * 1e3
+        out["pipeline_256cubed"] = {
+            "ms_per_sweep": ms_sweep, "sweep_passes": 4 + 2 + 6 + 24,
+            "s_per_measurement": t2 - t1, "gauge_fix_iterations": itf + itp, "theta": th,
+            "projected_s_2000_sweeps_100_measurements": 2000 * ms_sweep / 1e3 + 100 * (t2 - t1),
+            "site_updates_per_s": vol(L) * 20 / (t1 - t0), "note": "host wall clock around synchronised calls"}
+        lat.close()
+    except Exception as e:
+        out["pipeline_256cubed"] = {"error": repr(e)[:300]}
     # batched ensemble: 96 chains (32 each of 16^3, 32^3, 48^3) over the
     # coupling grid, against the same chains run one context at a time
     try:
@@ -470,6 +502,26 @@ def run_reference(args):
     print(json.dumps(line), flush=True)
 
 
+def quick_gauge_fix(args):
+    """The Fourier-accelerated gauge fixing as a profiling case: args.quick_gauge_fix
+    iterations (7 kernel launches each) from G = 1, stopped by the iteration cap."""
+    from lceqcd_b200 import Lattice, LceError
+    n = args.lattice or 128
+    lat = Lattice((n, n, n), **COUP, precision="f32", seed=21, lam=1.7, limit_or=1e-10)
+    lat.init_hot(22)
+    lat.sweeps(20, 0)
+    lat.synchronize()
+    t0 = time.perf_counter()
+    try:
+        lat.landau_gauge_fourier("identity", max_iters=args.quick_gauge_fix)
+    except LceError as e:
+        if e.code != -3:  # LCE_ERR_GF_NOT_CONVERGED: the cap stopped it, as intended
+            raise
+    lat.synchronize()
+    print(json.dumps({"quick_gauge_fix": args.quick_gauge_fix, "L": n, "theta": lat.theta(),
+                      "s": time.perf_counter() - t0}), flush=True)
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -483,7 +535,13 @@ def main():
     ap.add_argument("--lattice", type=int, default=0, help="cubic extent for --quick runs (default 64)")
     ap.add_argument("--sweep-mode", default="auto", choices=["auto", "passes", "persistent"],
                     help="sweep form (default: the library's autotuner chooses)")
+    ap.add_argument("--quick-gauge-fix", type=int, default=0, metavar="ITERS",
+                    help="profiling case: ITERS Fourier-accelerated gauge-fixing iterations on a thermalised "
+                         "--lattice^3 FP32 configuration, then exit")
     args = ap.parse_args()
+    if args.quick_gauge_fix:
+        quick_gauge_fix(args)
+        return
     if args.warmup < 3:
         args.warmup = 3
     if args.lattice and not args.quick:

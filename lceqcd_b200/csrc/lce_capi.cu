@@ -710,14 +710,20 @@ int gf_loop(lce_ctx* c, int chain, double* theta, int* iters, int max_iters, int
   return LCE_OK;
 }
 
-int fa_buffers(lce_ctx* c, const ChainDev& ch) {
-  const size_t need = fa_buffer_bytes(ch);
-  if (c->fa_bytes >= need) return LCE_OK;
-  if (c->fa_d) CK(cudaFree(c->fa_d));
-  c->fa_d = nullptr;
-  c->fa_bytes = 0;
-  if (cudaMalloc(&c->fa_d, need) != cudaSuccess) return fail(c, LCE_ERR_NOMEM, "Fourier-accelerated fixing buffers");
+// one allocation for the largest chain, allocated once: the captured graphs
+// of every chain keep pointing into it
+size_t fa_vcap(const lce_ctx* c) { return 2 * (size_t)c->max_nh; }
+
+int fa_buffers(lce_ctx* c) {
+  if (c->fa_d) return LCE_OK;
+  const size_t need = fa_buffer_bytes(fa_vcap(c));
+  if (cudaMalloc(&c->fa_d, need) != cudaSuccess) {
+    c->fa_d = nullptr;
+    return fail(c, LCE_ERR_NOMEM, "Fourier-accelerated fixing buffers");
+  }
   c->fa_bytes = need;
+  fa_init_table(c->fa_d, fa_vcap(c), c->stream);
+  CK(cudaGetLastError());
   return LCE_OK;
 }
 
@@ -725,7 +731,7 @@ int fa_buffers(lce_ctx* c, const ChainDev& ch) {
 // the cap; same graph batching and progress guard as gf_loop
 int fa_loop(lce_ctx* c, int chain, double step, double limit, double* theta, int* iters, int cap) {
   const ChainDev& ch = c->ch[chain];
-  int rc = fa_buffers(c, ch);
+  int rc = fa_buffers(c);
   if (rc) return rc;
   ChainState cs;
   CK(cudaMemcpyAsync(&cs, c->cst_d + chain, sizeof(cs), cudaMemcpyDeviceToHost, c->stream));
@@ -748,11 +754,11 @@ int fa_loop(lce_ctx* c, int chain, double step, double limit, double* theta, int
       CK(cudaStreamBeginCapture(c->stream, cudaStreamCaptureModeThreadLocal));
       for (int k = 0; k < batch; ++k) {
         if (c->prec == LCE_PREC_F64)
-          launch_fa_iteration<double>(c->ch_d + chain, ch, c->cst_d + chain, step, c->fa_d, part, nullptr, 1, true,
-                                      true, c->stream);
+          launch_fa_iteration<double>(c->ch_d + chain, ch, c->cst_d + chain, step, c->fa_d, fa_vcap(c), part,
+                                      nullptr, 1, true, true, c->stream);
         else
-          launch_fa_iteration<float>(c->ch_d + chain, ch, c->cst_d + chain, step, c->fa_d, part, nullptr, 1, true,
-                                     true, c->stream);
+          launch_fa_iteration<float>(c->ch_d + chain, ch, c->cst_d + chain, step, c->fa_d, fa_vcap(c), part,
+                                     nullptr, 1, true, true, c->stream);
       }
       CK(cudaStreamEndCapture(c->stream, &g));
       cudaGraphExec_t ex;
@@ -1250,17 +1256,17 @@ int lce_debug_fourier_step(lce_ctx* c, int chain, double step, double* omega) {
   if (!c || !omega || chain < 0 || chain >= c->nchains) return LCE_ERR_INVALID;
   const ChainDev& ch = c->ch[chain];
   if (!fa_supported(ch)) return fail(c, LCE_ERR_UNSUPPORTED, "power-of-two extents needed");
-  int rc = fa_buffers(c, ch);
+  int rc = fa_buffers(c);
   if (rc) return rc;
   double* om = nullptr;
   const size_t ob = sizeof(double) * 3 * 2 * (size_t)ch.nh;
   CK(cudaMalloc(&om, ob));
   if (c->prec == LCE_PREC_F64)
-    launch_fa_iteration<double>(c->ch_d + chain, ch, nullptr, step, c->fa_d, c->scratch_d, om, 0, false, false,
-                                c->stream);
+    launch_fa_iteration<double>(c->ch_d + chain, ch, nullptr, step, c->fa_d, fa_vcap(c), c->scratch_d, om, 0, false,
+                                false, c->stream);
   else
-    launch_fa_iteration<float>(c->ch_d + chain, ch, nullptr, step, c->fa_d, c->scratch_d, om, 0, false, false,
-                               c->stream);
+    launch_fa_iteration<float>(c->ch_d + chain, ch, nullptr, step, c->fa_d, fa_vcap(c), c->scratch_d, om, 0, false,
+                               false, c->stream);
   cudaError_t e = cudaGetLastError();
   if (e == cudaSuccess) e = cudaMemcpyAsync(omega, om, ob, cudaMemcpyDeviceToHost, c->stream);
   if (e == cudaSuccess) e = cudaStreamSynchronize(c->stream);

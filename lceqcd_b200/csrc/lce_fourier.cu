@@ -27,9 +27,10 @@
 // U_f, A_f and the tracked transform G.  The FFTs are radix-2 in shared
 // memory over a block of lines (512 complex points per block; lines padded by
 // one element against bank conflicts); extents must be powers of two up to
-// 512.  The divergence, the transforms, g and its application are FP64 for
-// either field precision: with FP32 arithmetic the step loses accuracy for the
-// amplified long-wavelength modes and the iteration slows below theta ~ 1e-8.  Two complex fields carry the three components:
+// 512.  The divergence, g and its application to the fields are FP64 for
+// either field precision (rounding the step's rotation to FP32 before
+// applying it slowed the iteration below theta ~ 1e-8 at 64^3); the
+// transforms themselves are FP32.  Two complex fields carry the three components:
 // (Delta_b) and (Delta_a3 + 0i); the multiplier is real and even in p, so the
 // inverse transform returns each component in its own slot.
 #include <algorithm>
@@ -40,20 +41,15 @@ namespace lce {
 namespace {
 
 constexpr int kFaThreads = 256;
+// complex type of the transforms: FP32 (timed on the B200: the same iteration
+// counts as FP64 transforms at 64^3-256^3, 20-30% less time per iteration)
+using FftR = float;
+using FftC = float2;
 // complex points per block and field, and the padded shared-memory size
 constexpr int kFaPoints = 512;
+constexpr int kFaLogPoints = 9;
+static_assert(1 << kFaLogPoints == kFaPoints, "points per block");
 constexpr int kFaSmem = kFaPoints + kFaPoints / 2;
-
-template <typename R>
-struct CX;
-template <>
-struct CX<float> {
-  using T = float2;
-};
-template <>
-struct CX<double> {
-  using T = double2;
-};
 
 template <typename T>
 __device__ __forceinline__ T cadd(T a, T b) { return T{a.x + b.x, a.y + b.y}; }
@@ -62,18 +58,14 @@ __device__ __forceinline__ T csub(T a, T b) { return T{a.x - b.x, a.y - b.y}; }
 template <typename T>
 __device__ __forceinline__ T cmul(T a, T b) { return T{a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x}; }
 
-__device__ __forceinline__ void sincospi_r(float x, float* s, float* c) { sincospif(x, s, c); }
-__device__ __forceinline__ void sincospi_r(double x, double* s, double* c) { sincospi(x, s, c); }
-__device__ __forceinline__ float sinpi_r(float x) { return sinpif(x); }
 __device__ __forceinline__ double sinpi_r(double x) { return sinpi(x); }
 
-// tw[k] = exp(sign 2 pi i k / n), k < n/2
-template <typename R>
-__device__ __forceinline__ void make_twiddles(typename CX<R>::T* tw, int n, int sign) {
+// tw[k] = exp(sign 2 pi i k / n), k < n/2, from the table tg[k] = exp(-2 pi i k / kFaPoints)
+__device__ __forceinline__ void load_twiddles(FftC* tw, const double2* tg, int n, int sign) {
+  const int stride = kFaPoints / n;
   for (int k = threadIdx.x; k < n / 2; k += blockDim.x) {
-    R s, c;
-    sincospi_r((R)(2 * k) / (R)n, &s, &c);
-    tw[k] = typename CX<R>::T{c, sign > 0 ? s : -s};
+    const double2 t = __ldg(tg + k * stride);
+    tw[k] = FftC{(FftR)t.x, (FftR)(sign > 0 ? -t.y : t.y)};
   }
 }
 
@@ -118,6 +110,7 @@ struct FaArgs {
   void* gstep;            // g per site, [parity][site], link layout
   double* part;           // [block]: theta (odd sites)
   double* omega_out;      // debug: omega per site [parity][site][3], or NULL
+  const double2* tw;      // exp(-2 pi i k / kFaPoints), k < kFaPoints / 2
   int L[3], logL[3];
   int track;
 };
@@ -125,33 +118,34 @@ struct FaArgs {
 __device__ __forceinline__ bool fa_done(const FaArgs& a) { return a.cst && a.cst->gf_done; }
 
 // line l of axis AX and position k along it -> natural index
+// (all extents are powers of two: divisions are shifts)
 template <int AX>
 __device__ __forceinline__ size_t nat_index(const FaArgs& a, int l, int k) {
-  const int L1 = a.L[0], L2 = a.L[1];
-  if (AX == 0) return (size_t)l * L1 + k;                                      // l = y + L2 z
-  if (AX == 1) return ((size_t)(l / L1) * L2 + k) * L1 + (l % L1);            // l = x + L1 z
-  return ((size_t)k * L2 + (l / L1)) * L1 + (l % L1);                          // l = x + L1 y
+  const int s1 = a.logL[0], s2 = a.logL[1], m1 = a.L[0] - 1;
+  if (AX == 0) return ((size_t)l << s1) + k;                                          // l = y + L2 z
+  if (AX == 1) return ((((size_t)(l >> s1) << s2) + k) << s1) + (l & m1);             // l = x + L1 z
+  return ((((size_t)k << s2) + (l >> s1)) << s1) + (l & m1);                          // l = x + L1 y
 }
 
 // (1) Delta on x-lines, forward FFT along x; partials of theta
 template <typename R>
 __global__ void __launch_bounds__(kFaThreads) fa_div_kernel(FaArgs a) {
-  using T = double2;
+  using T = FftC;
   __shared__ T sm[2][kFaSmem];
   __shared__ T tw[kFaPoints / 2];
   if (fa_done(a)) return;
   const ChainDev& ch = *a.ch;
   const int n = a.L[0], logn = a.logL[0], ld = n + 1;
-  const int nl = kFaPoints / n, nlines = a.L[1] * a.L[2];
+  const int nl = kFaPoints >> logn, nlines = a.L[1] * a.L[2];
   const int l0 = blockIdx.x * nl;
-  make_twiddles<double>(tw, n, -1);
+  load_twiddles(tw, a.tw, n, -1);
   const double al = ch.alpha;
   double q[1] = {0.0};
   for (int e = threadIdx.x; e < nl * n; e += blockDim.x) {
-    const int j = e / n, x = e - j * n, l = l0 + j;
+    const int j = e >> logn, x = e & (n - 1), l = l0 + j;
     T v0{0, 0}, v1{0, 0};
     if (l < nlines) {
-      const int y = l % a.L[1], z = l / a.L[1];
+      const int y = l & (a.L[1] - 1), z = l >> a.logL[1];
       const int p = (x + y + z) & 1, op = 1 - p;
       const int s = site_index(x, y, z, ch.hx, ch.nxy);
       const int xm[3] = {site_index(wrap(x - 1, ch.L1), y, z, ch.hx, ch.nxy),
@@ -168,8 +162,8 @@ __global__ void __launch_bounds__(kFaThreads) fa_div_kernel(FaArgs a) {
         dbi += c * ((double)u.b.im - (double)w.b.im);
       }
       if (p == 1) q[0] += d3 * d3 + dbr * dbr + dbi * dbi;
-      v0 = T{dbr, dbi};
-      v1 = T{d3, 0.0};
+      v0 = T{(FftR)dbr, (FftR)dbi};
+      v1 = T{(FftR)d3, (FftR)0};
     }
     const int pos = j * ld + brev(x, logn);
     sm[0][pos] = v0;
@@ -182,7 +176,7 @@ __global__ void __launch_bounds__(kFaThreads) fa_div_kernel(FaArgs a) {
   const size_t V = (size_t)a.L[0] * a.L[1] * a.L[2];
   T* F = reinterpret_cast<T*>(a.fft);
   for (int e = threadIdx.x; e < nl * n; e += blockDim.x) {
-    const int j = e / n, k = e - j * n, l = l0 + j;
+    const int j = e >> logn, k = e & (n - 1), l = l0 + j;
     if (l >= nlines) continue;
     const size_t gi = nat_index<0>(a, l, k);
     F[gi] = sm[0][j * ld + k];
@@ -216,45 +210,55 @@ __global__ void __launch_bounds__(1024) fa_check_kernel(const ChainDev* chp, Cha
 // SCALE: forward, multiply by gamma / (p_c^2 V), inverse
 template <typename R, int AX, int SIGN, bool SCALE>
 __global__ void __launch_bounds__(kFaThreads) fa_fft_kernel(FaArgs a) {
-  using T = double2;
+  using T = FftC;
   __shared__ T sm[kFaSmem];
   __shared__ T tw[kFaPoints / 2];
   __shared__ T twi[SCALE ? kFaPoints / 2 : 1];
   if (fa_done(a)) return;
   const int n = a.L[AX], logn = a.logL[AX], ld = n + 1;
-  const int nl = kFaPoints / n;
-  const int nlines = (a.L[0] * a.L[1] * a.L[2]) / n;
+  const int lnl = kFaLogPoints - logn, nl = 1 << lnl;
+  const int nlines = (a.L[0] * a.L[1] * a.L[2]) >> logn;
   const int l0 = blockIdx.x * nl;
   const int fld = blockIdx.y;
   const size_t V = (size_t)a.L[0] * a.L[1] * a.L[2];
   T* F = reinterpret_cast<T*>(a.fft) + fld * V;
-  make_twiddles<double>(tw, n, SIGN);
-  if (SCALE) make_twiddles<double>(twi, n, -SIGN);
+  __shared__ double sz2[SCALE ? kFaPoints : 1];  // alpha sin^2(pi kz / L3)
+  __shared__ double sxy[SCALE ? kFaPoints : 1];  // sin^2(pi kx / L1) + sin^2(pi ky / L2) per line
+  load_twiddles(tw, a.tw, n, SIGN);
+  if (SCALE) {
+    load_twiddles(twi, a.tw, n, -SIGN);
+    const double al = a.ch->alpha;
+    for (int k = threadIdx.x; k < n; k += blockDim.x) {
+      const double sz = sinpi_r((double)k / a.L[2]);
+      sz2[k] = al * sz * sz;
+    }
+    for (int j = threadIdx.x; j < nl; j += blockDim.x) {
+      const int l = l0 + j, kx = l & (a.L[0] - 1), ky = l >> a.logL[0];
+      const double sx = sinpi_r((double)kx / a.L[0]), sy = sinpi_r((double)ky / a.L[1]);
+      sxy[j] = sx * sx + sy * sy;
+    }
+  }
   // element e -> (line j = e % nl, position k = e / nl): consecutive threads
   // read consecutive lines, i.e. consecutive x
   for (int e = threadIdx.x; e < nl * n; e += blockDim.x) {
-    const int j = e % nl, k = e / nl, l = l0 + j;
+    const int j = e & (nl - 1), k = e >> lnl, l = l0 + j;
     sm[j * ld + brev(k, logn)] = l < nlines ? F[nat_index<AX>(a, l, k)] : T{0, 0};
   }
   __syncthreads();
   fft_lines<T>(sm, nl, logn, tw);
   if (SCALE) {
-    const double gamma = a.cst ? a.cst->gf_step : a.gamma;
-    const double al = a.ch->alpha;
+    const double gv = (a.cst ? a.cst->gf_step : a.gamma) / (4.0 * (double)V);
     for (int e = threadIdx.x; e < nl * n; e += blockDim.x) {
-      const int j = e / n, kz = e - j * n, l = l0 + j;
-      const int kx = l % a.L[0], ky = l / a.L[0];
-      const double sx = sinpi_r((double)kx / a.L[0]), sy = sinpi_r((double)ky / a.L[1]),
-                   sz = sinpi_r((double)kz / a.L[2]);
-      const double p2 = 4.0 * (sx * sx + sy * sy + al * sz * sz);
-      const double m = (kx | ky | kz) ? gamma / (p2 * (double)V) : 0.0;
+      const int j = e >> logn, kz = e & (n - 1), l = l0 + j;
+      const double p2 = sxy[j] + sz2[kz];
+      const double m = (l | kz) ? gv / p2 : 0.0;
       const int q = j * ld + kz;
-      sm[q] = T{sm[q].x * m, sm[q].y * m};
+      sm[q] = T{(FftR)(sm[q].x * m), (FftR)(sm[q].y * m)};
     }
     __syncthreads();
     // bit-reverse permutation for the inverse transform
     for (int e = threadIdx.x; e < nl * n; e += blockDim.x) {
-      const int j = e / n, k = e - j * n, r = brev(k, logn);
+      const int j = e >> logn, k = e & (n - 1), r = brev(k, logn);
       if (r > k) {
         const T t = sm[j * ld + k];
         sm[j * ld + k] = sm[j * ld + r];
@@ -265,7 +269,7 @@ __global__ void __launch_bounds__(kFaThreads) fa_fft_kernel(FaArgs a) {
     fft_lines<T>(sm, nl, logn, twi);
   }
   for (int e = threadIdx.x; e < nl * n; e += blockDim.x) {
-    const int j = e % nl, k = e / nl, l = l0 + j;
+    const int j = e & (nl - 1), k = e >> lnl, l = l0 + j;
     if (l < nlines) F[nat_index<AX>(a, l, k)] = sm[j * ld + k];
   }
 }
@@ -273,19 +277,19 @@ __global__ void __launch_bounds__(kFaThreads) fa_fft_kernel(FaArgs a) {
 // (6) inverse FFT along x; g(x) = exp(-i omega.sigma) per site
 template <typename R>
 __global__ void __launch_bounds__(kFaThreads) fa_g_kernel(FaArgs a) {
-  using T = double2;
+  using T = FftC;
   __shared__ T sm[2][kFaSmem];
   __shared__ T tw[kFaPoints / 2];
   if (fa_done(a)) return;
   const ChainDev& ch = *a.ch;
   const int n = a.L[0], logn = a.logL[0], ld = n + 1;
-  const int nl = kFaPoints / n, nlines = a.L[1] * a.L[2];
+  const int nl = kFaPoints >> logn, nlines = a.L[1] * a.L[2];
   const int l0 = blockIdx.x * nl;
   const size_t V = (size_t)a.L[0] * a.L[1] * a.L[2];
   const T* F = reinterpret_cast<const T*>(a.fft);
-  make_twiddles<double>(tw, n, +1);
+  load_twiddles(tw, a.tw, n, +1);
   for (int e = threadIdx.x; e < nl * n; e += blockDim.x) {
-    const int j = e / n, k = e - j * n, l = l0 + j;
+    const int j = e >> logn, k = e & (n - 1), l = l0 + j;
     const size_t gi = l < nlines ? nat_index<0>(a, l, k) : 0;
     sm[0][j * ld + brev(k, logn)] = l < nlines ? F[gi] : T{0, 0};
     sm[1][j * ld + brev(k, logn)] = l < nlines ? F[V + gi] : T{0, 0};
@@ -294,9 +298,9 @@ __global__ void __launch_bounds__(kFaThreads) fa_g_kernel(FaArgs a) {
   fft_lines<T>(sm[0], nl, logn, tw);
   fft_lines<T>(sm[1], nl, logn, tw);
   for (int e = threadIdx.x; e < nl * n; e += blockDim.x) {
-    const int j = e / n, x = e - j * n, l = l0 + j;
+    const int j = e >> logn, x = e & (n - 1), l = l0 + j;
     if (l >= nlines) continue;
-    const int y = l % a.L[1], z = l / a.L[1];
+    const int y = l & (a.L[1] - 1), z = l >> a.logL[1];
     const int p = (x + y + z) & 1, s = site_index(x, y, z, ch.hx, ch.nxy);
     const double w3 = sm[1][j * ld + x].x, wbr = sm[0][j * ld + x].x, wbi = sm[0][j * ld + x].y;
     const double nw = sqrt(w3 * w3 + wbr * wbr + wbi * wbi);
@@ -368,9 +372,31 @@ bool fa_supported(const ChainDev& ch) {
 }
 
 // two FP64 complex fields and the FP64 step transform
-size_t fa_buffer_bytes(const ChainDev& ch) {
-  const size_t V = 2 * (size_t)ch.nh;
-  return 2 * V * sizeof(double2) + V * 32 + 256;
+// Buffer layout for chains of up to vcap sites: two FP64 complex fields,
+// the FP64 step transform and the twiddle table (fixed offsets, so graphs
+// captured for one chain stay valid while others use the same buffer)
+size_t fa_buffer_bytes(size_t vcap) {
+  return 2 * vcap * sizeof(FftC) + vcap * 32 + kFaPoints / 2 * sizeof(double2) + 256;
+}
+namespace {
+void* fa_gstep(void* buf, size_t vcap) { return reinterpret_cast<char*>(buf) + 2 * vcap * sizeof(FftC); }
+double2* fa_table(void* buf, size_t vcap) {
+  return reinterpret_cast<double2*>(reinterpret_cast<char*>(buf) + 2 * vcap * sizeof(FftC) + vcap * 32);
+}
+}  // namespace
+
+namespace {
+__global__ void fa_twiddle_table_kernel(double2* tg) {
+  const int k = blockIdx.x * blockDim.x + threadIdx.x;
+  if (k >= kFaPoints / 2) return;
+  double s, c;
+  sincospi((double)(2 * k) / kFaPoints, &s, &c);
+  tg[k] = double2{c, -s};
+}
+}  // namespace
+
+void fa_init_table(void* buf, size_t vcap, cudaStream_t s) {
+  fa_twiddle_table_kernel<<<1, kFaPoints / 2, 0, s>>>(fa_table(buf, vcap));
 }
 
 template <typename R>
@@ -379,7 +405,7 @@ int fa_blocks_div(const ChainDev& ch) { return ceil_div((long)ch.L2 * ch.L3, kFa
 // enqueue one Fourier-accelerated iteration (kernels 1-7)
 template <typename R>
 void launch_fa_iteration(const ChainDev* chd, const ChainDev& ch, ChainState* cst, double gamma, void* buf,
-                         double* part, double* omega_out, int track, bool with_check, bool with_apply,
+                         size_t vcap, double* part, double* omega_out, int track, bool with_check, bool with_apply,
                          cudaStream_t s) {
   FaArgs a;
   a.ch = chd;
@@ -387,9 +413,10 @@ void launch_fa_iteration(const ChainDev* chd, const ChainDev& ch, ChainState* cs
   a.gamma = gamma;
   a.fft = buf;
   const size_t V = 2 * (size_t)ch.nh;
-  a.gstep = reinterpret_cast<char*>(buf) + 2 * V * sizeof(double2);
+  a.gstep = fa_gstep(buf, vcap);
   a.part = part;
   a.omega_out = omega_out;
+  a.tw = fa_table(buf, vcap);
   a.L[0] = ch.L1;
   a.L[1] = ch.L2;
   a.L[2] = ch.L3;
@@ -407,9 +434,9 @@ void launch_fa_iteration(const ChainDev* chd, const ChainDev& ch, ChainState* cs
   if (with_apply) fa_apply_kernel<R><<<ceil_div((long)V, kBlock), kBlock, 0, s>>>(a);
 }
 
-template void launch_fa_iteration<float>(const ChainDev*, const ChainDev&, ChainState*, double, void*, double*,
-                                         double*, int, bool, bool, cudaStream_t);
-template void launch_fa_iteration<double>(const ChainDev*, const ChainDev&, ChainState*, double, void*, double*,
-                                          double*, int, bool, bool, cudaStream_t);
+template void launch_fa_iteration<float>(const ChainDev*, const ChainDev&, ChainState*, double, void*, size_t,
+                                         double*, double*, int, bool, bool, cudaStream_t);
+template void launch_fa_iteration<double>(const ChainDev*, const ChainDev&, ChainState*, double, void*, size_t,
+                                          double*, double*, int, bool, bool, cudaStream_t);
 
 }  // namespace lce

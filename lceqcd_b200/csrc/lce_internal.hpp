@@ -187,11 +187,14 @@ void launch_transform_identity(void* g, int nh, cudaStream_t s);
 
 // ---- Fourier-accelerated gauge fixing (lce_fourier.cu)
 bool fa_supported(const ChainDev& ch);
-size_t fa_buffer_bytes(const ChainDev& ch);
+// buffers for chains of up to vcap sites (fixed layout)
+size_t fa_buffer_bytes(size_t vcap);
+// fill the twiddle table of freshly allocated buffers
+void fa_init_table(void* buf, size_t vcap, cudaStream_t s);
 // one iteration; cst NULL (debug): never done, step gamma instead of the chain state's
 template <typename R>
 void launch_fa_iteration(const ChainDev* chd, const ChainDev& ch, ChainState* cst, double gamma, void* buf,
-                         double* part, double* omega_out, int track, bool with_check, bool with_apply,
+                         size_t vcap, double* part, double* omega_out, int track, bool with_check, bool with_apply,
                          cudaStream_t s);
 template <typename R>
 void launch_gf_theta(const ChainDev* ch, double* part, int nh, cudaStream_t s);

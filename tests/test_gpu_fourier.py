@@ -39,9 +39,11 @@ def numpy_direction(uf, L, alpha, step):
     return out.reshape(2, nh, 3), D
 
 
-@pytest.mark.parametrize("precision,L,tol", [("f64", (8, 8, 8), 1e-12), ("f64", (16, 4, 8), 1e-12),
-                                             ("f32", (8, 16, 4), 1e-11), ("f32", (32, 32, 32), 1e-11),
-                                             ("f64", (4, 4, 64), 1e-12)])
+# the transforms are FP32 (the divergence and the step's application FP64):
+# the direction agrees with numpy's FP64 FFT to FP32 accuracy
+@pytest.mark.parametrize("precision,L,tol", [("f64", (8, 8, 8), 2e-6), ("f64", (16, 4, 8), 2e-6),
+                                             ("f32", (8, 16, 4), 2e-6), ("f32", (32, 32, 32), 5e-6),
+                                             ("f64", (4, 4, 64), 5e-6), ("f32", (128, 4, 2), 5e-6)])
 def test_preconditioned_direction_matches_numpy_fft(precision, L, tol):
     from lceqcd_b200 import Lattice
     # alpha exactly representable: FP32 contexts hold the couplings in FP32
@@ -128,3 +130,21 @@ def test_fourier_from_a_warm_start_and_with_a_plain_finish():
     g.sweeps(3, 0)
     th, itf3, itp3 = g.landau_gauge_fourier("identity", theta_switch=1e-6)
     assert th <= 1e-10 and itp3 >= 1 and itf3 < itf
+
+
+def test_fourier_in_a_batch_of_uneven_volumes():
+    """Chains of different volumes share the context's buffers; each chain's
+    captured iteration graphs stay valid when the others run in between."""
+    from lceqcd_b200 import Ensemble, Params
+    specs = [Params(L=(16, 16, 16), **COUP, limit_or=1e-10, seed=1),
+             Params(L=(32, 16, 8), **COUP, limit_or=1e-10, seed=2),
+             Params(L=(8, 8, 8), **COUP, limit_or=1e-10, seed=3)]
+    ens = Ensemble(specs)
+    ens.init_hot(4)
+    ens.sweeps(30, 0)
+    for rnd in range(2):
+        for c in (2, 0, 1) if rnd else (0, 1, 2):
+            th, itf, itp = ens.landau_gauge_fourier("identity" if rnd == 0 else "transform", chain=c)
+            assert th <= 1e-10 and itp == 0
+            assert ens.theta(chain=c) <= 1e-10
+        ens.sweeps(2, 0)
