@@ -196,10 +196,13 @@ def extras(args, peak):
     import numpy as np
     from lceqcd_b200 import Ensemble, Lattice, Params
     out = {}
-    for L in ((128, 128, 128), (256, 256, 256)):
-        key = f"sweep_{L[0]}cubed"
+    # the reference's sweep composition at 128^3 and 256^3, and at 128^3 the
+    # production composition of the heatbath + overrelaxation runs (the link
+    # heatbath followed by 4 link overrelaxation hits: 4 + 30 passes)
+    for L, nor in (((128, 128, 128), 0), ((256, 256, 256), 0), ((128, 128, 128), 4)):
+        key = f"sweep_{L[0]}cubed" + (f"_hb_{nor}or" if nor else "")
         try:
-            lat = Lattice(L, **COUP, precision="f32", seed=11)
+            lat = Lattice(L, **COUP, precision="f32", seed=11, n_link_or=nor)
             lat.init_hot(12)
             lat.sweeps(3, 0)
             timed_sweeps(lat, 3)
@@ -208,8 +211,10 @@ def extras(args, peak):
             prof = kernel_profile(lat, reps=3)
             link = float(np.mean(prof[4:10])) if len(prof) >= 10 else None
             sps = vol(L) * K / (ms / 1e3)
+            bs = B_SWEEP + 6 * nor * B_LINK  # algorithmic bytes per site of this composition
             out[key] = {"site_updates_per_s": sps, "ms_per_sweep": ms / K, "sweep_mode": lat.sweep_mode(),
-                        "sweep_hbm_gbs": sps * B_SWEEP / 1e9, "sweep_frac_of_measured_hbm": sps * B_SWEEP / 1e9 / peak,
+                        "passes": 10 + 6 * nor, "bytes_per_site": bs,
+                        "sweep_hbm_gbs": sps * bs / 1e9, "sweep_frac_of_measured_hbm": sps * bs / 1e9 / peak,
                         "link_kernel_ms": link,
                         "link_kernel_frac_of_measured_hbm": (B_LINK * vol(L) / (link / 1e3) / 1e9 / peak) if link else None}
             lat.close()
@@ -336,7 +341,8 @@ def run_gpu(args):
     peak, peak_src = peaks()
     L = (args.lattice,) * 3 if args.lattice else L_MAIN
     V = vol(L)
-    lat = Lattice(L, **COUP, precision="f32", seed=1000 + rank, device=local, sweep_mode=args.sweep_mode)
+    lat = Lattice(L, **COUP, precision="f32", seed=1000 + rank, device=local, sweep_mode=args.sweep_mode,
+                  n_link_or=args.link_or)
     lat.init_hot(2000 + rank)
     lat.sweeps(20, 0)
     timed_sweeps(lat, args.warmup)
@@ -359,8 +365,12 @@ def run_gpu(args):
     launches = args.steps * ((1 if mode == "persistent" else 11) + 2)
     if args.quick:
         if rank == 0:
+            passes = 4 + 6 * (1 + args.link_or)
+            sweep_bytes = B_HIGGS * 4 + B_LINK * 6 * (1 + args.link_or)
             print(json.dumps({"metric": METRIC, "value": value, "unit": UNIT, "L": list(L), "steps": args.steps,
-                              "ms_per_step": ms_max / args.steps, "sweep_mode": mode, "quick": True}), flush=True)
+                              "ms_per_step": ms_max / args.steps, "sweep_mode": mode, "quick": True,
+                              "link_or": args.link_or, "passes": passes, "bytes_per_site": sweep_bytes,
+                              "frac_of_measured_hbm": value * sweep_bytes / 1e9 / peak}), flush=True)
         lat.close()
         return
 
@@ -535,6 +545,8 @@ def main():
     ap.add_argument("--lattice", type=int, default=0, help="cubic extent for --quick runs (default 64)")
     ap.add_argument("--sweep-mode", default="auto", choices=["auto", "passes", "persistent"],
                     help="sweep form (default: the library's autotuner chooses)")
+    ap.add_argument("--link-or", type=int, default=0, metavar="N",
+                    help="--quick runs: N link overrelaxation hits per sweep after the heatbath")
     ap.add_argument("--quick-gauge-fix", type=int, default=0, metavar="ITERS",
                     help="profiling case: ITERS Fourier-accelerated gauge-fixing iterations on a thermalised "
                          "--lattice^3 FP32 configuration, then exit")
@@ -544,8 +556,9 @@ def main():
         return
     if args.warmup < 3:
         args.warmup = 3
-    if args.lattice and not args.quick:
-        ap.error("--lattice only applies to --quick profiling runs; the headline workload is 64^3")
+    if (args.lattice or args.link_or) and not (args.quick or args.quick_gauge_fix):
+        ap.error("--lattice / --link-or only apply to --quick profiling runs; the headline workload is the "
+                 "standard 64^3 sweep")
     if args.impl == "reference":
         run_reference(args)
     else:

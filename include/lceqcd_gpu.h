@@ -240,7 +240,7 @@ int lce_landau_gauge_from(lce_ctx* ctx, int chain, int start, double* theta_star
  * overrelaxed iteration continues to theta <= limit_or -- the stopping
  * criterion of lce_landau_gauge either way.  step <= 0 selects 1 (a Newton
  * step near the Landau gauge); a step that doubles theta is shortened by 0.7
- * on the device.  Extents must be powers of two up to 512, else
+ * on the device.  Extents must be powers of two up to 1024, else
  * LCE_ERR_UNSUPPORTED.  max_iters caps both phases together. */
 int lce_landau_gauge_fourier(lce_ctx* ctx, int chain, int start, double step, double theta_switch, double* theta,
                              int* iters_fourier, int* iters_plain, int max_iters);

@@ -53,3 +53,17 @@ def effective_mass(corr: np.ndarray) -> np.ndarray:
         if r >= 1.0:
             out[z] = np.arccosh(r)
     return out
+
+
+def jackknife(fn, samples: np.ndarray, nbins: int = 20):
+    """Jackknife mean and error of fn(mean of samples) over nbins contiguous
+    bins (bins long against the autocorrelation time keep the error honest).
+    samples: [n, ...]; returns (estimate, error)."""
+    x = np.asarray(samples, np.float64)
+    n = (x.shape[0] // nbins) * nbins
+    bins = x[:n].reshape((nbins, n // nbins) + x.shape[1:]).mean(axis=1)
+    tot = bins.sum(axis=0)
+    vals = np.array([fn((tot - bins[i]) / (nbins - 1)) for i in range(nbins)])
+    est = fn(tot / nbins)
+    err = np.sqrt((nbins - 1) / nbins * ((vals - vals.mean(axis=0)) ** 2).sum(axis=0))
+    return est, err

@@ -25,9 +25,9 @@
 // (3) forward FFT along y; (4) forward FFT along z, scale, inverse FFT along
 // z; (5) inverse FFT along y; (6) inverse FFT along x + build g; (7) apply g to
 // U_f, A_f and the tracked transform G.  The FFTs are radix-2 in shared
-// memory over a block of lines (512 complex points per block; lines padded by
-// one element against bank conflicts); extents must be powers of two up to
-// 512.  The divergence, g and its application to the fields are FP64 for
+// memory over a block of lines (1024 complex points per block; lines padded
+// by one element against bank conflicts; radix-4 levels); extents must be
+// powers of two up to 1024.  The divergence, g and its application to the fields are FP64 for
 // either field precision (rounding the step's rotation to FP32 before
 // applying it slowed the iteration below theta ~ 1e-8 at 64^3); the
 // transforms themselves are FP32.  Two complex fields carry the three components:
@@ -46,8 +46,8 @@ constexpr int kFaThreads = 256;
 using FftR = float;
 using FftC = float2;
 // complex points per block and field, and the padded shared-memory size
-constexpr int kFaPoints = 512;
-constexpr int kFaLogPoints = 9;
+constexpr int kFaPoints = 1024;
+constexpr int kFaLogPoints = 10;
 static_assert(1 << kFaLogPoints == kFaPoints, "points per block");
 constexpr int kFaSmem = kFaPoints + kFaPoints / 2;
 
@@ -69,23 +69,43 @@ __device__ __forceinline__ void load_twiddles(FftC* tw, const double2* tg, int n
   }
 }
 
-// In-place radix-2 decimation-in-time FFT of nl lines of length n = 2^logn
-// held in shared memory at d[j*(n+1) + k], input in bit-reversed order,
-// output natural.  Ends with __syncthreads.
+// In-place decimation-in-time FFT of nl lines of length n = 2^logn held in
+// shared memory at d[j*(n+1) + k], input in bit-reversed order, output
+// natural.  Levels are fused in pairs (radix 4: two radix-2 levels per item,
+// in registers) after one radix-2 level when logn is odd; tw[k] = exp(sign 2
+// pi i k / n), k < n/2.  Ends with __syncthreads.
 template <typename T>
 __device__ __forceinline__ void fft_lines(T* d, int nl, int logn, const T* tw) {
-  const int n = 1 << logn, hn = n >> 1, ld = n + 1;
-  const int nb = nl * hn;
-  for (int st = 0; st < logn; ++st) {
-    const int half = 1 << st, tws = n >> (st + 1);
+  const int n = 1 << logn, ld = n + 1;
+  int st = 0;
+  if (logn & 1) {
+    // level 0: pairs (2i, 2i+1), twiddle 1
+    const int hn = n >> 1, nb = nl * hn;
     for (int b = threadIdx.x; b < nb; b += blockDim.x) {
-      const int j = b >> (logn - 1), r = b & (hn - 1);
-      const int i = r & (half - 1), grp = r >> st;
-      const int p = j * ld + grp * 2 * half + i, q = p + half;
-      const T t = cmul(tw[i * tws], d[q]);
-      const T u = d[p];
-      d[p] = cadd(u, t);
-      d[q] = csub(u, t);
+      const int p = (b >> (logn - 1)) * ld + 2 * (b & (hn - 1));
+      const T u = d[p], v = d[p + 1];
+      d[p] = cadd(u, v);
+      d[p + 1] = csub(u, v);
+    }
+    __syncthreads();
+    st = 1;
+  }
+  for (; st < logn; st += 2) {
+    // levels st (pairs at distance m) and st + 1 (distance 2m) on groups of 4m
+    const int m = 1 << st, q = n >> 2, nb = nl * q;
+    const int t1 = n >> (st + 1), t2 = n >> (st + 2);
+    for (int b = threadIdx.x; b < nb; b += blockDim.x) {
+      const int r = b & (q - 1), i = r & (m - 1);
+      const int base = (b >> (logn - 2)) * ld + (r >> st) * 4 * m + i;
+      const T a0 = d[base], a1 = d[base + m], a2 = d[base + 2 * m], a3 = d[base + 3 * m];
+      const T w = tw[i * t1];
+      const T wa1 = cmul(w, a1), wa3 = cmul(w, a3);
+      const T b0 = cadd(a0, wa1), b1 = csub(a0, wa1), b2 = cadd(a2, wa3), b3 = csub(a2, wa3);
+      const T x2 = cmul(tw[i * t2], b2), x3 = cmul(tw[(i + m) * t2], b3);
+      d[base] = cadd(b0, x2);
+      d[base + 2 * m] = csub(b0, x2);
+      d[base + m] = cadd(b1, x3);
+      d[base + 3 * m] = csub(b1, x3);
     }
     __syncthreads();
   }

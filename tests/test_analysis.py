@@ -25,3 +25,15 @@ def test_effective_mass_of_cosh():
     z = np.arange(n)
     c = np.cosh(m * (z - n / 2))
     np.testing.assert_allclose(effective_mass(c)[1:n // 2], m, rtol=1e-10)
+
+
+def test_jackknife_mean_error_and_nonlinear_function():
+    import numpy as np
+    from lceqcd_b200.analysis import jackknife
+    rng = np.random.default_rng(1)
+    x = rng.normal(2.0, 1.0, size=(20000, 2))
+    est, err = jackknife(lambda c: c[0], x, nbins=50)
+    assert abs(est - 2.0) < 0.05 and 0.7 * 1 / np.sqrt(20000) < err < 1.3 / np.sqrt(20000)
+    # ratio of means: error by propagation ~ sqrt(2) * sigma / (2 sqrt(n))
+    est, err = jackknife(lambda c: c[0] / c[1], x, nbins=50)
+    assert abs(est - 1.0) < 0.02 and 0.6 * np.sqrt(2) / 2 / np.sqrt(20000) < err < 1.5 * np.sqrt(2) / 2 / np.sqrt(20000)
