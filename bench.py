@@ -386,9 +386,11 @@ def run_gpu(args):
         dom_name = "sweep_persistent_kernel (whole sweep: 4 Higgs + 6 link passes, one cooperative launch)"
     else:
         dom_ms, dom_bytes = link_ms, B_LINK * V
-        dom_name = "link_kernel (agauge pass, one parity x one mu)"
+        dom_name = "link_kernel (agauge pass, one parity x one mu" + (
+            ", two sites per thread)" if mode == "passes2" else ")")
     achieved = dom_bytes / (dom_ms / 1e3) / 1e9
-    traffic = profile_traffic(mode)
+    # the same bytes move whether a thread takes one site or two
+    traffic = profile_traffic("passes" if mode == "passes2" else mode)
 
     # End to end through the C ABI with pinned host buffers.  A step uploads
     # the configuration (the step's input, lce_upload), runs one measured
@@ -543,7 +545,7 @@ def main():
     ap.add_argument("--quick", action="store_true",
                     help="timed sweeps only (no e2e, CPU baseline, extras or clocks): the ncu profiling case")
     ap.add_argument("--lattice", type=int, default=0, help="cubic extent for --quick runs (default 64)")
-    ap.add_argument("--sweep-mode", default="auto", choices=["auto", "passes", "persistent"],
+    ap.add_argument("--sweep-mode", default="auto", choices=["auto", "passes", "passes2", "persistent"],
                     help="sweep form (default: the library's autotuner chooses)")
     ap.add_argument("--link-or", type=int, default=0, metavar="N",
                     help="--quick runs: N link overrelaxation hits per sweep after the heatbath")

@@ -67,11 +67,14 @@ extern "C" {
 #define LCE_GF_ATAN2 1
 
 /* execution form of lce_sweep(s): one kernel per parity pass chained in a
- * CUDA graph, or one cooperative persistent kernel per sweep that loops over
- * the (chain, tile) work list of every pass with a grid barrier in between */
+ * CUDA graph (one site per thread, or two sites per thread: tiles of 512
+ * sites), or one cooperative persistent kernel per sweep that loops over the
+ * (chain, tile) work list of every pass with a grid barrier in between.
+ * AUTO times the forms on the first sweeps and keeps the fastest. */
 #define LCE_SWEEP_AUTO 0
 #define LCE_SWEEP_PASSES 1
 #define LCE_SWEEP_PERSISTENT 2
+#define LCE_SWEEP_PASSES2 3
 
 /* field selectors for upload/download */
 #define LCE_FIELDS 0        /* u, a        (COMMON /linkvar/ u, a) */
@@ -97,9 +100,9 @@ typedef struct lce_params {
   double delta0;         /* initial ahiggs1 step */
   int gf_angle;          /* gauge-fixing rotation angle: LCE_GF_ACOS (the
                             reference, f/or_gauge_fixing1.f:174) or LCE_GF_ATAN2 */
-  int sweep_mode;        /* LCE_SWEEP_AUTO (time both forms on the first sweeps
-                            and keep the faster), LCE_SWEEP_PASSES or
-                            LCE_SWEEP_PERSISTENT */
+  int sweep_mode;        /* LCE_SWEEP_AUTO (time the forms on the first sweeps
+                            and keep the fastest), LCE_SWEEP_PASSES,
+                            LCE_SWEEP_PASSES2 or LCE_SWEEP_PERSISTENT */
   int agauge_hits;       /* link update of lce_sweep: 1 = f/agauge.f (default;
                             0 is read as 1), 3 = f/agauge1.f (three heatbath +
                             Metropolis hits per link) -- the reference selects

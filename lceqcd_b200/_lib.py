@@ -30,6 +30,7 @@ LCE_GF_ATAN2 = 1
 LCE_SWEEP_AUTO = 0
 LCE_SWEEP_PASSES = 1
 LCE_SWEEP_PERSISTENT = 2
+LCE_SWEEP_PASSES2 = 3
 LCE_FIELDS = 0
 LCE_FIELDS_FIXED = 1
 LCE_GF_START_IDENTITY = 0

@@ -43,10 +43,12 @@ struct lce_ctx {
   int agauge_hits = 1;  // 1: f/agauge.f, 3: f/agauge1.f in lce_sweep
   std::vector<lce_params> params;
   std::vector<ChainDev> ch;
-  std::vector<int> blk;  // prefix of blocks per pass
+  std::vector<int> blk;   // prefix of blocks per pass (tiles of kBlock sites)
+  std::vector<int> blk2;  // the same for tiles of 2 * kBlock sites (two per thread)
   int max_nh = 0, max_L3 = 0;
   ChainDev* ch_d = nullptr;
   int* blk_d = nullptr;
+  int* blk2_d = nullptr;
   CtxState* st_d = nullptr;
   ChainState* cst_d = nullptr;
   lce_meas* meas_d = nullptr;
@@ -70,12 +72,13 @@ struct lce_ctx {
   cudaStream_t own = nullptr, stream = nullptr;
   cudaEvent_t ev0 = nullptr, ev1 = nullptr;
   cudaGraphExec_t sweep_exec[2] = {nullptr, nullptr};     // per-pass kernels, per measflag
+  cudaGraphExec_t sweep2_exec[2] = {nullptr, nullptr};    // per-pass kernels, two sites per thread
   cudaGraphExec_t persist_exec[2] = {nullptr, nullptr};   // persistent kernel, per measflag
   GridBar* bar_d = nullptr;
   int persist_grid = 0;
   int sweep_mode = LCE_SWEEP_AUTO;   // requested
   int mode = LCE_SWEEP_AUTO;         // in use (AUTO while tuning)
-  std::vector<float> tune_ms[2];     // autotune samples per form
+  std::vector<float> tune_ms[3];     // autotune samples: passes, persistent, passes x2
   std::map<std::pair<int, int>, cudaGraphExec_t> gf_exec;
   std::string err;
 };
@@ -145,8 +148,8 @@ bool valid_params(const lce_params& p, std::string& why) {
     why = "imode must be 0 or 1";
     return false;
   }
-  if (p.sweep_mode < LCE_SWEEP_AUTO || p.sweep_mode > LCE_SWEEP_PERSISTENT) {
-    why = "sweep_mode must be LCE_SWEEP_AUTO, LCE_SWEEP_PASSES or LCE_SWEEP_PERSISTENT";
+  if (p.sweep_mode < LCE_SWEEP_AUTO || p.sweep_mode > LCE_SWEEP_PASSES2) {
+    why = "sweep_mode must be LCE_SWEEP_AUTO, LCE_SWEEP_PASSES, LCE_SWEEP_PASSES2 or LCE_SWEEP_PERSISTENT";
     return false;
   }
   if (p.gf_angle != LCE_GF_ACOS && p.gf_angle != LCE_GF_ATAN2) {
@@ -213,13 +216,15 @@ void expand(unsigned char kind, std::vector<Pass>& out) {
 // Queue the passes of the given routines and one finalize kernel.
 // events: optional array receiving an event record after every pass.
 int enqueue(lce_ctx* c, const std::vector<unsigned char>& routines, int measflag, bool fuse_renorm,
-            cudaEvent_t* events = nullptr) {
+            cudaEvent_t* events = nullptr, int spt = 1) {
+  const std::vector<int>& blk = spt == 2 ? c->blk2 : c->blk;
+  int* blk_d = spt == 2 ? c->blk2_d : c->blk_d;
   std::vector<Pass> passes;
   for (unsigned char r : routines) expand(r, passes);
   FinalizeArgs f;
   std::memset(&f, 0, sizeof(f));
   f.chains = c->ch_d;
-  f.blk_begin = c->blk_d;
+  f.blk_begin = blk_d;
   f.st = c->st_d;
   f.cst = c->cst_d;
   f.meas = c->meas_d;
@@ -228,7 +233,7 @@ int enqueue(lce_ctx* c, const std::vector<unsigned char>& routines, int measflag
   f.totals = c->totals_d;
   f.nchains = c->nchains;
   f.single = c->prec == LCE_PREC_F32;
-  const int nblocks = c->blk.back();
+  const int nblocks = blk.back();
   unsigned long long soff = 0;
   unsigned int poff = 0;
   int slot = 0;
@@ -238,7 +243,8 @@ int enqueue(lce_ctx* c, const std::vector<unsigned char>& routines, int measflag
     if (reduce && slot >= c->part_slots) return fail(c, LCE_ERR_INVALID, "too many reduction slots");
     PassArgs a;
     a.chains = c->ch_d;
-    a.blk_begin = c->blk_d;
+    a.blk_begin = blk_d;
+    a.spt = spt;
     a.st = c->st_d;
     a.cst = c->cst_d;
     a.part = reduce ? c->part_d + (size_t)slot * c->slot_stride : nullptr;
@@ -293,6 +299,7 @@ int enqueue_persistent(lce_ctx* c, const std::vector<unsigned char>& routines, i
   b.stream_n = c->stream_n;
   b.nchains = c->nchains;
   b.fuse_renorm = fuse_renorm ? 1 : 0;
+  b.spt = 1;
   FinalizeArgs& f = a.fin;
   f.chains = c->ch_d;
   f.blk_begin = c->blk_d;
@@ -339,7 +346,8 @@ constexpr size_t kTuneSamples = 3;
 // form and measflag).  The persistent form falls back to the per-pass form
 // under LCE_SWEEP_AUTO if it cannot be captured on this device.
 int sweep_graph(lce_ctx* c, int form, int mf, cudaGraphExec_t* out) {
-  cudaGraphExec_t* slot = form == LCE_SWEEP_PERSISTENT ? &c->persist_exec[mf] : &c->sweep_exec[mf];
+  cudaGraphExec_t* slot = form == LCE_SWEEP_PERSISTENT ? &c->persist_exec[mf]
+                          : (form == LCE_SWEEP_PASSES2 ? &c->sweep2_exec[mf] : &c->sweep_exec[mf]);
   if (!*slot) {
     cudaGraph_t g;
     CK(cudaStreamBeginCapture(c->stream, cudaStreamCaptureModeThreadLocal));
@@ -348,7 +356,7 @@ int sweep_graph(lce_ctx* c, int form, int mf, cudaGraphExec_t* out) {
       rc = c->prec == LCE_PREC_F64 ? enqueue_persistent<double>(c, sweep_routines(c), mf, true)
                                    : enqueue_persistent<float>(c, sweep_routines(c), mf, true);
     else
-      rc = enqueue(c, sweep_routines(c), mf, true);
+      rc = enqueue(c, sweep_routines(c), mf, true, nullptr, form == LCE_SWEEP_PASSES2 ? 2 : 1);
     const cudaError_t ec = cudaStreamEndCapture(c->stream, &g);
     cudaError_t ei = cudaSuccess;
     if (ec == cudaSuccess) {
@@ -540,6 +548,7 @@ lce_ctx* create_impl(const lce_params* p, int n) {
   size_t off = 0;
   std::vector<size_t> offs;
   c->blk.assign(1, 0);
+  c->blk2.assign(1, 0);
   for (int i = 0; i < n; ++i) {
     ChainDev d;
     std::memset(&d, 0, sizeof(d));
@@ -582,6 +591,7 @@ lce_ctx* create_impl(const lce_params* p, int n) {
     off += 2 * (align256((size_t)6 * d.nh * lb) + align256((size_t)6 * d.nh * rb)) + align256((size_t)2 * d.nh * lb);
     c->ch.push_back(d);
     c->blk.push_back(c->blk.back() + ceil_div(d.nh, kBlock));
+    c->blk2.push_back(c->blk2.back() + ceil_div(d.nh, 2 * kBlock));
     c->max_nh = std::max(c->max_nh, d.nh);
     c->max_L3 = std::max(c->max_L3, d.L3);
   }
@@ -603,6 +613,9 @@ lce_ctx* create_impl(const lce_params* p, int n) {
   if ((e = cudaMalloc(&c->blk_d, sizeof(int) * (n + 1))) != cudaSuccess) return bail(e, "cudaMalloc(blk)");
   if ((e = cudaMemcpy(c->blk_d, c->blk.data(), sizeof(int) * (n + 1), cudaMemcpyHostToDevice)) != cudaSuccess)
     return bail(e, "cudaMemcpy(blk)");
+  if ((e = cudaMalloc(&c->blk2_d, sizeof(int) * (n + 1))) != cudaSuccess) return bail(e, "cudaMalloc(blk2)");
+  if ((e = cudaMemcpy(c->blk2_d, c->blk2.data(), sizeof(int) * (n + 1), cudaMemcpyHostToDevice)) != cudaSuccess)
+    return bail(e, "cudaMemcpy(blk2)");
   if ((e = cudaMalloc(&c->st_d, sizeof(CtxState))) != cudaSuccess) return bail(e, "cudaMalloc(state)");
   if ((e = cudaMemset(c->st_d, 0, sizeof(CtxState))) != cudaSuccess) return bail(e, "cudaMemset(state)");
   if ((e = cudaMalloc(&c->cst_d, sizeof(ChainState) * n)) != cudaSuccess) return bail(e, "cudaMalloc(cstate)");
@@ -860,11 +873,12 @@ void lce_destroy(lce_ctx* c) {
   if (c->stream) cudaStreamSynchronize(c->stream);
   for (int i = 0; i < 2; ++i) {
     if (c->sweep_exec[i]) cudaGraphExecDestroy(c->sweep_exec[i]);
+    if (c->sweep2_exec[i]) cudaGraphExecDestroy(c->sweep2_exec[i]);
     if (c->persist_exec[i]) cudaGraphExecDestroy(c->persist_exec[i]);
   }
   for (auto& kv : c->gf_exec) cudaGraphExecDestroy(kv.second);
   for (auto& kv : c->fa_exec) cudaGraphExecDestroy(kv.second);
-  void* ptrs[] = {c->ch_d, c->blk_d, c->st_d, c->cst_d, c->meas_d, c->part_d, c->totals_d,
+  void* ptrs[] = {c->ch_d, c->blk_d, c->blk2_d, c->st_d, c->cst_d, c->meas_d, c->part_d, c->totals_d,
                   c->scratch_d, c->fields_d, c->stream_d, c->staging_d, c->flush_d, c->bar_d,
                   c->gsave_d, c->fa_d};
   for (void* q : ptrs)
@@ -954,6 +968,10 @@ int lce_set_rng_stream(lce_ctx* c, const double* u, size_t n) {
       cudaGraphExecDestroy(c->sweep_exec[i]);
       c->sweep_exec[i] = nullptr;
     }
+    if (c->sweep2_exec[i]) {
+      cudaGraphExecDestroy(c->sweep2_exec[i]);
+      c->sweep2_exec[i] = nullptr;
+    }
     if (c->persist_exec[i]) {
       cudaGraphExecDestroy(c->persist_exec[i]);
       c->persist_exec[i] = nullptr;
@@ -1034,13 +1052,20 @@ int lce_sweeps(lce_ctx* c, int nsweeps, int measflag) {
   if (!c || nsweeps < 0) return LCE_ERR_INVALID;
   const int mf = measflag == 1 ? 1 : 0;
   int done = 0;
-  // autotune: alternate the two forms on real sweeps, one timed sweep at a
-  // time, until each has kTuneSamples samples; then keep the faster.
+  // autotune: rotate through the forms on real sweeps, one timed sweep at a
+  // time, until each has kTuneSamples samples (after a discarded first one);
+  // then keep the fastest.  Forms: 0 per-pass kernels, 1 persistent kernel
+  // (when it can be resident), 2 per-pass kernels with two sites per thread.
+  const int kForm[3] = {LCE_SWEEP_PASSES, LCE_SWEEP_PERSISTENT, LCE_SWEEP_PASSES2};
+  const int nforms = 3;
   while (c->mode == LCE_SWEEP_AUTO && done < nsweeps) {
-    const int form = (c->tune_ms[0].size() <= c->tune_ms[1].size()) ? 0 : 1;
+    int form = 0;
+    for (int f = 1; f < nforms; ++f)
+      if (c->tune_ms[f].size() < c->tune_ms[form].size()) form = f;
     cudaGraphExec_t ex;
-    int rc = sweep_graph(c, form == 0 ? LCE_SWEEP_PASSES : LCE_SWEEP_PERSISTENT, mf, &ex);
+    int rc = sweep_graph(c, kForm[form], mf, &ex);
     if (rc) return rc;
+    if (c->mode != LCE_SWEEP_AUTO) break;  // the persistent form was unavailable
     CK(cudaEventRecord(c->ev0, c->stream));
     CK(cudaGraphLaunch(ex, c->stream));
     CK(cudaEventRecord(c->ev1, c->stream));
@@ -1049,15 +1074,22 @@ int lce_sweeps(lce_ctx* c, int nsweeps, int measflag) {
     CK(cudaEventElapsedTime(&ms, c->ev0, c->ev1));
     c->tune_ms[form].push_back(ms);
     ++done;
-    if (c->tune_ms[0].size() >= kTuneSamples + 1 && c->tune_ms[1].size() >= kTuneSamples + 1) {
+    bool complete = true;
+    for (int f = 0; f < nforms; ++f) complete = complete && c->tune_ms[f].size() >= kTuneSamples + 1;
+    if (complete) {
       // drop each form's first (instantiation-cold) sample, compare medians
-      float med[2];
-      for (int f = 0; f < 2; ++f) {
+      int best = 0;
+      float best_med = 0;
+      for (int f = 0; f < nforms; ++f) {
         std::vector<float> v(c->tune_ms[f].begin() + 1, c->tune_ms[f].end());
         std::sort(v.begin(), v.end());
-        med[f] = v[v.size() / 2];
+        const float med = v[v.size() / 2];
+        if (f == 0 || med < best_med) {
+          best = f;
+          best_med = med;
+        }
       }
-      c->mode = med[1] < med[0] ? LCE_SWEEP_PERSISTENT : LCE_SWEEP_PASSES;
+      c->mode = kForm[best];
     }
   }
   if (done < nsweeps) {
@@ -1453,7 +1485,7 @@ int lce_profile_sweep(lce_ctx* c, int measflag, float* ms, int max_passes) {
   std::vector<cudaEvent_t> ev(np + 1);
   for (auto& e : ev) CK(cudaEventCreate(&e));
   CK(cudaEventRecord(ev[0], c->stream));
-  int rc = enqueue(c, r, measflag == 1 ? 1 : 0, true, ev.data() + 1);
+  int rc = enqueue(c, r, measflag == 1 ? 1 : 0, true, ev.data() + 1, c->mode == LCE_SWEEP_PASSES2 ? 2 : 1);
   if (rc == LCE_OK) {
     CK(cudaStreamSynchronize(c->stream));
     for (int i = 0; i < np && i < max_passes; ++i) CK(cudaEventElapsedTime(&ms[i], ev[i], ev[i + 1]));

@@ -113,6 +113,7 @@ struct PassArgs {
   int nchains;
   int eo;
   int fuse_renorm;
+  int spt;                // sites per thread (a tile is kBlock * spt sites)
 };
 
 struct FinalizeArgs {

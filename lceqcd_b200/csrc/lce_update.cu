@@ -168,19 +168,25 @@ __device__ __forceinline__ bool setup_uniforms(const PassArgs& p, const ChainDev
 // ------------------------------------------------------------------ Higgs
 // One tile (kBlock consecutive sites of one chain) of a Higgs pass.  PDL:
 // trigger dependents and wait for the previous kernel (per-pass form only).
-template <typename R, int MODE, bool PDL>
+template <typename R, int MODE, bool PDL, int SPT = 1>
 __device__ __forceinline__ void higgs_tile(const PassArgs& p, int tile) {
   if (PDL) pdl_trigger();
   // the chain table is written once at context creation: safe before pdl_wait
   const int c = p.nchains > 1 ? find_chain(p.blk_begin, p.nchains, tile) : 0;
   const ChainDev& ch = p.chains[c];
-  const int s = (tile - __ldg(p.blk_begin + c)) * kBlock + threadIdx.x;
+  // a tile is kBlock * SPT consecutive sites; thread t takes t, t + kBlock, ...
+  const int s0 = (tile - __ldg(p.blk_begin + c)) * kBlock * SPT + threadIdx.x;
   const int eo = p.eo, nh = ch.nh;
-  const Coord X = site_coord(eo, s < nh ? s : 0, ch.hx, ch.nxy, ch.dhx, ch.dnxy);
+  const Coord X0 = site_coord(eo, s0 < nh ? s0 : 0, ch.hx, ch.nxy, ch.dhx, ch.dnxy);
   unsigned acc[1] = {0u};
   double q[3] = {0.0, 0.0, 0.0};
   if (PDL) pdl_wait();
-  if (s < nh) {
+#pragma unroll 1
+  for (int r = 0; r < SPT; ++r) {
+  const int s = s0 + r * kBlock;
+  if (s >= nh) break;
+  const Coord X = r == 0 ? X0 : site_coord(eo, s, ch.hx, ch.nxy, ch.dhx, ch.dnxy);
+  {
     constexpr int NS = MODE == 0 ? 7 : (MODE == 1 ? 1 : 4);
     const int layout = MODE == 2 ? kTriple : kPlanar;
     Uniforms<R, NS> Un;
@@ -256,15 +262,16 @@ __device__ __forceinline__ void higgs_tile(const PassArgs& p, int tile) {
         }
         rho_o = rho_n;
         sf_o = sf_n;
-        acc[0] = 1u;
+        acc[0] += 1u;
       }
       if (p.part) {
-        q[0] = (double)rho_o;
-        q[1] = (double)rho_o * (double)rho_o;
-        if (MODE == 2) q[2] = (double)sf_o;
-        else q[2] = (double)ao[0] * f[0] + (double)ao[1] * f[1] + (double)ao[2] * f[2];
+        q[0] += (double)rho_o;
+        q[1] += (double)rho_o * (double)rho_o;
+        if (MODE == 2) q[2] += (double)sf_o;
+        else q[2] += (double)ao[0] * f[0] + (double)ao[1] * f[1] + (double)ao[2] * f[2];
       }
     }
+  }
   }
   // partials {accepted, sum rho, sum rho^2, sum a.F}
   if (p.part) block_reduce_cs<1, 3, kNQ>(acc, q, p.part + (size_t)tile * kNQ);
@@ -274,18 +281,24 @@ __device__ __forceinline__ void higgs_tile(const PassArgs& p, int tile) {
 // NHIT = 3 is f/agauge1.f: the staple is built once and the heatbath +
 // Metropolis hit is repeated on the updated link, each hit with its own
 // uniforms (f/agauge1.f:95-198).
-template <typename R, int MU, int OR, bool PDL, int NHIT = 1>
+template <typename R, int MU, int OR, bool PDL, int NHIT = 1, int SPT = 1>
 __device__ __forceinline__ void link_tile(const PassArgs& p, int tile) {
   if (PDL) pdl_trigger();
   const int c = p.nchains > 1 ? find_chain(p.blk_begin, p.nchains, tile) : 0;
   const ChainDev& ch = p.chains[c];
-  const int s = (tile - __ldg(p.blk_begin + c)) * kBlock + threadIdx.x;
+  // a tile is kBlock * SPT consecutive sites; thread t takes t, t + kBlock, ...
+  const int s0 = (tile - __ldg(p.blk_begin + c)) * kBlock * SPT + threadIdx.x;
   const int eo = p.eo, oe = 1 - eo, nh = ch.nh;
-  const Coord X = site_coord(eo, s < nh ? s : 0, ch.hx, ch.nxy, ch.dhx, ch.dnxy);
+  const Coord X0 = site_coord(eo, s0 < nh ? s0 : 0, ch.hx, ch.nxy, ch.dhx, ch.dnxy);
   unsigned cnt[2] = {0u, 0u};
   double pl[1] = {0.0};
   if (PDL) pdl_wait();
-  if (s < nh) {
+#pragma unroll 1
+  for (int r = 0; r < SPT; ++r) {
+  const int s = s0 + r * kBlock;
+  if (s >= nh) break;
+  const Coord X = r == 0 ? X0 : site_coord(eo, s, ch.hx, ch.nxy, ch.dhx, ch.dnxy);
+  {
     Uniforms<R, OR ? 1 : 7> Un;
     if (setup_uniforms<R, OR ? 1 : 7>(p, ch, s, OR ? kPlanar : kTriple, Un)) {
       const su2<R> V = staple<R, MU, PDL>(ch, eo, X, s);
@@ -344,8 +357,9 @@ __device__ __forceinline__ void link_tile(const PassArgs& p, int tile) {
       }
       if (changed) LinkIO<R>::st(ch.u, li, p.fuse_renorm ? unitarise64(uo) : uo);
       // f/agauge.f:179-185 plaquette against the staple
-      if (!OR && p.part) pl[0] = (double)nn(uo, V).a.re;
+      if (!OR && p.part) pl[0] += (double)nn(uo, V).a.re;
     }
+  }
   }
   // partials {KP accepted, Metropolis accepted, sum plaquette} / {OR accepted}
   if (p.part) {
@@ -358,20 +372,21 @@ __device__ __forceinline__ void link_tile(const PassArgs& p, int tile) {
   }
 }
 
-template <typename R, int MODE>
+// SPT = sites per thread (1, or 2 for the LCE_SWEEP_PASSES2 form)
+template <typename R, int MODE, int SPT>
 __global__ void __launch_bounds__(kBlock, min_blocks<R>()) higgs_kernel(PassArgs p) {
-  higgs_tile<R, MODE, true>(p, blockIdx.x);
+  higgs_tile<R, MODE, true, SPT>(p, blockIdx.x);
 }
 
-template <typename R, int MU, int OR>
+template <typename R, int MU, int OR, int SPT>
 __global__ void __launch_bounds__(kBlock, min_blocks<R>()) link_kernel(PassArgs p) {
-  link_tile<R, MU, OR, true>(p, blockIdx.x);
+  link_tile<R, MU, OR, true, 1, SPT>(p, blockIdx.x);
 }
 
 // f/agauge1.f (3 hits)
-template <typename R, int MU>
+template <typename R, int MU, int SPT>
 __global__ void __launch_bounds__(kBlock, min_blocks<R>()) link3_kernel(PassArgs p) {
-  link_tile<R, MU, 0, true, 3>(p, blockIdx.x);
+  link_tile<R, MU, 0, true, 3, SPT>(p, blockIdx.x);
 }
 
 // ------------------------------------------------------------------ finalize
@@ -622,19 +637,35 @@ __global__ void debug_force_kernel(const ChainDev* chp, int eo, double* out) {
 // ------------------------------------------------------------------ launchers
 // The pass kernels and the finalize kernel are launched with programmatic
 // dependent launch (lce_common.cuh: launch_pdl / pdl_wait).
-template <typename R>
-void launch_higgs(int mode, const PassArgs& a, int nblocks, cudaStream_t s) {
-  void (*k)(PassArgs) = mode == 0 ? higgs_kernel<R, 0> : (mode == 1 ? higgs_kernel<R, 1> : higgs_kernel<R, 2>);
+template <typename R, int SPT>
+void launch_higgs_t(int mode, const PassArgs& a, int nblocks, cudaStream_t s) {
+  void (*k)(PassArgs) =
+      mode == 0 ? higgs_kernel<R, 0, SPT> : (mode == 1 ? higgs_kernel<R, 1, SPT> : higgs_kernel<R, 2, SPT>);
+  (void)launch_pdl(k, nblocks, kBlock, 0, s, a);
+}
+
+template <typename R, int SPT>
+void launch_link_t(int mode, int mu, const PassArgs& a, int nblocks, cudaStream_t s) {
+  void (*k)(PassArgs);
+  if (mode == 0)
+    k = mu == 0 ? link_kernel<R, 0, 0, SPT> : (mu == 1 ? link_kernel<R, 1, 0, SPT> : link_kernel<R, 2, 0, SPT>);
+  else if (mode == 1)
+    k = mu == 0 ? link_kernel<R, 0, 1, SPT> : (mu == 1 ? link_kernel<R, 1, 1, SPT> : link_kernel<R, 2, 1, SPT>);
+  else
+    k = mu == 0 ? link3_kernel<R, 0, SPT> : (mu == 1 ? link3_kernel<R, 1, SPT> : link3_kernel<R, 2, SPT>);
   (void)launch_pdl(k, nblocks, kBlock, 0, s, a);
 }
 
 template <typename R>
+void launch_higgs(int mode, const PassArgs& a, int nblocks, cudaStream_t s) {
+  if (a.spt == 2) launch_higgs_t<R, 2>(mode, a, nblocks, s);
+  else launch_higgs_t<R, 1>(mode, a, nblocks, s);
+}
+
+template <typename R>
 void launch_link(int mode, int mu, const PassArgs& a, int nblocks, cudaStream_t s) {
-  void (*k)(PassArgs);
-  if (mode == 0) k = mu == 0 ? link_kernel<R, 0, 0> : (mu == 1 ? link_kernel<R, 1, 0> : link_kernel<R, 2, 0>);
-  else if (mode == 1) k = mu == 0 ? link_kernel<R, 0, 1> : (mu == 1 ? link_kernel<R, 1, 1> : link_kernel<R, 2, 1>);
-  else k = mu == 0 ? link3_kernel<R, 0> : (mu == 1 ? link3_kernel<R, 1> : link3_kernel<R, 2>);
-  (void)launch_pdl(k, nblocks, kBlock, 0, s, a);
+  if (a.spt == 2) launch_link_t<R, 2>(mode, mu, a, nblocks, s);
+  else launch_link_t<R, 1>(mode, mu, a, nblocks, s);
 }
 
 void launch_finalize(const FinalizeArgs& f, cudaStream_t s) {
