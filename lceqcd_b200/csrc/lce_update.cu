@@ -183,10 +183,9 @@ __device__ __forceinline__ void higgs_tile(const PassArgs& p, int tile) {
   if (PDL) pdl_wait();
 #pragma unroll 1
   for (int r = 0; r < SPT; ++r) {
-  const int s = s0 + r * kBlock;
-  if (s >= nh) break;
-  const Coord X = r == 0 ? X0 : site_coord(eo, s, ch.hx, ch.nxy, ch.dhx, ch.dnxy);
-  {
+    const int s = s0 + r * kBlock;
+    if (s >= nh) break;
+    const Coord X = r == 0 ? X0 : site_coord(eo, s, ch.hx, ch.nxy, ch.dhx, ch.dnxy);
     constexpr int NS = MODE == 0 ? 7 : (MODE == 1 ? 1 : 4);
     const int layout = MODE == 2 ? kTriple : kPlanar;
     Uniforms<R, NS> Un;
@@ -272,7 +271,6 @@ __device__ __forceinline__ void higgs_tile(const PassArgs& p, int tile) {
       }
     }
   }
-  }
   // partials {accepted, sum rho, sum rho^2, sum a.F}
   if (p.part) block_reduce_cs<1, 3, kNQ>(acc, q, p.part + (size_t)tile * kNQ);
 }
@@ -295,10 +293,9 @@ __device__ __forceinline__ void link_tile(const PassArgs& p, int tile) {
   if (PDL) pdl_wait();
 #pragma unroll 1
   for (int r = 0; r < SPT; ++r) {
-  const int s = s0 + r * kBlock;
-  if (s >= nh) break;
-  const Coord X = r == 0 ? X0 : site_coord(eo, s, ch.hx, ch.nxy, ch.dhx, ch.dnxy);
-  {
+    const int s = s0 + r * kBlock;
+    if (s >= nh) break;
+    const Coord X = r == 0 ? X0 : site_coord(eo, s, ch.hx, ch.nxy, ch.dhx, ch.dnxy);
     Uniforms<R, OR ? 1 : 7> Un;
     if (setup_uniforms<R, OR ? 1 : 7>(p, ch, s, OR ? kPlanar : kTriple, Un)) {
       const su2<R> V = staple<R, MU, PDL>(ch, eo, X, s);
@@ -359,7 +356,6 @@ __device__ __forceinline__ void link_tile(const PassArgs& p, int tile) {
       // f/agauge.f:179-185 plaquette against the staple
       if (!OR && p.part) pl[0] += (double)nn(uo, V).a.re;
     }
-  }
   }
   // partials {KP accepted, Metropolis accepted, sum plaquette} / {OR accepted}
   if (p.part) {
