@@ -1246,6 +1246,10 @@ int lce_landau_gauge_warm(lce_ctx* c, int chain, lce_net* net, int flags, int* s
     if ((rc = net_record(net, ch, c->gsave_d, f64, c->stream))) return fail(c, rc, "record training pair");
     CK(cudaStreamSynchronize(c->stream));
   }
+  if (rc == LCE_OK && use_net) {
+    CK(cudaStreamSynchronize(c->stream));
+    if ((rc = net_status(net))) return fail(c, rc, lce_last_error(nullptr));
+  }
   return rc;
 }
 

@@ -214,6 +214,8 @@ inline int ceil_div(long a, long b) { return (int)((a + b - 1) / b); }
 
 // ---- learned warm start (lce_net.cu); all work on stream s
 int net_device(lce_net* n);
+// LCE_OK, or an error if a tensor-core kernel of the network gave up waiting
+int net_status(lce_net* n);
 // network input from the chain's U_f, A_f
 int net_features(lce_net* n, const ChainDev* chd, const ChainDev& ch, bool f64, cudaStream_t s);
 void net_predict(lce_net* n, const ChainDev& ch, cudaStream_t s);

@@ -137,6 +137,189 @@ __global__ void __launch_bounds__(32 * kConvWarps) conv_kernel(const __nv_bfloat
   }
 }
 
+// ------------------------------------------------------------------ tcgen05 path
+// The same convolution on the 5th-generation tensor cores when L1 is a
+// multiple of 128: a CTA of 128 threads computes the 16 output channels of
+// 128 consecutive sites of one x-line.  It stages, for each of the 9 (dy, dz)
+// neighbour lines, the 130 input rows x0-1 .. x0+128 (periodic) in shared
+// memory as two "channel planes" (channels 0-7 and 8-15, 16 B per row), so
+// that the A operand of offset (dx, dy, dz) -- 128 sites x 16 channels -- is
+// the canonical K-major layout without swizzle (8-row core matrices of 16 B
+// rows, stride 128 B; the second K chunk one plane further) starting dx + 1
+// rows into its segment.  The weights of the 27 offsets sit in the same
+// layout.  One thread issues the 27 tcgen05.mma (M 128, N 16, K 16, BF16 in,
+// FP32 accumulate in tensor memory), commits them to an mbarrier, and after
+// the (bounded) wait each warp reads its 32 rows out of tensor memory for the
+// epilogue.
+constexpr int kTcRows = 136;                         // staged rows per plane (130 used)
+constexpr int kTcActBytes = 18 * kTcRows * 16;        // 9 segments x 2 planes
+constexpr int kTcWtBytes = kK * 2 * kC * 16;          // 27 offsets x 2 planes x 16 rows
+constexpr int kTcSmem = kTcActBytes + kTcWtBytes + 16;
+constexpr unsigned kTcSpin = 1u << 24;                // mbarrier polls before giving up
+
+// tcgen05.mma instruction descriptor: BF16 A and B (K-major), FP32 D, M 128, N 16
+constexpr uint32_t kTcIdesc = (1u << 4) | (1u << 7) | (1u << 10) | ((16u >> 3) << 17) | ((128u >> 4) << 24);
+
+// shared-memory matrix descriptor, no swizzle: start address, leading-dimension
+// byte offset (between the two K chunks), stride-dimension byte offset
+// (between 8-row core matrices), all in 16 B units; version 1
+__device__ __forceinline__ uint64_t tc_desc(uint32_t addr, uint32_t lbo, uint32_t sbo) {
+  return (uint64_t)((addr >> 4) & 0x3FFF) | ((uint64_t)((lbo >> 4) & 0x3FFF) << 16) |
+         ((uint64_t)((sbo >> 4) & 0x3FFF) << 32) | (1ull << 46);
+}
+
+__device__ __forceinline__ uint32_t smem_u32(const void* p) { return (uint32_t)__cvta_generic_to_shared(p); }
+
+__device__ __forceinline__ bool tc_try_wait(uint32_t mbar, uint32_t phase) {
+  uint32_t ok;
+  asm volatile(
+      "{\n\t.reg .pred P1;\n\t"
+      "mbarrier.try_wait.parity.shared::cta.b64 P1, [%1], %2;\n\t"
+      "selp.b32 %0, 1, 0, P1;\n\t}"
+      : "=r"(ok)
+      : "r"(mbar), "r"(phase)
+      : "memory");
+  return ok != 0;
+}
+
+__device__ __forceinline__ bool tc_wait(uint32_t mbar, uint32_t phase) {
+  for (unsigned i = 0; i < kTcSpin; ++i)
+    if (tc_try_wait(mbar, phase)) return true;
+  return false;
+}
+
+// flat (parity-split) index of site (x, y, z), coordinates in range
+__device__ __forceinline__ int tc_flat(const NetGeom& g, int x, int y, int z) {
+  return ((x + y + z) & 1) * g.nh + site_index(x, y, z, g.hx, g.nxy);
+}
+
+template <int MODE>
+__global__ void __launch_bounds__(128) conv_tc_kernel(const __nv_bfloat16* __restrict__ in,
+                                                      const __nv_bfloat16* __restrict__ W,
+                                                      const float* __restrict__ bias,
+                                                      __nv_bfloat16* __restrict__ out16, float* __restrict__ out32,
+                                                      const __nv_bfloat16* __restrict__ mask_src, NetGeom g,
+                                                      unsigned* status) {
+  extern __shared__ __align__(1024) uint8_t tc_sm[];
+  uint8_t* act = tc_sm;
+  uint8_t* wts = tc_sm + kTcActBytes;
+  uint64_t* mbar = reinterpret_cast<uint64_t*>(wts + kTcWtBytes);
+  uint32_t* tslot = reinterpret_cast<uint32_t*>(mbar + 1);
+  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+  const int segs = g.L1 >> 7;
+  int t = blockIdx.x;
+  const int x0 = (t % segs) << 7;
+  t /= segs;
+  const int y = t % g.L2, z = t / g.L2;
+
+  if (warp == 0) {
+    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(tslot)), "r"(32)
+                 : "memory");
+    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+  }
+  if (tid == 0) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(mbar)), "r"(1) : "memory");
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+  }
+
+  // weights: plane (k, c), row o holds inputs 8c .. 8c+7 of output o
+  const uint4* W4 = reinterpret_cast<const uint4*>(W);
+  for (int e = tid; e < kK * kC * 2; e += blockDim.x) {
+    const int k = e >> 5, o = (e >> 1) & 15, c = e & 1;
+    reinterpret_cast<uint4*>(wts)[(k * 2 + c) * kC + o] = __ldg(W4 + (k * kC + o) * 2 + c);
+  }
+  // activations: segment (dy, dz), plane c, row r = input site x0 - 1 + r
+  const uint4* in4 = reinterpret_cast<const uint4*>(in);
+  for (int e = tid; e < 9 * 130; e += blockDim.x) {
+    const int seg = e / 130, r = e - seg * 130;
+    const int yy = wrap(y + seg / 3 - 1, g.L2), zz = wrap(z + seg % 3 - 1, g.L3);
+    const int xx = wrap(x0 - 1 + r, g.L1);
+    const int f = tc_flat(g, xx, yy, zz);
+    reinterpret_cast<uint4*>(act)[(seg * 2) * kTcRows + r] = __ldg(in4 + (size_t)f * 2);
+    reinterpret_cast<uint4*>(act)[(seg * 2 + 1) * kTcRows + r] = __ldg(in4 + (size_t)f * 2 + 1);
+  }
+  // generic-proxy shared-memory writes -> visible to the tensor core (async proxy)
+  asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+  asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+  __syncthreads();
+  asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+  const uint32_t tmem = *tslot;
+
+  if (tid == 0) {
+    const uint32_t a0 = smem_u32(act), b0 = smem_u32(wts);
+#pragma unroll 1
+    for (int k = 0; k < kK; ++k) {
+      const int dx = k / 9 - 1, seg = k % 9;
+      const uint64_t ad = tc_desc(a0 + ((seg * 2) * kTcRows + dx + 1) * 16, kTcRows * 16, 128);
+      const uint64_t bd = tc_desc(b0 + (k * 2 * kC) * 16, kC * 16, 128);
+      const uint32_t acc = k > 0 ? 1u : 0u;
+      asm volatile(
+          "{\n\t.reg .pred p;\n\t"
+          "setp.ne.b32 p, %4, 0;\n\t"
+          "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n\t}"
+          ::"r"(tmem), "l"(ad), "l"(bd), "r"(kTcIdesc), "r"(acc)
+          : "memory");
+    }
+    asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(smem_u32(mbar))
+                 : "memory");
+  }
+  const bool done = tc_wait(smem_u32(mbar), 0);
+  if (!done) {
+    // record the failure, give the MMAs a second bounded wait, then clean up
+    if (lane == 0) atomicOr(status, 1u);
+    tc_wait(smem_u32(mbar), 0);
+  }
+  asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+  uint32_t v[16];
+  asm volatile(
+      "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, %13, %14, %15}, "
+      "[%16];"
+      : "=r"(v[0]), "=r"(v[1]), "=r"(v[2]), "=r"(v[3]), "=r"(v[4]), "=r"(v[5]), "=r"(v[6]), "=r"(v[7]), "=r"(v[8]),
+        "=r"(v[9]), "=r"(v[10]), "=r"(v[11]), "=r"(v[12]), "=r"(v[13]), "=r"(v[14]), "=r"(v[15])
+      : "r"(tmem + ((uint32_t)(warp * 32) << 16)));
+  asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+
+  if (done) {
+    const int f = tc_flat(g, x0 + tid, y, z);  // row tid = warp*32 + lane: site x0 + tid
+    float o[kC];
+#pragma unroll
+    for (int c = 0; c < kC; ++c) o[c] = __uint_as_float(v[c]) + (MODE != 2 ? bias[c] : 0.f);
+    if (MODE == 1) {
+      float4* d = reinterpret_cast<float4*>(out32 + (size_t)f * 8);
+      d[0] = make_float4(o[0], o[1], o[2], o[3]);
+      d[1] = make_float4(o[4], o[5], o[6], o[7]);
+    } else {
+      if (MODE == 0) {
+#pragma unroll
+        for (int c = 0; c < kC; ++c) o[c] = fmaxf(o[c], 0.f);
+      } else {
+        const __nv_bfloat16* m = mask_src + (size_t)f * kC;
+#pragma unroll
+        for (int c = 0; c < kC; ++c)
+          if (!(__bfloat162float(m[c]) > 0.f)) o[c] = 0.f;
+      }
+      uint4 w0, w1;
+      w0.x = pack2(__float2bfloat16_rn(o[0]), __float2bfloat16_rn(o[1]));
+      w0.y = pack2(__float2bfloat16_rn(o[2]), __float2bfloat16_rn(o[3]));
+      w0.z = pack2(__float2bfloat16_rn(o[4]), __float2bfloat16_rn(o[5]));
+      w0.w = pack2(__float2bfloat16_rn(o[6]), __float2bfloat16_rn(o[7]));
+      w1.x = pack2(__float2bfloat16_rn(o[8]), __float2bfloat16_rn(o[9]));
+      w1.y = pack2(__float2bfloat16_rn(o[10]), __float2bfloat16_rn(o[11]));
+      w1.z = pack2(__float2bfloat16_rn(o[12]), __float2bfloat16_rn(o[13]));
+      w1.w = pack2(__float2bfloat16_rn(o[14]), __float2bfloat16_rn(o[15]));
+      uint4* d = reinterpret_cast<uint4*>(out16) + (size_t)f * 2;
+      d[0] = w0;
+      d[1] = w1;
+    }
+  }
+  asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+  __syncthreads();
+  if (warp == 0) {
+    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(32) : "memory");
+  }
+}
+
 // partial[k][chunk][co][ci] = sum over the chunk's sites of gz[i][co] x[nbr_k(i)][ci]
 __global__ void __launch_bounds__(128) wgrad_kernel(const __nv_bfloat16* __restrict__ gz,
                                                     const __nv_bfloat16* __restrict__ x, float* __restrict__ part,
@@ -352,6 +535,7 @@ struct lce_net {
   double* part = nullptr;
   float* wpart = nullptr;
   int nchunk = 0;
+  unsigned* flag = nullptr;  // set on the device when a tensor-core wait gave up
   // recorded training pairs
   struct Pair {
     NetGeom g;
@@ -409,16 +593,30 @@ int conv_grid(long nsites) {
 }
 
 // forward through all layers from act[0]; output in n->out
+// one convolution: the tcgen05 kernel when L1 is a multiple of 128, else the
+// mma.sync kernel
+template <int MODE>
+void launch_conv(lce_net* n, const __nv_bfloat16* in, const __nv_bfloat16* W, const float* bias,
+                 __nv_bfloat16* out16, float* out32, const __nv_bfloat16* mask, const NetGeom& g, cudaStream_t s) {
+  if (g.L1 % 128 == 0) {
+    static bool attr = false;  // per MODE instantiation
+    if (!attr) {
+      cudaFuncSetAttribute(conv_tc_kernel<MODE>, cudaFuncAttributeMaxDynamicSharedMemorySize, kTcSmem);
+      attr = true;
+    }
+    const int grid = (g.L1 / 128) * g.L2 * g.L3;
+    conv_tc_kernel<MODE><<<grid, 128, kTcSmem, s>>>(in, W, bias, out16, out32, mask, g, n->flag);
+  } else {
+    conv_kernel<MODE><<<conv_grid(2L * g.nh), 32 * kConvWarps, 0, s>>>(in, W, bias, out16, out32, mask, g);
+  }
+}
+
 void net_forward(lce_net* n, const NetGeom& g, cudaStream_t s) {
-  const long ns = 2L * g.nh;
-  const int grid = conv_grid(ns);
   for (int l = 0; l < kLayers; ++l) {
     const __nv_bfloat16* W = n->w16 + (size_t)l * kWl;
     const float* b = n->w32 + (size_t)l * kPl + kWl;
-    if (l < kLayers - 1)
-      conv_kernel<0><<<grid, 32 * kConvWarps, 0, s>>>(n->act[l], W, b, n->act[l + 1], nullptr, nullptr, g);
-    else
-      conv_kernel<1><<<grid, 32 * kConvWarps, 0, s>>>(n->act[l], W, b, nullptr, n->out, nullptr, g);
+    if (l < kLayers - 1) launch_conv<0>(n, n->act[l], W, b, n->act[l + 1], nullptr, nullptr, g, s);
+    else launch_conv<1>(n, n->act[l], W, b, nullptr, n->out, nullptr, g, s);
   }
 }
 
@@ -426,7 +624,6 @@ void net_forward(lce_net* n, const NetGeom& g, cudaStream_t s) {
 // loss through part (device) -- caller sums
 void net_backward(lce_net* n, const NetGeom& g, cudaStream_t s) {
   const long ns = 2L * g.nh;
-  const int grid = conv_grid(ns);
   loss_kernel<<<ceil_div(ns, 256), 256, 0, s>>>(n->out, n->target, (int)ns, n->gz, n->part);
   __nv_bfloat16* gz = n->gz;   // gradient at the output of layer l (pre-activation)
   __nv_bfloat16* gy = n->gy;
@@ -436,8 +633,7 @@ void net_backward(lce_net* n, const NetGeom& g, cudaStream_t s) {
     wgrad_sum_kernel<<<kK + 1, kC * kC, 0, s>>>(n->wpart, n->nchunk, gW);
     if (l > 0) {
       // gradient w.r.t. act[l] = conv_T(gz, W_l), times relu'(layer l-1) = (act[l] > 0)
-      conv_kernel<2><<<grid, 32 * kConvWarps, 0, s>>>(gz, n->wt16 + (size_t)l * kWl, nullptr, gy, nullptr,
-                                                       n->act[l], g);
+      launch_conv<2>(n, gz, n->wt16 + (size_t)l * kWl, nullptr, gy, nullptr, n->act[l], g, s);
       __nv_bfloat16* t = gz;
       gz = gy;
       gy = t;
@@ -446,6 +642,21 @@ void net_backward(lce_net* n, const NetGeom& g, cudaStream_t s) {
 }
 
 void net_refresh(lce_net* n, cudaStream_t s) { refresh_kernel<<<kLayers, 256, 0, s>>>(n->w32, n->w16, n->wt16); }
+
+}  // namespace
+
+// the device flag of the tensor-core kernels (a wait that gave up), read and
+// cleared; the work of the network's stream and of the caller's stream must
+// have completed
+int lce::net_status(lce_net* n) {
+  unsigned f = 0;
+  NCK(cudaMemcpy(&f, n->flag, sizeof(f), cudaMemcpyDeviceToHost));
+  if (!f) return LCE_OK;
+  NCK(cudaMemset(n->flag, 0, sizeof(unsigned)));
+  return net_fail(n, LCE_ERR_CUDA, "warm-start network: a tensor-core completion wait timed out");
+}
+
+namespace {
 
 }  // namespace
 
@@ -468,6 +679,8 @@ lce_net* lce_net_create(int device, unsigned long long seed) {
   if ((e = cudaMalloc(&n->grad, sizeof(float) * kNParam)) != cudaSuccess) return bad(e, "cudaMalloc");
   if ((e = cudaMalloc(&n->w16, sizeof(__nv_bfloat16) * kLayers * kWl)) != cudaSuccess) return bad(e, "cudaMalloc");
   if ((e = cudaMalloc(&n->wt16, sizeof(__nv_bfloat16) * kLayers * kWl)) != cudaSuccess) return bad(e, "cudaMalloc");
+  if ((e = cudaMalloc(&n->flag, sizeof(unsigned))) != cudaSuccess) return bad(e, "cudaMalloc");
+  cudaMemsetAsync(n->flag, 0, sizeof(unsigned), n->stream);
   cudaMemsetAsync(n->m, 0, sizeof(float) * kNParam, n->stream);
   cudaMemsetAsync(n->v, 0, sizeof(float) * kNParam, n->stream);
   init_params_kernel<<<64, 256, 0, n->stream>>>(n->w32, (uint32_t)seed, (uint32_t)(seed >> 32));
@@ -486,7 +699,8 @@ void lce_net_destroy(lce_net* n) {
   }
   for (auto& a : n->act)
     if (a) cudaFree(a);
-  void* ptrs[] = {n->w32, n->m, n->v, n->grad, n->w16, n->wt16, n->gz, n->gy, n->out, n->target, n->part, n->wpart};
+  void* ptrs[] = {n->w32, n->m, n->v, n->grad, n->w16, n->wt16, n->gz, n->gy, n->out, n->target, n->part, n->wpart,
+                  n->flag};
   for (void* q : ptrs)
     if (q) cudaFree(q);
   if (n->stream) cudaStreamDestroy(n->stream);
@@ -566,6 +780,7 @@ int lce_net_eval(lce_net* n, int L1, int L2, int L3, const float* feat, const fl
   double l = 0;
   for (double x : lp) l += x;
   if (loss) *loss = l / ns;
+  if (int rc = lce::net_status(n)) return rc;
   return LCE_OK;
 }
 
@@ -619,6 +834,7 @@ int lce_net_train(lce_net* n, int epochs, double lr, double* mean_loss) {
     last_epoch = tot / order.size();
   }
   if (mean_loss) *mean_loss = last_epoch;
+  if (int rc = lce::net_status(n)) return rc;
   return LCE_OK;
 }
 

@@ -30,7 +30,9 @@ def _problem(L, seed):
     return feat, t.astype(np.float32)
 
 
-@pytest.mark.parametrize("L", [(4, 4, 6), (8, 6, 4), (6, 10, 8)])
+# extents with L1 a multiple of 128 run the convolutions on tcgen05 (tensor
+# memory accumulators), the others on mma.sync
+@pytest.mark.parametrize("L", [(4, 4, 6), (8, 6, 4), (6, 10, 8), (128, 4, 2), (256, 2, 4), (128, 6, 6)])
 def test_forward_loss_gradient_match_fp64_reference(L):
     from lceqcd_b200 import GaugeNet
     net = GaugeNet(seed=1)
