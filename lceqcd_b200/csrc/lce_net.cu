@@ -12,7 +12,10 @@
 // the loss 1 - Omega . T per site.
 //
 // Arithmetic: BF16 weights and activations, FP32 accumulation, on the tensor
-// cores through mma.sync.m16n8k16 (bf16 x bf16 -> f32).  A convolution is 27
+// cores.  When L1 is a multiple of 128 all three contractions (forward, input
+// gradient, weight gradient) run on tcgen05 with tensor-memory accumulators
+// (conv_tc_kernel, wgrad_tc_kernel below); other extents use mma.sync.m16n8k16
+// (bf16 x bf16 -> f32), which this paragraph describes.  A convolution is 27
 // shifted 16x16 products: a warp owns 16 sites x 16 output channels (two
 // m16n8 tiles), gathers the 16 neighbour rows of each offset straight into
 // A fragments and takes the offset's weights (B) from shared memory.  The
@@ -21,6 +24,7 @@
 // K = 16 sites per step) into per-chunk partials summed in a fixed order.
 #include <cuda_bf16.h>
 
+#include <algorithm>
 #include <cmath>
 #include <cstdio>
 #include <cstring>
@@ -320,6 +324,168 @@ __global__ void __launch_bounds__(128) conv_tc_kernel(const __nv_bfloat16* __res
   }
 }
 
+// ------------------------------------------------------------------ tcgen05 weight gradient
+// gW[k][co][ci] = sum_i gz[i][co] x[i + d_k][ci], d_k = (dx, dy, dz), when L1
+// is a multiple of 128.  Substituting j = i + dx e_x turns every x offset into
+// a shift of gz: gW = sum_j x[j + (0, dy, dz)][ci] gz[j - dx e_x][co].  A tile
+// is 128 consecutive sites j of one x-line; a CTA (at most 4 per SM, each with
+// 128 tensor-memory columns) loops over tiles and accumulates in tensor
+// memory:
+//   A (M 128 = 8 (dy, dz) lines x 16 ci, K = 128 sites), MN-major: the 9 lines
+//     of x staged as 18 channel planes of 128 rows (16 B each); M groups of 8
+//     channels are one plane apart.  M = 128 covers lines 0-7; lines 1-8 form
+//     the second accumulator, of which only line 8's 16 rows are used;
+//   B (K = 128 sites, N 48 = 3 dx x 16 co), MN-major: gz staged three times,
+//     shifted by -dx, as 6 channel planes of 128 rows;
+//   2 accumulators x 48 FP32 columns, 8 K steps of 16 sites: 16 MMAs per tile.
+// The partial sums of each CTA go to part[k][cta][co][ci] (bias: sum of gz)
+// and are reduced in a fixed order by wgrad_sum_kernel.
+constexpr int kTgRows = 128;                            // sites per tile
+constexpr int kTgActBytes = 18 * kTgRows * 16;          // 9 lines x 2 planes
+constexpr int kTgGzBytes = 6 * kTgRows * 16;            // 3 shifts x 2 planes
+constexpr int kTgSmem = 52 * 1024;  // padded so that at most 4 CTAs (4 x 128 columns) share an SM
+static_assert(kTgActBytes + kTgGzBytes + 16 + 16 + 8 * kC * 4 <= kTgSmem, "wgrad shared memory");
+constexpr int kTgMaxCtasPerSm = 4;
+// BF16 A and B, both MN-major, FP32 D, M 128, N 48
+constexpr uint32_t kTgIdesc =
+    (1u << 4) | (1u << 7) | (1u << 10) | (1u << 15) | (1u << 16) | ((48u >> 3) << 17) | ((128u >> 4) << 24);
+
+__global__ void __launch_bounds__(128) wgrad_tc_kernel(const __nv_bfloat16* __restrict__ gz,
+                                                       const __nv_bfloat16* __restrict__ x, float* __restrict__ part,
+                                                       int nchunk, NetGeom g, unsigned* status) {
+  extern __shared__ __align__(1024) uint8_t tg_sm[];
+  uint8_t* act = tg_sm;
+  uint8_t* gzs = tg_sm + kTgActBytes;
+  uint64_t* mbar = reinterpret_cast<uint64_t*>(gzs + kTgGzBytes);
+  uint32_t* tslot = reinterpret_cast<uint32_t*>(mbar + 1);
+  float* bred = reinterpret_cast<float*>(tslot + 4);  // [8][16]
+  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+  const int segs = g.L1 >> 7, ntiles = segs * g.L2 * g.L3;
+
+  if (warp == 0) {
+    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(tslot)), "r"(128)
+                 : "memory");
+    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+  }
+  if (tid == 0) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(mbar)), "r"(1) : "memory");
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+  }
+  asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+  __syncthreads();
+  asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+  const uint32_t tmem = *tslot;
+
+  const uint4* x4 = reinterpret_cast<const uint4*>(x);
+  const uint4* gz4 = reinterpret_cast<const uint4*>(gz);
+  const int bco = tid & 15, brow = tid >> 4;  // bias: channel, row group
+  float bsum = 0.f;
+  uint32_t phase = 0;
+  bool ok = true;
+  int ndone = 0;
+  for (int t = blockIdx.x; t < ntiles; t += gridDim.x) {
+    const int x0 = (t % segs) << 7, y = (t / segs) % g.L2, z = (t / segs) / g.L2;
+    // x: line (dy, dz) = seg, plane c, row r = site x0 + r
+#pragma unroll 3
+    for (int seg = 0; seg < 9; ++seg) {
+      const int yy = wrap(y + seg / 3 - 1, g.L2), zz = wrap(z + seg % 3 - 1, g.L3);
+      const int f = tc_flat(g, x0 + tid, yy, zz);
+      reinterpret_cast<uint4*>(act)[(seg * 2) * kTgRows + tid] = __ldg(x4 + (size_t)f * 2);
+      reinterpret_cast<uint4*>(act)[(seg * 2 + 1) * kTgRows + tid] = __ldg(x4 + (size_t)f * 2 + 1);
+    }
+    // gz: shift s = dx + 1, plane c, row r = site x0 + r - dx
+#pragma unroll
+    for (int sh = 0; sh < 3; ++sh) {
+      const int f = tc_flat(g, wrap(x0 + tid - (sh - 1), g.L1), y, z);
+      reinterpret_cast<uint4*>(gzs)[(sh * 2) * kTgRows + tid] = __ldg(gz4 + (size_t)f * 2);
+      reinterpret_cast<uint4*>(gzs)[(sh * 2 + 1) * kTgRows + tid] = __ldg(gz4 + (size_t)f * 2 + 1);
+    }
+    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+    asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+    __syncthreads();
+    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+    if (tid == 0) {
+      const uint32_t a0 = smem_u32(act), b0 = smem_u32(gzs);
+#pragma unroll 1
+      for (int kk = 0; kk < kTgRows / 16; ++kk) {
+        const uint64_t bd = tc_desc(b0 + kk * 16 * 16, 128, kTgRows * 16);
+#pragma unroll
+        for (int h = 0; h < 2; ++h) {
+          const uint64_t ad = tc_desc(a0 + ((2 * h) * kTgRows + kk * 16) * 16, 128, kTgRows * 16);
+          const uint32_t acc = (ndone > 0 || kk > 0) ? 1u : 0u;
+          asm volatile(
+              "{\n\t.reg .pred p;\n\t"
+              "setp.ne.b32 p, %4, 0;\n\t"
+              "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n\t}"
+              ::"r"(tmem + (uint32_t)(h * 48)), "l"(ad), "l"(bd), "r"(kTgIdesc), "r"(acc)
+              : "memory");
+        }
+      }
+      asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(smem_u32(mbar))
+                   : "memory");
+    }
+    // bias gradient from the unshifted gz planes (generic reads beside the MMAs)
+    {
+      const __nv_bfloat16* p = reinterpret_cast<const __nv_bfloat16*>(gzs) + (size_t)(2 + (bco >> 3)) * kTgRows * 8;
+#pragma unroll
+      for (int j = 0; j < 16; ++j) bsum += __bfloat162float(p[(brow + 8 * j) * 8 + (bco & 7)]);
+    }
+    const uint32_t ph = phase;
+    phase ^= 1u;
+    const bool done = tc_wait(smem_u32(mbar), ph);
+    ++ndone;
+    if (__syncthreads_or(!done)) {
+      // record the failure, give the MMAs a second bounded wait, then stop
+      if (!done) {
+        if (lane == 0) atomicOr(status, 1u);
+        tc_wait(smem_u32(mbar), ph);
+      }
+      ok = false;
+      break;
+    }
+  }
+  asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+
+  // epilogue: warp w reads tensor-memory lanes 32w .. 32w+31 (M rows)
+  const int m = warp * 32 + lane, ci = m & 15;
+  const bool valid = ok && ndone > 0;
+#pragma unroll
+  for (int h = 0; h < 2; ++h) {
+    if (h == 1 && warp != 3) continue;  // second accumulator: only line 8 (rows 112-127)
+#pragma unroll
+    for (int sh = 0; sh < 3; ++sh) {
+      uint32_t v[16];
+      asm volatile(
+          "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, %13, %14, "
+          "%15}, [%16];"
+          : "=r"(v[0]), "=r"(v[1]), "=r"(v[2]), "=r"(v[3]), "=r"(v[4]), "=r"(v[5]), "=r"(v[6]), "=r"(v[7]),
+            "=r"(v[8]), "=r"(v[9]), "=r"(v[10]), "=r"(v[11]), "=r"(v[12]), "=r"(v[13]), "=r"(v[14]), "=r"(v[15])
+          : "r"(tmem + ((uint32_t)(warp * 32) << 16) + (uint32_t)(h * 48 + sh * 16)));
+      asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+      const int seg = h + (m >> 4);
+      if (h == 0 || m >= 112) {
+        const int k = sh * 9 + seg;
+        float* d = part + ((size_t)k * nchunk + blockIdx.x) * kC * kC + ci;
+#pragma unroll
+        for (int co = 0; co < kC; ++co) d[co * kC] = valid ? __uint_as_float(v[co]) : 0.f;
+      }
+    }
+  }
+  bred[brow * kC + bco] = bsum;
+  asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+  __syncthreads();
+  if (tid < kC) {
+    float b = 0.f;
+#pragma unroll
+    for (int q = 0; q < 8; ++q) b += bred[q * kC + tid];
+    part[(size_t)kK * nchunk * kC * kC + (size_t)blockIdx.x * kC + tid] = valid ? b : 0.f;
+  }
+  if (warp == 0) {
+    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(128) : "memory");
+  }
+}
+
 // partial[k][chunk][co][ci] = sum over the chunk's sites of gz[i][co] x[nbr_k(i)][ci]
 __global__ void __launch_bounds__(128) wgrad_kernel(const __nv_bfloat16* __restrict__ gz,
                                                     const __nv_bfloat16* __restrict__ x, float* __restrict__ part,
@@ -535,6 +701,7 @@ struct lce_net {
   double* part = nullptr;
   float* wpart = nullptr;
   int nchunk = 0;
+  int tg_grid = 0;   // CTAs of the tcgen05 weight gradient
   unsigned* flag = nullptr;  // set on the device when a tensor-core wait gave up
   // recorded training pairs
   struct Pair {
@@ -559,6 +726,18 @@ int net_fail(lce_net* n, int code, const std::string& m) {
     if (e_ != cudaSuccess) return net_fail(n, LCE_ERR_CUDA, std::string(#call) + ": " + cudaGetErrorString(e_)); \
   } while (0)
 
+// CTAs of the tcgen05 weight gradient: resident ones, at most 4 per SM (tensor
+// memory: 4 x 128 columns)
+int wgrad_tc_grid(lce_net* n) {
+  if (n->tg_grid > 0) return n->tg_grid;
+  int nsm = 0, occ = 0;
+  cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, n->device);
+  cudaFuncSetAttribute(wgrad_tc_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, kTgSmem);
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, wgrad_tc_kernel, 128, kTgSmem);
+  n->tg_grid = std::max(1, nsm) * std::max(1, std::min(occ, kTgMaxCtasPerSm));
+  return n->tg_grid;
+}
+
 int net_buffers(lce_net* n, long nsites) {
   if (n->nsites == nsites) return LCE_OK;
   // the buffers may still be in use by work queued on a context's stream
@@ -582,7 +761,9 @@ int net_buffers(lce_net* n, long nsites) {
   NCK(cudaMalloc(&n->target, (size_t)nsites * 4 * sizeof(float)));
   NCK(cudaMalloc(&n->part, (size_t)ceil_div(nsites, 256) * sizeof(double) + 64));
   n->nchunk = ceil_div(nsites, kChunk);
-  NCK(cudaMalloc(&n->wpart, ((size_t)kK * n->nchunk * kC * kC + (size_t)n->nchunk * kC) * sizeof(float)));
+  // partial sums of the mma.sync (per chunk) or the tcgen05 (per CTA) weight gradient
+  const size_t nparts = std::max(n->nchunk, wgrad_tc_grid(n));
+  NCK(cudaMalloc(&n->wpart, ((size_t)kK * nparts * kC * kC + nparts * kC) * sizeof(float)));
   n->nsites = nsites;
   return LCE_OK;
 }
@@ -629,8 +810,14 @@ void net_backward(lce_net* n, const NetGeom& g, cudaStream_t s) {
   __nv_bfloat16* gy = n->gy;
   for (int l = kLayers - 1; l >= 0; --l) {
     float* gW = n->grad + (size_t)l * kPl;
-    wgrad_kernel<<<dim3(n->nchunk, kK), 128, 0, s>>>(gz, n->act[l], n->wpart, n->nchunk, g);
-    wgrad_sum_kernel<<<kK + 1, kC * kC, 0, s>>>(n->wpart, n->nchunk, gW);
+    if (g.L1 % 128 == 0) {
+      const int grid = std::min(wgrad_tc_grid(n), (g.L1 / 128) * g.L2 * g.L3);
+      wgrad_tc_kernel<<<grid, 128, kTgSmem, s>>>(gz, n->act[l], n->wpart, grid, g, n->flag);
+      wgrad_sum_kernel<<<kK + 1, kC * kC, 0, s>>>(n->wpart, grid, gW);
+    } else {
+      wgrad_kernel<<<dim3(n->nchunk, kK), 128, 0, s>>>(gz, n->act[l], n->wpart, n->nchunk, g);
+      wgrad_sum_kernel<<<kK + 1, kC * kC, 0, s>>>(n->wpart, n->nchunk, gW);
+    }
     if (l > 0) {
       // gradient w.r.t. act[l] = conv_T(gz, W_l), times relu'(layer l-1) = (act[l] > 0)
       launch_conv<2>(n, gz, n->wt16 + (size_t)l * kWl, nullptr, gy, nullptr, n->act[l], g, s);
