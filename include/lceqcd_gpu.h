@@ -247,6 +247,34 @@ int lce_landau_gauge_from(lce_ctx* ctx, int chain, int start, double* theta_star
  * LCE_ERR_UNSUPPORTED.  max_iters caps both phases together. */
 int lce_landau_gauge_fourier(lce_ctx* ctx, int chain, int start, double step, double theta_switch, double* theta,
                              int* iters_fourier, int* iters_plain, int max_iters);
+/* The reference's iterative gauge fixing, f/it_gauge_fixing.f:5-214
+ * (compiled into the reference, never called by it).  One iteration, parity
+ * by parity: g = antihermitian part of sum_mu [U_f(x,mu) - U_f(x-mu,mu)]
+ * in first-row form, Omega = exp(step g) = cos|step g| + step g
+ * sin|step g|/|step g|, U_f and A_f transformed as in the overrelaxed
+ * iteration; *da1 = mean |g|^2 over the second parity, before its step
+ * (f/it_gauge_fixing.f:116-120).  step <= 0 takes the context's alpha, the
+ * reference's step.  flags:
+ *   LCE_ITGF_FIX_COMPONENT  second component g1(2) - g2(2); the reference
+ *                           writes g1(1) - g2(2) (f/it_gauge_fixing.f:110),
+ *                           with which the iteration does not converge
+ *   LCE_ITGF_ASCEND         Omega = exp(-step g): raises the Landau
+ *                           functional (the reference's sign lowers it and
+ *                           ends at the Z2 mirror, U_f -> -U_f on one
+ *                           parity's transform, physically equivalent)
+ *   LCE_ITGF_TRACK          also G(x) -> Omega(x) G(x)
+ * The single iteration does not reunitarise (the reference's subroutine
+ * does not).  Steepest descent is stable only for steps below ~1/3. */
+#define LCE_ITGF_FIX_COMPONENT 1
+#define LCE_ITGF_ASCEND 2
+#define LCE_ITGF_TRACK 4
+int lce_it_gauge_fixing(lce_ctx* ctx, int chain, double step, int flags, double* da1);
+/* f/landau_gauge.f:303-334 with it_gauge_fixing in place of
+ * or_gauge_fixing: copy U,A -> U_f,A_f (and G = 1 with LCE_ITGF_TRACK),
+ * then iterate + reunitarise U_f until da1 <= limit_or, on the device in
+ * captured batches like lce_landau_gauge.  max_iters <= 0: 10^6 cap;
+ * LCE_ERR_GF_NOT_CONVERGED when the cap ends the loop. */
+int lce_it_landau_gauge(lce_ctx* ctx, int chain, double step, int flags, double* da1, int* iters, int max_iters);
 /* one preconditioned direction omega [2][V/2][3] (components a3, Re b, Im b
  * of the vector part, parity-split order) from the current U_f; nothing is
  * updated (test hook for the FFT path) */

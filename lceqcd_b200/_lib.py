@@ -36,6 +36,9 @@ LCE_FIELDS_FIXED = 1
 LCE_GF_START_IDENTITY = 0
 LCE_GF_START_TRANSFORM = 1
 LCE_GF_START_NET = 2
+LCE_ITGF_FIX_COMPONENT = 1
+LCE_ITGF_ASCEND = 2
+LCE_ITGF_TRACK = 4
 LCE_WARM_NET = 1
 LCE_WARM_JUDGE = 2
 LCE_WARM_RECORD = 4
@@ -111,6 +114,8 @@ SIGNATURES = {
     "lce_get_meas_batch": (I, [P, P]),
     "lce_landau_gauge": (I, [P, I, P, P, I]),
     "lce_gauge_fix_continue": (I, [P, I, P, P, I]),
+    "lce_it_gauge_fixing": (I, [P, I, D, I, P]),
+    "lce_it_landau_gauge": (I, [P, I, D, I, P, P, I]),
     "lce_landau_gauge_from": (I, [P, I, I, P, P, P, I]),
     "lce_apply_transform": (I, [P, I]),
     "lce_landau_gauge_fourier": (I, [P, I, I, D, D, P, P, P, I]),

@@ -674,7 +674,9 @@ int get_slices(lce_ctx* c, int chain, double*& out) {
   return LCE_OK;
 }
 
-int gf_loop(lce_ctx* c, int chain, double* theta, int* iters, int max_iters, int track = 0) {
+// it_flags >= 0: the iterative form (LCE_ITGF_* flags, step), else overrelaxation
+int gf_loop(lce_ctx* c, int chain, double* theta, int* iters, int max_iters, int track = 0, int it_flags = -1,
+            double step = 0.0) {
   const ChainDev& ch = c->ch[chain];
   // bounded on the device in every case; no cap requested means 10^6
   const int cap = max_iters > 0 ? max_iters : 1000000;
@@ -685,21 +687,29 @@ int gf_loop(lce_ctx* c, int chain, double* theta, int* iters, int max_iters, int
   cs.gf_iters = 0;
   cs.gf_cap = cap;
   cs.gf_theta = 1.0e4;
+  if (it_flags >= 0) cs.gf_step = step;
   CK(cudaMemcpyAsync(c->cst_d + chain, &cs, sizeof(cs), cudaMemcpyHostToDevice, c->stream));
   CK(cudaStreamSynchronize(c->stream));
   double* part = c->scratch_d;
   int batch = 8;
   while (true) {
-    auto key = std::make_pair(chain, 2 * batch + (track ? 1 : 0));
+    // graph key: form (0 overrelaxation, 1 + flags iterative), batch, tracking
+    auto key = std::make_pair(chain, ((it_flags + 1) << 10) + 2 * batch + (track ? 1 : 0));
     auto it = c->gf_exec.find(key);
     if (it == c->gf_exec.end()) {
       cudaGraph_t g;
       CK(cudaStreamBeginCapture(c->stream, cudaStreamCaptureModeThreadLocal));
       for (int k = 0; k < batch; ++k) {
-        if (c->prec == LCE_PREC_F64)
+        if (it_flags >= 0) {
+          if (c->prec == LCE_PREC_F64)
+            launch_it_iteration<double>(c->ch_d + chain, c->cst_d + chain, it_flags, 1, part, ch.nh, c->stream);
+          else
+            launch_it_iteration<float>(c->ch_d + chain, c->cst_d + chain, it_flags, 1, part, ch.nh, c->stream);
+        } else if (c->prec == LCE_PREC_F64) {
           launch_gf_iteration<double>(c->ch_d + chain, c->cst_d + chain, track, part, ch.nh, c->stream);
-        else
+        } else {
           launch_gf_iteration<float>(c->ch_d + chain, c->cst_d + chain, track, part, ch.nh, c->stream);
+        }
       }
       CK(cudaStreamEndCapture(c->stream, &g));
       cudaGraphExec_t ex;
@@ -1136,6 +1146,46 @@ int lce_landau_gauge(lce_ctx* c, int chain, double* theta, int* iters, int max_i
 int lce_gauge_fix_continue(lce_ctx* c, int chain, double* theta, int* iters, int max_iters) {
   if (!c || chain < 0 || chain >= c->nchains) return LCE_ERR_INVALID;
   return gf_loop(c, chain, theta, iters, max_iters);
+}
+
+int lce_it_gauge_fixing(lce_ctx* c, int chain, double step, int flags, double* da1) {
+  if (!c || chain < 0 || chain >= c->nchains || (flags & ~(LCE_ITGF_FIX_COMPONENT | LCE_ITGF_ASCEND | LCE_ITGF_TRACK)))
+    return LCE_ERR_INVALID;
+  const ChainDev& ch = c->ch[chain];
+  ChainState cs;
+  CK(cudaMemcpyAsync(&cs, c->cst_d + chain, sizeof(cs), cudaMemcpyDeviceToHost, c->stream));
+  CK(cudaStreamSynchronize(c->stream));
+  cs.gf_done = 0;
+  cs.gf_iters = 0;
+  cs.gf_cap = 1;
+  cs.gf_theta = 1.0e4;
+  cs.gf_step = step > 0.0 ? step : ch.alpha;
+  CK(cudaMemcpyAsync(c->cst_d + chain, &cs, sizeof(cs), cudaMemcpyHostToDevice, c->stream));
+  // the subroutine itself: no reunitarisation
+  if (c->prec == LCE_PREC_F64)
+    launch_it_iteration<double>(c->ch_d + chain, c->cst_d + chain, flags, 0, c->scratch_d, ch.nh, c->stream);
+  else
+    launch_it_iteration<float>(c->ch_d + chain, c->cst_d + chain, flags, 0, c->scratch_d, ch.nh, c->stream);
+  CK(cudaGetLastError());
+  CK(cudaMemcpyAsync(&cs, c->cst_d + chain, sizeof(cs), cudaMemcpyDeviceToHost, c->stream));
+  CK(cudaStreamSynchronize(c->stream));
+  if (da1) *da1 = cs.gf_theta;
+  if (!std::isfinite(cs.gf_theta)) return fail(c, LCE_ERR_NAN, "it_gauge_fixing: da1 is not finite");
+  return LCE_OK;
+}
+
+int lce_it_landau_gauge(lce_ctx* c, int chain, double step, int flags, double* da1, int* iters, int max_iters) {
+  if (!c || chain < 0 || chain >= c->nchains || (flags & ~(LCE_ITGF_FIX_COMPONENT | LCE_ITGF_ASCEND | LCE_ITGF_TRACK)))
+    return LCE_ERR_INVALID;
+  const ChainDev& ch = c->ch[chain];
+  const size_t ub = (size_t)6 * ch.nh * link_bytes(c->prec), ab = (size_t)6 * ch.nh * real_bytes(c->prec);
+  CK(cudaMemcpyAsync(ch.uf, ch.u, ub, cudaMemcpyDeviceToDevice, c->stream));
+  CK(cudaMemcpyAsync(ch.af, ch.a, ab, cudaMemcpyDeviceToDevice, c->stream));
+  if (flags & LCE_ITGF_TRACK) {
+    if (c->prec == LCE_PREC_F64) launch_transform_identity<double>(ch.g, ch.nh, c->stream);
+    else launch_transform_identity<float>(ch.g, ch.nh, c->stream);
+  }
+  return gf_loop(c, chain, da1, iters, max_iters, 0, flags, step > 0.0 ? step : ch.alpha);
 }
 
 int lce_apply_transform(lce_ctx* c, int chain) {

@@ -1,4 +1,5 @@
-// lce_gaugefix.cu -- overrelaxed Landau gauge fixing on the device.
+// lce_gaugefix.cu -- overrelaxed Landau gauge fixing on the device, and the
+// reference's iterative (steepest-descent) form, f/it_gauge_fixing.f.
 //
 // One iteration of f/or_gauge_fixing1.f:52-337 is two half-steps (eo = 0, 1).
 // A half-step kernel gives one thread per site x of parity eo; the thread
@@ -148,6 +149,84 @@ __global__ void __launch_bounds__(kBlock) gf_half_kernel(const ChainDev* chp, co
   if (eo == 1) block_reduce_store<1>(th, part + blockIdx.x);
 }
 
+// One parity of f/it_gauge_fixing.f:52-210 (the reference's iterative gauge
+// fixing): g = sum_mu (i Im a, b) of U_f(x,mu) minus the same of
+// U_f(x-mu,mu) (:62-84), the second component as written g1(1) - g2(2)
+// (:110) unless LCE_ITGF_FIX_COMPONENT; |g|^2 into the partial sums on the
+// second parity (:116-120); Omega = exp(h), h = +-step g (:122-141); the
+// transform of A_f and of the links at both ends (:143-210).  g, |g|^2 and
+// Omega in FP64.  The step comes from the chain state (gf_step); renorm
+// reunitarises the links on the second parity (u_f_renorm after the
+// iteration, as f/landau_gauge.f:56-57 does for the overrelaxed form).
+template <typename R>
+__global__ void __launch_bounds__(kBlock) it_half_kernel(const ChainDev* chp, const ChainState* cst, int eo,
+                                                         double* part, int flags, int renorm) {
+  pdl_trigger();
+  const ChainDev& ch = *chp;
+  const int s = blockIdx.x * kBlock + threadIdx.x;
+  const int oe = 1 - eo, nh = ch.nh;
+  const Coord X = site_coord(eo, s < nh ? s : 0, ch.hx, ch.nxy, ch.dhx, ch.dnxy);
+  const int xm[3] = {nbr_dn<0>(ch, X), nbr_dn<1>(ch, X), nbr_dn<2>(ch, X)};
+  pdl_wait();
+  if (cst->gf_done) return;
+  double th[1] = {0.0};
+  if (s < nh) {
+    su2<R> um[3], ud[3];
+    double g1a = 0, g1br = 0, g1bi = 0, g2a = 0, g2br = 0, g2bi = 0;
+#pragma unroll
+    for (int mu = 0; mu < 3; ++mu) {
+      um[mu] = ldUf<R>(ch, mu, eo, s);
+      ud[mu] = ldUf<R>(ch, mu, oe, xm[mu]);
+    }
+#pragma unroll
+    for (int mu = 0; mu < 3; ++mu) {
+      g1a += (double)um[mu].a.im;
+      g1br += (double)um[mu].b.re;
+      g1bi += (double)um[mu].b.im;
+    }
+#pragma unroll
+    for (int mu = 0; mu < 3; ++mu) {
+      g2a += (double)ud[mu].a.im;
+      g2br += (double)ud[mu].b.re;
+      g2bi += (double)ud[mu].b.im;
+    }
+    const bool fix = (flags & LCE_ITGF_FIX_COMPONENT) != 0;
+    const double ga = g1a - g2a;
+    const double gbr = fix ? g1br - g2br : -g2br;
+    const double gbi = fix ? g1bi - g2bi : g1a - g2bi;
+    if (eo == 1) th[0] = ga * ga + (gbr * gbr + gbi * gbi);
+    const double st = (flags & LCE_ITGF_ASCEND) ? -cst->gf_step : cst->gf_step;
+    const double ha = st * ga, hbr = st * gbr, hbi = st * gbi;
+    const double t1 = sqrt(ha * ha + hbr * hbr + hbi * hbi);
+    // the reference divides 0 by 0 where g = 0; the limit is 1
+    const double t2 = t1 > 0.0 ? sin(t1) / t1 : 1.0;
+    const su2<R> o{{(R)cos(t1), (R)(ha * t2)}, {(R)(hbr * t2), (R)(hbi * t2)}};
+    R* Af = reinterpret_cast<R*>(ch.af);
+    const R a1 = Af[((size_t)(eo * 3 + 0)) * nh + s], a2 = Af[((size_t)(eo * 3 + 1)) * nh + s],
+            a3 = Af[((size_t)(eo * 3 + 2)) * nh + s];
+    const su2<R> ta = nn(o, ad(a1, a2, a3, o));
+    Af[((size_t)(eo * 3 + 0)) * nh + s] = ta.b.im;
+    Af[((size_t)(eo * 3 + 1)) * nh + s] = ta.b.re;
+    Af[((size_t)(eo * 3 + 2)) * nh + s] = ta.a.im;
+#pragma unroll
+    for (int mu = 0; mu < 3; ++mu) {
+      su2<R> a = nn(o, um[mu]);
+      su2<R> b = nd(ud[mu], o);
+      if (renorm && eo == 1) {
+        a = unitarise64(a);
+        b = unitarise64(b);
+      }
+      LinkIO<R>::st(ch.uf, ((size_t)(mu * 2 + eo)) * nh + s, a);
+      LinkIO<R>::st(ch.uf, ((size_t)(mu * 2 + oe)) * nh + xm[mu], b);
+    }
+    if (flags & LCE_ITGF_TRACK) {
+      const size_t gi = (size_t)eo * nh + s;
+      LinkIO<R>::st(ch.g, gi, unitarise64(nn(o, LinkIO<R>::ld_cg(ch.g, gi))));
+    }
+  }
+  if (eo == 1) block_reduce_store<1>(th, part + blockIdx.x);
+}
+
 // U_f(x,mu) = G(x) U(x,mu) G(x+mu)^+ and A_f(x) -> G(x) A(x) G(x)^+, one
 // thread per site of both parities
 template <typename R>
@@ -249,6 +328,15 @@ void launch_gf_iteration(const ChainDev* ch, ChainState* cst, int track, double*
 }
 
 template <typename R>
+void launch_it_iteration(const ChainDev* ch, ChainState* cst, int flags, int renorm, double* part, int nh,
+                         cudaStream_t s) {
+  const int nb = ceil_div(nh, kBlock);
+  (void)launch_pdl(it_half_kernel<R>, nb, kBlock, 0, s, ch, (const ChainState*)cst, 0, part, flags, renorm);
+  (void)launch_pdl(it_half_kernel<R>, nb, kBlock, 0, s, ch, (const ChainState*)cst, 1, part, flags, renorm);
+  (void)launch_pdl(gf_check_kernel, 1, 1024, 0, s, ch, cst, (const double*)part, nb);
+}
+
+template <typename R>
 void launch_gauge_apply(const ChainDev* ch, int nh, cudaStream_t s) {
   gauge_apply_kernel<R><<<ceil_div(2L * nh, kBlock), kBlock, 0, s>>>(ch);
 }
@@ -276,6 +364,8 @@ void launch_sum_partials(const double* part, int nblocks, int nq, double* out, c
 
 template void launch_gf_iteration<float>(const ChainDev*, ChainState*, int, double*, int, cudaStream_t);
 template void launch_gf_iteration<double>(const ChainDev*, ChainState*, int, double*, int, cudaStream_t);
+template void launch_it_iteration<float>(const ChainDev*, ChainState*, int, int, double*, int, cudaStream_t);
+template void launch_it_iteration<double>(const ChainDev*, ChainState*, int, int, double*, int, cudaStream_t);
 template void launch_gf_theta<float>(const ChainDev*, double*, int, cudaStream_t);
 template void launch_gf_theta<double>(const ChainDev*, double*, int, cudaStream_t);
 

@@ -181,6 +181,11 @@ void launch_flush(void* buf, size_t bytes, cudaStream_t s);
 template <typename R>
 void launch_gf_iteration(const ChainDev* ch, ChainState* cst, int track, double* part, int nh,
                          cudaStream_t s);
+// one iteration of f/it_gauge_fixing.f (flags LCE_ITGF_*, step from cst->gf_step),
+// then the convergence check of the overrelaxed form
+template <typename R>
+void launch_it_iteration(const ChainDev* ch, ChainState* cst, int flags, int renorm, double* part, int nh,
+                         cudaStream_t s);
 template <typename R>
 void launch_gauge_apply(const ChainDev* ch, int nh, cudaStream_t s);
 template <typename R>

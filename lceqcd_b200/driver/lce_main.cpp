@@ -11,14 +11,17 @@
 //   lce_main [--input FILE] [--dir DIR] [--precision f32|f64] [--seed N]
 //            [--corr-flag 1|2|3] [--therm N] [--max-gf-iters N]
 //            [--gf-angle acos|atan2] [--device N] [--agauge-hits 1|3]
-//            [--gauge-fix plain|warm|fourier]
+//            [--gauge-fix plain|warm|fourier|it] [--it-step S]
 //
 // --agauge-hits 3 runs the 3-hit link update of f/agauge1.f (the reference
 // picks agauge.f or agauge1.f at build time).  --gauge-fix: plain is
 // f/landau_gauge.f (copy, overrelaxation from G = 1); warm starts every
 // measurement after the first from the previous converged transform; fourier
 // uses the Fourier-accelerated iteration (power-of-two extents) from that warm
-// start.  All three stop at theta <= limit_or.
+// start; it is f/landau_gauge.f with the reference's iterative form
+// f/it_gauge_fixing.f in place of the overrelaxation, component corrected and
+// ascending, step --it-step (default 0.3; the reference's alpha diverges).
+// All stop at theta <= limit_or.
 //
 // Deviations: init = 0 is a Haar hot start on the device (the reference's
 // randomconf is not Haar distributed, f/confget.f:115-149); the per-site
@@ -176,6 +179,7 @@ int main(int argc, char** argv) {
   int prec = LCE_PREC_F32, corr_flag = 1, therm = 100, device = 0, max_gf = 0, gf_angle = LCE_GF_ATAN2;
   int agauge_hits = 1;
   std::string gauge_fix = "plain";
+  double it_step = 0.3;
   unsigned long long seed = 314159;
   for (int i = 1; i < argc; ++i) {
     std::string a = argv[i];
@@ -194,6 +198,7 @@ int main(int argc, char** argv) {
     else if (a == "--gf-angle") gf_angle = next() == "acos" ? LCE_GF_ACOS : LCE_GF_ATAN2;
     else if (a == "--agauge-hits") agauge_hits = std::atoi(next().c_str());
     else if (a == "--gauge-fix") gauge_fix = next();
+    else if (a == "--it-step") it_step = std::atof(next().c_str());
     else die("unknown option %s", a.c_str());
   }
   const Input in = read_input(input);
@@ -217,7 +222,8 @@ int main(int argc, char** argv) {
   p.device = device;
   p.gf_angle = gf_angle;
   p.agauge_hits = agauge_hits;
-  if (gauge_fix != "plain" && gauge_fix != "warm" && gauge_fix != "fourier") die("unknown --gauge-fix %s", gauge_fix.c_str());
+  if (gauge_fix != "plain" && gauge_fix != "warm" && gauge_fix != "fourier" && gauge_fix != "it")
+    die("unknown --gauge-fix %s", gauge_fix.c_str());
   lce_ctx* ctx = lce_create(&p);
   if (!ctx) die("lce_create: %s", lce_last_error(nullptr));
 
@@ -317,6 +323,8 @@ int main(int argc, char** argv) {
         int it_plain = 0;
         rc = lce_landau_gauge_fourier(ctx, 0, start, 0.0, 0.0, &theta, &iters, &it_plain, max_gf);
         iters += it_plain;
+      } else if (gauge_fix == "it") {
+        rc = lce_it_landau_gauge(ctx, 0, it_step, LCE_ITGF_FIX_COMPONENT | LCE_ITGF_ASCEND, &theta, &iters, max_gf);
       } else {
         rc = lce_landau_gauge(ctx, 0, &theta, &iters, max_gf);
       }

@@ -265,6 +265,32 @@ class _Context:
         self._ck(self.lib.lce_gauge_fix_continue(self.h, chain, C.byref(th), C.byref(it), int(max_iters)))
         return th.value, it.value
 
+    @staticmethod
+    def _itgf_flags(fix_component: bool, ascend: bool, track: bool) -> int:
+        return ((_lib.LCE_ITGF_FIX_COMPONENT if fix_component else 0) | (_lib.LCE_ITGF_ASCEND if ascend else 0)
+                | (_lib.LCE_ITGF_TRACK if track else 0))
+
+    def it_gauge_fixing(self, step: float = 0.0, fix_component: bool = False, ascend: bool = False,
+                        track: bool = False, chain: int = 0) -> float:
+        """One iteration of f/it_gauge_fixing.f on U_f, A_f; returns da1.
+        step <= 0: the context's alpha (the reference's step).  Defaults are
+        the reference as written; fix_component and ascend select the
+        corrected steepest ascent (lce_it_gauge_fixing)."""
+        da1 = C.c_double()
+        self._ck(self.lib.lce_it_gauge_fixing(self.h, chain, float(step),
+                                              self._itgf_flags(fix_component, ascend, track), C.byref(da1)))
+        return da1.value
+
+    def it_landau_gauge(self, step: float = 0.0, fix_component: bool = False, ascend: bool = False,
+                        track: bool = False, max_iters: int = 0, chain: int = 0):
+        """f/landau_gauge.f with it_gauge_fixing: copy, iterate and
+        reunitarise until da1 <= limit_or.  Returns (da1, iterations)."""
+        da1, it = C.c_double(), C.c_int()
+        self._ck(self.lib.lce_it_landau_gauge(self.h, chain, float(step),
+                                              self._itgf_flags(fix_component, ascend, track), C.byref(da1),
+                                              C.byref(it), int(max_iters)))
+        return da1.value, it.value
+
     def landau_gauge_from(self, start: str = "identity", max_iters: int = 0, chain: int = 0):
         """Gauge fixing tracking the transform G; start 'identity' or 'transform'
         (the current G).  Returns (theta_start, theta, iterations)."""

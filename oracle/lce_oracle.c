@@ -961,6 +961,93 @@ double lco_or_gauge_fixing(lco_ctx *c) {
   return da1;
 }
 
+/* f/it_gauge_fixing.f:5-214, one iteration of the reference's iterative
+ * (steepest-descent) gauge fixing, parity by parity (the transform of a
+ * parity is applied before the next parity's g is formed, :94-99):
+ *   g1 = sum_mu (i Im a, b) of U_f(x,mu), g2 the same of U_f(x-mu,mu)
+ *   (:62-84: the antihermitian part in first-row form);
+ *   g(1) = g1(1) - g2(1); g(2) = g1(1) - g2(2) as written at :110
+ *   (flag 1: g1(2) - g2(2), the antihermitian part of sum [U - U(x-mu)]);
+ *   on the second parity da1 = mean |g|^2 (:116-120), before the step;
+ *   Omega = cos|h| + h sin|h|/|h|, h = step g (:122-141; flag 2: h = -step g,
+ *   the direction that raises the Landau functional; as written the step
+ *   lowers it);
+ *   U_mu(x) -> Omega(x) U_mu(x), U_mu(y) -> U_mu(y) Omega(y+mu)^+ and
+ *   A_f -> Omega (iA_f) Omega^+ (:143-210).
+ * g, |g|^2 and Omega are formed in double in both builds (the device does
+ * the same); the transform is applied in the build's precision.  Where
+ * |h| = 0 the reference divides 0 by 0; the limit sin(t)/t = 1 is used. */
+double lco_it_gauge_fixing(lco_ctx *c, double step, int flags) {
+  const int nh = c->nh;
+  double da1 = 0;
+  su2 *om = (su2 *)malloc(sizeof(su2) * nh);
+  const double st = (flags & 2) ? -step : step;
+  for (int eo = 0; eo < 2; ++eo) {
+    const int oe = 1 - eo;
+    double dsum = 0;
+#pragma omp parallel for num_threads(c->nthreads) schedule(static) reduction(+ : dsum)
+    for (int s = 0; s < nh; ++s) {
+      double g1a = 0, g1br = 0, g1bi = 0, g2a = 0, g2br = 0, g2bi = 0;
+      for (int mu = 0; mu < 3; ++mu) {
+        su2 u = ld_su2(c->uf + UIDX(c, mu, eo, s));
+        g1a += u.a.im; g1br += u.b.re; g1bi += u.b.im;
+      }
+      for (int mu = 0; mu < 3; ++mu) {
+        su2 u = ld_su2(c->uf + UIDX(c, mu, oe, DN(c, eo, mu, s)));
+        g2a += u.a.im; g2br += u.b.re; g2bi += u.b.im;
+      }
+      const double ga = g1a - g2a;
+      const double gbr = (flags & 1) ? g1br - g2br : -g2br;
+      const double gbi = (flags & 1) ? g1bi - g2bi : g1a - g2bi;
+      if (eo == 1) dsum += ga * ga + (gbr * gbr + gbi * gbi);
+      const double ha = st * ga, hbr = st * gbr, hbi = st * gbi;
+      const double t1 = sqrt(ha * ha + hbr * hbr + hbi * hbi);
+      const double t2 = t1 > 0 ? sin(t1) / t1 : 1.0;
+      su2 o = {{(real)cos(t1), (real)(ha * t2)}, {(real)(hbr * t2), (real)(hbi * t2)}};
+      om[s] = o;
+    }
+    if (eo == 1) da1 = dsum / nh;
+#pragma omp parallel for num_threads(c->nthreads) schedule(static)
+    for (int s = 0; s < nh; ++s) {
+      real *af = c->af + AIDX(c, eo, s);
+      su2 t2 = mul_nn(om[s], mul_ad(af, om[s]));
+      af[0] = t2.b.im;
+      af[1] = t2.b.re;
+      af[2] = t2.a.im;
+    }
+    for (int mu = 0; mu < 3; ++mu) {
+#pragma omp parallel for num_threads(c->nthreads) schedule(static)
+      for (int s = 0; s < nh; ++s) {
+        real *p = c->uf + UIDX(c, mu, eo, s);
+        st_su2(p, mul_nn(om[s], ld_su2(p)));
+      }
+#pragma omp parallel for num_threads(c->nthreads) schedule(static)
+      for (int s = 0; s < nh; ++s) {
+        real *p = c->uf + UIDX(c, mu, oe, s);
+        st_su2(p, mul_nd(ld_su2(p), om[UP(c, oe, mu, s)]));
+      }
+    }
+  }
+  free(om);
+  return da1;
+}
+
+/* f/landau_gauge.f:303-334 with it_gauge_fixing in place of
+ * or_gauge_fixing: copy, then iterate + u_f_renorm while da1 > limit_or */
+int lco_it_landau_gauge(lco_ctx *c, double step, int flags, int max_iters, double *da1_out) {
+  double da1 = 10000.0;
+  int it = 0;
+  lco_landau_copy(c);
+  while (da1 > (double)c->limit_or) {
+    if (max_iters > 0 && it >= max_iters) break;
+    it++;
+    da1 = lco_it_gauge_fixing(c, step, flags);
+    lco_u_f_renorm(c);
+  }
+  if (da1_out) *da1_out = da1;
+  return it;
+}
+
 /* f/landau_gauge.f:303-334; max_iters <= 0 means no cap (as the reference) */
 int lco_landau_gauge(lco_ctx *c, int max_iters, double *da1_out) {
   double da1 = 10000.0;

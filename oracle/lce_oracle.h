@@ -18,7 +18,7 @@
  *   gauss            f/gauss.f:10-31
  *   Higgs updates    f/ahiggs1.f, f/ahiggs2.f, f/ahiggs3.f
  *   reunitarisation  f/renorm.f, f/u_f_renorm.f
- *   gauge fixing     f/landau_gauge.f, f/or_gauge_fixing1.f
+ *   gauge fixing     f/landau_gauge.f, f/or_gauge_fixing1.f, f/it_gauge_fixing.f
  *   measurements     f/correlator.f, f/polyakov.f, f/scalarcorr.f,
  *                    f/meas1.f, f/meas2a.f
  *   RANLUX           f/luxury.f (pinned to the expected output in f/luxtst.f:392-466)
@@ -126,6 +126,10 @@ void lco_landau_copy(lco_ctx *c);
 double lco_or_gauge_fixing(lco_ctx *c);          /* one iteration, returns da1 */
 void lco_u_f_renorm(lco_ctx *c);
 int  lco_landau_gauge(lco_ctx *c, int max_iters, double *da1);  /* returns iterations */
+/* f/it_gauge_fixing.f: one iteration (returns da1); flags 1 = second
+ * component from g1(2), 2 = rotate by exp(-step g) */
+double lco_it_gauge_fixing(lco_ctx *c, double step, int flags);
+int  lco_it_landau_gauge(lco_ctx *c, double step, int flags, int max_iters, double *da1);
 double lco_gauge_functional(const lco_ctx *c);   /* (1/3V) sum Re Tr_2/2 U_f */
 double lco_theta_direct(const lco_ctx *c);       /* mean over odd sites, fresh */
 void lco_correlator(const lco_ctx *c, double *corr_a, double *corr_u, double *corr_3);

@@ -83,6 +83,8 @@ def _lib(bits: int) -> C.CDLL:
         "lco_or_gauge_fixing": (C.c_double, [P]),
         "lco_u_f_renorm": (None, [P]),
         "lco_landau_gauge": (C.c_int, [P, C.c_int, P]),
+        "lco_it_gauge_fixing": (C.c_double, [P, C.c_double, C.c_int]),
+        "lco_it_landau_gauge": (C.c_int, [P, C.c_double, C.c_int, C.c_int, P]),
         "lco_gauge_functional": (C.c_double, [P]),
         "lco_theta_direct": (C.c_double, [P]),
         "lco_correlator": (None, [P, P, P, P]),
@@ -330,6 +332,15 @@ class Oracle:
     def landau_gauge(self, max_iters: int = 0):
         da1 = C.c_double()
         it = self.lib.lco_landau_gauge(self.h, max_iters, C.byref(da1))
+        return da1.value, it
+
+    # f/it_gauge_fixing.f: flags 1 = second component from g1(2), 2 = ascend
+    def it_gauge_fixing(self, step: float, flags: int = 0) -> float:
+        return self.lib.lco_it_gauge_fixing(self.h, step, flags)
+
+    def it_landau_gauge(self, step: float, flags: int = 0, max_iters: int = 0):
+        da1 = C.c_double()
+        it = self.lib.lco_it_landau_gauge(self.h, step, flags, max_iters, C.byref(da1))
         return da1.value, it
 
     def gauge_functional(self) -> float:

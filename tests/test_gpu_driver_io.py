@@ -133,3 +133,21 @@ def test_driver_rejects_bad_inputfile(tmp_path):
     r = subprocess.run([DRIVER, "--input", str(inp), "--dir", str(tmp_path)], capture_output=True, text=True,
                        timeout=60)
     assert r.returncode != 0 and "data input" in r.stderr
+
+
+def test_driver_iterative_gauge_fixing(tmp_path):
+    """--gauge-fix it: f/landau_gauge.f with the reference's iterative form
+    (component corrected, ascending); same files as the overrelaxed run."""
+    inp = tmp_path / "inputfile"
+    inp.write_text(INPUT.format(L=8, init=2, start=0))
+    r = subprocess.run([DRIVER, "--input", str(inp), "--dir", str(tmp_path), "--therm", "20",
+                        "--gauge-fix", "it", "--it-step", "0.3"], capture_output=True, text=True, timeout=300)
+    assert r.returncode == 0, r.stderr
+    tag = "s08_be09000_x01000_y04500_u000000"
+    correl = (tmp_path / f"correl_{tag}").read_text().splitlines()
+    assert correl[3] == "001" and len(correl) == 3 + 2 * (1 + 8)
+    vals = np.array([float(v) for l in correl[4:] if not l.strip().isdigit() for v in l.split()])
+    assert vals.size > 0 and np.all(np.isfinite(vals))
+    r = subprocess.run([DRIVER, "--input", str(inp), "--dir", str(tmp_path), "--gauge-fix", "sd"],
+                       capture_output=True, text=True, timeout=60)
+    assert r.returncode != 0 and "gauge-fix" in r.stderr

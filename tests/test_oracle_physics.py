@@ -209,3 +209,70 @@ def test_ahiggs1_step_adaptation():
     assert acc < 0.4 and abs(d - 10.0 * 0.8989669) < 1e-5
     acc, d2 = o.ahiggs1(0.01, 1)
     assert acc > 0.6 and abs(d2 - 0.01 * 1.1131241) < 1e-8
+
+
+# ---- the reference's iterative gauge fixing, f/it_gauge_fixing.f
+
+def _thermalised(L, sweeps=30, seed=5):
+    o = Oracle(L, 12.0, 0.09, 0.3, lam=1.7, limit_or=1e-10)
+    o.set_fields(*hot_config(L, seed=seed))
+    o.set_philox(seed + 2)
+    for _ in range(sweeps):
+        o.sweep(0)
+    return o.get_fields()
+
+
+def test_it_gauge_fixing_unit_configuration():
+    """g = 0 on the unit configuration: Omega = 1 (the sin(t)/t -> 1 limit
+    where the reference divides 0 by 0), da1 = 0, fields unchanged."""
+    o = Oracle((4, 4, 6), 9.0, 0.1, 0.45)
+    o.unitconf(1.0)
+    o.landau_copy()
+    u, a = o.get_fields(0)
+    for flags in range(4):
+        assert o.it_gauge_fixing(1.0, flags) == 0.0
+    uf, af = o.get_fields(1)
+    np.testing.assert_array_equal(uf, u)
+    np.testing.assert_allclose(af, a, atol=1e-15)
+
+
+def test_it_gauge_fixing_forms():
+    """On a thermalised 8^3 configuration: the corrected steepest ascent
+    (flags 3) converges to the overrelaxed iteration's Landau gauge; the
+    reference's sign (flags 1) ends at its Z2 mirror, functional -F; the
+    second component as written at f/it_gauge_fixing.f:110 (flags 0) does not
+    converge; steps above ~1/3 diverge."""
+    L = (8, 8, 8)
+    u, a = _thermalised(L)
+
+    def run(step, flags, cap):
+        o = Oracle(L, 12.0, 0.09, 0.3, lam=1.7, limit_or=1e-10)
+        o.set_fields(u, a)
+        da1, it = o.it_landau_gauge(step, flags, max_iters=cap)
+        return da1, it, o.gauge_functional()
+
+    o = Oracle(L, 12.0, 0.09, 0.3, lam=1.7, limit_or=1e-10)
+    o.set_fields(u, a)
+    o.landau_gauge(max_iters=20000)
+    F = o.gauge_functional()
+    da1, it, F3 = run(0.3, 3, 2000)
+    assert da1 <= 1e-10 and it < 200 and abs(F3 - F) < 1e-6
+    da1, it, F1 = run(0.3, 1, 2000)
+    assert da1 <= 1e-10 and abs(F1 + F) < 1e-6
+    da1, it, _ = run(0.1, 0, 1000)
+    assert it == 1000 and da1 > 1e-3
+    da1, it, _ = run(0.5, 3, 1000)
+    assert it == 1000 and da1 > 1.0
+
+
+def test_it_gauge_fixing_da1_is_theta_for_small_steps():
+    """With the component corrected, |g|^2 is theta of the overrelaxed form
+    (alpha = 1): for a negligible step da1 equals the direct evaluation."""
+    L = (4, 6, 4)
+    u, a = hot_config(L, seed=9)
+    o = Oracle(L, 9.0, 0.1, 0.45, alpha=1.0)
+    o.set_fields(u, a)
+    o.landau_copy()
+    th = o.theta_direct()
+    da1 = o.it_gauge_fixing(1e-13, 1)
+    assert abs(da1 - th) <= 1e-9 * th
