@@ -104,6 +104,33 @@ def test_philox_stream_matches_oracle(L):
     assert rel_err(g.download(dtype=np.float64)[0], o.get_fields()[0]) < 1e-11
 
 
+def test_composed_routines_philox_match_oracle():
+    """Single-routine calls in a composed order (agauge, 4 x link_or, ahiggs1,
+    2 x ahiggs3, renorm) draw the same Philox uniforms as the oracle: FP64
+    fields agree after every routine, and the pass counters match."""
+    L = (4, 6, 4)
+    o, g, _, _ = pair(L, seed=15, rng="philox")
+    o.set_philox(12345, 0)
+    do = dg = 0.5
+    for _ in range(3):
+        steps = [("agauge", ()), *[("link_or", ())] * 4, ("ahiggs1", None), ("ahiggs3", ()), ("ahiggs3", ()),
+                 ("renorm", None)]
+        for name, args in steps:
+            if name == "ahiggs1":
+                _, do = o.ahiggs1(do, 1)
+                _, dg = g.ahiggs1(dg, 1)
+            elif name == "renorm":
+                o.renorm()
+                g.renorm()
+            else:
+                getattr(o, name)(1)
+                getattr(g, name)(1)
+            uo, ao = o.get_fields()
+            ug, ag = g.download(dtype=np.float64)
+            assert rel_err(ug, uo) < 1e-11 and rel_err(ag, ao) < 1e-11, name
+            assert g.rng_position()[0] == o.pass_ctr(), name
+
+
 def test_ahiggs1_and_link_or_fp64():
     L = (4, 6, 4)
     o, g, _, _ = pair(L, seed=11)
