@@ -143,26 +143,35 @@ __global__ void __launch_bounds__(32 * kConvWarps) conv_kernel(const __nv_bfloat
 
 // ------------------------------------------------------------------ tcgen05 path
 // The same convolution on the 5th-generation tensor cores when L1 is a
-// multiple of 128: a CTA of 128 threads computes the 16 output channels of
-// 128 consecutive sites of one x-line.  It stages, for each of the 9 (dy, dz)
-// neighbour lines, the 130 input rows x0-1 .. x0+128 (periodic) in shared
-// memory as two "channel planes" (channels 0-7 and 8-15, 16 B per row), so
-// that the A operand of offset (dx, dy, dz) -- 128 sites x 16 channels -- is
-// the canonical K-major layout without swizzle (8-row core matrices of 16 B
-// rows, stride 128 B; the second K chunk one plane further) starting dx + 1
-// rows into its segment.  The weights of the 27 offsets sit in the same
-// layout.  One thread issues the 27 tcgen05.mma (M 128, N 16, K 16, BF16 in,
-// FP32 accumulate in tensor memory), commits them to an mbarrier, and after
-// the (bounded) wait each warp reads its 32 rows out of tensor memory for the
-// epilogue.
-constexpr int kTcRows = 136;                         // staged rows per plane (130 used)
-constexpr int kTcActBytes = 18 * kTcRows * 16;        // 9 segments x 2 planes
-constexpr int kTcWtBytes = kK * 2 * kC * 16;          // 27 offsets x 2 planes x 16 rows
-constexpr int kTcSmem = kTcActBytes + kTcWtBytes + 16;
+// multiple of 128.  A tile is 128 consecutive sites j = x0 .. x0+127 of one
+// x-line (y, z).  Moving the x offset out of the operand,
+//   P_dx[j][co] = sum_{(dy,dz)} sum_ci in[(j, y+dy, z+dz)][ci] W[dx,dy,dz][co][ci]
+//   out[i][co]  = P_-1[i-1][co] + P_0[i][co] + P_+1[i+1][co],
+// makes the tile one GEMM: M = 128 sites, K = 9 lines x 16 channels,
+// N = 3 dx x 16 output channels -- 9 tcgen05.mma of M 128, N 48, K 16 (BF16
+// in, FP32 accumulate in 48 tensor-memory columns) instead of 27 of N 16.
+// The 9 (dy, dz) lines sit in shared memory as channel planes (channels 0-7
+// and 8-15, 16-byte rows): the canonical K-major layout without swizzle
+// (8-row core matrices of 128 B, the second K chunk one plane further); the
+// weights, staged once per CTA, in the same layout with N = 48 rows per line.
+// The epilogue reads each warp's 32 rows out of tensor memory and forms the
+// x-shifted sum with warp shuffles; the rows across warp boundaries go
+// through shared memory, and the two rows outside the tile (P_-1 at x0-1,
+// P_+1 at x0+128) are computed on the CUDA cores from staged halo sites.
+// CTAs are persistent (4 per SM) and loop over tiles.
+constexpr int kTcRows = 128;                          // sites per tile
+constexpr int kTcN = 3 * kC;                          // N: 3 dx x 16 output channels
+constexpr int kTcActBytes = 18 * kTcRows * 16;        // 9 lines x 2 planes
+constexpr int kTcWtBytes = 9 * 2 * kTcN * 16;         // 9 lines x 2 planes x 48 rows
+constexpr int kTcHaloBytes = 2 * 9 * 2 * 16;          // x0-1 and x0+128: 9 lines x 2 planes
+constexpr int kTcXchBytes = (2 * 4 + 2) * kC * 4;     // warp-boundary and edge rows (FP32)
+constexpr int kTcSmem = kTcActBytes + kTcWtBytes + kTcHaloBytes + kTcXchBytes + 16;
+constexpr int kTcCtasPerSm = 4;
+static_assert(kTcCtasPerSm * (kTcSmem + 1024) <= 228 * 1024, "conv CTAs per SM");
 constexpr unsigned kTcSpin = 1u << 24;                // mbarrier polls before giving up
 
-// tcgen05.mma instruction descriptor: BF16 A and B (K-major), FP32 D, M 128, N 16
-constexpr uint32_t kTcIdesc = (1u << 4) | (1u << 7) | (1u << 10) | ((16u >> 3) << 17) | ((128u >> 4) << 24);
+// tcgen05.mma instruction descriptor: BF16 A and B (K-major), FP32 D, M 128, N 48
+constexpr uint32_t kTcIdesc = (1u << 4) | (1u << 7) | (1u << 10) | ((kTcN >> 3) << 17) | ((128u >> 4) << 24);
 
 // shared-memory matrix descriptor, no swizzle: start address, leading-dimension
 // byte offset (between the two K chunks), stride-dimension byte offset
@@ -206,6 +215,15 @@ __device__ __forceinline__ int tc_flat(const NetGeom& g, int x, int y, int z) {
   return ((x + y + z) & 1) * g.nh + site_index(x, y, z, g.hx, g.nxy);
 }
 
+// x-line tile t -> (x0, y, z)
+__device__ __forceinline__ void tc_tile(const NetGeom& g, int t, int& x0, int& y, int& z) {
+  const int segs = g.L1 >> 7;
+  x0 = (t % segs) << 7;
+  t /= segs;
+  y = t % g.L2;
+  z = t / g.L2;
+}
+
 template <int MODE>
 __global__ void __launch_bounds__(128) conv_tc_kernel(const __nv_bfloat16* __restrict__ in,
                                                       const __nv_bfloat16* __restrict__ W,
@@ -215,18 +233,16 @@ __global__ void __launch_bounds__(128) conv_tc_kernel(const __nv_bfloat16* __res
                                                       unsigned* status) {
   extern __shared__ __align__(1024) uint8_t tc_sm[];
   uint8_t* act = tc_sm;
-  uint8_t* wts = tc_sm + kTcActBytes;
-  uint64_t* mbar = reinterpret_cast<uint64_t*>(wts + kTcWtBytes);
+  uint8_t* wts = act + kTcActBytes;
+  uint8_t* halo = wts + kTcWtBytes;                          // [side][line][plane] 16 B
+  float* xch = reinterpret_cast<float*>(halo + kTcHaloBytes);  // [0..3] P_-1 of lane 31, [4..7] P_+1 of lane 0, [8] edge lo, [9] edge hi
+  uint64_t* mbar = reinterpret_cast<uint64_t*>(xch + (2 * 4 + 2) * kC);
   uint32_t* tslot = reinterpret_cast<uint32_t*>(mbar + 1);
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
-  const int segs = g.L1 >> 7;
-  int t = blockIdx.x;
-  const int x0 = (t % segs) << 7;
-  t /= segs;
-  const int y = t % g.L2, z = t / g.L2;
+  const int ntiles = (g.L1 >> 7) * g.L2 * g.L3;
 
   if (warp == 0) {
-    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(tslot)), "r"(32)
+    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(tslot)), "r"(64)
                  : "memory");
     asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
   }
@@ -234,70 +250,131 @@ __global__ void __launch_bounds__(128) conv_tc_kernel(const __nv_bfloat16* __res
     asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(mbar)), "r"(1) : "memory");
     asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
   }
-
-  // weights: plane (k, c), row o holds inputs 8c .. 8c+7 of output o
+  // weights once per CTA: line s, plane c, row n = dx_index * 16 + o holds
+  // inputs 8c .. 8c+7 of output o at offset k = dx_index * 9 + s
   const uint4* W4 = reinterpret_cast<const uint4*>(W);
-  for (int e = tid; e < kK * kC * 2; e += blockDim.x) {
-    const int k = e >> 5, o = (e >> 1) & 15, c = e & 1;
-    cp16(reinterpret_cast<uint4*>(wts) + (k * 2 + c) * kC + o, W4 + (k * kC + o) * 2 + c);
+  for (int e = tid; e < 9 * 2 * kTcN; e += blockDim.x) {
+    const int sg = e / (2 * kTcN), c = (e / kTcN) & 1, n = e % kTcN;
+    const int k = (n >> 4) * 9 + sg, o = n & 15;
+    cp16(reinterpret_cast<uint4*>(wts) + e, W4 + (k * kC + o) * 2 + c);
   }
-  // activations: segment (dy, dz), plane c, row r = input site x0 - 1 + r
-  const uint4* in4 = reinterpret_cast<const uint4*>(in);
-  for (int e = tid; e < 9 * 130; e += blockDim.x) {
-    const int seg = e / 130, r = e - seg * 130;
-    const int yy = wrap(y + seg / 3 - 1, g.L2), zz = wrap(z + seg % 3 - 1, g.L3);
-    const int xx = wrap(x0 - 1 + r, g.L1);
-    const int f = tc_flat(g, xx, yy, zz);
-    cp16(reinterpret_cast<uint4*>(act) + (seg * 2) * kTcRows + r, in4 + (size_t)f * 2);
-    cp16(reinterpret_cast<uint4*>(act) + (seg * 2 + 1) * kTcRows + r, in4 + (size_t)f * 2 + 1);
-  }
-  cp_wait_all();
-  // generic-proxy shared-memory writes -> visible to the tensor core (async proxy)
-  asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
   asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
   __syncthreads();
   asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
   const uint32_t tmem = *tslot;
+  const uint4* in4 = reinterpret_cast<const uint4*>(in);
+  const __nv_bfloat16* wb = reinterpret_cast<const __nv_bfloat16*>(wts);
+  const __nv_bfloat16* hb = reinterpret_cast<const __nv_bfloat16*>(halo);
+  uint32_t phase = 0;
 
-  if (tid == 0) {
-    const uint32_t a0 = smem_u32(act), b0 = smem_u32(wts);
-#pragma unroll 1
-    for (int k = 0; k < kK; ++k) {
-      const int dx = k / 9 - 1, seg = k % 9;
-      const uint64_t ad = tc_desc(a0 + ((seg * 2) * kTcRows + dx + 1) * 16, kTcRows * 16, 128);
-      const uint64_t bd = tc_desc(b0 + (k * 2 * kC) * 16, kC * 16, 128);
-      const uint32_t acc = k > 0 ? 1u : 0u;
-      asm volatile(
-          "{\n\t.reg .pred p;\n\t"
-          "setp.ne.b32 p, %4, 0;\n\t"
-          "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n\t}"
-          ::"r"(tmem), "l"(ad), "l"(bd), "r"(kTcIdesc), "r"(acc)
-          : "memory");
+  for (int t = blockIdx.x; t < ntiles; t += gridDim.x) {
+    int x0, y, z;
+    tc_tile(g, t, x0, y, z);
+    // line s = (dy, dz), plane c, row r = site x0 + r; halo sites x0-1, x0+128
+#pragma unroll
+    for (int sg = 0; sg < 9; ++sg) {
+      const int yy = wrap(y + sg / 3 - 1, g.L2), zz = wrap(z + sg % 3 - 1, g.L3);
+      const size_t f = (size_t)tc_flat(g, x0 + tid, yy, zz) * 2;
+      cp16(reinterpret_cast<uint4*>(act) + (sg * 2) * kTcRows + tid, in4 + f);
+      cp16(reinterpret_cast<uint4*>(act) + (sg * 2 + 1) * kTcRows + tid, in4 + f + 1);
     }
-    asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(smem_u32(mbar))
-                 : "memory");
-  }
-  const bool done = tc_wait(smem_u32(mbar), 0);
-  if (!done) {
-    // record the failure, give the MMAs a second bounded wait, then clean up
-    if (lane == 0) atomicOr(status, 1u);
-    tc_wait(smem_u32(mbar), 0);
-  }
-  asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-  uint32_t v[16];
-  asm volatile(
-      "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, %13, %14, %15}, "
-      "[%16];"
-      : "=r"(v[0]), "=r"(v[1]), "=r"(v[2]), "=r"(v[3]), "=r"(v[4]), "=r"(v[5]), "=r"(v[6]), "=r"(v[7]), "=r"(v[8]),
-        "=r"(v[9]), "=r"(v[10]), "=r"(v[11]), "=r"(v[12]), "=r"(v[13]), "=r"(v[14]), "=r"(v[15])
-      : "r"(tmem + ((uint32_t)(warp * 32) << 16)));
-  asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+    if (tid < 36) {
+      const int side = tid / 18, sg = (tid >> 1) % 9, c = tid & 1;
+      const int yy = wrap(y + sg / 3 - 1, g.L2), zz = wrap(z + sg % 3 - 1, g.L3);
+      const int xx = wrap(side ? x0 + kTcRows : x0 - 1, g.L1);
+      cp16(reinterpret_cast<uint4*>(halo) + tid, in4 + (size_t)tc_flat(g, xx, yy, zz) * 2 + c);
+    }
+    cp_wait_all();
+    // generic-proxy shared-memory writes -> visible to the tensor core (async proxy)
+    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+    asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+    __syncthreads();
+    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
 
-  if (done) {
-    const int f = tc_flat(g, x0 + tid, y, z);  // row tid = warp*32 + lane: site x0 + tid
+    if (tid == 0) {
+      const uint32_t a0 = smem_u32(act), b0 = smem_u32(wts);
+#pragma unroll 1
+      for (int sg = 0; sg < 9; ++sg) {
+        const uint64_t ad = tc_desc(a0 + (sg * 2 * kTcRows) * 16, kTcRows * 16, 128);
+        const uint64_t bd = tc_desc(b0 + (sg * 2 * kTcN) * 16, kTcN * 16, 128);
+        const uint32_t acc = sg > 0 ? 1u : 0u;
+        asm volatile(
+            "{\n\t.reg .pred p;\n\t"
+            "setp.ne.b32 p, %4, 0;\n\t"
+            "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n\t}"
+            ::"r"(tmem), "l"(ad), "l"(bd), "r"(kTcIdesc), "r"(acc)
+            : "memory");
+      }
+      asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(
+                       smem_u32(mbar))
+                   : "memory");
+    }
+    if (warp == 1) {
+      // the rows outside the tile on the CUDA cores: lanes 0-15 P_-1[x0-1][o],
+      // lanes 16-31 P_+1[x0+128][o]
+      const int side = lane >> 4, o = lane & 15, n = (side ? 2 : 0) * kC + o;
+      float v = 0.f;
+#pragma unroll 1
+      for (int sg = 0; sg < 9; ++sg) {
+#pragma unroll
+        for (int c = 0; c < 2; ++c) {
+          const __nv_bfloat16* xr = hb + ((side * 9 + sg) * 2 + c) * 8;
+          const __nv_bfloat16* wr = wb + ((size_t)(sg * 2 + c) * kTcN + n) * 8;
+#pragma unroll
+          for (int q = 0; q < 8; ++q) v = fmaf(__bfloat162float(xr[q]), __bfloat162float(wr[q]), v);
+        }
+      }
+      xch[(8 + side) * kC + o] = v;
+    }
+    const uint32_t ph = phase;
+    phase ^= 1u;
+    const bool done = tc_wait(smem_u32(mbar), ph);
+    if (__syncthreads_or(!done)) {
+      // record the failure, give the MMAs a second bounded wait, then stop
+      if (!done) {
+        if (lane == 0) atomicOr(status, 1u);
+        tc_wait(smem_u32(mbar), ph);
+      }
+      break;
+    }
+    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+    // row j = 32 warp + lane: P_-1[j] (columns 0-15), P_0[j] (16-31), P_+1[j] (32-47)
+    uint32_t vm[16], v0[16], vp[16];
+    const uint32_t ta = tmem + ((uint32_t)(warp * 32) << 16);
+#define LCE_TC_LD16(dst, col)                                                                                   \
+  asm volatile(                                                                                                 \
+      "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, %13, %14, " \
+      "%15}, [%16];"                                                                                            \
+      : "=r"(dst[0]), "=r"(dst[1]), "=r"(dst[2]), "=r"(dst[3]), "=r"(dst[4]), "=r"(dst[5]), "=r"(dst[6]),       \
+        "=r"(dst[7]), "=r"(dst[8]), "=r"(dst[9]), "=r"(dst[10]), "=r"(dst[11]), "=r"(dst[12]), "=r"(dst[13]),   \
+        "=r"(dst[14]), "=r"(dst[15])                                                                            \
+      : "r"(ta + (col)))
+    LCE_TC_LD16(vm, 0);
+    LCE_TC_LD16(v0, 16);
+    LCE_TC_LD16(vp, 32);
+#undef LCE_TC_LD16
+    asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+    // rows across warp boundaries
+    if (lane == 31) {
+#pragma unroll
+      for (int c = 0; c < kC; ++c) xch[warp * kC + c] = __uint_as_float(vm[c]);
+    }
+    if (lane == 0) {
+#pragma unroll
+      for (int c = 0; c < kC; ++c) xch[(4 + warp) * kC + c] = __uint_as_float(vp[c]);
+    }
+    asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+    __syncthreads();
+    const float* lo = lane == 0 ? (warp == 0 ? xch + 8 * kC : xch + (warp - 1) * kC) : nullptr;
+    const float* hi = lane == 31 ? (warp == 3 ? xch + 9 * kC : xch + (4 + warp + 1) * kC) : nullptr;
     float o[kC];
 #pragma unroll
-    for (int c = 0; c < kC; ++c) o[c] = __uint_as_float(v[c]) + (MODE != 2 ? bias[c] : 0.f);
+    for (int c = 0; c < kC; ++c) {
+      const float pm = __shfl_up_sync(0xffffffffu, __uint_as_float(vm[c]), 1);
+      const float pp = __shfl_down_sync(0xffffffffu, __uint_as_float(vp[c]), 1);
+      o[c] = (lo ? lo[c] : pm) + __uint_as_float(v0[c]) + (hi ? hi[c] : pp) + (MODE != 2 ? bias[c] : 0.f);
+    }
+    const int f = tc_flat(g, x0 + tid, y, z);
     if (MODE == 1) {
       float4* d = reinterpret_cast<float4*>(out32 + (size_t)f * 8);
       d[0] = make_float4(o[0], o[1], o[2], o[3]);
@@ -325,12 +402,14 @@ __global__ void __launch_bounds__(128) conv_tc_kernel(const __nv_bfloat16* __res
       d[0] = w0;
       d[1] = w1;
     }
+    // the exchange rows, the staged tile and the accumulator are reused by the next tile
+    __syncthreads();
   }
   asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
   __syncthreads();
   if (warp == 0) {
     asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(32) : "memory");
+    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(64) : "memory");
   }
 }
 
@@ -798,9 +877,12 @@ void launch_conv(lce_net* n, const __nv_bfloat16* in, const __nv_bfloat16* W, co
     static bool attr = false;  // per MODE instantiation
     if (!attr) {
       cudaFuncSetAttribute(conv_tc_kernel<MODE>, cudaFuncAttributeMaxDynamicSharedMemorySize, kTcSmem);
+      cudaFuncSetAttribute(conv_tc_kernel<MODE>, cudaFuncAttributePreferredSharedMemoryCarveout,
+                           (int)cudaSharedmemCarveoutMaxShared);
       attr = true;
     }
-    const int grid = (g.L1 / 128) * g.L2 * g.L3;
+    // persistent CTAs, 4 per SM (as many SMs as the weight gradient uses)
+    const int grid = std::min(wgrad_tc_grid(n), (g.L1 / 128) * g.L2 * g.L3);
     conv_tc_kernel<MODE><<<grid, 128, kTcSmem, s>>>(in, W, bias, out16, out32, mask, g, n->flag);
   } else {
     conv_kernel<MODE><<<conv_grid(2L * g.nh), 32 * kConvWarps, 0, s>>>(in, W, bias, out16, out32, mask, g);
