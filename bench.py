@@ -36,6 +36,9 @@ UNIT = "site-updates/s"
 # algorithmic HBM bytes per lattice site (FP32 fields): one link pass
 # (eo, mu) moves 68 B*V, one Higgs pass 66 B*V, the sweep 672 B*V.
 B_LINK, B_HIGGS, B_SWEEP = 68, 66, 672
+# forward FLOPs per site of the warm-start network: 4 layers of 27 offsets x
+# 16 x 16 multiply-adds
+NET_FWD_FLOP_PER_SITE = 4 * 27 * 16 * 16 * 2
 FALLBACK_HBM_GBS = 6650.0
 
 
@@ -293,6 +296,39 @@ def extras(args, peak):
         lat.close()
     except Exception as e:
         out["pipeline_256cubed"] = {"error": repr(e)[:300]}
+    # the warm-start network's training at 128^3 (its tcgen05 convolution and
+    # weight-gradient kernels): 4 recorded (configuration, transform) pairs,
+    # one untimed epoch, then 5 timed epochs of Adam steps (one per pair)
+    try:
+        from lceqcd_b200 import GaugeNet
+        L = (128, 128, 128)
+        lat = Lattice(L, **COUP, precision="f32", seed=41, lam=1.7, limit_or=1e-10)
+        lat.init_hot(42)
+        lat.sweeps(100, 0)
+        lat.landau_gauge_fourier("identity")
+        net = GaugeNet(seed=43)
+        npairs = 4
+        for _ in range(npairs):
+            lat.sweeps(10, 0)
+            lat.landau_gauge_warm(net, use_net=False, judge=False, record=True, fourier=True)
+        net.train(1, lr=1e-3)
+        epochs = 5
+        t0 = time.perf_counter()
+        net.train(epochs, lr=1e-3)  # returns after the step's loss is read back
+        t = time.perf_counter() - t0
+        steps = epochs * npairs
+        flop = 3 * NET_FWD_FLOP_PER_SITE * vol(L) * steps  # forward, input gradient, weight gradient
+        tf = flop / t / 1e12
+        bf16_peak = json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json"))).get("bf16_tflops")
+        out["net_train_128cubed"] = {"ms_per_step": t / steps * 1e3, "tflops_bf16": tf, "steps": steps,
+                                     "bound": "tensor", "peak_tflops": bf16_peak,
+                                     "frac_of_measured_bf16": tf / bf16_peak if bf16_peak else None,
+                                     "note": "host wall clock around synchronised training calls; 27 x 16 x 16 "
+                                             "per-site contractions, 3 per step"}
+        net.close()
+        lat.close()
+    except Exception as e:
+        out["net_train_128cubed"] = {"error": repr(e)[:300]}
     # batched ensemble: 96 chains (32 each of 16^3, 32^3, 48^3) over the
     # coupling grid, against the same chains run one context at a time
     try:
