@@ -820,14 +820,24 @@ int net_fail(lce_net* n, int code, const std::string& m) {
 // shared memory; tensor memory: 4 x 128 columns).  The runtime's occupancy
 // query reported 1 per SM for this kernel where the launch itself holds 4.
 static_assert(kTgMaxCtasPerSm * (kTgSmem + 1024) <= 228 * 1024, "wgrad CTAs per SM");
+static_assert(kTcCtasPerSm == kTgMaxCtasPerSm, "the convolution uses the weight gradient's grid");
+template <typename K>
+void tc_attributes(K kernel, int smem) {
+  cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+  // all of the unified L1 / shared memory as shared memory
+  cudaFuncSetAttribute(kernel, cudaFuncAttributePreferredSharedMemoryCarveout, (int)cudaSharedmemCarveoutMaxShared);
+}
+
+// the grid of the persistent tcgen05 kernels; the first call for a network
+// (on its device) also sets their shared-memory attributes there
 int wgrad_tc_grid(lce_net* n) {
   if (n->tg_grid > 0) return n->tg_grid;
   int nsm = 0;
   cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, n->device);
-  cudaFuncSetAttribute(wgrad_tc_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, kTgSmem);
-  // all of the unified L1 / shared memory as shared memory
-  cudaFuncSetAttribute(wgrad_tc_kernel, cudaFuncAttributePreferredSharedMemoryCarveout,
-                       (int)cudaSharedmemCarveoutMaxShared);
+  tc_attributes(wgrad_tc_kernel, kTgSmem);
+  tc_attributes(conv_tc_kernel<0>, kTcSmem);
+  tc_attributes(conv_tc_kernel<1>, kTcSmem);
+  tc_attributes(conv_tc_kernel<2>, kTcSmem);
   n->tg_grid = std::max(1, nsm) * kTgMaxCtasPerSm;
   return n->tg_grid;
 }
@@ -874,14 +884,7 @@ template <int MODE>
 void launch_conv(lce_net* n, const __nv_bfloat16* in, const __nv_bfloat16* W, const float* bias,
                  __nv_bfloat16* out16, float* out32, const __nv_bfloat16* mask, const NetGeom& g, cudaStream_t s) {
   if (g.L1 % 128 == 0) {
-    static bool attr = false;  // per MODE instantiation
-    if (!attr) {
-      cudaFuncSetAttribute(conv_tc_kernel<MODE>, cudaFuncAttributeMaxDynamicSharedMemorySize, kTcSmem);
-      cudaFuncSetAttribute(conv_tc_kernel<MODE>, cudaFuncAttributePreferredSharedMemoryCarveout,
-                           (int)cudaSharedmemCarveoutMaxShared);
-      attr = true;
-    }
-    // persistent CTAs, 4 per SM (as many SMs as the weight gradient uses)
+    // persistent CTAs, 4 per SM, like the weight gradient
     const int grid = std::min(wgrad_tc_grid(n), (g.L1 / 128) * g.L2 * g.L3);
     conv_tc_kernel<MODE><<<grid, 128, kTcSmem, s>>>(in, W, bias, out16, out32, mask, g, n->flag);
   } else {
