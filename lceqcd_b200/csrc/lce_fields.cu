@@ -8,6 +8,8 @@
 // [eo][k][site] SoA.
 #include <algorithm>
 
+#include <atomic>
+
 #include "lce_internal.hpp"
 
 namespace lce {
@@ -153,10 +155,10 @@ void launch_init_hot(void* u, void* a, int nh, uint32_t k0, uint32_t k1, cudaStr
 }
 // buf holds 2 x bytes: the first half is written, the second half read.
 void launch_flush(void* buf, size_t bytes, cudaStream_t s) {
-  static uint32_t tag = 1;
+  static std::atomic<uint32_t> tag{1};  // a new value per flush, from any host thread
   size_t n = bytes / sizeof(uint4);
   uint4* b = reinterpret_cast<uint4*>(buf);
-  flush_kernel<<<148 * 8, 512, 0, s>>>(b, n, tag++);
+  flush_kernel<<<148 * 8, 512, 0, s>>>(b, n, tag.fetch_add(1, std::memory_order_relaxed));
   flush_read_kernel<<<148 * 8, 512, 0, s>>>(b + n, n, reinterpret_cast<uint32_t*>(b));
 }
 

@@ -1111,6 +1111,7 @@ int lce_net_train(lce_net* n, int epochs, double lr, double* mean_loss) {
       const float c1 = 1.f - std::pow(b1, (float)n->step), c2 = 1.f - std::pow(b2, (float)n->step);
       adam_kernel<<<64, 256, 0, n->stream>>>(n->w32, n->m, n->v, n->grad, kNParam, (float)lr, b1, b2, eps, c1, c2);
       net_refresh(n, n->stream);
+      NCK(cudaGetLastError());
       std::vector<double> lp(ceil_div(ns, 256));
       NCK(cudaMemcpyAsync(lp.data(), n->part, lp.size() * sizeof(double), cudaMemcpyDeviceToHost, n->stream));
       NCK(cudaStreamSynchronize(n->stream));
