@@ -24,10 +24,16 @@
 // theta; (2) the check (sum, count, done flag);
 // (3) forward FFT along y; (4) forward FFT along z, scale, inverse FFT along
 // z; (5) inverse FFT along y; (6) inverse FFT along x + build g; (7) apply g to
-// U_f, A_f and the tracked transform G.  The FFTs are radix-2 in shared
-// memory over a block of lines (1024 complex points per block; lines padded
-// by one element against bank conflicts; radix-4 levels); extents must be
-// powers of two up to 1024.  The divergence, g and its application to the fields are FP64 for
+// U_f, A_f and the tracked transform G.  A block transforms 4096 complex
+// points (lines of one axis, one or both fields).  A line of n = N1 x N2
+// points is transformed in two steps through shared memory: N2 threads each
+// take N1 points of stride N2 into registers, do an N1-point DFT there
+// (radix-2 butterflies, fully unrolled), multiply by the twiddles
+// W_n^(n2 k1) and store a row; then N1 threads each take a row of N2 points,
+// do the N2-point DFT and store the results in natural order (N1, N2 <= 32).
+// Threads walk the lines fastest, and the padded line strides keep the
+// shared-memory accesses free of bank conflicts.  The FFTs are in shared
+// memory over a block of lines; extents must be powers of two up to 1024.  The divergence, g and its application to the fields are FP64 for
 // either field precision (rounding the step's rotation to FP32 before
 // applying it slowed the iteration below theta ~ 1e-8 at 64^3); the
 // transforms themselves are FP32.  Two complex fields carry the three components:
@@ -45,11 +51,11 @@ constexpr int kFaThreads = 256;
 // counts as FP64 transforms at 64^3-256^3, 20-30% less time per iteration)
 using FftR = float;
 using FftC = float2;
-// complex points per block and field, and the padded shared-memory size
+// longest line (and size of the twiddle table exp(-2 pi i k / kFaPoints))
 constexpr int kFaPoints = 1024;
-constexpr int kFaLogPoints = 10;
-static_assert(1 << kFaLogPoints == kFaPoints, "points per block");
-constexpr int kFaSmem = kFaPoints + kFaPoints / 2;
+// complex points transformed per block (all fields), 2^kFaBlockLog
+constexpr int kFaBlockLog = 12;
+constexpr int kFaBlockPts = 1 << kFaBlockLog;
 
 template <typename T>
 __device__ __forceinline__ T cadd(T a, T b) { return T{a.x + b.x, a.y + b.y}; }
@@ -69,46 +75,117 @@ __device__ __forceinline__ void load_twiddles(FftC* tw, const double2* tg, int n
   }
 }
 
-// In-place decimation-in-time FFT of nl lines of length n = 2^logn held in
-// shared memory at d[j*(n+1) + k], input in bit-reversed order, output
-// natural.  Levels are fused in pairs (radix 4: two radix-2 levels per item,
-// in registers) after one radix-2 level when logn is odd; tw[k] = exp(sign 2
-// pi i k / n), k < n/2.  Ends with __syncthreads.
-template <typename T>
-__device__ __forceinline__ void fft_lines(T* d, int nl, int logn, const T* tw) {
-  const int n = 1 << logn, ld = n + 1;
-  int st = 0;
-  if (logn & 1) {
-    // level 0: pairs (2i, 2i+1), twiddle 1
-    const int hn = n >> 1, nb = nl * hn;
-    for (int b = threadIdx.x; b < nb; b += blockDim.x) {
-      const int p = (b >> (logn - 1)) * ld + 2 * (b & (hn - 1));
-      const T u = d[p], v = d[p + 1];
-      d[p] = cadd(u, v);
-      d[p + 1] = csub(u, v);
-    }
-    __syncthreads();
-    st = 1;
+// n = 2^LOGN = N1 x N2, N1 points per thread in the first step
+template <int LOGN>
+struct FaLines {
+  static constexpr int n = 1 << LOGN;
+  static constexpr int N1 = LOGN <= 4 ? n : (LOGN <= 8 ? 16 : 32);
+  static constexpr int N2 = n / N1;
+  static constexpr int NLT = kFaBlockPts >> LOGN;               // lines per block (all fields)
+  static constexpr int ld = n + 1;                               // line stride
+  static constexpr int ldm = N2 > 1 ? N1 * (N2 + 1) + 1 : 0;     // intermediate line stride
+  static constexpr int ntw = n / 2 > 0 ? n / 2 : 1;              // twiddle table entries
+  // lines, intermediate rows, ntab twiddle tables and nd doubles
+  static constexpr size_t smem(int ntab, int nd) {
+    return ((size_t)NLT * (ld + ldm) + (size_t)ntab * ntw) * sizeof(FftC) + (size_t)nd * sizeof(double);
   }
-  for (; st < logn; st += 2) {
-    // levels st (pairs at distance m) and st + 1 (distance 2m) on groups of 4m
-    const int m = 1 << st, q = n >> 2, nb = nl * q;
-    const int t1 = n >> (st + 1), t2 = n >> (st + 2);
-    for (int b = threadIdx.x; b < nb; b += blockDim.x) {
-      const int r = b & (q - 1), i = r & (m - 1);
-      const int base = (b >> (logn - 2)) * ld + (r >> st) * 4 * m + i;
-      const T a0 = d[base], a1 = d[base + m], a2 = d[base + 2 * m], a3 = d[base + 3 * m];
-      const T w = tw[i * t1];
-      const T wa1 = cmul(w, a1), wa3 = cmul(w, a3);
-      const T b0 = cadd(a0, wa1), b1 = csub(a0, wa1), b2 = cadd(a2, wa3), b3 = csub(a2, wa3);
-      const T x2 = cmul(tw[i * t2], b2), x3 = cmul(tw[(i + m) * t2], b3);
-      d[base] = cadd(b0, x2);
-      d[base + 2 * m] = csub(b0, x2);
-      d[base + m] = cadd(b1, x3);
-      d[base + 3 * m] = csub(b1, x3);
+};
+
+__host__ __device__ constexpr int cbrev(int k, int bits) {
+  int r = 0;
+  for (int i = 0; i < bits; ++i) r = (r << 1) | ((k >> i) & 1);
+  return r;
+}
+template <int N>
+struct ILog2 {
+  static constexpr int v = 1 + ILog2<N / 2>::v;
+};
+template <>
+struct ILog2<1> {
+  static constexpr int v = 0;
+};
+
+// radix-2 stages S, S+1, ... of an N-point decimation-in-time DFT in
+// registers; one loop of constant trip count per stage, so that every index
+// is a compile-time constant after unrolling.  tw[k] = exp(sign 2 pi i k / n),
+// k < n/2: W_2m^j = tw[j n / 2m].
+template <int N, int n, int S>
+__device__ __forceinline__ void dft_stages(FftC (&t)[N], const FftC* tw) {
+  if constexpr ((1 << S) < N) {
+    constexpr int m = 1 << S;
+#pragma unroll
+    for (int b = 0; b < N / 2; ++b) {
+      const int j = b % m, k = (b / m) * 2 * m;
+      FftC u = t[k + j + m];
+      if (j > 0) u = cmul(tw[j * (n / (2 * m))], u);
+      t[k + j + m] = csub(t[k + j], u);
+      t[k + j] = cadd(t[k + j], u);
     }
-    __syncthreads();
+    dft_stages<N, n, S + 1>(t, tw);
   }
+}
+
+// N-point DFT in registers, natural order in and out (decimation in time on
+// the bit-reversed copy)
+template <int N, int n>
+__device__ __forceinline__ void dft_reg(FftC (&v)[N], const FftC* tw) {
+  constexpr int LG = ILog2<N>::v;
+  FftC t[N];
+#pragma unroll
+  for (int i = 0; i < N; ++i) t[cbrev(i, LG)] = v[i];
+  dft_stages<N, n, 0>(t, tw);
+#pragma unroll
+  for (int i = 0; i < N; ++i) v[i] = t[i];
+}
+
+// In-place FFT of the block's NLT lines at d[j*ld + x] (natural order in and
+// out), through the intermediate rows mid.  Ends with __syncthreads.
+template <int LOGN>
+__device__ __forceinline__ void fft2_lines(FftC* d, FftC* mid, const FftC* tw) {
+  using G = FaLines<LOGN>;
+  constexpr int n = G::n, N1 = G::N1, N2 = G::N2, NLT = G::NLT, ld = G::ld, ldm = G::ldm;
+  // step 1: item (line j, column n2), lines fastest
+  for (int it = threadIdx.x; it < NLT * N2; it += blockDim.x) {
+    const int j = it % NLT, n2 = it / NLT;
+    const FftC* src = d + j * ld + n2;
+    FftC v[N1];
+#pragma unroll
+    for (int i = 0; i < N1; ++i) v[i] = src[i * N2];
+    dft_reg<N1, n>(v, tw);
+    if constexpr (N2 == 1) {
+      FftC* dst = d + j * ld;
+#pragma unroll
+      for (int k = 0; k < N1; ++k) dst[k] = v[k];
+    } else {
+      FftC* dst = mid + j * ldm + n2;
+#pragma unroll
+      for (int k1 = 0; k1 < N1; ++k1) {
+        FftC y = v[k1];
+        if (k1 > 0) {
+          const int e = n2 * k1;  // < n; W_n^e = -W_n^(e - n/2) for e >= n/2
+          const FftC w = e < n / 2 ? tw[e] : FftC{-tw[e - n / 2].x, -tw[e - n / 2].y};
+          y = cmul(w, y);
+        }
+        dst[k1 * (N2 + 1)] = y;
+      }
+    }
+  }
+  if constexpr (N2 > 1) {
+    __syncthreads();
+    // step 2: item (line j, row k1): X[k1 + N1 k2]
+    for (int it = threadIdx.x; it < NLT * N1; it += blockDim.x) {
+      const int j = it % NLT, k1 = it / NLT;
+      const FftC* src = mid + j * ldm + k1 * (N2 + 1);
+      FftC v[N2];
+#pragma unroll
+      for (int i = 0; i < N2; ++i) v[i] = src[i];
+      dft_reg<N2, n>(v, tw);
+      FftC* dst = d + j * ld + k1;
+#pragma unroll
+      for (int k2 = 0; k2 < N2; ++k2) dst[k2 * N1] = v[k2];
+    }
+  }
+  __syncthreads();
 }
 
 template <typename R>
@@ -119,8 +196,6 @@ template <typename R>
 __device__ __forceinline__ su2<R> to_r(su2<double> u) {
   return su2<R>{{(R)u.a.re, (R)u.a.im}, {(R)u.b.re, (R)u.b.im}};
 }
-
-__device__ __forceinline__ int brev(int k, int logn) { return logn ? (int)(__brev((unsigned)k) >> (32 - logn)) : 0; }
 
 struct FaArgs {
   const ChainDev* ch;
@@ -147,23 +222,27 @@ __device__ __forceinline__ size_t nat_index(const FaArgs& a, int l, int k) {
   return ((((size_t)k << s2) + (l >> s1)) << s1) + (l & m1);                          // l = x + L1 y
 }
 
-// (1) Delta on x-lines, forward FFT along x; partials of theta
-template <typename R>
+// (1) Delta on x-lines, forward FFT along x; partials of theta.  A block
+// takes NL x-lines of both fields: lines 0 .. NL-1 hold Delta_b, NL .. 2NL-1
+// hold Delta_a3.
+template <typename R, int LOGN>
 __global__ void __launch_bounds__(kFaThreads) fa_div_kernel(FaArgs a) {
-  using T = FftC;
-  __shared__ T sm[2][kFaSmem];
-  __shared__ T tw[kFaPoints / 2];
+  using G = FaLines<LOGN>;
+  constexpr int n = G::n, ld = G::ld, NL = G::NLT / 2;
+  extern __shared__ __align__(16) FftC fa_sm[];
+  FftC* d = fa_sm;
+  FftC* mid = d + G::NLT * ld;
+  FftC* tw = mid + G::NLT * G::ldm;
   if (fa_done(a)) return;
   const ChainDev& ch = *a.ch;
-  const int n = a.L[0], logn = a.logL[0], ld = n + 1;
-  const int nl = kFaPoints >> logn, nlines = a.L[1] * a.L[2];
-  const int l0 = blockIdx.x * nl;
+  const int nlines = a.L[1] * a.L[2];
+  const int l0 = blockIdx.x * NL;
   load_twiddles(tw, a.tw, n, -1);
   const double al = ch.alpha;
   double q[1] = {0.0};
-  for (int e = threadIdx.x; e < nl * n; e += blockDim.x) {
-    const int j = e >> logn, x = e & (n - 1), l = l0 + j;
-    T v0{0, 0}, v1{0, 0};
+  for (int e = threadIdx.x; e < NL * n; e += blockDim.x) {
+    const int j = e >> LOGN, x = e & (n - 1), l = l0 + j;
+    FftC v0{0, 0}, v1{0, 0};
     if (l < nlines) {
       const int y = l & (a.L[1] - 1), z = l >> a.logL[1];
       const int p = (x + y + z) & 1, op = 1 - p;
@@ -182,25 +261,23 @@ __global__ void __launch_bounds__(kFaThreads) fa_div_kernel(FaArgs a) {
         dbi += c * ((double)u.b.im - (double)w.b.im);
       }
       if (p == 1) q[0] += d3 * d3 + dbr * dbr + dbi * dbi;
-      v0 = T{(FftR)dbr, (FftR)dbi};
-      v1 = T{(FftR)d3, (FftR)0};
+      v0 = FftC{(FftR)dbr, (FftR)dbi};
+      v1 = FftC{(FftR)d3, (FftR)0};
     }
-    const int pos = j * ld + brev(x, logn);
-    sm[0][pos] = v0;
-    sm[1][pos] = v1;
+    d[j * ld + x] = v0;
+    d[(NL + j) * ld + x] = v1;
   }
   block_reduce_store<1>(q, a.part + blockIdx.x);
   __syncthreads();
-  fft_lines<T>(sm[0], nl, logn, tw);
-  fft_lines<T>(sm[1], nl, logn, tw);
+  fft2_lines<LOGN>(d, mid, tw);
   const size_t V = (size_t)a.L[0] * a.L[1] * a.L[2];
-  T* F = reinterpret_cast<T*>(a.fft);
-  for (int e = threadIdx.x; e < nl * n; e += blockDim.x) {
-    const int j = e >> logn, k = e & (n - 1), l = l0 + j;
+  FftC* F = reinterpret_cast<FftC*>(a.fft);
+  for (int e = threadIdx.x; e < NL * n; e += blockDim.x) {
+    const int j = e >> LOGN, k = e & (n - 1), l = l0 + j;
     if (l >= nlines) continue;
     const size_t gi = nat_index<0>(a, l, k);
-    F[gi] = sm[0][j * ld + k];
-    F[V + gi] = sm[1][j * ld + k];
+    F[gi] = d[j * ld + k];
+    F[V + gi] = d[(NL + j) * ld + k];
   }
 }
 
@@ -226,24 +303,24 @@ __global__ void __launch_bounds__(1024) fa_check_kernel(const ChainDev* chp, Cha
   }
 }
 
-// (3)-(5) FFT of both fields along axis AX (1: y, 2: z); for AX = 2 with
-// SCALE: forward, multiply by gamma / (p_c^2 V), inverse
-template <typename R, int AX, int SIGN, bool SCALE>
+// (3)-(5) FFT of one field (blockIdx.y) along axis AX (1: y, 2: z); for
+// AX = 2 with SCALE: forward, multiply by gamma / (p_c^2 V), inverse
+template <int AX, int SIGN, bool SCALE, int LOGN>
 __global__ void __launch_bounds__(kFaThreads) fa_fft_kernel(FaArgs a) {
-  using T = FftC;
-  __shared__ T sm[kFaSmem];
-  __shared__ T tw[kFaPoints / 2];
-  __shared__ T twi[SCALE ? kFaPoints / 2 : 1];
+  using G = FaLines<LOGN>;
+  constexpr int n = G::n, ld = G::ld, NL = G::NLT, LNL = kFaBlockLog - LOGN;
+  extern __shared__ __align__(16) FftC fa_sm[];
+  FftC* d = fa_sm;
+  FftC* mid = d + NL * ld;
+  FftC* tw = mid + NL * G::ldm;
+  FftC* twi = tw + G::ntw;                                       // SCALE: inverse twiddles
+  double* sz2 = reinterpret_cast<double*>(twi + G::ntw);         // SCALE: alpha sin^2(pi kz / L3)
+  double* sxy = sz2 + n;                                         // SCALE: sin^2(pi kx/L1) + sin^2(pi ky/L2)
   if (fa_done(a)) return;
-  const int n = a.L[AX], logn = a.logL[AX], ld = n + 1;
-  const int lnl = kFaLogPoints - logn, nl = 1 << lnl;
-  const int nlines = (a.L[0] * a.L[1] * a.L[2]) >> logn;
-  const int l0 = blockIdx.x * nl;
-  const int fld = blockIdx.y;
+  const int nlines = (a.L[0] * a.L[1] * a.L[2]) >> LOGN;
+  const int l0 = blockIdx.x * NL;
   const size_t V = (size_t)a.L[0] * a.L[1] * a.L[2];
-  T* F = reinterpret_cast<T*>(a.fft) + fld * V;
-  __shared__ double sz2[SCALE ? kFaPoints : 1];  // alpha sin^2(pi kz / L3)
-  __shared__ double sxy[SCALE ? kFaPoints : 1];  // sin^2(pi kx / L1) + sin^2(pi ky / L2) per line
+  FftC* F = reinterpret_cast<FftC*>(a.fft) + blockIdx.y * V;
   load_twiddles(tw, a.tw, n, SIGN);
   if (SCALE) {
     load_twiddles(twi, a.tw, n, -SIGN);
@@ -252,86 +329,77 @@ __global__ void __launch_bounds__(kFaThreads) fa_fft_kernel(FaArgs a) {
       const double sz = sinpi_r((double)k / a.L[2]);
       sz2[k] = al * sz * sz;
     }
-    for (int j = threadIdx.x; j < nl; j += blockDim.x) {
+    for (int j = threadIdx.x; j < NL; j += blockDim.x) {
       const int l = l0 + j, kx = l & (a.L[0] - 1), ky = l >> a.logL[0];
       const double sx = sinpi_r((double)kx / a.L[0]), sy = sinpi_r((double)ky / a.L[1]);
       sxy[j] = sx * sx + sy * sy;
     }
   }
-  // element e -> (line j = e % nl, position k = e / nl): consecutive threads
+  // element e -> (line j = e % NL, position k = e / NL): consecutive threads
   // read consecutive lines, i.e. consecutive x
-  for (int e = threadIdx.x; e < nl * n; e += blockDim.x) {
-    const int j = e & (nl - 1), k = e >> lnl, l = l0 + j;
-    sm[j * ld + brev(k, logn)] = l < nlines ? F[nat_index<AX>(a, l, k)] : T{0, 0};
+  for (int e = threadIdx.x; e < NL * n; e += blockDim.x) {
+    const int j = e & (NL - 1), k = e >> LNL, l = l0 + j;
+    d[j * ld + k] = l < nlines ? F[nat_index<AX>(a, l, k)] : FftC{0, 0};
   }
   __syncthreads();
-  fft_lines<T>(sm, nl, logn, tw);
+  fft2_lines<LOGN>(d, mid, tw);
   if (SCALE) {
     const double gv = (a.cst ? a.cst->gf_step : a.gamma) / (4.0 * (double)V);
-    for (int e = threadIdx.x; e < nl * n; e += blockDim.x) {
-      const int j = e >> logn, kz = e & (n - 1), l = l0 + j;
+    for (int e = threadIdx.x; e < NL * n; e += blockDim.x) {
+      const int j = e >> LOGN, kz = e & (n - 1), l = l0 + j;
       const double p2 = sxy[j] + sz2[kz];
       const double m = (l | kz) ? gv / p2 : 0.0;
       const int q = j * ld + kz;
-      sm[q] = T{(FftR)(sm[q].x * m), (FftR)(sm[q].y * m)};
+      d[q] = FftC{(FftR)(d[q].x * m), (FftR)(d[q].y * m)};
     }
     __syncthreads();
-    // bit-reverse permutation for the inverse transform
-    for (int e = threadIdx.x; e < nl * n; e += blockDim.x) {
-      const int j = e >> logn, k = e & (n - 1), r = brev(k, logn);
-      if (r > k) {
-        const T t = sm[j * ld + k];
-        sm[j * ld + k] = sm[j * ld + r];
-        sm[j * ld + r] = t;
-      }
-    }
-    __syncthreads();
-    fft_lines<T>(sm, nl, logn, twi);
+    fft2_lines<LOGN>(d, mid, twi);
   }
-  for (int e = threadIdx.x; e < nl * n; e += blockDim.x) {
-    const int j = e & (nl - 1), k = e >> lnl, l = l0 + j;
-    if (l < nlines) F[nat_index<AX>(a, l, k)] = sm[j * ld + k];
+  for (int e = threadIdx.x; e < NL * n; e += blockDim.x) {
+    const int j = e & (NL - 1), k = e >> LNL, l = l0 + j;
+    if (l < nlines) F[nat_index<AX>(a, l, k)] = d[j * ld + k];
   }
 }
 
 // (6) inverse FFT along x; g(x) = exp(-i omega.sigma) per site
-template <typename R>
+template <typename R, int LOGN>
 __global__ void __launch_bounds__(kFaThreads) fa_g_kernel(FaArgs a) {
-  using T = FftC;
-  __shared__ T sm[2][kFaSmem];
-  __shared__ T tw[kFaPoints / 2];
+  using G = FaLines<LOGN>;
+  constexpr int n = G::n, ld = G::ld, NL = G::NLT / 2;
+  extern __shared__ __align__(16) FftC fa_sm[];
+  FftC* d = fa_sm;
+  FftC* mid = d + G::NLT * ld;
+  FftC* tw = mid + G::NLT * G::ldm;
   if (fa_done(a)) return;
   const ChainDev& ch = *a.ch;
-  const int n = a.L[0], logn = a.logL[0], ld = n + 1;
-  const int nl = kFaPoints >> logn, nlines = a.L[1] * a.L[2];
-  const int l0 = blockIdx.x * nl;
+  const int nlines = a.L[1] * a.L[2];
+  const int l0 = blockIdx.x * NL;
   const size_t V = (size_t)a.L[0] * a.L[1] * a.L[2];
-  const T* F = reinterpret_cast<const T*>(a.fft);
+  const FftC* F = reinterpret_cast<const FftC*>(a.fft);
   load_twiddles(tw, a.tw, n, +1);
-  for (int e = threadIdx.x; e < nl * n; e += blockDim.x) {
-    const int j = e >> logn, k = e & (n - 1), l = l0 + j;
+  for (int e = threadIdx.x; e < NL * n; e += blockDim.x) {
+    const int j = e >> LOGN, k = e & (n - 1), l = l0 + j;
     const size_t gi = l < nlines ? nat_index<0>(a, l, k) : 0;
-    sm[0][j * ld + brev(k, logn)] = l < nlines ? F[gi] : T{0, 0};
-    sm[1][j * ld + brev(k, logn)] = l < nlines ? F[V + gi] : T{0, 0};
+    d[j * ld + k] = l < nlines ? F[gi] : FftC{0, 0};
+    d[(NL + j) * ld + k] = l < nlines ? F[V + gi] : FftC{0, 0};
   }
   __syncthreads();
-  fft_lines<T>(sm[0], nl, logn, tw);
-  fft_lines<T>(sm[1], nl, logn, tw);
-  for (int e = threadIdx.x; e < nl * n; e += blockDim.x) {
-    const int j = e >> logn, x = e & (n - 1), l = l0 + j;
+  fft2_lines<LOGN>(d, mid, tw);
+  for (int e = threadIdx.x; e < NL * n; e += blockDim.x) {
+    const int j = e >> LOGN, x = e & (n - 1), l = l0 + j;
     if (l >= nlines) continue;
     const int y = l & (a.L[1] - 1), z = l >> a.logL[1];
     const int p = (x + y + z) & 1, s = site_index(x, y, z, ch.hx, ch.nxy);
-    const double w3 = sm[1][j * ld + x].x, wbr = sm[0][j * ld + x].x, wbi = sm[0][j * ld + x].y;
+    const double w3 = d[(NL + j) * ld + x].x, wbr = d[j * ld + x].x, wbi = d[j * ld + x].y;
     const double nw = sqrt(w3 * w3 + wbr * wbr + wbi * wbi);
-    su2<double> g{{1.0, 0.0}, {0.0, 0.0}};
+    su2<double> gg{{1.0, 0.0}, {0.0, 0.0}};
     if (nw > 0.0) {
       double sn, cs;
       sincos(nw, &sn, &cs);
       const double f = sn / nw;
-      g = su2<double>{{cs, -f * w3}, {-f * wbr, -f * wbi}};
+      gg = su2<double>{{cs, -f * w3}, {-f * wbr, -f * wbi}};
     }
-    LinkIO<double>::st(a.gstep, (size_t)p * ch.nh + s, g);
+    LinkIO<double>::st(a.gstep, (size_t)p * ch.nh + s, gg);
     if (a.omega_out) {
       double* o = a.omega_out + ((size_t)p * ch.nh + s) * 3;
       o[0] = (double)w3;
@@ -419,8 +487,46 @@ void fa_init_table(void* buf, size_t vcap, cudaStream_t s) {
   fa_twiddle_table_kernel<<<1, kFaPoints / 2, 0, s>>>(fa_table(buf, vcap));
 }
 
-template <typename R>
-int fa_blocks_div(const ChainDev& ch) { return ceil_div((long)ch.L2 * ch.L3, kFaPoints / ch.L1); }
+// launchers per line length (the kernels are compiled for each power of two)
+template <typename K>
+void fa_launch(K kernel, dim3 grid, size_t smem, const FaArgs& a, cudaStream_t s) {
+  cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  kernel<<<grid, kFaThreads, smem, s>>>(a);
+}
+template <typename R, int LOGN>
+void fa_div_launch(const FaArgs& a, int nb, cudaStream_t s) {
+  fa_launch(fa_div_kernel<R, LOGN>, dim3(nb), FaLines<LOGN>::smem(1, 0), a, s);
+}
+template <typename R, int LOGN>
+void fa_g_launch(const FaArgs& a, int nb, cudaStream_t s) {
+  fa_launch(fa_g_kernel<R, LOGN>, dim3(nb), FaLines<LOGN>::smem(1, 0), a, s);
+}
+template <int AX, int SIGN, bool SCALE, int LOGN>
+void fa_fft_launch(const FaArgs& a, int nb, cudaStream_t s) {
+  using G = FaLines<LOGN>;
+  fa_launch(fa_fft_kernel<AX, SIGN, SCALE, LOGN>, dim3(nb, 2), G::smem(SCALE ? 2 : 1, SCALE ? G::n + G::NLT : 0), a,
+            s);
+}
+#define LCE_FA_SWITCH(logn, CALL) \
+  switch (logn) {                 \
+    case 1: CALL(1); break;       \
+    case 2: CALL(2); break;       \
+    case 3: CALL(3); break;       \
+    case 4: CALL(4); break;       \
+    case 5: CALL(5); break;       \
+    case 6: CALL(6); break;       \
+    case 7: CALL(7); break;       \
+    case 8: CALL(8); break;       \
+    case 9: CALL(9); break;       \
+    case 10: CALL(10); break;     \
+    default: break;               \
+  }
+
+// blocks of a transform kernel over lines of length 2^logn (all fields of
+// the block share its 4096 points)
+int fa_blocks(long nlines, int logn, int fields) {
+  return ceil_div(nlines, (long)(kFaBlockPts >> logn) / fields);
+}
 
 // enqueue one Fourier-accelerated iteration (kernels 1-7)
 template <typename R>
@@ -442,15 +548,24 @@ void launch_fa_iteration(const ChainDev* chd, const ChainDev& ch, ChainState* cs
   a.L[2] = ch.L3;
   for (int d = 0; d < 3; ++d) a.logL[d] = ilog2_exact(a.L[d]);
   a.track = track;
-  const int nbd = fa_blocks_div<R>(ch);
-  fa_div_kernel<R><<<nbd, kFaThreads, 0, s>>>(a);
+  const int nbd = fa_blocks((long)ch.L2 * ch.L3, a.logL[0], 2);
+#define LCE_FA_DIV(L) fa_div_launch<R, L>(a, nbd, s)
+  LCE_FA_SWITCH(a.logL[0], LCE_FA_DIV)
+#undef LCE_FA_DIV
   if (with_check) fa_check_kernel<<<1, 1024, 0, s>>>(chd, cst, part, nbd);
-  constexpr int P = kFaPoints;
-  const dim3 gy(ceil_div((long)V / ch.L2, P / ch.L2), 2), gz(ceil_div((long)V / ch.L3, P / ch.L3), 2);
-  fa_fft_kernel<R, 1, -1, false><<<gy, kFaThreads, 0, s>>>(a);
-  fa_fft_kernel<R, 2, -1, true><<<gz, kFaThreads, 0, s>>>(a);
-  fa_fft_kernel<R, 1, +1, false><<<gy, kFaThreads, 0, s>>>(a);
-  fa_g_kernel<R><<<nbd, kFaThreads, 0, s>>>(a);
+  const int nby = fa_blocks((long)V / ch.L2, a.logL[1], 1), nbz = fa_blocks((long)V / ch.L3, a.logL[2], 1);
+#define LCE_FA_Y(L) fa_fft_launch<1, -1, false, L>(a, nby, s)
+  LCE_FA_SWITCH(a.logL[1], LCE_FA_Y)
+#undef LCE_FA_Y
+#define LCE_FA_Z(L) fa_fft_launch<2, -1, true, L>(a, nbz, s)
+  LCE_FA_SWITCH(a.logL[2], LCE_FA_Z)
+#undef LCE_FA_Z
+#define LCE_FA_YI(L) fa_fft_launch<1, +1, false, L>(a, nby, s)
+  LCE_FA_SWITCH(a.logL[1], LCE_FA_YI)
+#undef LCE_FA_YI
+#define LCE_FA_G(L) fa_g_launch<R, L>(a, nbd, s)
+  LCE_FA_SWITCH(a.logL[0], LCE_FA_G)
+#undef LCE_FA_G
   if (with_apply) fa_apply_kernel<R><<<ceil_div((long)V, kBlock), kBlock, 0, s>>>(a);
 }
 
