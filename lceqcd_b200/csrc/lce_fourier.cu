@@ -25,16 +25,17 @@
 // (3) forward FFT along y; (4) forward FFT along z, scale, inverse FFT along
 // z; (5) inverse FFT along y; (6) inverse FFT along x + build g; (7) apply g to
 // U_f, A_f and the tracked transform G.  A block transforms 4096 complex
-// points (lines of one axis, one or both fields).  A line of n = N1 x N2
-// points is transformed in two steps through shared memory: N2 threads each
+// points (lines of one axis, one or both fields) held in shared memory.  A
+// line of n = N1 x N2 points is transformed in two steps: N2 threads each
 // take N1 points of stride N2 into registers, do an N1-point DFT there
 // (radix-2 butterflies, fully unrolled), multiply by the twiddles
 // W_n^(n2 k1) and store a row; then N1 threads each take a row of N2 points,
 // do the N2-point DFT and store the results in natural order (N1, N2 <= 32).
-// Threads walk the lines fastest, and the padded line strides keep the
-// shared-memory accesses free of bank conflicts.  The FFTs are in shared
-// memory over a block of lines; extents must be powers of two up to 1024.  The divergence, g and its application to the fields are FP64 for
-// either field precision (rounding the step's rotation to FP32 before
+// Both steps read into registers before writing, so the two layouts share
+// the buffer.  Threads walk the lines fastest, and the padded line stride
+// keeps the shared-memory accesses free of bank conflicts.  Extents must be
+// powers of two up to 1024.  The divergence, g and its application to the
+// fields are FP64 for either field precision (rounding the step's rotation to FP32 before
 // applying it slowed the iteration below theta ~ 1e-8 at 64^3); the
 // transforms themselves are FP32.  Two complex fields carry the three components:
 // (Delta_b) and (Delta_a3 + 0i); the multiplier is real and even in p, so the
@@ -82,12 +83,16 @@ struct FaLines {
   static constexpr int N1 = LOGN <= 4 ? n : (LOGN <= 8 ? 16 : 32);
   static constexpr int N2 = n / N1;
   static constexpr int NLT = kFaBlockPts >> LOGN;               // lines per block (all fields)
-  static constexpr int ld = n + 1;                               // line stride
-  static constexpr int ldm = N2 > 1 ? N1 * (N2 + 1) + 1 : 0;     // intermediate line stride
+  // line stride: a line in natural order, or (between the two steps) N1 rows
+  // of N2 points, each row padded by one; n + N1 + 1 = 2 mod 32 words apart
+  static constexpr int ld = N2 > 1 ? N1 * (N2 + 1) + 1 : n + 1;
   static constexpr int ntw = n / 2 > 0 ? n / 2 : 1;              // twiddle table entries
-  // lines, intermediate rows, ntab twiddle tables and nd doubles
+  // items per thread of the two steps
+  static constexpr int IA = (NLT * N2 + kFaThreads - 1) / kFaThreads;
+  static constexpr int IB = (NLT * N1 + kFaThreads - 1) / kFaThreads;
+  // lines, ntab twiddle tables and nd doubles
   static constexpr size_t smem(int ntab, int nd) {
-    return ((size_t)NLT * (ld + ldm) + (size_t)ntab * ntw) * sizeof(FftC) + (size_t)nd * sizeof(double);
+    return ((size_t)NLT * ld + (size_t)ntab * ntw) * sizeof(FftC) + (size_t)nd * sizeof(double);
   }
 };
 
@@ -139,50 +144,75 @@ __device__ __forceinline__ void dft_reg(FftC (&v)[N], const FftC* tw) {
 }
 
 // In-place FFT of the block's NLT lines at d[j*ld + x] (natural order in and
-// out), through the intermediate rows mid.  Ends with __syncthreads.
+// out).  Each step reads its items into registers, transforms them, waits for
+// the block and writes back, so the two layouts share one buffer.  Ends with
+// __syncthreads.
 template <int LOGN>
-__device__ __forceinline__ void fft2_lines(FftC* d, FftC* mid, const FftC* tw) {
+__device__ __forceinline__ void fft2_lines(FftC* d, const FftC* tw) {
   using G = FaLines<LOGN>;
-  constexpr int n = G::n, N1 = G::N1, N2 = G::N2, NLT = G::NLT, ld = G::ld, ldm = G::ldm;
-  // step 1: item (line j, column n2), lines fastest
-  for (int it = threadIdx.x; it < NLT * N2; it += blockDim.x) {
-    const int j = it % NLT, n2 = it / NLT;
-    const FftC* src = d + j * ld + n2;
-    FftC v[N1];
+  constexpr int n = G::n, N1 = G::N1, N2 = G::N2, NLT = G::NLT, ld = G::ld;
+  if constexpr (N2 == 1) {
+    // one thread per line
+    for (int j = threadIdx.x; j < NLT; j += blockDim.x) {
+      FftC v[N1];
 #pragma unroll
-    for (int i = 0; i < N1; ++i) v[i] = src[i * N2];
-    dft_reg<N1, n>(v, tw);
-    if constexpr (N2 == 1) {
-      FftC* dst = d + j * ld;
+      for (int i = 0; i < N1; ++i) v[i] = d[j * ld + i];
+      dft_reg<N1, n>(v, tw);
 #pragma unroll
-      for (int k = 0; k < N1; ++k) dst[k] = v[k];
-    } else {
-      FftC* dst = mid + j * ldm + n2;
+      for (int k = 0; k < N1; ++k) d[j * ld + k] = v[k];
+    }
+  } else {
+    // step 1: item (line j, column n2), lines fastest: N1 points of stride N2,
+    // DFT, twiddles W_n^(n2 k1); stored as row k1, column n2
+    FftC r[G::IA][N1];
 #pragma unroll
-      for (int k1 = 0; k1 < N1; ++k1) {
-        FftC y = v[k1];
-        if (k1 > 0) {
+    for (int q = 0; q < G::IA; ++q) {
+      const int it = threadIdx.x + q * kFaThreads;
+      if (it < NLT * N2) {
+        const int j = it % NLT, n2 = it / NLT;
+#pragma unroll
+        for (int i = 0; i < N1; ++i) r[q][i] = d[j * ld + i * N2 + n2];
+        dft_reg<N1, n>(r[q], tw);
+#pragma unroll
+        for (int k1 = 1; k1 < N1; ++k1) {
           const int e = n2 * k1;  // < n; W_n^e = -W_n^(e - n/2) for e >= n/2
           const FftC w = e < n / 2 ? tw[e] : FftC{-tw[e - n / 2].x, -tw[e - n / 2].y};
-          y = cmul(w, y);
+          r[q][k1] = cmul(w, r[q][k1]);
         }
-        dst[k1 * (N2 + 1)] = y;
       }
     }
-  }
-  if constexpr (N2 > 1) {
     __syncthreads();
-    // step 2: item (line j, row k1): X[k1 + N1 k2]
-    for (int it = threadIdx.x; it < NLT * N1; it += blockDim.x) {
-      const int j = it % NLT, k1 = it / NLT;
-      const FftC* src = mid + j * ldm + k1 * (N2 + 1);
-      FftC v[N2];
 #pragma unroll
-      for (int i = 0; i < N2; ++i) v[i] = src[i];
-      dft_reg<N2, n>(v, tw);
-      FftC* dst = d + j * ld + k1;
+    for (int q = 0; q < G::IA; ++q) {
+      const int it = threadIdx.x + q * kFaThreads;
+      if (it < NLT * N2) {
+        const int j = it % NLT, n2 = it / NLT;
 #pragma unroll
-      for (int k2 = 0; k2 < N2; ++k2) dst[k2 * N1] = v[k2];
+        for (int k1 = 0; k1 < N1; ++k1) d[j * ld + k1 * (N2 + 1) + n2] = r[q][k1];
+      }
+    }
+    __syncthreads();
+    // step 2: item (line j, row k1): N2-point DFT, X[k1 + N1 k2] in natural order
+    FftC w2[G::IB][N2];
+#pragma unroll
+    for (int q = 0; q < G::IB; ++q) {
+      const int it = threadIdx.x + q * kFaThreads;
+      if (it < NLT * N1) {
+        const int j = it % NLT, k1 = it / NLT;
+#pragma unroll
+        for (int i = 0; i < N2; ++i) w2[q][i] = d[j * ld + k1 * (N2 + 1) + i];
+        dft_reg<N2, n>(w2[q], tw);
+      }
+    }
+    __syncthreads();
+#pragma unroll
+    for (int q = 0; q < G::IB; ++q) {
+      const int it = threadIdx.x + q * kFaThreads;
+      if (it < NLT * N1) {
+        const int j = it % NLT, k1 = it / NLT;
+#pragma unroll
+        for (int k2 = 0; k2 < N2; ++k2) d[j * ld + k1 + k2 * N1] = w2[q][k2];
+      }
     }
   }
   __syncthreads();
@@ -231,8 +261,7 @@ __global__ void __launch_bounds__(kFaThreads) fa_div_kernel(FaArgs a) {
   constexpr int n = G::n, ld = G::ld, NL = G::NLT / 2;
   extern __shared__ __align__(16) FftC fa_sm[];
   FftC* d = fa_sm;
-  FftC* mid = d + G::NLT * ld;
-  FftC* tw = mid + G::NLT * G::ldm;
+  FftC* tw = d + G::NLT * ld;
   if (fa_done(a)) return;
   const ChainDev& ch = *a.ch;
   const int nlines = a.L[1] * a.L[2];
@@ -269,7 +298,7 @@ __global__ void __launch_bounds__(kFaThreads) fa_div_kernel(FaArgs a) {
   }
   block_reduce_store<1>(q, a.part + blockIdx.x);
   __syncthreads();
-  fft2_lines<LOGN>(d, mid, tw);
+  fft2_lines<LOGN>(d, tw);
   const size_t V = (size_t)a.L[0] * a.L[1] * a.L[2];
   FftC* F = reinterpret_cast<FftC*>(a.fft);
   for (int e = threadIdx.x; e < NL * n; e += blockDim.x) {
@@ -305,14 +334,14 @@ __global__ void __launch_bounds__(1024) fa_check_kernel(const ChainDev* chp, Cha
 
 // (3)-(5) FFT of one field (blockIdx.y) along axis AX (1: y, 2: z); for
 // AX = 2 with SCALE: forward, multiply by gamma / (p_c^2 V), inverse
+// (the forward-scale-inverse form is held to 64 registers, 4 blocks per SM)
 template <int AX, int SIGN, bool SCALE, int LOGN>
-__global__ void __launch_bounds__(kFaThreads) fa_fft_kernel(FaArgs a) {
+__global__ void __launch_bounds__(kFaThreads, SCALE && LOGN <= 8 ? 4 : 1) fa_fft_kernel(FaArgs a) {
   using G = FaLines<LOGN>;
   constexpr int n = G::n, ld = G::ld, NL = G::NLT, LNL = kFaBlockLog - LOGN;
   extern __shared__ __align__(16) FftC fa_sm[];
   FftC* d = fa_sm;
-  FftC* mid = d + NL * ld;
-  FftC* tw = mid + NL * G::ldm;
+  FftC* tw = d + NL * ld;
   FftC* twi = tw + G::ntw;                                       // SCALE: inverse twiddles
   double* sz2 = reinterpret_cast<double*>(twi + G::ntw);         // SCALE: alpha sin^2(pi kz / L3)
   double* sxy = sz2 + n;                                         // SCALE: sin^2(pi kx/L1) + sin^2(pi ky/L2)
@@ -342,7 +371,7 @@ __global__ void __launch_bounds__(kFaThreads) fa_fft_kernel(FaArgs a) {
     d[j * ld + k] = l < nlines ? F[nat_index<AX>(a, l, k)] : FftC{0, 0};
   }
   __syncthreads();
-  fft2_lines<LOGN>(d, mid, tw);
+  fft2_lines<LOGN>(d, tw);
   if (SCALE) {
     const double gv = (a.cst ? a.cst->gf_step : a.gamma) / (4.0 * (double)V);
     for (int e = threadIdx.x; e < NL * n; e += blockDim.x) {
@@ -353,7 +382,7 @@ __global__ void __launch_bounds__(kFaThreads) fa_fft_kernel(FaArgs a) {
       d[q] = FftC{(FftR)(d[q].x * m), (FftR)(d[q].y * m)};
     }
     __syncthreads();
-    fft2_lines<LOGN>(d, mid, twi);
+    fft2_lines<LOGN>(d, twi);
   }
   for (int e = threadIdx.x; e < NL * n; e += blockDim.x) {
     const int j = e & (NL - 1), k = e >> LNL, l = l0 + j;
@@ -368,8 +397,7 @@ __global__ void __launch_bounds__(kFaThreads) fa_g_kernel(FaArgs a) {
   constexpr int n = G::n, ld = G::ld, NL = G::NLT / 2;
   extern __shared__ __align__(16) FftC fa_sm[];
   FftC* d = fa_sm;
-  FftC* mid = d + G::NLT * ld;
-  FftC* tw = mid + G::NLT * G::ldm;
+  FftC* tw = d + G::NLT * ld;
   if (fa_done(a)) return;
   const ChainDev& ch = *a.ch;
   const int nlines = a.L[1] * a.L[2];
@@ -384,7 +412,7 @@ __global__ void __launch_bounds__(kFaThreads) fa_g_kernel(FaArgs a) {
     d[(NL + j) * ld + k] = l < nlines ? F[V + gi] : FftC{0, 0};
   }
   __syncthreads();
-  fft2_lines<LOGN>(d, mid, tw);
+  fft2_lines<LOGN>(d, tw);
   for (int e = threadIdx.x; e < NL * n; e += blockDim.x) {
     const int j = e >> LOGN, x = e & (n - 1), l = l0 + j;
     if (l >= nlines) continue;
