@@ -493,11 +493,6 @@ int download_t(lce_ctx* c, int chain, int which, Rout* u, Rout* a, long ld) {
   return LCE_OK;
 }
 
-int set_device(lce_ctx* c) {
-  CK(cudaSetDevice(c->device));
-  return LCE_OK;
-}
-
 lce_ctx* create_impl(const lce_params* p, int n) {
   g_create_error.clear();
   if (!p || n < 1) {
@@ -874,10 +869,17 @@ int lce_geometry_tables(int L1, int L2, int L3, int* siteup, int* sitedn) {
   return LCE_OK;
 }
 
-lce_ctx* lce_create(const lce_params* p) { return create_impl(p, 1); }
-lce_ctx* lce_create_batch(const lce_params* p, int nchains) { return create_impl(p, nchains); }
+lce_ctx* lce_create(const lce_params* p) {
+  DeviceScope ds_(p ? p->device : -1);
+  return create_impl(p, 1);
+}
+lce_ctx* lce_create_batch(const lce_params* p, int nchains) {
+  DeviceScope ds_(p && nchains > 0 ? p->device : -1);
+  return create_impl(p, nchains);
+}
 
 void lce_destroy(lce_ctx* c) {
+  DeviceScope ds_(c ? c->device : -1);
   if (!c) return;
   cudaSetDevice(c->device);
   if (c->stream) cudaStreamSynchronize(c->stream);
@@ -902,6 +904,7 @@ void lce_destroy(lce_ctx* c) {
 int lce_nchains(lce_ctx* c) { return c ? c->nchains : LCE_ERR_INVALID; }
 
 int lce_get_extents(lce_ctx* c, int chain, int L[3]) {
+  DeviceScope ds_(c ? c->device : -1);
   if (!c || !L || chain < 0 || chain >= c->nchains) return LCE_ERR_INVALID;
   L[0] = c->ch[chain].L1;
   L[1] = c->ch[chain].L2;
@@ -910,35 +913,42 @@ int lce_get_extents(lce_ctx* c, int chain, int L[3]) {
 }
 
 int lce_set_stream(lce_ctx* c, void* s) {
+  DeviceScope ds_(c ? c->device : -1);
   if (!c) return LCE_ERR_INVALID;
   c->stream = s ? (cudaStream_t)s : c->own;
   return LCE_OK;
 }
 
 int lce_synchronize(lce_ctx* c) {
+  DeviceScope ds_(c ? c->device : -1);
   if (!c) return LCE_ERR_INVALID;
   CK(cudaStreamSynchronize(c->stream));
   return status_check(c);
 }
 
 int lce_upload(lce_ctx* c, int chain, int which, const float* u, const float* a, long ld) {
+  DeviceScope ds_(c ? c->device : -1);
   if (!c) return LCE_ERR_INVALID;
   return upload_t<float>(c, chain, which, u, a, ld);
 }
 int lce_upload_f64(lce_ctx* c, int chain, int which, const double* u, const double* a, long ld) {
+  DeviceScope ds_(c ? c->device : -1);
   if (!c) return LCE_ERR_INVALID;
   return upload_t<double>(c, chain, which, u, a, ld);
 }
 int lce_download(lce_ctx* c, int chain, int which, float* u, float* a, long ld) {
+  DeviceScope ds_(c ? c->device : -1);
   if (!c) return LCE_ERR_INVALID;
   return download_t<float>(c, chain, which, u, a, ld);
 }
 int lce_download_f64(lce_ctx* c, int chain, int which, double* u, double* a, long ld) {
+  DeviceScope ds_(c ? c->device : -1);
   if (!c) return LCE_ERR_INVALID;
   return download_t<double>(c, chain, which, u, a, ld);
 }
 
 int lce_init_unit(lce_ctx* c, double a3) {
+  DeviceScope ds_(c ? c->device : -1);
   if (!c) return LCE_ERR_INVALID;
   for (int i = 0; i < c->nchains; ++i) {
     if (c->prec == LCE_PREC_F64) launch_init_unit<double>(c->ch[i].u, c->ch[i].a, c->ch[i].nh, a3, c->stream);
@@ -949,6 +959,7 @@ int lce_init_unit(lce_ctx* c, double a3) {
 }
 
 int lce_init_hot(lce_ctx* c, unsigned long long seed) {
+  DeviceScope ds_(c ? c->device : -1);
   if (!c) return LCE_ERR_INVALID;
   for (int i = 0; i < c->nchains; ++i) {
     const unsigned long long k = seed + 0x9E3779B97F4A7C15ull * (unsigned long long)i;
@@ -961,6 +972,7 @@ int lce_init_hot(lce_ctx* c, unsigned long long seed) {
 }
 
 int lce_set_rng_stream(lce_ctx* c, const double* u, size_t n) {
+  DeviceScope ds_(c ? c->device : -1);
   if (!c || (!u && n)) return LCE_ERR_INVALID;
   if (c->rng != LCE_RNG_STREAM) return fail(c, LCE_ERR_UNSUPPORTED, "context was not created with LCE_RNG_STREAM");
   CK(cudaStreamSynchronize(c->stream));
@@ -993,6 +1005,7 @@ int lce_set_rng_stream(lce_ctx* c, const double* u, size_t n) {
 }
 
 int lce_get_rng_position(lce_ctx* c, unsigned long long* pass_ctr, unsigned long long* stream_pos) {
+  DeviceScope ds_(c ? c->device : -1);
   if (!c) return LCE_ERR_INVALID;
   CtxState st;
   CK(cudaMemcpyAsync(&st, c->st_d, sizeof(st), cudaMemcpyDeviceToHost, c->stream));
@@ -1003,6 +1016,7 @@ int lce_get_rng_position(lce_ctx* c, unsigned long long* pass_ctr, unsigned long
 }
 
 int lce_set_rng_position(lce_ctx* c, unsigned long long pass_ctr, unsigned long long stream_pos) {
+  DeviceScope ds_(c ? c->device : -1);
   if (!c) return LCE_ERR_INVALID;
   CK(cudaStreamSynchronize(c->stream));
   CK(cudaMemcpy(&c->st_d->pass_ctr, &pass_ctr, sizeof(pass_ctr), cudaMemcpyHostToDevice));
@@ -1011,6 +1025,7 @@ int lce_set_rng_position(lce_ctx* c, unsigned long long pass_ctr, unsigned long 
 }
 
 int lce_ahiggs1(lce_ctx* c, float* delta, int measflag, float* accept) {
+  DeviceScope ds_(c ? c->device : -1);
   if (!c) return LCE_ERR_INVALID;
   if (delta) {
     // the step lives on the device; the caller's value is the one to use
@@ -1033,22 +1048,28 @@ int lce_ahiggs1(lce_ctx* c, float* delta, int measflag, float* accept) {
 }
 
 int lce_ahiggs2(lce_ctx* c, int measflag, float* accept) {
+  DeviceScope ds_(c ? c->device : -1);
   return c ? routine_call(c, kHiggsHB, measflag, accept, false) : LCE_ERR_INVALID;
 }
 int lce_ahiggs3(lce_ctx* c, int measflag, float* accept) {
+  DeviceScope ds_(c ? c->device : -1);
   return c ? routine_call(c, kHiggsOR, measflag, accept, false) : LCE_ERR_INVALID;
 }
 int lce_agauge(lce_ctx* c, int measflag, float* accept) {
+  DeviceScope ds_(c ? c->device : -1);
   return c ? routine_call(c, kLinkHB, measflag, accept, false) : LCE_ERR_INVALID;
 }
 int lce_agauge1(lce_ctx* c, int measflag, float* accept) {
+  DeviceScope ds_(c ? c->device : -1);
   return c ? routine_call(c, kLinkHB3, measflag, accept, false) : LCE_ERR_INVALID;
 }
 int lce_link_or(lce_ctx* c, int measflag, float* accept) {
+  DeviceScope ds_(c ? c->device : -1);
   return c ? routine_call(c, kLinkOR, measflag, accept, false) : LCE_ERR_INVALID;
 }
 
 int lce_renorm(lce_ctx* c) {
+  DeviceScope ds_(c ? c->device : -1);
   if (!c) return LCE_ERR_INVALID;
   for (int i = 0; i < c->nchains; ++i) {
     if (c->prec == LCE_PREC_F64) launch_renorm<double>(c->ch[i].u, (size_t)6 * c->ch[i].nh, c->stream);
@@ -1059,6 +1080,7 @@ int lce_renorm(lce_ctx* c) {
 }
 
 int lce_sweeps(lce_ctx* c, int nsweeps, int measflag) {
+  DeviceScope ds_(c ? c->device : -1);
   if (!c || nsweeps < 0) return LCE_ERR_INVALID;
   const int mf = measflag == 1 ? 1 : 0;
   int done = 0;
@@ -1114,12 +1136,14 @@ int lce_sweeps(lce_ctx* c, int nsweeps, int measflag) {
 int lce_get_sweep_mode(lce_ctx* c) { return c ? c->mode : LCE_ERR_INVALID; }
 
 int lce_sweep(lce_ctx* c, int measflag, lce_meas* m) {
+  DeviceScope ds_(c ? c->device : -1);
   int rc = lce_sweeps(c, 1, measflag);
   if (rc || !m) return rc;
   return lce_get_meas(c, 0, m);
 }
 
 int lce_get_meas(lce_ctx* c, int chain, lce_meas* m) {
+  DeviceScope ds_(c ? c->device : -1);
   if (!c || !m || chain < 0 || chain >= c->nchains) return LCE_ERR_INVALID;
   CK(cudaMemcpyAsync(m, c->meas_d + chain, sizeof(*m), cudaMemcpyDeviceToHost, c->stream));
   int rc = status_check(c);
@@ -1128,12 +1152,14 @@ int lce_get_meas(lce_ctx* c, int chain, lce_meas* m) {
 }
 
 int lce_get_meas_batch(lce_ctx* c, lce_meas* m) {
+  DeviceScope ds_(c ? c->device : -1);
   if (!c || !m) return LCE_ERR_INVALID;
   CK(cudaMemcpyAsync(m, c->meas_d, sizeof(lce_meas) * c->nchains, cudaMemcpyDeviceToHost, c->stream));
   return status_check(c);
 }
 
 int lce_landau_gauge(lce_ctx* c, int chain, double* theta, int* iters, int max_iters) {
+  DeviceScope ds_(c ? c->device : -1);
   if (!c || chain < 0 || chain >= c->nchains) return LCE_ERR_INVALID;
   const ChainDev& ch = c->ch[chain];
   // f/landau_gauge.f:308-324 copy u -> u_f, a -> a_f
@@ -1144,11 +1170,13 @@ int lce_landau_gauge(lce_ctx* c, int chain, double* theta, int* iters, int max_i
 }
 
 int lce_gauge_fix_continue(lce_ctx* c, int chain, double* theta, int* iters, int max_iters) {
+  DeviceScope ds_(c ? c->device : -1);
   if (!c || chain < 0 || chain >= c->nchains) return LCE_ERR_INVALID;
   return gf_loop(c, chain, theta, iters, max_iters);
 }
 
 int lce_it_gauge_fixing(lce_ctx* c, int chain, double step, int flags, double* da1) {
+  DeviceScope ds_(c ? c->device : -1);
   if (!c || chain < 0 || chain >= c->nchains || (flags & ~(LCE_ITGF_FIX_COMPONENT | LCE_ITGF_ASCEND | LCE_ITGF_TRACK)))
     return LCE_ERR_INVALID;
   const ChainDev& ch = c->ch[chain];
@@ -1175,6 +1203,7 @@ int lce_it_gauge_fixing(lce_ctx* c, int chain, double step, int flags, double* d
 }
 
 int lce_it_landau_gauge(lce_ctx* c, int chain, double step, int flags, double* da1, int* iters, int max_iters) {
+  DeviceScope ds_(c ? c->device : -1);
   if (!c || chain < 0 || chain >= c->nchains || (flags & ~(LCE_ITGF_FIX_COMPONENT | LCE_ITGF_ASCEND | LCE_ITGF_TRACK)))
     return LCE_ERR_INVALID;
   const ChainDev& ch = c->ch[chain];
@@ -1189,6 +1218,7 @@ int lce_it_landau_gauge(lce_ctx* c, int chain, double step, int flags, double* d
 }
 
 int lce_apply_transform(lce_ctx* c, int chain) {
+  DeviceScope ds_(c ? c->device : -1);
   if (!c || chain < 0 || chain >= c->nchains) return LCE_ERR_INVALID;
   if (c->prec == LCE_PREC_F64) launch_gauge_apply<double>(c->ch_d + chain, c->ch[chain].nh, c->stream);
   else launch_gauge_apply<float>(c->ch_d + chain, c->ch[chain].nh, c->stream);
@@ -1198,6 +1228,7 @@ int lce_apply_transform(lce_ctx* c, int chain) {
 
 int lce_landau_gauge_from(lce_ctx* c, int chain, int start, double* theta_start, double* theta, int* iters,
                           int max_iters) {
+  DeviceScope ds_(c ? c->device : -1);
   if (!c || chain < 0 || chain >= c->nchains) return LCE_ERR_INVALID;
   const ChainDev& ch = c->ch[chain];
   if (start == LCE_GF_START_IDENTITY) {
@@ -1221,6 +1252,7 @@ int lce_landau_gauge_from(lce_ctx* c, int chain, int start, double* theta_start,
 
 int lce_landau_gauge_warm(lce_ctx* c, int chain, lce_net* net, int flags, int* start_used, double functional[3],
                           double* theta, int* iters, int max_iters) {
+  DeviceScope ds_(c ? c->device : -1);
   if (!c || chain < 0 || chain >= c->nchains ||
       (flags & ~(LCE_WARM_NET | LCE_WARM_JUDGE | LCE_WARM_RECORD | LCE_WARM_FOURIER)))
     return LCE_ERR_INVALID;
@@ -1305,6 +1337,7 @@ int lce_landau_gauge_warm(lce_ctx* c, int chain, lce_net* net, int flags, int* s
 
 int lce_landau_gauge_fourier(lce_ctx* c, int chain, int start, double step, double theta_switch, double* theta,
                              int* iters_fourier, int* iters_plain, int max_iters) {
+  DeviceScope ds_(c ? c->device : -1);
   if (!c || chain < 0 || chain >= c->nchains) return LCE_ERR_INVALID;
   const ChainDev& ch = c->ch[chain];
   if (!fa_supported(ch)) return fail(c, LCE_ERR_UNSUPPORTED, "Fourier-accelerated fixing needs power-of-two extents");
@@ -1339,6 +1372,7 @@ int lce_landau_gauge_fourier(lce_ctx* c, int chain, int start, double step, doub
 }
 
 int lce_debug_fourier_step(lce_ctx* c, int chain, double step, double* omega) {
+  DeviceScope ds_(c ? c->device : -1);
   if (!c || !omega || chain < 0 || chain >= c->nchains) return LCE_ERR_INVALID;
   const ChainDev& ch = c->ch[chain];
   if (!fa_supported(ch)) return fail(c, LCE_ERR_UNSUPPORTED, "power-of-two extents needed");
@@ -1362,6 +1396,7 @@ int lce_debug_fourier_step(lce_ctx* c, int chain, double step, double* omega) {
 }
 
 int lce_set_transform(lce_ctx* c, int chain, const float* g, long ld) {
+  DeviceScope ds_(c ? c->device : -1);
   if (!c || !g || chain < 0 || chain >= c->nchains || ld < c->ch[chain].nh) return LCE_ERR_INVALID;
   const ChainDev& ch = c->ch[chain];
   const int nh = ch.nh;
@@ -1379,6 +1414,7 @@ int lce_set_transform(lce_ctx* c, int chain, const float* g, long ld) {
 }
 
 int lce_get_transform(lce_ctx* c, int chain, float* g, long ld) {
+  DeviceScope ds_(c ? c->device : -1);
   if (!c || !g || chain < 0 || chain >= c->nchains || ld < c->ch[chain].nh) return LCE_ERR_INVALID;
   const ChainDev& ch = c->ch[chain];
   const int nh = ch.nh;
@@ -1397,6 +1433,7 @@ int lce_get_transform(lce_ctx* c, int chain, float* g, long ld) {
 }
 
 int lce_gauge_functional(lce_ctx* c, int chain, double* value) {
+  DeviceScope ds_(c ? c->device : -1);
   if (!c || !value || chain < 0 || chain >= c->nchains) return LCE_ERR_INVALID;
   const ChainDev& ch = c->ch[chain];
   const int nb = ceil_div(2L * ch.nh, 256);
@@ -1414,6 +1451,7 @@ int lce_gauge_functional(lce_ctx* c, int chain, double* value) {
 }
 
 int lce_theta(lce_ctx* c, int chain, double* theta) {
+  DeviceScope ds_(c ? c->device : -1);
   if (!c || !theta || chain < 0 || chain >= c->nchains) return LCE_ERR_INVALID;
   const ChainDev& ch = c->ch[chain];
   const int nb = ceil_div(ch.nh, kBlock);
@@ -1431,6 +1469,7 @@ int lce_theta(lce_ctx* c, int chain, double* theta) {
 }
 
 int lce_correlator(lce_ctx* c, int chain, double* corr_a, double* corr_u, double* corr_3, double af[3]) {
+  DeviceScope ds_(c ? c->device : -1);
   if (!c || chain < 0 || chain >= c->nchains) return LCE_ERR_INVALID;
   const int L3 = c->ch[chain].L3;
   double* out;
@@ -1447,6 +1486,7 @@ int lce_correlator(lce_ctx* c, int chain, double* corr_a, double* corr_u, double
 }
 
 int lce_polyakov(lce_ctx* c, int chain, double* slice, double* corr, double* mean2) {
+  DeviceScope ds_(c ? c->device : -1);
   if (!c || chain < 0 || chain >= c->nchains) return LCE_ERR_INVALID;
   const int L3 = c->ch[chain].L3;
   double* out;
@@ -1462,6 +1502,7 @@ int lce_polyakov(lce_ctx* c, int chain, double* slice, double* corr, double* mea
 }
 
 int lce_scalarcorr(lce_ctx* c, int chain, double* slice, double* corr, double* mean) {
+  DeviceScope ds_(c ? c->device : -1);
   if (!c || chain < 0 || chain >= c->nchains) return LCE_ERR_INVALID;
   const int L3 = c->ch[chain].L3;
   double* out;
@@ -1477,6 +1518,7 @@ int lce_scalarcorr(lce_ctx* c, int chain, double* slice, double* corr, double* m
 }
 
 int lce_plaquette(lce_ctx* c, int chain, double* plaq) {
+  DeviceScope ds_(c ? c->device : -1);
   if (!c || !plaq || chain < 0 || chain >= c->nchains) return LCE_ERR_INVALID;
   const ChainDev& ch = c->ch[chain];
   const int nb = ceil_div(2L * ch.nh, 256);
@@ -1494,6 +1536,7 @@ int lce_plaquette(lce_ctx* c, int chain, double* plaq) {
 }
 
 int lce_debug_staple(lce_ctx* c, int eo, int mu, double* out) {
+  DeviceScope ds_(c ? c->device : -1);
   if (!c || !out || eo < 0 || eo > 1 || mu < 0 || mu > 2) return LCE_ERR_INVALID;
   const int nh = c->ch[0].nh;
   int rc = ensure_staging(c, (size_t)nh * 4 * sizeof(double));
@@ -1507,6 +1550,7 @@ int lce_debug_staple(lce_ctx* c, int eo, int mu, double* out) {
 }
 
 int lce_debug_force(lce_ctx* c, int eo, double* out) {
+  DeviceScope ds_(c ? c->device : -1);
   if (!c || !out || eo < 0 || eo > 1) return LCE_ERR_INVALID;
   const int nh = c->ch[0].nh;
   int rc = ensure_staging(c, (size_t)nh * 3 * sizeof(double));
@@ -1520,6 +1564,7 @@ int lce_debug_force(lce_ctx* c, int eo, double* out) {
 }
 
 int lce_flush_l2(lce_ctx* c) {
+  DeviceScope ds_(c ? c->device : -1);
   if (!c) return LCE_ERR_INVALID;
   if (!c->flush_d) {
     c->flush_bytes = (size_t)256 << 20;  // written; a second 256 MB half is read
@@ -1531,6 +1576,7 @@ int lce_flush_l2(lce_ctx* c) {
 }
 
 int lce_profile_sweep(lce_ctx* c, int measflag, float* ms, int max_passes) {
+  DeviceScope ds_(c ? c->device : -1);
   if (!c || !ms) return LCE_ERR_INVALID;
   std::vector<unsigned char> r = sweep_routines(c);
   std::vector<Pass> passes;
@@ -1549,12 +1595,14 @@ int lce_profile_sweep(lce_ctx* c, int measflag, float* ms, int max_passes) {
 }
 
 int lce_timer_start(lce_ctx* c) {
+  DeviceScope ds_(c ? c->device : -1);
   if (!c) return LCE_ERR_INVALID;
   CK(cudaEventRecord(c->ev0, c->stream));
   return LCE_OK;
 }
 
 int lce_timer_stop(lce_ctx* c, float* ms) {
+  DeviceScope ds_(c ? c->device : -1);
   if (!c || !ms) return LCE_ERR_INVALID;
   CK(cudaEventRecord(c->ev1, c->stream));
   CK(cudaEventSynchronize(c->ev1));

@@ -87,9 +87,6 @@ struct FaLines {
   // of N2 points, each row padded by one; n + N1 + 1 = 2 mod 32 words apart
   static constexpr int ld = N2 > 1 ? N1 * (N2 + 1) + 1 : n + 1;
   static constexpr int ntw = n / 2 > 0 ? n / 2 : 1;              // twiddle table entries
-  // items per thread of the two steps
-  static constexpr int IA = (NLT * N2 + kFaThreads - 1) / kFaThreads;
-  static constexpr int IB = (NLT * N1 + kFaThreads - 1) / kFaThreads;
   // lines, ntab twiddle tables and nd doubles
   static constexpr size_t smem(int ntab, int nd) {
     return ((size_t)NLT * ld + (size_t)ntab * ntw) * sizeof(FftC) + (size_t)nd * sizeof(double);
@@ -162,11 +159,14 @@ __device__ __forceinline__ void fft2_lines(FftC* d, const FftC* tw) {
       for (int k = 0; k < N1; ++k) d[j * ld + k] = v[k];
     }
   } else {
+    // items per thread of the two steps
+    constexpr int IA = (NLT * N2 + kFaThreads - 1) / kFaThreads;
+    constexpr int IB = (NLT * N1 + kFaThreads - 1) / kFaThreads;
     // step 1: item (line j, column n2), lines fastest: N1 points of stride N2,
     // DFT, twiddles W_n^(n2 k1); stored as row k1, column n2
-    FftC r[G::IA][N1];
+    FftC r[IA][N1];
 #pragma unroll
-    for (int q = 0; q < G::IA; ++q) {
+    for (int q = 0; q < IA; ++q) {
       const int it = threadIdx.x + q * kFaThreads;
       if (it < NLT * N2) {
         const int j = it % NLT, n2 = it / NLT;
@@ -183,7 +183,7 @@ __device__ __forceinline__ void fft2_lines(FftC* d, const FftC* tw) {
     }
     __syncthreads();
 #pragma unroll
-    for (int q = 0; q < G::IA; ++q) {
+    for (int q = 0; q < IA; ++q) {
       const int it = threadIdx.x + q * kFaThreads;
       if (it < NLT * N2) {
         const int j = it % NLT, n2 = it / NLT;
@@ -193,9 +193,9 @@ __device__ __forceinline__ void fft2_lines(FftC* d, const FftC* tw) {
     }
     __syncthreads();
     // step 2: item (line j, row k1): N2-point DFT, X[k1 + N1 k2] in natural order
-    FftC w2[G::IB][N2];
+    FftC w2[IB][N2];
 #pragma unroll
-    for (int q = 0; q < G::IB; ++q) {
+    for (int q = 0; q < IB; ++q) {
       const int it = threadIdx.x + q * kFaThreads;
       if (it < NLT * N1) {
         const int j = it % NLT, k1 = it / NLT;
@@ -206,7 +206,7 @@ __device__ __forceinline__ void fft2_lines(FftC* d, const FftC* tw) {
     }
     __syncthreads();
 #pragma unroll
-    for (int q = 0; q < G::IB; ++q) {
+    for (int q = 0; q < IB; ++q) {
       const int it = threadIdx.x + q * kFaThreads;
       if (it < NLT * N1) {
         const int j = it % NLT, k1 = it / NLT;

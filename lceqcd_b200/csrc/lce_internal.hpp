@@ -232,4 +232,24 @@ int net_record(lce_net* n, const ChainDev& ch, const void* gprev, bool f64, cuda
 // message returned by lce_last_error(NULL) on this host thread
 void set_thread_error(const std::string& msg);
 
+// Makes `device` current for the duration of one entry point and gives the
+// caller back its own current device afterwards: a host thread may drive
+// contexts (and networks) on several GPUs.  device < 0: nothing to do.
+class DeviceScope {
+ public:
+  explicit DeviceScope(int device) {
+    if (device < 0 || cudaGetDevice(&prev_) != cudaSuccess) return;
+    if (prev_ != device && cudaSetDevice(device) == cudaSuccess) restore_ = true;
+  }
+  ~DeviceScope() {
+    if (restore_) cudaSetDevice(prev_);
+  }
+  DeviceScope(const DeviceScope&) = delete;
+  DeviceScope& operator=(const DeviceScope&) = delete;
+
+ private:
+  int prev_ = -1;
+  bool restore_ = false;
+};
+
 }  // namespace lce

@@ -950,6 +950,7 @@ namespace {
 extern "C" {
 
 lce_net* lce_net_create(int device, unsigned long long seed) {
+  DeviceScope ds_(device);
   lce_net* n = new lce_net();
   n->device = device;
   auto bad = [&](cudaError_t e, const char* w) -> lce_net* {
@@ -977,6 +978,7 @@ lce_net* lce_net_create(int device, unsigned long long seed) {
 }
 
 void lce_net_destroy(lce_net* n) {
+  DeviceScope ds_(n ? n->device : -1);
   if (!n) return;
   cudaSetDevice(n->device);
   if (n->stream) cudaStreamSynchronize(n->stream);
@@ -997,6 +999,7 @@ void lce_net_destroy(lce_net* n) {
 int lce_net_num_params(lce_net* n) { return n ? kNParam : LCE_ERR_INVALID; }
 
 int lce_net_get_params(lce_net* n, float* w) {
+  DeviceScope ds_(n ? n->device : -1);
   if (!n || !w) return LCE_ERR_INVALID;
   NCK(cudaMemcpyAsync(w, n->w32, sizeof(float) * kNParam, cudaMemcpyDeviceToHost, n->stream));
   NCK(cudaStreamSynchronize(n->stream));
@@ -1004,6 +1007,7 @@ int lce_net_get_params(lce_net* n, float* w) {
 }
 
 int lce_net_set_params(lce_net* n, const float* w) {
+  DeviceScope ds_(n ? n->device : -1);
   if (!n || !w) return LCE_ERR_INVALID;
   NCK(cudaMemcpyAsync(n->w32, w, sizeof(float) * kNParam, cudaMemcpyHostToDevice, n->stream));
   net_refresh(n, n->stream);
@@ -1012,6 +1016,7 @@ int lce_net_set_params(lce_net* n, const float* w) {
 }
 
 int lce_net_save(lce_net* n, const char* path) {
+  DeviceScope ds_(n ? n->device : -1);
   std::vector<float> w(kNParam);
   int rc = lce_net_get_params(n, w.data());
   if (rc) return rc;
@@ -1024,6 +1029,7 @@ int lce_net_save(lce_net* n, const char* path) {
 }
 
 int lce_net_load(lce_net* n, const char* path) {
+  DeviceScope ds_(n ? n->device : -1);
   if (!n || !path) return LCE_ERR_INVALID;
   FILE* f = std::fopen(path, "rb");
   if (!f) return net_fail(n, LCE_ERR_INVALID, std::string("lce_net_load: cannot open ") + path);
@@ -1041,6 +1047,7 @@ int lce_net_load(lce_net* n, const char* path) {
 // [nparam] may be NULL
 int lce_net_eval(lce_net* n, int L1, int L2, int L3, const float* feat, const float* target, float* out, float* grad,
                  double* loss) {
+  DeviceScope ds_(n ? n->device : -1);
   if (!n || !feat || !target || L1 < 2 || L2 < 2 || L3 < 2 || ((L1 | L2 | L3) & 1)) return LCE_ERR_INVALID;
   const NetGeom g = make_geom(L1, L2, L3);
   const long ns = 2L * g.nh;
@@ -1074,6 +1081,7 @@ int lce_net_eval(lce_net* n, int L1, int L2, int L3, const float* feat, const fl
 int lce_net_num_pairs(lce_net* n) { return n ? (int)n->pairs.size() : LCE_ERR_INVALID; }
 
 int lce_net_clear_pairs(lce_net* n) {
+  DeviceScope ds_(n ? n->device : -1);
   if (!n) return LCE_ERR_INVALID;
   NCK(cudaStreamSynchronize(n->stream));
   for (auto& p : n->pairs) {
@@ -1086,6 +1094,7 @@ int lce_net_clear_pairs(lce_net* n) {
 
 // Adam over the recorded pairs, `epochs` passes in an order shuffled per epoch
 int lce_net_train(lce_net* n, int epochs, double lr, double* mean_loss) {
+  DeviceScope ds_(n ? n->device : -1);
   if (!n || epochs < 0 || n->pairs.empty()) return LCE_ERR_INVALID;
   const float b1 = 0.9f, b2 = 0.999f, eps = 1e-8f;
   std::vector<int> order(n->pairs.size());
