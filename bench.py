@@ -118,6 +118,66 @@ class Clocks:
                 "reasons": sorted(reasons), "samples": len(sm)}
 
 
+class NvmlClocks:
+    """NVML sampling every ~1 ms (SM clock, clock-event reasons) in a thread,
+    for timed regions too short for nvidia-smi's 200 ms interval.  Reads only."""
+
+    REASONS = (("nvmlClocksEventReasonHwSlowdown", "hw_slowdown"),
+               ("nvmlClocksEventReasonHwThermalSlowdown", "hw_thermal_slowdown"),
+               ("nvmlClocksEventReasonSwThermalSlowdown", "sw_thermal_slowdown"),
+               ("nvmlClocksEventReasonSwPowerCap", "sw_power_cap"),
+               ("nvmlClocksEventReasonHwPowerBrakeSlowdown", "hw_power_brake_slowdown"))
+
+    def __init__(self, index: str):
+        self.index = index
+        self.samples = []
+        self.thread = None
+        self.h = None
+        self.nvml = None
+
+    def start(self):
+        import threading
+        try:
+            import pynvml
+            pynvml.nvmlInit()
+            self.nvml = pynvml
+            self.h = (pynvml.nvmlDeviceGetHandleByIndex(int(self.index)) if self.index.isdigit()
+                      else pynvml.nvmlDeviceGetHandleByUUID(self.index))
+        except Exception:
+            self.h = None
+            return
+        self.stop_flag = False
+
+        def run():
+            n, h = self.nvml, self.h
+            while not self.stop_flag:
+                try:
+                    self.samples.append((n.nvmlDeviceGetClockInfo(h, n.NVML_CLOCK_SM),
+                                         n.nvmlDeviceGetCurrentClocksEventReasons(h)))
+                except Exception:
+                    break
+                time.sleep(0.001)
+
+        self.thread = threading.Thread(target=run, daemon=True)
+        self.thread.start()
+
+    def stop(self):
+        if self.thread is None:
+            return None
+        self.stop_flag = True
+        self.thread.join()
+        n = self.nvml
+        smax = n.nvmlDeviceGetMaxClockInfo(self.h, n.NVML_CLOCK_SM)
+        reasons = set()
+        for _, r in self.samples:
+            for attr, name in self.REASONS:
+                if r & getattr(n, attr, 0):
+                    reasons.add(name)
+        sm = [s for s, _ in self.samples]
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": smax, "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
 def dist_setup():
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
@@ -385,14 +445,23 @@ def run_gpu(args):
     lat.synchronize()
     barrier(world)
     clk = Clocks(local)
+    fast = NvmlClocks(clk.index)
     if not args.quick:
         clk.start()
+        fast.start()
     wall0 = time.perf_counter()
     ms = timed_sweeps(lat, args.steps)
     lat.synchronize()
     wall = time.perf_counter() - wall0
+    fast_clocks = fast.stop() if not args.quick else None
     barrier(world)
     clocks = clk.stop() if not args.quick else None
+    if clocks is not None and fast_clocks and fast_clocks["samples"]:
+        # the ~1 ms NVML samples cover the timed region; nvidia-smi's (every
+        # 200 ms, started before it) are kept beside them
+        clocks = {**fast_clocks, "source": "nvml, ~1 ms interval, during the timed region",
+                  "reasons": sorted(set(fast_clocks["reasons"]) | set(clocks.get("reasons", []))),
+                  "nvidia_smi": clocks}
     ms_max = max_over_ranks(ms, world)
     value = world * V * args.steps / (ms_max / 1e3)
     mode = lat.sweep_mode()  # chosen by the library's autotuner during the untimed sweeps
