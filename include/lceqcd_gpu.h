@@ -317,6 +317,32 @@ int lce_profile_sweep(lce_ctx* ctx, int measflag, float* ms, int max_passes);
 int lce_timer_start(lce_ctx* ctx);
 int lce_timer_stop(lce_ctx* ctx, float* ms);
 
+
+/* ---- z-slab decomposition (f/topology.f with dimproc = (1, 1, n): the
+ * reference's MPI domain decomposition and the halo exchange of
+ * f/staples.f / f/a_force.f), for lattices larger than one GPU's memory.
+ * The lattice of *p is split along z into nslabs slabs of L3/nslabs planes
+ * (an even number >= 2); slab k lives on devices[k] (a device may hold
+ * several).  A slab keeps one halo plane on each side; after every pass the
+ * written field's boundary planes are copied to the neighbouring slabs
+ * (peer copies between devices, ordered by events).  The Philox counters use
+ * whole-lattice site indices, so the fields after a sweep are bit for bit
+ * those of an undecomposed context with the same seed; measurements are the
+ * whole lattice's (sums over slabs, in another order).  Philox only, the
+ * sweep composition of lce_sweep without ahiggs1 (n_higgs_metro = 0); no
+ * gauge fixing or correlators on a decomposed lattice. */
+typedef struct lce_slabs lce_slabs;
+lce_slabs* lce_slabs_create(const lce_params* p, int nslabs, const int* devices);  /* NULL: lce_last_error(NULL) */
+void lce_slabs_destroy(lce_slabs* s);
+/* the whole lattice in the reference order of lce_upload / lce_download */
+int lce_slabs_upload(lce_slabs* s, const float* u, const float* a, long ld);
+int lce_slabs_upload_f64(lce_slabs* s, const double* u, const double* a, long ld);
+int lce_slabs_download(lce_slabs* s, float* u, float* a, long ld);
+int lce_slabs_download_f64(lce_slabs* s, double* u, double* a, long ld);
+/* one sweep of f/main.f:38-41 over all slabs; m (may be NULL) receives the
+ * whole lattice's measurements when measflag = 1 */
+int lce_slabs_sweep(lce_slabs* s, int measflag, lce_meas* m);
+
 /* ---- allocation-free measurement ----
  * No counterpart in the reference.  For callers that cannot let this library
  * allocate device memory -- a driver whose GPU memory belongs to another

@@ -115,6 +115,13 @@ SIGNATURES = {
     "lce_landau_gauge": (I, [P, I, P, P, I]),
     "lce_gauge_fix_continue": (I, [P, I, P, P, I]),
     "lce_it_gauge_fixing": (I, [P, I, D, I, P]),
+    "lce_slabs_create": (P, [P, I, P]),
+    "lce_slabs_destroy": (None, [P]),
+    "lce_slabs_upload": (I, [P, P, P, C.c_long]),
+    "lce_slabs_upload_f64": (I, [P, P, P, C.c_long]),
+    "lce_slabs_download": (I, [P, P, P, C.c_long]),
+    "lce_slabs_download_f64": (I, [P, P, P, C.c_long]),
+    "lce_slabs_sweep": (I, [P, I, P]),
     "lce_it_landau_gauge": (I, [P, I, D, I, P, P, I]),
     "lce_landau_gauge_from": (I, [P, I, I, P, P, P, I]),
     "lce_apply_transform": (I, [P, I]),

@@ -9,6 +9,7 @@
 // The RNG counters live on the device, so a replayed graph draws fresh
 // numbers every time.
 #include <algorithm>
+#include <type_traits>
 #include <cmath>
 #include <cstdio>
 #include <cstring>
@@ -40,6 +41,7 @@ struct lce_ctx {
   int rng = LCE_RNG_PHILOX;
   int nchains = 0;
   int n_link_or = 0, n_higgs_metro = 0;
+  int eo_flip = 0;        // a z-slab's local parity of whole-lattice parity 0
   int agauge_hits = 1;  // 1: f/agauge.f, 3: f/agauge1.f in lce_sweep
   std::vector<lce_params> params;
   std::vector<ChainDev> ch;
@@ -215,16 +217,34 @@ void expand(unsigned char kind, std::vector<Pass>& out) {
 
 // Queue the passes of the given routines and one finalize kernel.
 // events: optional array receiving an event record after every pass.
-int enqueue(lce_ctx* c, const std::vector<unsigned char>& routines, int measflag, bool fuse_renorm,
-            cudaEvent_t* events = nullptr, int spt = 1) {
-  const std::vector<int>& blk = spt == 2 ? c->blk2 : c->blk;
-  int* blk_d = spt == 2 ? c->blk2_d : c->blk_d;
+// The passes of a list of routines, queued one at a time: enq_begin plans
+// them, enq_pass launches pass i, enq_end queues the finalize reduction.
+struct Enq {
   std::vector<Pass> passes;
-  for (unsigned char r : routines) expand(r, passes);
   FinalizeArgs f;
+  const std::vector<int>* blk = nullptr;
+  int* blk_d = nullptr;
+  int spt = 1;
+  int measflag = 0;
+  bool fuse = false;
+  unsigned long long soff = 0;
+  unsigned int poff = 0;
+  int slot = 0;
+};
+
+void enq_begin(lce_ctx* c, const std::vector<unsigned char>& routines, int measflag, bool fuse_renorm, int spt,
+               Enq& q) {
+  q.blk = spt == 2 ? &c->blk2 : &c->blk;
+  q.blk_d = spt == 2 ? c->blk2_d : c->blk_d;
+  q.spt = spt;
+  q.measflag = measflag;
+  q.fuse = fuse_renorm;
+  q.passes.clear();
+  for (unsigned char r : routines) expand(r, q.passes);
+  FinalizeArgs& f = q.f;
   std::memset(&f, 0, sizeof(f));
   f.chains = c->ch_d;
-  f.blk_begin = blk_d;
+  f.blk_begin = q.blk_d;
   f.st = c->st_d;
   f.cst = c->cst_d;
   f.meas = c->meas_d;
@@ -233,50 +253,65 @@ int enqueue(lce_ctx* c, const std::vector<unsigned char>& routines, int measflag
   f.totals = c->totals_d;
   f.nchains = c->nchains;
   f.single = c->prec == LCE_PREC_F32;
-  const int nblocks = blk.back();
-  unsigned long long soff = 0;
-  unsigned int poff = 0;
-  int slot = 0;
-  for (size_t i = 0; i < passes.size(); ++i) {
-    const Pass& ps = passes[i];
-    const bool reduce = measflag == 1 || ps.kind == kHiggsMetro;
-    if (reduce && slot >= c->part_slots) return fail(c, LCE_ERR_INVALID, "too many reduction slots");
-    PassArgs a;
-    a.chains = c->ch_d;
-    a.blk_begin = blk_d;
-    a.spt = spt;
-    a.st = c->st_d;
-    a.cst = c->cst_d;
-    a.part = reduce ? c->part_d + (size_t)slot * c->slot_stride : nullptr;
-    a.stream = c->rng == LCE_RNG_STREAM ? c->stream_d : nullptr;
-    a.stream_n = c->stream_n;
-    a.stream_off = soff;
-    a.pass_off = poff;
-    a.nchains = c->nchains;
-    a.eo = ps.eo;
-    a.fuse_renorm = fuse_renorm ? 1 : 0;
-    if (ps.kind <= kHiggsMetro) {
-      if (c->prec == LCE_PREC_F64) launch_higgs<double>(ps.kind, a, nblocks, c->stream);
-      else launch_higgs<float>(ps.kind, a, nblocks, c->stream);
-    } else {
-      const int mode = ps.kind == kLinkHB ? 0 : (ps.kind == kLinkOR ? 1 : 2);
-      if (c->prec == LCE_PREC_F64) launch_link<double>(mode, ps.mu, a, nblocks, c->stream);
-      else launch_link<float>(mode, ps.mu, a, nblocks, c->stream);
-    }
-    if (events) CK(cudaEventRecord(events[i], c->stream));
-    if (reduce) {
-      f.kinds[slot] = (unsigned char)(ps.kind | (ps.end ? kKindEnd : 0));
-      ++slot;
-    }
-    if (c->nchains == 1) soff += (unsigned long long)nslots_of(ps.kind) * c->ch[0].nh;
-    poff += philox_passes(ps.kind);
+  q.soff = 0;
+  q.poff = 0;
+  q.slot = 0;
+}
+
+int enq_pass(lce_ctx* c, Enq& q, size_t i) {
+  const Pass& ps = q.passes[i];
+  const int nblocks = q.blk->back();
+  const bool reduce = q.measflag == 1 || ps.kind == kHiggsMetro;
+  if (reduce && q.slot >= c->part_slots) return fail(c, LCE_ERR_INVALID, "too many reduction slots");
+  PassArgs a;
+  a.chains = c->ch_d;
+  a.blk_begin = q.blk_d;
+  a.spt = q.spt;
+  a.st = c->st_d;
+  a.cst = c->cst_d;
+  a.part = reduce ? c->part_d + (size_t)q.slot * c->slot_stride : nullptr;
+  a.stream = c->rng == LCE_RNG_STREAM ? c->stream_d : nullptr;
+  a.stream_n = c->stream_n;
+  a.stream_off = q.soff;
+  a.pass_off = q.poff;
+  a.nchains = c->nchains;
+  a.eo = ps.eo ^ c->eo_flip;
+  a.fuse_renorm = q.fuse ? 1 : 0;
+  if (ps.kind <= kHiggsMetro) {
+    if (c->prec == LCE_PREC_F64) launch_higgs<double>(ps.kind, a, nblocks, c->stream);
+    else launch_higgs<float>(ps.kind, a, nblocks, c->stream);
+  } else {
+    const int mode = ps.kind == kLinkHB ? 0 : (ps.kind == kLinkOR ? 1 : 2);
+    if (c->prec == LCE_PREC_F64) launch_link<double>(mode, ps.mu, a, nblocks, c->stream);
+    else launch_link<float>(mode, ps.mu, a, nblocks, c->stream);
   }
-  f.nslots = slot;
-  f.npasses = poff;
-  f.nstream = c->rng == LCE_RNG_STREAM ? soff : 0;
-  launch_finalize(f, c->stream);
+  if (reduce) {
+    q.f.kinds[q.slot] = (unsigned char)(ps.kind | (ps.end ? kKindEnd : 0));
+    ++q.slot;
+  }
+  if (c->nchains == 1) q.soff += (unsigned long long)nslots_of(ps.kind) * c->ch[0].nh;
+  q.poff += philox_passes(ps.kind);
+  return LCE_OK;
+}
+
+int enq_end(lce_ctx* c, Enq& q) {
+  q.f.nslots = q.slot;
+  q.f.npasses = q.poff;
+  q.f.nstream = c->rng == LCE_RNG_STREAM ? q.soff : 0;
+  launch_finalize(q.f, c->stream);
   CK(cudaGetLastError());
   return LCE_OK;
+}
+
+int enqueue(lce_ctx* c, const std::vector<unsigned char>& routines, int measflag, bool fuse_renorm,
+            cudaEvent_t* events = nullptr, int spt = 1) {
+  Enq q;
+  enq_begin(c, routines, measflag, fuse_renorm, spt, q);
+  for (size_t i = 0; i < q.passes.size(); ++i) {
+    if (int rc = enq_pass(c, q, i)) return rc;
+    if (events) CK(cudaEventRecord(events[i], c->stream));
+  }
+  return enq_end(c, q);
 }
 
 std::vector<unsigned char> sweep_routines(const lce_ctx* c);
@@ -320,7 +355,7 @@ int enqueue_persistent(lce_ctx* c, const std::vector<unsigned char>& routines, i
     if (reduce && slot >= c->part_slots) return fail(c, LCE_ERR_INVALID, "too many reduction slots");
     a.pass_off[i] = (unsigned short)poff;
     poff += philox_passes(ps.kind);
-    a.plan[i] = PlanEntry{ps.kind, (unsigned char)ps.eo, (unsigned char)ps.mu,
+    a.plan[i] = PlanEntry{ps.kind, (unsigned char)(ps.eo ^ c->eo_flip), (unsigned char)ps.mu,
                           reduce ? (unsigned char)slot : kNoSlot};
     a.stream_off[i] = soff;
     if (reduce) {
@@ -493,7 +528,14 @@ int download_t(lce_ctx* c, int chain, int which, Rout* u, Rout* a, long ld) {
   return LCE_OK;
 }
 
-lce_ctx* create_impl(const lce_params* p, int n) {
+// one z-slab of a decomposed lattice: its chain's first and last planes are
+// halos, the update passes visit the planes between them
+struct SlabInfo {
+  int site_off;  // site index of the first local site in the whole lattice (plane z0 - 1)
+  int eo_flip;   // local parity = whole-lattice parity ^ eo_flip
+};
+
+lce_ctx* create_impl(const lce_params* p, int n, const SlabInfo* slab = nullptr) {
   g_create_error.clear();
   if (!p || n < 1) {
     fail(nullptr, LCE_ERR_INVALID, "create: null params or no chains");
@@ -524,6 +566,7 @@ lce_ctx* create_impl(const lce_params* p, int n) {
   c->n_link_or = p[0].n_link_or;
   c->n_higgs_metro = p[0].n_higgs_metro;
   c->agauge_hits = p[0].agauge_hits == 3 ? 3 : 1;
+  c->eo_flip = slab ? slab->eo_flip : 0;
   c->params.assign(p, p + n);
   auto bail = [&](cudaError_t e, const char* where) -> lce_ctx* {
     g_create_error = std::string(where) + ": " + cudaGetErrorString(e);
@@ -582,11 +625,14 @@ lce_ctx* create_impl(const lce_params* p, int n) {
     d.gf_angle = p[i].gf_angle;
     d.key0 = (uint32_t)p[i].seed;
     d.key1 = (uint32_t)(p[i].seed >> 32);
+    d.s_lo = slab ? d.nxy : 0;
+    d.s_hi = slab ? d.nh - d.nxy : d.nh;
+    d.site_off = slab ? slab->site_off : 0;
     offs.push_back(off);
     off += 2 * (align256((size_t)6 * d.nh * lb) + align256((size_t)6 * d.nh * rb)) + align256((size_t)2 * d.nh * lb);
     c->ch.push_back(d);
-    c->blk.push_back(c->blk.back() + ceil_div(d.nh, kBlock));
-    c->blk2.push_back(c->blk2.back() + ceil_div(d.nh, 2 * kBlock));
+    c->blk.push_back(c->blk.back() + ceil_div(d.s_hi - d.s_lo, kBlock));
+    c->blk2.push_back(c->blk2.back() + ceil_div(d.s_hi - d.s_lo, 2 * kBlock));
     c->max_nh = std::max(c->max_nh, d.nh);
     c->max_L3 = std::max(c->max_L3, d.L3);
   }
@@ -803,6 +849,198 @@ int fa_loop(lce_ctx* c, int chain, double step, double limit, double* theta, int
 }  // namespace
 
 // ====================================================================== C ABI
+// ------------------------------------------------------------------ z-slabs
+// A lattice split along z into slabs (the reference's domain decomposition,
+// f/topology.f with dimproc = (1, 1, n), and its halo exchange around every
+// pass of f/staples.f / f/a_force.f), each slab a one-chain context on its
+// own device or sharing one.  Slab k holds the whole lattice's planes
+// z0 - 1 .. z0 + nz (z0 = k nz): its first and last local planes are halos,
+// the update passes visit the nz planes between them, and the Philox
+// counters use whole-lattice site indices, so a decomposed run draws the
+// uniforms of the undecomposed one and reproduces its fields bit for bit.
+// After every pass the written field's parity is exchanged: slab k copies
+// the last interior plane of slab k-1 into its plane 0 and the first
+// interior plane of slab k+1 into its plane nz+1 (periodic), on its own
+// stream, ordered by events (peer copies between devices).
+struct lce_slabs {
+  std::vector<lce_ctx*> slab;
+  std::vector<cudaEvent_t> ev_pass, ev_copy;
+  int L[3] = {0, 0, 0};
+  int nz = 0, nxy = 0, prec = LCE_PREC_F32;
+};
+
+namespace {
+
+int slabs_fail(int code, const std::string& m) {
+  set_thread_error(m);
+  return code;
+}
+#define SCK(call)                                                                                   \
+  do {                                                                                              \
+    cudaError_t e_ = (call);                                                                        \
+    if (e_ != cudaSuccess) return slabs_fail(LCE_ERR_CUDA, std::string(#call) + ": " + cudaGetErrorString(e_)); \
+  } while (0)
+
+// a slab context's error, made the thread's last error (lce_last_error(NULL))
+int slab_rc(lce_ctx* c, int rc) {
+  if (rc && !c->err.empty()) set_thread_error(c->err);
+  return rc;
+}
+
+// device address of local plane z of a slab's field at local parity p: the
+// links U_mu (f = mu) or component k of the Higgs field (f = -1)
+char* slab_plane(lce_ctx* c, int f, int p, int z, int k) {
+  const ChainDev& d = c->ch[0];
+  if (f >= 0) return (char*)d.u + (((size_t)(f * 2 + p)) * d.nh + (size_t)z * d.nxy) * link_bytes(c->prec);
+  return (char*)d.a + (((size_t)(p * 3 + k)) * d.nh + (size_t)z * d.nxy) * real_bytes(c->prec);
+}
+
+// halo planes of field f at whole-lattice parity pg, once every slab's
+// stream has recorded ev_pass; then each stream waits for its neighbours'
+// copies before a later pass may overwrite the planes they read
+int slab_exchange(lce_slabs* S, int f, int pg) {
+  const int n = (int)S->slab.size(), nz = S->nz;
+  for (int k = 0; k < n; ++k) {
+    lce_ctx* c = S->slab[k];
+    DeviceScope ds_(c->device);
+    for (int side = 0; side < 2; ++side) {
+      const int j = side == 0 ? (k + n - 1) % n : (k + 1) % n;
+      lce_ctx* cj = S->slab[j];
+      const int zs = side == 0 ? nz : 1, zd = side == 0 ? 0 : nz + 1;
+      const int ps = pg ^ cj->eo_flip, pd = pg ^ c->eo_flip;
+      const size_t bytes = (size_t)S->nxy * (f >= 0 ? link_bytes(c->prec) : real_bytes(c->prec));
+      SCK(cudaStreamWaitEvent(c->stream, S->ev_pass[j], 0));
+      for (int comp = 0; comp < (f >= 0 ? 1 : 3); ++comp) {
+        void* dst = slab_plane(c, f, pd, zd, comp);
+        const void* src = slab_plane(cj, f, ps, zs, comp);
+        if (c->device == cj->device) SCK(cudaMemcpyAsync(dst, src, bytes, cudaMemcpyDeviceToDevice, c->stream));
+        else SCK(cudaMemcpyPeerAsync(dst, c->device, src, cj->device, bytes, c->stream));
+      }
+    }
+    SCK(cudaEventRecord(S->ev_copy[k], c->stream));
+  }
+  for (int k = 0; k < n; ++k) {
+    lce_ctx* c = S->slab[k];
+    DeviceScope ds_(c->device);
+    SCK(cudaStreamWaitEvent(c->stream, S->ev_copy[(k + n - 1) % n], 0));
+    SCK(cudaStreamWaitEvent(c->stream, S->ev_copy[(k + 1) % n], 0));
+  }
+  return LCE_OK;
+}
+
+// the measured quantities of the whole lattice from the slabs' summed
+// per-slot totals: the formulas of the finalize kernel (f/meas1.f inputs,
+// f/ahiggs2.f:259-264, f/agauge.f:195-200, f/agauge1.f:226-231)
+void slab_meas(const std::vector<double>& tot, const FinalizeArgs& f, double V, lce_meas* m) {
+  double h[kNQ] = {0, 0, 0, 0}, l[kNQ] = {0, 0, 0, 0};
+  for (int i = 0; i < f.nslots; ++i) {
+    const double* t = tot.data() + (size_t)i * kNQ;
+    const int kind = f.kinds[i] & 0x7f;
+    const bool end = (f.kinds[i] & kKindEnd) != 0;
+    double* acc = kind <= kHiggsMetro ? h : l;
+    for (int q = 0; q < kNQ; ++q) acc[q] += t[q];
+    if (!end) continue;
+    if (kind == kHiggsHB || kind == kHiggsOR) {
+      m->a2 = h[1] / V;
+      m->a4 = h[2] / V;
+      m->akin = h[3] / (6.0 * V);
+      (kind == kHiggsHB ? m->acc_hb : m->acc_or) = h[0] / V;
+    } else if (kind == kLinkHB) {
+      m->plaq = l[2] / (12.0 * V);
+      m->acc_gauge = (l[0] / (3.0 * V)) * (l[1] / (12.0 * V));
+    } else if (kind == kLinkHB3) {
+      m->plaq = l[2] / (12.0 * V);
+      m->acc_gauge = (l[0] / (3.0 * V)) * (l[1] / (12.0 * V) / 3.0);
+    } else if (kind == kLinkOR) {
+      m->acc_link_or = l[0] / (3.0 * V);
+    }
+    for (int q = 0; q < kNQ; ++q) acc[q] = 0.0;
+  }
+}
+
+int slab_sweep(lce_slabs* S, int measflag, lce_meas* m) {
+  const int n = (int)S->slab.size();
+  std::vector<Enq> q(n);
+  const std::vector<unsigned char> routines = sweep_routines(S->slab[0]);
+  for (int k = 0; k < n; ++k) enq_begin(S->slab[k], routines, measflag, true, 1, q[k]);
+  for (size_t i = 0; i < q[0].passes.size(); ++i) {
+    for (int k = 0; k < n; ++k) {
+      lce_ctx* c = S->slab[k];
+      DeviceScope ds_(c->device);
+      if (int rc = enq_pass(c, q[k], i)) return slab_rc(c, rc);
+      SCK(cudaEventRecord(S->ev_pass[k], c->stream));
+    }
+    const Pass& ps = q[0].passes[i];
+    if (int rc = slab_exchange(S, ps.kind <= kHiggsMetro ? -1 : ps.mu, ps.eo)) return rc;
+  }
+  for (int k = 0; k < n; ++k) {
+    lce_ctx* c = S->slab[k];
+    DeviceScope ds_(c->device);
+    if (int rc = enq_end(c, q[k])) return slab_rc(c, rc);
+  }
+  // per-slot totals (the slot count is known once the finalize is queued)
+  std::vector<double> tot((size_t)q[0].f.nslots * kNQ, 0.0), t(tot.size());
+  for (int k = 0; k < n; ++k) {
+    lce_ctx* c = S->slab[k];
+    DeviceScope ds_(c->device);
+    if (int rc = status_check(c)) return slab_rc(c, rc);  // synchronises the slab's stream
+    if (measflag == 1 && !t.empty()) {
+      SCK(cudaMemcpy(t.data(), c->totals_d, t.size() * sizeof(double), cudaMemcpyDeviceToHost));
+      for (size_t e = 0; e < t.size(); ++e) tot[e] += t[e];
+    }
+  }
+  if (m) {
+    std::memset(m, 0, sizeof(*m));
+    m->delta = S->slab[0]->params[0].delta0;
+    if (measflag == 1) slab_meas(tot, q[0].f, (double)S->L[0] * S->L[1] * S->L[2], m);
+  }
+  return LCE_OK;
+}
+
+// whole-lattice arrays (reference order: u[mu][eo][site < ld][4],
+// a[eo][site < ld][3]) <-> each slab's planes, halos included on the way in
+template <typename T>
+int slabs_copy(lce_slabs* S, T* u, T* a, long ld, bool in) {
+  const int n = (int)S->slab.size(), nz = S->nz, nxy = S->nxy, L3 = S->L[2];
+  const long nhl = (long)(nz + 2) * nxy;
+  std::vector<T> ul((size_t)6 * nhl * 4), al((size_t)2 * nhl * 3);
+  for (int k = 0; k < n; ++k) {
+    lce_ctx* c = S->slab[k];
+    const int z0 = k * nz;
+    if (!in) {
+      int rc = std::is_same<T, double>::value
+                   ? lce_download_f64(c, 0, LCE_FIELDS, (double*)ul.data(), (double*)al.data(), nhl)
+                   : lce_download(c, 0, LCE_FIELDS, (float*)ul.data(), (float*)al.data(), nhl);
+      if (rc) return slab_rc(c, rc);
+    }
+    for (int zl = in ? 0 : 1; zl <= (in ? nz + 1 : nz); ++zl) {
+      const int zg = (z0 - 1 + zl + L3) % L3;
+      for (int pl = 0; pl < 2; ++pl) {
+        const int pg = pl ^ c->eo_flip;
+        for (int mu = 0; mu < 3; ++mu) {
+          T* loc = &ul[(((size_t)mu * 2 + pl) * nhl + (size_t)zl * nxy) * 4];
+          T* glo = &u[(((size_t)mu * 2 + pg) * ld + (size_t)zg * nxy) * 4];
+          if (in) std::memcpy(loc, glo, sizeof(T) * 4 * nxy);
+          else std::memcpy(glo, loc, sizeof(T) * 4 * nxy);
+        }
+        T* loc = &al[((size_t)pl * nhl + (size_t)zl * nxy) * 3];
+        T* glo = &a[((size_t)pg * ld + (size_t)zg * nxy) * 3];
+        if (in) std::memcpy(loc, glo, sizeof(T) * 3 * nxy);
+        else std::memcpy(glo, loc, sizeof(T) * 3 * nxy);
+      }
+    }
+    if (in) {
+      int rc = std::is_same<T, double>::value
+                   ? lce_upload_f64(c, 0, LCE_FIELDS, (const double*)ul.data(), (const double*)al.data(), nhl)
+                   : lce_upload(c, 0, LCE_FIELDS, (const float*)ul.data(), (const float*)al.data(), nhl);
+      if (rc) return slab_rc(c, rc);
+    }
+  }
+  return LCE_OK;
+}
+
+}  // namespace
+
 extern "C" {
 
 const char* lce_version(void) { return "lceqcd_b200 1.0 (sm_100a)"; }
@@ -1608,6 +1846,126 @@ int lce_timer_stop(lce_ctx* c, float* ms) {
   CK(cudaEventSynchronize(c->ev1));
   CK(cudaEventElapsedTime(ms, c->ev0, c->ev1));
   return LCE_OK;
+}
+
+// ---- z-slab decomposition
+lce_slabs* lce_slabs_create(const lce_params* p, int nslabs, const int* devices) {
+  g_create_error.clear();
+  if (!p || nslabs < 1 || !devices) {
+    slabs_fail(LCE_ERR_INVALID, "slabs_create: null params or devices, or no slabs");
+    return nullptr;
+  }
+  std::string why;
+  if (!valid_params(*p, why)) {
+    slabs_fail(LCE_ERR_INVALID, "slabs_create: " + why);
+    return nullptr;
+  }
+  const int L3 = p->L[2], nz = L3 / nslabs;
+  if (L3 % nslabs != 0 || nz < 2 || (nz & 1)) {
+    slabs_fail(LCE_ERR_INVALID, "slabs_create: L3 must split into slabs of an even number (>= 2) of planes");
+    return nullptr;
+  }
+  if (p->rng != LCE_RNG_PHILOX || p->n_higgs_metro != 0) {
+    slabs_fail(LCE_ERR_UNSUPPORTED,
+               "slabs_create: Philox uniforms only, and no Higgs Metropolis step (its step size adapts to the "
+               "whole lattice's acceptance)");
+    return nullptr;
+  }
+  lce_slabs* S = new lce_slabs();
+  S->L[0] = p->L[0];
+  S->L[1] = p->L[1];
+  S->L[2] = L3;
+  S->nz = nz;
+  S->nxy = p->L[0] * p->L[1] / 2;
+  S->prec = p->precision;
+  for (int k = 0; k < nslabs; ++k) {
+    lce_params q = *p;
+    q.L[2] = nz + 2;
+    q.device = devices[k];
+    q.sweep_mode = LCE_SWEEP_PASSES;
+    const int z0 = k * nz;
+    const SlabInfo si{(z0 - 1) * S->nxy, (z0 + 1) & 1};
+    DeviceScope ds_(devices[k]);
+    lce_ctx* c = create_impl(&q, 1, &si);
+    if (!c) {
+      const std::string m = "slabs_create: slab " + std::to_string(k) + ": " + g_create_error;
+      lce_slabs_destroy(S);
+      slabs_fail(LCE_ERR_CUDA, m);
+      g_create_error = m;
+      return nullptr;
+    }
+    S->slab.push_back(c);
+    cudaEvent_t e1 = nullptr, e2 = nullptr;
+    if (cudaEventCreateWithFlags(&e1, cudaEventDisableTiming) != cudaSuccess ||
+        cudaEventCreateWithFlags(&e2, cudaEventDisableTiming) != cudaSuccess) {
+      if (e1) cudaEventDestroy(e1);
+      lce_slabs_destroy(S);
+      g_create_error = "slabs_create: cudaEventCreate";
+      slabs_fail(LCE_ERR_CUDA, g_create_error);
+      return nullptr;
+    }
+    S->ev_pass.push_back(e1);
+    S->ev_copy.push_back(e2);
+  }
+  // direct peer copies between the devices that hold neighbouring slabs
+  for (int k = 0; k < nslabs; ++k) {
+    const int d0 = devices[k], d1 = devices[(k + 1) % nslabs];
+    if (d0 == d1) continue;
+    int ok01 = 0, ok10 = 0;
+    cudaDeviceCanAccessPeer(&ok01, d0, d1);
+    cudaDeviceCanAccessPeer(&ok10, d1, d0);
+    if (ok01) {
+      DeviceScope ds_(d0);
+      if (cudaDeviceEnablePeerAccess(d1, 0) != cudaSuccess) cudaGetLastError();  // already enabled is fine
+    }
+    if (ok10) {
+      DeviceScope ds_(d1);
+      if (cudaDeviceEnablePeerAccess(d0, 0) != cudaSuccess) cudaGetLastError();
+    }
+  }
+  return S;
+}
+
+void lce_slabs_destroy(lce_slabs* h) {
+  lce_slabs* S = h;
+  if (!S) return;
+  for (size_t k = 0; k < S->slab.size(); ++k) {
+    DeviceScope ds_(S->slab[k]->device);
+    if (k < S->ev_pass.size()) cudaEventDestroy(S->ev_pass[k]);
+    if (k < S->ev_copy.size()) cudaEventDestroy(S->ev_copy[k]);
+    lce_destroy(S->slab[k]);
+  }
+  delete S;
+}
+
+int lce_slabs_upload(lce_slabs* h, const float* u, const float* a, long ld) {
+  lce_slabs* S = h;
+  if (!S || !u || !a || ld < (long)S->nxy * S->L[2]) return LCE_ERR_INVALID;
+  return slabs_copy<float>(S, const_cast<float*>(u), const_cast<float*>(a), ld, true);
+}
+
+int lce_slabs_upload_f64(lce_slabs* h, const double* u, const double* a, long ld) {
+  lce_slabs* S = h;
+  if (!S || !u || !a || ld < (long)S->nxy * S->L[2]) return LCE_ERR_INVALID;
+  return slabs_copy<double>(S, const_cast<double*>(u), const_cast<double*>(a), ld, true);
+}
+
+int lce_slabs_download(lce_slabs* h, float* u, float* a, long ld) {
+  lce_slabs* S = h;
+  if (!S || !u || !a || ld < (long)S->nxy * S->L[2]) return LCE_ERR_INVALID;
+  return slabs_copy<float>(S, u, a, ld, false);
+}
+
+int lce_slabs_download_f64(lce_slabs* h, double* u, double* a, long ld) {
+  lce_slabs* S = h;
+  if (!S || !u || !a || ld < (long)S->nxy * S->L[2]) return LCE_ERR_INVALID;
+  return slabs_copy<double>(S, u, a, ld, false);
+}
+
+int lce_slabs_sweep(lce_slabs* h, int measflag, lce_meas* m) {
+  lce_slabs* S = h;
+  if (!S || (measflag != 0 && measflag != 1)) return LCE_ERR_INVALID;
+  return slab_sweep(S, measflag, m);
 }
 
 }  // extern "C"

@@ -54,6 +54,11 @@ struct ChainDev {
   void* uf;
   void* af;
   void* g;   // gauge transform of the last tracked gauge fixing, [parity][site]
+  // sites the update passes visit, [s_lo, s_hi) within each parity (0, nh for
+  // a whole lattice; the interior planes of a z-slab, whose first and last
+  // planes are halos), and the offset that turns a site index into the
+  // whole lattice's for the Philox counters
+  int s_lo, s_hi, site_off;
 };
 
 // mutable state shared by the chains of one context

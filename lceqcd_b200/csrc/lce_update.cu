@@ -160,7 +160,7 @@ __device__ __forceinline__ bool setup_uniforms(const PassArgs& p, const ChainDev
     }
     U.fill_stream(p.stream + base, ch.nh, layout, s);
   } else {
-    U.fill_philox(ch.key0, ch.key1, p.st->pass_ctr + p.pass_off + hit, s);
+    U.fill_philox(ch.key0, ch.key1, p.st->pass_ctr + p.pass_off + hit, s + ch.site_off);
   }
   return true;
 }
@@ -175,16 +175,16 @@ __device__ __forceinline__ void higgs_tile(const PassArgs& p, int tile) {
   const int c = p.nchains > 1 ? find_chain(p.blk_begin, p.nchains, tile) : 0;
   const ChainDev& ch = p.chains[c];
   // a tile is kBlock * SPT consecutive sites; thread t takes t, t + kBlock, ...
-  const int s0 = (tile - __ldg(p.blk_begin + c)) * kBlock * SPT + threadIdx.x;
-  const int eo = p.eo, nh = ch.nh;
-  const Coord X0 = site_coord(eo, s0 < nh ? s0 : 0, ch.hx, ch.nxy, ch.dhx, ch.dnxy);
+  const int s0 = ch.s_lo + (tile - __ldg(p.blk_begin + c)) * kBlock * SPT + threadIdx.x;
+  const int eo = p.eo, nh = ch.nh, s_hi = ch.s_hi;
+  const Coord X0 = site_coord(eo, s0 < s_hi ? s0 : ch.s_lo, ch.hx, ch.nxy, ch.dhx, ch.dnxy);
   unsigned acc[1] = {0u};
   double q[3] = {0.0, 0.0, 0.0};
   if (PDL) pdl_wait();
 #pragma unroll 1
   for (int r = 0; r < SPT; ++r) {
     const int s = s0 + r * kBlock;
-    if (s >= nh) break;
+    if (s >= s_hi) break;
     const Coord X = r == 0 ? X0 : site_coord(eo, s, ch.hx, ch.nxy, ch.dhx, ch.dnxy);
     constexpr int NS = MODE == 0 ? 7 : (MODE == 1 ? 1 : 4);
     const int layout = MODE == 2 ? kTriple : kPlanar;
@@ -285,16 +285,16 @@ __device__ __forceinline__ void link_tile(const PassArgs& p, int tile) {
   const int c = p.nchains > 1 ? find_chain(p.blk_begin, p.nchains, tile) : 0;
   const ChainDev& ch = p.chains[c];
   // a tile is kBlock * SPT consecutive sites; thread t takes t, t + kBlock, ...
-  const int s0 = (tile - __ldg(p.blk_begin + c)) * kBlock * SPT + threadIdx.x;
-  const int eo = p.eo, oe = 1 - eo, nh = ch.nh;
-  const Coord X0 = site_coord(eo, s0 < nh ? s0 : 0, ch.hx, ch.nxy, ch.dhx, ch.dnxy);
+  const int s0 = ch.s_lo + (tile - __ldg(p.blk_begin + c)) * kBlock * SPT + threadIdx.x;
+  const int eo = p.eo, oe = 1 - eo, nh = ch.nh, s_hi = ch.s_hi;
+  const Coord X0 = site_coord(eo, s0 < s_hi ? s0 : ch.s_lo, ch.hx, ch.nxy, ch.dhx, ch.dnxy);
   unsigned cnt[2] = {0u, 0u};
   double pl[1] = {0.0};
   if (PDL) pdl_wait();
 #pragma unroll 1
   for (int r = 0; r < SPT; ++r) {
     const int s = s0 + r * kBlock;
-    if (s >= nh) break;
+    if (s >= s_hi) break;
     const Coord X = r == 0 ? X0 : site_coord(eo, s, ch.hx, ch.nxy, ch.dhx, ch.dnxy);
     Uniforms<R, OR ? 1 : 7> Un;
     if (setup_uniforms<R, OR ? 1 : 7>(p, ch, s, OR ? kPlanar : kTriple, Un)) {

@@ -474,6 +474,62 @@ class GaugeNet:
         return loss.value
 
 
+class SlabLattice:
+    """A lattice split along z into slabs on one or more GPUs (lce_slabs_*:
+    the reference's domain decomposition with a halo exchange after every
+    pass).  A sweep reproduces the fields of an undecomposed Lattice with
+    the same parameters bit for bit; measurements are the whole lattice's."""
+
+    def __init__(self, L=(16, 16, 16), nslabs=2, devices=None, beta=9.0, x=0.1, y=0.5, **kw):
+        self.lib = load()
+        self.params = Params(L=tuple(L), beta=beta, x=x, y=y, **kw)
+        devs = list(devices) if devices is not None else [self.params.device] * nslabs
+        if len(devs) != nslabs:
+            raise ValueError("one device per slab")
+        arr = (C.c_int * nslabs)(*devs)
+        p = self.params.to_c()
+        h = self.lib.lce_slabs_create(C.byref(p), nslabs, arr)
+        if not h:
+            raise _lib.LceError(_lib.LCE_ERR_INVALID, "lce_slabs_create: " + self.lib.lce_last_error(None).decode())
+        self.h = C.c_void_p(h)
+        self.nh = L[0] * L[1] * L[2] // 2
+        self.dtype = np.float64 if self.params.precision == "f64" else np.float32
+
+    def _ck(self, rc):
+        if rc < 0:
+            raise _lib.LceError(rc, f"{self.lib.lce_strerror(rc).decode()}: {self.lib.lce_last_error(None).decode()}")
+        return rc
+
+    def upload(self, u, a):
+        f64 = np.asarray(u).dtype == np.float64
+        dt = np.float64 if f64 else np.float32
+        uu = np.ascontiguousarray(u, dt).reshape(3, 2, self.nh, 4)
+        aa = np.ascontiguousarray(a, dt).reshape(2, self.nh, 3)
+        fn = self.lib.lce_slabs_upload_f64 if f64 else self.lib.lce_slabs_upload
+        self._ck(fn(self.h, _ptr(uu), _ptr(aa), self.nh))
+
+    def download(self, dtype=None):
+        dt = dtype or self.dtype
+        u = np.zeros((3, 2, self.nh, 4), dt)
+        a = np.zeros((2, self.nh, 3), dt)
+        fn = self.lib.lce_slabs_download_f64 if dt == np.float64 else self.lib.lce_slabs_download
+        self._ck(fn(self.h, _ptr(u), _ptr(a), self.nh))
+        return u, a
+
+    def sweep(self, measflag: int = 1) -> dict:
+        m = LceMeas()
+        self._ck(self.lib.lce_slabs_sweep(self.h, measflag, C.byref(m)))
+        return m.as_dict()
+
+    def close(self):
+        if getattr(self, "h", None):
+            self.lib.lce_slabs_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        self.close()
+
+
 class Lattice(_Context):
     """One chain on one GPU (the drop-in for the reference's single lattice)."""
 

@@ -1,0 +1,65 @@
+"""z-slab decomposition (lce_slabs_*, the reference's MPI domain
+decomposition with a halo exchange after every pass): the lattice split over
+1, 2 or 4 slabs reproduces the undecomposed context's fields bit for bit
+(whole-lattice Philox counters) and its measurements to summation order, in
+FP64 and FP32; the slabs here share one GPU, so the halo copies are
+device-to-device (peer copies between GPUs take the same path)."""
+import numpy as np
+import pytest
+
+from oracle.oracle import hot_config
+
+pytestmark = pytest.mark.gpu
+lce = pytest.importorskip("lceqcd_b200")
+from lceqcd_b200 import LceError, Lattice, SlabLattice  # noqa: E402
+
+KEYS = ("plaq", "akin", "a2", "a4", "acc_gauge", "acc_hb", "acc_or")
+
+
+@pytest.mark.parametrize("precision", ["f64", "f32"])
+@pytest.mark.parametrize("L,nslabs", [((4, 4, 8), 1), ((4, 4, 8), 2), ((8, 6, 8), 4), ((6, 4, 12), 3),
+                                      ((8, 8, 16), 2)])
+def test_slabs_reproduce_the_whole_lattice(precision, L, nslabs):
+    dt = np.float64 if precision == "f64" else np.float32
+    u, a = hot_config(L, seed=31, dtype=dt)
+    kw = dict(beta=12.0, x=0.09, y=0.3, precision=precision, seed=4242, n_link_or=1)
+    g = Lattice(L, sweep_mode="passes", **kw)
+    g.upload(u, a)
+    s = SlabLattice(L, nslabs, **kw)
+    s.upload(u, a)
+    for k in range(3):
+        mg, ms = g.sweep(1), s.sweep(1)
+        ug, ag = g.download(dtype=dt)
+        us, as_ = s.download(dtype=dt)
+        np.testing.assert_array_equal(us, ug)
+        np.testing.assert_array_equal(as_, ag)
+        for key in KEYS + ("acc_link_or",):
+            assert abs(ms[key] - mg[key]) <= 1e-12 * max(1.0, abs(mg[key])), (k, key)
+    s.sweep(0)
+    g.sweep(0)
+    np.testing.assert_array_equal(s.download(dtype=dt)[0], g.download(dtype=dt)[0])
+    s.close()
+
+
+def test_slabs_three_hit_link_update():
+    L = (4, 6, 8)
+    u, a = hot_config(L, seed=5)
+    kw = dict(beta=9.0, x=0.1, y=0.45, precision="f64", seed=7, agauge_hits=3)
+    g = Lattice(L, sweep_mode="passes", **kw)
+    g.upload(u, a)
+    s = SlabLattice(L, 2, **kw)
+    s.upload(u, a)
+    for _ in range(2):
+        mg, ms = g.sweep(1), s.sweep(1)
+    np.testing.assert_array_equal(s.download()[0], g.download()[0])
+    assert abs(ms["acc_gauge"] - mg["acc_gauge"]) <= 1e-12
+
+
+def test_slabs_reject_what_they_cannot_do():
+    for L, n in (((4, 4, 6), 2), ((4, 4, 8), 8), ((4, 4, 8), 3)):  # odd, too thin, not a divisor
+        with pytest.raises(LceError):
+            SlabLattice(L, n, precision="f64")
+    with pytest.raises(LceError):
+        SlabLattice((4, 4, 8), 2, rng="stream")
+    with pytest.raises(LceError):
+        SlabLattice((4, 4, 8), 2, n_higgs_metro=1)
