@@ -42,6 +42,7 @@ struct lce_ctx {
   int nchains = 0;
   int n_link_or = 0, n_higgs_metro = 0;
   int eo_flip = 0;        // a z-slab's local parity of whole-lattice parity 0
+  int s_lo = 0, site_off = 0;  // a z-slab's first visited site and Philox site offset (PassArgs)
   int agauge_hits = 1;  // 1: f/agauge.f, 3: f/agauge1.f in lce_sweep
   std::vector<lce_params> params;
   std::vector<ChainDev> ch;
@@ -277,6 +278,8 @@ int enq_pass(lce_ctx* c, Enq& q, size_t i) {
   a.nchains = c->nchains;
   a.eo = ps.eo ^ c->eo_flip;
   a.fuse_renorm = q.fuse ? 1 : 0;
+  a.s_lo = c->s_lo;
+  a.site_off = c->site_off;
   if (ps.kind <= kHiggsMetro) {
     if (c->prec == LCE_PREC_F64) launch_higgs<double>(ps.kind, a, nblocks, c->stream);
     else launch_higgs<float>(ps.kind, a, nblocks, c->stream);
@@ -335,6 +338,8 @@ int enqueue_persistent(lce_ctx* c, const std::vector<unsigned char>& routines, i
   b.nchains = c->nchains;
   b.fuse_renorm = fuse_renorm ? 1 : 0;
   b.spt = 1;
+  b.s_lo = c->s_lo;
+  b.site_off = c->site_off;
   FinalizeArgs& f = a.fin;
   f.chains = c->ch_d;
   f.blk_begin = c->blk_d;
@@ -567,6 +572,8 @@ lce_ctx* create_impl(const lce_params* p, int n, const SlabInfo* slab = nullptr)
   c->n_higgs_metro = p[0].n_higgs_metro;
   c->agauge_hits = p[0].agauge_hits == 3 ? 3 : 1;
   c->eo_flip = slab ? slab->eo_flip : 0;
+  c->s_lo = slab ? p[0].L[0] * p[0].L[1] / 2 : 0;
+  c->site_off = slab ? slab->site_off : 0;
   c->params.assign(p, p + n);
   auto bail = [&](cudaError_t e, const char* where) -> lce_ctx* {
     g_create_error = std::string(where) + ": " + cudaGetErrorString(e);
@@ -625,14 +632,13 @@ lce_ctx* create_impl(const lce_params* p, int n, const SlabInfo* slab = nullptr)
     d.gf_angle = p[i].gf_angle;
     d.key0 = (uint32_t)p[i].seed;
     d.key1 = (uint32_t)(p[i].seed >> 32);
-    d.s_lo = slab ? d.nxy : 0;
-    d.s_hi = slab ? d.nh - d.nxy : d.nh;
-    d.site_off = slab ? slab->site_off : 0;
+
     offs.push_back(off);
     off += 2 * (align256((size_t)6 * d.nh * lb) + align256((size_t)6 * d.nh * rb)) + align256((size_t)2 * d.nh * lb);
     c->ch.push_back(d);
-    c->blk.push_back(c->blk.back() + ceil_div(d.s_hi - d.s_lo, kBlock));
-    c->blk2.push_back(c->blk2.back() + ceil_div(d.s_hi - d.s_lo, 2 * kBlock));
+    const int nvis = slab ? d.nh - 2 * d.nxy : d.nh;  // sites a pass visits per parity
+    c->blk.push_back(c->blk.back() + ceil_div(nvis, kBlock));
+    c->blk2.push_back(c->blk2.back() + ceil_div(nvis, 2 * kBlock));
     c->max_nh = std::max(c->max_nh, d.nh);
     c->max_L3 = std::max(c->max_L3, d.L3);
   }

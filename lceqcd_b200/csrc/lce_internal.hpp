@@ -54,11 +54,6 @@ struct ChainDev {
   void* uf;
   void* af;
   void* g;   // gauge transform of the last tracked gauge fixing, [parity][site]
-  // sites the update passes visit, [s_lo, s_hi) within each parity (0, nh for
-  // a whole lattice; the interior planes of a z-slab, whose first and last
-  // planes are halos), and the offset that turns a site index into the
-  // whole lattice's for the Philox counters
-  int s_lo, s_hi, site_off;
 };
 
 // mutable state shared by the chains of one context
@@ -119,6 +114,11 @@ struct PassArgs {
   int eo;
   int fuse_renorm;
   int spt;                // sites per thread (a tile is kBlock * spt sites)
+  // z-slab of a decomposed lattice (single-chain contexts): the passes visit
+  // sites [s_lo, nh - s_lo) of each parity (the first and last planes are
+  // halos), and site_off turns a site index into the whole lattice's for the
+  // Philox counters; both 0 otherwise
+  int s_lo, site_off;
 };
 
 struct FinalizeArgs {

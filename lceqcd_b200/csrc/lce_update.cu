@@ -160,7 +160,7 @@ __device__ __forceinline__ bool setup_uniforms(const PassArgs& p, const ChainDev
     }
     U.fill_stream(p.stream + base, ch.nh, layout, s);
   } else {
-    U.fill_philox(ch.key0, ch.key1, p.st->pass_ctr + p.pass_off + hit, s + ch.site_off);
+    U.fill_philox(ch.key0, ch.key1, p.st->pass_ctr + p.pass_off + hit, s + p.site_off);
   }
   return true;
 }
@@ -175,9 +175,9 @@ __device__ __forceinline__ void higgs_tile(const PassArgs& p, int tile) {
   const int c = p.nchains > 1 ? find_chain(p.blk_begin, p.nchains, tile) : 0;
   const ChainDev& ch = p.chains[c];
   // a tile is kBlock * SPT consecutive sites; thread t takes t, t + kBlock, ...
-  const int s0 = ch.s_lo + (tile - __ldg(p.blk_begin + c)) * kBlock * SPT + threadIdx.x;
-  const int eo = p.eo, nh = ch.nh, s_hi = ch.s_hi;
-  const Coord X0 = site_coord(eo, s0 < s_hi ? s0 : ch.s_lo, ch.hx, ch.nxy, ch.dhx, ch.dnxy);
+  const int s0 = p.s_lo + (tile - __ldg(p.blk_begin + c)) * kBlock * SPT + threadIdx.x;
+  const int eo = p.eo, nh = ch.nh, s_hi = nh - p.s_lo;
+  const Coord X0 = site_coord(eo, s0 < s_hi ? s0 : p.s_lo, ch.hx, ch.nxy, ch.dhx, ch.dnxy);
   unsigned acc[1] = {0u};
   double q[3] = {0.0, 0.0, 0.0};
   if (PDL) pdl_wait();
@@ -285,9 +285,9 @@ __device__ __forceinline__ void link_tile(const PassArgs& p, int tile) {
   const int c = p.nchains > 1 ? find_chain(p.blk_begin, p.nchains, tile) : 0;
   const ChainDev& ch = p.chains[c];
   // a tile is kBlock * SPT consecutive sites; thread t takes t, t + kBlock, ...
-  const int s0 = ch.s_lo + (tile - __ldg(p.blk_begin + c)) * kBlock * SPT + threadIdx.x;
-  const int eo = p.eo, oe = 1 - eo, nh = ch.nh, s_hi = ch.s_hi;
-  const Coord X0 = site_coord(eo, s0 < s_hi ? s0 : ch.s_lo, ch.hx, ch.nxy, ch.dhx, ch.dnxy);
+  const int s0 = p.s_lo + (tile - __ldg(p.blk_begin + c)) * kBlock * SPT + threadIdx.x;
+  const int eo = p.eo, oe = 1 - eo, nh = ch.nh, s_hi = nh - p.s_lo;
+  const Coord X0 = site_coord(eo, s0 < s_hi ? s0 : p.s_lo, ch.hx, ch.nxy, ch.dhx, ch.dnxy);
   unsigned cnt[2] = {0u, 0u};
   double pl[1] = {0.0};
   if (PDL) pdl_wait();
