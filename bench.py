@@ -389,6 +389,35 @@ def extras(args, peak):
         lat.close()
     except Exception as e:
         out["net_train_128cubed"] = {"error": repr(e)[:300]}
+    # z-slab decomposition on one GPU: the 256^3 sweep split into 2 slabs (halo
+    # exchange after every pass, launches without a graph) against the same
+    # lattice undecomposed -- the cost of the decomposition itself
+    try:
+        from lceqcd_b200 import SlabLattice
+        L = (256, 256, 256)
+        g = Lattice(L, **COUP, precision="f32", seed=51, sweep_mode="passes")
+        g.init_hot(52)
+        u, a = g.download()
+        s = SlabLattice(L, 2, **COUP, precision="f32", seed=51)
+        s.upload(u, a)
+        del u, a
+
+        def wall(fn, n):
+            fn()
+            t0 = time.perf_counter()
+            for _ in range(n):
+                fn()
+            return (time.perf_counter() - t0) / n * 1e3
+
+        ms_s = wall(lambda: s.sweep(1), 5)  # returns after every slab's stream is synchronised
+        ms_g = wall(lambda: g.sweep(1), 5)  # returns after the measurements are read back
+        out["slabs_256cubed_one_gpu"] = {"ms_per_sweep_2_slabs": ms_s, "ms_per_sweep_undecomposed": ms_g,
+                                         "overhead": ms_s / ms_g - 1.0,
+                                         "note": "host wall clock around synchronised sweeps; both on one GPU"}
+        s.close()
+        g.close()
+    except Exception as e:
+        out["slabs_256cubed_one_gpu"] = {"error": repr(e)[:300]}
     # batched ensemble: 96 chains (32 each of 16^3, 32^3, 48^3) over the
     # coupling grid, against the same chains run one context at a time
     try:
