@@ -328,9 +328,10 @@ int lce_timer_stop(lce_ctx* ctx, float* ms);
  * (peer copies between devices, ordered by events).  The Philox counters use
  * whole-lattice site indices, so the fields after a sweep are bit for bit
  * those of an undecomposed context with the same seed; measurements are the
- * whole lattice's (sums over slabs, in another order).  Philox only, the
- * sweep composition of lce_sweep without ahiggs1 (n_higgs_metro = 0); no
- * gauge fixing or correlators on a decomposed lattice. */
+ * whole lattice's (sums over slabs, in another order), and the ahiggs1 step
+ * adapts to the whole lattice's acceptance.  Philox only, the sweep
+ * composition of lce_sweep; no gauge fixing or correlators on a decomposed
+ * lattice. */
 typedef struct lce_slabs lce_slabs;
 lce_slabs* lce_slabs_create(const lce_params* p, int nslabs, const int* devices);  /* NULL: lce_last_error(NULL) */
 void lce_slabs_destroy(lce_slabs* s);

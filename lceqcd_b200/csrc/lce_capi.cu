@@ -873,6 +873,7 @@ struct lce_slabs {
   std::vector<cudaEvent_t> ev_pass, ev_copy;
   int L[3] = {0, 0, 0};
   int nz = 0, nxy = 0, prec = LCE_PREC_F32;
+  double delta = 0.0;  // ahiggs1 step of the whole lattice (every slab holds a copy)
 };
 
 namespace {
@@ -937,7 +938,10 @@ int slab_exchange(lce_slabs* S, int f, int pg) {
 // the measured quantities of the whole lattice from the slabs' summed
 // per-slot totals: the formulas of the finalize kernel (f/meas1.f inputs,
 // f/ahiggs2.f:259-264, f/agauge.f:195-200, f/agauge1.f:226-231)
-void slab_meas(const std::vector<double>& tot, const FinalizeArgs& f, double V, lce_meas* m) {
+// delta: the whole lattice's ahiggs1 step, adapted as the finalize kernel
+// adapts it (f/ahiggs1.f:113-123, in the fields' precision) from the whole
+// lattice's acceptance
+void slab_meas(const std::vector<double>& tot, const FinalizeArgs& f, double V, lce_meas* m, double* delta) {
   double h[kNQ] = {0, 0, 0, 0}, l[kNQ] = {0, 0, 0, 0};
   for (int i = 0; i < f.nslots; ++i) {
     const double* t = tot.data() + (size_t)i * kNQ;
@@ -946,11 +950,27 @@ void slab_meas(const std::vector<double>& tot, const FinalizeArgs& f, double V, 
     double* acc = kind <= kHiggsMetro ? h : l;
     for (int q = 0; q < kNQ; ++q) acc[q] += t[q];
     if (!end) continue;
-    if (kind == kHiggsHB || kind == kHiggsOR) {
+    if (kind == kHiggsHB || kind == kHiggsOR || kind == kHiggsMetro) {
       m->a2 = h[1] / V;
       m->a4 = h[2] / V;
       m->akin = h[3] / (6.0 * V);
-      (kind == kHiggsHB ? m->acc_hb : m->acc_or) = h[0] / V;
+      if (kind == kHiggsHB) m->acc_hb = h[0] / V;
+      if (kind == kHiggsOR) m->acc_or = h[0] / V;
+      if (kind == kHiggsMetro) {
+        if (f.single) {
+          const float a = (float)h[0] / (float)V;
+          float d = (float)*delta;
+          if (fabsf(a - 0.5f) > 0.1f) d = (a > 0.5f) ? 1.1131241f * d : 0.8989669f * d;
+          m->acc_metro = a;
+          *delta = d;
+        } else {
+          const double a = h[0] / V;
+          double d = *delta;
+          if (fabs(a - 0.5) > 0.1) d = (a > 0.5) ? 1.1131241 * d : 0.8989669 * d;
+          m->acc_metro = a;
+          *delta = d;
+        }
+      }
     } else if (kind == kLinkHB) {
       m->plaq = l[2] / (12.0 * V);
       m->acc_gauge = (l[0] / (3.0 * V)) * (l[1] / (12.0 * V));
@@ -990,16 +1010,25 @@ int slab_sweep(lce_slabs* S, int measflag, lce_meas* m) {
     lce_ctx* c = S->slab[k];
     DeviceScope ds_(c->device);
     if (int rc = status_check(c)) return slab_rc(c, rc);  // synchronises the slab's stream
-    if (measflag == 1 && !t.empty()) {
+    if (!t.empty()) {  // measured slots, and the Metropolis slots of every sweep
       SCK(cudaMemcpy(t.data(), c->totals_d, t.size() * sizeof(double), cudaMemcpyDeviceToHost));
       for (size_t e = 0; e < t.size(); ++e) tot[e] += t[e];
     }
   }
-  if (m) {
-    std::memset(m, 0, sizeof(*m));
-    m->delta = S->slab[0]->params[0].delta0;
-    if (measflag == 1) slab_meas(tot, q[0].f, (double)S->L[0] * S->L[1] * S->L[2], m);
+  lce_meas mm;
+  std::memset(&mm, 0, sizeof(mm));
+  slab_meas(tot, q[0].f, (double)S->L[0] * S->L[1] * S->L[2], &mm, &S->delta);
+  mm.delta = S->delta;
+  if (S->slab[0]->n_higgs_metro > 0) {
+    // every slab's finalize adapted the step to its own acceptance: give them
+    // the whole lattice's
+    for (int k = 0; k < n; ++k) {
+      lce_ctx* c = S->slab[k];
+      DeviceScope ds_(c->device);
+      SCK(cudaMemcpy(&c->cst_d[0].delta, &S->delta, sizeof(double), cudaMemcpyHostToDevice));
+    }
   }
+  if (m) *m = mm;
   return LCE_OK;
 }
 
@@ -1871,10 +1900,8 @@ lce_slabs* lce_slabs_create(const lce_params* p, int nslabs, const int* devices)
     slabs_fail(LCE_ERR_INVALID, "slabs_create: L3 must split into slabs of an even number (>= 2) of planes");
     return nullptr;
   }
-  if (p->rng != LCE_RNG_PHILOX || p->n_higgs_metro != 0) {
-    slabs_fail(LCE_ERR_UNSUPPORTED,
-               "slabs_create: Philox uniforms only, and no Higgs Metropolis step (its step size adapts to the "
-               "whole lattice's acceptance)");
+  if (p->rng != LCE_RNG_PHILOX) {
+    slabs_fail(LCE_ERR_UNSUPPORTED, "slabs_create: Philox uniforms only");
     return nullptr;
   }
   lce_slabs* S = new lce_slabs();
@@ -1884,6 +1911,7 @@ lce_slabs* lce_slabs_create(const lce_params* p, int nslabs, const int* devices)
   S->nz = nz;
   S->nxy = p->L[0] * p->L[1] / 2;
   S->prec = p->precision;
+  S->delta = p->delta0;
   for (int k = 0; k < nslabs; ++k) {
     lce_params q = *p;
     q.L[2] = nz + 2;

@@ -22,7 +22,8 @@ KEYS = ("plaq", "akin", "a2", "a4", "acc_gauge", "acc_hb", "acc_or")
 def test_slabs_reproduce_the_whole_lattice(precision, L, nslabs):
     dt = np.float64 if precision == "f64" else np.float32
     u, a = hot_config(L, seed=31, dtype=dt)
-    kw = dict(beta=12.0, x=0.09, y=0.3, precision=precision, seed=4242, n_link_or=1)
+    kw = dict(beta=12.0, x=0.09, y=0.3, precision=precision, seed=4242, n_link_or=1, n_higgs_metro=1,
+              delta0=0.75)
     g = Lattice(L, sweep_mode="passes", **kw)
     g.upload(u, a)
     s = SlabLattice(L, nslabs, **kw)
@@ -33,12 +34,32 @@ def test_slabs_reproduce_the_whole_lattice(precision, L, nslabs):
         us, as_ = s.download(dtype=dt)
         np.testing.assert_array_equal(us, ug)
         np.testing.assert_array_equal(as_, ag)
-        for key in KEYS + ("acc_link_or",):
+        for key in KEYS + ("acc_link_or", "acc_metro", "delta"):
             assert abs(ms[key] - mg[key]) <= 1e-12 * max(1.0, abs(mg[key])), (k, key)
     s.sweep(0)
     g.sweep(0)
     np.testing.assert_array_equal(s.download(dtype=dt)[0], g.download(dtype=dt)[0])
     s.close()
+
+
+def test_slabs_metropolis_step_adapts_to_the_whole_lattice():
+    """The ahiggs1 step follows the whole lattice's acceptance (f/ahiggs1.f:
+    113-123): a step far from 50% acceptance is rescaled identically on every
+    slab and in the undecomposed run, over several sweeps."""
+    L = (8, 4, 8)
+    u, a = hot_config(L, seed=9)
+    kw = dict(beta=9.0, x=0.1, y=0.45, precision="f64", seed=11, n_higgs_metro=2, delta0=5.0)
+    g = Lattice(L, sweep_mode="passes", **kw)
+    g.upload(u, a)
+    s = SlabLattice(L, 4, **kw)
+    s.upload(u, a)
+    deltas = []
+    for k in range(4):
+        mg, ms = g.sweep(k % 2), s.sweep(k % 2)
+        assert ms["delta"] == mg["delta"], k
+        deltas.append(ms["delta"])
+    assert deltas[-1] < 5.0  # a step of 5 is accepted rarely: it shrinks
+    np.testing.assert_array_equal(s.download()[1], g.download()[1])
 
 
 def test_slabs_three_hit_link_update():
@@ -61,5 +82,3 @@ def test_slabs_reject_what_they_cannot_do():
             SlabLattice(L, n, precision="f64")
     with pytest.raises(LceError):
         SlabLattice((4, 4, 8), 2, rng="stream")
-    with pytest.raises(LceError):
-        SlabLattice((4, 4, 8), 2, n_higgs_metro=1)
