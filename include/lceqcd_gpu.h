@@ -330,8 +330,8 @@ int lce_timer_stop(lce_ctx* ctx, float* ms);
  * those of an undecomposed context with the same seed; measurements are the
  * whole lattice's (sums over slabs, in another order), and the ahiggs1 step
  * adapts to the whole lattice's acceptance.  Philox only, the sweep
- * composition of lce_sweep; no gauge fixing or correlators on a decomposed
- * lattice. */
+ * composition of lce_sweep.  Gauge fixing (the overrelaxed method of
+ * lce_landau_gauge) and the z-slice measurements also run on the slabs. */
 typedef struct lce_slabs lce_slabs;
 lce_slabs* lce_slabs_create(const lce_params* p, int nslabs, const int* devices);  /* NULL: lce_last_error(NULL) */
 void lce_slabs_destroy(lce_slabs* s);
@@ -343,6 +343,20 @@ int lce_slabs_download_f64(lce_slabs* s, double* u, double* a, long ld);
 /* one sweep of f/main.f:38-41 over all slabs; m (may be NULL) receives the
  * whole lattice's measurements when measflag = 1 */
 int lce_slabs_sweep(lce_slabs* s, int measflag, lce_meas* m);
+/* u_f, a_f (LCE_FIELDS_FIXED of lce_download) of the whole lattice */
+int lce_slabs_download_fixed(lce_slabs* s, float* u, float* a, long ld);
+int lce_slabs_download_fixed_f64(lce_slabs* s, double* u, double* a, long ld);
+/* lce_landau_gauge (f/landau_gauge.f:308-324, f/or_gauge_fixing1.f) on the
+ * slabs: a half-step's update of the U_z links below a slab's first plane
+ * goes back to the slab below, theta is the whole lattice's; same iterations
+ * and (up to the order of the theta sum) the same u_f, a_f as undecomposed */
+int lce_slabs_landau_gauge(lce_slabs* s, double* theta, int* iters, int max_iters);
+/* lce_correlator / lce_polyakov / lce_scalarcorr of the whole lattice
+ * (f/correlator.f, f/polyakov.f, f/scalarcorr.f): slice sums per slab,
+ * correlated on the first slab's device */
+int lce_slabs_correlator(lce_slabs* s, double* corr_a, double* corr_u, double* corr_3, double af[3]);
+int lce_slabs_polyakov(lce_slabs* s, double* slice, double* corr, double* mean2);
+int lce_slabs_scalarcorr(lce_slabs* s, double* slice, double* corr, double* mean);
 
 /* ---- allocation-free measurement ----
  * No counterpart in the reference.  For callers that cannot let this library

@@ -122,6 +122,12 @@ SIGNATURES = {
     "lce_slabs_download": (I, [P, P, P, C.c_long]),
     "lce_slabs_download_f64": (I, [P, P, P, C.c_long]),
     "lce_slabs_sweep": (I, [P, I, P]),
+    "lce_slabs_download_fixed": (I, [P, P, P, C.c_long]),
+    "lce_slabs_download_fixed_f64": (I, [P, P, P, C.c_long]),
+    "lce_slabs_landau_gauge": (I, [P, P, P, I]),
+    "lce_slabs_correlator": (I, [P, P, P, P, P]),
+    "lce_slabs_polyakov": (I, [P, P, P, P]),
+    "lce_slabs_scalarcorr": (I, [P, P, P, P]),
     "lce_it_landau_gauge": (I, [P, I, D, I, P, P, I]),
     "lce_landau_gauge_from": (I, [P, I, I, P, P, P, I]),
     "lce_apply_transform": (I, [P, I]),

@@ -11,6 +11,7 @@
 #include <algorithm>
 #include <type_traits>
 #include <cmath>
+#include <cstddef>
 #include <cstdio>
 #include <cstring>
 #include <map>
@@ -867,10 +868,13 @@ int fa_loop(lce_ctx* c, int chain, double step, double limit, double* theta, int
 // After every pass the written field's parity is exchanged: slab k copies
 // the last interior plane of slab k-1 into its plane 0 and the first
 // interior plane of slab k+1 into its plane nz+1 (periodic), on its own
-// stream, ordered by events (peer copies between devices).
+// stream, ordered by events (peer copies between devices).  Gauge fixing and
+// the correlators gather per-slab sums on slab 0's device (g_d).
 struct lce_slabs {
   std::vector<lce_ctx*> slab;
-  std::vector<cudaEvent_t> ev_pass, ev_copy;
+  std::vector<cudaEvent_t> ev_pass, ev_copy, ev_sum;
+  cudaEvent_t ev_chk = nullptr;
+  double* g_d = nullptr;  // slab 0's device: theta sums [n], slice sums [14 L3], correlators [7 L3 + 5]
   int L[3] = {0, 0, 0};
   int nz = 0, nxy = 0, prec = LCE_PREC_F32;
   double delta = 0.0;  // ahiggs1 step of the whole lattice (every slab holds a copy)
@@ -895,35 +899,47 @@ int slab_rc(lce_ctx* c, int rc) {
 }
 
 // device address of local plane z of a slab's field at local parity p: the
-// links U_mu (f = mu) or component k of the Higgs field (f = -1)
-char* slab_plane(lce_ctx* c, int f, int p, int z, int k) {
+// links U_mu (f = mu) or component k of the Higgs field (f = -1); fixed:
+// the gauge-fixed copies U_f, A_f
+char* slab_plane(lce_ctx* c, int f, int p, int z, int k, bool fixed = false) {
   const ChainDev& d = c->ch[0];
-  if (f >= 0) return (char*)d.u + (((size_t)(f * 2 + p)) * d.nh + (size_t)z * d.nxy) * link_bytes(c->prec);
-  return (char*)d.a + (((size_t)(p * 3 + k)) * d.nh + (size_t)z * d.nxy) * real_bytes(c->prec);
+  if (f >= 0)
+    return (char*)(fixed ? d.uf : d.u) + (((size_t)(f * 2 + p)) * d.nh + (size_t)z * d.nxy) * link_bytes(c->prec);
+  return (char*)(fixed ? d.af : d.a) + (((size_t)(p * 3 + k)) * d.nh + (size_t)z * d.nxy) * real_bytes(c->prec);
 }
 
-// halo planes of field f at whole-lattice parity pg, once every slab's
-// stream has recorded ev_pass; then each stream waits for its neighbours'
-// copies before a later pass may overwrite the planes they read
-int slab_exchange(lce_slabs* S, int f, int pg) {
-  const int n = (int)S->slab.size(), nz = S->nz;
+// one plane of an exchange: slab k's local plane zd of field f (a link
+// direction, or -1 for the Higgs field) at whole-lattice parity pg, from
+// plane zs of its neighbour k + dk (dk = -1 or +1, periodic)
+struct PlaneCopy {
+  int dk, zs, zd, f, pg;
+  bool fixed;
+};
+
+int slab_copy_plane(lce_ctx* c, lce_ctx* cj, const PlaneCopy& q, size_t nxy) {
+  const int ps = q.pg ^ cj->eo_flip, pd = q.pg ^ c->eo_flip;
+  const size_t bytes = nxy * (q.f >= 0 ? link_bytes(c->prec) : real_bytes(c->prec));
+  for (int comp = 0; comp < (q.f >= 0 ? 1 : 3); ++comp) {
+    void* dst = slab_plane(c, q.f, pd, q.zd, comp, q.fixed);
+    const void* src = slab_plane(cj, q.f, ps, q.zs, comp, q.fixed);
+    if (c->device == cj->device) SCK(cudaMemcpyAsync(dst, src, bytes, cudaMemcpyDeviceToDevice, c->stream));
+    else SCK(cudaMemcpyPeerAsync(dst, c->device, src, cj->device, bytes, c->stream));
+  }
+  return LCE_OK;
+}
+
+// the planes cp[0..ncp) of every slab, once its neighbours' streams have
+// recorded ev_pass; then each stream waits for its neighbours' copies before
+// a later pass may overwrite the planes they read
+int slab_exchange(lce_slabs* S, const PlaneCopy* cp, int ncp) {
+  const int n = (int)S->slab.size();
   for (int k = 0; k < n; ++k) {
     lce_ctx* c = S->slab[k];
     DeviceScope ds_(c->device);
-    for (int side = 0; side < 2; ++side) {
-      const int j = side == 0 ? (k + n - 1) % n : (k + 1) % n;
-      lce_ctx* cj = S->slab[j];
-      const int zs = side == 0 ? nz : 1, zd = side == 0 ? 0 : nz + 1;
-      const int ps = pg ^ cj->eo_flip, pd = pg ^ c->eo_flip;
-      const size_t bytes = (size_t)S->nxy * (f >= 0 ? link_bytes(c->prec) : real_bytes(c->prec));
-      SCK(cudaStreamWaitEvent(c->stream, S->ev_pass[j], 0));
-      for (int comp = 0; comp < (f >= 0 ? 1 : 3); ++comp) {
-        void* dst = slab_plane(c, f, pd, zd, comp);
-        const void* src = slab_plane(cj, f, ps, zs, comp);
-        if (c->device == cj->device) SCK(cudaMemcpyAsync(dst, src, bytes, cudaMemcpyDeviceToDevice, c->stream));
-        else SCK(cudaMemcpyPeerAsync(dst, c->device, src, cj->device, bytes, c->stream));
-      }
-    }
+    SCK(cudaStreamWaitEvent(c->stream, S->ev_pass[(k + n - 1) % n], 0));
+    SCK(cudaStreamWaitEvent(c->stream, S->ev_pass[(k + 1) % n], 0));
+    for (int i = 0; i < ncp; ++i)
+      if (int rc = slab_copy_plane(c, S->slab[(k + n + cp[i].dk) % n], cp[i], S->nxy)) return rc;
     SCK(cudaEventRecord(S->ev_copy[k], c->stream));
   }
   for (int k = 0; k < n; ++k) {
@@ -997,7 +1013,9 @@ int slab_sweep(lce_slabs* S, int measflag, lce_meas* m) {
       SCK(cudaEventRecord(S->ev_pass[k], c->stream));
     }
     const Pass& ps = q[0].passes[i];
-    if (int rc = slab_exchange(S, ps.kind <= kHiggsMetro ? -1 : ps.mu, ps.eo)) return rc;
+    const int f = ps.kind <= kHiggsMetro ? -1 : ps.mu, nz = S->nz;
+    const PlaneCopy cp[2] = {{-1, nz, 0, f, ps.eo, false}, {+1, 1, nz + 1, f, ps.eo, false}};
+    if (int rc = slab_exchange(S, cp, 2)) return rc;
   }
   for (int k = 0; k < n; ++k) {
     lce_ctx* c = S->slab[k];
@@ -1032,10 +1050,154 @@ int slab_sweep(lce_slabs* S, int measflag, lce_meas* m) {
   return LCE_OK;
 }
 
+// the overrelaxed Landau gauge fixing of f/landau_gauge.f:308-324 and
+// f/or_gauge_fixing1.f on the slabs.  A half-step updates the U_z link below
+// each site of a slab's first interior plane, which lives in the lower halo
+// and belongs to slab k-1: after it that link goes back to slab k-1 (its
+// plane nz), and slab k-1's plane nz of the updated parity comes forward into
+// slab k's halo (the next half-step's U_f(x - z, z)).  Nothing else crosses
+// a slab boundary.  Theta (the whole lattice's odd sites, before their
+// update) is summed per slab, combined on slab 0's device, and the count and
+// verdict copied to every slab's chain state, all ordered by events: no host
+// round trip inside a batch of iterations.
+template <typename R>
+int slab_gf_iterations(lce_slabs* S, int batch) {
+  const int n = (int)S->slab.size(), nz = S->nz;
+  lce_ctx* c0 = S->slab[0];
+  const size_t off = offsetof(ChainState, gf_theta), len = offsetof(ChainState, gf_pad) - off;
+  const double nh_all = (double)S->nxy * S->L[2];
+  for (int it = 0; it < batch; ++it) {
+    for (int pg = 0; pg < 2; ++pg) {
+      for (int k = 0; k < n; ++k) {
+        lce_ctx* c = S->slab[k];
+        DeviceScope ds_(c->device);
+        launch_gf_half<R>(c->ch_d, c->cst_d, pg ^ c->eo_flip, pg, c->scratch_d, c->ch[0].nh, c->s_lo, c->stream);
+        SCK(cudaGetLastError());
+        SCK(cudaEventRecord(S->ev_pass[k], c->stream));
+      }
+      const PlaneCopy cp[2] = {{+1, 0, nz, 2, pg ^ 1, true}, {-1, nz, 0, 2, pg, true}};
+      if (int rc = slab_exchange(S, cp, 2)) return rc;
+    }
+    for (int k = 0; k < n; ++k) {
+      lce_ctx* c = S->slab[k];
+      DeviceScope ds_(c->device);
+      const int nb = ceil_div(c->ch[0].nh - 2 * c->s_lo, kBlock);
+      launch_sum_partials(c->scratch_d, nb, 1, c->scratch_d + nb, c->stream);
+      SCK(cudaGetLastError());
+      if (c->device == c0->device)
+        SCK(cudaMemcpyAsync(S->g_d + k, c->scratch_d + nb, sizeof(double), cudaMemcpyDeviceToDevice, c->stream));
+      else
+        SCK(cudaMemcpyPeerAsync(S->g_d + k, c0->device, c->scratch_d + nb, c->device, sizeof(double), c->stream));
+      SCK(cudaEventRecord(S->ev_sum[k], c->stream));
+    }
+    {
+      DeviceScope ds_(c0->device);
+      for (int k = 1; k < n; ++k) SCK(cudaStreamWaitEvent(c0->stream, S->ev_sum[k], 0));
+      launch_gf_check_slabs(c0->ch_d, c0->cst_d, S->g_d, n, nh_all, c0->stream);
+      SCK(cudaGetLastError());
+      SCK(cudaEventRecord(S->ev_chk, c0->stream));
+    }
+    for (int k = 1; k < n; ++k) {
+      lce_ctx* c = S->slab[k];
+      DeviceScope ds_(c->device);
+      SCK(cudaStreamWaitEvent(c->stream, S->ev_chk, 0));
+      char* dst = (char*)c->cst_d + off;
+      const char* src = (const char*)c0->cst_d + off;
+      if (c->device == c0->device) SCK(cudaMemcpyAsync(dst, src, len, cudaMemcpyDeviceToDevice, c->stream));
+      else SCK(cudaMemcpyPeerAsync(dst, c->device, src, c0->device, len, c->stream));
+    }
+  }
+  return LCE_OK;
+}
+
+int slab_landau_gauge(lce_slabs* S, double* theta, int* iters, int max_iters) {
+  const int n = (int)S->slab.size();
+  lce_ctx* c0 = S->slab[0];
+  const int cap = max_iters > 0 ? max_iters : 1000000;
+  for (int k = 0; k < n; ++k) {
+    lce_ctx* c = S->slab[k];
+    DeviceScope ds_(c->device);
+    const ChainDev& ch = c->ch[0];
+    const size_t ub = (size_t)6 * ch.nh * link_bytes(c->prec), ab = (size_t)6 * ch.nh * real_bytes(c->prec);
+    SCK(cudaMemcpyAsync(ch.uf, ch.u, ub, cudaMemcpyDeviceToDevice, c->stream));
+    SCK(cudaMemcpyAsync(ch.af, ch.a, ab, cudaMemcpyDeviceToDevice, c->stream));
+    ChainState cs;
+    SCK(cudaMemcpyAsync(&cs, c->cst_d, sizeof(cs), cudaMemcpyDeviceToHost, c->stream));
+    SCK(cudaStreamSynchronize(c->stream));
+    cs.gf_done = 0;
+    cs.gf_iters = 0;
+    cs.gf_cap = cap;
+    cs.gf_theta = 1.0e4;
+    SCK(cudaMemcpyAsync(c->cst_d, &cs, sizeof(cs), cudaMemcpyHostToDevice, c->stream));
+    SCK(cudaStreamSynchronize(c->stream));
+  }
+  ChainState cs;
+  std::memset(&cs, 0, sizeof(cs));
+  int batch = 8;
+  while (true) {
+    const int rc = S->prec == LCE_PREC_F64 ? slab_gf_iterations<double>(S, batch) : slab_gf_iterations<float>(S, batch);
+    if (rc) return rc;
+    const int before = cs.gf_iters;
+    {
+      DeviceScope ds_(c0->device);
+      SCK(cudaMemcpyAsync(&cs, c0->cst_d, sizeof(cs), cudaMemcpyDeviceToHost, c0->stream));
+      SCK(cudaStreamSynchronize(c0->stream));
+    }
+    if (cs.gf_done) break;
+    if (cs.gf_iters <= before) return slabs_fail(LCE_ERR_CUDA, "slabs gauge fixing: a batch made no progress");
+    if (batch < 64) batch *= 2;
+  }
+  for (int k = 0; k < n; ++k) {
+    lce_ctx* c = S->slab[k];
+    DeviceScope ds_(c->device);
+    SCK(cudaStreamSynchronize(c->stream));
+  }
+  if (theta) *theta = cs.gf_theta;
+  if (iters) *iters = cs.gf_iters;
+  if (!std::isfinite(cs.gf_theta)) return slabs_fail(LCE_ERR_NAN, "slabs gauge fixing: theta is not finite");
+  if (cs.gf_theta > c0->ch[0].limit_or)
+    return slabs_fail(LCE_ERR_GF_NOT_CONVERGED, "slabs gauge fixing: iteration cap reached");
+  return LCE_OK;
+}
+
+// the z-slice sums of every slab's interior planes (the slice_sums kernel on
+// each slab's own device), gathered into the whole lattice's slices on slab
+// 0's device, and the correlators of lce_correlator formed there; h
+// receives the 7 L3 + 5 values of the correlator kernel's output
+int slab_slices(lce_slabs* S, std::vector<double>& h) {
+  const int n = (int)S->slab.size(), nz = S->nz, L3 = S->L[2];
+  lce_ctx* c0 = S->slab[0];
+  double* slices = S->g_d + n;
+  double* out = slices + (size_t)14 * L3;
+  for (int k = 0; k < n; ++k) {
+    lce_ctx* c = S->slab[k];
+    DeviceScope ds_(c->device);
+    if (S->prec == LCE_PREC_F64) launch_slice_sums<double>(c->ch_d, nz + 2, c->scratch_d, c->stream);
+    else launch_slice_sums<float>(c->ch_d, nz + 2, c->scratch_d, c->stream);
+    SCK(cudaGetLastError());
+    const size_t bytes = (size_t)14 * nz * sizeof(double);
+    double* dst = slices + (size_t)14 * k * nz;
+    if (c->device == c0->device)
+      SCK(cudaMemcpyAsync(dst, c->scratch_d + 14, bytes, cudaMemcpyDeviceToDevice, c->stream));
+    else
+      SCK(cudaMemcpyPeerAsync(dst, c0->device, c->scratch_d + 14, c->device, bytes, c->stream));
+    SCK(cudaEventRecord(S->ev_sum[k], c->stream));
+  }
+  DeviceScope ds_(c0->device);
+  for (int k = 1; k < n; ++k) SCK(cudaStreamWaitEvent(c0->stream, S->ev_sum[k], 0));
+  launch_correlators(slices, S->L[0], S->L[1], L3, out, c0->stream);
+  SCK(cudaGetLastError());
+  h.assign((size_t)7 * L3 + 5, 0.0);
+  SCK(cudaMemcpyAsync(h.data(), out, h.size() * sizeof(double), cudaMemcpyDeviceToHost, c0->stream));
+  SCK(cudaStreamSynchronize(c0->stream));
+  return LCE_OK;
+}
+
 // whole-lattice arrays (reference order: u[mu][eo][site < ld][4],
-// a[eo][site < ld][3]) <-> each slab's planes, halos included on the way in
+// a[eo][site < ld][3]) <-> each slab's planes, halos included on the way in;
+// which: the fields or (downloads only) the gauge-fixed copies
 template <typename T>
-int slabs_copy(lce_slabs* S, T* u, T* a, long ld, bool in) {
+int slabs_copy(lce_slabs* S, T* u, T* a, long ld, bool in, int which = LCE_FIELDS) {
   const int n = (int)S->slab.size(), nz = S->nz, nxy = S->nxy, L3 = S->L[2];
   const long nhl = (long)(nz + 2) * nxy;
   std::vector<T> ul((size_t)6 * nhl * 4), al((size_t)2 * nhl * 3);
@@ -1044,8 +1206,8 @@ int slabs_copy(lce_slabs* S, T* u, T* a, long ld, bool in) {
     const int z0 = k * nz;
     if (!in) {
       int rc = std::is_same<T, double>::value
-                   ? lce_download_f64(c, 0, LCE_FIELDS, (double*)ul.data(), (double*)al.data(), nhl)
-                   : lce_download(c, 0, LCE_FIELDS, (float*)ul.data(), (float*)al.data(), nhl);
+                   ? lce_download_f64(c, 0, which, (double*)ul.data(), (double*)al.data(), nhl)
+                   : lce_download(c, 0, which, (float*)ul.data(), (float*)al.data(), nhl);
       if (rc) return slab_rc(c, rc);
     }
     for (int zl = in ? 0 : 1; zl <= (in ? nz + 1 : nz); ++zl) {
@@ -1904,6 +2066,10 @@ lce_slabs* lce_slabs_create(const lce_params* p, int nslabs, const int* devices)
     slabs_fail(LCE_ERR_UNSUPPORTED, "slabs_create: Philox uniforms only");
     return nullptr;
   }
+  if ((size_t)L3 * 14 * sizeof(double) > 200 * 1024) {
+    slabs_fail(LCE_ERR_INVALID, "slabs_create: L3 too large for the correlator kernel");
+    return nullptr;
+  }
   lce_slabs* S = new lce_slabs();
   S->L[0] = p->L[0];
   S->L[1] = p->L[1];
@@ -1940,6 +2106,28 @@ lce_slabs* lce_slabs_create(const lce_params* p, int nslabs, const int* devices)
     }
     S->ev_pass.push_back(e1);
     S->ev_copy.push_back(e2);
+    cudaEvent_t e3 = nullptr;
+    if (cudaEventCreateWithFlags(&e3, cudaEventDisableTiming) != cudaSuccess) {
+      lce_slabs_destroy(S);
+      g_create_error = "slabs_create: cudaEventCreate";
+      slabs_fail(LCE_ERR_CUDA, g_create_error);
+      return nullptr;
+    }
+    S->ev_sum.push_back(e3);
+  }
+  {
+    // theta sums, slice sums and correlators of the whole lattice on slab 0's device
+    DeviceScope ds_(devices[0]);
+    const size_t gn = (size_t)nslabs + (size_t)21 * L3 + 5;
+    if (cudaEventCreateWithFlags(&S->ev_chk, cudaEventDisableTiming) != cudaSuccess ||
+        cudaMalloc(&S->g_d, gn * sizeof(double)) != cudaSuccess) {
+      cudaGetLastError();
+      S->g_d = nullptr;
+      lce_slabs_destroy(S);
+      g_create_error = "slabs_create: slab 0 gather buffer";
+      slabs_fail(LCE_ERR_NOMEM, g_create_error);
+      return nullptr;
+    }
   }
   // direct peer copies between the devices that hold neighbouring slabs
   for (int k = 0; k < nslabs; ++k) {
@@ -1963,10 +2151,16 @@ lce_slabs* lce_slabs_create(const lce_params* p, int nslabs, const int* devices)
 void lce_slabs_destroy(lce_slabs* h) {
   lce_slabs* S = h;
   if (!S) return;
+  if (!S->slab.empty()) {
+    DeviceScope ds_(S->slab[0]->device);
+    if (S->g_d) cudaFree(S->g_d);
+    if (S->ev_chk) cudaEventDestroy(S->ev_chk);
+  }
   for (size_t k = 0; k < S->slab.size(); ++k) {
     DeviceScope ds_(S->slab[k]->device);
     if (k < S->ev_pass.size()) cudaEventDestroy(S->ev_pass[k]);
     if (k < S->ev_copy.size()) cudaEventDestroy(S->ev_copy[k]);
+    if (k < S->ev_sum.size()) cudaEventDestroy(S->ev_sum[k]);
     lce_destroy(S->slab[k]);
   }
   delete S;
@@ -2000,6 +2194,61 @@ int lce_slabs_sweep(lce_slabs* h, int measflag, lce_meas* m) {
   lce_slabs* S = h;
   if (!S || (measflag != 0 && measflag != 1)) return LCE_ERR_INVALID;
   return slab_sweep(S, measflag, m);
+}
+
+int lce_slabs_download_fixed(lce_slabs* h, float* u, float* a, long ld) {
+  lce_slabs* S = h;
+  if (!S || !u || !a || ld < (long)S->nxy * S->L[2]) return LCE_ERR_INVALID;
+  return slabs_copy<float>(S, u, a, ld, false, LCE_FIELDS_FIXED);
+}
+
+int lce_slabs_download_fixed_f64(lce_slabs* h, double* u, double* a, long ld) {
+  lce_slabs* S = h;
+  if (!S || !u || !a || ld < (long)S->nxy * S->L[2]) return LCE_ERR_INVALID;
+  return slabs_copy<double>(S, u, a, ld, false, LCE_FIELDS_FIXED);
+}
+
+int lce_slabs_landau_gauge(lce_slabs* h, double* theta, int* iters, int max_iters) {
+  lce_slabs* S = h;
+  if (!S) return LCE_ERR_INVALID;
+  return slab_landau_gauge(S, theta, iters, max_iters);
+}
+
+int lce_slabs_correlator(lce_slabs* h, double* corr_a, double* corr_u, double* corr_3, double af[3]) {
+  lce_slabs* S = h;
+  if (!S) return LCE_ERR_INVALID;
+  std::vector<double> v;
+  if (int rc = slab_slices(S, v)) return rc;
+  const int L3 = S->L[2];
+  if (corr_a) std::memcpy(corr_a, v.data(), L3 * sizeof(double));
+  if (corr_u) std::memcpy(corr_u, v.data() + L3, L3 * sizeof(double));
+  if (corr_3) std::memcpy(corr_3, v.data() + 2 * L3, L3 * sizeof(double));
+  if (af) std::memcpy(af, v.data() + 7 * L3, 3 * sizeof(double));
+  return LCE_OK;
+}
+
+int lce_slabs_polyakov(lce_slabs* h, double* slice, double* corr, double* mean2) {
+  lce_slabs* S = h;
+  if (!S) return LCE_ERR_INVALID;
+  std::vector<double> v;
+  if (int rc = slab_slices(S, v)) return rc;
+  const int L3 = S->L[2];
+  if (slice) std::memcpy(slice, v.data() + 3 * L3, L3 * sizeof(double));
+  if (corr) std::memcpy(corr, v.data() + 4 * L3, L3 * sizeof(double));
+  if (mean2) *mean2 = v[7 * L3 + 3];
+  return LCE_OK;
+}
+
+int lce_slabs_scalarcorr(lce_slabs* h, double* slice, double* corr, double* mean) {
+  lce_slabs* S = h;
+  if (!S) return LCE_ERR_INVALID;
+  std::vector<double> v;
+  if (int rc = slab_slices(S, v)) return rc;
+  const int L3 = S->L[2];
+  if (slice) std::memcpy(slice, v.data() + 5 * L3, L3 * sizeof(double));
+  if (corr) std::memcpy(corr, v.data() + 6 * L3, L3 * sizeof(double));
+  if (mean) *mean = v[7 * L3 + 4];
+  return LCE_OK;
 }
 
 }  // extern "C"

@@ -63,20 +63,24 @@ __device__ __forceinline__ void gf_sums(const ChainDev& ch, const su2<R> (&um)[3
 // track != 0: also accumulate the gauge transform, G(x) -> Omega(x) G(x), so
 // that U_f(x,mu) = G(x) U(x,mu) G(x+mu)^+ holds throughout.  FP32 is held to
 // 64 registers (4 blocks per SM; 68 allowed 3): 8.5% less time per
-// iteration at 128^3, the kernel being latency-bound.
+// iteration at 128^3, the kernel being latency-bound.  s_lo: a z-slab's
+// first visited site (its first and last planes are halos; sites
+// [s_lo, nh - s_lo) are visited), 0 for a whole lattice.  last: the
+// iteration's second half-step (the whole lattice's odd sites; a slab's
+// local parity eo may be flipped), which sums theta and reunitarises.
 template <typename R>
-__global__ void __launch_bounds__(kBlock, sizeof(R) == 4 ? 4 : 1) gf_half_kernel(const ChainDev* chp, const ChainState* cst, int eo,
-                                                         double* part, int track) {
+__global__ void __launch_bounds__(kBlock, sizeof(R) == 4 ? 4 : 1)
+    gf_half_kernel(const ChainDev* chp, const ChainState* cst, int eo, double* part, int track, int s_lo, int last) {
   pdl_trigger();
   const ChainDev& ch = *chp;
-  const int s = blockIdx.x * kBlock + threadIdx.x;
-  const int oe = 1 - eo, nh = ch.nh;
-  const Coord X = site_coord(eo, s < nh ? s : 0, ch.hx, ch.nxy, ch.dhx, ch.dnxy);
+  const int s = s_lo + blockIdx.x * kBlock + threadIdx.x;
+  const int oe = 1 - eo, nh = ch.nh, s_hi = nh - s_lo;
+  const Coord X = site_coord(eo, s < s_hi ? s : s_lo, ch.hx, ch.nxy, ch.dhx, ch.dnxy);
   const int xm[3] = {nbr_dn<0>(ch, X), nbr_dn<1>(ch, X), nbr_dn<2>(ch, X)};
   pdl_wait();
   if (cst->gf_done) return;
   double th[1] = {0.0};
-  if (s < nh) {
+  if (s < s_hi) {
     su2<R> um[3], ud[3];
 #pragma unroll
     for (int mu = 0; mu < 3; ++mu) {
@@ -87,7 +91,7 @@ __global__ void __launch_bounds__(kBlock, sizeof(R) == 4 ? 4 : 1) gf_half_kernel
     gf_sums<R>(ch, um, ud, t1, t2);
     // (:145-146) w = first row of sum [U + U^+(x-mu)]
     const cpx<double> w1 = t1.a + cj(t2.a), w2 = t1.b - t2.b;
-    if (eo == 1) {
+    if (last) {
       // (:153-158)
       const double d = t1.a.im - t2.a.im;
       th[0] = d * d + (w2.re * w2.re + w2.im * w2.im);
@@ -136,7 +140,7 @@ __global__ void __launch_bounds__(kBlock, sizeof(R) == 4 ? 4 : 1) gf_half_kernel
     for (int mu = 0; mu < 3; ++mu) {
       su2<R> a = nn(o, um[mu]);
       su2<R> b = nd(ud[mu], o);
-      if (eo == 1) {
+      if (last) {
         a = unitarise64(a);
         b = unitarise64(b);
       }
@@ -148,7 +152,7 @@ __global__ void __launch_bounds__(kBlock, sizeof(R) == 4 ? 4 : 1) gf_half_kernel
       LinkIO<R>::st(ch.g, gi, unitarise64(nn(o, LinkIO<R>::ld_cg(ch.g, gi))));
     }
   }
-  if (eo == 1) block_reduce_store<1>(th, part + blockIdx.x);
+  if (last) block_reduce_store<1>(th, part + blockIdx.x);
 }
 
 // One parity of f/it_gauge_fixing.f:52-210 (the reference's iterative gauge
@@ -284,6 +288,21 @@ __global__ void __launch_bounds__(1024) gf_check_kernel(const ChainDev* chp, Cha
   }
 }
 
+// the same test for a lattice split into z-slabs: the slabs' theta sums (in
+// slab order) over the whole lattice's nh odd sites, counted into slab 0's
+// chain state, which the host copies to the other slabs
+__global__ void gf_check_slabs_kernel(const ChainDev* chp, ChainState* cst, const double* sums, int nslabs,
+                                      double nh) {
+  if (cst->gf_done) return;
+  double tot = 0.0;
+  for (int j = 0; j < nslabs; ++j) tot += sums[j];
+  const double theta = tot / nh;
+  const int it = cst->gf_iters + 1;
+  cst->gf_iters = it;
+  cst->gf_theta = theta;
+  if (!(theta > chp->limit_or) || (cst->gf_cap > 0 && it >= cst->gf_cap)) cst->gf_done = 1;
+}
+
 // theta of the current U_f without updating (odd sites)
 template <typename R>
 __global__ void __launch_bounds__(kBlock) gf_theta_kernel(const ChainDev* chp, double* part) {
@@ -324,9 +343,22 @@ template <typename R>
 void launch_gf_iteration(const ChainDev* ch, ChainState* cst, int track, double* part, int nh, cudaStream_t s) {
   const int nb = ceil_div(nh, kBlock);
   // programmatic dependent launch: each kernel waits in griddepcontrol.wait
-  (void)launch_pdl(gf_half_kernel<R>, nb, kBlock, 0, s, ch, (const ChainState*)cst, 0, part, track);
-  (void)launch_pdl(gf_half_kernel<R>, nb, kBlock, 0, s, ch, (const ChainState*)cst, 1, part, track);
+  (void)launch_pdl(gf_half_kernel<R>, nb, kBlock, 0, s, ch, (const ChainState*)cst, 0, part, track, 0, 0);
+  (void)launch_pdl(gf_half_kernel<R>, nb, kBlock, 0, s, ch, (const ChainState*)cst, 1, part, track, 0, 1);
   (void)launch_pdl(gf_check_kernel, 1, 1024, 0, s, ch, cst, (const double*)part, nb);
+}
+
+template <typename R>
+int launch_gf_half(const ChainDev* ch, ChainState* cst, int eo, int last, double* part, int nh, int s_lo,
+                   cudaStream_t s) {
+  const int nb = ceil_div(nh - 2 * s_lo, kBlock);
+  (void)launch_pdl(gf_half_kernel<R>, nb, kBlock, 0, s, ch, (const ChainState*)cst, eo, part, 0, s_lo, last);
+  return nb;
+}
+
+void launch_gf_check_slabs(const ChainDev* ch, ChainState* cst, const double* sums, int nslabs, double nh,
+                           cudaStream_t s) {
+  gf_check_slabs_kernel<<<1, 1, 0, s>>>(ch, cst, sums, nslabs, nh);
 }
 
 template <typename R>
@@ -366,6 +398,8 @@ void launch_sum_partials(const double* part, int nblocks, int nq, double* out, c
 
 template void launch_gf_iteration<float>(const ChainDev*, ChainState*, int, double*, int, cudaStream_t);
 template void launch_gf_iteration<double>(const ChainDev*, ChainState*, int, double*, int, cudaStream_t);
+template int launch_gf_half<float>(const ChainDev*, ChainState*, int, int, double*, int, int, cudaStream_t);
+template int launch_gf_half<double>(const ChainDev*, ChainState*, int, int, double*, int, int, cudaStream_t);
 template void launch_it_iteration<float>(const ChainDev*, ChainState*, int, int, double*, int, cudaStream_t);
 template void launch_it_iteration<double>(const ChainDev*, ChainState*, int, int, double*, int, cudaStream_t);
 template void launch_gf_theta<float>(const ChainDev*, double*, int, cudaStream_t);

@@ -186,6 +186,16 @@ void launch_flush(void* buf, size_t bytes, cudaStream_t s);
 template <typename R>
 void launch_gf_iteration(const ChainDev* ch, ChainState* cst, int track, double* part, int nh,
                          cudaStream_t s);
+// one overrelaxed half-step over sites [s_lo, nh - s_lo) of local parity eo
+// (a z-slab: s_lo = one plane); last: the second half-step, which writes the
+// theta partials into part and reunitarises; returns the number of blocks
+// (partials)
+template <typename R>
+int launch_gf_half(const ChainDev* ch, ChainState* cst, int eo, int last, double* part, int nh, int s_lo,
+                   cudaStream_t s);
+// convergence test of a z-slab decomposed fixing from the slabs' theta sums
+void launch_gf_check_slabs(const ChainDev* ch, ChainState* cst, const double* sums, int nslabs, double nh,
+                           cudaStream_t s);
 // one iteration of f/it_gauge_fixing.f (flags LCE_ITGF_*, step from cst->gf_step),
 // then the convergence check of the overrelaxed form
 template <typename R>

@@ -508,11 +508,15 @@ class SlabLattice:
         fn = self.lib.lce_slabs_upload_f64 if f64 else self.lib.lce_slabs_upload
         self._ck(fn(self.h, _ptr(uu), _ptr(aa), self.nh))
 
-    def download(self, dtype=None):
+    def download(self, dtype=None, fixed: bool = False):
+        """u, a of the whole lattice (fixed: the gauge-fixed u_f, a_f)."""
         dt = dtype or self.dtype
         u = np.zeros((3, 2, self.nh, 4), dt)
         a = np.zeros((2, self.nh, 3), dt)
-        fn = self.lib.lce_slabs_download_f64 if dt == np.float64 else self.lib.lce_slabs_download
+        if fixed:
+            fn = self.lib.lce_slabs_download_fixed_f64 if dt == np.float64 else self.lib.lce_slabs_download_fixed
+        else:
+            fn = self.lib.lce_slabs_download_f64 if dt == np.float64 else self.lib.lce_slabs_download
         self._ck(fn(self.h, _ptr(u), _ptr(a), self.nh))
         return u, a
 
@@ -520,6 +524,31 @@ class SlabLattice:
         m = LceMeas()
         self._ck(self.lib.lce_slabs_sweep(self.h, measflag, C.byref(m)))
         return m.as_dict()
+
+    def landau_gauge(self, max_iters: int = 0):
+        """The overrelaxed Landau gauge fixing of Lattice.landau_gauge on the
+        slabs; returns (theta, iterations)."""
+        th, it = C.c_double(), C.c_int()
+        self._ck(self.lib.lce_slabs_landau_gauge(self.h, C.byref(th), C.byref(it), int(max_iters)))
+        return th.value, it.value
+
+    def correlator(self):
+        L3 = self.params.L[2]
+        ca, cu, c3, af = np.zeros(L3), np.zeros(L3), np.zeros(L3), np.zeros(3)
+        self._ck(self.lib.lce_slabs_correlator(self.h, _ptr(ca), _ptr(cu), _ptr(c3), _ptr(af)))
+        return ca, cu, c3, af
+
+    def polyakov(self):
+        L3 = self.params.L[2]
+        sl, co, m = np.zeros(L3), np.zeros(L3), C.c_double()
+        self._ck(self.lib.lce_slabs_polyakov(self.h, _ptr(sl), _ptr(co), C.byref(m)))
+        return sl, co, m.value
+
+    def scalarcorr(self):
+        L3 = self.params.L[2]
+        sl, co, m = np.zeros(L3), np.zeros(L3), C.c_double()
+        self._ck(self.lib.lce_slabs_scalarcorr(self.h, _ptr(sl), _ptr(co), C.byref(m)))
+        return sl, co, m.value
 
     def close(self):
         if getattr(self, "h", None):

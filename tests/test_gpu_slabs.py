@@ -82,3 +82,73 @@ def test_slabs_reject_what_they_cannot_do():
             SlabLattice(L, n, precision="f64")
     with pytest.raises(LceError):
         SlabLattice((4, 4, 8), 2, rng="stream")
+
+
+def _thermalised_pair(L, nslabs, precision, limit_or, sweeps=3, seed=17):
+    dt = np.float64 if precision == "f64" else np.float32
+    u, a = hot_config(L, seed=seed, dtype=dt)
+    kw = dict(beta=9.0, x=0.1, y=0.45, lam=1.7, limit_or=limit_or, precision=precision, seed=seed + 1)
+    g = Lattice(L, sweep_mode="passes", **kw)
+    g.upload(u, a)
+    s = SlabLattice(L, nslabs, **kw)
+    s.upload(u, a)
+    for _ in range(sweeps):
+        g.sweep(0)
+        s.sweep(0)
+    return g, s, dt
+
+
+@pytest.mark.parametrize("precision,limit_or", [("f64", 1e-10), ("f32", 1e-6)])
+@pytest.mark.parametrize("L,nslabs", [((8, 8, 8), 1), ((8, 8, 8), 2), ((8, 6, 12), 3), ((6, 8, 16), 4)])
+def test_slabs_landau_gauge_reproduces_the_whole_lattice(precision, limit_or, L, nslabs):
+    """f/landau_gauge.f's overrelaxed fixing on the slabs: the same
+    iteration count, theta to summation order, and u_f, a_f bit for bit
+    (every site's update is the undecomposed one; the U_z links a slab's
+    first plane updates in its halo go back to the slab below)."""
+    g, s, dt = _thermalised_pair(L, nslabs, precision, limit_or)
+    tg, ig = g.landau_gauge()
+    ts, is_ = s.landau_gauge()
+    assert is_ == ig and ig > 10
+    assert tg <= limit_or and abs(ts - tg) <= 1e-9 * tg
+    ug, ag = _fixed(g, dt)
+    us, as_ = s.download(dtype=dt, fixed=True)
+    np.testing.assert_array_equal(us, ug)
+    np.testing.assert_array_equal(as_, ag)
+    # the un-fixed fields are untouched
+    np.testing.assert_array_equal(s.download(dtype=dt)[0], g.download(dtype=dt)[0])
+    s.close()
+
+
+def _fixed(g, dt):
+    return g.download(which=1, dtype=dt)  # LCE_FIELDS_FIXED
+
+
+def test_slabs_landau_gauge_cap():
+    """An iteration cap stops both runs at the same iteration with the
+    reference's not-converged status and the same partly fixed u_f."""
+    g, s, dt = _thermalised_pair((8, 8, 8), 2, "f64", 1e-12)
+    with pytest.raises(LceError):
+        g.landau_gauge(max_iters=7)
+    with pytest.raises(LceError):
+        s.landau_gauge(max_iters=7)
+    np.testing.assert_array_equal(s.download(fixed=True)[0], _fixed(g, dt)[0])
+    s.close()
+
+
+@pytest.mark.parametrize("nslabs", [1, 2, 4])
+def test_slabs_correlators_match_the_whole_lattice(nslabs):
+    """f/correlator.f, f/polyakov.f and f/scalarcorr.f on the slabs: slice
+    sums per slab gathered on the first slab's device, correlated there; the
+    whole lattice's values to summation order."""
+    L = (8, 6, 16)
+    g, s, dt = _thermalised_pair(L, nslabs, "f64", 1e-10, seed=23)
+    g.landau_gauge()
+    s.landau_gauge()
+    for vg, vs in zip(g.correlator(), s.correlator()):
+        np.testing.assert_allclose(vs, vg, rtol=1e-12, atol=1e-13)
+    for fn in ("polyakov", "scalarcorr"):
+        rg, rs = getattr(g, fn)(), getattr(s, fn)()
+        np.testing.assert_allclose(rs[0], rg[0], rtol=1e-12, atol=1e-13)
+        np.testing.assert_allclose(rs[1], rg[1], rtol=1e-12, atol=1e-13)
+        assert abs(rs[2] - rg[2]) <= 1e-12 * max(1.0, abs(rg[2]))
+    s.close()
