@@ -247,6 +247,16 @@ int lce_landau_gauge_from(lce_ctx* ctx, int chain, int start, double* theta_star
  * LCE_ERR_UNSUPPORTED.  max_iters caps both phases together. */
 int lce_landau_gauge_fourier(lce_ctx* ctx, int chain, int start, double step, double theta_switch, double* theta,
                              int* iters_fourier, int* iters_plain, int max_iters);
+/* The same fixing by nonlinear conjugate gradients with the same Fourier
+ * preconditioner (after Hudspith, Comput. Phys. Commun. 187 (2015) 115):
+ * direction s = F^-1[F[Delta]/p^2] + beta s_prev, beta = max(0,
+ * Polak-Ribiere), and the step along s that maximises the second-order
+ * expansion of the gauge functional (computed exactly per link in FP64),
+ * bounded by a trust region on the rotation angle.
+ * No reference counterpart; arguments and stopping criterion as
+ * lce_landau_gauge_fourier (no step argument). */
+int lce_landau_gauge_fourier_cg(lce_ctx* ctx, int chain, int start, double theta_switch, double* theta,
+                                int* iters_fourier, int* iters_plain, int max_iters);
 /* The reference's iterative gauge fixing, f/it_gauge_fixing.f:5-214
  * (compiled into the reference, never called by it).  One iteration, parity
  * by parity: g = antihermitian part of sum_mu [U_f(x,mu) - U_f(x-mu,mu)]
@@ -416,12 +426,14 @@ int lce_net_train(lce_net* net, int epochs, double lr, double* mean_loss);
  * (configuration in G_prev gauge, G_new G_prev^+) for lce_net_train after
  * convergence.  LCE_WARM_FOURIER iterates from the chosen start with the
  * Fourier-accelerated step of lce_landau_gauge_fourier instead of the plain
- * overrelaxation (power-of-two extents).  net may be NULL when neither NET
- * nor RECORD is set. */
+ * overrelaxation (power-of-two extents); with LCE_WARM_CG as well, the
+ * conjugate-gradient form of lce_landau_gauge_fourier_cg.  net may be NULL
+ * when neither NET nor RECORD is set. */
 #define LCE_WARM_NET 1
 #define LCE_WARM_JUDGE 2
 #define LCE_WARM_RECORD 4
 #define LCE_WARM_FOURIER 8
+#define LCE_WARM_CG 16
 #define LCE_GF_START_NET 2
 int lce_landau_gauge_warm(lce_ctx* ctx, int chain, lce_net* net, int flags, int* start_used, double functional[3],
                           double* theta, int* iters, int max_iters);

@@ -43,6 +43,7 @@ LCE_WARM_NET = 1
 LCE_WARM_JUDGE = 2
 LCE_WARM_RECORD = 4
 LCE_WARM_FOURIER = 8
+LCE_WARM_CG = 16
 
 
 class LceParams(C.Structure):
@@ -132,6 +133,7 @@ SIGNATURES = {
     "lce_landau_gauge_from": (I, [P, I, I, P, P, P, I]),
     "lce_apply_transform": (I, [P, I]),
     "lce_landau_gauge_fourier": (I, [P, I, I, D, D, P, P, P, I]),
+    "lce_landau_gauge_fourier_cg": (I, [P, I, I, D, P, P, P, I]),
     "lce_debug_fourier_step": (I, [P, I, D, P]),
     "lce_set_transform": (I, [P, I, P, C.c_long]),
     "lce_get_transform": (I, [P, I, P, C.c_long]),

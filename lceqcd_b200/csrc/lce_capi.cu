@@ -799,8 +799,9 @@ int fa_buffers(lce_ctx* c) {
 }
 
 // Fourier-accelerated iterations on U_f (tracking G) until theta <= limit or
-// the cap; same graph batching and progress guard as gf_loop
-int fa_loop(lce_ctx* c, int chain, double step, double limit, double* theta, int* iters, int cap) {
+// the cap; same graph batching and progress guard as gf_loop; cg: the
+// conjugate-gradient form (its direction starts afresh)
+int fa_loop(lce_ctx* c, int chain, double step, double limit, double* theta, int* iters, int cap, bool cg = false) {
   const ChainDev& ch = c->ch[chain];
   int rc = fa_buffers(c);
   if (rc) return rc;
@@ -816,9 +817,10 @@ int fa_loop(lce_ctx* c, int chain, double step, double limit, double* theta, int
   CK(cudaMemcpyAsync(c->cst_d + chain, &cs, sizeof(cs), cudaMemcpyHostToDevice, c->stream));
   CK(cudaStreamSynchronize(c->stream));
   double* part = c->scratch_d;
+  if (cg) fa_cg_reset(c->fa_d, fa_vcap(c), c->stream);
   int batch = 4;
   while (true) {
-    auto key = std::make_pair(chain, batch);
+    auto key = std::make_pair(chain, 2 * batch + (cg ? 1 : 0));
     auto it = c->fa_exec.find(key);
     if (it == c->fa_exec.end()) {
       cudaGraph_t g;
@@ -826,10 +828,10 @@ int fa_loop(lce_ctx* c, int chain, double step, double limit, double* theta, int
       for (int k = 0; k < batch; ++k) {
         if (c->prec == LCE_PREC_F64)
           launch_fa_iteration<double>(c->ch_d + chain, ch, c->cst_d + chain, step, c->fa_d, fa_vcap(c), part,
-                                      nullptr, 1, true, true, c->stream);
+                                      nullptr, 1, true, true, cg, c->stream);
         else
           launch_fa_iteration<float>(c->ch_d + chain, ch, c->cst_d + chain, step, c->fa_d, fa_vcap(c), part,
-                                     nullptr, 1, true, true, c->stream);
+                                     nullptr, 1, true, true, cg, c->stream);
       }
       CK(cudaStreamEndCapture(c->stream, &g));
       cudaGraphExec_t ex;
@@ -1689,7 +1691,7 @@ int lce_landau_gauge_warm(lce_ctx* c, int chain, lce_net* net, int flags, int* s
                           double* theta, int* iters, int max_iters) {
   DeviceScope ds_(c ? c->device : -1);
   if (!c || chain < 0 || chain >= c->nchains ||
-      (flags & ~(LCE_WARM_NET | LCE_WARM_JUDGE | LCE_WARM_RECORD | LCE_WARM_FOURIER)))
+      (flags & ~(LCE_WARM_NET | LCE_WARM_JUDGE | LCE_WARM_RECORD | LCE_WARM_FOURIER | LCE_WARM_CG)))
     return LCE_ERR_INVALID;
   const bool use_net = flags & LCE_WARM_NET, judge = flags & LCE_WARM_JUDGE, record = flags & LCE_WARM_RECORD;
   if ((use_net || record) && !net) return fail(c, LCE_ERR_INVALID, "landau_gauge_warm: no network given");
@@ -1752,7 +1754,7 @@ int lce_landau_gauge_warm(lce_ctx* c, int chain, lce_net* net, int flags, int* s
     const int cap = max_iters > 0 ? max_iters : 1000000;
     double th = 0.0;
     int it = 0;
-    rc = fa_loop(c, chain, 1.0, ch.limit_or, &th, &it, cap);
+    rc = fa_loop(c, chain, 1.0, ch.limit_or, &th, &it, cap, (flags & LCE_WARM_CG) != 0);
     if (theta) *theta = th;
     if (iters) *iters = it;
     if (rc == LCE_OK && th > ch.limit_or) rc = fail(c, LCE_ERR_GF_NOT_CONVERGED, "gauge fixing: iteration cap reached");
@@ -1770,10 +1772,11 @@ int lce_landau_gauge_warm(lce_ctx* c, int chain, lce_net* net, int flags, int* s
   return rc;
 }
 
-int lce_landau_gauge_fourier(lce_ctx* c, int chain, int start, double step, double theta_switch, double* theta,
-                             int* iters_fourier, int* iters_plain, int max_iters) {
-  DeviceScope ds_(c ? c->device : -1);
-  if (!c || chain < 0 || chain >= c->nchains) return LCE_ERR_INVALID;
+}  // extern "C"
+
+namespace {
+int fourier_fix(lce_ctx* c, int chain, int start, double step, double theta_switch, double* theta,
+                int* iters_fourier, int* iters_plain, int max_iters, bool cg) {
   const ChainDev& ch = c->ch[chain];
   if (!fa_supported(ch)) return fail(c, LCE_ERR_UNSUPPORTED, "Fourier-accelerated fixing needs power-of-two extents");
   if (!(step > 0.0)) step = 1.0;
@@ -1793,7 +1796,7 @@ int lce_landau_gauge_fourier(lce_ctx* c, int chain, int start, double step, doub
   const int cap = max_iters > 0 ? max_iters : 1000000;
   double th_fa = 0.0;
   int it_fa = 0, it_or = 0;
-  int rc = fa_loop(c, chain, step, theta_switch, &th_fa, &it_fa, cap);
+  int rc = fa_loop(c, chain, step, theta_switch, &th_fa, &it_fa, cap, cg);
   if (iters_fourier) *iters_fourier = it_fa;
   if (iters_plain) *iters_plain = 0;
   if (theta) *theta = th_fa;
@@ -1804,6 +1807,23 @@ int lce_landau_gauge_fourier(lce_ctx* c, int chain, int start, double step, doub
   rc = gf_loop(c, chain, theta, &it_or, cap - it_fa, 1);
   if (iters_plain) *iters_plain = it_or;
   return rc;
+}
+}  // namespace
+
+extern "C" {
+
+int lce_landau_gauge_fourier(lce_ctx* c, int chain, int start, double step, double theta_switch, double* theta,
+                             int* iters_fourier, int* iters_plain, int max_iters) {
+  DeviceScope ds_(c ? c->device : -1);
+  if (!c || chain < 0 || chain >= c->nchains) return LCE_ERR_INVALID;
+  return fourier_fix(c, chain, start, step, theta_switch, theta, iters_fourier, iters_plain, max_iters, false);
+}
+
+int lce_landau_gauge_fourier_cg(lce_ctx* c, int chain, int start, double theta_switch, double* theta,
+                                int* iters_fourier, int* iters_plain, int max_iters) {
+  DeviceScope ds_(c ? c->device : -1);
+  if (!c || chain < 0 || chain >= c->nchains) return LCE_ERR_INVALID;
+  return fourier_fix(c, chain, start, 1.0, theta_switch, theta, iters_fourier, iters_plain, max_iters, true);
 }
 
 int lce_debug_fourier_step(lce_ctx* c, int chain, double step, double* omega) {
@@ -1818,10 +1838,10 @@ int lce_debug_fourier_step(lce_ctx* c, int chain, double step, double* omega) {
   CK(cudaMalloc(&om, ob));
   if (c->prec == LCE_PREC_F64)
     launch_fa_iteration<double>(c->ch_d + chain, ch, nullptr, step, c->fa_d, fa_vcap(c), c->scratch_d, om, 0, false,
-                                false, c->stream);
+                                false, false, c->stream);
   else
     launch_fa_iteration<float>(c->ch_d + chain, ch, nullptr, step, c->fa_d, fa_vcap(c), c->scratch_d, om, 0, false,
-                               false, c->stream);
+                               false, false, c->stream);
   cudaError_t e = cudaGetLastError();
   if (e == cudaSuccess) e = cudaMemcpyAsync(omega, om, ob, cudaMemcpyDeviceToHost, c->stream);
   if (e == cudaSuccess) e = cudaStreamSynchronize(c->stream);

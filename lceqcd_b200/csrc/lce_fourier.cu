@@ -40,6 +40,23 @@
 // transforms themselves are FP32.  Two complex fields carry the three components:
 // (Delta_b) and (Delta_a3 + 0i); the multiplier is real and even in p, so the
 // inverse transform returns each component in its own slot.
+//
+// Conjugate-gradient form (nonlinear CG on the gauge functional with the same
+// Fourier preconditioner, after Hudspith, Comput. Phys. Commun. 187 (2015)
+// 115): the preconditioned gradient g_k = F^-1[F[Delta_k] / p_c^2] enters a
+// direction s_k = g_k + beta_k s_(k-1), beta_k = max(0, Polak-Ribiere) with
+// its inner products sum_x Delta_k.g_k and sum_x Delta_k.g_(k-1) taken in
+// momentum space (Parseval: sum_p |F_k|^2 / p_c^2 and
+// sum_p Re(F_k^* F_(k-1)) / p_c^2, the previous F kept), and the step along
+// s_k maximises the second-order expansion of the functional
+// F(alpha) = sum_(x,mu) c_mu Re a[g_a(x) U(x,mu) g_a(x+mu)^+], g_a = exp(alpha X),
+// X = -i s.sigma: with Y = X(x+mu),
+//   F'(0)  = sum c_mu Re a[X U - U Y]
+//   F''(0) = sum c_mu Re a[X^2 U + U Y^2 - 2 X U Y],
+// alpha = F'(0) / -F''(0) (exact per link to second order, FP64).  Four more
+// kernels per iteration: the beta reduction, the line derivatives, the alpha
+// reduction and g = exp(alpha X) per site.  The step is bounded by a trust
+// region (fa_alpha_kernel).
 #include <algorithm>
 
 #include "lce_internal.hpp"
@@ -227,6 +244,17 @@ __device__ __forceinline__ su2<R> to_r(su2<double> u) {
   return su2<R>{{(R)u.a.re, (R)u.a.im}, {(R)u.b.re, (R)u.b.im}};
 }
 
+// state of the conjugate-gradient form (device, in the buffer)
+struct FaCg {
+  double s_prev;  // sum_p |F_(k-1)|^2 / p_c^2
+  double beta;    // this iteration's Polak-Ribiere coefficient
+  double alpha;   // this iteration's step along the direction
+  int restart;    // the next direction is the preconditioned gradient alone
+  int n_restart;  // directions that did not ascend (diagnostic)
+  int parity;     // F_k goes to prev[parity], F_(k-1) is read from prev[parity ^ 1]
+  int pad;
+};
+
 struct FaArgs {
   const ChainDev* ch;
   const ChainState* cst;  // done flag and step; NULL: never done, step gamma
@@ -236,6 +264,10 @@ struct FaArgs {
   double* part;           // [block]: theta (odd sites)
   double* omega_out;      // debug: omega per site [parity][site][3], or NULL
   const double2* tw;      // exp(-2 pi i k / kFaPoints), k < kFaPoints / 2
+  void* prev;             // CG: F of this and the previous iteration, [2][2 fields][V] complex, natural order
+  float* sdir;            // CG: direction s, [component][parity][site]
+  double* cgpart;         // CG: per-block pairs of sums
+  FaCg* cg;               // CG: state
   int L[3], logL[3];
   int track;
 };
@@ -313,7 +345,7 @@ __global__ void __launch_bounds__(kFaThreads) fa_div_kernel(FaArgs a) {
 // (2) theta = sum / nh (odd sites); count; done flag at theta <= gf_limit or
 // the cap
 __global__ void __launch_bounds__(1024) fa_check_kernel(const ChainDev* chp, ChainState* cst, const double* part,
-                                                        int nblocks) {
+                                                        int nblocks, int adapt) {
   if (cst->gf_done) return;
   double v[1] = {0.0};
   for (int b = threadIdx.x; b < nblocks; b += blockDim.x) v[0] += part[b];
@@ -325,7 +357,8 @@ __global__ void __launch_bounds__(1024) fa_check_kernel(const ChainDev* chp, Cha
     const int it = cst->gf_iters + 1;
     // a step that doubled theta overshot (far from the Landau gauge the
     // linearised step can be too long): shorten it for the rest of the run
-    if (it > 1 && theta > 2.0 * cst->gf_theta) cst->gf_step = fmax(0.1, 0.7 * cst->gf_step);
+    // (the conjugate-gradient form chooses its own step)
+    if (adapt && it > 1 && theta > 2.0 * cst->gf_theta) cst->gf_step = fmax(0.1, 0.7 * cst->gf_step);
     cst->gf_iters = it;
     cst->gf_theta = theta;
     if (!(theta > cst->gf_limit) || (cst->gf_cap > 0 && it >= cst->gf_cap)) cst->gf_done = 1;
@@ -335,7 +368,9 @@ __global__ void __launch_bounds__(1024) fa_check_kernel(const ChainDev* chp, Cha
 // (3)-(5) FFT of one field (blockIdx.y) along axis AX (1: y, 2: z); for
 // AX = 2 with SCALE: forward, multiply by gamma / (p_c^2 V), inverse
 // (the forward-scale-inverse form is held to 64 registers, 4 blocks per SM)
-template <int AX, int SIGN, bool SCALE, int LOGN>
+// CG (with SCALE): the block's sums of |F|^2 / p_c^2 and Re(F^* F_prev) / p_c^2
+// into cgpart, and F kept as the next F_prev
+template <int AX, int SIGN, bool SCALE, int LOGN, bool CG = false>
 __global__ void __launch_bounds__(kFaThreads, SCALE && LOGN <= 8 ? 4 : 1) fa_fft_kernel(FaArgs a) {
   using G = FaLines<LOGN>;
   constexpr int n = G::n, ld = G::ld, NL = G::NLT, LNL = kFaBlockLog - LOGN;
@@ -372,6 +407,26 @@ __global__ void __launch_bounds__(kFaThreads, SCALE && LOGN <= 8 ? 4 : 1) fa_fft
   }
   __syncthreads();
   fft2_lines<LOGN>(d, tw);
+  if (CG) {
+    // two buffers: a read-modify-write of one stalled every element on its
+    // own load (5x the kernel's time at 128^3)
+    const int par = a.cg->parity;
+    FftC* Pn = reinterpret_cast<FftC*>(a.prev) + ((size_t)par * 2 + blockIdx.y) * V;
+    const FftC* Po = reinterpret_cast<const FftC*>(a.prev) + ((size_t)(par ^ 1) * 2 + blockIdx.y) * V;
+    double v[2] = {0.0, 0.0};
+    for (int e = threadIdx.x; e < NL * n; e += blockDim.x) {
+      const int j = e & (NL - 1), k = e >> LNL, l = l0 + j;
+      if (l >= nlines) continue;
+      const size_t gi = nat_index<AX>(a, l, k);
+      const FftC f = d[j * ld + k], pv = __ldg(Po + gi);
+      Pn[gi] = f;
+      if ((l | k) == 0) continue;
+      const double m0 = 1.0 / (4.0 * (sxy[j] + sz2[k]));
+      v[0] += m0 * ((double)f.x * f.x + (double)f.y * f.y);
+      v[1] += m0 * ((double)f.x * pv.x + (double)f.y * pv.y);
+    }
+    block_reduce_store<2>(v, a.cgpart + 2 * ((size_t)blockIdx.y * gridDim.x + blockIdx.x));
+  }
   if (SCALE) {
     const double gv = (a.cst ? a.cst->gf_step : a.gamma) / (4.0 * (double)V);
     for (int e = threadIdx.x; e < NL * n; e += blockDim.x) {
@@ -390,8 +445,9 @@ __global__ void __launch_bounds__(kFaThreads, SCALE && LOGN <= 8 ? 4 : 1) fa_fft
   }
 }
 
-// (6) inverse FFT along x; g(x) = exp(-i omega.sigma) per site
-template <typename R, int LOGN>
+// (6) inverse FFT along x; g(x) = exp(-i omega.sigma) per site (CG: the
+// direction s = omega + beta s instead)
+template <typename R, int LOGN, bool CG = false>
 __global__ void __launch_bounds__(kFaThreads) fa_g_kernel(FaArgs a) {
   using G = FaLines<LOGN>;
   constexpr int n = G::n, ld = G::ld, NL = G::NLT / 2;
@@ -419,6 +475,16 @@ __global__ void __launch_bounds__(kFaThreads) fa_g_kernel(FaArgs a) {
     const int y = l & (a.L[1] - 1), z = l >> a.logL[1];
     const int p = (x + y + z) & 1, s = site_index(x, y, z, ch.hx, ch.nxy);
     const double w3 = d[(NL + j) * ld + x].x, wbr = d[j * ld + x].x, wbi = d[j * ld + x].y;
+    if (CG) {
+      const double beta = a.cg->beta;
+      const size_t V2 = 2 * (size_t)ch.nh, gi = (size_t)p * ch.nh + s;
+      float* S = a.sdir;
+      // beta = 0 starts afresh (the old direction is not read)
+      S[gi] = (float)(beta > 0.0 ? w3 + beta * (double)S[gi] : w3);
+      S[V2 + gi] = (float)(beta > 0.0 ? wbr + beta * (double)S[V2 + gi] : wbr);
+      S[2 * V2 + gi] = (float)(beta > 0.0 ? wbi + beta * (double)S[2 * V2 + gi] : wbi);
+      continue;
+    }
     const double nw = sqrt(w3 * w3 + wbr * wbr + wbi * wbi);
     su2<double> gg{{1.0, 0.0}, {0.0, 0.0}};
     if (nw > 0.0) {
@@ -470,6 +536,121 @@ __global__ void __launch_bounds__(kBlock) fa_apply_kernel(FaArgs a) {
   }
 }
 
+// CG: beta = max(0, (S_k - C_k) / S_(k-1)) from the scale kernel's sums
+__global__ void __launch_bounds__(1024) fa_beta_kernel(FaArgs a, int nparts) {
+  if (fa_done(a)) return;
+  double v[2] = {0.0, 0.0};
+  for (int b = threadIdx.x; b < nparts; b += blockDim.x) {
+    v[0] += a.cgpart[2 * b];
+    v[1] += a.cgpart[2 * b + 1];
+  }
+  __shared__ double t[2];
+  block_reduce_store<2>(v, t);
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    FaCg* g = a.cg;
+    double beta = 0.0;
+    if (!g->restart && g->s_prev > 0.0) beta = fmax(0.0, (t[0] - t[1]) / g->s_prev);
+    g->beta = beta;
+    g->s_prev = t[0];
+    g->restart = 0;
+    g->parity ^= 1;
+  }
+}
+
+// X = -i s.sigma in first-row form (the generator of exp(-i omega.sigma) above)
+__device__ __forceinline__ su2<double> fa_gen(const float* S, size_t V2, size_t gi) {
+  return su2<double>{{0.0, -(double)S[gi]}, {-(double)S[V2 + gi], -(double)S[2 * V2 + gi]}};
+}
+
+// CG: per-block F'(0), F''(0) along s and sum |s|^2 (one thread per site,
+// both parities)
+template <typename R>
+__global__ void __launch_bounds__(kBlock) fa_line_kernel(FaArgs a) {
+  if (fa_done(a)) return;
+  const ChainDev& ch = *a.ch;
+  const int i = blockIdx.x * kBlock + threadIdx.x;
+  double v[3] = {0.0, 0.0, 0.0};
+  if (i < 2 * ch.nh) {
+    const int eo = i >= ch.nh ? 1 : 0, oe = 1 - eo, s = i - eo * ch.nh, nh = ch.nh;
+    const size_t V2 = 2 * (size_t)nh;
+    const Coord X = site_coord(eo, s, ch.hx, ch.nxy, ch.dhx, ch.dnxy);
+    const su2<double> gx = fa_gen(a.sdir, V2, (size_t)eo * nh + s);
+    const double xx = gx.a.im * gx.a.im + gx.b.re * gx.b.re + gx.b.im * gx.b.im;
+    v[2] = xx;
+    const int L[3] = {ch.L1, ch.L2, ch.L3};
+#pragma unroll
+    for (int mu = 0; mu < 3; ++mu) {
+      int c[3] = {X.x, X.y, X.z};
+      c[mu] = wrap(c[mu] + 1, L[mu]);
+      const int sp = site_index(c[0], c[1], c[2], ch.hx, ch.nxy);
+      const su2<double> gy = fa_gen(a.sdir, V2, (size_t)oe * nh + sp);
+      const double yy = gy.a.im * gy.a.im + gy.b.re * gy.b.re + gy.b.im * gy.b.im;
+      const su2<double> u = to_d(LinkIO<R>::ld_cg(ch.uf, ((size_t)(mu * 2 + eo)) * nh + s));
+      const double w = mu == 2 ? ch.alpha : 1.0;
+      const su2<double> xu = nn(gx, u);
+      v[0] += w * (xu.a.re - nn(u, gy).a.re);
+      v[1] += w * (-(xx + yy) * u.a.re - 2.0 * nn(xu, gy).a.re);
+    }
+  }
+  block_reduce_store<3>(v, a.cgpart + 3 * (size_t)blockIdx.x);
+}
+
+// CG step: the maximum of the quadratic model, alpha = F'(0) / -F''(0), inside
+// a trust region: at most 10, and an rms rotation angle alpha |s|_rms of at
+// most 0.5 (far from the Landau gauge the model's maximum lies where the
+// functional is no longer quadratic).  Near the gauge the slow modes are the
+// low modes of the Faddeev-Popov operator, for which the free Laplacian
+// overestimates the curvature: alpha ~ 4 there, where the steepest-ascent form
+// takes 1.  A non-concave line takes alpha = 1 (within the angle bound), one
+// that does not ascend moves nothing; both restart from the gradient.
+__global__ void __launch_bounds__(1024) fa_alpha_kernel(FaArgs a, int nparts) {
+  if (fa_done(a)) return;
+  double v[3] = {0.0, 0.0, 0.0};
+  for (int b = threadIdx.x; b < nparts; b += blockDim.x) {
+    v[0] += a.cgpart[3 * b];
+    v[1] += a.cgpart[3 * b + 1];
+    v[2] += a.cgpart[3 * b + 2];
+  }
+  __shared__ double t[3];
+  block_reduce_store<3>(v, t);
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    FaCg* g = a.cg;
+    const double d1 = t[0], d2 = t[1], rms = sqrt(t[2] / (2.0 * a.ch->nh));
+    const double amax = rms > 0.0 ? fmin(10.0, 0.5 / rms) : 10.0;
+    double al;
+    if (d1 > 0.0 && d2 < 0.0) {
+      al = fmin(d1 / -d2, amax);
+    } else {
+      al = d1 > 0.0 ? fmin(1.0, amax) : 0.0;
+      g->restart = 1;
+      g->n_restart += 1;
+    }
+    g->alpha = al;
+  }
+}
+
+// CG: g(x) = exp(alpha X(x)) per site
+__global__ void __launch_bounds__(kBlock) fa_gstep_kernel(FaArgs a) {
+  if (fa_done(a)) return;
+  const ChainDev& ch = *a.ch;
+  const int i = blockIdx.x * kBlock + threadIdx.x;
+  if (i >= 2 * ch.nh) return;
+  const size_t V2 = 2 * (size_t)ch.nh;
+  const double al = a.cg->alpha;
+  const double w3 = al * a.sdir[i], wbr = al * a.sdir[V2 + i], wbi = al * a.sdir[2 * V2 + i];
+  const double nw = sqrt(w3 * w3 + wbr * wbr + wbi * wbi);
+  su2<double> gg{{1.0, 0.0}, {0.0, 0.0}};
+  if (nw > 0.0) {
+    double sn, cs;
+    sincos(nw, &sn, &cs);
+    const double f = sn / nw;
+    gg = su2<double>{{cs, -f * w3}, {-f * wbr, -f * wbi}};
+  }
+  LinkIO<double>::st(a.gstep, (size_t)i, gg);
+}
+
 int ilog2_exact(int n) {
   int l = 0;
   while ((1 << l) < n) ++l;
@@ -487,18 +668,24 @@ bool fa_supported(const ChainDev& ch) {
   return true;
 }
 
-// two FP64 complex fields and the FP64 step transform
-// Buffer layout for chains of up to vcap sites: two FP64 complex fields,
-// the FP64 step transform and the twiddle table (fixed offsets, so graphs
-// captured for one chain stay valid while others use the same buffer)
-size_t fa_buffer_bytes(size_t vcap) {
-  return 2 * vcap * sizeof(FftC) + vcap * 32 + kFaPoints / 2 * sizeof(double2) + 256;
-}
+// Buffer layout for chains of up to vcap sites: two complex fields, the
+// FP64 step transform, the twiddle table, then the conjugate-gradient form's
+// state, this and the previous F (two complex fields each), direction (3
+// FP32 per site) and per-block sums (fixed offsets, so graphs captured for
+// one chain stay valid while others use the same buffer)
 namespace {
-void* fa_gstep(void* buf, size_t vcap) { return reinterpret_cast<char*>(buf) + 2 * vcap * sizeof(FftC); }
-double2* fa_table(void* buf, size_t vcap) {
-  return reinterpret_cast<double2*>(reinterpret_cast<char*>(buf) + 2 * vcap * sizeof(FftC) + vcap * 32);
-}
+size_t fa_off_table(size_t vcap) { return 2 * vcap * sizeof(FftC) + vcap * 32; }
+size_t fa_off_cg(size_t vcap) { return (fa_off_table(vcap) + kFaPoints / 2 * sizeof(double2) + 255) & ~(size_t)255; }
+size_t fa_off_prev(size_t vcap) { return fa_off_cg(vcap) + 256; }
+size_t fa_off_sdir(size_t vcap) { return fa_off_prev(vcap) + 4 * vcap * sizeof(FftC); }
+size_t fa_off_cgpart(size_t vcap) { return (fa_off_sdir(vcap) + 3 * vcap * sizeof(float) + 255) & ~(size_t)255; }
+size_t fa_cgpart_n(size_t vcap) { return 3 * (vcap / 128 + 64); }  // doubles: triples for >= V/256 + 64 blocks
+}  // namespace
+size_t fa_buffer_bytes(size_t vcap) { return fa_off_cgpart(vcap) + fa_cgpart_n(vcap) * sizeof(double) + 256; }
+namespace {
+char* fa_at(void* buf, size_t off) { return reinterpret_cast<char*>(buf) + off; }
+void* fa_gstep(void* buf, size_t vcap) { return fa_at(buf, 2 * vcap * sizeof(FftC)); }
+double2* fa_table(void* buf, size_t vcap) { return reinterpret_cast<double2*>(fa_at(buf, fa_off_table(vcap))); }
 }  // namespace
 
 namespace {
@@ -515,6 +702,21 @@ void fa_init_table(void* buf, size_t vcap, cudaStream_t s) {
   fa_twiddle_table_kernel<<<1, kFaPoints / 2, 0, s>>>(fa_table(buf, vcap));
 }
 
+namespace {
+__global__ void fa_cg_reset_kernel(FaCg* g) {
+  g->s_prev = 0.0;
+  g->beta = 0.0;
+  g->alpha = 0.0;
+  g->restart = 1;
+  g->n_restart = 0;
+  g->parity = 0;
+}
+}  // namespace
+
+void fa_cg_reset(void* buf, size_t vcap, cudaStream_t s) {
+  fa_cg_reset_kernel<<<1, 1, 0, s>>>(reinterpret_cast<FaCg*>(fa_at(buf, fa_off_cg(vcap))));
+}
+
 // launchers per line length (the kernels are compiled for each power of two)
 template <typename K>
 void fa_launch(K kernel, dim3 grid, size_t smem, const FaArgs& a, cudaStream_t s) {
@@ -525,15 +727,15 @@ template <typename R, int LOGN>
 void fa_div_launch(const FaArgs& a, int nb, cudaStream_t s) {
   fa_launch(fa_div_kernel<R, LOGN>, dim3(nb), FaLines<LOGN>::smem(1, 0), a, s);
 }
-template <typename R, int LOGN>
+template <typename R, int LOGN, bool CG = false>
 void fa_g_launch(const FaArgs& a, int nb, cudaStream_t s) {
-  fa_launch(fa_g_kernel<R, LOGN>, dim3(nb), FaLines<LOGN>::smem(1, 0), a, s);
+  fa_launch(fa_g_kernel<R, LOGN, CG>, dim3(nb), FaLines<LOGN>::smem(1, 0), a, s);
 }
-template <int AX, int SIGN, bool SCALE, int LOGN>
+template <int AX, int SIGN, bool SCALE, int LOGN, bool CG = false>
 void fa_fft_launch(const FaArgs& a, int nb, cudaStream_t s) {
   using G = FaLines<LOGN>;
-  fa_launch(fa_fft_kernel<AX, SIGN, SCALE, LOGN>, dim3(nb, 2), G::smem(SCALE ? 2 : 1, SCALE ? G::n + G::NLT : 0), a,
-            s);
+  fa_launch(fa_fft_kernel<AX, SIGN, SCALE, LOGN, CG>, dim3(nb, 2),
+            G::smem(SCALE ? 2 : 1, SCALE ? G::n + G::NLT : 0), a, s);
 }
 #define LCE_FA_SWITCH(logn, CALL) \
   switch (logn) {                 \
@@ -556,11 +758,12 @@ int fa_blocks(long nlines, int logn, int fields) {
   return ceil_div(nlines, (long)(kFaBlockPts >> logn) / fields);
 }
 
-// enqueue one Fourier-accelerated iteration (kernels 1-7)
+// enqueue one Fourier-accelerated iteration (kernels 1-7; cg: the
+// conjugate-gradient form, 11 kernels)
 template <typename R>
 void launch_fa_iteration(const ChainDev* chd, const ChainDev& ch, ChainState* cst, double gamma, void* buf,
                          size_t vcap, double* part, double* omega_out, int track, bool with_check, bool with_apply,
-                         cudaStream_t s) {
+                         bool cg, cudaStream_t s) {
   FaArgs a;
   a.ch = chd;
   a.cst = cst;
@@ -576,30 +779,51 @@ void launch_fa_iteration(const ChainDev* chd, const ChainDev& ch, ChainState* cs
   a.L[2] = ch.L3;
   for (int d = 0; d < 3; ++d) a.logL[d] = ilog2_exact(a.L[d]);
   a.track = track;
+  a.cg = reinterpret_cast<FaCg*>(fa_at(buf, fa_off_cg(vcap)));
+  a.prev = fa_at(buf, fa_off_prev(vcap));
+  a.sdir = reinterpret_cast<float*>(fa_at(buf, fa_off_sdir(vcap)));
+  a.cgpart = reinterpret_cast<double*>(fa_at(buf, fa_off_cgpart(vcap)));
   const int nbd = fa_blocks((long)ch.L2 * ch.L3, a.logL[0], 2);
 #define LCE_FA_DIV(L) fa_div_launch<R, L>(a, nbd, s)
   LCE_FA_SWITCH(a.logL[0], LCE_FA_DIV)
 #undef LCE_FA_DIV
-  if (with_check) fa_check_kernel<<<1, 1024, 0, s>>>(chd, cst, part, nbd);
+  if (with_check) fa_check_kernel<<<1, 1024, 0, s>>>(chd, cst, part, nbd, cg ? 0 : 1);
   const int nby = fa_blocks((long)V / ch.L2, a.logL[1], 1), nbz = fa_blocks((long)V / ch.L3, a.logL[2], 1);
 #define LCE_FA_Y(L) fa_fft_launch<1, -1, false, L>(a, nby, s)
   LCE_FA_SWITCH(a.logL[1], LCE_FA_Y)
 #undef LCE_FA_Y
+  if (cg) {
+#define LCE_FA_ZC(L) fa_fft_launch<2, -1, true, L, true>(a, nbz, s)
+    LCE_FA_SWITCH(a.logL[2], LCE_FA_ZC)
+#undef LCE_FA_ZC
+    fa_beta_kernel<<<1, 1024, 0, s>>>(a, 2 * nbz);
+  } else {
 #define LCE_FA_Z(L) fa_fft_launch<2, -1, true, L>(a, nbz, s)
-  LCE_FA_SWITCH(a.logL[2], LCE_FA_Z)
+    LCE_FA_SWITCH(a.logL[2], LCE_FA_Z)
 #undef LCE_FA_Z
+  }
 #define LCE_FA_YI(L) fa_fft_launch<1, +1, false, L>(a, nby, s)
   LCE_FA_SWITCH(a.logL[1], LCE_FA_YI)
 #undef LCE_FA_YI
+  const int nbv = ceil_div((long)V, kBlock);
+  if (cg) {
+#define LCE_FA_GC(L) fa_g_launch<R, L, true>(a, nbd, s)
+    LCE_FA_SWITCH(a.logL[0], LCE_FA_GC)
+#undef LCE_FA_GC
+    fa_line_kernel<R><<<nbv, kBlock, 0, s>>>(a);
+    fa_alpha_kernel<<<1, 1024, 0, s>>>(a, nbv);
+    fa_gstep_kernel<<<nbv, kBlock, 0, s>>>(a);
+  } else {
 #define LCE_FA_G(L) fa_g_launch<R, L>(a, nbd, s)
-  LCE_FA_SWITCH(a.logL[0], LCE_FA_G)
+    LCE_FA_SWITCH(a.logL[0], LCE_FA_G)
 #undef LCE_FA_G
-  if (with_apply) fa_apply_kernel<R><<<ceil_div((long)V, kBlock), kBlock, 0, s>>>(a);
+  }
+  if (with_apply) fa_apply_kernel<R><<<nbv, kBlock, 0, s>>>(a);
 }
 
 template void launch_fa_iteration<float>(const ChainDev*, const ChainDev&, ChainState*, double, void*, size_t,
-                                         double*, double*, int, bool, bool, cudaStream_t);
+                                         double*, double*, int, bool, bool, bool, cudaStream_t);
 template void launch_fa_iteration<double>(const ChainDev*, const ChainDev&, ChainState*, double, void*, size_t,
-                                          double*, double*, int, bool, bool, cudaStream_t);
+                                          double*, double*, int, bool, bool, bool, cudaStream_t);
 
 }  // namespace lce

@@ -212,11 +212,14 @@ bool fa_supported(const ChainDev& ch);
 size_t fa_buffer_bytes(size_t vcap);
 // fill the twiddle table of freshly allocated buffers
 void fa_init_table(void* buf, size_t vcap, cudaStream_t s);
-// one iteration; cst NULL (debug): never done, step gamma instead of the chain state's
+// one iteration; cst NULL (debug): never done, step gamma instead of the
+// chain state's; cg: the conjugate-gradient form
 template <typename R>
 void launch_fa_iteration(const ChainDev* chd, const ChainDev& ch, ChainState* cst, double gamma, void* buf,
                          size_t vcap, double* part, double* omega_out, int track, bool with_check, bool with_apply,
-                         cudaStream_t s);
+                         bool cg, cudaStream_t s);
+// the conjugate-gradient form starts its next iteration from the gradient
+void fa_cg_reset(void* buf, size_t vcap, cudaStream_t s);
 template <typename R>
 void launch_gf_theta(const ChainDev* ch, double* part, int nh, cudaStream_t s);
 void launch_sum_partials(const double* part, int nblocks, int nq, double* out, cudaStream_t s);

@@ -1,7 +1,8 @@
 """Landau gauge fixing of thermalised configurations to theta < limit_or:
 the reference's method (overrelaxation from G = 1) against the same
 iteration from the previous configuration's converged transform and the
-Fourier-accelerated iteration from G = 1 and from that transform.
+Fourier-accelerated iteration (steepest ascent and conjugate gradients) from
+G = 1 and from that transform.
 
     python -m lceqcd_b200.gauge_fix_study [--L 64] [--configs 4] [--no-plain]
 
@@ -34,7 +35,8 @@ def main(argv=None):
     g.init_hot(a.seed + 1)
     g.sweeps(200, 0)
     g.landau_gauge_fourier("identity")  # the chain's first transform
-    rows = {k: [] for k in ("plain_identity", "plain_warm", "fourier_identity", "fourier_warm")}
+    rows = {k: [] for k in ("plain_identity", "plain_warm", "fourier_identity", "fourier_warm",
+                            "fourier_cg_identity", "fourier_cg_warm")}
 
     def timed(name, fn):
         g.synchronize()
@@ -51,8 +53,11 @@ def main(argv=None):
             g.set_transform(G)
             timed("plain_warm", lambda: g.landau_gauge_from("transform")[2])
         timed("fourier_identity", lambda: sum(g.landau_gauge_fourier("identity")[1:]))
+        timed("fourier_cg_identity", lambda: sum(g.landau_gauge_fourier_cg("identity")[1:]))
         g.set_transform(G)
         timed("fourier_warm", lambda: sum(g.landau_gauge_fourier("transform")[1:]))
+        g.set_transform(G)
+        timed("fourier_cg_warm", lambda: sum(g.landau_gauge_fourier_cg("transform")[1:]))
     out = {"L": a.L, "configs": a.configs, "limit": 1e-10}
     for k, rs in rows.items():
         if rs:

@@ -301,7 +301,7 @@ class _Context:
         return ts.value, th.value, it.value
 
     def landau_gauge_warm(self, net=None, use_net: bool = True, judge: bool = True, record: bool = False,
-                          fourier: bool = False, max_iters: int = 0, chain: int = 0):
+                          fourier: bool = False, max_iters: int = 0, chain: int = 0, cg: bool = False):
         """Tracked gauge fixing from a warm start (the previous transform, or the
         network's correction of it; with judge the start of largest gauge
         functional among identity / previous / network).  Returns
@@ -309,7 +309,7 @@ class _Context:
         'transform' or 'net'."""
         flags = ((_lib.LCE_WARM_NET if (use_net and net is not None) else 0) |
                  (_lib.LCE_WARM_JUDGE if judge else 0) | (_lib.LCE_WARM_RECORD if record else 0) |
-                 (_lib.LCE_WARM_FOURIER if fourier else 0))
+                 (_lib.LCE_WARM_FOURIER if fourier else 0) | (_lib.LCE_WARM_CG if cg else 0))
         su, th, it = C.c_int(), C.c_double(), C.c_int()
         F = (C.c_double * 3)()
         self._ck(self.lib.lce_landau_gauge_warm(self.h, chain, net.h if net is not None else None, flags,
@@ -324,6 +324,16 @@ class _Context:
         code = {"identity": _lib.LCE_GF_START_IDENTITY, "transform": _lib.LCE_GF_START_TRANSFORM}[start]
         self._ck(self.lib.lce_landau_gauge_fourier(self.h, chain, code, float(step), float(theta_switch),
                                                    C.byref(th), C.byref(itf), C.byref(itp), int(max_iters)))
+        return th.value, itf.value, itp.value
+
+    def landau_gauge_fourier_cg(self, start: str = "identity", theta_switch: float = 0.0, max_iters: int = 0,
+                                chain: int = 0):
+        """The conjugate-gradient form of landau_gauge_fourier (lce_landau_gauge_fourier_cg).
+        Returns (theta, fourier_iters, plain_iters)."""
+        th, itf, itp = C.c_double(), C.c_int(), C.c_int()
+        code = {"identity": _lib.LCE_GF_START_IDENTITY, "transform": _lib.LCE_GF_START_TRANSFORM}[start]
+        self._ck(self.lib.lce_landau_gauge_fourier_cg(self.h, chain, code, float(theta_switch), C.byref(th),
+                                                      C.byref(itf), C.byref(itp), int(max_iters)))
         return th.value, itf.value, itp.value
 
     def debug_fourier_step(self, step: float = 1.0, chain: int = 0) -> np.ndarray:
