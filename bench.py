@@ -293,7 +293,7 @@ def extras(args, peak):
         lat.init_hot(22)
         lat.sweeps(200, 0)
         lat.landau_gauge_fourier("identity")  # the chain's first transform
-        rows = {"plain_identity": [], "plain_warm": [], "fourier_warm": []}
+        rows = {"plain_identity": [], "plain_warm": [], "fourier_warm": [], "fourier_cg_warm": []}
 
         def timed(fn):
             lat.synchronize()
@@ -311,6 +311,9 @@ def extras(args, peak):
             lat.set_transform(G)
             rows["fourier_warm"].append(
                 timed(lambda: (lambda r: (r[0], r[1] + r[2]))(lat.landau_gauge_fourier("transform"))))
+            lat.set_transform(G)
+            rows["fourier_cg_warm"].append(
+                timed(lambda: (lambda r: (r[0], r[1] + r[2]))(lat.landau_gauge_fourier_cg("transform"))))
         gf = {"limit": 1e-10, "configs": 2, "omega_or": 1.7}
         for k, rs in rows.items():
             gf[k] = {"s_per_config": statistics.mean(r[0] for r in rs), "iterations": [r[1] for r in rs],
@@ -319,6 +322,8 @@ def extras(args, peak):
                                                              sum(gf["fourier_warm"]["iterations"]))
         gf["time_plain_identity_over_fourier_warm"] = (gf["plain_identity"]["s_per_config"] /
                                                        gf["fourier_warm"]["s_per_config"])
+        gf["time_plain_identity_over_fourier_cg_warm"] = (gf["plain_identity"]["s_per_config"] /
+                                                          gf["fourier_cg_warm"]["s_per_config"])
         gf["plain_hbm_gbs"] = statistics.mean(216 * vol(L) * r[1] / r[0] / 1e9 for r in rows["plain_identity"])
         out["gauge_fix_128cubed"] = gf
         lat.close()
@@ -327,8 +332,8 @@ def extras(args, peak):
     # the full production pipeline at 256^3 (beta = 16, x = 0.08, y = 0.2): a
     # sweep is ahiggs2, ahiggs3, one ahiggs1, the agauge heatbath and 4 link
     # overrelaxation hits; a measurement every 20 sweeps is a warm-started
-    # Fourier-accelerated Landau gauge fixing to theta < 1e-10 and the
-    # correlators.  Timed: 20 sweeps + 1 measurement, after thermalisation and a
+    # Fourier-accelerated Landau gauge fixing (conjugate-gradient form) to
+    # theta < 1e-10 and the correlators.  Timed: 20 sweeps + 1 measurement, after thermalisation and a
     # first gauge fixing from G = 1; the 2000-sweep run is projected from them.
     try:
         L = (256, 256, 256)
@@ -343,7 +348,7 @@ def extras(args, peak):
         lat.sweep(1)
         lat.synchronize()
         t1 = time.perf_counter()
-        th, itf, itp = lat.landau_gauge_fourier("transform")
+        th, itf, itp = lat.landau_gauge_fourier_cg("transform")
         lat.correlator()
         lat.synchronize()
         t2 = time.perf_counter()

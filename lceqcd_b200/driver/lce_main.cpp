@@ -11,14 +11,14 @@
 //   lce_main [--input FILE] [--dir DIR] [--precision f32|f64] [--seed N]
 //            [--corr-flag 1|2|3] [--therm N] [--max-gf-iters N]
 //            [--gf-angle acos|atan2] [--device N] [--agauge-hits 1|3]
-//            [--gauge-fix plain|warm|fourier|it] [--it-step S]
+//            [--gauge-fix plain|warm|fourier|fourier-cg|it] [--it-step S]
 //
 // --agauge-hits 3 runs the 3-hit link update of f/agauge1.f (the reference
 // picks agauge.f or agauge1.f at build time).  --gauge-fix: plain is
 // f/landau_gauge.f (copy, overrelaxation from G = 1); warm starts every
 // measurement after the first from the previous converged transform; fourier
 // uses the Fourier-accelerated iteration (power-of-two extents) from that warm
-// start; it is f/landau_gauge.f with the reference's iterative form
+// start, fourier-cg its conjugate-gradient form; it is f/landau_gauge.f with the reference's iterative form
 // f/it_gauge_fixing.f in place of the overrelaxation, component corrected and
 // ascending, step --it-step (default 0.3; the reference's alpha diverges).
 // All stop at theta <= limit_or.
@@ -222,7 +222,8 @@ int main(int argc, char** argv) {
   p.device = device;
   p.gf_angle = gf_angle;
   p.agauge_hits = agauge_hits;
-  if (gauge_fix != "plain" && gauge_fix != "warm" && gauge_fix != "fourier" && gauge_fix != "it")
+  if (gauge_fix != "plain" && gauge_fix != "warm" && gauge_fix != "fourier" && gauge_fix != "fourier-cg" &&
+      gauge_fix != "it")
     die("unknown --gauge-fix %s", gauge_fix.c_str());
   lce_ctx* ctx = lce_create(&p);
   if (!ctx) die("lce_create: %s", lce_last_error(nullptr));
@@ -322,6 +323,10 @@ int main(int argc, char** argv) {
       } else if (gauge_fix == "fourier") {
         int it_plain = 0;
         rc = lce_landau_gauge_fourier(ctx, 0, start, 0.0, 0.0, &theta, &iters, &it_plain, max_gf);
+        iters += it_plain;
+      } else if (gauge_fix == "fourier-cg") {
+        int it_plain = 0;
+        rc = lce_landau_gauge_fourier_cg(ctx, 0, start, 0.0, &theta, &iters, &it_plain, max_gf);
         iters += it_plain;
       } else if (gauge_fix == "it") {
         rc = lce_it_landau_gauge(ctx, 0, it_step, LCE_ITGF_FIX_COMPONENT | LCE_ITGF_ASCEND, &theta, &iters, max_gf);

@@ -5,9 +5,9 @@ overrelaxation hits, the Higgs heatbath, overrelaxation and Metropolis steps
 (f/main.f:38-41 with the 3 link updates and ahiggs1), meas1 every sweep and
 every `--meas-every` sweeps the gauge-fixed measurements of f/main.f:57-79:
 warm-started Landau gauge fixing to theta < 1e-10 (the Fourier-accelerated
-iteration from the previous transform or the network's correction of it,
-whichever starts at the larger functional) and the z-correlators, Polyakov
-loop and scalar correlator.
+iteration, conjugate-gradient form unless --no-cg, from the previous
+transform or the network's correction of it, whichever starts at the larger
+functional) and the z-correlators, Polyakov loop and scalar correlator.
 
     python -m lceqcd_b200.pipeline_study [--L 256] [--sweeps 100] [--meas-every 20]
         [--therm 200] [--pairs 4] [--judge-L 128]
@@ -74,12 +74,13 @@ def main(argv=None):
     ap.add_argument("--judge-L", type=int, default=128)
     ap.add_argument("--judge-sweeps", type=int, default=300)
     ap.add_argument("--seed", type=int, default=1)
+    ap.add_argument("--no-cg", dest="cg", action="store_false")
     a = ap.parse_args(argv)
     L = (a.L,) * 3
     V = a.L ** 3
     peak, peak_kind = hbm_peak()
     out = {"L": a.L, "couplings": COUP, "precision": "f32", "link_or_hits": a.n_or, "higgs_metro": a.metro,
-           "sweeps": a.sweeps, "meas_every": a.meas_every, "therm": a.therm, "limit": 1e-10}
+           "cg": a.cg, "sweeps": a.sweeps, "meas_every": a.meas_every, "therm": a.therm, "limit": 1e-10}
 
     g = chain(L, "f32", a.seed, a.n_or, a.metro)
     g.sweeps(a.therm, 0)
@@ -112,7 +113,7 @@ def main(argv=None):
         done += n
         if n == a.meas_every:
             t = time.perf_counter()
-            start, F, theta, iters = g.landau_gauge_warm(net, use_net=True, judge=True, fourier=True)
+            start, F, theta, iters = g.landau_gauge_warm(net, use_net=True, judge=True, fourier=True, cg=a.cg)
             ca, cu, _, _ = g.correlator()
             _, pc, _ = g.polyakov()
             _, sc, _ = g.scalarcorr()

@@ -151,3 +151,20 @@ def test_driver_iterative_gauge_fixing(tmp_path):
     r = subprocess.run([DRIVER, "--input", str(inp), "--dir", str(tmp_path), "--gauge-fix", "sd"],
                        capture_output=True, text=True, timeout=60)
     assert r.returncode != 0 and "gauge-fix" in r.stderr
+
+
+@pytest.mark.parametrize("form", ["fourier", "fourier-cg"])
+def test_driver_fourier_gauge_fixing(tmp_path, form):
+    """--gauge-fix fourier / fourier-cg: the measurement files of the
+    overrelaxed run, the Fourier-accelerated iteration (steepest ascent or
+    conjugate gradients) from the previous transform."""
+    inp = tmp_path / "inputfile"
+    inp.write_text(INPUT.format(L=8, init=2, start=0))
+    r = subprocess.run([DRIVER, "--input", str(inp), "--dir", str(tmp_path), "--therm", "20",
+                        "--gauge-fix", form], capture_output=True, text=True, timeout=300)
+    assert r.returncode == 0, r.stderr
+    tag = "s08_be09000_x01000_y04500_u000000"
+    correl = (tmp_path / f"correl_{tag}").read_text().splitlines()
+    assert correl[3] == "001" and len(correl) == 3 + 2 * (1 + 8)
+    vals = np.array([float(v) for l in correl[4:] if not l.strip().isdigit() for v in l.split()])
+    assert vals.size > 0 and np.all(np.isfinite(vals))
