@@ -655,7 +655,8 @@ def run_reference(args):
 
 def quick_gauge_fix(args):
     """The Fourier-accelerated gauge fixing as a profiling case: args.quick_gauge_fix
-    iterations (7 kernel launches each) from G = 1, stopped by the iteration cap."""
+    iterations (7 kernel launches each; 11 for the conjugate-gradient form with
+    --gauge-fix-cg) from G = 1, stopped by the iteration cap."""
     from lceqcd_b200 import Lattice, LceError
     n = args.lattice or 128
     lat = Lattice((n, n, n), **COUP, precision="f32", seed=21, lam=1.7, limit_or=1e-10)
@@ -664,13 +665,16 @@ def quick_gauge_fix(args):
     lat.synchronize()
     t0 = time.perf_counter()
     try:
-        lat.landau_gauge_fourier("identity", max_iters=args.quick_gauge_fix)
+        if args.gauge_fix_cg:
+            lat.landau_gauge_fourier_cg("identity", max_iters=args.quick_gauge_fix)
+        else:
+            lat.landau_gauge_fourier("identity", max_iters=args.quick_gauge_fix)
     except LceError as e:
         if e.code != -3:  # LCE_ERR_GF_NOT_CONVERGED: the cap stopped it, as intended
             raise
     lat.synchronize()
-    print(json.dumps({"quick_gauge_fix": args.quick_gauge_fix, "L": n, "theta": lat.theta(),
-                      "s": time.perf_counter() - t0}), flush=True)
+    print(json.dumps({"quick_gauge_fix": args.quick_gauge_fix, "cg": args.gauge_fix_cg, "L": n,
+                      "theta": lat.theta(), "s": time.perf_counter() - t0}), flush=True)
 
 
 def main():
@@ -691,6 +695,8 @@ def main():
     ap.add_argument("--quick-gauge-fix", type=int, default=0, metavar="ITERS",
                     help="profiling case: ITERS Fourier-accelerated gauge-fixing iterations on a thermalised "
                          "--lattice^3 FP32 configuration, then exit")
+    ap.add_argument("--gauge-fix-cg", action="store_true",
+                    help="with --quick-gauge-fix: the conjugate-gradient form")
     args = ap.parse_args()
     if args.quick_gauge_fix:
         quick_gauge_fix(args)
