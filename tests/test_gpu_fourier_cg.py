@@ -79,3 +79,25 @@ def test_cg_needs_power_of_two_extents():
     g.init_hot(1)
     with pytest.raises(LceError):
         g.landau_gauge_fourier_cg("identity")
+
+
+def test_cg_in_a_batch_of_uneven_volumes():
+    """Chains of different volumes share the context's buffers (transforms,
+    previous F, direction, CG state); the CG state restarts for each chain,
+    and steepest-ascent and CG runs interleave with their graphs intact."""
+    from lceqcd_b200 import Ensemble, Params
+    specs = [Params(L=(16, 16, 16), **COUP, limit_or=1e-10, seed=1),
+             Params(L=(32, 16, 8), **COUP, limit_or=1e-10, seed=2),
+             Params(L=(8, 8, 8), **COUP, limit_or=1e-10, seed=3)]
+    ens = Ensemble(specs)
+    ens.init_hot(4)
+    ens.sweeps(30, 0)
+    for rnd in range(2):
+        for c in (2, 0, 1) if rnd else (0, 1, 2):
+            start = "identity" if rnd == 0 else "transform"
+            th, itf, itp = ens.landau_gauge_fourier_cg(start, chain=c)
+            assert th <= 1e-10 and itp == 0
+            assert ens.theta(chain=c) <= 1e-10
+            th, itf, itp = ens.landau_gauge_fourier(start, chain=c)
+            assert th <= 1e-10
+        ens.sweeps(2, 0)
