@@ -251,8 +251,8 @@ int lce_landau_gauge_fourier(lce_ctx* ctx, int chain, int start, double step, do
  * preconditioner (after Hudspith, Comput. Phys. Commun. 187 (2015) 115):
  * direction s = F^-1[F[Delta]/p^2] + beta s_prev, beta = max(0,
  * Polak-Ribiere), and the step along s that maximises the second-order
- * expansion of the gauge functional (computed exactly per link in FP64),
- * bounded by a trust region on the rotation angle.
+ * expansion of the gauge functional (its derivatives exact per link, summed
+ * in FP64), bounded by a trust region on the rotation angle.
  * No reference counterpart; arguments and stopping criterion as
  * lce_landau_gauge_fourier (no step argument). */
 int lce_landau_gauge_fourier_cg(lce_ctx* ctx, int chain, int start, double theta_switch, double* theta,

@@ -53,7 +53,7 @@
 // X = -i s.sigma: with Y = X(x+mu),
 //   F'(0)  = sum c_mu Re a[X U - U Y]
 //   F''(0) = sum c_mu Re a[X^2 U + U Y^2 - 2 X U Y],
-// alpha = F'(0) / -F''(0) (exact per link to second order, FP64).  Four more
+// alpha = F'(0) / -F''(0) (exact per link to second order).  Four more
 // kernels per iteration: the beta reduction, the line derivatives, the alpha
 // reduction and g = exp(alpha X) per site.  The step is bounded by a trust
 // region (fa_alpha_kernel).
@@ -503,6 +503,36 @@ __global__ void __launch_bounds__(kFaThreads) fa_g_kernel(FaArgs a) {
   }
 }
 
+// CG: g = exp(alpha X) at flat index gi of the direction, X = -i s.sigma:
+// cos n - (sin n / n) i (alpha s).sigma, n = alpha |s|; below n = 0.05 by the
+// Taylor series of cos n and sin n / n through n^8 (the first term left out
+// is below 3e-20), else by sincos
+__device__ __forceinline__ su2<double> fa_exp_dir(const float* S, size_t V2, size_t gi, double al) {
+  const double w3 = al * S[gi], wbr = al * S[V2 + gi], wbi = al * S[2 * V2 + gi];
+  const double n2 = w3 * w3 + wbr * wbr + wbi * wbi;
+  double c, f;
+  if (n2 < 0.0025) {
+    c = 1.0 + n2 * (-1.0 / 2.0 + n2 * (1.0 / 24.0 + n2 * (-1.0 / 720.0 + n2 * (1.0 / 40320.0))));
+    f = 1.0 + n2 * (-1.0 / 6.0 + n2 * (1.0 / 120.0 + n2 * (-1.0 / 5040.0 + n2 * (1.0 / 362880.0))));
+  } else {
+    const double n = sqrt(n2);
+    double sn;
+    sincos(n, &sn, &c);
+    f = sn / n;
+  }
+  return su2<double>{{c, -f * w3}, {-f * wbr, -f * wbi}};
+}
+
+// CG: g(x) = exp(alpha X(x)) per site.  (Forming it inside the apply kernel
+// instead, four exponentials per site, took 108 us against 17 + 69 us at
+// 128^3 for the first iterations from G = 1, whose large angles take sincos.)
+__global__ void __launch_bounds__(kBlock) fa_gstep_kernel(FaArgs a) {
+  if (fa_done(a)) return;
+  const int i = blockIdx.x * kBlock + threadIdx.x;
+  if (i >= 2 * a.ch->nh) return;
+  LinkIO<double>::st(a.gstep, (size_t)i, fa_exp_dir(a.sdir, 2 * (size_t)a.ch->nh, (size_t)i, a.cg->alpha));
+}
+
 // (7) U_f(x,mu) -> g(x) U_f(x,mu) g(x+mu)^+, A_f -> g A_f g^+, G -> g G
 template <typename R>
 __global__ void __launch_bounds__(kBlock) fa_apply_kernel(FaArgs a) {
@@ -559,12 +589,15 @@ __global__ void __launch_bounds__(1024) fa_beta_kernel(FaArgs a, int nparts) {
 }
 
 // X = -i s.sigma in first-row form (the generator of exp(-i omega.sigma) above)
-__device__ __forceinline__ su2<double> fa_gen(const float* S, size_t V2, size_t gi) {
-  return su2<double>{{0.0, -(double)S[gi]}, {-(double)S[V2 + gi], -(double)S[2 * V2 + gi]}};
+template <typename R>
+__device__ __forceinline__ su2<R> fa_gen(const float* S, size_t V2, size_t gi) {
+  return su2<R>{{(R)0, -(R)S[gi]}, {-(R)S[V2 + gi], -(R)S[2 * V2 + gi]}};
 }
 
 // CG: per-block F'(0), F''(0) along s and sum |s|^2 (one thread per site,
-// both parities)
+// both parities).  Per link in the fields' precision (they only set the step
+// length; the cancellation in F'' ~ |s(x) - s(x+mu)|^2 loses at most ~(L/2pi)^2
+// of the relative precision), summed in FP64.
 template <typename R>
 __global__ void __launch_bounds__(kBlock) fa_line_kernel(FaArgs a) {
   if (fa_done(a)) return;
@@ -575,22 +608,22 @@ __global__ void __launch_bounds__(kBlock) fa_line_kernel(FaArgs a) {
     const int eo = i >= ch.nh ? 1 : 0, oe = 1 - eo, s = i - eo * ch.nh, nh = ch.nh;
     const size_t V2 = 2 * (size_t)nh;
     const Coord X = site_coord(eo, s, ch.hx, ch.nxy, ch.dhx, ch.dnxy);
-    const su2<double> gx = fa_gen(a.sdir, V2, (size_t)eo * nh + s);
-    const double xx = gx.a.im * gx.a.im + gx.b.re * gx.b.re + gx.b.im * gx.b.im;
-    v[2] = xx;
+    const su2<R> gx = fa_gen<R>(a.sdir, V2, (size_t)eo * nh + s);
+    const R xx = gx.a.im * gx.a.im + gx.b.re * gx.b.re + gx.b.im * gx.b.im;
+    v[2] = (double)xx;
     const int L[3] = {ch.L1, ch.L2, ch.L3};
 #pragma unroll
     for (int mu = 0; mu < 3; ++mu) {
       int c[3] = {X.x, X.y, X.z};
       c[mu] = wrap(c[mu] + 1, L[mu]);
       const int sp = site_index(c[0], c[1], c[2], ch.hx, ch.nxy);
-      const su2<double> gy = fa_gen(a.sdir, V2, (size_t)oe * nh + sp);
-      const double yy = gy.a.im * gy.a.im + gy.b.re * gy.b.re + gy.b.im * gy.b.im;
-      const su2<double> u = to_d(LinkIO<R>::ld_cg(ch.uf, ((size_t)(mu * 2 + eo)) * nh + s));
+      const su2<R> gy = fa_gen<R>(a.sdir, V2, (size_t)oe * nh + sp);
+      const R yy = gy.a.im * gy.a.im + gy.b.re * gy.b.re + gy.b.im * gy.b.im;
+      const su2<R> u = LinkIO<R>::ld_cg(ch.uf, ((size_t)(mu * 2 + eo)) * nh + s);
       const double w = mu == 2 ? ch.alpha : 1.0;
-      const su2<double> xu = nn(gx, u);
-      v[0] += w * (xu.a.re - nn(u, gy).a.re);
-      v[1] += w * (-(xx + yy) * u.a.re - 2.0 * nn(xu, gy).a.re);
+      const su2<R> xu = nn(gx, u);
+      v[0] += w * (double)(xu.a.re - nn(u, gy).a.re);
+      v[1] += w * (double)(-(xx + yy) * u.a.re - (R)2 * nn(xu, gy).a.re);
     }
   }
   block_reduce_store<3>(v, a.cgpart + 3 * (size_t)blockIdx.x);
@@ -629,26 +662,6 @@ __global__ void __launch_bounds__(1024) fa_alpha_kernel(FaArgs a, int nparts) {
     }
     g->alpha = al;
   }
-}
-
-// CG: g(x) = exp(alpha X(x)) per site
-__global__ void __launch_bounds__(kBlock) fa_gstep_kernel(FaArgs a) {
-  if (fa_done(a)) return;
-  const ChainDev& ch = *a.ch;
-  const int i = blockIdx.x * kBlock + threadIdx.x;
-  if (i >= 2 * ch.nh) return;
-  const size_t V2 = 2 * (size_t)ch.nh;
-  const double al = a.cg->alpha;
-  const double w3 = al * a.sdir[i], wbr = al * a.sdir[V2 + i], wbi = al * a.sdir[2 * V2 + i];
-  const double nw = sqrt(w3 * w3 + wbr * wbr + wbi * wbi);
-  su2<double> gg{{1.0, 0.0}, {0.0, 0.0}};
-  if (nw > 0.0) {
-    double sn, cs;
-    sincos(nw, &sn, &cs);
-    const double f = sn / nw;
-    gg = su2<double>{{cs, -f * w3}, {-f * wbr, -f * wbi}};
-  }
-  LinkIO<double>::st(a.gstep, (size_t)i, gg);
 }
 
 int ilog2_exact(int n) {
