@@ -1,6 +1,7 @@
 """Gauge-fixed observables of production ensembles against the plain FP64 GPU
-path: the FP32 chain is fixed by the Fourier-accelerated iteration from the
-previous measurement's transform, the FP64 chain by the reference's method
+path: FP32 chains are fixed by the Fourier-accelerated iteration (steepest
+ascent, and in a second chain conjugate gradients) from the previous
+measurement's transform, the FP64 chain by the reference's method
 (overrelaxation from G = 1).  The Landau-gauge A0 and link correlators, their
 effective masses (jackknife over bins) and the final gauge functional agree
 within errors; the warm-started accelerated fixing takes far fewer
@@ -28,6 +29,9 @@ def series(precision, seed, method):
         g.sweeps(EVERY, 0)
         if method == "plain":
             th, it = g.landau_gauge()
+        elif method == "cg":
+            th, itf, itp = g.landau_gauge_fourier_cg("transform" if k else "identity")
+            it = itf + itp
         else:
             th, itf, itp = g.landau_gauge_fourier("transform" if k else "identity")
             it = itf + itp
@@ -42,12 +46,13 @@ def series(precision, seed, method):
 
 @pytest.fixture(scope="module")
 def runs():
-    return {"fa": series("f32", 31, "fourier"), "plain": series("f64", 32, "plain")}
+    return {"fa": series("f32", 31, "fourier"), "cg": series("f32", 33, "cg"), "plain": series("f64", 32, "plain")}
 
 
+@pytest.mark.parametrize("form", ["fa", "cg"])
 @pytest.mark.parametrize("obs", ["ca", "cu"])
-def test_correlators_and_masses_match(runs, obs):
-    a, b = runs["fa"][obs], runs["plain"][obs]
+def test_correlators_and_masses_match(runs, obs, form):
+    a, b = runs[form][obs], runs["plain"][obs]
     for z in range(0, 4):
         ea, sa = jackknife(lambda c: c[z], a)
         eb, sb = jackknife(lambda c: c[z], b)
@@ -63,10 +68,12 @@ def test_correlators_and_masses_match(runs, obs):
             assert abs(zz) < 3.0
 
 
-def test_functional_and_iterations(runs):
-    fa, pl = mean_err(runs["fa"]["F"]), mean_err(runs["plain"]["F"])
-    print(f"functional: fa {fa[0]:.6f}+-{fa[1]:.6f} plain {pl[0]:.6f}+-{pl[1]:.6f}")
+@pytest.mark.parametrize("form", ["fa", "cg"])
+def test_functional_and_iterations(runs, form):
+    fa, pl = mean_err(runs[form]["F"]), mean_err(runs["plain"]["F"])
+    print(f"functional: {form} {fa[0]:.6f}+-{fa[1]:.6f} plain {pl[0]:.6f}+-{pl[1]:.6f}")
     assert abs(z_score(fa, pl)) < 3.0
-    print("mean iterations: fourier warm", runs["fa"]["iters"].mean(), "plain", runs["plain"]["iters"].mean())
-    # at 8x8x16 the gain is ~1.8x; it grows with the volume (48x at 128^3 in the bench)
-    assert runs["fa"]["iters"].mean() * 1.4 < runs["plain"]["iters"].mean()
+    print("mean iterations:", form, runs[form]["iters"].mean(), "plain", runs["plain"]["iters"].mean())
+    # at 8x8x16 the steepest-ascent gain is ~1.8x; it grows with the volume
+    # (59x at 128^3 in the bench, ~190x for the conjugate-gradient form)
+    assert runs[form]["iters"].mean() * 1.4 < runs["plain"]["iters"].mean()
