@@ -2,7 +2,7 @@
 workload: thermalised L^3 configurations (beta = 12, x = 0.09, y = 0.3, 10
 sweeps apart), overrelaxation parameter 1.7, theta < 1e-10.
 
-    python -m lceqcd_b200.warm_start_study [--L 128] [--pairs 400] [--test 50] [--epochs 10]
+    python -m lceqcd_b200.warm_start_study [--L 128] [--pairs 400] [--test 50] [--epochs 10] [--cg]
 
 Records `pairs` training pairs from the Fourier-accelerated fixing started at
 the previous configuration's transform, trains the network on the device,
@@ -36,6 +36,8 @@ def main(argv=None):
     ap.add_argument("--epochs", type=int, default=10)
     ap.add_argument("--lr", type=float, default=1e-3)
     ap.add_argument("--seed", type=int, default=3)
+    ap.add_argument("--cg", action="store_true",
+                    help="test fixings by the conjugate-gradient form (recording stays steepest ascent)")
     a = ap.parse_args(argv)
     L = (a.L,) * 3
     V = a.L ** 3
@@ -72,16 +74,18 @@ def main(argv=None):
         rows[name].append((it, time.perf_counter() - t, g.gauge_functional()))
 
     def judge():
-        start, _, _, it = g.landau_gauge_warm(net, use_net=True, judge=True, fourier=True)
+        start, _, _, it = g.landau_gauge_warm(net, use_net=True, judge=True, fourier=True, cg=a.cg)
         judged[start] += 1
         return it
 
     for k in range(a.test):
         g.sweeps(10, 0)
         G = g.get_transform()
-        run("fourier_previous", lambda: g.landau_gauge_warm(net, use_net=False, judge=False, fourier=True)[3])
+        run("fourier_previous",
+            lambda: g.landau_gauge_warm(net, use_net=False, judge=False, fourier=True, cg=a.cg)[3])
         g.set_transform(G)
-        run("fourier_network", lambda: g.landau_gauge_warm(net, use_net=True, judge=False, fourier=True)[3])
+        run("fourier_network",
+            lambda: g.landau_gauge_warm(net, use_net=True, judge=False, fourier=True, cg=a.cg)[3])
         g.set_transform(G)
         run("fourier_judge", judge)
         if k < a.plain:
@@ -90,7 +94,7 @@ def main(argv=None):
         g.set_transform(G)
         g.landau_gauge_warm(net, use_net=False, judge=False, fourier=True)
 
-    out = {"L": a.L, "pairs": a.pairs, "test_configs": a.test, "epochs": a.epochs,
+    out = {"L": a.L, "pairs": a.pairs, "test_configs": a.test, "epochs": a.epochs, "cg": a.cg,
            "record_s": t_rec, "record_mean_iterations": statistics.mean(rec_iters),
            "train_s": t_train, "train_steps": steps, "train_tflops_bf16": train_tflops,
            "loss_per_epoch": losses, "judge_choices": judged}
