@@ -126,6 +126,22 @@ def test_composed_sweep_ensemble_matches(composed, one, other, obs):
     assert abs(z) < 3.0
 
 
+@pytest.mark.parametrize("obs", ["plaq", "a2", "pol"])
+def test_composed_sweep_from_the_reference_init2_start(composed, obs):
+    """The same workload from the reference's init = 2 cold start
+    (f/confget.f unitconf: U = 1, A0 = (0, 0, 1)) thermalises to the
+    ensemble of the A0 = 0 start (the FP64 run above)."""
+    if "init2" not in composed:
+        g = Lattice(L16, beta=9.0, x=0.1, y=0.45, precision="f32", seed=24)
+        g.init_unit(1.0)
+        composed["init2"] = composed_series(g, lambda h: h.polyakov()[2])
+    a = mean_err(composed["init2"][obs])
+    b = mean_err(composed["f64"][obs])
+    z = z_score(a, b)
+    print(f"{obs}: init2 f32 {a[0]:.6f}+-{a[1]:.6f}  A0=0 f64 {b[0]:.6f}+-{b[1]:.6f}  z={z:+.2f}")
+    assert abs(z) < 3.0
+
+
 def test_composed_sweep_metropolis_step_is_tuned(composed):
     """f/ahiggs1.f:117-123 rescales the step while |acceptance - 1/2| > 0.1."""
     for k in ("f32", "f64", "oracle"):
