@@ -147,3 +147,30 @@ def test_composed_sweep_metropolis_step_is_tuned(composed):
     for k in ("f32", "f64", "oracle"):
         acc = composed[k]["acc_metro"]
         assert 0.35 < acc.mean() < 0.65, (k, acc.mean())
+
+
+# ---- the mixed-precision single-chain workload: 64^3, beta 12, x 0.09,
+# y 0.3, hot start, 500 sweeps (the headline sweep); FP32 fields with FP64
+# reunitarisation and sums against the FP64 path, measured over the last
+# 400 sweeps of two chains started alike
+L64 = (64, 64, 64)
+
+
+@pytest.fixture(scope="module")
+def mixed64():
+    out = {}
+    for prec, seed in (("f32", 41), ("f64", 42)):
+        g = Lattice(L64, beta=12.0, x=0.09, y=0.3, precision=prec, seed=seed)
+        g.init_hot(seed)
+        rows = [g.sweep(1) for _ in range(500)][100:]
+        out[prec] = {k: np.array([r[k] for r in rows]) for k in ("plaq", "a2", "a4")}
+        g.close()
+    return out
+
+
+@pytest.mark.parametrize("obs", ["plaq", "a2", "a4"])
+def test_mixed_precision_64cubed_observables_match_fp64(mixed64, obs):
+    a, b = mean_err(mixed64["f32"][obs]), mean_err(mixed64["f64"][obs])
+    z = z_score(a, b)
+    print(f"64^3 {obs}: f32 {a[0]:.7f}+-{a[1]:.7f} (tau {a[2]:.1f})  f64 {b[0]:.7f}+-{b[1]:.7f}  z={z:+.2f}")
+    assert abs(z) < 3.0
