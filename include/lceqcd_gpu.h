@@ -11,7 +11,7 @@
  * The reference exposes no plugin API: the boundary replaced here is the set
  * of Fortran subroutines that f/main.f:21-78 calls inside its sweep loop, and
  * the COMMON blocks they share (f/INCLUDE/gaugefield.inc:35-36,
- * f/INCLUDE/measurement.inc:228-233).  Each declaration below names the
+ * f/INCLUDE/measurement.inc:30-35).  Each declaration below names the
  * reference routine it replaces.
  *
  * Host field layout ("reference order"), matching the COMMON arrays
@@ -83,7 +83,7 @@ extern "C" {
 typedef struct lce_ctx lce_ctx;
 
 /* Input parameters: the hot-path subset of the reference's inputfile
- * (f/paraminit.f:325-344) plus build-only knobs. */
+ * (f/paraminit.f:82-101) plus build-only knobs. */
 typedef struct lce_params {
   int L[3];              /* global lattice extents (even)            inputfile line 1 */
   double beta, x, y;     /* couplings                                  lines 8-10 */
@@ -131,7 +131,7 @@ const char* lce_strerror(int status);
 /* last CUDA/validation error message of a context (or of the last failed create) */
 const char* lce_last_error(lce_ctx* ctx);
 void lce_default_params(lce_params* p);
-/* f/paraminit.f:393-396: beta_a, beta_2, beta_4 from beta, x, y (FP64) */
+/* f/paraminit.f:150-153: beta_a, beta_2, beta_4 from beta, x, y (FP64) */
 int lce_couplings(const lce_params* p, double out[3]);
 /* f/adresses.f:91-337 neighbour tables (single rank, periodic), 0-based:
  * t[(eo*3 + mu)*nh + site]; computed by the same index arithmetic the kernels use */
@@ -185,19 +185,19 @@ int lce_set_rng_position(lce_ctx* ctx, unsigned long long pass_ctr, unsigned lon
 /* ---- Monte Carlo updates (accept may be NULL: no synchronisation) ---- */
 /* f/ahiggs1.f:7-127 Metropolis; *delta is adapted as the reference does */
 int lce_ahiggs1(lce_ctx* ctx, float* delta, int measflag, float* accept);
-/* f/ahiggs2.f:124-267 heatbath (with f/a_force.f, f/gauss.f) */
+/* f/ahiggs2.f:7-152 heatbath (with f/a_force.f, f/gauss.f) */
 int lce_ahiggs2(lce_ctx* ctx, int measflag, float* accept);
-/* f/ahiggs3.f:283-424 overrelaxation */
+/* f/ahiggs3.f:7-148 overrelaxation */
 int lce_ahiggs3(lce_ctx* ctx, int measflag, float* accept);
 /* f/agauge.f:7-205 with f/staples.f, f/heat_kpi.f */
 int lce_agauge(lce_ctx* ctx, int measflag, float* accept);
-/* f/agauge1.f:7-235: the 3-hit link update (staple once per (parity, mu),
+/* f/agauge1.f:7-237: the 3-hit link update (staple once per (parity, mu),
  * then three heatbath + Metropolis hits of 7 uniforms per site each; the
  * acceptance divides the Metropolis count by the hits, :226-231) */
 int lce_agauge1(lce_ctx* ctx, int measflag, float* accept);
 /* link overrelaxation with the agauge Metropolis test (no reference counterpart) */
 int lce_link_or(lce_ctx* ctx, int measflag, float* accept);
-/* f/renorm.f:205-236 */
+/* f/renorm.f:6-37 */
 int lce_renorm(lce_ctx* ctx);
 /* f/main.f:38-41: ahiggs2, ahiggs3, [ahiggs1 x n_higgs_metro], agauge,
  * [link OR x n_link_or], reunitarisation fused into the link writers; one
@@ -213,7 +213,7 @@ int lce_get_sweep_mode(lce_ctx* ctx);
 int lce_get_meas(lce_ctx* ctx, int chain, lce_meas* m);
 int lce_get_meas_batch(lce_ctx* ctx, lce_meas* m /* [nchains] */);
 
-/* ---- gauge fixing (f/landau_gauge.f:281-338, f/or_gauge_fixing1.f) ---- */
+/* ---- gauge fixing (f/landau_gauge.f:6-63, f/or_gauge_fixing1.f) ---- */
 /* copy U,A -> U_f,A_f, iterate overrelaxed gauge fixing until theta <= limit_or.
  * max_iters <= 0 means no cap (the reference has none).  Returns
  * LCE_ERR_GF_NOT_CONVERGED when the cap ends the loop. */
@@ -223,7 +223,7 @@ int lce_gauge_fix_continue(lce_ctx* ctx, int chain, double* theta, int* iters, i
 /* Gauge fixing that also tracks the accumulated transform G, with
  * U_f(x,mu) = G(x) U(x,mu) G(x+mu)^+ and A_f = G A G^+ throughout (no
  * reference counterpart: the reference keeps no transform).  start:
- *   LCE_GF_START_IDENTITY   G = 1 (the reference's start, f/landau_gauge.f:308-324)
+ *   LCE_GF_START_IDENTITY   G = 1 (the reference's start, f/landau_gauge.f:33-49)
  *   LCE_GF_START_TRANSFORM  start from the context's current G (warm start:
  *                           the previous measurement's converged transform,
  *                           a transform set by lce_set_transform)
@@ -257,7 +257,7 @@ int lce_landau_gauge_fourier(lce_ctx* ctx, int chain, int start, double step, do
  * lce_landau_gauge_fourier (no step argument). */
 int lce_landau_gauge_fourier_cg(lce_ctx* ctx, int chain, int start, double theta_switch, double* theta,
                                 int* iters_fourier, int* iters_plain, int max_iters);
-/* The reference's iterative gauge fixing, f/it_gauge_fixing.f:5-214
+/* The reference's iterative gauge fixing, f/it_gauge_fixing.f:5-206
  * (compiled into the reference, never called by it).  One iteration, parity
  * by parity: g = antihermitian part of sum_mu [U_f(x,mu) - U_f(x-mu,mu)]
  * in first-row form, Omega = exp(step g) = cos|step g| + step g
@@ -279,7 +279,7 @@ int lce_landau_gauge_fourier_cg(lce_ctx* ctx, int chain, int start, double theta
 #define LCE_ITGF_ASCEND 2
 #define LCE_ITGF_TRACK 4
 int lce_it_gauge_fixing(lce_ctx* ctx, int chain, double step, int flags, double* da1);
-/* f/landau_gauge.f:303-334 with it_gauge_fixing in place of
+/* f/landau_gauge.f:28-59 with it_gauge_fixing in place of
  * or_gauge_fixing: copy U,A -> U_f,A_f (and G = 1 with LCE_ITGF_TRACK),
  * then iterate + reunitarise U_f until da1 <= limit_or, on the device in
  * captured batches like lce_landau_gauge.  max_iters <= 0: 10^6 cap;
@@ -301,12 +301,12 @@ int lce_theta(lce_ctx* ctx, int chain, double* theta);
 
 /* ---- measurements ---- */
 /* f/correlator.f:11-186 (z-slice correlators of A_f and U_f, all z) and
- * f/meas2a.f:168-178 (average of A_f); any output may be NULL */
+ * f/meas2a.f:39-49 (average of A_f); any output may be NULL */
 int lce_correlator(lce_ctx* ctx, int chain, double* corr_a, double* corr_u, double* corr_3,
                    double af[3]);
-/* f/polyakov.f:202-315: slice means of cos(4|A|), their correlator, mean^2 */
+/* f/polyakov.f:10-123: slice means of cos(4|A|), their correlator, mean^2 */
 int lce_polyakov(lce_ctx* ctx, int chain, double* slice, double* corr, double* mean2);
-/* f/scalarcorr.f:331-440: slice means of |A|^2, their correlator, mean */
+/* f/scalarcorr.f:10-119: slice means of |A|^2, their correlator, mean */
 int lce_scalarcorr(lce_ctx* ctx, int chain, double* slice, double* corr, double* mean);
 /* average plaquette 1/2 Re Tr of the current U (all 3V plaquettes) */
 int lce_plaquette(lce_ctx* ctx, int chain, double* plaq);
@@ -356,7 +356,7 @@ int lce_slabs_sweep(lce_slabs* s, int measflag, lce_meas* m);
 /* u_f, a_f (LCE_FIELDS_FIXED of lce_download) of the whole lattice */
 int lce_slabs_download_fixed(lce_slabs* s, float* u, float* a, long ld);
 int lce_slabs_download_fixed_f64(lce_slabs* s, double* u, double* a, long ld);
-/* lce_landau_gauge (f/landau_gauge.f:308-324, f/or_gauge_fixing1.f) on the
+/* lce_landau_gauge (f/landau_gauge.f:33-49, f/or_gauge_fixing1.f) on the
  * slabs: a half-step's update of the U_z links below a slab's first plane
  * goes back to the slab below, theta is the whole lattice's; same iterations
  * and (up to the order of the theta sum) the same u_f, a_f as undecomposed */

@@ -109,7 +109,7 @@ size_t link_bytes(int prec) { return prec == LCE_PREC_F64 ? 32 : 16; }
 size_t real_bytes(int prec) { return prec == LCE_PREC_F64 ? 8 : 4; }
 size_t align256(size_t n) { return (n + 255) & ~(size_t)255; }
 
-// f/paraminit.f:287-290 and :393-396, in the precision of the fields
+// f/paraminit.f:44-47 and :150-153, in the precision of the fields
 template <typename T>
 void couplings_t(double beta, double x, double y, double out[3]) {
   const T pi = (T)2.0 * (T)std::acos((T)0.0);
@@ -955,7 +955,7 @@ int slab_exchange(lce_slabs* S, const PlaneCopy* cp, int ncp) {
 
 // the measured quantities of the whole lattice from the slabs' summed
 // per-slot totals: the formulas of the finalize kernel (f/meas1.f inputs,
-// f/ahiggs2.f:259-264, f/agauge.f:195-200, f/agauge1.f:226-231)
+// f/ahiggs2.f:142-147, f/agauge.f:195-200, f/agauge1.f:227-232)
 // delta: the whole lattice's ahiggs1 step, adapted as the finalize kernel
 // adapts it (f/ahiggs1.f:113-123, in the fields' precision) from the whole
 // lattice's acceptance
@@ -1052,7 +1052,7 @@ int slab_sweep(lce_slabs* S, int measflag, lce_meas* m) {
   return LCE_OK;
 }
 
-// the overrelaxed Landau gauge fixing of f/landau_gauge.f:308-324 and
+// the overrelaxed Landau gauge fixing of f/landau_gauge.f:33-49 and
 // f/or_gauge_fixing1.f on the slabs.  A half-step updates the U_z link below
 // each site of a slab's first interior plane, which lives in the lower halo
 // and belongs to slab k-1: after it that link goes back to slab k-1 (its
@@ -1599,7 +1599,7 @@ int lce_landau_gauge(lce_ctx* c, int chain, double* theta, int* iters, int max_i
   DeviceScope ds_(c ? c->device : -1);
   if (!c || chain < 0 || chain >= c->nchains) return LCE_ERR_INVALID;
   const ChainDev& ch = c->ch[chain];
-  // f/landau_gauge.f:308-324 copy u -> u_f, a -> a_f
+  // f/landau_gauge.f:33-49 copy u -> u_f, a -> a_f
   const size_t ub = (size_t)6 * ch.nh * link_bytes(c->prec), ab = (size_t)6 * ch.nh * real_bytes(c->prec);
   CK(cudaMemcpyAsync(ch.uf, ch.u, ub, cudaMemcpyDeviceToDevice, c->stream));
   CK(cudaMemcpyAsync(ch.af, ch.a, ab, cudaMemcpyDeviceToDevice, c->stream));

@@ -124,7 +124,7 @@ struct LinkIO<double> {
   }
 };
 
-// Reunitarise in FP64 before storing (f/renorm.f:226-230 fused into the writer).
+// Reunitarise in FP64 before storing (f/renorm.f:27-31 fused into the writer).
 // The norm is formed in FP64 from the stored components; for n = 1 + e with
 // |e| < 1e-4 (every link written by an update) 1/sqrt(n) is the series
 // 1 - e/2 + 3e^2/8 - 5e^3/16, whose truncation error (35/128) e^4 < 3e-17 is

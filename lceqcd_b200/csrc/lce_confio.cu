@@ -26,7 +26,7 @@
 extern "C" int lce_conf_filename(char* buf, size_t n, const char* prefix, int L3, double beta, double x, double y,
                                  int number) {
   if (!buf || !prefix || n == 0) return LCE_ERR_INVALID;
-  // f/measinit.f:1000 format: '<prefix>_s', i2.2, '_be', i5.5, '_x', i5.5, '_y', i5.5, '_u', i6.6
+  // f/measinit.f:240 format: '<prefix>_s', i2.2, '_be', i5.5, '_x', i5.5, '_y', i5.5, '_u', i6.6
   const long betaint = std::lround(1000.0 * beta), xint = std::lround(10000.0 * x), yint = std::lround(10000.0 * y);
   const int r = std::snprintf(buf, n, "%s_s%02d_be%05ld_x%05ld_y%05ld_u%06d", prefix, L3, betaint, xint, yint, number);
   return (r < 0 || (size_t)r >= n) ? LCE_ERR_INVALID : LCE_OK;

@@ -11,7 +11,7 @@
 // Every link touched in a half-step belongs to exactly one thread, so the
 // update is race free.  All links are rewritten in the eo = 1 half-step, so
 // reunitarising there is exactly f/u_f_renorm.f after the iteration
-// (f/landau_gauge.f:329-334).  A one-block check kernel sums the partials in a
+// (f/landau_gauge.f:54-59).  A one-block check kernel sums the partials in a
 // fixed order, counts the iteration and raises a device flag when theta <=
 // limit_or (or the cap is reached); later kernels of a captured batch of
 // iterations see the flag and return at once, so the host reads the state
@@ -155,7 +155,7 @@ __global__ void __launch_bounds__(kBlock, sizeof(R) == 4 ? 4 : 1)
   if (last) block_reduce_store<1>(th, part + blockIdx.x);
 }
 
-// One parity of f/it_gauge_fixing.f:52-210 (the reference's iterative gauge
+// One parity of f/it_gauge_fixing.f:52-206 (the reference's iterative gauge
 // fixing): g = sum_mu (i Im a, b) of U_f(x,mu) minus the same of
 // U_f(x-mu,mu) (:62-84), the second component as written g1(1) - g2(2)
 // (:110) unless LCE_ITGF_FIX_COMPONENT; |g|^2 into the partial sums on the

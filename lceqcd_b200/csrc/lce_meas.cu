@@ -4,10 +4,10 @@
 // FP64, the quantities the reference accumulates per slice:
 //   0..2   A_f                        f/correlator.f:58-59
 //   3..11  per mu: Im a, Im b, -Re b  of U_f  (Im a and -i b, :61-74)
-//   12     cos(4 |A|) on the un-fixed A     f/polyakov.f:244-247
-//   13     |A|^2 on the un-fixed A          f/scalarcorr.f:369-372
+//   12     cos(4 |A|) on the un-fixed A     f/polyakov.f:52-55
+//   13     |A|^2 on the un-fixed A          f/scalarcorr.f:48-51
 // correlators_kernel then forms the periodic z autocorrelations of
-// f/correlator.f:139-164, f/polyakov.f:292-305 and f/scalarcorr.f:417-430
+// f/correlator.f:139-164, f/polyakov.f:100-108 and f/scalarcorr.f:96-104
 // (all z = 0..L3-1, as the reference writes them) and the meas2a average.
 #include "lce_internal.hpp"
 

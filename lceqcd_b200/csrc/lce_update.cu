@@ -33,7 +33,7 @@
 namespace lce {
 
 // The reference evaluates cos(tpi*u) and sin(tpi*u) with tpi = 2 acos(-1)
-// (f/heat_kpi.f:250, f/gauss.f:185); M<R>::cos2pi / sincos2pi take u itself
+// (f/heat_kpi.f:29, f/gauss.f:17); M<R>::cos2pi / sincos2pi take u itself
 // (lce_common.cuh).
 
 __device__ __forceinline__ int find_chain(const int* blk_begin, int n, int b) {
@@ -87,7 +87,7 @@ __device__ __forceinline__ su2<R> ldU(const ChainDev& ch, int mu, int p, int s) 
   return NC ? LinkIO<R>::ld(ch.u, i) : LinkIO<R>::ld_cg(ch.u, i);
 }
 
-// f/staples.f:259-415: for each nu != mu (ascending),
+// f/staples.f:65-221: for each nu != mu (ascending),
 //   upper  = U_nu(x+mu) [U_mu(x+nu)^+ U_nu(x)^+]          (NN of DD)
 //   lower  = U_nu(x-nu+mu)^+ [U_mu(x-nu)^+ U_nu(x-nu)]    (DN of DN)
 //   V      = (V + upper) + lower
@@ -199,7 +199,7 @@ __device__ __forceinline__ void higgs_tile(const PassArgs& p, int tile) {
       const R beta_a = (R)ch.beta_a, beta_2 = (R)ch.beta_2, beta_4 = (R)ch.beta_4;
       R alph = (R)0, sf_o = (R)0, sf_n = (R)0;
       if constexpr (MODE == 0 || MODE == 1) {
-        // f/ahiggs2.f:169-194 width / cxval / alph
+        // f/ahiggs2.f:52-77 width / cxval / alph
         R rr, cxval;
         if (ch.imode == 1) {
           R conf2 = (R)0;
@@ -215,7 +215,7 @@ __device__ __forceinline__ void higgs_tile(const PassArgs& p, int tile) {
           cxval = (R)ch.cxval0;      // 1/beta_2/2
         }
         if constexpr (MODE == 0) {
-          // f/gauss.f:186-197: X = sqrt(-ln(W1)/R) cos(2 pi W2); f/ahiggs2.f:204-208
+          // f/gauss.f:17-29: X = sqrt(-ln(W1)/R) cos(2 pi W2); f/ahiggs2.f:83-91
 #pragma unroll
           for (int i = 0; i < 3; ++i) {
             const R w1 = -(R)1 * rr * M<R>::log(Un.v[2 * i]);
@@ -223,7 +223,7 @@ __device__ __forceinline__ void higgs_tile(const PassArgs& p, int tile) {
             an_[i] = g + beta_a * f[i] * cxval;
           }
         } else {
-          // f/ahiggs3.f:359-363
+          // f/ahiggs3.f:83-87
 #pragma unroll
           for (int i = 0; i < 3; ++i) an_[i] = -ao[i] + (R)2 * beta_a * f[i] * cxval;
         }
@@ -249,7 +249,7 @@ __device__ __forceinline__ void higgs_tile(const PassArgs& p, int tile) {
         boltz = M<R>::exp(-beta_a * (sf_o - sf_n) + beta_2 * (rho_o - rho_n) +
                           beta_4 * (rho_o * rho_o - rho_n * rho_n));
       } else {
-        // f/ahiggs2.f:225-226
+        // f/ahiggs2.f:108-109
         boltz = M<R>::exp(-alph * (rho_o - rho_n) + beta_4 * (rho_o * rho_o - rho_n * rho_n));
       }
       constexpr int acc_slot = MODE == 0 ? 6 : (MODE == 1 ? 0 : 3);
@@ -318,7 +318,7 @@ __device__ __forceinline__ void link_tile(const PassArgs& p, int tile) {
         if constexpr (!OR) {
           const R t1 = M<R>::div(tn, (R)ch.beta);
           const R t2 = (uo.a * vh.a - uo.b * cj(vh.b)).re;
-          // f/heat_kpi.f:254-319 single-trial Kennedy-Pendleton
+          // f/heat_kpi.f:33-98 single-trial Kennedy-Pendleton
           R a1 = Un.v[0], a2 = Un.v[1], a3 = Un.v[2];
           if (a1 == (R)0) a1 = (R)0.0000033;
           if (a2 == (R)0) a2 = (R)0.0000066;
@@ -418,7 +418,7 @@ __device__ __forceinline__ void finalize_combine(const FinalizeArgs& f) {
       if (kind <= kHiggsMetro) {
         for (int q = 0; q < kNQ; ++q) h[q] += t[q];
         if (end) {
-          // f/ahiggs2.f:259-264 (same in ahiggs1/3)
+          // f/ahiggs2.f:142-147 (same in ahiggs1/3)
           m.a2 = h[1] / V;
           m.a4 = h[2] / V;
           m.akin = h[3] / (6.0 * V);
@@ -453,7 +453,7 @@ __device__ __forceinline__ void finalize_combine(const FinalizeArgs& f) {
       } else if (kind == kLinkHB3) {
         for (int q = 0; q < kNQ; ++q) l[q] += t[q];
         if (end) {
-          // f/agauge1.f:226-231: the Metropolis count is divided by the 3 hits
+          // f/agauge1.f:227-232: the Metropolis count is divided by the 3 hits
           m.plaq = l[2] / (12.0 * V);
           m.acc_gauge = (l[0] / (3.0 * V)) * (l[1] / (12.0 * V) / 3.0);
           l[0] = l[1] = l[2] = l[3] = 0;
@@ -596,7 +596,7 @@ __global__ void __launch_bounds__(kBlock, kPersistMinBlocks) sweep_persistent_ke
 }
 
 // ------------------------------------------------------------------ renorm
-// f/renorm.f:223-233, in FP64 arithmetic for FP32 links
+// f/renorm.f:24-34, in FP64 arithmetic for FP32 links
 template <typename R>
 __global__ void renorm_kernel(void* u, size_t n) {
   for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x)

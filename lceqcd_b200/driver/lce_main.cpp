@@ -1,6 +1,6 @@
 // lce_main.cpp -- the reference driver f/main.f restated in C++ over the C ABI.
 //
-// Reads the same 20-line inputfile (f/paraminit.f:325-344), starts the lattice
+// Reads the same 20-line inputfile (f/paraminit.f:82-101), starts the lattice
 // as f/confget.f does (init 0..4), runs the thermalisation and the sweep loop
 // of f/main.f:20-83 on the GPU, and writes the reference's measurement files
 // with their names and formats (f/measinit.f, f/meas1.f, f/meas2a.f,
@@ -164,7 +164,7 @@ void append(const std::string& path, const std::string& text) {
   std::fclose(f);
 }
 
-// f/measinit.f:1001-1003 header
+// f/measinit.f:234-238 header
 std::string header(const Input& in) {
   char b[256];
   std::snprintf(b, sizeof b, "# %02d %02d %02d \n# %7.4f %7.4f %7.4f \n# %05d\n", in.n_lattice[0], in.n_lattice[1],
@@ -246,7 +246,7 @@ int main(int argc, char** argv) {
     check(ctx, lce_init_hot(ctx, seed), "init 0 (hot start)");
   } else if (in.init == 1 || in.init == 4) {
     std::vector<float> u((size_t)24 * nh), a((size_t)6 * nh);
-    if (in.init == 1) {  // onerandconf f/confget.f:158-275: one SU(2) matrix and one A everywhere
+    if (in.init == 1) {  // onerandconf f/confget.f:166-264: one SU(2) matrix and one A everywhere
       float x1 = 2.0f * unif(host_rng) - 1.0f, s1 = std::sqrt(1.0f - x1 * x1);
       float s2 = 2.0f * unif(host_rng) - 1.0f, x2 = s1 * s2, s3 = std::sqrt(1.0f - s2 * s2), s4 = s1 * s3;
       float s5 = twopi * unif(host_rng), x4 = s4 * std::cos(s5), x3 = s4 * std::sin(s5);
@@ -349,7 +349,7 @@ int main(int argc, char** argv) {
       }
       append(f_correl, t);
       append(f_checkp, t3);
-      // f/meas2a.f:206-226
+      // f/meas2a.f:77-99
       if (meas == nmeas) {
         const long itg = nmeas > 0 ? iter_or / nmeas : 0;
         append(f_joblog, std::string("number of iteration for or. gauge fixing : ") + fi(itg, 20, 1) + "\n" +

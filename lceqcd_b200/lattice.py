@@ -3,16 +3,16 @@
 `Lattice` exposes the subroutines f/main.f calls inside its sweep loop under
 their reference names and argument meanings:
 
-    ahiggs2(measflag) -> accept            f/ahiggs2.f:124
-    ahiggs3(measflag) -> accept            f/ahiggs3.f:283
+    ahiggs2(measflag) -> accept            f/ahiggs2.f:7
+    ahiggs3(measflag) -> accept            f/ahiggs3.f:7
     ahiggs1(delta, measflag) -> (accept, delta)   f/ahiggs1.f:7
     agauge(measflag) -> accept             f/agauge.f:7
-    renorm()                               f/renorm.f:205
-    landau_gauge() -> (da1, iter_or1)      f/landau_gauge.f:281
+    renorm()                               f/renorm.f:6
+    landau_gauge() -> (da1, iter_or1)      f/landau_gauge.f:6
     meas1() -> dict(plaq, akin, a2, a4)    f/meas1.f:7 (the reduced values)
-    meas2() -> af(3)                       f/meas2a.f:138
+    meas2() -> af(3)                       f/meas2a.f:9
     correlator() -> corr_a, corr_u, corr_3 f/correlator.f:11
-    polyakov(), scalarcorr()               f/polyakov.f:202, f/scalarcorr.f:331
+    polyakov(), scalarcorr()               f/polyakov.f:10, f/scalarcorr.f:10
 
 Errors raise LceError (the reference calls abort()).  Fields move in the
 reference's array order: u[mu, eo, site, 4] = (Re a, Im a, Re b, Im b) of the
@@ -82,7 +82,7 @@ class Params:
 
 
 def couplings(beta: float, x: float, y: float, precision: str = "f64"):
-    """beta_a, beta_2, beta_4 of f/paraminit.f:393-396."""
+    """beta_a, beta_2, beta_4 of f/paraminit.f:150-153."""
     p = Params(beta=beta, x=x, y=y, precision=precision).to_c()
     out = np.zeros(3)
     check(load().lce_couplings(C.byref(p), _ptr(out)))
@@ -594,7 +594,7 @@ INPUTFILE_KEYS = [
 
 
 def read_inputfile(path: str) -> dict:
-    """The 20-line positional inputfile of f/paraminit.f:325-344 (list-directed
+    """The 20-line positional inputfile of f/paraminit.f:82-101 (list-directed
     reads: the leading values of each line, the rest is a comment).  Raises
     ValueError where the reference would abort()."""
     with open(path) as f:

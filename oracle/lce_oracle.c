@@ -291,7 +291,7 @@ lco_ctx *lco_create(int L1, int L2, int L3, double beta, double x, double y,
   c->beta = (real)beta; c->x = (real)x; c->y = (real)y;
   c->lambda = (real)lambda; c->alpha = (real)alpha; c->limit_or = (real)limit_or;
   c->imode = imode;
-  /* f/paraminit.f:287-290 constants and :393-396 couplings, in the build's precision */
+  /* f/paraminit.f:44-47 constants and :150-153 couplings, in the build's precision */
   const real pi = (real)2.0 * (real)acos((real)0.0);
   const real sigma = (real)3.1759114;
   const real b = c->beta, xx = c->x, yy = c->y;
@@ -495,14 +495,14 @@ static int agauge_hits(lco_ctx *c, int measflag, int nhit, lco_real *accept_out)
         if (draw_pass(c, 7, LAY_TRIPLE)) return -1;
 #pragma omp parallel for num_threads(c->nthreads) schedule(static) reduction(+ : pass_kp, pass_acc)
         for (int s = 0; s < nh; ++s) {
-          /* 2) normalise the staple (f/agauge.f:71-84, f/agauge1.f:72-85) */
+          /* 2) normalise the staple (f/agauge.f:71-84, f/agauge1.f:80-91) */
           const real *vp = c->v + UIDX(c, mu, eo, s);
           su2 vv = ld_su2(vp);
           real t1 = vv.a.re * vv.a.re + vv.a.im * vv.a.im + vv.b.re * vv.b.re + vv.b.im * vv.b.im;
           t1 = (real)1.0 / (real)sqrt(t1);
           su2 vh = {{t1 * vv.a.re, t1 * vv.a.im}, {t1 * vv.b.re, t1 * vv.b.im}};
           t1 = t1 / c->beta;
-          /* the current link: updated by an earlier hit (f/agauge1.f:100-103) */
+          /* the current link: updated by an earlier hit (f/agauge1.f:101-108) */
           su2 uo = ld_su2(c->u + UIDX(c, mu, eo, s));
           real t2 = csub(cmul(uo.a, vh.a), cmul(uo.b, cconj(vh.b))).re;
           /* 3) heat_kpi (f/heat_kpi.f:33-98) */
@@ -545,7 +545,7 @@ static int agauge_hits(lco_ctx *c, int measflag, int nhit, lco_real *accept_out)
           }
         }
       }
-      /* plaquette against the staple, after the hits (f/agauge.f:179-185, f/agauge1.f:207-214) */
+      /* plaquette against the staple, after the hits (f/agauge.f:179-185, f/agauge1.f:205-211) */
       if (measflag == 1) {
 #pragma omp parallel for num_threads(c->nthreads) schedule(static) reduction(+ : pass_plaq)
         for (int s = 0; s < nh; ++s)
@@ -558,7 +558,7 @@ static int agauge_hits(lco_ctx *c, int measflag, int nhit, lco_real *accept_out)
   }
   double accept = kp_acc;
   if (measflag == 1) {
-    /* f/agauge.f:195-200; f/agauge1.f:226-231 divides acc1 by nhit too */
+    /* f/agauge.f:195-200; f/agauge1.f:227-232 divides acc1 by nhit too */
     c->plaq0 = plaq / (12.0 * c->vol);
     accept = accept / (3.0 * c->vol);
     acc1 = acc1 / (12.0 * c->vol) / nhit;
@@ -699,7 +699,7 @@ static void higgs_finish(lco_ctx *c, int eo, real *an_all, int acc_slot, int lay
   *acc += lacc; *s2 += l2; *s4 += l4; *skin += lk;
 }
 
-/* f/ahiggs2.f:124-267 heatbath; gauss per f/gauss.f:10-31 */
+/* f/ahiggs2.f:7-152 heatbath; gauss per f/gauss.f:10-31 */
 int lco_ahiggs2(lco_ctx *c, int measflag, lco_real *accept) {
   const int nh = c->nh;
   const real tpi = (real)2.0 * (real)acos((real)-1.);
@@ -735,7 +735,7 @@ int lco_ahiggs2(lco_ctx *c, int measflag, lco_real *accept) {
   return 0;
 }
 
-/* f/ahiggs3.f:283-424 overrelaxation */
+/* f/ahiggs3.f:7-148 overrelaxation */
 int lco_ahiggs3(lco_ctx *c, int measflag, lco_real *accept) {
   const int nh = c->nh;
   double acc = 0, s2 = 0, s4 = 0, sk = 0;
@@ -816,7 +816,7 @@ int lco_ahiggs1(lco_ctx *c, lco_real *delta, int measflag, lco_real *accept) {
   return 0;
 }
 
-/* f/renorm.f:223-233 */
+/* f/renorm.f:24-34 */
 void lco_renorm(lco_ctx *c) {
   const size_t n = (size_t)3 * 2 * c->nh;
 #pragma omp parallel for num_threads(c->nthreads) schedule(static)
@@ -847,7 +847,7 @@ void lco_landau_copy(lco_ctx *c) {
   memcpy(c->af, c->a, (size_t)2 * c->nh * 3 * sizeof(real));
 }
 
-/* f/u_f_renorm.f:261-271 */
+/* f/u_f_renorm.f:24-34 */
 void lco_u_f_renorm(lco_ctx *c) {
   const size_t n = (size_t)3 * 2 * c->nh;
 #pragma omp parallel for num_threads(c->nthreads) schedule(static)
@@ -961,7 +961,7 @@ double lco_or_gauge_fixing(lco_ctx *c) {
   return da1;
 }
 
-/* f/it_gauge_fixing.f:5-214, one iteration of the reference's iterative
+/* f/it_gauge_fixing.f:5-206, one iteration of the reference's iterative
  * (steepest-descent) gauge fixing, parity by parity (the transform of a
  * parity is applied before the next parity's g is formed, :94-99):
  *   g1 = sum_mu (i Im a, b) of U_f(x,mu), g2 the same of U_f(x-mu,mu)
@@ -1032,7 +1032,7 @@ double lco_it_gauge_fixing(lco_ctx *c, double step, int flags) {
   return da1;
 }
 
-/* f/landau_gauge.f:303-334 with it_gauge_fixing in place of
+/* f/landau_gauge.f:28-59 with it_gauge_fixing in place of
  * or_gauge_fixing: copy, then iterate + u_f_renorm while da1 > limit_or */
 int lco_it_landau_gauge(lco_ctx *c, double step, int flags, int max_iters, double *da1_out) {
   double da1 = 10000.0;
@@ -1048,7 +1048,7 @@ int lco_it_landau_gauge(lco_ctx *c, double step, int flags, int max_iters, doubl
   return it;
 }
 
-/* f/landau_gauge.f:303-334; max_iters <= 0 means no cap (as the reference) */
+/* f/landau_gauge.f:28-59; max_iters <= 0 means no cap (as the reference) */
 int lco_landau_gauge(lco_ctx *c, int max_iters, double *da1_out) {
   double da1 = 10000.0;
   int it = 0;
@@ -1139,7 +1139,7 @@ void lco_correlator(const lco_ctx *c, double *corr_a, double *corr_u, double *co
   free(as); free(us);
 }
 
-/* f/polyakov.f:239-305 on the un-fixed A */
+/* f/polyakov.f:47-108 on the un-fixed A */
 void lco_polyakov(const lco_ctx *c, double *slice, double *corr, double *mean2) {
   const int L3 = c->L[2], nxy = c->nxy;
   for (int z = 0; z < L3; ++z) slice[z] = 0;
@@ -1159,7 +1159,7 @@ void lco_polyakov(const lco_ctx *c, double *slice, double *corr, double *mean2) 
   *mean2 = (tot / L3) * (tot / L3);
 }
 
-/* f/scalarcorr.f:364-430 */
+/* f/scalarcorr.f:43-104 */
 void lco_scalarcorr(const lco_ctx *c, double *slice, double *corr, double *mean) {
   const int L3 = c->L[2], nxy = c->nxy;
   for (int z = 0; z < L3; ++z) slice[z] = 0;
@@ -1179,7 +1179,7 @@ void lco_scalarcorr(const lco_ctx *c, double *slice, double *corr, double *mean)
   *mean = tot / L3;
 }
 
-/* f/meas2a.f:168-178 */
+/* f/meas2a.f:39-49 */
 void lco_meas2(const lco_ctx *c, double af[3]) {
   af[0] = af[1] = af[2] = 0;
   for (int eo = 0; eo < 2; ++eo)

@@ -21,7 +21,7 @@
  *   gauge fixing     f/landau_gauge.f, f/or_gauge_fixing1.f, f/it_gauge_fixing.f
  *   measurements     f/correlator.f, f/polyakov.f, f/scalarcorr.f,
  *                    f/meas1.f, f/meas2a.f
- *   RANLUX           f/luxury.f (pinned to the expected output in f/luxtst.f:392-466)
+ *   RANLUX           f/luxury.f (pinned to the expected output in f/luxtst.f:88-162)
  *   configurations   f/confget.f unitconf/randomconf/testconf
  *
  * Parity status: RANLUX is pinned to the reference's own known-answer block.

@@ -194,7 +194,7 @@ class Oracle:
             self.lib.lco_destroy(self.h)
             self.h = None
 
-    # --- couplings f/paraminit.f:393-396
+    # --- couplings f/paraminit.f:150-153
     def couplings(self):
         out = np.zeros(3, np.float64)
         self.lib.lco_couplings(self.h, _ptr(out))

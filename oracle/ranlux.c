@@ -7,7 +7,7 @@
  * it as a host-side uniform stream for validation mode.
  *
  * Arithmetic is single precision, as in the Fortran (default REAL), so the
- * outputs reproduce the expected values pinned in f/luxtst.f:392-466.
+ * outputs reproduce the expected values pinned in f/luxtst.f:88-162.
  * State lives in file-scope statics, mirroring the /LUX1/ and /LUX2/ COMMON
  * blocks of f/luxury.h.
  */

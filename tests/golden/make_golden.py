@@ -1,11 +1,11 @@
 """Generate tests/golden/ranlux_luxtst.json from the reference's own
 known-answer block for RANLUX: the expected output of the luxtst program,
-written as comments at f/luxtst.f:392-466 of derek-teaney/lceqcd.
+written as comments at f/luxtst.f:88-162 of derek-teaney/lceqcd.
 
 Run in a checkout where the reference is available:
     python tests/golden/make_golden.py /path/to/lceqcd
 
-The JSON records, for each case of the luxtst program (f/luxtst.f:314-371),
+The JSON records, for each case of the luxtst program (f/luxtst.f:10-66),
 the call sequence and the printed numbers 1-5 and 101-105 (8 decimals), and
 the 25-integer restart vector.  These are the only golden vectors the
 reference repository holds.
@@ -49,14 +49,16 @@ def parse(path: str) -> dict:
         {"setup": "rluxin(restart)", "first": nums[10], "second": nums[11]},
     ]
     return {
-        "source": "f/luxtst.f:392-466 (expected output of the luxtst program)",
+        "source": "f/luxtst.f:88-162 (expected output of the luxtst program)",
         "cases": cases,
         "restart": restart[:25],
     }
 
 
 def main() -> None:
-    ref = sys.argv[1] if len(sys.argv) > 1 else "/root/reference"
+    if len(sys.argv) != 2:
+        sys.exit("usage: python tests/golden/make_golden.py <path to the lceqcd checkout>")
+    ref = sys.argv[1]
     data = parse(os.path.join(ref, "f", "luxtst.f"))
     out = os.path.join(os.path.dirname(os.path.abspath(__file__)), "ranlux_luxtst.json")
     with open(out, "w") as f:

@@ -1,6 +1,6 @@
 """Host-side checks of the C ABI that need no GPU: every symbol declared in
 include/lceqcd_gpu.h is exported by liblceqcd_gpu.so, the coupling
-derivation (f/paraminit.f:393-396) and the neighbour arithmetic
+derivation (f/paraminit.f:150-153) and the neighbour arithmetic
 (f/adresses.f:91-337) agree bit for bit with the oracle, and the inputfile
 reader handles the reference's 20-line format."""
 import ctypes as C

@@ -1,5 +1,5 @@
 """The oracle's RANLUX restatement against the reference's only golden
-vectors: the expected output of the luxtst program (f/luxtst.f:392-466),
+vectors: the expected output of the luxtst program (f/luxtst.f:88-162),
 captured in tests/golden/ranlux_luxtst.json by tests/golden/make_golden.py."""
 import json
 import os
