@@ -36,6 +36,16 @@ UNIT = "site-updates/s"
 # algorithmic HBM bytes per lattice site (FP32 fields): one link pass
 # (eo, mu) moves 68 B*V, one Higgs pass 66 B*V, the sweep 672 B*V.
 B_LINK, B_HIGGS, B_SWEEP = 68, 66, 672
+
+
+def workload_config(L):
+    """The config both arms print (identical dicts, so the two lines name one
+    workload): the 64^3 mixed-precision single chain."""
+    return {"workload": "single chain 64^3, beta=12, x=0.09, y=0.3, hot start; FP32 fields, FP64 "
+                        "reunitarisation and sums; sweep = ahiggs2+ahiggs3+agauge (+renorm), the reference's "
+                        "composition",
+            "L": list(L), "sites": vol(L),
+            "l2": "GPU arm: 256 MB L2 flush between timed steps; CPU arm: no flush (fields 16 MB, host caches)"}
 # forward FLOPs per site of the warm-start network: 4 layers of 27 offsets x
 # 16 x 16 multiply-adds
 NET_FWD_FLOP_PER_SITE = 4 * 27 * 16 * 16 * 2
@@ -221,6 +231,19 @@ def timed_sweeps(lat, K, flush=True):
     return tot
 
 
+def settle(lat, measflag=1, limit=60):
+    """Untimed sweeps until the library's autotuner has chosen a sweep form
+    and tile shape (4 timed sweeps per candidate), so that no timed region
+    contains tuning sweeps."""
+    n = 0
+    while lat.sweep_mode() == "auto" and n < limit:
+        lat.sweeps(4, measflag)
+        lat.synchronize()
+        n += 4
+    if lat.sweep_mode() == "auto":
+        raise RuntimeError(f"the sweep autotuner has not decided after {n} sweeps")
+
+
 def kernel_profile(lat, reps=10):
     """Per-pass durations (events between kernels) of the sweep, averaged."""
     acc = None
@@ -267,7 +290,7 @@ def extras(args, peak):
         try:
             lat = Lattice(L, **COUP, precision="f32", seed=11, n_link_or=nor)
             lat.init_hot(12)
-            lat.sweeps(3, 0)
+            settle(lat)
             timed_sweeps(lat, 3)
             K = 20 if L[0] <= 128 else 10
             ms = timed_sweeps(lat, K)
@@ -276,6 +299,7 @@ def extras(args, peak):
             sps = vol(L) * K / (ms / 1e3)
             bs = B_SWEEP + 6 * nor * B_LINK  # algorithmic bytes per site of this composition
             out[key] = {"site_updates_per_s": sps, "ms_per_sweep": ms / K, "sweep_mode": lat.sweep_mode(),
+                        "tile_shape": list(lat.tile_shape()),
                         "passes": 10 + 6 * nor, "bytes_per_site": bs,
                         "sweep_hbm_gbs": sps * bs / 1e9, "sweep_frac_of_measured_hbm": sps * bs / 1e9 / peak,
                         "link_kernel_ms": link,
@@ -435,11 +459,12 @@ def extras(args, peak):
         sites = sum(vol(s.L) for s in specs)
         ens = Ensemble(specs)
         ens.init_hot(5)
-        ens.sweeps(10, 0)   # includes the library's choice of sweep form
+        settle(ens)   # the library's choice of sweep form and tile shape
         timed_sweeps(ens, 3)
         K = 20
         ms_b = timed_sweeps(ens, K)
         ens_mode = ens.sweep_mode()
+        ens_tile = list(ens.tile_shape())
         ens.close()
         # the plain path: each chain alone in its own context, one kernel per pass
         plain = {}
@@ -458,7 +483,8 @@ def extras(args, peak):
         out["batched_96_chains"] = {"site_updates_per_s": bat, "plain_f64_site_updates_per_s": plain["f64"],
                                     "plain_f32_site_updates_per_s": plain["f32"],
                                     "speedup_vs_plain_f64": bat / plain["f64"], "speedup_vs_plain_f32": bat / plain["f32"],
-                                    "sites": sites, "sweep_mode": ens_mode}
+                                    "sites": sites, "sweep_mode": ens_mode,
+                                    "tile_shape": ens_tile}
     except Exception as e:
         out["batched_96_chains"] = {"error": repr(e)[:300]}
     return out
@@ -472,9 +498,11 @@ def run_gpu(args):
     L = (args.lattice,) * 3 if args.lattice else L_MAIN
     V = vol(L)
     lat = Lattice(L, **COUP, precision="f32", seed=1000 + rank, device=local, sweep_mode=args.sweep_mode,
-                  n_link_or=args.link_or)
+                  n_link_or=args.link_or, tile_threads=args.tile_threads)
     lat.init_hot(2000 + rank)
-    lat.sweeps(20, 0)
+    # untimed: the library's autotuner times its candidates (sweep forms x tile
+    # shapes, 4 sweeps each) on the first sweeps and keeps the fastest
+    settle(lat)
     timed_sweeps(lat, args.warmup)
     lat.synchronize()
     barrier(world)
@@ -499,6 +527,7 @@ def run_gpu(args):
     ms_max = max_over_ranks(ms, world)
     value = world * V * args.steps / (ms_max / 1e3)
     mode = lat.sweep_mode()  # chosen by the library's autotuner during the untimed sweeps
+    tile_bs, tile_spt = lat.tile_shape()
     # per step: the sweep (one persistent kernel, or 10 pass kernels + finalize)
     # and the two L2-flush kernels
     launches = args.steps * ((1 if mode == "persistent" else 11) + 2)
@@ -508,6 +537,7 @@ def run_gpu(args):
             sweep_bytes = B_HIGGS * 4 + B_LINK * 6 * (1 + args.link_or)
             print(json.dumps({"metric": METRIC, "value": value, "unit": UNIT, "L": list(L), "steps": args.steps,
                               "ms_per_step": ms_max / args.steps, "sweep_mode": mode, "quick": True,
+                              "tile_shape": [tile_bs, tile_spt],
                               "link_or": args.link_or, "passes": passes, "bytes_per_site": sweep_bytes,
                               "frac_of_measured_hbm": value * sweep_bytes / 1e9 / peak}), flush=True)
         lat.close()
@@ -572,18 +602,18 @@ def run_gpu(args):
         "warmup": args.warmup, "ms_per_step": ms_max / args.steps, "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "f32",
         "data": "synthetic (hot start: Haar links, A0 ~ N(0,1))",
-        "config": {"workload": "single chain 64^3, beta=12, x=0.09, y=0.3, hot start; FP32 fields, FP64 "
-                               "reunitarisation and sums; sweep = ahiggs2+ahiggs3+agauge (+fused renorm), "
-                               "measurements every sweep",
-                   "L": list(L), "sites": V, "l2": "flushed between timed steps (256 MB write)",
-                   "parallelism": f"replicas x{world}" if world > 1 else "single GPU",
-                   "wall_s_timed_region": wall},
+        "config": workload_config(L),
+        "parallelism": f"replicas x{world}" if world > 1 else "single GPU",
+        "wall_s_timed_region": wall,
         "e2e": {"value": e2e_val, "unit": UNIT, "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
                 "note": "per step: lce_upload(pinned host fields) + lce_sweep(measflag=1, measurements read back)",
                 "with_field_download": {"value": world * V * Ke / (rt_ms / 1e3), "d2h_bytes_per_step": d2h + h2d}},
         "gpu_launches": launches,
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
                      "traffic": traffic, "kernel": dom_name, "sweep_mode": mode,
+                     "tile_shape": {"threads_per_block": tile_bs, "sites_per_thread": tile_spt,
+                                    "chosen_by": "the library's autotuner" if args.sweep_mode == "auto"
+                                    else f"--sweep-mode {args.sweep_mode}"},
                      "algorithmic_bytes_per_launch": dom_bytes, "avg_launch_ms": dom_ms,
                      "peak_source": f"{peak_src} (MEASURED_PEAKS.json hbm_gbs)" if peak_src == "measured" else "fallback",
                      "pass_kernels": {"link_kernel_ms": link_ms, "link_kernel_frac": B_LINK * V / (link_ms / 1e3) / 1e9 / peak,
@@ -643,8 +673,7 @@ def run_reference(args):
     line = {"metric": METRIC, "value": v, "unit": UNIT, "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
             "ms_per_step": el / K * 1e3, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
             "dtype": "f32", "data": "synthetic (hot start)", "impl": "reference",
-            "config": {"workload": "single chain 64^3, beta=12, x=0.09, y=0.3, hot start; FP32; reference sweep "
-                                   "composition", "L": list(L_MAIN), "sites": vol(L_MAIN)},
+            "config": workload_config(L_MAIN),
             "cpu_baseline": {"value": v, "unit": UNIT, "cores": threads, "kind": "port",
                              "sample": f"{K} of {args.steps} steps timed (bounded to ~{budget:.0f} s), each a full "
                                        "64^3 sweep of the FP32 oracle restatement (the Fortran reference has no "
@@ -690,6 +719,9 @@ def main():
     ap.add_argument("--lattice", type=int, default=0, help="cubic extent for --quick runs (default 64)")
     ap.add_argument("--sweep-mode", default="auto", choices=["auto", "passes", "passes2", "persistent"],
                     help="sweep form (default: the library's autotuner chooses)")
+    ap.add_argument("--tile-threads", type=int, default=0, choices=[0, 128, 256, 512],
+                    help="threads per block of the update kernels (default 0: the autotuner chooses with "
+                         "--sweep-mode auto, else 256)")
     ap.add_argument("--link-or", type=int, default=0, metavar="N",
                     help="--quick runs: N link overrelaxation hits per sweep after the heatbath")
     ap.add_argument("--quick-gauge-fix", type=int, default=0, metavar="ITERS",

@@ -67,10 +67,12 @@ extern "C" {
 #define LCE_GF_ATAN2 1
 
 /* execution form of lce_sweep(s): one kernel per parity pass chained in a
- * CUDA graph (one site per thread, or two sites per thread: tiles of 512
- * sites), or one cooperative persistent kernel per sweep that loops over the
- * (chain, tile) work list of every pass with a grid barrier in between.
- * AUTO times the forms on the first sweeps and keeps the fastest. */
+ * CUDA graph (one site per thread, or two sites per thread), or one
+ * cooperative persistent kernel per sweep that loops over the (chain, tile)
+ * work list of every pass with a grid barrier in between.  AUTO times the
+ * forms -- and, for FP32 contexts, the tile shapes of the per-pass forms
+ * (128, 256 or 512 threads per block, see lce_params.tile_threads) -- on the
+ * first sweeps and keeps the fastest (lce_get_sweep_mode, lce_get_tile_shape). */
 #define LCE_SWEEP_AUTO 0
 #define LCE_SWEEP_PASSES 1
 #define LCE_SWEEP_PERSISTENT 2
@@ -107,6 +109,12 @@ typedef struct lce_params {
                             0 is read as 1), 3 = f/agauge1.f (three heatbath +
                             Metropolis hits per link) -- the reference selects
                             one of the two files at build time */
+  int tile_threads;      /* threads per block of the per-pass update kernels:
+                            0 (default) = tuned with LCE_SWEEP_AUTO, else 256;
+                            or 128, 256, 512.  FP32 only: the FP64 validation
+                            path and z-slabs use 256.  Results do not depend on
+                            it (per-site work and random numbers are the same;
+                            FP64 sums are grouped per tile). */
 } lce_params;
 
 /* Measured quantities: /aver_loc/ (plaq0, a0kin, a02, a04, a0f) and the
@@ -193,7 +201,7 @@ int lce_ahiggs3(lce_ctx* ctx, int measflag, float* accept);
 int lce_agauge(lce_ctx* ctx, int measflag, float* accept);
 /* f/agauge1.f:7-237: the 3-hit link update (staple once per (parity, mu),
  * then three heatbath + Metropolis hits of 7 uniforms per site each; the
- * acceptance divides the Metropolis count by the hits, :226-231) */
+ * acceptance divides the Metropolis count by the hits, :227-232) */
 int lce_agauge1(lce_ctx* ctx, int measflag, float* accept);
 /* link overrelaxation with the agauge Metropolis test (no reference counterpart) */
 int lce_link_or(lce_ctx* ctx, int measflag, float* accept);
@@ -204,11 +212,14 @@ int lce_renorm(lce_ctx* ctx);
  * CUDA graph per measflag.  m (chain 0) may be NULL: no synchronisation. */
 int lce_sweep(lce_ctx* ctx, int measflag, lce_meas* m);
 /* nsweeps graph replays without synchronisation (with LCE_SWEEP_AUTO the first
- * sweeps of a context alternate the two forms under CUDA events -- every one
- * of them a real sweep -- and the faster form is kept) */
+ * sweeps of a context rotate through the forms and tile shapes under CUDA
+ * events -- every one of them a real sweep -- and the fastest is kept) */
 int lce_sweeps(lce_ctx* ctx, int nsweeps, int measflag);
 /* the form lce_sweeps uses now (LCE_SWEEP_AUTO while still undecided) */
 int lce_get_sweep_mode(lce_ctx* ctx);
+/* the tile shape of the update kernels in use: threads per block and sites
+ * per thread (a tuned choice once lce_get_sweep_mode is no longer AUTO) */
+int lce_get_tile_shape(lce_ctx* ctx, int* threads, int* sites_per_thread);
 /* f/meas1.f inputs: the last measured quantities of a chain */
 int lce_get_meas(lce_ctx* ctx, int chain, lce_meas* m);
 int lce_get_meas_batch(lce_ctx* ctx, lce_meas* m /* [nchains] */);
@@ -381,8 +392,10 @@ int lce_slabs_scalarcorr(lce_slabs* s, double* slice, double* corr, double* mean
  * array held by every GPU that loads the library; lattices larger than
  * 16,777,216 sites (256^3) are rejected with LCE_ERR_INVALID.  The first call
  * on a device looks up the array's address (make it before any stream
- * capture).  All calls share the array: calls whose kernels overlap on the GPU
- * race and must be serialised by the caller. */
+ * capture) and keeps it for the life of the process: do not call it across a
+ * cudaDeviceReset, which reloads the module elsewhere.  All calls share the
+ * array: calls whose kernels overlap on the GPU race and must be serialised
+ * by the caller. */
 int lce_plaquette_noalloc(const float* u, long ld, int L1, int L2, int L3, double* plaq, void* stream);
 
 /* ---- learned warm start for Landau gauge fixing (no reference counterpart;

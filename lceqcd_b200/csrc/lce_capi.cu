@@ -15,6 +15,7 @@
 #include <cstdio>
 #include <cstring>
 #include <map>
+#include <tuple>
 #include <string>
 #include <vector>
 
@@ -36,6 +37,13 @@ struct Pass {
 
 void lce::set_thread_error(const std::string& msg) { g_create_error = msg; }
 
+// one autotune candidate: a sweep form and, for the per-pass forms, the tile
+// shape (threads per block, sites per thread), with its timed samples
+struct TuneForm {
+  int form, bs, spt;
+  std::vector<float> ms;
+};
+
 struct lce_ctx {
   int device = 0;
   int prec = LCE_PREC_F32;
@@ -47,12 +55,15 @@ struct lce_ctx {
   int agauge_hits = 1;  // 1: f/agauge.f, 3: f/agauge1.f in lce_sweep
   std::vector<lce_params> params;
   std::vector<ChainDev> ch;
-  std::vector<int> blk;   // prefix of blocks per pass (tiles of kBlock sites)
-  std::vector<int> blk2;  // the same for tiles of 2 * kBlock sites (two per thread)
+  // prefix over chains of the tiles of one pass, for tiles of 128, 256 and
+  // 512 sites (tile = threads per block x sites per thread); tiles of kBlock
+  // sites (blk) serve the persistent form and size the partial-sum slots
+  std::vector<int> tiles[3];
+  std::vector<int>& blk = tiles[1];
   int max_nh = 0, max_L3 = 0;
   ChainDev* ch_d = nullptr;
-  int* blk_d = nullptr;
-  int* blk2_d = nullptr;
+  int* tiles_d[3] = {nullptr, nullptr, nullptr};
+  int* blk_d = nullptr;   // = tiles_d[1]
   CtxState* st_d = nullptr;
   ChainState* cst_d = nullptr;
   lce_meas* meas_d = nullptr;
@@ -75,14 +86,15 @@ struct lce_ctx {
   std::map<std::pair<int, int>, cudaGraphExec_t> fa_exec;
   cudaStream_t own = nullptr, stream = nullptr;
   cudaEvent_t ev0 = nullptr, ev1 = nullptr;
-  cudaGraphExec_t sweep_exec[2] = {nullptr, nullptr};     // per-pass kernels, per measflag
-  cudaGraphExec_t sweep2_exec[2] = {nullptr, nullptr};    // per-pass kernels, two sites per thread
-  cudaGraphExec_t persist_exec[2] = {nullptr, nullptr};   // persistent kernel, per measflag
+  // instantiated sweep graphs by (form, threads per block, sites per thread, measflag)
+  std::map<std::tuple<int, int, int, int>, cudaGraphExec_t> sweep_graphs;
   GridBar* bar_d = nullptr;
   int persist_grid = 0;
   int sweep_mode = LCE_SWEEP_AUTO;   // requested
   int mode = LCE_SWEEP_AUTO;         // in use (AUTO while tuning)
-  std::vector<float> tune_ms[3];     // autotune samples: passes, persistent, passes x2
+  int tile_req = 0;                  // requested threads per block (0: tuned under AUTO, else 256)
+  int tile_bs = kBlock, tile_spt = 1;  // tile shape of the per-pass kernels in use
+  std::vector<TuneForm> tune;        // autotune candidates and their samples
   std::map<std::pair<int, int>, cudaGraphExec_t> gf_exec;
   std::string err;
 };
@@ -156,6 +168,10 @@ bool valid_params(const lce_params& p, std::string& why) {
     why = "sweep_mode must be LCE_SWEEP_AUTO, LCE_SWEEP_PASSES, LCE_SWEEP_PASSES2 or LCE_SWEEP_PERSISTENT";
     return false;
   }
+  if (p.tile_threads != 0 && p.tile_threads != 128 && p.tile_threads != 256 && p.tile_threads != 512) {
+    why = "tile_threads must be 0 (tuned), 128, 256 or 512";
+    return false;
+  }
   if (p.gf_angle != LCE_GF_ACOS && p.gf_angle != LCE_GF_ATAN2) {
     why = "gf_angle must be LCE_GF_ACOS or LCE_GF_ATAN2";
     return false;
@@ -226,7 +242,7 @@ struct Enq {
   FinalizeArgs f;
   const std::vector<int>* blk = nullptr;
   int* blk_d = nullptr;
-  int spt = 1;
+  int spt = 1, bs = kBlock;
   int measflag = 0;
   bool fuse = false;
   unsigned long long soff = 0;
@@ -234,11 +250,16 @@ struct Enq {
   int slot = 0;
 };
 
-void enq_begin(lce_ctx* c, const std::vector<unsigned char>& routines, int measflag, bool fuse_renorm, int spt,
-               Enq& q) {
-  q.blk = spt == 2 ? &c->blk2 : &c->blk;
-  q.blk_d = spt == 2 ? c->blk2_d : c->blk_d;
+// index of the chain table for tiles of bs * spt sites (128, 256 or 512)
+int tile_index(int bs, int spt) { return bs * spt == 128 ? 0 : (bs * spt == 256 ? 1 : 2); }
+
+void enq_begin(lce_ctx* c, const std::vector<unsigned char>& routines, int measflag, bool fuse_renorm, int bs,
+               int spt, Enq& q) {
+  const int ti = tile_index(bs, spt);
+  q.blk = &c->tiles[ti];
+  q.blk_d = c->tiles_d[ti];
   q.spt = spt;
+  q.bs = bs;
   q.measflag = measflag;
   q.fuse = fuse_renorm;
   q.passes.clear();
@@ -269,6 +290,7 @@ int enq_pass(lce_ctx* c, Enq& q, size_t i) {
   a.chains = c->ch_d;
   a.blk_begin = q.blk_d;
   a.spt = q.spt;
+  a.bs = q.bs;
   a.st = c->st_d;
   a.cst = c->cst_d;
   a.part = reduce ? c->part_d + (size_t)q.slot * c->slot_stride : nullptr;
@@ -307,10 +329,11 @@ int enq_end(lce_ctx* c, Enq& q) {
   return LCE_OK;
 }
 
+// bs, spt: the tile shape (0: the context's shape in use)
 int enqueue(lce_ctx* c, const std::vector<unsigned char>& routines, int measflag, bool fuse_renorm,
-            cudaEvent_t* events = nullptr, int spt = 1) {
+            cudaEvent_t* events = nullptr, int bs = 0, int spt = 0) {
   Enq q;
-  enq_begin(c, routines, measflag, fuse_renorm, spt, q);
+  enq_begin(c, routines, measflag, fuse_renorm, bs ? bs : c->tile_bs, spt ? spt : c->tile_spt, q);
   for (size_t i = 0; i < q.passes.size(); ++i) {
     if (int rc = enq_pass(c, q, i)) return rc;
     if (events) CK(cudaEventRecord(events[i], c->stream));
@@ -339,6 +362,7 @@ int enqueue_persistent(lce_ctx* c, const std::vector<unsigned char>& routines, i
   b.nchains = c->nchains;
   b.fuse_renorm = fuse_renorm ? 1 : 0;
   b.spt = 1;
+  b.bs = kBlock;
   b.s_lo = c->s_lo;
   b.site_off = c->site_off;
   FinalizeArgs& f = a.fin;
@@ -386,9 +410,9 @@ constexpr size_t kTuneSamples = 3;
 // The instantiated graph of one sweep in the given form (built once per
 // form and measflag).  The persistent form falls back to the per-pass form
 // under LCE_SWEEP_AUTO if it cannot be captured on this device.
-int sweep_graph(lce_ctx* c, int form, int mf, cudaGraphExec_t* out) {
-  cudaGraphExec_t* slot = form == LCE_SWEEP_PERSISTENT ? &c->persist_exec[mf]
-                          : (form == LCE_SWEEP_PASSES2 ? &c->sweep2_exec[mf] : &c->sweep_exec[mf]);
+int sweep_graph(lce_ctx* c, int form, int bs, int spt, int mf, cudaGraphExec_t* out) {
+  if (form == LCE_SWEEP_PERSISTENT) bs = kBlock, spt = 1;
+  cudaGraphExec_t* slot = &c->sweep_graphs[std::make_tuple(form, bs, spt, mf)];
   if (!*slot) {
     cudaGraph_t g;
     CK(cudaStreamBeginCapture(c->stream, cudaStreamCaptureModeThreadLocal));
@@ -397,7 +421,7 @@ int sweep_graph(lce_ctx* c, int form, int mf, cudaGraphExec_t* out) {
       rc = c->prec == LCE_PREC_F64 ? enqueue_persistent<double>(c, sweep_routines(c), mf, true)
                                    : enqueue_persistent<float>(c, sweep_routines(c), mf, true);
     else
-      rc = enqueue(c, sweep_routines(c), mf, true, nullptr, form == LCE_SWEEP_PASSES2 ? 2 : 1);
+      rc = enqueue(c, sweep_routines(c), mf, true, nullptr, bs, spt);
     const cudaError_t ec = cudaStreamEndCapture(c->stream, &g);
     cudaError_t ei = cudaSuccess;
     if (ec == cudaSuccess) {
@@ -412,7 +436,8 @@ int sweep_graph(lce_ctx* c, int form, int mf, cudaGraphExec_t* out) {
       if (form == LCE_SWEEP_PERSISTENT && c->sweep_mode == LCE_SWEEP_AUTO) {
         c->err = std::string("persistent sweep unavailable: ") + cudaGetErrorString(e);
         c->mode = LCE_SWEEP_PASSES;
-        return sweep_graph(c, LCE_SWEEP_PASSES, mf, out);
+        c->tune.clear();
+        return sweep_graph(c, LCE_SWEEP_PASSES, c->tile_bs, c->tile_spt, mf, out);
       }
       return cuda_fail(c, e, "sweep graph capture");
     }
@@ -593,8 +618,7 @@ lce_ctx* create_impl(const lce_params* p, int n, const SlabInfo* slab = nullptr)
   const size_t lb = link_bytes(c->prec), rb = real_bytes(c->prec);
   size_t off = 0;
   std::vector<size_t> offs;
-  c->blk.assign(1, 0);
-  c->blk2.assign(1, 0);
+  for (auto& t : c->tiles) t.assign(1, 0);
   for (int i = 0; i < n; ++i) {
     ChainDev d;
     std::memset(&d, 0, sizeof(d));
@@ -638,8 +662,7 @@ lce_ctx* create_impl(const lce_params* p, int n, const SlabInfo* slab = nullptr)
     off += 2 * (align256((size_t)6 * d.nh * lb) + align256((size_t)6 * d.nh * rb)) + align256((size_t)2 * d.nh * lb);
     c->ch.push_back(d);
     const int nvis = slab ? d.nh - 2 * d.nxy : d.nh;  // sites a pass visits per parity
-    c->blk.push_back(c->blk.back() + ceil_div(nvis, kBlock));
-    c->blk2.push_back(c->blk2.back() + ceil_div(nvis, 2 * kBlock));
+    for (int t = 0; t < 3; ++t) c->tiles[t].push_back(c->tiles[t].back() + ceil_div(nvis, 128 << t));
     c->max_nh = std::max(c->max_nh, d.nh);
     c->max_L3 = std::max(c->max_L3, d.L3);
   }
@@ -658,12 +681,13 @@ lce_ctx* create_impl(const lce_params* p, int n, const SlabInfo* slab = nullptr)
   if ((e = cudaMalloc(&c->ch_d, sizeof(ChainDev) * n)) != cudaSuccess) return bail(e, "cudaMalloc(chains)");
   if ((e = cudaMemcpy(c->ch_d, c->ch.data(), sizeof(ChainDev) * n, cudaMemcpyHostToDevice)) != cudaSuccess)
     return bail(e, "cudaMemcpy(chains)");
-  if ((e = cudaMalloc(&c->blk_d, sizeof(int) * (n + 1))) != cudaSuccess) return bail(e, "cudaMalloc(blk)");
-  if ((e = cudaMemcpy(c->blk_d, c->blk.data(), sizeof(int) * (n + 1), cudaMemcpyHostToDevice)) != cudaSuccess)
-    return bail(e, "cudaMemcpy(blk)");
-  if ((e = cudaMalloc(&c->blk2_d, sizeof(int) * (n + 1))) != cudaSuccess) return bail(e, "cudaMalloc(blk2)");
-  if ((e = cudaMemcpy(c->blk2_d, c->blk2.data(), sizeof(int) * (n + 1), cudaMemcpyHostToDevice)) != cudaSuccess)
-    return bail(e, "cudaMemcpy(blk2)");
+  for (int t = 0; t < 3; ++t) {
+    if ((e = cudaMalloc(&c->tiles_d[t], sizeof(int) * (n + 1))) != cudaSuccess) return bail(e, "cudaMalloc(tiles)");
+    if ((e = cudaMemcpy(c->tiles_d[t], c->tiles[t].data(), sizeof(int) * (n + 1), cudaMemcpyHostToDevice)) !=
+        cudaSuccess)
+      return bail(e, "cudaMemcpy(tiles)");
+  }
+  c->blk_d = c->tiles_d[1];
   if ((e = cudaMalloc(&c->st_d, sizeof(CtxState))) != cudaSuccess) return bail(e, "cudaMalloc(state)");
   if ((e = cudaMemset(c->st_d, 0, sizeof(CtxState))) != cudaSuccess) return bail(e, "cudaMemset(state)");
   if ((e = cudaMalloc(&c->cst_d, sizeof(ChainState) * n)) != cudaSuccess) return bail(e, "cudaMalloc(cstate)");
@@ -682,17 +706,31 @@ lce_ctx* create_impl(const lce_params* p, int n, const SlabInfo* slab = nullptr)
   c->sweep_mode = p[0].sweep_mode;
   c->mode = p[0].sweep_mode;
   c->persist_grid = c->prec == LCE_PREC_F64 ? persistent_grid<double>() : persistent_grid<float>();
-  if (c->persist_grid <= 0) {
-    if (c->sweep_mode == LCE_SWEEP_PERSISTENT) {
-      g_create_error = "create: the persistent sweep kernel cannot be made resident on this device";
-      lce_destroy(c);
-      return nullptr;
+  if (c->persist_grid <= 0 && c->sweep_mode == LCE_SWEEP_PERSISTENT) {
+    g_create_error = "create: the persistent sweep kernel cannot be made resident on this device";
+    lce_destroy(c);
+    return nullptr;
+  }
+  // tile shape: FP32 contexts tune threads per block (128, 256, 512) and sites
+  // per thread under AUTO unless tile_threads fixes the block; the FP64
+  // validation path and z-slabs use kBlock threads
+  c->tile_req = (c->prec == LCE_PREC_F32 && !slab) ? p[0].tile_threads : kBlock;
+  c->tile_bs = c->tile_req ? c->tile_req : kBlock;
+  c->tile_spt = c->mode == LCE_SWEEP_PASSES2 ? 2 : 1;
+  if (c->tile_spt == 2 && c->tile_bs == 512) c->tile_bs = kBlock;  // (512, 2) is not compiled
+  if (c->mode == LCE_SWEEP_AUTO) {
+    const int bss[3] = {128, 256, 512};
+    for (int b : bss) {
+      if (c->tile_req && b != c->tile_req) continue;
+      if (c->prec == LCE_PREC_F64 && b != kBlock) continue;
+      c->tune.push_back(TuneForm{LCE_SWEEP_PASSES, b, 1, {}});
+      if (b != 512) c->tune.push_back(TuneForm{LCE_SWEEP_PASSES2, b, 2, {}});
     }
-    c->mode = LCE_SWEEP_PASSES;
+    if (c->persist_grid > 0) c->tune.push_back(TuneForm{LCE_SWEEP_PERSISTENT, kBlock, 1, {}});
   }
   if ((e = cudaMemset(c->meas_d, 0, sizeof(lce_meas) * n)) != cudaSuccess) return bail(e, "cudaMemset(meas)");
   c->part_slots = std::max(6, 4 + 6 + 2 * c->n_higgs_metro + 6 * c->n_link_or);
-  c->slot_stride = (size_t)c->blk.back() * kNQ;
+  c->slot_stride = (size_t)c->tiles[0].back() * kNQ;  // the most tiles: 128 sites each
   if ((e = cudaMalloc(&c->part_d, sizeof(double) * c->slot_stride * c->part_slots)) != cudaSuccess)
     return bail(e, "cudaMalloc(partials)");
   if ((e = cudaMalloc(&c->totals_d, sizeof(double) * (size_t)n * kMaxSlots * kNQ)) != cudaSuccess)
@@ -833,7 +871,14 @@ int fa_loop(lce_ctx* c, int chain, double step, double limit, double* theta, int
           launch_fa_iteration<float>(c->ch_d + chain, ch, c->cst_d + chain, step, c->fa_d, fa_vcap(c), part,
                                      nullptr, 1, true, true, cg, c->stream);
       }
-      CK(cudaStreamEndCapture(c->stream, &g));
+      const cudaError_t ec = cudaStreamEndCapture(c->stream, &g);
+      const std::string fe = fa_take_error();
+      if (!fe.empty()) {
+        if (ec == cudaSuccess) cudaGraphDestroy(g);
+        cudaGetLastError();
+        return fail(c, LCE_ERR_CUDA, "Fourier-accelerated fixing: " + fe);
+      }
+      if (ec != cudaSuccess) return cuda_fail(c, ec, "cudaStreamEndCapture(Fourier-accelerated fixing)");
       cudaGraphExec_t ex;
       cudaError_t e = cudaGraphInstantiate(&ex, g, 0);
       cudaGraphDestroy(g);
@@ -1006,7 +1051,7 @@ int slab_sweep(lce_slabs* S, int measflag, lce_meas* m) {
   const int n = (int)S->slab.size();
   std::vector<Enq> q(n);
   const std::vector<unsigned char> routines = sweep_routines(S->slab[0]);
-  for (int k = 0; k < n; ++k) enq_begin(S->slab[k], routines, measflag, true, 1, q[k]);
+  for (int k = 0; k < n; ++k) enq_begin(S->slab[k], routines, measflag, true, kBlock, 1, q[k]);
   for (size_t i = 0; i < q[0].passes.size(); ++i) {
     for (int k = 0; k < n; ++k) {
       lce_ctx* c = S->slab[k];
@@ -1320,14 +1365,11 @@ void lce_destroy(lce_ctx* c) {
   if (!c) return;
   cudaSetDevice(c->device);
   if (c->stream) cudaStreamSynchronize(c->stream);
-  for (int i = 0; i < 2; ++i) {
-    if (c->sweep_exec[i]) cudaGraphExecDestroy(c->sweep_exec[i]);
-    if (c->sweep2_exec[i]) cudaGraphExecDestroy(c->sweep2_exec[i]);
-    if (c->persist_exec[i]) cudaGraphExecDestroy(c->persist_exec[i]);
-  }
+  for (auto& kv : c->sweep_graphs)
+    if (kv.second) cudaGraphExecDestroy(kv.second);
   for (auto& kv : c->gf_exec) cudaGraphExecDestroy(kv.second);
   for (auto& kv : c->fa_exec) cudaGraphExecDestroy(kv.second);
-  void* ptrs[] = {c->ch_d, c->blk_d, c->blk2_d, c->st_d, c->cst_d, c->meas_d, c->part_d, c->totals_d,
+  void* ptrs[] = {c->ch_d, c->tiles_d[0], c->tiles_d[1], c->tiles_d[2], c->st_d, c->cst_d, c->meas_d, c->part_d, c->totals_d,
                   c->scratch_d, c->fields_d, c->stream_d, c->staging_d, c->flush_d, c->bar_d,
                   c->gsave_d, c->fa_d};
   for (void* q : ptrs)
@@ -1422,20 +1464,9 @@ int lce_set_rng_stream(lce_ctx* c, const double* u, size_t n) {
   }
   c->stream_n = n;
   // graphs captured the old stream pointer
-  for (int i = 0; i < 2; ++i) {
-    if (c->sweep_exec[i]) {
-      cudaGraphExecDestroy(c->sweep_exec[i]);
-      c->sweep_exec[i] = nullptr;
-    }
-    if (c->sweep2_exec[i]) {
-      cudaGraphExecDestroy(c->sweep2_exec[i]);
-      c->sweep2_exec[i] = nullptr;
-    }
-    if (c->persist_exec[i]) {
-      cudaGraphExecDestroy(c->persist_exec[i]);
-      c->persist_exec[i] = nullptr;
-    }
-  }
+  for (auto& kv : c->sweep_graphs)
+    if (kv.second) cudaGraphExecDestroy(kv.second);
+  c->sweep_graphs.clear();
   unsigned long long z = 0;
   CK(cudaMemcpy(&c->st_d->stream_pos, &z, sizeof(z), cudaMemcpyHostToDevice));
   return LCE_OK;
@@ -1521,18 +1552,16 @@ int lce_sweeps(lce_ctx* c, int nsweeps, int measflag) {
   if (!c || nsweeps < 0) return LCE_ERR_INVALID;
   const int mf = measflag == 1 ? 1 : 0;
   int done = 0;
-  // autotune: rotate through the forms on real sweeps, one timed sweep at a
-  // time, until each has kTuneSamples samples (after a discarded first one);
-  // then keep the fastest.  Forms: 0 per-pass kernels, 1 persistent kernel
-  // (when it can be resident), 2 per-pass kernels with two sites per thread.
-  const int kForm[3] = {LCE_SWEEP_PASSES, LCE_SWEEP_PERSISTENT, LCE_SWEEP_PASSES2};
-  const int nforms = 3;
+  // autotune: rotate through the candidates (sweep forms and tile shapes) on
+  // real sweeps, one timed sweep at a time, until each has kTuneSamples
+  // samples after a discarded first one; then keep the fastest by median.
   while (c->mode == LCE_SWEEP_AUTO && done < nsweeps) {
-    int form = 0;
-    for (int f = 1; f < nforms; ++f)
-      if (c->tune_ms[f].size() < c->tune_ms[form].size()) form = f;
+    int k = 0;
+    for (int f = 1; f < (int)c->tune.size(); ++f)
+      if (c->tune[f].ms.size() < c->tune[k].ms.size()) k = f;
+    const TuneForm tf = c->tune[k];
     cudaGraphExec_t ex;
-    int rc = sweep_graph(c, kForm[form], mf, &ex);
+    int rc = sweep_graph(c, tf.form, tf.bs, tf.spt, mf, &ex);
     if (rc) return rc;
     if (c->mode != LCE_SWEEP_AUTO) break;  // the persistent form was unavailable
     CK(cudaEventRecord(c->ev0, c->stream));
@@ -1541,16 +1570,15 @@ int lce_sweeps(lce_ctx* c, int nsweeps, int measflag) {
     CK(cudaEventSynchronize(c->ev1));
     float ms = 0;
     CK(cudaEventElapsedTime(&ms, c->ev0, c->ev1));
-    c->tune_ms[form].push_back(ms);
+    c->tune[k].ms.push_back(ms);
     ++done;
     bool complete = true;
-    for (int f = 0; f < nforms; ++f) complete = complete && c->tune_ms[f].size() >= kTuneSamples + 1;
+    for (const TuneForm& f : c->tune) complete = complete && f.ms.size() >= kTuneSamples + 1;
     if (complete) {
-      // drop each form's first (instantiation-cold) sample, compare medians
       int best = 0;
       float best_med = 0;
-      for (int f = 0; f < nforms; ++f) {
-        std::vector<float> v(c->tune_ms[f].begin() + 1, c->tune_ms[f].end());
+      for (int f = 0; f < (int)c->tune.size(); ++f) {
+        std::vector<float> v(c->tune[f].ms.begin() + 1, c->tune[f].ms.end());
         std::sort(v.begin(), v.end());
         const float med = v[v.size() / 2];
         if (f == 0 || med < best_med) {
@@ -1558,12 +1586,14 @@ int lce_sweeps(lce_ctx* c, int nsweeps, int measflag) {
           best_med = med;
         }
       }
-      c->mode = kForm[best];
+      c->mode = c->tune[best].form;
+      c->tile_bs = c->tune[best].bs;
+      c->tile_spt = c->tune[best].spt;
     }
   }
   if (done < nsweeps) {
     cudaGraphExec_t ex;
-    int rc = sweep_graph(c, c->mode, mf, &ex);
+    int rc = sweep_graph(c, c->mode, c->tile_bs, c->tile_spt, mf, &ex);
     if (rc) return rc;
     for (int i = done; i < nsweeps; ++i) CK(cudaGraphLaunch(ex, c->stream));
   }
@@ -1571,6 +1601,13 @@ int lce_sweeps(lce_ctx* c, int nsweeps, int measflag) {
 }
 
 int lce_get_sweep_mode(lce_ctx* c) { return c ? c->mode : LCE_ERR_INVALID; }
+
+int lce_get_tile_shape(lce_ctx* c, int* threads, int* sites_per_thread) {
+  if (!c) return LCE_ERR_INVALID;
+  if (threads) *threads = c->mode == LCE_SWEEP_PERSISTENT ? kBlock : c->tile_bs;
+  if (sites_per_thread) *sites_per_thread = c->mode == LCE_SWEEP_PERSISTENT ? 1 : c->tile_spt;
+  return LCE_OK;
+}
 
 int lce_sweep(lce_ctx* c, int measflag, lce_meas* m) {
   DeviceScope ds_(c ? c->device : -1);
@@ -1843,9 +1880,11 @@ int lce_debug_fourier_step(lce_ctx* c, int chain, double step, double* omega) {
     launch_fa_iteration<float>(c->ch_d + chain, ch, nullptr, step, c->fa_d, fa_vcap(c), c->scratch_d, om, 0, false,
                                false, false, c->stream);
   cudaError_t e = cudaGetLastError();
-  if (e == cudaSuccess) e = cudaMemcpyAsync(omega, om, ob, cudaMemcpyDeviceToHost, c->stream);
-  if (e == cudaSuccess) e = cudaStreamSynchronize(c->stream);
+  const std::string fe = fa_take_error();
+  if (e == cudaSuccess && fe.empty()) e = cudaMemcpyAsync(omega, om, ob, cudaMemcpyDeviceToHost, c->stream);
+  if (e == cudaSuccess && fe.empty()) e = cudaStreamSynchronize(c->stream);
   cudaFree(om);
+  if (!fe.empty()) return fail(c, LCE_ERR_CUDA, "debug_fourier_step: " + fe);
   if (e != cudaSuccess) return cuda_fail(c, e, "debug_fourier_step");
   return LCE_OK;
 }
@@ -2040,7 +2079,7 @@ int lce_profile_sweep(lce_ctx* c, int measflag, float* ms, int max_passes) {
   std::vector<cudaEvent_t> ev(np + 1);
   for (auto& e : ev) CK(cudaEventCreate(&e));
   CK(cudaEventRecord(ev[0], c->stream));
-  int rc = enqueue(c, r, measflag == 1 ? 1 : 0, true, ev.data() + 1, c->mode == LCE_SWEEP_PASSES2 ? 2 : 1);
+  int rc = enqueue(c, r, measflag == 1 ? 1 : 0, true, ev.data() + 1);
   if (rc == LCE_OK) {
     CK(cudaStreamSynchronize(c->stream));
     for (int i = 0; i < np && i < max_passes; ++i) CK(cudaEventElapsedTime(&ms[i], ev[i], ev[i + 1]));

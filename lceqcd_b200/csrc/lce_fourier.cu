@@ -59,6 +59,8 @@
 // region (fa_alpha_kernel).
 #include <algorithm>
 
+#include <string>
+
 #include "lce_internal.hpp"
 
 namespace lce {
@@ -730,24 +732,44 @@ void fa_cg_reset(void* buf, size_t vcap, cudaStream_t s) {
   fa_cg_reset_kernel<<<1, 1, 0, s>>>(reinterpret_cast<FaCg*>(fa_at(buf, fa_off_cg(vcap))));
 }
 
+// The first failed launch set-up of this host thread since the last
+// fa_take_error(): which kernel, its line length and the shared memory it
+// asked for.  A kernel whose set-up failed is not launched.
+namespace {
+thread_local std::string t_fa_error;
+}
+
+std::string fa_take_error() {
+  std::string e;
+  e.swap(t_fa_error);
+  return e;
+}
+
 // launchers per line length (the kernels are compiled for each power of two)
 template <typename K>
-void fa_launch(K kernel, dim3 grid, size_t smem, const FaArgs& a, cudaStream_t s) {
-  cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+void fa_launch(K kernel, const char* what, int logn, dim3 grid, size_t smem, const FaArgs& a, cudaStream_t s) {
+  const cudaError_t e = cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  if (e != cudaSuccess) {
+    if (t_fa_error.empty())
+      t_fa_error = std::string(what) + " for lines of " + std::to_string(1 << logn) +
+                   " points: cudaFuncSetAttribute(MaxDynamicSharedMemorySize = " + std::to_string(smem) +
+                   " bytes): " + cudaGetErrorString(e);
+    return;
+  }
   kernel<<<grid, kFaThreads, smem, s>>>(a);
 }
 template <typename R, int LOGN>
 void fa_div_launch(const FaArgs& a, int nb, cudaStream_t s) {
-  fa_launch(fa_div_kernel<R, LOGN>, dim3(nb), FaLines<LOGN>::smem(1, 0), a, s);
+  fa_launch(fa_div_kernel<R, LOGN>, "fa_div_kernel", LOGN, dim3(nb), FaLines<LOGN>::smem(1, 0), a, s);
 }
 template <typename R, int LOGN, bool CG = false>
 void fa_g_launch(const FaArgs& a, int nb, cudaStream_t s) {
-  fa_launch(fa_g_kernel<R, LOGN, CG>, dim3(nb), FaLines<LOGN>::smem(1, 0), a, s);
+  fa_launch(fa_g_kernel<R, LOGN, CG>, "fa_g_kernel", LOGN, dim3(nb), FaLines<LOGN>::smem(1, 0), a, s);
 }
 template <int AX, int SIGN, bool SCALE, int LOGN, bool CG = false>
 void fa_fft_launch(const FaArgs& a, int nb, cudaStream_t s) {
   using G = FaLines<LOGN>;
-  fa_launch(fa_fft_kernel<AX, SIGN, SCALE, LOGN, CG>, dim3(nb, 2),
+  fa_launch(fa_fft_kernel<AX, SIGN, SCALE, LOGN, CG>, "fa_fft_kernel", LOGN, dim3(nb, 2),
             G::smem(SCALE ? 2 : 1, SCALE ? G::n + G::NLT : 0), a, s);
 }
 #define LCE_FA_SWITCH(logn, CALL) \

@@ -113,7 +113,8 @@ struct PassArgs {
   int nchains;
   int eo;
   int fuse_renorm;
-  int spt;                // sites per thread (a tile is kBlock * spt sites)
+  int spt;                // sites per thread (a tile is bs * spt sites)
+  int bs;                 // threads per block of the per-pass kernels
   // z-slab of a decomposed lattice (single-chain contexts): the passes visit
   // sites [s_lo, nh - s_lo) of each parity (the first and last planes are
   // halos), and site_off turns a site index into the whole lattice's for the
@@ -220,6 +221,9 @@ void launch_fa_iteration(const ChainDev* chd, const ChainDev& ch, ChainState* cs
                          bool cg, cudaStream_t s);
 // the conjugate-gradient form starts its next iteration from the gradient
 void fa_cg_reset(void* buf, size_t vcap, cudaStream_t s);
+// the first launch set-up failure of this host thread's Fourier kernels
+// since the last call (kernel, line length, shared memory), or ""
+std::string fa_take_error();
 template <typename R>
 void launch_gf_theta(const ChainDev* ch, double* part, int nh, cudaStream_t s);
 void launch_sum_partials(const double* part, int nblocks, int nq, double* out, cudaStream_t s);

@@ -14,7 +14,10 @@
 // contents; each call overwrites every entry it reads, so nothing needs to
 // start at zero.  Calls whose kernels overlap on the GPU (different streams,
 // or different host threads) race on the array and must be serialised by the
-// caller.
+// caller.  The array's device address is looked up on a device's first call
+// and kept until the process exits: after a cudaDeviceReset (which tears down
+// the primary context and reloads this module) the kept address is stale, so
+// the entry point must not be used across a device reset.
 #include <mutex>
 
 #include "lce_internal.hpp"

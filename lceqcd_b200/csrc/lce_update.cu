@@ -1,7 +1,9 @@
 // lce_update.cu -- checkerboard Monte Carlo update kernels.
 //
 // One pass = one routine over one parity (and one mu for links), one thread
-// per site, sites grouped in tiles of kBlock consecutive sites of one chain.
+// per site (or two), sites grouped in tiles of consecutive sites of one chain
+// (the tile shape -- threads per block and sites per thread -- is chosen per
+// context; the persistent form uses kBlock threads and one site per thread).
 // The per-tile bodies fuse what the reference does as a chain of whole-lattice
 // array passes (multall*, halo exchanges, temporaries): neighbour gathers, the
 // SU(2) algebra, the random proposal, the accept/reject and the FP64 partial
@@ -59,26 +61,24 @@ __device__ __forceinline__ R ldA(const R* A, int nh, int p, int k, int s) {
   return NC ? __ldg(q) : __ldcg(q);
 }
 
-// neighbour of X one step along mu (d = +1 / -1), index inside its parity
-template <int MU>
-__device__ __forceinline__ int nbr(const ChainDev& ch, Coord X, int d) {
-  int x = X.x, y = X.y, z = X.z;
-  if (MU == 0) x = wrap(x + d, ch.L1);
-  if (MU == 1) y = wrap(y + d, ch.L2);
-  if (MU == 2) z = wrap(z + d, ch.L3);
-  return site_index(x, y, z, ch.hx, ch.nxy);
-}
-// two steps: +d1 along M1 and +d2 along M2 (M1 != M2)
-template <int M1, int M2>
-__device__ __forceinline__ int nbr2(const ChainDev& ch, Coord X, int d1, int d2) {
-  int x = X.x, y = X.y, z = X.z;
-  if (M1 == 0) x = wrap(x + d1, ch.L1);
-  if (M1 == 1) y = wrap(y + d1, ch.L2);
-  if (M1 == 2) z = wrap(z + d1, ch.L3);
-  if (M2 == 0) x = wrap(x + d2, ch.L1);
-  if (M2 == 1) y = wrap(y + d2, ch.L2);
-  if (M2 == 2) z = wrap(z + d2, ch.L3);
-  return site_index(x, y, z, ch.hx, ch.nxy);
+// Neighbour offsets of one site.  The half-row index s = z*nxy + y*hx + (x>>1)
+// of f/adresses.f is a sum of per-axis terms, so the index of any neighbour,
+// one step or two steps along different axes, is s plus the steps' offsets;
+// p[k] / m[k] are the offsets of +1 / -1 along axis k (periodic).  Computed
+// once per site instead of re-deriving every neighbour from coordinates.
+struct NbrOff {
+  int p[3], m[3];
+};
+__device__ __forceinline__ NbrOff nbr_offsets(const ChainDev& ch, Coord X) {
+  NbrOff o;
+  const int xh = X.x >> 1;
+  o.p[0] = X.x + 1 == ch.L1 ? -xh : ((X.x + 1) >> 1) - xh;
+  o.m[0] = X.x == 0 ? ch.hx - 1 : ((X.x - 1) >> 1) - xh;
+  o.p[1] = X.y + 1 == ch.L2 ? ch.hx - ch.nxy : ch.hx;
+  o.m[1] = X.y == 0 ? ch.nxy - ch.hx : -ch.hx;
+  o.p[2] = X.z + 1 == ch.L3 ? ch.nxy - ch.nh : ch.nxy;
+  o.m[2] = X.z == 0 ? ch.nh - ch.nxy : -ch.nxy;
+  return o;
 }
 
 template <typename R, bool NC = true>
@@ -92,10 +92,10 @@ __device__ __forceinline__ su2<R> ldU(const ChainDev& ch, int mu, int p, int s) 
 //   lower  = U_nu(x-nu+mu)^+ [U_mu(x-nu)^+ U_nu(x-nu)]    (DN of DN)
 //   V      = (V + upper) + lower
 template <typename R, int MU, int NU, bool NC>
-__device__ __forceinline__ void staple_add(const ChainDev& ch, int eo, Coord X, int s, su2<R>& V) {
+__device__ __forceinline__ void staple_add(const ChainDev& ch, int eo, const NbrOff& o, int s, su2<R>& V) {
   const int oe = 1 - eo;
-  const int xpmu = nbr<MU>(ch, X, +1), xpnu = nbr<NU>(ch, X, +1), xmnu = nbr<NU>(ch, X, -1);
-  const int xmnupmu = nbr2<NU, MU>(ch, X, -1, +1);
+  const int xpmu = s + o.p[MU], xpnu = s + o.p[NU], xmnu = s + o.m[NU];
+  const int xmnupmu = xmnu + o.p[MU];
   su2<R> up1 = dd(ldU<R, NC>(ch, MU, oe, xpnu), ldU<R, NC>(ch, NU, eo, s));
   su2<R> up2 = nn(ldU<R, NC>(ch, NU, oe, xpmu), up1);
   su2<R> bt1 = dn(ldU<R, NC>(ch, MU, oe, xmnu), ldU<R, NC>(ch, NU, oe, xmnu));
@@ -105,17 +105,17 @@ __device__ __forceinline__ void staple_add(const ChainDev& ch, int eo, Coord X, 
 }
 
 template <typename R, int MU, bool NC = true>
-__device__ __forceinline__ su2<R> staple(const ChainDev& ch, int eo, Coord X, int s) {
+__device__ __forceinline__ su2<R> staple(const ChainDev& ch, int eo, const NbrOff& o, int s) {
   su2<R> V{{(R)0, (R)0}, {(R)0, (R)0}};
   if (MU == 0) {
-    staple_add<R, 0, 1, NC>(ch, eo, X, s, V);
-    staple_add<R, 0, 2, NC>(ch, eo, X, s, V);
+    staple_add<R, 0, 1, NC>(ch, eo, o, s, V);
+    staple_add<R, 0, 2, NC>(ch, eo, o, s, V);
   } else if (MU == 1) {
-    staple_add<R, 1, 0, NC>(ch, eo, X, s, V);
-    staple_add<R, 1, 2, NC>(ch, eo, X, s, V);
+    staple_add<R, 1, 0, NC>(ch, eo, o, s, V);
+    staple_add<R, 1, 2, NC>(ch, eo, o, s, V);
   } else {
-    staple_add<R, 2, 0, NC>(ch, eo, X, s, V);
-    staple_add<R, 2, 1, NC>(ch, eo, X, s, V);
+    staple_add<R, 2, 0, NC>(ch, eo, o, s, V);
+    staple_add<R, 2, 1, NC>(ch, eo, o, s, V);
   }
   return V;
 }
@@ -123,11 +123,11 @@ __device__ __forceinline__ su2<R> staple(const ChainDev& ch, int eo, Coord X, in
 // f/a_force.f:54-110: F = sum_mu [U(x)(iA(x+mu))U(x)^+ + U(x-mu)^+(iA(x-mu))U(x-mu)],
 // components F3 = Im(.)_a, F2 = Re(.)_b, F1 = Im(.)_b
 template <typename R, int MU, bool NC>
-__device__ __forceinline__ void force_add(const ChainDev& ch, int eo, Coord X, int s, R& f1, R& f2,
+__device__ __forceinline__ void force_add(const ChainDev& ch, int eo, const NbrOff& o, int s, R& f1, R& f2,
                                           R& f3) {
   const int oe = 1 - eo, nh = ch.nh;
   const R* A = reinterpret_cast<const R*>(ch.a);
-  const int xp = nbr<MU>(ch, X, +1), xm = nbr<MU>(ch, X, -1);
+  const int xp = s + o.p[MU], xm = s + o.m[MU];
   su2<R> ux = ldU<R, NC>(ch, MU, eo, s);
   su2<R> ud = ldU<R, NC>(ch, MU, oe, xm);
   su2<R> t1 = nn(ux, ad(ldA<R, NC>(A, nh, oe, 0, xp), ldA<R, NC>(A, nh, oe, 1, xp), ldA<R, NC>(A, nh, oe, 2, xp), ux));
@@ -138,12 +138,12 @@ __device__ __forceinline__ void force_add(const ChainDev& ch, int eo, Coord X, i
 }
 
 template <typename R, bool NC = true>
-__device__ __forceinline__ void higgs_force(const ChainDev& ch, int eo, Coord X, int s, R& f1, R& f2,
+__device__ __forceinline__ void higgs_force(const ChainDev& ch, int eo, const NbrOff& o, int s, R& f1, R& f2,
                                             R& f3) {
   f1 = f2 = f3 = (R)0;
-  force_add<R, 0, NC>(ch, eo, X, s, f1, f2, f3);
-  force_add<R, 1, NC>(ch, eo, X, s, f1, f2, f3);
-  force_add<R, 2, NC>(ch, eo, X, s, f1, f2, f3);
+  force_add<R, 0, NC>(ch, eo, o, s, f1, f2, f3);
+  force_add<R, 1, NC>(ch, eo, o, s, f1, f2, f3);
+  force_add<R, 2, NC>(ch, eo, o, s, f1, f2, f3);
 }
 
 // Set up the uniform source of this pass (of hit `hit` of a multi-hit pass:
@@ -166,16 +166,17 @@ __device__ __forceinline__ bool setup_uniforms(const PassArgs& p, const ChainDev
 }
 
 // ------------------------------------------------------------------ Higgs
-// One tile (kBlock consecutive sites of one chain) of a Higgs pass.  PDL:
-// trigger dependents and wait for the previous kernel (per-pass form only).
-template <typename R, int MODE, bool PDL, int SPT = 1>
+// One tile (BS * SPT consecutive sites of one chain, BS threads) of a Higgs
+// pass.  PDL: trigger dependents and wait for the previous kernel (per-pass
+// form only).
+template <typename R, int MODE, bool PDL, int SPT = 1, int BS = kBlock>
 __device__ __forceinline__ void higgs_tile(const PassArgs& p, int tile) {
   if (PDL) pdl_trigger();
   // the chain table is written once at context creation: safe before pdl_wait
   const int c = p.nchains > 1 ? find_chain(p.blk_begin, p.nchains, tile) : 0;
   const ChainDev& ch = p.chains[c];
-  // a tile is kBlock * SPT consecutive sites; thread t takes t, t + kBlock, ...
-  const int s0 = p.s_lo + (tile - __ldg(p.blk_begin + c)) * kBlock * SPT + threadIdx.x;
+  // a tile is BS * SPT consecutive sites; thread t takes t, t + BS, ...
+  const int s0 = p.s_lo + (tile - __ldg(p.blk_begin + c)) * BS * SPT + threadIdx.x;
   const int eo = p.eo, nh = ch.nh, s_hi = nh - p.s_lo;
   const Coord X0 = site_coord(eo, s0 < s_hi ? s0 : p.s_lo, ch.hx, ch.nxy, ch.dhx, ch.dnxy);
   unsigned acc[1] = {0u};
@@ -183,15 +184,16 @@ __device__ __forceinline__ void higgs_tile(const PassArgs& p, int tile) {
   if (PDL) pdl_wait();
 #pragma unroll 1
   for (int r = 0; r < SPT; ++r) {
-    const int s = s0 + r * kBlock;
+    const int s = s0 + r * BS;
     if (s >= s_hi) break;
     const Coord X = r == 0 ? X0 : site_coord(eo, s, ch.hx, ch.nxy, ch.dhx, ch.dnxy);
+    const NbrOff no = nbr_offsets(ch, X);
     constexpr int NS = MODE == 0 ? 7 : (MODE == 1 ? 1 : 4);
     const int layout = MODE == 2 ? kTriple : kPlanar;
     Uniforms<R, NS> Un;
     if (setup_uniforms<R, NS>(p, ch, s, layout, Un)) {
       R f[3];
-      higgs_force<R, PDL>(ch, eo, X, s, f[0], f[1], f[2]);
+      higgs_force<R, PDL>(ch, eo, no, s, f[0], f[1], f[2]);
       R* A = reinterpret_cast<R*>(ch.a);
       R ao[3], an_[3];
 #pragma unroll
@@ -279,13 +281,13 @@ __device__ __forceinline__ void higgs_tile(const PassArgs& p, int tile) {
 // NHIT = 3 is f/agauge1.f: the staple is built once and the heatbath +
 // Metropolis hit is repeated on the updated link, each hit with its own
 // uniforms (f/agauge1.f:95-198).
-template <typename R, int MU, int OR, bool PDL, int NHIT = 1, int SPT = 1>
+template <typename R, int MU, int OR, bool PDL, int NHIT = 1, int SPT = 1, int BS = kBlock>
 __device__ __forceinline__ void link_tile(const PassArgs& p, int tile) {
   if (PDL) pdl_trigger();
   const int c = p.nchains > 1 ? find_chain(p.blk_begin, p.nchains, tile) : 0;
   const ChainDev& ch = p.chains[c];
-  // a tile is kBlock * SPT consecutive sites; thread t takes t, t + kBlock, ...
-  const int s0 = p.s_lo + (tile - __ldg(p.blk_begin + c)) * kBlock * SPT + threadIdx.x;
+  // a tile is BS * SPT consecutive sites; thread t takes t, t + BS, ...
+  const int s0 = p.s_lo + (tile - __ldg(p.blk_begin + c)) * BS * SPT + threadIdx.x;
   const int eo = p.eo, oe = 1 - eo, nh = ch.nh, s_hi = nh - p.s_lo;
   const Coord X0 = site_coord(eo, s0 < s_hi ? s0 : p.s_lo, ch.hx, ch.nxy, ch.dhx, ch.dnxy);
   unsigned cnt[2] = {0u, 0u};
@@ -293,12 +295,13 @@ __device__ __forceinline__ void link_tile(const PassArgs& p, int tile) {
   if (PDL) pdl_wait();
 #pragma unroll 1
   for (int r = 0; r < SPT; ++r) {
-    const int s = s0 + r * kBlock;
+    const int s = s0 + r * BS;
     if (s >= s_hi) break;
     const Coord X = r == 0 ? X0 : site_coord(eo, s, ch.hx, ch.nxy, ch.dhx, ch.dnxy);
+    const NbrOff no = nbr_offsets(ch, X);
     Uniforms<R, OR ? 1 : 7> Un;
     if (setup_uniforms<R, OR ? 1 : 7>(p, ch, s, OR ? kPlanar : kTriple, Un)) {
-      const su2<R> V = staple<R, MU, PDL>(ch, eo, X, s);
+      const su2<R> V = staple<R, MU, PDL>(ch, eo, no, s);
       const size_t li = ((size_t)(MU * 2 + eo)) * nh + s;
       su2<R> uo = PDL ? LinkIO<R>::ld(ch.u, li) : LinkIO<R>::ld_cg(ch.u, li);
       // f/agauge.f:71-84: normalised staple, 1/(beta |V|), 1/2 Re Tr(U Vhat)
@@ -306,7 +309,7 @@ __device__ __forceinline__ void link_tile(const PassArgs& p, int tile) {
       const su2<R> vh{{tn * V.a.re, tn * V.a.im}, {tn * V.b.re, tn * V.b.im}};
       // f/agauge.f:126-174 hopping term beta_a Re[(iA(x) U)(iA(x+mu) U^+)]_11 and accept
       const R* A = reinterpret_cast<const R*>(ch.a);
-      const int xp = nbr<MU>(ch, X, +1);
+      const int xp = s + no.p[MU];
       const R x1 = ldA<R, PDL>(A, nh, eo, 0, s), x2 = ldA<R, PDL>(A, nh, eo, 1, s), x3 = ldA<R, PDL>(A, nh, eo, 2, s);
       const R y1 = ldA<R, PDL>(A, nh, oe, 0, xp), y2 = ldA<R, PDL>(A, nh, oe, 1, xp), y3 = ldA<R, PDL>(A, nh, oe, 2, xp);
       const R beta_a = (R)ch.beta_a;
@@ -368,21 +371,26 @@ __device__ __forceinline__ void link_tile(const PassArgs& p, int tile) {
   }
 }
 
-// SPT = sites per thread (1, or 2 for the LCE_SWEEP_PASSES2 form)
-template <typename R, int MODE, int SPT>
-__global__ void __launch_bounds__(kBlock, min_blocks<R>()) higgs_kernel(PassArgs p) {
-  higgs_tile<R, MODE, true, SPT>(p, blockIdx.x);
+// Tile shape: BS threads per block, SPT sites per thread (1, or 2 for the
+// LCE_SWEEP_PASSES2 form).  The register cap is the same for every BS: the
+// resident threads per SM of min_blocks<R>() blocks of kBlock threads.
+template <typename R, int BS>
+constexpr int min_blocks_bs() { return min_blocks<R>() * kBlock / BS > 0 ? min_blocks<R>() * kBlock / BS : 1; }
+
+template <typename R, int MODE, int SPT, int BS>
+__global__ void __launch_bounds__(BS, min_blocks_bs<R, BS>()) higgs_kernel(PassArgs p) {
+  higgs_tile<R, MODE, true, SPT, BS>(p, blockIdx.x);
 }
 
-template <typename R, int MU, int OR, int SPT>
-__global__ void __launch_bounds__(kBlock, min_blocks<R>()) link_kernel(PassArgs p) {
-  link_tile<R, MU, OR, true, 1, SPT>(p, blockIdx.x);
+template <typename R, int MU, int OR, int SPT, int BS>
+__global__ void __launch_bounds__(BS, min_blocks_bs<R, BS>()) link_kernel(PassArgs p) {
+  link_tile<R, MU, OR, true, 1, SPT, BS>(p, blockIdx.x);
 }
 
 // f/agauge1.f (3 hits)
-template <typename R, int MU, int SPT>
-__global__ void __launch_bounds__(kBlock, min_blocks<R>()) link3_kernel(PassArgs p) {
-  link_tile<R, MU, 0, true, 3, SPT>(p, blockIdx.x);
+template <typename R, int MU, int SPT, int BS>
+__global__ void __launch_bounds__(BS, min_blocks_bs<R, BS>()) link3_kernel(PassArgs p) {
+  link_tile<R, MU, 0, true, 3, SPT, BS>(p, blockIdx.x);
 }
 
 // ------------------------------------------------------------------ finalize
@@ -610,7 +618,7 @@ __global__ void debug_staple_kernel(const ChainDev* chp, int eo, double* out) {
   const int s = blockIdx.x * blockDim.x + threadIdx.x;
   if (s >= ch.nh) return;
   Coord X = site_coord(eo, s, ch.hx, ch.nxy, ch.dhx, ch.dnxy);
-  su2<R> V = staple<R, MU>(ch, eo, X, s);
+  su2<R> V = staple<R, MU>(ch, eo, nbr_offsets(ch, X), s);
   out[(size_t)s * 4 + 0] = V.a.re;
   out[(size_t)s * 4 + 1] = V.a.im;
   out[(size_t)s * 4 + 2] = V.b.re;
@@ -624,7 +632,7 @@ __global__ void debug_force_kernel(const ChainDev* chp, int eo, double* out) {
   if (s >= ch.nh) return;
   Coord X = site_coord(eo, s, ch.hx, ch.nxy, ch.dhx, ch.dnxy);
   R f1, f2, f3;
-  higgs_force<R>(ch, eo, X, s, f1, f2, f3);
+  higgs_force<R>(ch, eo, nbr_offsets(ch, X), s, f1, f2, f3);
   out[(size_t)s * 3 + 0] = f1;
   out[(size_t)s * 3 + 1] = f2;
   out[(size_t)s * 3 + 2] = f3;
@@ -633,35 +641,59 @@ __global__ void debug_force_kernel(const ChainDev* chp, int eo, double* out) {
 // ------------------------------------------------------------------ launchers
 // The pass kernels and the finalize kernel are launched with programmatic
 // dependent launch (lce_common.cuh: launch_pdl / pdl_wait).
-template <typename R, int SPT>
+template <typename R, int SPT, int BS>
 void launch_higgs_t(int mode, const PassArgs& a, int nblocks, cudaStream_t s) {
-  void (*k)(PassArgs) =
-      mode == 0 ? higgs_kernel<R, 0, SPT> : (mode == 1 ? higgs_kernel<R, 1, SPT> : higgs_kernel<R, 2, SPT>);
-  (void)launch_pdl(k, nblocks, kBlock, 0, s, a);
+  void (*k)(PassArgs) = mode == 0 ? higgs_kernel<R, 0, SPT, BS>
+                                  : (mode == 1 ? higgs_kernel<R, 1, SPT, BS> : higgs_kernel<R, 2, SPT, BS>);
+  (void)launch_pdl(k, nblocks, BS, 0, s, a);
 }
 
-template <typename R, int SPT>
+template <typename R, int SPT, int BS>
 void launch_link_t(int mode, int mu, const PassArgs& a, int nblocks, cudaStream_t s) {
   void (*k)(PassArgs);
   if (mode == 0)
-    k = mu == 0 ? link_kernel<R, 0, 0, SPT> : (mu == 1 ? link_kernel<R, 1, 0, SPT> : link_kernel<R, 2, 0, SPT>);
+    k = mu == 0 ? link_kernel<R, 0, 0, SPT, BS> : (mu == 1 ? link_kernel<R, 1, 0, SPT, BS> : link_kernel<R, 2, 0, SPT, BS>);
   else if (mode == 1)
-    k = mu == 0 ? link_kernel<R, 0, 1, SPT> : (mu == 1 ? link_kernel<R, 1, 1, SPT> : link_kernel<R, 2, 1, SPT>);
+    k = mu == 0 ? link_kernel<R, 0, 1, SPT, BS> : (mu == 1 ? link_kernel<R, 1, 1, SPT, BS> : link_kernel<R, 2, 1, SPT, BS>);
   else
-    k = mu == 0 ? link3_kernel<R, 0, SPT> : (mu == 1 ? link3_kernel<R, 1, SPT> : link3_kernel<R, 2, SPT>);
-  (void)launch_pdl(k, nblocks, kBlock, 0, s, a);
+    k = mu == 0 ? link3_kernel<R, 0, SPT, BS> : (mu == 1 ? link3_kernel<R, 1, SPT, BS> : link3_kernel<R, 2, SPT, BS>);
+  (void)launch_pdl(k, nblocks, BS, 0, s, a);
 }
 
+// Tile shapes compiled: FP32 (BS, SPT) in {128, 256, 512} x {1} and
+// {128, 256} x {2}; the FP64 validation path only BS = 256.
 template <typename R>
 void launch_higgs(int mode, const PassArgs& a, int nblocks, cudaStream_t s) {
-  if (a.spt == 2) launch_higgs_t<R, 2>(mode, a, nblocks, s);
-  else launch_higgs_t<R, 1>(mode, a, nblocks, s);
+  if constexpr (sizeof(R) == 4) {
+    if (a.bs == 128) {
+      if (a.spt == 2) launch_higgs_t<R, 2, 128>(mode, a, nblocks, s);
+      else launch_higgs_t<R, 1, 128>(mode, a, nblocks, s);
+      return;
+    }
+    if (a.bs == 512) {
+      launch_higgs_t<R, 1, 512>(mode, a, nblocks, s);
+      return;
+    }
+  }
+  if (a.spt == 2) launch_higgs_t<R, 2, 256>(mode, a, nblocks, s);
+  else launch_higgs_t<R, 1, 256>(mode, a, nblocks, s);
 }
 
 template <typename R>
 void launch_link(int mode, int mu, const PassArgs& a, int nblocks, cudaStream_t s) {
-  if (a.spt == 2) launch_link_t<R, 2>(mode, mu, a, nblocks, s);
-  else launch_link_t<R, 1>(mode, mu, a, nblocks, s);
+  if constexpr (sizeof(R) == 4) {
+    if (a.bs == 128) {
+      if (a.spt == 2) launch_link_t<R, 2, 128>(mode, mu, a, nblocks, s);
+      else launch_link_t<R, 1, 128>(mode, mu, a, nblocks, s);
+      return;
+    }
+    if (a.bs == 512) {
+      launch_link_t<R, 1, 512>(mode, mu, a, nblocks, s);
+      return;
+    }
+  }
+  if (a.spt == 2) launch_link_t<R, 2, 256>(mode, mu, a, nblocks, s);
+  else launch_link_t<R, 1, 256>(mode, mu, a, nblocks, s);
 }
 
 void launch_finalize(const FinalizeArgs& f, cudaStream_t s) {

@@ -59,6 +59,7 @@ class Params:
     gf_angle: str = "atan2"
     sweep_mode: str = "auto"
     agauge_hits: int = 1
+    tile_threads: int = 0
 
     def to_c(self) -> LceParams:
         p = LceParams()
@@ -78,6 +79,7 @@ class Params:
         p.gf_angle = {"acos": _lib.LCE_GF_ACOS, "atan2": _lib.LCE_GF_ATAN2}[self.gf_angle]
         p.sweep_mode = SWEEP_MODES[self.sweep_mode]
         p.agauge_hits = int(self.agauge_hits)
+        p.tile_threads = int(self.tile_threads)
         return p
 
 
@@ -236,6 +238,12 @@ class _Context:
 
     def sweeps(self, n: int, measflag: int = 0):
         self._ck(self.lib.lce_sweeps(self.h, int(n), measflag))
+
+    def tile_shape(self):
+        """(threads per block, sites per thread) of the update kernels in use."""
+        bs, spt = C.c_int(), C.c_int()
+        self._ck(self.lib.lce_get_tile_shape(self.h, C.byref(bs), C.byref(spt)))
+        return bs.value, spt.value
 
     def sweep_mode(self) -> str:
         m = self._ck(self.lib.lce_get_sweep_mode(self.h))

@@ -320,7 +320,7 @@ def test_persistent_batch_and_autotune():
     for mode in ("passes", "persistent", "auto"):
         ens = Ensemble([Params(**{**s.__dict__, "sweep_mode": mode}) for s in specs])
         ens.init_hot(3)
-        ens.sweeps(12, 1)
+        ens.sweeps(30, 1)
         if mode == "auto":
             assert ens.sweep_mode() in ("passes", "passes2", "persistent")
         outs.append(([ens.download(chain=i) for i in range(2)], ens.meas_batch()))
@@ -448,7 +448,7 @@ def test_two_sites_per_thread_batch_and_three_way_autotune():
     for mode in ("passes", "passes2", "auto"):
         ens = Ensemble([Params(**{**s.__dict__, "sweep_mode": mode}) for s in specs])
         ens.init_hot(3)
-        ens.sweeps(16, 1)
+        ens.sweeps(30, 1)
         if mode == "auto":
             assert ens.sweep_mode() in ("passes", "passes2", "persistent")
         outs.append([ens.download(chain=i) for i in range(3)])
@@ -456,3 +456,79 @@ def test_two_sites_per_thread_batch_and_three_way_autotune():
         for i in range(3):
             np.testing.assert_array_equal(o[i][0], outs[0][i][0])
             np.testing.assert_array_equal(o[i][1], outs[0][i][1])
+
+
+SHAPES = [(256, "passes"), (128, "passes"), (512, "passes"), (128, "passes2"), (256, "passes2")]
+
+
+@pytest.mark.parametrize("L", [(16, 8, 12), (64, 32, 34)])
+def test_tile_shapes_update_identically(L):
+    """Every tile shape of the per-pass kernels (128, 256 or 512 threads per
+    block; one or two sites per thread) updates every site exactly as the
+    others; only the grouping of the FP64 measurement sums differs."""
+    res = []
+    for bs, mode in SHAPES:
+        g = Lattice(L, beta=12.0, x=0.09, y=0.3, seed=77, sweep_mode=mode, tile_threads=bs, n_link_or=1,
+                    n_higgs_metro=1)
+        g.init_hot(8)
+        ms = [g.sweep(1) for _ in range(3)]
+        assert g.tile_shape() == (bs, 2 if mode == "passes2" else 1)
+        res.append((g.download(), ms, g.rng_position()))
+        g.close()
+    for (u, a), ms, pos in res[1:]:
+        np.testing.assert_array_equal(u, res[0][0][0])
+        np.testing.assert_array_equal(a, res[0][0][1])
+        assert pos == res[0][2]
+        for m0, m1 in zip(res[0][1], ms):
+            for k in ("plaq", "akin", "a2", "a4", "acc_gauge", "acc_hb", "acc_or", "acc_metro", "acc_link_or"):
+                assert abs(m0[k] - m1[k]) <= 1e-12 * max(1.0, abs(m0[k])), k
+
+
+def test_tile_shapes_batch_of_uneven_volumes():
+    specs = [Params(L=(16, 16, 16), beta=6.0, x=0.1, y=0.1, seed=5),
+             Params(L=(8, 12, 6), beta=16.0, x=0.08, y=0.5, seed=6, imode=1),
+             Params(L=(34, 8, 8), beta=9.0, x=0.1, y=0.3, seed=7)]
+    outs = []
+    for bs, mode in SHAPES:
+        ens = Ensemble([Params(**{**s.__dict__, "sweep_mode": mode, "tile_threads": bs}) for s in specs])
+        ens.init_hot(3)
+        ens.sweeps(4, 1)
+        outs.append([ens.download(chain=i) for i in range(3)])
+        ens.close()
+    for o in outs[1:]:
+        for i in range(3):
+            np.testing.assert_array_equal(o[i][0], outs[0][i][0])
+            np.testing.assert_array_equal(o[i][1], outs[0][i][1])
+
+
+def test_autotune_chooses_form_and_tile_shape():
+    """LCE_SWEEP_AUTO times every candidate (per-pass forms at each tile
+    shape, and the persistent form) on real sweeps and keeps one; with
+    tile_threads fixed only that block size is a per-pass candidate.  The
+    fields equal a fixed-shape run's."""
+    L = (32, 32, 32)
+    ref = Lattice(L, beta=12.0, x=0.09, y=0.3, seed=3, sweep_mode="passes", tile_threads=256)
+    ref.init_hot(1)
+    ref.sweeps(30, 0)
+    u_ref, a_ref = ref.download()
+    ref.close()
+    for req in (0, 128):
+        g = Lattice(L, beta=12.0, x=0.09, y=0.3, seed=3, sweep_mode="auto", tile_threads=req)
+        g.init_hot(1)
+        g.sweeps(30, 0)
+        mode = g.sweep_mode()
+        bs, spt = g.tile_shape()
+        assert mode in ("passes", "passes2", "persistent")
+        if mode == "persistent":
+            assert (bs, spt) == (256, 1)
+        else:
+            assert bs in ((128, 256, 512) if req == 0 else (req,)) and spt == (2 if mode == "passes2" else 1)
+        u, a = g.download()
+        g.close()
+        np.testing.assert_array_equal(u, u_ref)
+        np.testing.assert_array_equal(a, a_ref)
+
+
+def test_tile_threads_rejected_when_invalid():
+    with pytest.raises(LceError):
+        Lattice((8, 8, 8), tile_threads=64)

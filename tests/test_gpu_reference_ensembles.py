@@ -1,0 +1,135 @@
+"""Production ensembles against the reference's CPU ensembles, at 2 sigma.
+
+The plain-method workload's lattice and couplings (16^3, beta = 9, x = 0.1,
+y = 0.45) with the reference's own sweep (f/main.f:38-41: ahiggs2, ahiggs3,
+agauge, renorm) from its init = 2 cold start (U = 1, A0 = (0, 0, 1),
+f/confget.f:295-307):
+
+* the GPU's FP32 production path (lce_sweep, one CUDA graph per sweep,
+  Philox uniforms; Landau gauge fixed to theta < 1e-10 by the
+  conjugate-gradient Fourier-accelerated iteration from the previous
+  transform), and
+* the CPU oracle in FP64 (its routines reproduce the reference's own Fortran
+  at 1e-12, tests/test_oracle_vs_reference.py; gauge fixed by the reference's
+  overrelaxed iteration from G = 1, as f/landau_gauge.f does),
+
+each as R = 4 independent chains (Philox keys fixed below, different on the
+two sides), 300 thermalisation and 3000 measurement sweeps per chain.
+
+Compared, as the north star names them: the plaquette, <Tr A0^2>, the
+Polyakov loop (root of f/polyakov.f's first output, the squared slice mean of
+cos(4|A0|)), and the correlator masses: the effective mass log(C(1)/C(2)) of
+the zero-momentum A0 and link correlators of f/correlator.f, every 10th
+sweep (the log ratio, not the cosh form, because both correlators carry a
+constant disconnected part that makes the cosh form undefined).
+Errors: per chain autocorrelation-corrected (Madras-Sokal window), combined
+over the chains; masses by jackknife over 20 contiguous bins (5 per chain).
+Each |z| must be below 2.
+
+For a true match each |z| < 2 holds with probability 0.954, so the five
+together pass 79% of the time; the seeds and statistics were fixed before the
+first run and are not changed after a failure.  The z-scores and their chi^2
+are printed.
+"""
+import os
+
+import numpy as np
+import pytest
+
+from lceqcd_b200.analysis import jackknife, mean_err
+
+pytestmark = pytest.mark.gpu
+lce = pytest.importorskip("lceqcd_b200")
+from lceqcd_b200 import Ensemble, Params  # noqa: E402
+from oracle.oracle import Oracle  # noqa: E402
+
+L = (16, 16, 16)
+COUP = dict(beta=9.0, x=0.1, y=0.45)
+R, NTHERM, NMEAS, EVERY = 4, 300, 3000, 10
+GPU_KEYS = (1001, 1002, 1003, 1004)
+CPU_KEYS = (2001, 2002, 2003, 2004)
+
+
+def gpu_runs():
+    ens = Ensemble([Params(L=L, **COUP, lam=1.7, limit_or=1e-10, precision="f32", seed=k) for k in GPU_KEYS])
+    ens.init_unit(1.0)
+    ens.sweeps(NTHERM, 0)
+    out = [dict(plaq=[], a2=[], pol=[], ca=[], cu=[]) for _ in range(R)]
+    for k in range(NMEAS):
+        ens.sweeps(1, 1)
+        ms = ens.meas_batch()
+        for i in range(R):
+            out[i]["plaq"].append(ms[i]["plaq"])
+            out[i]["a2"].append(ms[i]["a2"])
+            out[i]["pol"].append(np.sqrt(ens.polyakov(chain=i)[2]))
+            if (k + 1) % EVERY == 0:
+                th, _, _ = ens.landau_gauge_fourier_cg("transform" if k + 1 > EVERY else "identity", chain=i)
+                assert th <= 1e-10
+                ca, cu, _, _ = ens.correlator(chain=i)
+                out[i]["ca"].append(ca)
+                out[i]["cu"].append(cu)
+    ens.close()
+    return [{k: np.array(v) for k, v in o.items()} for o in out]
+
+
+def cpu_runs():
+    threads = os.cpu_count() or 1
+    out = []
+    for key in CPU_KEYS:
+        o = Oracle(L, COUP["beta"], COUP["x"], COUP["y"], lam=1.7, limit_or=1e-10, bits=64, threads=threads)
+        o.unitconf(1.0)
+        o.set_philox(key, 0)
+        for _ in range(NTHERM):
+            o.sweep(0)
+        r = dict(plaq=[], a2=[], pol=[], ca=[], cu=[])
+        for k in range(NMEAS):
+            m = o.sweep(1)
+            r["plaq"].append(m["plaq"])
+            r["a2"].append(m["a2"])
+            r["pol"].append(np.sqrt(o.polyakov()[2]))
+            if (k + 1) % EVERY == 0:
+                th, _ = o.landau_gauge(0)
+                assert th <= 1e-10
+                ca, cu, _ = o.correlator()
+                r["ca"].append(ca)
+                r["cu"].append(cu)
+        out.append({k: np.array(v) for k, v in r.items()})
+    return out
+
+
+@pytest.fixture(scope="module")
+def runs():
+    return {"gpu": gpu_runs(), "cpu": cpu_runs()}
+
+
+def pooled(chains, obs):
+    """Mean over the chains of each chain's mean; error from the chains'
+    autocorrelation-corrected errors."""
+    ests = [mean_err(c[obs]) for c in chains]
+    return float(np.mean([e[0] for e in ests])), float(np.sqrt(sum(e[1] ** 2 for e in ests)) / len(ests))
+
+
+def mass(chains, obs, z=1):
+    samples = np.concatenate([c[obs] for c in chains])
+    return jackknife(lambda c: np.log(c[z] / c[z + 1]), samples)
+
+
+OBS = ["plaq", "a2", "pol", "m_A0", "m_link"]
+ZS = {}
+
+
+@pytest.mark.parametrize("obs", OBS)
+def test_gpu_ensemble_matches_reference_cpu_ensemble(runs, obs):
+    if obs.startswith("m_"):
+        key = "ca" if obs == "m_A0" else "cu"
+        a, b = mass(runs["gpu"], key), mass(runs["cpu"], key)
+    else:
+        a, b = pooled(runs["gpu"], obs), pooled(runs["cpu"], obs)
+    assert np.isfinite(a[0]) and np.isfinite(b[0]) and a[1] > 0 and b[1] > 0
+    z = (a[0] - b[0]) / np.hypot(a[1], b[1])
+    ZS[obs] = z
+    print(f"{obs}: GPU f32 {a[0]:.6f}+-{a[1]:.6f}  CPU f64 {b[0]:.6f}+-{b[1]:.6f}  z={z:+.2f}")
+    if len(ZS) == len(OBS):
+        chi2 = sum(v * v for v in ZS.values())
+        print(f"chi^2 of the {len(OBS)} z-scores: {chi2:.2f}")
+    assert abs(z) < 2.0
