@@ -320,34 +320,49 @@ def extras(args, peak):
         rows = {"plain_identity": [], "plain_warm": [], "fourier_warm": [], "fourier_cg_warm": []}
 
         def timed(fn):
+            # device time between CUDA events on the context stream around the
+            # whole fixing (the library's host loop included)
             lat.synchronize()
-            t0 = time.perf_counter()
+            lat.timer_start()
             th, it = fn()
-            lat.synchronize()
-            return (time.perf_counter() - t0, it, th, lat.gauge_functional())
+            ms = lat.timer_stop()
+            return (ms / 1e3, it, th, lat.gauge_functional())
 
-        for _ in range(2):
+        n_all, n_cg, n_plain_warm = 10, 50, 2
+        for k in range(n_cg):
             lat.sweeps(10, 0)
             G = lat.get_transform()
-            rows["plain_identity"].append(timed(lambda: lat.landau_gauge(max_iters=300000)))
-            lat.set_transform(G)
-            rows["plain_warm"].append(timed(lambda: lat.landau_gauge_from("transform", max_iters=300000)[1:]))
-            lat.set_transform(G)
-            rows["fourier_warm"].append(
-                timed(lambda: (lambda r: (r[0], r[1] + r[2]))(lat.landau_gauge_fourier("transform"))))
-            lat.set_transform(G)
+            if k < n_all:
+                rows["plain_identity"].append(timed(lambda: lat.landau_gauge(max_iters=300000)))
+                if k < n_plain_warm:
+                    lat.set_transform(G)
+                    rows["plain_warm"].append(
+                        timed(lambda: lat.landau_gauge_from("transform", max_iters=300000)[1:]))
+                lat.set_transform(G)
+                rows["fourier_warm"].append(
+                    timed(lambda: (lambda r: (r[0], r[1] + r[2]))(lat.landau_gauge_fourier("transform"))))
+                lat.set_transform(G)
             rows["fourier_cg_warm"].append(
                 timed(lambda: (lambda r: (r[0], r[1] + r[2]))(lat.landau_gauge_fourier_cg("transform"))))
-        gf = {"limit": 1e-10, "configs": 2, "omega_or": 1.7}
+        gf = {"limit": 1e-10, "omega_or": 1.7,
+              "configs": {k: len(v) for k, v in rows.items()},
+              "timing": "CUDA events on the context stream around each fixing",
+              "configurations": "thermalised 128^3 (beta 12, x 0.09, y 0.3), 10 sweeps apart; plain_identity, "
+                                "fourier_warm and the first 10 fourier_cg_warm on the same configurations",
+              "warm_start": "from the previous configuration's converged transform; every fixing runs to "
+                            "theta < 1e-10"}
         for k, rs in rows.items():
-            gf[k] = {"s_per_config": statistics.mean(r[0] for r in rs), "iterations": [r[1] for r in rs],
-                     "theta": [r[2] for r in rs], "functional": [r[3] for r in rs]}
-        gf["iterations_plain_identity_over_fourier_warm"] = (sum(gf["plain_identity"]["iterations"]) /
-                                                             sum(gf["fourier_warm"]["iterations"]))
+            gf[k] = {"s_per_config": statistics.mean(r[0] for r in rs),
+                     "mean_iterations": statistics.mean(r[1] for r in rs),
+                     "iterations": [r[1] for r in rs], "theta_max": max(r[2] for r in rs),
+                     "functional_mean": statistics.mean(r[3] for r in rs)}
+        same = rows["fourier_cg_warm"][:n_all]
+        gf["iterations_plain_identity_over_fourier_warm"] = (sum(r[1] for r in rows["plain_identity"]) /
+                                                             sum(r[1] for r in rows["fourier_warm"]))
         gf["time_plain_identity_over_fourier_warm"] = (gf["plain_identity"]["s_per_config"] /
                                                        gf["fourier_warm"]["s_per_config"])
-        gf["time_plain_identity_over_fourier_cg_warm"] = (gf["plain_identity"]["s_per_config"] /
-                                                          gf["fourier_cg_warm"]["s_per_config"])
+        gf["time_plain_identity_over_fourier_cg_warm_same_configs"] = (
+            gf["plain_identity"]["s_per_config"] / statistics.mean(r[0] for r in same))
         gf["plain_hbm_gbs"] = statistics.mean(216 * vol(L) * r[1] / r[0] / 1e9 for r in rows["plain_identity"])
         out["gauge_fix_128cubed"] = gf
         lat.close()
@@ -413,7 +428,14 @@ def extras(args, peak):
                                      "bound": "tensor", "peak_tflops": bf16_peak,
                                      "frac_of_measured_bf16": tf / bf16_peak if bf16_peak else None,
                                      "note": "host wall clock around synchronised training calls; 27 x 16 x 16 "
-                                             "per-site contractions, 3 per step"}
+                                             "per-site contractions, 3 per step",
+                                     "judge_rule": "the warm start's judge takes, of the identity, the previous "
+                                                   "transform and the network's start, the one with the highest "
+                                                   "gauge functional, not the lowest theta as the north star words "
+                                                   "it: the previous transform starts at a worse theta (~7 against "
+                                                   "~4.5 from G = 1) yet converges in 1.3-2x fewer iterations; the "
+                                                   "plain iteration then runs to theta < limit_or from the start "
+                                                   "taken"}
         net.close()
         lat.close()
     except Exception as e:
@@ -632,6 +654,16 @@ def run_gpu(args):
             line["cpu_baseline"] = {"value": None, "unit": UNIT, "cores": 0, "kind": "port", "sample": repr(e)[:200]}
         if args.extras:
             line["secondary"] = extras(args, peak)
+            # the larger volumes' sweep and link-kernel fractions, beside the
+            # headline kernel's (the same figures as in secondary)
+            byvol = {}
+            for key in ("sweep_128cubed", "sweep_256cubed", "sweep_128cubed_hb_4or"):
+                r = line["secondary"].get(key, {})
+                if "sweep_frac_of_measured_hbm" in r:
+                    byvol[key] = {"sweep_frac": r["sweep_frac_of_measured_hbm"],
+                                  "link_kernel_frac": r["link_kernel_frac_of_measured_hbm"],
+                                  "tile_shape": r.get("tile_shape"), "sweep_mode": r.get("sweep_mode")}
+            line["roofline"]["by_volume"] = byvol
     lat.close()
     if rank == 0:
         print(json.dumps(line), flush=True)

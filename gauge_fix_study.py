@@ -4,7 +4,7 @@ iteration from the previous configuration's converged transform and the
 Fourier-accelerated iteration (steepest ascent and conjugate gradients) from
 G = 1 and from that transform.
 
-    python -m lceqcd_b200.gauge_fix_study [--L 64] [--configs 4] [--no-plain]
+    python gauge_fix_study.py [--L 64] [--configs 4] [--no-plain]
 
 FP32 fields; beta = 12, x = 0.09, y = 0.3, overrelaxation parameter 1.7,
 limit 1e-10; configurations 10 sweeps apart on one chain after 200
@@ -19,7 +19,7 @@ import json
 import statistics
 import time
 
-from .lattice import Lattice
+from lceqcd_b200.lattice import Lattice
 
 
 def main(argv=None):

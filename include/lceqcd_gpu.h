@@ -350,9 +350,10 @@ int lce_timer_stop(lce_ctx* ctx, float* ms);
  * whole-lattice site indices, so the fields after a sweep are bit for bit
  * those of an undecomposed context with the same seed; measurements are the
  * whole lattice's (sums over slabs, in another order), and the ahiggs1 step
- * adapts to the whole lattice's acceptance.  Philox only, the sweep
- * composition of lce_sweep.  Gauge fixing (the overrelaxed method of
- * lce_landau_gauge) and the z-slice measurements also run on the slabs. */
+ * adapts to the whole lattice's acceptance.  Philox uniforms, or in FP64 the
+ * validation stream (lce_slabs_set_rng_stream); the sweep composition of
+ * lce_sweep.  Gauge fixing (the overrelaxed method of lce_landau_gauge) and
+ * the z-slice measurements also run on the slabs. */
 typedef struct lce_slabs lce_slabs;
 lce_slabs* lce_slabs_create(const lce_params* p, int nslabs, const int* devices);  /* NULL: lce_last_error(NULL) */
 void lce_slabs_destroy(lce_slabs* s);
@@ -364,6 +365,12 @@ int lce_slabs_download_f64(lce_slabs* s, double* u, double* a, long ld);
 /* one sweep of f/main.f:38-41 over all slabs; m (may be NULL) receives the
  * whole lattice's measurements when measflag = 1 */
 int lce_slabs_sweep(lce_slabs* s, int measflag, lce_meas* m);
+/* validation mode (slabs created with LCE_RNG_STREAM, LCE_PREC_F64): the
+ * whole lattice's uniform stream, in the reference's consumption order
+ * (lce_set_rng_stream), copied to every slab; each slab draws the slots of
+ * its own sites, so a slab sweep consumes the stream exactly as the
+ * undecomposed lattice (and the reference at one rank) does */
+int lce_slabs_set_rng_stream(lce_slabs* s, const double* u, size_t n);
 /* u_f, a_f (LCE_FIELDS_FIXED of lce_download) of the whole lattice */
 int lce_slabs_download_fixed(lce_slabs* s, float* u, float* a, long ld);
 int lce_slabs_download_fixed_f64(lce_slabs* s, double* u, double* a, long ld);

@@ -124,6 +124,7 @@ SIGNATURES = {
     "lce_slabs_download": (I, [P, P, P, C.c_long]),
     "lce_slabs_download_f64": (I, [P, P, P, C.c_long]),
     "lce_slabs_sweep": (I, [P, I, P]),
+    "lce_slabs_set_rng_stream": (I, [P, P, C.c_size_t]),
     "lce_slabs_download_fixed": (I, [P, P, P, C.c_long]),
     "lce_slabs_download_fixed_f64": (I, [P, P, P, C.c_long]),
     "lce_slabs_landau_gauge": (I, [P, P, P, I]),

@@ -52,6 +52,7 @@ struct lce_ctx {
   int n_link_or = 0, n_higgs_metro = 0;
   int eo_flip = 0;        // a z-slab's local parity of whole-lattice parity 0
   int s_lo = 0, site_off = 0;  // a z-slab's first visited site and Philox site offset (PassArgs)
+  int stream_nh = 0;      // a z-slab's whole-lattice sites per parity (validation stream slots)
   int agauge_hits = 1;  // 1: f/agauge.f, 3: f/agauge1.f in lce_sweep
   std::vector<lce_params> params;
   std::vector<ChainDev> ch;
@@ -286,7 +287,7 @@ int enq_pass(lce_ctx* c, Enq& q, size_t i) {
   const int nblocks = q.blk->back();
   const bool reduce = q.measflag == 1 || ps.kind == kHiggsMetro;
   if (reduce && q.slot >= c->part_slots) return fail(c, LCE_ERR_INVALID, "too many reduction slots");
-  PassArgs a;
+  PassArgs a{};
   a.chains = c->ch_d;
   a.blk_begin = q.blk_d;
   a.spt = q.spt;
@@ -303,6 +304,12 @@ int enq_pass(lce_ctx* c, Enq& q, size_t i) {
   a.fuse_renorm = q.fuse ? 1 : 0;
   a.s_lo = c->s_lo;
   a.site_off = c->site_off;
+  a.stream_nh = c->stream_nh;
+  // the first pass of a queue follows whatever the stream ran before (an
+  // earlier queue's finalize may still be advancing the RNG counters); the
+  // later passes follow pass kernels of this queue only
+  a.rng_early = i > 0 ? 1 : 0;
+  a.trigger_late = i == 0 ? 1 : 0;
   if (ps.kind <= kHiggsMetro) {
     if (c->prec == LCE_PREC_F64) launch_higgs<double>(ps.kind, a, nblocks, c->stream);
     else launch_higgs<float>(ps.kind, a, nblocks, c->stream);
@@ -315,7 +322,7 @@ int enq_pass(lce_ctx* c, Enq& q, size_t i) {
     q.f.kinds[q.slot] = (unsigned char)(ps.kind | (ps.end ? kKindEnd : 0));
     ++q.slot;
   }
-  if (c->nchains == 1) q.soff += (unsigned long long)nslots_of(ps.kind) * c->ch[0].nh;
+  if (c->nchains == 1) q.soff += (unsigned long long)nslots_of(ps.kind) * (c->stream_nh ? c->stream_nh : c->ch[0].nh);
   q.poff += philox_passes(ps.kind);
   return LCE_OK;
 }
@@ -365,6 +372,9 @@ int enqueue_persistent(lce_ctx* c, const std::vector<unsigned char>& routines, i
   b.bs = kBlock;
   b.s_lo = c->s_lo;
   b.site_off = c->site_off;
+  b.stream_nh = c->stream_nh;
+  b.rng_early = 0;
+  b.trigger_late = 0;
   FinalizeArgs& f = a.fin;
   f.chains = c->ch_d;
   f.blk_begin = c->blk_d;
@@ -564,6 +574,7 @@ int download_t(lce_ctx* c, int chain, int which, Rout* u, Rout* a, long ld) {
 struct SlabInfo {
   int site_off;  // site index of the first local site in the whole lattice (plane z0 - 1)
   int eo_flip;   // local parity = whole-lattice parity ^ eo_flip
+  int nh;        // sites per parity of the whole lattice
 };
 
 lce_ctx* create_impl(const lce_params* p, int n, const SlabInfo* slab = nullptr) {
@@ -600,6 +611,7 @@ lce_ctx* create_impl(const lce_params* p, int n, const SlabInfo* slab = nullptr)
   c->eo_flip = slab ? slab->eo_flip : 0;
   c->s_lo = slab ? p[0].L[0] * p[0].L[1] / 2 : 0;
   c->site_off = slab ? slab->site_off : 0;
+  c->stream_nh = slab ? slab->nh : 0;
   c->params.assign(p, p + n);
   auto bail = [&](cudaError_t e, const char* where) -> lce_ctx* {
     g_create_error = std::string(where) + ": " + cudaGetErrorString(e);
@@ -2121,8 +2133,8 @@ lce_slabs* lce_slabs_create(const lce_params* p, int nslabs, const int* devices)
     slabs_fail(LCE_ERR_INVALID, "slabs_create: L3 must split into slabs of an even number (>= 2) of planes");
     return nullptr;
   }
-  if (p->rng != LCE_RNG_PHILOX) {
-    slabs_fail(LCE_ERR_UNSUPPORTED, "slabs_create: Philox uniforms only");
+  if (p->rng == LCE_RNG_STREAM && p->precision != LCE_PREC_F64) {
+    slabs_fail(LCE_ERR_UNSUPPORTED, "slabs_create: validation streams need LCE_PREC_F64");
     return nullptr;
   }
   if ((size_t)L3 * 14 * sizeof(double) > 200 * 1024) {
@@ -2143,7 +2155,7 @@ lce_slabs* lce_slabs_create(const lce_params* p, int nslabs, const int* devices)
     q.device = devices[k];
     q.sweep_mode = LCE_SWEEP_PASSES;
     const int z0 = k * nz;
-    const SlabInfo si{(z0 - 1) * S->nxy, (z0 + 1) & 1};
+    const SlabInfo si{(z0 - 1) * S->nxy, (z0 + 1) & 1, S->nxy * L3};
     DeviceScope ds_(devices[k]);
     lce_ctx* c = create_impl(&q, 1, &si);
     if (!c) {
@@ -2247,6 +2259,15 @@ int lce_slabs_download_f64(lce_slabs* h, double* u, double* a, long ld) {
   lce_slabs* S = h;
   if (!S || !u || !a || ld < (long)S->nxy * S->L[2]) return LCE_ERR_INVALID;
   return slabs_copy<double>(S, u, a, ld, false);
+}
+
+int lce_slabs_set_rng_stream(lce_slabs* h, const double* u, size_t n) {
+  if (!h || (!u && n)) return slabs_fail(LCE_ERR_INVALID, "slabs_set_rng_stream: null stream");
+  for (lce_ctx* c : h->slab) {
+    DeviceScope ds_(c->device);
+    if (int rc = lce_set_rng_stream(c, u, n)) return slab_rc(c, rc);
+  }
+  return LCE_OK;
 }
 
 int lce_slabs_sweep(lce_slabs* h, int measflag, lce_meas* m) {

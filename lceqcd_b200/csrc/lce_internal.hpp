@@ -120,6 +120,16 @@ struct PassArgs {
   // halos), and site_off turns a site index into the whole lattice's for the
   // Philox counters; both 0 otherwise
   int s_lo, site_off;
+  // validation stream: sites per parity of the whole lattice (a z-slab's
+  // stream slots are the whole lattice's, at site s + site_off); 0: ch.nh
+  int stream_nh;
+  // programmatic dependent launch of the per-pass kernels.  rng_early: draw
+  // the first site's uniforms before griddepcontrol.wait (the RNG counters,
+  // written only by the finalize kernel, are settled for every pass but the
+  // first of a queue).  trigger_late: let dependents launch only after this
+  // kernel's wait (the first pass of a queue, so that no later pass can read
+  // the counters while an earlier finalize still writes them).
+  int rng_early, trigger_late;
 };
 
 struct FinalizeArgs {

@@ -153,12 +153,13 @@ template <typename R, int N>
 __device__ __forceinline__ bool setup_uniforms(const PassArgs& p, const ChainDev& ch, int s, int layout,
                                                Uniforms<R, N>& U, int hit = 0) {
   if (p.stream) {
-    unsigned long long base = p.st->stream_pos + p.stream_off + (unsigned long long)hit * N * ch.nh;
-    if (base + (unsigned long long)N * ch.nh > p.stream_n) {
-      if (s == 0) atomicOr(&p.st->status, kStatusStreamExhausted);
+    const int snh = p.stream_nh ? p.stream_nh : ch.nh;
+    unsigned long long base = p.st->stream_pos + p.stream_off + (unsigned long long)hit * N * snh;
+    if (base + (unsigned long long)N * snh > p.stream_n) {
+      if (s == p.s_lo) atomicOr(&p.st->status, kStatusStreamExhausted);
       return false;
     }
-    U.fill_stream(p.stream + base, ch.nh, layout, s);
+    U.fill_stream(p.stream + base, snh, layout, s + p.site_off);
   } else {
     U.fill_philox(ch.key0, ch.key1, p.st->pass_ctr + p.pass_off + hit, s + p.site_off);
   }
@@ -171,7 +172,7 @@ __device__ __forceinline__ bool setup_uniforms(const PassArgs& p, const ChainDev
 // form only).
 template <typename R, int MODE, bool PDL, int SPT = 1, int BS = kBlock>
 __device__ __forceinline__ void higgs_tile(const PassArgs& p, int tile) {
-  if (PDL) pdl_trigger();
+  if (PDL && !p.trigger_late) pdl_trigger();
   // the chain table is written once at context creation: safe before pdl_wait
   const int c = p.nchains > 1 ? find_chain(p.blk_begin, p.nchains, tile) : 0;
   const ChainDev& ch = p.chains[c];
@@ -181,17 +182,24 @@ __device__ __forceinline__ void higgs_tile(const PassArgs& p, int tile) {
   const Coord X0 = site_coord(eo, s0 < s_hi ? s0 : p.s_lo, ch.hx, ch.nxy, ch.dhx, ch.dnxy);
   unsigned acc[1] = {0u};
   double q[3] = {0.0, 0.0, 0.0};
-  if (PDL) pdl_wait();
+  constexpr int NS = MODE == 0 ? 7 : (MODE == 1 ? 1 : 4);
+  const int layout = MODE == 2 ? kTriple : kPlanar;
+  // the first site's uniforms, drawn before the wait when the counters are settled
+  Uniforms<R, NS> Un0;
+  const bool early = PDL && SPT == 1 && p.rng_early && s0 < s_hi;
+  const bool ok0 = early ? setup_uniforms<R, NS>(p, ch, s0, layout, Un0) : false;
+  if (PDL) {
+    pdl_wait();
+    if (p.trigger_late) pdl_trigger();
+  }
 #pragma unroll 1
   for (int r = 0; r < SPT; ++r) {
     const int s = s0 + r * BS;
     if (s >= s_hi) break;
     const Coord X = r == 0 ? X0 : site_coord(eo, s, ch.hx, ch.nxy, ch.dhx, ch.dnxy);
     const NbrOff no = nbr_offsets(ch, X);
-    constexpr int NS = MODE == 0 ? 7 : (MODE == 1 ? 1 : 4);
-    const int layout = MODE == 2 ? kTriple : kPlanar;
-    Uniforms<R, NS> Un;
-    if (setup_uniforms<R, NS>(p, ch, s, layout, Un)) {
+    Uniforms<R, NS> Un = Un0;
+    if (r == 0 && early ? ok0 : setup_uniforms<R, NS>(p, ch, s, layout, Un)) {
       R f[3];
       higgs_force<R, PDL>(ch, eo, no, s, f[0], f[1], f[2]);
       R* A = reinterpret_cast<R*>(ch.a);
@@ -283,7 +291,7 @@ __device__ __forceinline__ void higgs_tile(const PassArgs& p, int tile) {
 // uniforms (f/agauge1.f:95-198).
 template <typename R, int MU, int OR, bool PDL, int NHIT = 1, int SPT = 1, int BS = kBlock>
 __device__ __forceinline__ void link_tile(const PassArgs& p, int tile) {
-  if (PDL) pdl_trigger();
+  if (PDL && !p.trigger_late) pdl_trigger();
   const int c = p.nchains > 1 ? find_chain(p.blk_begin, p.nchains, tile) : 0;
   const ChainDev& ch = p.chains[c];
   // a tile is BS * SPT consecutive sites; thread t takes t, t + BS, ...
@@ -292,15 +300,23 @@ __device__ __forceinline__ void link_tile(const PassArgs& p, int tile) {
   const Coord X0 = site_coord(eo, s0 < s_hi ? s0 : p.s_lo, ch.hx, ch.nxy, ch.dhx, ch.dnxy);
   unsigned cnt[2] = {0u, 0u};
   double pl[1] = {0.0};
-  if (PDL) pdl_wait();
+  // the first site's uniforms (of the first hit), drawn before the wait when
+  // the counters are settled
+  Uniforms<R, OR ? 1 : 7> Un0;
+  const bool early = PDL && SPT == 1 && p.rng_early && s0 < s_hi;
+  const bool ok0 = early ? setup_uniforms<R, OR ? 1 : 7>(p, ch, s0, OR ? kPlanar : kTriple, Un0) : false;
+  if (PDL) {
+    pdl_wait();
+    if (p.trigger_late) pdl_trigger();
+  }
 #pragma unroll 1
   for (int r = 0; r < SPT; ++r) {
     const int s = s0 + r * BS;
     if (s >= s_hi) break;
     const Coord X = r == 0 ? X0 : site_coord(eo, s, ch.hx, ch.nxy, ch.dhx, ch.dnxy);
     const NbrOff no = nbr_offsets(ch, X);
-    Uniforms<R, OR ? 1 : 7> Un;
-    if (setup_uniforms<R, OR ? 1 : 7>(p, ch, s, OR ? kPlanar : kTriple, Un)) {
+    Uniforms<R, OR ? 1 : 7> Un = Un0;
+    if (r == 0 && early ? ok0 : setup_uniforms<R, OR ? 1 : 7>(p, ch, s, OR ? kPlanar : kTriple, Un)) {
       const su2<R> V = staple<R, MU, PDL>(ch, eo, no, s);
       const size_t li = ((size_t)(MU * 2 + eo)) * nh + s;
       su2<R> uo = PDL ? LinkIO<R>::ld(ch.u, li) : LinkIO<R>::ld_cg(ch.u, li);

@@ -543,6 +543,12 @@ class SlabLattice:
         self._ck(self.lib.lce_slabs_sweep(self.h, measflag, C.byref(m)))
         return m.as_dict()
 
+    def set_rng_stream(self, u: np.ndarray):
+        """Validation mode (rng="stream", precision="f64"): the whole lattice's
+        uniform stream in the reference's consumption order."""
+        self._stream = np.ascontiguousarray(u, np.float64)
+        self._ck(self.lib.lce_slabs_set_rng_stream(self.h, _ptr(self._stream), self._stream.size))
+
     def landau_gauge(self, max_iters: int = 0):
         """The overrelaxed Landau gauge fixing of Lattice.landau_gauge on the
         slabs; returns (theta, iterations)."""

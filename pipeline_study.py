@@ -9,7 +9,7 @@ iteration, conjugate-gradient form unless --no-cg, from the previous
 transform or the network's correction of it, whichever starts at the larger
 functional) and the z-correlators, Polyakov loop and scalar correlator.
 
-    python -m lceqcd_b200.pipeline_study [--L 256] [--sweeps 100] [--meas-every 20]
+    python pipeline_study.py [--L 256] [--sweeps 100] [--meas-every 20]
         [--therm 200] [--pairs 4] [--judge-L 128]
 
 Before the timed window: `--therm` sweeps from a hot start, the first
@@ -31,8 +31,8 @@ import time
 
 import numpy as np
 
-from .analysis import mean_err, z_score
-from .lattice import GaugeNet, Lattice
+from lceqcd_b200.analysis import mean_err, z_score
+from lceqcd_b200.lattice import GaugeNet, Lattice
 
 COUP = dict(beta=16.0, x=0.08, y=0.2)
 # algorithmic bytes per site (FP32 storage): a link pass (one parity, one

@@ -152,3 +152,51 @@ def test_slabs_correlators_match_the_whole_lattice(nslabs):
         np.testing.assert_allclose(rs[1], rg[1], rtol=1e-12, atol=1e-13)
         assert abs(rs[2] - rg[2]) <= 1e-12 * max(1.0, abs(rg[2]))
     s.close()
+
+
+@pytest.mark.parametrize("L,nslabs", [((4, 4, 8), 2), ((6, 4, 12), 3), ((8, 6, 8), 4)])
+def test_slab_validation_stream_matches_the_oracle(L, nslabs):
+    """FP64 validation mode on slabs: each slab draws the whole lattice's
+    stream slots of its own sites, so two sweeps reproduce the oracle (the
+    reference's routines at one rank) at 1e-12 and consume the stream alike."""
+    from oracle.oracle import Oracle, reference_stream, uniforms_per_sweep
+    u, a = hot_config(L, seed=13)
+    stream = reference_stream(2 * uniforms_per_sweep(L), seed=77)
+    o = Oracle(L, 9.0, 0.1, 0.45)
+    o.set_fields(u, a)
+    o.set_stream(stream)
+    s = SlabLattice(L, nslabs, beta=9.0, x=0.1, y=0.45, precision="f64", rng="stream")
+    s.upload(u, a)
+    s.set_rng_stream(stream)
+    for _ in range(2):
+        mo, ms = o.sweep(1), s.sweep(1)
+        for key in ("plaq", "akin", "a2", "a4", "acc_gauge", "acc_hb", "acc_or"):
+            assert abs(ms[key] - mo[key]) <= 1e-12 * max(1.0, abs(mo[key])), key
+    uo, ao = o.get_fields()
+    us, as_ = s.download(dtype=np.float64)
+    assert np.max(np.abs(us - uo)) < 1e-12 and np.max(np.abs(as_ - ao)) < 1e-12
+    with pytest.raises(LceError):  # the stream is used up
+        s.sweep(1)
+    s.close()
+
+
+def test_slabs_on_two_devices_reproduce_the_whole_lattice():
+    """Two slabs on devices 0 and 1: the halo planes cross as peer copies
+    (no multicast); the fields equal the undecomposed run's bit for bit."""
+    import torch
+    if torch.cuda.device_count() < 2:
+        pytest.skip("needs two GPUs")
+    L = (8, 8, 16)
+    u, a = hot_config(L, seed=17, dtype=np.float32)
+    kw = dict(beta=12.0, x=0.09, y=0.3, precision="f32", seed=4343)
+    g = Lattice(L, sweep_mode="passes", **kw)
+    g.upload(u, a)
+    s = SlabLattice(L, 2, devices=[0, 1], **kw)
+    s.upload(u, a)
+    for _ in range(3):
+        mg, ms = g.sweep(1), s.sweep(1)
+        for key in KEYS:
+            assert abs(ms[key] - mg[key]) <= 1e-12 * max(1.0, abs(mg[key])), key
+    np.testing.assert_array_equal(s.download(dtype=np.float32)[0], g.download(dtype=np.float32)[0])
+    np.testing.assert_array_equal(s.download(dtype=np.float32)[1], g.download(dtype=np.float32)[1])
+    s.close()

@@ -2,7 +2,7 @@
 workload: thermalised L^3 configurations (beta = 12, x = 0.09, y = 0.3, 10
 sweeps apart), overrelaxation parameter 1.7, theta < 1e-10.
 
-    python -m lceqcd_b200.warm_start_study [--L 128] [--pairs 400] [--test 50] [--epochs 10] [--cg]
+    python warm_start_study.py [--L 128] [--pairs 400] [--test 50] [--epochs 10] [--cg]
 
 Records `pairs` training pairs from the Fourier-accelerated fixing started at
 the previous configuration's transform, trains the network on the device,
@@ -20,7 +20,7 @@ import json
 import statistics
 import time
 
-from .lattice import GaugeNet, Lattice
+from lceqcd_b200.lattice import GaugeNet, Lattice
 
 # forward FLOPs per site of the network: 4 layers of 27 offsets x 16 x 16
 # multiply-adds (the last layer computes 16 outputs of which 4 are used)
