@@ -245,7 +245,11 @@ def settle(lat, measflag=1, limit=60):
 
 
 def kernel_profile(lat, reps=10):
-    """Per-pass durations (events between kernels) of the sweep, averaged."""
+    """Per-pass durations of the sweep, averaged over reps L2-flushed sweeps:
+    each sweep runs as a CUDA graph with a timing event after every pass on a
+    side stream (lce_profile_sweep), so the passes keep the programmatic
+    overlap they have in the timed sweeps; a pass's duration is the time
+    between its completion and the previous pass's."""
     acc = None
     for _ in range(reps):
         lat.flush_l2()

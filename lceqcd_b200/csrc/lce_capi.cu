@@ -87,6 +87,11 @@ struct lce_ctx {
   std::map<std::pair<int, int>, cudaGraphExec_t> fa_exec;
   cudaStream_t own = nullptr, stream = nullptr;
   cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+  // per-pass timing inside a sweep graph (lce_profile_sweep): a side stream
+  // with its fork/join events and one timing event per pass boundary
+  cudaStream_t side = nullptr;
+  cudaEvent_t fork_ev = nullptr, join_ev = nullptr;
+  std::vector<cudaEvent_t> prof_ev;
   // instantiated sweep graphs by (form, threads per block, sites per thread, measflag)
   std::map<std::tuple<int, int, int, int>, cudaGraphExec_t> sweep_graphs;
   GridBar* bar_d = nullptr;
@@ -1388,6 +1393,10 @@ void lce_destroy(lce_ctx* c) {
     if (q) cudaFree(q);
   if (c->ev0) cudaEventDestroy(c->ev0);
   if (c->ev1) cudaEventDestroy(c->ev1);
+  for (cudaEvent_t e : c->prof_ev) cudaEventDestroy(e);
+  if (c->fork_ev) cudaEventDestroy(c->fork_ev);
+  if (c->join_ev) cudaEventDestroy(c->join_ev);
+  if (c->side) cudaStreamDestroy(c->side);
   if (c->own) cudaStreamDestroy(c->own);
   delete c;
 }
@@ -2081,23 +2090,73 @@ int lce_flush_l2(lce_ctx* c) {
   return LCE_OK;
 }
 
+// One sweep of the per-pass form as a CUDA graph whose pass kernels are timed
+// without being disturbed: after pass i an event-record node on a side stream
+// fires when the pass has completed, while pass i + 1 keeps its
+// programmatic-dependent-launch edge to pass i (the timing nodes hang off the
+// kernel chain instead of sitting on it, as events between the launches
+// would).  ms[i] = completion of pass i minus completion of pass i - 1 (pass
+// 0: from the graph's start), ms[npasses] = the finalize kernel's; returns
+// the pass count.  The graph is built once per measflag and tile shape.
 int lce_profile_sweep(lce_ctx* c, int measflag, float* ms, int max_passes) {
   DeviceScope ds_(c ? c->device : -1);
-  if (!c || !ms) return LCE_ERR_INVALID;
-  std::vector<unsigned char> r = sweep_routines(c);
+  if (!c || !ms || max_passes < 1) return LCE_ERR_INVALID;
+  const int mf = measflag == 1 ? 1 : 0;
+  const std::vector<unsigned char> r = sweep_routines(c);
   std::vector<Pass> passes;
   for (unsigned char k : r) expand(k, passes);
   const int np = (int)passes.size();
-  std::vector<cudaEvent_t> ev(np + 1);
-  for (auto& e : ev) CK(cudaEventCreate(&e));
-  CK(cudaEventRecord(ev[0], c->stream));
-  int rc = enqueue(c, r, measflag == 1 ? 1 : 0, true, ev.data() + 1);
-  if (rc == LCE_OK) {
-    CK(cudaStreamSynchronize(c->stream));
-    for (int i = 0; i < np && i < max_passes; ++i) CK(cudaEventElapsedTime(&ms[i], ev[i], ev[i + 1]));
+  if (!c->side) {
+    CK(cudaStreamCreateWithFlags(&c->side, cudaStreamNonBlocking));
+    CK(cudaEventCreateWithFlags(&c->fork_ev, cudaEventDisableTiming));
+    CK(cudaEventCreateWithFlags(&c->join_ev, cudaEventDisableTiming));
   }
-  for (auto& e : ev) cudaEventDestroy(e);
-  return rc ? rc : np;
+  while ((int)c->prof_ev.size() < np + 2) {
+    cudaEvent_t e;
+    CK(cudaEventCreate(&e));
+    c->prof_ev.push_back(e);
+  }
+  cudaGraphExec_t* slot = &c->sweep_graphs[std::make_tuple(-1, c->tile_bs, c->tile_spt, mf)];
+  if (!*slot) {
+    cudaGraph_t g;
+    CK(cudaStreamBeginCapture(c->stream, cudaStreamCaptureModeThreadLocal));
+    cudaError_t e = cudaEventRecordWithFlags(c->prof_ev[0], c->stream, cudaEventRecordExternal);
+    Enq q;
+    int rc = LCE_OK;
+    if (e == cudaSuccess) {
+      enq_begin(c, r, mf, true, c->tile_bs, c->tile_spt, q);
+      for (int i = 0; i < np && rc == LCE_OK && e == cudaSuccess; ++i) {
+        rc = enq_pass(c, q, i);
+        if (rc == LCE_OK) e = cudaEventRecord(c->fork_ev, c->stream);
+        if (e == cudaSuccess) e = cudaStreamWaitEvent(c->side, c->fork_ev, 0);
+        if (e == cudaSuccess) e = cudaEventRecordWithFlags(c->prof_ev[i + 1], c->side, cudaEventRecordExternal);
+      }
+      if (rc == LCE_OK && e == cudaSuccess) rc = enq_end(c, q);
+      if (rc == LCE_OK && e == cudaSuccess)
+        e = cudaEventRecordWithFlags(c->prof_ev[np + 1], c->stream, cudaEventRecordExternal);
+    }
+    // rejoin the side stream whatever happened, so that the capture can end
+    const cudaError_t ej1 = cudaEventRecord(c->join_ev, c->side);
+    const cudaError_t ej2 = cudaStreamWaitEvent(c->stream, c->join_ev, 0);
+    const cudaError_t ec = cudaStreamEndCapture(c->stream, &g);
+    cudaError_t ei = cudaSuccess;
+    if (ec == cudaSuccess) {
+      if (rc == LCE_OK && e == cudaSuccess && ej1 == cudaSuccess && ej2 == cudaSuccess)
+        ei = cudaGraphInstantiate(slot, g, 0);
+      cudaGraphDestroy(g);
+    }
+    if (rc) return rc;
+    for (cudaError_t x : {e, ej1, ej2, ec, ei})
+      if (x != cudaSuccess) {
+        *slot = nullptr;
+        cudaGetLastError();
+        return cuda_fail(c, x, "profile_sweep graph");
+      }
+  }
+  CK(cudaGraphLaunch(*slot, c->stream));
+  CK(cudaStreamSynchronize(c->stream));
+  for (int i = 0; i <= np && i < max_passes; ++i) CK(cudaEventElapsedTime(&ms[i], c->prof_ev[i], c->prof_ev[i + 1]));
+  return np;
 }
 
 int lce_timer_start(lce_ctx* c) {

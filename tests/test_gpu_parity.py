@@ -532,3 +532,26 @@ def test_autotune_chooses_form_and_tile_shape():
 def test_tile_threads_rejected_when_invalid():
     with pytest.raises(LceError):
         Lattice((8, 8, 8), tile_threads=64)
+
+
+def test_profiled_sweep_graph_is_an_ordinary_sweep():
+    """lce_profile_sweep runs one sweep as a graph with timing events hung off
+    the pass kernels: it updates the fields exactly as lce_sweep does, and
+    returns one positive duration per pass (10 for the reference
+    composition)."""
+    L = (16, 8, 12)
+    a = Lattice(L, beta=12.0, x=0.09, y=0.3, seed=5, sweep_mode="passes")
+    b = Lattice(L, beta=12.0, x=0.09, y=0.3, seed=5, sweep_mode="passes")
+    for g in (a, b):
+        g.init_hot(6)
+        g.sweeps(2, 1)
+    a.sweeps(1, 1)
+    ms = b.profile_sweep(1)
+    assert len(ms) == 10 and np.all(ms > 0)
+    assert a.rng_position() == b.rng_position()
+    np.testing.assert_array_equal(a.download()[0], b.download()[0])
+    np.testing.assert_array_equal(a.download()[1], b.download()[1])
+    ms2 = b.profile_sweep(0)  # a second graph, without the measurements
+    assert len(ms2) == 10 and np.all(ms2 > 0)
+    a.close()
+    b.close()
