@@ -303,7 +303,7 @@ def extras(args, peak):
             sps = vol(L) * K / (ms / 1e3)
             bs = B_SWEEP + 6 * nor * B_LINK  # algorithmic bytes per site of this composition
             out[key] = {"site_updates_per_s": sps, "ms_per_sweep": ms / K, "sweep_mode": lat.sweep_mode(),
-                        "tile_shape": list(lat.tile_shape()),
+                        "tile_shape": list(lat.tile_shape(registers=True)),
                         "passes": 10 + 6 * nor, "bytes_per_site": bs,
                         "sweep_hbm_gbs": sps * bs / 1e9, "sweep_frac_of_measured_hbm": sps * bs / 1e9 / peak,
                         "link_kernel_ms": link,
@@ -490,7 +490,7 @@ def extras(args, peak):
         K = 20
         ms_b = timed_sweeps(ens, K)
         ens_mode = ens.sweep_mode()
-        ens_tile = list(ens.tile_shape())
+        ens_tile = list(ens.tile_shape(registers=True))
         ens.close()
         # the plain path: each chain alone in its own context, one kernel per pass
         plain = {}
@@ -524,7 +524,7 @@ def run_gpu(args):
     L = (args.lattice,) * 3 if args.lattice else L_MAIN
     V = vol(L)
     lat = Lattice(L, **COUP, precision="f32", seed=1000 + rank, device=local, sweep_mode=args.sweep_mode,
-                  n_link_or=args.link_or, tile_threads=args.tile_threads)
+                  n_link_or=args.link_or, tile_threads=args.tile_threads, tile_registers=args.tile_registers)
     lat.init_hot(2000 + rank)
     # untimed: the library's autotuner times its candidates (sweep forms x tile
     # shapes, 4 sweeps each) on the first sweeps and keeps the fastest
@@ -553,7 +553,7 @@ def run_gpu(args):
     ms_max = max_over_ranks(ms, world)
     value = world * V * args.steps / (ms_max / 1e3)
     mode = lat.sweep_mode()  # chosen by the library's autotuner during the untimed sweeps
-    tile_bs, tile_spt = lat.tile_shape()
+    tile_bs, tile_spt, tile_regs = lat.tile_shape(registers=True)
     # per step: the sweep (one persistent kernel, or 10 pass kernels + finalize)
     # and the two L2-flush kernels
     launches = args.steps * ((1 if mode == "persistent" else 11) + 2)
@@ -563,7 +563,7 @@ def run_gpu(args):
             sweep_bytes = B_HIGGS * 4 + B_LINK * 6 * (1 + args.link_or)
             print(json.dumps({"metric": METRIC, "value": value, "unit": UNIT, "L": list(L), "steps": args.steps,
                               "ms_per_step": ms_max / args.steps, "sweep_mode": mode, "quick": True,
-                              "tile_shape": [tile_bs, tile_spt],
+                              "tile_shape": [tile_bs, tile_spt, tile_regs],
                               "link_or": args.link_or, "passes": passes, "bytes_per_site": sweep_bytes,
                               "frac_of_measured_hbm": value * sweep_bytes / 1e9 / peak}), flush=True)
         lat.close()
@@ -638,6 +638,7 @@ def run_gpu(args):
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
                      "traffic": traffic, "kernel": dom_name, "sweep_mode": mode,
                      "tile_shape": {"threads_per_block": tile_bs, "sites_per_thread": tile_spt,
+                                    "register_cap": tile_regs,
                                     "chosen_by": "the library's autotuner" if args.sweep_mode == "auto"
                                     else f"--sweep-mode {args.sweep_mode}"},
                      "algorithmic_bytes_per_launch": dom_bytes, "avg_launch_ms": dom_ms,
@@ -755,6 +756,8 @@ def main():
     ap.add_argument("--lattice", type=int, default=0, help="cubic extent for --quick runs (default 64)")
     ap.add_argument("--sweep-mode", default="auto", choices=["auto", "passes", "passes2", "persistent"],
                     help="sweep form (default: the library's autotuner chooses)")
+    ap.add_argument("--tile-registers", type=int, default=0, choices=[0, 56],
+                    help="register cap of the update kernels (56 needs --tile-threads 128)")
     ap.add_argument("--tile-threads", type=int, default=0, choices=[0, 128, 256, 512],
                     help="threads per block of the update kernels (default 0: the autotuner chooses with "
                          "--sweep-mode auto, else 256)")

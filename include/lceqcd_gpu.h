@@ -115,6 +115,9 @@ typedef struct lce_params {
                             path and z-slabs use 256.  Results do not depend on
                             it (per-site work and random numbers are the same;
                             FP64 sums are grouped per tile). */
+  int tile_registers;    /* per-thread register cap of those kernels: 0
+                            (default: 64 in FP32), or 56 with tile_threads =
+                            128 (nine blocks per SM; FP32 only) */
 } lce_params;
 
 /* Measured quantities: /aver_loc/ (plaq0, a0kin, a02, a04, a0f) and the
@@ -217,9 +220,10 @@ int lce_sweep(lce_ctx* ctx, int measflag, lce_meas* m);
 int lce_sweeps(lce_ctx* ctx, int nsweeps, int measflag);
 /* the form lce_sweeps uses now (LCE_SWEEP_AUTO while still undecided) */
 int lce_get_sweep_mode(lce_ctx* ctx);
-/* the tile shape of the update kernels in use: threads per block and sites
- * per thread (a tuned choice once lce_get_sweep_mode is no longer AUTO) */
-int lce_get_tile_shape(lce_ctx* ctx, int* threads, int* sites_per_thread);
+/* the tile shape of the update kernels in use: threads per block, sites per
+ * thread and the per-thread register cap they are compiled for (a tuned
+ * choice once lce_get_sweep_mode is no longer AUTO); any output may be NULL */
+int lce_get_tile_shape(lce_ctx* ctx, int* threads, int* sites_per_thread, int* register_cap);
 /* f/meas1.f inputs: the last measured quantities of a chain */
 int lce_get_meas(lce_ctx* ctx, int chain, lce_meas* m);
 int lce_get_meas_batch(lce_ctx* ctx, lce_meas* m /* [nchains] */);

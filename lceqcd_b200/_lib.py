@@ -55,7 +55,7 @@ class LceParams(C.Structure):
         ("seed", C.c_ulonglong), ("device", C.c_int),
         ("n_link_or", C.c_int), ("n_higgs_metro", C.c_int),
         ("delta0", C.c_double), ("gf_angle", C.c_int), ("sweep_mode", C.c_int),
-        ("agauge_hits", C.c_int), ("tile_threads", C.c_int),
+        ("agauge_hits", C.c_int), ("tile_threads", C.c_int), ("tile_registers", C.c_int),
     ]
 
 
@@ -111,7 +111,7 @@ SIGNATURES = {
     "lce_sweep": (I, [P, I, P]),
     "lce_sweeps": (I, [P, I, I]),
     "lce_get_sweep_mode": (I, [P]),
-    "lce_get_tile_shape": (I, [P, P, P]),
+    "lce_get_tile_shape": (I, [P, P, P, P]),
     "lce_get_meas": (I, [P, I, P]),
     "lce_get_meas_batch": (I, [P, P]),
     "lce_landau_gauge": (I, [P, I, P, P, I]),

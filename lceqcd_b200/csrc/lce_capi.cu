@@ -40,7 +40,7 @@ void lce::set_thread_error(const std::string& msg) { g_create_error = msg; }
 // one autotune candidate: a sweep form and, for the per-pass forms, the tile
 // shape (threads per block, sites per thread), with its timed samples
 struct TuneForm {
-  int form, bs, spt;
+  int form, bs, spt, occ;  // occ: resident threads per SM of the register cap (0: the default)
   std::vector<float> ms;
 };
 
@@ -92,14 +92,16 @@ struct lce_ctx {
   cudaStream_t side = nullptr;
   cudaEvent_t fork_ev = nullptr, join_ev = nullptr;
   std::vector<cudaEvent_t> prof_ev;
-  // instantiated sweep graphs by (form, threads per block, sites per thread, measflag)
-  std::map<std::tuple<int, int, int, int>, cudaGraphExec_t> sweep_graphs;
+  // instantiated sweep graphs by (form, threads per block, sites per thread,
+  // register-cap occupancy, measflag)
+  std::map<std::tuple<int, int, int, int, int>, cudaGraphExec_t> sweep_graphs;
   GridBar* bar_d = nullptr;
   int persist_grid = 0;
   int sweep_mode = LCE_SWEEP_AUTO;   // requested
   int mode = LCE_SWEEP_AUTO;         // in use (AUTO while tuning)
   int tile_req = 0;                  // requested threads per block (0: tuned under AUTO, else 256)
   int tile_bs = kBlock, tile_spt = 1;  // tile shape of the per-pass kernels in use
+  int tile_occ = 0;                    // its register-cap occupancy (0: the default)
   std::vector<TuneForm> tune;        // autotune candidates and their samples
   std::map<std::pair<int, int>, cudaGraphExec_t> gf_exec;
   std::string err;
@@ -178,6 +180,10 @@ bool valid_params(const lce_params& p, std::string& why) {
     why = "tile_threads must be 0 (tuned), 128, 256 or 512";
     return false;
   }
+  if (p.tile_registers != 0 && !(p.tile_registers == 56 && p.tile_threads == 128 && p.precision == LCE_PREC_F32)) {
+    why = "tile_registers must be 0, or 56 with tile_threads = 128 in FP32";
+    return false;
+  }
   if (p.gf_angle != LCE_GF_ACOS && p.gf_angle != LCE_GF_ATAN2) {
     why = "gf_angle must be LCE_GF_ACOS or LCE_GF_ATAN2";
     return false;
@@ -248,7 +254,7 @@ struct Enq {
   FinalizeArgs f;
   const std::vector<int>* blk = nullptr;
   int* blk_d = nullptr;
-  int spt = 1, bs = kBlock;
+  int spt = 1, bs = kBlock, occ = 0;
   int measflag = 0;
   bool fuse = false;
   unsigned long long soff = 0;
@@ -260,12 +266,13 @@ struct Enq {
 int tile_index(int bs, int spt) { return bs * spt == 128 ? 0 : (bs * spt == 256 ? 1 : 2); }
 
 void enq_begin(lce_ctx* c, const std::vector<unsigned char>& routines, int measflag, bool fuse_renorm, int bs,
-               int spt, Enq& q) {
+               int spt, int occ, Enq& q) {
   const int ti = tile_index(bs, spt);
   q.blk = &c->tiles[ti];
   q.blk_d = c->tiles_d[ti];
   q.spt = spt;
   q.bs = bs;
+  q.occ = occ;
   q.measflag = measflag;
   q.fuse = fuse_renorm;
   q.passes.clear();
@@ -297,6 +304,7 @@ int enq_pass(lce_ctx* c, Enq& q, size_t i) {
   a.blk_begin = q.blk_d;
   a.spt = q.spt;
   a.bs = q.bs;
+  a.occ = q.occ;
   a.st = c->st_d;
   a.cst = c->cst_d;
   a.part = reduce ? c->part_d + (size_t)q.slot * c->slot_stride : nullptr;
@@ -341,11 +349,16 @@ int enq_end(lce_ctx* c, Enq& q) {
   return LCE_OK;
 }
 
-// bs, spt: the tile shape (0: the context's shape in use)
+// bs, spt, occ: the tile shape (bs = 0: the context's shape in use)
 int enqueue(lce_ctx* c, const std::vector<unsigned char>& routines, int measflag, bool fuse_renorm,
-            cudaEvent_t* events = nullptr, int bs = 0, int spt = 0) {
+            cudaEvent_t* events = nullptr, int bs = 0, int spt = 0, int occ = 0) {
   Enq q;
-  enq_begin(c, routines, measflag, fuse_renorm, bs ? bs : c->tile_bs, spt ? spt : c->tile_spt, q);
+  if (!bs) {
+    bs = c->tile_bs;
+    spt = c->tile_spt;
+    occ = c->tile_occ;
+  }
+  enq_begin(c, routines, measflag, fuse_renorm, bs, spt, occ, q);
   for (size_t i = 0; i < q.passes.size(); ++i) {
     if (int rc = enq_pass(c, q, i)) return rc;
     if (events) CK(cudaEventRecord(events[i], c->stream));
@@ -375,6 +388,7 @@ int enqueue_persistent(lce_ctx* c, const std::vector<unsigned char>& routines, i
   b.fuse_renorm = fuse_renorm ? 1 : 0;
   b.spt = 1;
   b.bs = kBlock;
+  b.occ = 0;
   b.s_lo = c->s_lo;
   b.site_off = c->site_off;
   b.stream_nh = c->stream_nh;
@@ -425,9 +439,9 @@ constexpr size_t kTuneSamples = 3;
 // The instantiated graph of one sweep in the given form (built once per
 // form and measflag).  The persistent form falls back to the per-pass form
 // under LCE_SWEEP_AUTO if it cannot be captured on this device.
-int sweep_graph(lce_ctx* c, int form, int bs, int spt, int mf, cudaGraphExec_t* out) {
-  if (form == LCE_SWEEP_PERSISTENT) bs = kBlock, spt = 1;
-  cudaGraphExec_t* slot = &c->sweep_graphs[std::make_tuple(form, bs, spt, mf)];
+int sweep_graph(lce_ctx* c, int form, int bs, int spt, int occ, int mf, cudaGraphExec_t* out) {
+  if (form == LCE_SWEEP_PERSISTENT) bs = kBlock, spt = 1, occ = 0;
+  cudaGraphExec_t* slot = &c->sweep_graphs[std::make_tuple(form, bs, spt, occ, mf)];
   if (!*slot) {
     cudaGraph_t g;
     CK(cudaStreamBeginCapture(c->stream, cudaStreamCaptureModeThreadLocal));
@@ -436,7 +450,7 @@ int sweep_graph(lce_ctx* c, int form, int bs, int spt, int mf, cudaGraphExec_t* 
       rc = c->prec == LCE_PREC_F64 ? enqueue_persistent<double>(c, sweep_routines(c), mf, true)
                                    : enqueue_persistent<float>(c, sweep_routines(c), mf, true);
     else
-      rc = enqueue(c, sweep_routines(c), mf, true, nullptr, bs, spt);
+      rc = enqueue(c, sweep_routines(c), mf, true, nullptr, bs, spt, occ);
     const cudaError_t ec = cudaStreamEndCapture(c->stream, &g);
     cudaError_t ei = cudaSuccess;
     if (ec == cudaSuccess) {
@@ -452,7 +466,7 @@ int sweep_graph(lce_ctx* c, int form, int bs, int spt, int mf, cudaGraphExec_t* 
         c->err = std::string("persistent sweep unavailable: ") + cudaGetErrorString(e);
         c->mode = LCE_SWEEP_PASSES;
         c->tune.clear();
-        return sweep_graph(c, LCE_SWEEP_PASSES, c->tile_bs, c->tile_spt, mf, out);
+        return sweep_graph(c, LCE_SWEEP_PASSES, c->tile_bs, c->tile_spt, c->tile_occ, mf, out);
       }
       return cuda_fail(c, e, "sweep graph capture");
     }
@@ -735,15 +749,27 @@ lce_ctx* create_impl(const lce_params* p, int n, const SlabInfo* slab = nullptr)
   c->tile_bs = c->tile_req ? c->tile_req : kBlock;
   c->tile_spt = c->mode == LCE_SWEEP_PASSES2 ? 2 : 1;
   if (c->tile_spt == 2 && c->tile_bs == 512) c->tile_bs = kBlock;  // (512, 2) is not compiled
+  const bool reg56 = !slab && p[0].tile_registers == 56;
+  if (reg56) {
+    c->tile_bs = 128;
+    c->tile_spt = 1;
+    c->tile_occ = 1152;
+  }
   if (c->mode == LCE_SWEEP_AUTO) {
     const int bss[3] = {128, 256, 512};
     for (int b : bss) {
+      if (reg56) {
+        c->tune.push_back(TuneForm{LCE_SWEEP_PASSES, 128, 1, 1152, {}});
+        break;
+      }
       if (c->tile_req && b != c->tile_req) continue;
       if (c->prec == LCE_PREC_F64 && b != kBlock) continue;
-      c->tune.push_back(TuneForm{LCE_SWEEP_PASSES, b, 1, {}});
-      if (b != 512) c->tune.push_back(TuneForm{LCE_SWEEP_PASSES2, b, 2, {}});
+      c->tune.push_back(TuneForm{LCE_SWEEP_PASSES, b, 1, 0, {}});
+      if (b != 512) c->tune.push_back(TuneForm{LCE_SWEEP_PASSES2, b, 2, 0, {}});
+      // 128 threads at a 56-register cap: nine blocks per SM, 12.5% more warps
+      if (b == 128) c->tune.push_back(TuneForm{LCE_SWEEP_PASSES, 128, 1, 1152, {}});
     }
-    if (c->persist_grid > 0) c->tune.push_back(TuneForm{LCE_SWEEP_PERSISTENT, kBlock, 1, {}});
+    if (c->persist_grid > 0) c->tune.push_back(TuneForm{LCE_SWEEP_PERSISTENT, kBlock, 1, 0, {}});
   }
   if ((e = cudaMemset(c->meas_d, 0, sizeof(lce_meas) * n)) != cudaSuccess) return bail(e, "cudaMemset(meas)");
   c->part_slots = std::max(6, 4 + 6 + 2 * c->n_higgs_metro + 6 * c->n_link_or);
@@ -1068,7 +1094,7 @@ int slab_sweep(lce_slabs* S, int measflag, lce_meas* m) {
   const int n = (int)S->slab.size();
   std::vector<Enq> q(n);
   const std::vector<unsigned char> routines = sweep_routines(S->slab[0]);
-  for (int k = 0; k < n; ++k) enq_begin(S->slab[k], routines, measflag, true, kBlock, 1, q[k]);
+  for (int k = 0; k < n; ++k) enq_begin(S->slab[k], routines, measflag, true, kBlock, 1, 0, q[k]);
   for (size_t i = 0; i < q[0].passes.size(); ++i) {
     for (int k = 0; k < n; ++k) {
       lce_ctx* c = S->slab[k];
@@ -1582,7 +1608,7 @@ int lce_sweeps(lce_ctx* c, int nsweeps, int measflag) {
       if (c->tune[f].ms.size() < c->tune[k].ms.size()) k = f;
     const TuneForm tf = c->tune[k];
     cudaGraphExec_t ex;
-    int rc = sweep_graph(c, tf.form, tf.bs, tf.spt, mf, &ex);
+    int rc = sweep_graph(c, tf.form, tf.bs, tf.spt, tf.occ, mf, &ex);
     if (rc) return rc;
     if (c->mode != LCE_SWEEP_AUTO) break;  // the persistent form was unavailable
     CK(cudaEventRecord(c->ev0, c->stream));
@@ -1610,11 +1636,12 @@ int lce_sweeps(lce_ctx* c, int nsweeps, int measflag) {
       c->mode = c->tune[best].form;
       c->tile_bs = c->tune[best].bs;
       c->tile_spt = c->tune[best].spt;
+      c->tile_occ = c->tune[best].occ;
     }
   }
   if (done < nsweeps) {
     cudaGraphExec_t ex;
-    int rc = sweep_graph(c, c->mode, c->tile_bs, c->tile_spt, mf, &ex);
+    int rc = sweep_graph(c, c->mode, c->tile_bs, c->tile_spt, c->tile_occ, mf, &ex);
     if (rc) return rc;
     for (int i = done; i < nsweeps; ++i) CK(cudaGraphLaunch(ex, c->stream));
   }
@@ -1623,10 +1650,15 @@ int lce_sweeps(lce_ctx* c, int nsweeps, int measflag) {
 
 int lce_get_sweep_mode(lce_ctx* c) { return c ? c->mode : LCE_ERR_INVALID; }
 
-int lce_get_tile_shape(lce_ctx* c, int* threads, int* sites_per_thread) {
+int lce_get_tile_shape(lce_ctx* c, int* threads, int* sites_per_thread, int* register_cap) {
   if (!c) return LCE_ERR_INVALID;
-  if (threads) *threads = c->mode == LCE_SWEEP_PERSISTENT ? kBlock : c->tile_bs;
-  if (sites_per_thread) *sites_per_thread = c->mode == LCE_SWEEP_PERSISTENT ? 1 : c->tile_spt;
+  const bool pers = c->mode == LCE_SWEEP_PERSISTENT;
+  if (threads) *threads = pers ? kBlock : c->tile_bs;
+  if (sites_per_thread) *sites_per_thread = pers ? 1 : c->tile_spt;
+  if (register_cap) {
+    const int occ = pers || !c->tile_occ ? (c->prec == LCE_PREC_F32 ? 4 : 3) * kBlock : c->tile_occ;
+    *register_cap = std::min(255, (65536 / occ) & ~7);
+  }
   return LCE_OK;
 }
 
@@ -2116,7 +2148,7 @@ int lce_profile_sweep(lce_ctx* c, int measflag, float* ms, int max_passes) {
     CK(cudaEventCreate(&e));
     c->prof_ev.push_back(e);
   }
-  cudaGraphExec_t* slot = &c->sweep_graphs[std::make_tuple(-1, c->tile_bs, c->tile_spt, mf)];
+  cudaGraphExec_t* slot = &c->sweep_graphs[std::make_tuple(-1, c->tile_bs, c->tile_spt, c->tile_occ, mf)];
   if (!*slot) {
     cudaGraph_t g;
     CK(cudaStreamBeginCapture(c->stream, cudaStreamCaptureModeThreadLocal));
@@ -2124,7 +2156,7 @@ int lce_profile_sweep(lce_ctx* c, int measflag, float* ms, int max_passes) {
     Enq q;
     int rc = LCE_OK;
     if (e == cudaSuccess) {
-      enq_begin(c, r, mf, true, c->tile_bs, c->tile_spt, q);
+      enq_begin(c, r, mf, true, c->tile_bs, c->tile_spt, c->tile_occ, q);
       for (int i = 0; i < np && rc == LCE_OK && e == cudaSuccess; ++i) {
         rc = enq_pass(c, q, i);
         if (rc == LCE_OK) e = cudaEventRecord(c->fork_ev, c->stream);

@@ -115,6 +115,7 @@ struct PassArgs {
   int fuse_renorm;
   int spt;                // sites per thread (a tile is bs * spt sites)
   int bs;                 // threads per block of the per-pass kernels
+  int occ;                // resident threads per SM of the register cap (0: 4 x 256)
   // z-slab of a decomposed lattice (single-chain contexts): the passes visit
   // sites [s_lo, nh - s_lo) of each parity (the first and last planes are
   // halos), and site_off turns a site index into the whole lattice's for the

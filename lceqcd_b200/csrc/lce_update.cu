@@ -388,24 +388,27 @@ __device__ __forceinline__ void link_tile(const PassArgs& p, int tile) {
 }
 
 // Tile shape: BS threads per block, SPT sites per thread (1, or 2 for the
-// LCE_SWEEP_PASSES2 form).  The register cap is the same for every BS: the
-// resident threads per SM of min_blocks<R>() blocks of kBlock threads.
-template <typename R, int BS>
-constexpr int min_blocks_bs() { return min_blocks<R>() * kBlock / BS > 0 ? min_blocks<R>() * kBlock / BS : 1; }
+// LCE_SWEEP_PASSES2 form), and OCC resident threads per SM the register cap
+// is set for: OCC = 0 keeps the cap of min_blocks<R>() blocks of kBlock
+// threads (64 registers in FP32); OCC = 1152 is nine blocks of 128 (56).
+template <typename R, int BS, int OCC>
+constexpr int min_blocks_bs() {
+  return OCC ? OCC / BS : (min_blocks<R>() * kBlock / BS > 0 ? min_blocks<R>() * kBlock / BS : 1);
+}
 
-template <typename R, int MODE, int SPT, int BS>
-__global__ void __launch_bounds__(BS, min_blocks_bs<R, BS>()) higgs_kernel(PassArgs p) {
+template <typename R, int MODE, int SPT, int BS, int OCC = 0>
+__global__ void __launch_bounds__(BS, min_blocks_bs<R, BS, OCC>()) higgs_kernel(PassArgs p) {
   higgs_tile<R, MODE, true, SPT, BS>(p, blockIdx.x);
 }
 
-template <typename R, int MU, int OR, int SPT, int BS>
-__global__ void __launch_bounds__(BS, min_blocks_bs<R, BS>()) link_kernel(PassArgs p) {
+template <typename R, int MU, int OR, int SPT, int BS, int OCC = 0>
+__global__ void __launch_bounds__(BS, min_blocks_bs<R, BS, OCC>()) link_kernel(PassArgs p) {
   link_tile<R, MU, OR, true, 1, SPT, BS>(p, blockIdx.x);
 }
 
 // f/agauge1.f (3 hits)
-template <typename R, int MU, int SPT, int BS>
-__global__ void __launch_bounds__(BS, min_blocks_bs<R, BS>()) link3_kernel(PassArgs p) {
+template <typename R, int MU, int SPT, int BS, int OCC = 0>
+__global__ void __launch_bounds__(BS, min_blocks_bs<R, BS, OCC>()) link3_kernel(PassArgs p) {
   link_tile<R, MU, 0, true, 3, SPT, BS>(p, blockIdx.x);
 }
 
@@ -657,30 +660,38 @@ __global__ void debug_force_kernel(const ChainDev* chp, int eo, double* out) {
 // ------------------------------------------------------------------ launchers
 // The pass kernels and the finalize kernel are launched with programmatic
 // dependent launch (lce_common.cuh: launch_pdl / pdl_wait).
-template <typename R, int SPT, int BS>
+template <typename R, int SPT, int BS, int OCC = 0>
 void launch_higgs_t(int mode, const PassArgs& a, int nblocks, cudaStream_t s) {
-  void (*k)(PassArgs) = mode == 0 ? higgs_kernel<R, 0, SPT, BS>
-                                  : (mode == 1 ? higgs_kernel<R, 1, SPT, BS> : higgs_kernel<R, 2, SPT, BS>);
+  void (*k)(PassArgs) = mode == 0 ? higgs_kernel<R, 0, SPT, BS, OCC>
+                                  : (mode == 1 ? higgs_kernel<R, 1, SPT, BS, OCC> : higgs_kernel<R, 2, SPT, BS, OCC>);
   (void)launch_pdl(k, nblocks, BS, 0, s, a);
 }
 
-template <typename R, int SPT, int BS>
+template <typename R, int SPT, int BS, int OCC = 0>
 void launch_link_t(int mode, int mu, const PassArgs& a, int nblocks, cudaStream_t s) {
   void (*k)(PassArgs);
   if (mode == 0)
-    k = mu == 0 ? link_kernel<R, 0, 0, SPT, BS> : (mu == 1 ? link_kernel<R, 1, 0, SPT, BS> : link_kernel<R, 2, 0, SPT, BS>);
+    k = mu == 0 ? link_kernel<R, 0, 0, SPT, BS, OCC>
+                : (mu == 1 ? link_kernel<R, 1, 0, SPT, BS, OCC> : link_kernel<R, 2, 0, SPT, BS, OCC>);
   else if (mode == 1)
-    k = mu == 0 ? link_kernel<R, 0, 1, SPT, BS> : (mu == 1 ? link_kernel<R, 1, 1, SPT, BS> : link_kernel<R, 2, 1, SPT, BS>);
+    k = mu == 0 ? link_kernel<R, 0, 1, SPT, BS, OCC>
+                : (mu == 1 ? link_kernel<R, 1, 1, SPT, BS, OCC> : link_kernel<R, 2, 1, SPT, BS, OCC>);
   else
-    k = mu == 0 ? link3_kernel<R, 0, SPT, BS> : (mu == 1 ? link3_kernel<R, 1, SPT, BS> : link3_kernel<R, 2, SPT, BS>);
+    k = mu == 0 ? link3_kernel<R, 0, SPT, BS, OCC>
+                : (mu == 1 ? link3_kernel<R, 1, SPT, BS, OCC> : link3_kernel<R, 2, SPT, BS, OCC>);
   (void)launch_pdl(k, nblocks, BS, 0, s, a);
 }
 
 // Tile shapes compiled: FP32 (BS, SPT) in {128, 256, 512} x {1} and
-// {128, 256} x {2}; the FP64 validation path only BS = 256.
+// {128, 256} x {2} at the 64-register cap, and (128, 1) at 56 registers
+// (a.occ = 1152); the FP64 validation path only BS = 256.
 template <typename R>
 void launch_higgs(int mode, const PassArgs& a, int nblocks, cudaStream_t s) {
   if constexpr (sizeof(R) == 4) {
+    if (a.bs == 128 && a.occ == 1152) {
+      launch_higgs_t<R, 1, 128, 1152>(mode, a, nblocks, s);
+      return;
+    }
     if (a.bs == 128) {
       if (a.spt == 2) launch_higgs_t<R, 2, 128>(mode, a, nblocks, s);
       else launch_higgs_t<R, 1, 128>(mode, a, nblocks, s);
@@ -698,6 +709,10 @@ void launch_higgs(int mode, const PassArgs& a, int nblocks, cudaStream_t s) {
 template <typename R>
 void launch_link(int mode, int mu, const PassArgs& a, int nblocks, cudaStream_t s) {
   if constexpr (sizeof(R) == 4) {
+    if (a.bs == 128 && a.occ == 1152) {
+      launch_link_t<R, 1, 128, 1152>(mode, mu, a, nblocks, s);
+      return;
+    }
     if (a.bs == 128) {
       if (a.spt == 2) launch_link_t<R, 2, 128>(mode, mu, a, nblocks, s);
       else launch_link_t<R, 1, 128>(mode, mu, a, nblocks, s);

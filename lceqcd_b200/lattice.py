@@ -60,6 +60,7 @@ class Params:
     sweep_mode: str = "auto"
     agauge_hits: int = 1
     tile_threads: int = 0
+    tile_registers: int = 0
 
     def to_c(self) -> LceParams:
         p = LceParams()
@@ -80,6 +81,7 @@ class Params:
         p.sweep_mode = SWEEP_MODES[self.sweep_mode]
         p.agauge_hits = int(self.agauge_hits)
         p.tile_threads = int(self.tile_threads)
+        p.tile_registers = int(self.tile_registers)
         return p
 
 
@@ -239,11 +241,12 @@ class _Context:
     def sweeps(self, n: int, measflag: int = 0):
         self._ck(self.lib.lce_sweeps(self.h, int(n), measflag))
 
-    def tile_shape(self):
-        """(threads per block, sites per thread) of the update kernels in use."""
-        bs, spt = C.c_int(), C.c_int()
-        self._ck(self.lib.lce_get_tile_shape(self.h, C.byref(bs), C.byref(spt)))
-        return bs.value, spt.value
+    def tile_shape(self, registers: bool = False):
+        """(threads per block, sites per thread) of the update kernels in use,
+        and with registers=True their per-thread register cap."""
+        bs, spt, reg = C.c_int(), C.c_int(), C.c_int()
+        self._ck(self.lib.lce_get_tile_shape(self.h, C.byref(bs), C.byref(spt), C.byref(reg)))
+        return (bs.value, spt.value, reg.value) if registers else (bs.value, spt.value)
 
     def sweep_mode(self) -> str:
         m = self._ck(self.lib.lce_get_sweep_mode(self.h))

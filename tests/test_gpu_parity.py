@@ -464,15 +464,17 @@ SHAPES = [(256, "passes"), (128, "passes"), (512, "passes"), (128, "passes2"), (
 @pytest.mark.parametrize("L", [(16, 8, 12), (64, 32, 34)])
 def test_tile_shapes_update_identically(L):
     """Every tile shape of the per-pass kernels (128, 256 or 512 threads per
-    block; one or two sites per thread) updates every site exactly as the
-    others; only the grouping of the FP64 measurement sums differs."""
+    block; one or two sites per thread; the 56-register 128-thread form)
+    updates every site exactly as the others; only the grouping of the FP64
+    measurement sums differs."""
     res = []
-    for bs, mode in SHAPES:
-        g = Lattice(L, beta=12.0, x=0.09, y=0.3, seed=77, sweep_mode=mode, tile_threads=bs, n_link_or=1,
-                    n_higgs_metro=1)
+    for bs, mode in SHAPES + [(128, "passes56")]:
+        regs = 56 if mode == "passes56" else 0
+        g = Lattice(L, beta=12.0, x=0.09, y=0.3, seed=77, sweep_mode=mode.replace("56", ""), tile_threads=bs,
+                    tile_registers=regs, n_link_or=1, n_higgs_metro=1)
         g.init_hot(8)
         ms = [g.sweep(1) for _ in range(3)]
-        assert g.tile_shape() == (bs, 2 if mode == "passes2" else 1)
+        assert g.tile_shape(registers=True) == (bs, 2 if mode == "passes2" else 1, regs or 64)
         res.append((g.download(), ms, g.rng_position()))
         g.close()
     for (u, a), ms, pos in res[1:]:
@@ -532,6 +534,10 @@ def test_autotune_chooses_form_and_tile_shape():
 def test_tile_threads_rejected_when_invalid():
     with pytest.raises(LceError):
         Lattice((8, 8, 8), tile_threads=64)
+    with pytest.raises(LceError):
+        Lattice((8, 8, 8), tile_threads=256, tile_registers=56)
+    with pytest.raises(LceError):
+        Lattice((8, 8, 8), tile_threads=128, tile_registers=56, precision="f64")
 
 
 def test_profiled_sweep_graph_is_an_ordinary_sweep():
