@@ -254,7 +254,7 @@ def kernel_profile(lat, reps=10):
     for _ in range(reps):
         lat.flush_l2()
         lat.synchronize()
-        ms = lat.profile_sweep(1)
+        ms = lat.profile_sweep(1, with_finalize=True)
         acc = ms if acc is None else acc + ms
     return acc / reps
 
@@ -573,9 +573,10 @@ def run_gpu(args):
     # launch, one launch per step) when the autotuner chose it, else the link
     # pass kernel (68 B*V per launch, 6 of the 10 passes); per-pass kernel
     # durations come from events between the pass kernels of profiled sweeps
-    prof = kernel_profile(lat, reps=10)
+    prof = kernel_profile(lat, reps=10)  # 10 passes, then the finalize kernel
     link_ms = float(np.mean(prof[4:10]))
     higgs_ms = float(np.mean(prof[0:4]))
+    fin_ms = float(prof[10])
     if mode == "persistent":
         dom_ms, dom_bytes = ms_max / args.steps, B_SWEEP * V
         dom_name = "sweep_persistent_kernel (whole sweep: 4 Higgs + 6 link passes, one cooperative launch)"
@@ -645,7 +646,16 @@ def run_gpu(args):
                      "peak_source": f"{peak_src} (MEASURED_PEAKS.json hbm_gbs)" if peak_src == "measured" else "fallback",
                      "pass_kernels": {"link_kernel_ms": link_ms, "link_kernel_frac": B_LINK * V / (link_ms / 1e3) / 1e9 / peak,
                                       "higgs_kernel_ms": higgs_ms,
-                                      "higgs_kernel_frac": B_HIGGS * V / (higgs_ms / 1e3) / 1e9 / peak},
+                                      "higgs_kernel_frac": B_HIGGS * V / (higgs_ms / 1e3) / 1e9 / peak,
+                                      "finalize_kernel_ms": fin_ms,
+                                      "per_pass_ms": [float(x) for x in prof],
+                                      "share_of_sweep": {"link_passes": 6 * link_ms / float(np.sum(prof)),
+                                                         "higgs_passes": 4 * higgs_ms / float(np.sum(prof)),
+                                                         "finalize": fin_ms / float(np.sum(prof))},
+                                      "timing": "CUDA events hung off each pass of a sweep graph on a side stream "
+                                                "(the passes keep their programmatic overlap); a pass's time is "
+                                                "its completion minus the previous pass's (pass 0 from the graph "
+                                                "start, after an L2 flush)"},
                      "sweep_frac": value / world * B_SWEEP / 1e9 / peak},
         "clocks": clocks,
     }

@@ -430,70 +430,92 @@ __device__ __forceinline__ void finalize_sum(const FinalizeArgs& f, int w) {
 
 // Per chain, in slot order, the reference's normalisations; then advance the
 // RNG counters.  Run by one block after every finalize_sum has completed.
+// One warp per chain: each lane loads two slots' totals (kMaxSlots = 64), all
+// loads in flight at once (L2, the sums of other blocks), then the in-order
+// scan over the slots reads them from the lanes by shuffles -- one L2 round
+// trip per chain instead of one per slot.
 __device__ __forceinline__ void finalize_combine(const FinalizeArgs& f) {
-  for (int c = threadIdx.x; c < f.nchains; c += blockDim.x) {
+  static_assert(kMaxSlots <= 64, "two slots per lane");
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarps = (int)(blockDim.x >> 5);
+  for (int c = warp; c < f.nchains; c += nwarps) {
     const ChainDev& ch = f.chains[c];
     const double V = 2.0 * ch.nh;
+    const double* base = f.totals + (size_t)c * kMaxSlots * kNQ;
+    double t0[kNQ], t1[kNQ];
+    bool bad = false;
+#pragma unroll
+    for (int q = 0; q < kNQ; ++q) {
+      t0[q] = lane < f.nslots ? __ldcg(base + (size_t)lane * kNQ + q) : 0.0;
+      t1[q] = lane + 32 < f.nslots ? __ldcg(base + (size_t)(lane + 32) * kNQ + q) : 0.0;
+      bad = bad || !isfinite(t0[q]) || !isfinite(t1[q]);
+    }
+    if (__any_sync(0xffffffffu, bad) && lane == 0) atomicOr(&f.st->status, kStatusNaN);
     lce_meas& m = f.meas[c];
     double h[kNQ] = {0, 0, 0, 0}, l[kNQ] = {0, 0, 0, 0};
     for (int i = 0; i < f.nslots; ++i) {
-      const volatile double* t = f.totals + ((size_t)c * kMaxSlots + i) * kNQ;
+      double t[kNQ];
+#pragma unroll
+      for (int q = 0; q < kNQ; ++q) t[q] = __shfl_sync(0xffffffffu, i < 32 ? t0[q] : t1[q], i & 31);
       const int kind = f.kinds[i] & 0x7f;
       const bool end = (f.kinds[i] & kKindEnd) != 0;
-      if (!isfinite(t[0]) || !isfinite(t[1]) || !isfinite(t[2]) || !isfinite(t[3]))
-        atomicOr(&f.st->status, kStatusNaN);
       if (kind <= kHiggsMetro) {
         for (int q = 0; q < kNQ; ++q) h[q] += t[q];
         if (end) {
-          // f/ahiggs2.f:142-147 (same in ahiggs1/3)
-          m.a2 = h[1] / V;
-          m.a4 = h[2] / V;
-          m.akin = h[3] / (6.0 * V);
-          const double acc = h[0] / V;
-          if (kind == kHiggsHB) m.acc_hb = acc;
-          if (kind == kHiggsOR) m.acc_or = acc;
-          if (kind == kHiggsMetro) {
-            // f/ahiggs1.f:113-123 step adaptation, in the build's precision
-            if (f.single) {
-              float a = (float)h[0] / (float)V, d = (float)f.cst[c].delta;
-              if (fabsf(a - 0.5f) > 0.1f) d = (a > 0.5f) ? 1.1131241f * d : 0.8989669f * d;
-              m.acc_metro = a;
-              f.cst[c].delta = d;
-            } else {
-              double d = f.cst[c].delta;
-              if (fabs(acc - 0.5) > 0.1) d = (acc > 0.5) ? 1.1131241 * d : 0.8989669 * d;
-              m.acc_metro = acc;
-              f.cst[c].delta = d;
+          if (lane == 0) {
+            // f/ahiggs2.f:142-147 (same in ahiggs1/3)
+            m.a2 = h[1] / V;
+            m.a4 = h[2] / V;
+            m.akin = h[3] / (6.0 * V);
+            const double acc = h[0] / V;
+            if (kind == kHiggsHB) m.acc_hb = acc;
+            if (kind == kHiggsOR) m.acc_or = acc;
+            if (kind == kHiggsMetro) {
+              // f/ahiggs1.f:113-123 step adaptation, in the build's precision
+              if (f.single) {
+                float a = (float)h[0] / (float)V, d = (float)f.cst[c].delta;
+                if (fabsf(a - 0.5f) > 0.1f) d = (a > 0.5f) ? 1.1131241f * d : 0.8989669f * d;
+                m.acc_metro = a;
+                f.cst[c].delta = d;
+              } else {
+                double d = f.cst[c].delta;
+                if (fabs(acc - 0.5) > 0.1) d = (acc > 0.5) ? 1.1131241 * d : 0.8989669 * d;
+                m.acc_metro = acc;
+                f.cst[c].delta = d;
+              }
+              m.delta = f.cst[c].delta;
             }
-            m.delta = f.cst[c].delta;
           }
           h[0] = h[1] = h[2] = h[3] = 0;
         }
       } else if (kind == kLinkHB) {
         for (int q = 0; q < kNQ; ++q) l[q] += t[q];
         if (end) {
-          // f/agauge.f:195-200
-          m.plaq = l[2] / (12.0 * V);
-          m.acc_gauge = (l[0] / (3.0 * V)) * (l[1] / (12.0 * V));
+          if (lane == 0) {
+            // f/agauge.f:195-200
+            m.plaq = l[2] / (12.0 * V);
+            m.acc_gauge = (l[0] / (3.0 * V)) * (l[1] / (12.0 * V));
+          }
           l[0] = l[1] = l[2] = l[3] = 0;
         }
       } else if (kind == kLinkHB3) {
         for (int q = 0; q < kNQ; ++q) l[q] += t[q];
         if (end) {
-          // f/agauge1.f:227-232: the Metropolis count is divided by the 3 hits
-          m.plaq = l[2] / (12.0 * V);
-          m.acc_gauge = (l[0] / (3.0 * V)) * (l[1] / (12.0 * V) / 3.0);
+          if (lane == 0) {
+            // f/agauge1.f:227-232: the Metropolis count is divided by the 3 hits
+            m.plaq = l[2] / (12.0 * V);
+            m.acc_gauge = (l[0] / (3.0 * V)) * (l[1] / (12.0 * V) / 3.0);
+          }
           l[0] = l[1] = l[2] = l[3] = 0;
         }
       } else if (kind == kLinkOR) {
         for (int q = 0; q < kNQ; ++q) l[q] += t[q];
         if (end) {
-          m.acc_link_or = l[0] / (3.0 * V);
+          if (lane == 0) m.acc_link_or = l[0] / (3.0 * V);
           l[0] = l[1] = l[2] = l[3] = 0;
         }
       }
     }
-    m.delta = f.cst[c].delta;
+    if (lane == 0) m.delta = f.cst[c].delta;
   }
   __syncthreads();
   if (threadIdx.x == 0) {

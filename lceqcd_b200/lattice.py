@@ -415,10 +415,13 @@ class _Context:
     def flush_l2(self):
         self._ck(self.lib.lce_flush_l2(self.h))
 
-    def profile_sweep(self, measflag: int = 0, max_passes: int = 64):
-        ms = np.zeros(max_passes, np.float32)
-        n = self._ck(self.lib.lce_profile_sweep(self.h, measflag, _ptr(ms), max_passes))
-        return ms[:n].astype(np.float64)
+    def profile_sweep(self, measflag: int = 0, max_passes: int = 64, with_finalize: bool = False):
+        """Per-pass durations (ms) of one sweep run as a graph with timing
+        events hung off the pass kernels; with_finalize appends the finalize
+        kernel's."""
+        ms = np.zeros(max_passes + 1, np.float32)
+        n = self._ck(self.lib.lce_profile_sweep(self.h, measflag, _ptr(ms), max_passes + 1))
+        return ms[:n + 1 if with_finalize else n].astype(np.float64)
 
     def timer_start(self):
         self._ck(self.lib.lce_timer_start(self.h))
