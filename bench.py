@@ -589,7 +589,7 @@ def run_gpu(args):
             ", two sites per thread)" if mode == "passes2" else ")")
     achieved = dom_bytes / (dom_ms / 1e3) / 1e9
     # the same bytes move whether a thread takes one site or two
-    traffic = profile_traffic("passes" if mode == "passes2" else mode)
+    traffic = profile_traffic("passes" if mode in ("passes2", "direct") else mode)
 
     # End to end through the C ABI with pinned host buffers.  A step uploads
     # the configuration (the step's input, lce_upload), runs one measured
@@ -769,7 +769,7 @@ def main():
     ap.add_argument("--quick", action="store_true",
                     help="timed sweeps only (no e2e, CPU baseline, extras or clocks): the ncu profiling case")
     ap.add_argument("--lattice", type=int, default=0, help="cubic extent for --quick runs (default 64)")
-    ap.add_argument("--sweep-mode", default="auto", choices=["auto", "passes", "passes2", "persistent"],
+    ap.add_argument("--sweep-mode", default="auto", choices=["auto", "passes", "passes2", "persistent", "direct"],
                     help="sweep form (default: the library's autotuner chooses)")
     ap.add_argument("--tile-registers", type=int, default=0, choices=[0, 56],
                     help="register cap of the update kernels (56 needs --tile-threads 128)")

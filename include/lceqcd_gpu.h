@@ -77,6 +77,8 @@ extern "C" {
 #define LCE_SWEEP_PASSES 1
 #define LCE_SWEEP_PERSISTENT 2
 #define LCE_SWEEP_PASSES2 3
+#define LCE_SWEEP_DIRECT 4   /* the per-pass kernels launched on the stream
+                                without a graph (one site per thread) */
 
 /* field selectors for upload/download */
 #define LCE_FIELDS 0        /* u, a        (COMMON /linkvar/ u, a) */
@@ -104,7 +106,8 @@ typedef struct lce_params {
                             reference, f/or_gauge_fixing1.f:174) or LCE_GF_ATAN2 */
   int sweep_mode;        /* LCE_SWEEP_AUTO (time the forms on the first sweeps
                             and keep the fastest), LCE_SWEEP_PASSES,
-                            LCE_SWEEP_PASSES2 or LCE_SWEEP_PERSISTENT */
+                            LCE_SWEEP_PASSES2, LCE_SWEEP_PERSISTENT or
+                            LCE_SWEEP_DIRECT */
   int agauge_hits;       /* link update of lce_sweep: 1 = f/agauge.f (default;
                             0 is read as 1), 3 = f/agauge1.f (three heatbath +
                             Metropolis hits per link) -- the reference selects

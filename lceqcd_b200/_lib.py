@@ -31,6 +31,7 @@ LCE_SWEEP_AUTO = 0
 LCE_SWEEP_PASSES = 1
 LCE_SWEEP_PERSISTENT = 2
 LCE_SWEEP_PASSES2 = 3
+LCE_SWEEP_DIRECT = 4
 LCE_FIELDS = 0
 LCE_FIELDS_FIXED = 1
 LCE_GF_START_IDENTITY = 0

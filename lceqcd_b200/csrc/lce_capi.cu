@@ -172,8 +172,9 @@ bool valid_params(const lce_params& p, std::string& why) {
     why = "imode must be 0 or 1";
     return false;
   }
-  if (p.sweep_mode < LCE_SWEEP_AUTO || p.sweep_mode > LCE_SWEEP_PASSES2) {
-    why = "sweep_mode must be LCE_SWEEP_AUTO, LCE_SWEEP_PASSES, LCE_SWEEP_PASSES2 or LCE_SWEEP_PERSISTENT";
+  if (p.sweep_mode < LCE_SWEEP_AUTO || p.sweep_mode > LCE_SWEEP_DIRECT) {
+    why = "sweep_mode must be LCE_SWEEP_AUTO, LCE_SWEEP_PASSES, LCE_SWEEP_PASSES2, LCE_SWEEP_PERSISTENT or "
+          "LCE_SWEEP_DIRECT";
     return false;
   }
   if (p.tile_threads != 0 && p.tile_threads != 128 && p.tile_threads != 256 && p.tile_threads != 512) {
@@ -769,6 +770,10 @@ lce_ctx* create_impl(const lce_params* p, int n, const SlabInfo* slab = nullptr)
       // 128 threads at a 56-register cap: nine blocks per SM, 12.5% more warps
       if (b == 128) c->tune.push_back(TuneForm{LCE_SWEEP_PASSES, 128, 1, 1152, {}});
     }
+    // the per-pass kernels launched on the stream without a graph: no graph
+    // start, but every launch goes through the host
+    c->tune.push_back(TuneForm{LCE_SWEEP_DIRECT, reg56 ? 128 : (c->tile_req ? c->tile_req : kBlock), 1,
+                               reg56 ? 1152 : 0, {}});
     if (c->persist_grid > 0) c->tune.push_back(TuneForm{LCE_SWEEP_PERSISTENT, kBlock, 1, 0, {}});
   }
   if ((e = cudaMemset(c->meas_d, 0, sizeof(lce_meas) * n)) != cudaSuccess) return bail(e, "cudaMemset(meas)");
@@ -1607,12 +1612,15 @@ int lce_sweeps(lce_ctx* c, int nsweeps, int measflag) {
     for (int f = 1; f < (int)c->tune.size(); ++f)
       if (c->tune[f].ms.size() < c->tune[k].ms.size()) k = f;
     const TuneForm tf = c->tune[k];
-    cudaGraphExec_t ex;
-    int rc = sweep_graph(c, tf.form, tf.bs, tf.spt, tf.occ, mf, &ex);
-    if (rc) return rc;
-    if (c->mode != LCE_SWEEP_AUTO) break;  // the persistent form was unavailable
+    cudaGraphExec_t ex = nullptr;
+    if (tf.form != LCE_SWEEP_DIRECT) {
+      int rc = sweep_graph(c, tf.form, tf.bs, tf.spt, tf.occ, mf, &ex);
+      if (rc) return rc;
+      if (c->mode != LCE_SWEEP_AUTO) break;  // the persistent form was unavailable
+    }
     CK(cudaEventRecord(c->ev0, c->stream));
-    CK(cudaGraphLaunch(ex, c->stream));
+    if (ex) CK(cudaGraphLaunch(ex, c->stream));
+    else if (int rc = enqueue(c, sweep_routines(c), mf, true, nullptr, tf.bs, tf.spt, tf.occ)) return rc;
     CK(cudaEventRecord(c->ev1, c->stream));
     CK(cudaEventSynchronize(c->ev1));
     float ms = 0;
@@ -1640,6 +1648,12 @@ int lce_sweeps(lce_ctx* c, int nsweeps, int measflag) {
     }
   }
   if (done < nsweeps) {
+    if (c->mode == LCE_SWEEP_DIRECT) {
+      const std::vector<unsigned char> r = sweep_routines(c);
+      for (int i = done; i < nsweeps; ++i)
+        if (int rc = enqueue(c, r, mf, true)) return rc;
+      return LCE_OK;
+    }
     cudaGraphExec_t ex;
     int rc = sweep_graph(c, c->mode, c->tile_bs, c->tile_spt, c->tile_occ, mf, &ex);
     if (rc) return rc;

@@ -31,7 +31,8 @@ from ._lib import LceMeas, LceParams, check, load
 PREC = {"f32": _lib.LCE_PREC_F32, "f64": _lib.LCE_PREC_F64}
 RNG = {"philox": _lib.LCE_RNG_PHILOX, "stream": _lib.LCE_RNG_STREAM}
 SWEEP_MODES = {"auto": _lib.LCE_SWEEP_AUTO, "passes": _lib.LCE_SWEEP_PASSES,
-               "persistent": _lib.LCE_SWEEP_PERSISTENT, "passes2": _lib.LCE_SWEEP_PASSES2}
+               "persistent": _lib.LCE_SWEEP_PERSISTENT, "passes2": _lib.LCE_SWEEP_PASSES2,
+               "direct": _lib.LCE_SWEEP_DIRECT}
 
 
 def _ptr(a: np.ndarray):

@@ -322,7 +322,7 @@ def test_persistent_batch_and_autotune():
         ens.init_hot(3)
         ens.sweeps(30, 1)
         if mode == "auto":
-            assert ens.sweep_mode() in ("passes", "passes2", "persistent")
+            assert ens.sweep_mode() in ("passes", "passes2", "persistent", "direct")
         outs.append(([ens.download(chain=i) for i in range(2)], ens.meas_batch()))
     for o in outs[1:]:
         for i in range(2):
@@ -450,7 +450,7 @@ def test_two_sites_per_thread_batch_and_three_way_autotune():
         ens.init_hot(3)
         ens.sweeps(30, 1)
         if mode == "auto":
-            assert ens.sweep_mode() in ("passes", "passes2", "persistent")
+            assert ens.sweep_mode() in ("passes", "passes2", "persistent", "direct")
         outs.append([ens.download(chain=i) for i in range(3)])
     for o in outs[1:]:
         for i in range(3):
@@ -458,7 +458,7 @@ def test_two_sites_per_thread_batch_and_three_way_autotune():
             np.testing.assert_array_equal(o[i][1], outs[0][i][1])
 
 
-SHAPES = [(256, "passes"), (128, "passes"), (512, "passes"), (128, "passes2"), (256, "passes2")]
+SHAPES = [(256, "passes"), (128, "passes"), (512, "passes"), (128, "passes2"), (256, "passes2"), (256, "direct")]
 
 
 @pytest.mark.parametrize("L", [(16, 8, 12), (64, 32, 34)])
@@ -520,7 +520,7 @@ def test_autotune_chooses_form_and_tile_shape():
         g.sweeps(30, 0)
         mode = g.sweep_mode()
         bs, spt = g.tile_shape()
-        assert mode in ("passes", "passes2", "persistent")
+        assert mode in ("passes", "passes2", "persistent", "direct")
         if mode == "persistent":
             assert (bs, spt) == (256, 1)
         else:
