@@ -413,19 +413,30 @@ __global__ void __launch_bounds__(BS, min_blocks_bs<R, BS, OCC>()) link3_kernel(
 }
 
 // ------------------------------------------------------------------ finalize
-// Work item w = (chain c, slot i): sum the partials of chain c in slot i in a
-// fixed order into totals[c][i].
-__device__ __forceinline__ void finalize_sum(const FinalizeArgs& f, int w) {
+// Work item w = (chain c, slot i), one warp: sum the tile partials of chain c
+// in slot i into totals[c][i].  Lane l adds the tiles l, l + 32, ... in
+// order and the lanes are combined by a fixed shuffle tree, so the order of
+// the sum does not depend on which warp or block takes the item (the
+// per-pass and persistent forms give the same bits).
+__device__ __forceinline__ void finalize_sum_warp(const FinalizeArgs& f, int w) {
+  const int lane = threadIdx.x & 31;
   const int c = w / f.nslots, i = w % f.nslots;
   const int b0 = f.blk_begin[c], b1 = f.blk_begin[c + 1];
   const double* part = f.part + (size_t)i * f.slot_stride;
   double v[kNQ] = {0.0, 0.0, 0.0, 0.0};
-  for (int b = b0 + threadIdx.x; b < b1; b += blockDim.x) {
+  for (int b = b0 + lane; b < b1; b += 32) {
 #pragma unroll
     for (int q = 0; q < kNQ; ++q) v[q] += __ldcg(part + (size_t)b * kNQ + q);
   }
-  __syncthreads();
-  block_reduce_store<kNQ>(v, f.totals + ((size_t)c * kMaxSlots + i) * kNQ);
+#pragma unroll
+  for (int q = 0; q < kNQ; ++q) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v[q] += __shfl_down_sync(0xffffffffu, v[q], o);
+  }
+  if (lane == 0) {
+#pragma unroll
+    for (int q = 0; q < kNQ; ++q) f.totals[((size_t)c * kMaxSlots + i) * kNQ + q] = v[q];
+  }
 }
 
 // Per chain, in slot order, the reference's normalisations; then advance the
@@ -524,12 +535,22 @@ __device__ __forceinline__ void finalize_combine(const FinalizeArgs& f) {
   }
 }
 
-// grid = nchains * nslots blocks (at least one); the last block to finish its
-// sum combines.
-__global__ void __launch_bounds__(256) finalize_kernel(FinalizeArgs f) {
+// kFinWarps warps per block, one (chain, slot) item per warp.  One block (a
+// single chain's slots): sum, then combine in the same block -- its own
+// global writes are visible to it after the barrier.  Several blocks (a
+// batch): the last block to finish, by an atomic ticket, combines.
+constexpr int kFinWarps = 32;
+__global__ void __launch_bounds__(kFinWarps * 32) finalize_kernel(FinalizeArgs f) {
   pdl_trigger();
   pdl_wait();
-  if ((int)blockIdx.x < f.nchains * f.nslots) finalize_sum(f, blockIdx.x);
+  const int nitems = f.nchains * f.nslots;
+  for (int w = blockIdx.x * kFinWarps + (threadIdx.x >> 5); w < nitems; w += gridDim.x * kFinWarps)
+    finalize_sum_warp(f, w);
+  if (gridDim.x == 1) {
+    __syncthreads();
+    finalize_combine(f);
+    return;
+  }
   __shared__ bool last;
   __threadfence();
   __syncthreads();
@@ -635,7 +656,11 @@ __global__ void __launch_bounds__(kBlock, kPersistMinBlocks) sweep_persistent_ke
     persistent_pass<R>(a, p, e);
     if (!grid_sync(a.bar, gridDim.x, target, &a.base.st->status)) return;
   }
-  for (int w = blockIdx.x; w < a.fin.nchains * a.fin.nslots; w += gridDim.x) finalize_sum(a.fin, w);
+  {
+    const int nw = (int)(blockDim.x >> 5);
+    for (int w = blockIdx.x * nw + (int)(threadIdx.x >> 5); w < a.fin.nchains * a.fin.nslots; w += gridDim.x * nw)
+      finalize_sum_warp(a.fin, w);
+  }
   if (!grid_sync(a.bar, gridDim.x, target, &a.base.st->status)) return;
   if (blockIdx.x == 0) {
     finalize_combine(a.fin);
@@ -750,9 +775,9 @@ void launch_link(int mode, int mu, const PassArgs& a, int nblocks, cudaStream_t 
 }
 
 void launch_finalize(const FinalizeArgs& f, cudaStream_t s) {
-  int grid = f.nchains * f.nslots;
+  int grid = (f.nchains * f.nslots + kFinWarps - 1) / kFinWarps;
   if (grid < 1) grid = 1;
-  (void)launch_pdl(finalize_kernel, grid, 256, 0, s, f);
+  (void)launch_pdl(finalize_kernel, grid, kFinWarps * 32, 0, s, f);
 }
 
 template <typename R>
