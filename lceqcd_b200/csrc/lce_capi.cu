@@ -767,13 +767,12 @@ lce_ctx* create_impl(const lce_params* p, int n, const SlabInfo* slab = nullptr)
       if (c->prec == LCE_PREC_F64 && b != kBlock) continue;
       c->tune.push_back(TuneForm{LCE_SWEEP_PASSES, b, 1, 0, {}});
       if (b != 512) c->tune.push_back(TuneForm{LCE_SWEEP_PASSES2, b, 2, 0, {}});
-      // 128 threads at a 56-register cap: nine blocks per SM, 12.5% more warps
-      if (b == 128) c->tune.push_back(TuneForm{LCE_SWEEP_PASSES, 128, 1, 1152, {}});
     }
-    // the per-pass kernels launched on the stream without a graph: no graph
-    // start, but every launch goes through the host
-    c->tune.push_back(TuneForm{LCE_SWEEP_DIRECT, reg56 ? 128 : (c->tile_req ? c->tile_req : kBlock), 1,
-                               reg56 ? 1152 : 0, {}});
+    // Not candidates, measured slower on the B200 at 64^3 and 128^3 (still
+    // selectable): the 56-register 128-thread form (tile_registers = 56,
+    // 71.1 / 381.1 us per sweep against 64.7 / 374-377 us) and the direct
+    // launches without a graph (LCE_SWEEP_DIRECT, 66.0 / 380.0 us against
+    // 64.6 / 377.5 us with the same tile).
     if (c->persist_grid > 0) c->tune.push_back(TuneForm{LCE_SWEEP_PERSISTENT, kBlock, 1, 0, {}});
   }
   if ((e = cudaMemset(c->meas_d, 0, sizeof(lce_meas) * n)) != cudaSuccess) return bail(e, "cudaMemset(meas)");

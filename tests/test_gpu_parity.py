@@ -320,7 +320,7 @@ def test_persistent_batch_and_autotune():
     for mode in ("passes", "persistent", "auto"):
         ens = Ensemble([Params(**{**s.__dict__, "sweep_mode": mode}) for s in specs])
         ens.init_hot(3)
-        ens.sweeps(30, 1)
+        ens.sweeps(40, 1)
         if mode == "auto":
             assert ens.sweep_mode() in ("passes", "passes2", "persistent", "direct")
         outs.append(([ens.download(chain=i) for i in range(2)], ens.meas_batch()))
@@ -448,7 +448,7 @@ def test_two_sites_per_thread_batch_and_three_way_autotune():
     for mode in ("passes", "passes2", "auto"):
         ens = Ensemble([Params(**{**s.__dict__, "sweep_mode": mode}) for s in specs])
         ens.init_hot(3)
-        ens.sweeps(30, 1)
+        ens.sweeps(40, 1)
         if mode == "auto":
             assert ens.sweep_mode() in ("passes", "passes2", "persistent", "direct")
         outs.append([ens.download(chain=i) for i in range(3)])
@@ -511,13 +511,13 @@ def test_autotune_chooses_form_and_tile_shape():
     L = (32, 32, 32)
     ref = Lattice(L, beta=12.0, x=0.09, y=0.3, seed=3, sweep_mode="passes", tile_threads=256)
     ref.init_hot(1)
-    ref.sweeps(30, 0)
+    ref.sweeps(40, 0)
     u_ref, a_ref = ref.download()
     ref.close()
     for req in (0, 128):
         g = Lattice(L, beta=12.0, x=0.09, y=0.3, seed=3, sweep_mode="auto", tile_threads=req)
         g.init_hot(1)
-        g.sweeps(30, 0)
+        g.sweeps(40, 0)
         mode = g.sweep_mode()
         bs, spt = g.tile_shape()
         assert mode in ("passes", "passes2", "persistent", "direct")
