@@ -81,24 +81,6 @@ __device__ __forceinline__ NbrOff nbr_offsets(const ChainDev& ch, Coord X) {
   return o;
 }
 
-// L2 prefetch of site s's elements of every field plane (6 link planes, 6 A
-// planes): all threads of a pass together cover every element, so the
-// neighbour gathers that follow find their lines in L2 or on the way.  Issued
-// by the first pass of a queue, which runs on the caches as it finds them
-// (cold after an L2 flush).  L2 is the point of coherence, so a prefetch
-// before griddepcontrol.wait cannot leave a stale line behind.
-__device__ __forceinline__ void prefetch_l2(const void* p) { asm volatile("prefetch.global.L2 [%0];" ::"l"(p)); }
-
-template <typename R>
-__device__ __forceinline__ void prefetch_site(const ChainDev& ch, int s) {
-  const char* u = reinterpret_cast<const char*>(ch.u);
-  const R* A = reinterpret_cast<const R*>(ch.a);
-#pragma unroll
-  for (int k = 0; k < 6; ++k) prefetch_l2(u + ((size_t)k * ch.nh + s) * LinkIO<R>::kBytes);
-#pragma unroll
-  for (int k = 0; k < 6; ++k) prefetch_l2(A + (size_t)k * ch.nh + s);
-}
-
 template <typename R, bool NC = true>
 __device__ __forceinline__ su2<R> ldU(const ChainDev& ch, int mu, int p, int s) {
   const size_t i = ((size_t)(mu * 2 + p)) * ch.nh + s;
@@ -202,11 +184,6 @@ __device__ __forceinline__ void higgs_tile(const PassArgs& p, int tile) {
   double q[3] = {0.0, 0.0, 0.0};
   constexpr int NS = MODE == 0 ? 7 : (MODE == 1 ? 1 : 4);
   const int layout = MODE == 2 ? kTriple : kPlanar;
-  if (PDL && p.trigger_late) {
-#pragma unroll 1
-    for (int r = 0; r < SPT; ++r)
-      if (s0 + r * BS < s_hi) prefetch_site<R>(ch, s0 + r * BS);
-  }
   // the first site's uniforms, drawn before the wait when the counters are settled
   Uniforms<R, NS> Un0;
   const bool early = PDL && SPT == 1 && p.rng_early && s0 < s_hi;
@@ -323,11 +300,6 @@ __device__ __forceinline__ void link_tile(const PassArgs& p, int tile) {
   const Coord X0 = site_coord(eo, s0 < s_hi ? s0 : p.s_lo, ch.hx, ch.nxy, ch.dhx, ch.dnxy);
   unsigned cnt[2] = {0u, 0u};
   double pl[1] = {0.0};
-  if (PDL && p.trigger_late) {
-#pragma unroll 1
-    for (int r = 0; r < SPT; ++r)
-      if (s0 + r * BS < s_hi) prefetch_site<R>(ch, s0 + r * BS);
-  }
   // the first site's uniforms (of the first hit), drawn before the wait when
   // the counters are settled
   Uniforms<R, OR ? 1 : 7> Un0;
