@@ -227,20 +227,6 @@ int lce_get_sweep_mode(lce_ctx* ctx);
  * thread and the per-thread register cap they are compiled for (a tuned
  * choice once lce_get_sweep_mode is no longer AUTO); any output may be NULL */
 int lce_get_tile_shape(lce_ctx* ctx, int* threads, int* sites_per_thread, int* register_cap);
-/* Chaining of the per-pass kernels (on = 1, or 0: every pass waits for the
- * whole previous pass).  Plane-synchronised: a tile of pass i starts once
- * pass i-1 has finished the z-planes it reads (z-1, z, z+1), counted on
- * per-plane completion counters, so the drain of a pass overlaps the start of
- * the next; the results are the same bit for bit.  Used by FP32 contexts on
- * whole lattices whose tiles are plane-aligned (L1*L2/2 a multiple of the
- * tile's sites); others keep the whole-pass wait. */
-int lce_set_plane_sync(lce_ctx* ctx, int on);
-/* returns 1 if plane synchronisation is switched on (0 if off, < 0 on error);
- * active: whether the sweeps of the tile shape in use run with it; fallbacks:
- * tiles that gave up polling a plane counter and waited for the whole
- * previous pass instead (a slow path with the same result; expected 0).
- * Either output may be NULL. */
-int lce_get_plane_sync(lce_ctx* ctx, int* active, unsigned* fallbacks);
 /* f/meas1.f inputs: the last measured quantities of a chain */
 int lce_get_meas(lce_ctx* ctx, int chain, lce_meas* m);
 int lce_get_meas_batch(lce_ctx* ctx, lce_meas* m /* [nchains] */);

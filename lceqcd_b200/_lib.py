@@ -113,8 +113,6 @@ SIGNATURES = {
     "lce_sweeps": (I, [P, I, I]),
     "lce_get_sweep_mode": (I, [P]),
     "lce_get_tile_shape": (I, [P, P, P, P]),
-    "lce_set_plane_sync": (I, [P, I]),
-    "lce_get_plane_sync": (I, [P, P, P]),
     "lce_get_meas": (I, [P, I, P]),
     "lce_get_meas_batch": (I, [P, P]),
     "lce_landau_gauge": (I, [P, I, P, P, I]),

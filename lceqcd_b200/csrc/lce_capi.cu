@@ -103,11 +103,6 @@ struct lce_ctx {
   int tile_bs = kBlock, tile_spt = 1;  // tile shape of the per-pass kernels in use
   int tile_occ = 0;                    // its register-cap occupancy (0: the default)
   std::vector<TuneForm> tune;        // autotune candidates and their samples
-  // per-plane completion counters of plane-synchronised queues (one per
-  // z-plane of every chain), and whether queues use them where they can
-  unsigned* plane_cnt_d = nullptr;
-  int nplanes = 0;
-  bool plane_sync = false;
   std::map<std::pair<int, int>, cudaGraphExec_t> gf_exec;
   std::string err;
 };
@@ -261,7 +256,6 @@ struct Enq {
   const std::vector<int>* blk = nullptr;
   int* blk_d = nullptr;
   int spt = 1, bs = kBlock, occ = 0;
-  bool plane = false;  // passes chained by the per-plane counters
   int measflag = 0;
   bool fuse = false;
   unsigned long long soff = 0;
@@ -271,17 +265,6 @@ struct Enq {
 
 // index of the chain table for tiles of bs * spt sites (128, 256 or 512)
 int tile_index(int bs, int spt) { return bs * spt == 128 ? 0 : (bs * spt == 256 ? 1 : 2); }
-
-// Can a queue of this context with this tile shape chain its passes by the
-// per-plane counters?  FP32, whole lattices (no z-slab), a compiled shape and
-// plane-aligned tiles in every chain.
-bool plane_sync_ok(const lce_ctx* c, int bs, int spt, int occ) {
-  if (!c->plane_sync || !c->plane_cnt_d || c->prec != LCE_PREC_F32 || c->s_lo != 0 || c->site_off != 0) return false;
-  if (!plane_sync_shape(bs, spt, occ)) return false;
-  for (const ChainDev& d : c->ch)
-    if (d.nxy % (bs * spt) != 0) return false;
-  return true;
-}
 
 void enq_begin(lce_ctx* c, const std::vector<unsigned char>& routines, int measflag, bool fuse_renorm, int bs,
                int spt, int occ, Enq& q) {
@@ -293,7 +276,6 @@ void enq_begin(lce_ctx* c, const std::vector<unsigned char>& routines, int measf
   q.occ = occ;
   q.measflag = measflag;
   q.fuse = fuse_renorm;
-  q.plane = plane_sync_ok(c, bs, spt, occ);
   q.passes.clear();
   for (unsigned char r : routines) expand(r, q.passes);
   FinalizeArgs& f = q.f;
@@ -308,8 +290,6 @@ void enq_begin(lce_ctx* c, const std::vector<unsigned char>& routines, int measf
   f.totals = c->totals_d;
   f.nchains = c->nchains;
   f.single = c->prec == LCE_PREC_F32;
-  f.plane_cnt = q.plane ? c->plane_cnt_d : nullptr;
-  f.nplanes = q.plane ? c->nplanes : 0;
   q.soff = 0;
   q.poff = 0;
   q.slot = 0;
@@ -344,8 +324,6 @@ int enq_pass(lce_ctx* c, Enq& q, size_t i) {
   // later passes follow pass kernels of this queue only
   a.rng_early = i > 0 ? 1 : 0;
   a.trigger_late = i == 0 ? 1 : 0;
-  a.plane_cnt = q.plane ? c->plane_cnt_d : nullptr;
-  a.plane_wait = q.plane ? (int)i : 0;
   if (ps.kind <= kHiggsMetro) {
     if (c->prec == LCE_PREC_F64) launch_higgs<double>(ps.kind, a, nblocks, c->stream);
     else launch_higgs<float>(ps.kind, a, nblocks, c->stream);
@@ -383,15 +361,7 @@ int enqueue(lce_ctx* c, const std::vector<unsigned char>& routines, int measflag
   }
   enq_begin(c, routines, measflag, fuse_renorm, bs, spt, occ, q);
   for (size_t i = 0; i < q.passes.size(); ++i) {
-    if (int rc = enq_pass(c, q, i)) {
-      // passes already queued have counted on the plane counters and no
-      // finalize follows to reset them (outside a capture, where they run)
-      cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
-      if (q.plane && i > 0 && cudaStreamIsCapturing(c->stream, &cs) == cudaSuccess &&
-          cs == cudaStreamCaptureStatusNone)
-        (void)cudaMemsetAsync(c->plane_cnt_d, 0, sizeof(unsigned) * c->nplanes, c->stream);
-      return rc;
-    }
+    if (int rc = enq_pass(c, q, i)) return rc;
     if (events) CK(cudaEventRecord(events[i], c->stream));
   }
   return enq_end(c, q);
@@ -425,8 +395,6 @@ int enqueue_persistent(lce_ctx* c, const std::vector<unsigned char>& routines, i
   b.stream_nh = c->stream_nh;
   b.rng_early = 0;
   b.trigger_late = 0;
-  b.plane_cnt = nullptr;
-  b.plane_wait = 0;
   FinalizeArgs& f = a.fin;
   f.chains = c->ch_d;
   f.blk_begin = c->blk_d;
@@ -724,8 +692,6 @@ lce_ctx* create_impl(const lce_params* p, int n, const SlabInfo* slab = nullptr)
 
     offs.push_back(off);
     off += 2 * (align256((size_t)6 * d.nh * lb) + align256((size_t)6 * d.nh * rb)) + align256((size_t)2 * d.nh * lb);
-    d.plane_off = c->nplanes;
-    c->nplanes += d.L3;
     c->ch.push_back(d);
     const int nvis = slab ? d.nh - 2 * d.nxy : d.nh;  // sites a pass visits per parity
     for (int t = 0; t < 3; ++t) c->tiles[t].push_back(c->tiles[t].back() + ceil_div(nvis, 128 << t));
@@ -769,10 +735,6 @@ lce_ctx* create_impl(const lce_params* p, int n, const SlabInfo* slab = nullptr)
   if ((e = cudaMalloc(&c->meas_d, sizeof(lce_meas) * n)) != cudaSuccess) return bail(e, "cudaMalloc(meas)");
   if ((e = cudaMalloc(&c->bar_d, sizeof(GridBar))) != cudaSuccess) return bail(e, "cudaMalloc(barrier)");
   if ((e = cudaMemset(c->bar_d, 0, sizeof(GridBar))) != cudaSuccess) return bail(e, "cudaMemset(barrier)");
-  if ((e = cudaMalloc(&c->plane_cnt_d, sizeof(unsigned) * c->nplanes)) != cudaSuccess)
-    return bail(e, "cudaMalloc(plane counters)");
-  if ((e = cudaMemset(c->plane_cnt_d, 0, sizeof(unsigned) * c->nplanes)) != cudaSuccess)
-    return bail(e, "cudaMemset(plane counters)");
   c->sweep_mode = p[0].sweep_mode;
   c->mode = p[0].sweep_mode;
   c->persist_grid = c->prec == LCE_PREC_F64 ? persistent_grid<double>() : persistent_grid<float>();
@@ -1456,7 +1418,7 @@ void lce_destroy(lce_ctx* c) {
   for (auto& kv : c->fa_exec) cudaGraphExecDestroy(kv.second);
   void* ptrs[] = {c->ch_d, c->tiles_d[0], c->tiles_d[1], c->tiles_d[2], c->st_d, c->cst_d, c->meas_d, c->part_d, c->totals_d,
                   c->scratch_d, c->fields_d, c->stream_d, c->staging_d, c->flush_d, c->bar_d,
-                  c->gsave_d, c->fa_d, c->plane_cnt_d};
+                  c->gsave_d, c->fa_d};
   for (void* q : ptrs)
     if (q) cudaFree(q);
   if (c->ev0) cudaEventDestroy(c->ev0);
@@ -1711,33 +1673,6 @@ int lce_get_tile_shape(lce_ctx* c, int* threads, int* sites_per_thread, int* reg
     *register_cap = std::min(255, (65536 / occ) & ~7);
   }
   return LCE_OK;
-}
-
-int lce_set_plane_sync(lce_ctx* c, int on) {
-  DeviceScope ds_(c ? c->device : -1);
-  if (!c || (on != 0 && on != 1)) return LCE_ERR_INVALID;
-  if (c->plane_sync == (on == 1)) return LCE_OK;
-  // the cached sweep graphs were built for the other chaining
-  CK(cudaStreamSynchronize(c->stream));
-  for (auto& kv : c->sweep_graphs)
-    if (kv.second) cudaGraphExecDestroy(kv.second);
-  c->sweep_graphs.clear();
-  c->plane_sync = on == 1;
-  return LCE_OK;
-}
-
-int lce_get_plane_sync(lce_ctx* c, int* active, unsigned* fallbacks) {
-  DeviceScope ds_(c ? c->device : -1);
-  if (!c) return LCE_ERR_INVALID;
-  if (active)
-    *active = c->mode != LCE_SWEEP_PERSISTENT && plane_sync_ok(c, c->tile_bs, c->tile_spt, c->tile_occ) ? 1 : 0;
-  if (fallbacks) {
-    CtxState st;
-    CK(cudaMemcpyAsync(&st, c->st_d, sizeof(st), cudaMemcpyDeviceToHost, c->stream));
-    CK(cudaStreamSynchronize(c->stream));
-    *fallbacks = st.plane_fallbacks;
-  }
-  return c->plane_sync ? 1 : 0;
 }
 
 int lce_sweep(lce_ctx* c, int measflag, lce_meas* m) {

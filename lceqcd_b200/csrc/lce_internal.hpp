@@ -54,8 +54,6 @@ struct ChainDev {
   void* uf;
   void* af;
   void* g;   // gauge transform of the last tracked gauge fixing, [parity][site]
-  int plane_off;  // this chain's first z-plane counter (plane-synchronised passes)
-  int pad_;
 };
 
 // mutable state shared by the chains of one context
@@ -64,8 +62,6 @@ struct CtxState {
   unsigned long long stream_pos;  // validation-stream position
   unsigned int status;            // LCE_STATUS_* bits
   unsigned int ticket;            // last-block ticket of the finalize kernel
-  unsigned int plane_fallbacks;   // plane-synchronised tiles that fell back to the grid wait
-  unsigned int pad_;
 };
 
 // per-chain mutable state
@@ -135,12 +131,6 @@ struct PassArgs {
   // kernel's wait (the first pass of a queue, so that no later pass can read
   // the counters while an earlier finalize still writes them).
   int rng_early, trigger_late;
-  // plane-synchronised queue (lce_update.cu): the per-plane completion
-  // counters, or null for passes chained by whole-grid completion;
-  // plane_wait: this pass's index in the queue (0: the first pass, which
-  // waits for the stream's earlier work with griddepcontrol.wait)
-  unsigned* plane_cnt;
-  int plane_wait;
 };
 
 struct FinalizeArgs {
@@ -157,8 +147,6 @@ struct FinalizeArgs {
   unsigned int npasses;           // advance of st->pass_ctr
   unsigned long long nstream;     // advance of st->stream_pos
   int single;                     // FP32 arithmetic for the ahiggs1 step update
-  unsigned* plane_cnt;            // plane counters to reset (plane-synchronised queue) or null
-  int nplanes;
   unsigned char kinds[kMaxSlots];
 };
 
@@ -183,7 +171,6 @@ void launch_higgs(int mode, const PassArgs& a, int nblocks, cudaStream_t s);
 template <typename R>
 void launch_link(int mode, int mu, const PassArgs& a, int nblocks, cudaStream_t s);
 void launch_finalize(const FinalizeArgs& f, cudaStream_t s);
-bool plane_sync_shape(int bs, int spt, int occ);  // tile shapes compiled for plane-synchronised queues
 template <typename R>
 void launch_renorm(void* u, size_t nlinks, cudaStream_t s);
 template <typename R>

@@ -48,31 +48,17 @@ __device__ __forceinline__ int find_chain(const int* blk_begin, int n, int b) {
   return lo;
 }
 
-// Field loads, by the execution form (LD):
-//   kLdNc     the read-only (non-coherent) path: per-pass kernels that start
-//             after the previous pass has completed (griddepcontrol.wait), so
-//             no writer runs while the kernel reads;
-//   kLdCg     L2 loads (ld.global.cg) for the persistent form, where fields
-//             written by other blocks before a grid barrier are read after it.
-//             Non-coherent loads are not enough there: measured on B200, lines
-//             an SM's L1 fetched before the barrier were still served after it
-//             (the persistent sweep then differs from the per-pass sweep);
-//   kLdPlain  coherent cached loads (ld.global.ca) for per-pass kernels that
-//             start on per-plane completion counters while the previous pass
-//             is still running elsewhere (plane_wait below): the acquire of the
-//             counters orders them after the previous pass's writes.
-enum : int { kLdCg = 0, kLdNc = 1, kLdPlain = 2 };
-
-template <int LD, typename T>
-__device__ __forceinline__ T ld_sel(const T* q) {
-  if constexpr (LD == kLdNc) return __ldg(q);
-  else if constexpr (LD == kLdCg) return __ldcg(q);
-  else return __ldca(q);
-}
-
-template <typename R, int LD = kLdNc>
+// Field loads.  NC = true: the read-only (non-coherent) path, valid when no
+// earlier writer runs in the same kernel (the per-pass form).  NC = false:
+// L2 loads (ld.global.cg) for the persistent form, where fields written by
+// other blocks before a grid barrier are read after it.  Ordinary cached
+// loads are not enough there: measured on B200, lines an SM's L1 fetched
+// before the barrier were still served after it (the persistent sweep then
+// differs from the per-pass sweep), so L1 is bypassed.
+template <typename R, bool NC = true>
 __device__ __forceinline__ R ldA(const R* A, int nh, int p, int k, int s) {
-  return ld_sel<LD>(A + ((size_t)(p * 3 + k)) * nh + s);
+  const R* q = A + ((size_t)(p * 3 + k)) * nh + s;
+  return NC ? __ldg(q) : __ldcg(q);
 }
 
 // Neighbour offsets of one site.  The half-row index s = z*nxy + y*hx + (x>>1)
@@ -95,169 +81,69 @@ __device__ __forceinline__ NbrOff nbr_offsets(const ChainDev& ch, Coord X) {
   return o;
 }
 
-template <typename R, int LD>
-__device__ __forceinline__ su2<R> ld_link(const void* base, size_t i) {
-  if constexpr (sizeof(R) == 4) {
-    const float4 v = ld_sel<LD>(reinterpret_cast<const float4*>(base) + i);
-    return su2<R>{{v.x, v.y}, {v.z, v.w}};
-  } else {
-    const double2* q = reinterpret_cast<const double2*>(base) + 2 * i;
-    const double2 x = ld_sel<LD>(q), y = ld_sel<LD>(q + 1);
-    return su2<R>{{x.x, x.y}, {y.x, y.y}};
-  }
-}
-
-template <typename R, int LD = kLdNc>
+template <typename R, bool NC = true>
 __device__ __forceinline__ su2<R> ldU(const ChainDev& ch, int mu, int p, int s) {
-  return ld_link<R, LD>(ch.u, ((size_t)(mu * 2 + p)) * ch.nh + s);
-}
-
-// ------------------------------------------------------------------ plane-synchronised passes
-// A queue of per-pass kernels can chain its passes through per-plane
-// completion counters instead of whole-grid completion.  Every update of a
-// site in z-plane z reads (and every field it writes is read by) sites of the
-// planes z-1, z, z+1 only (periodic): the staples' x+mu-nu corners and the
-// Higgs force's x+-mu neighbours.  So a tile of pass i may start once pass
-// i-1 has finished those three planes, while other tiles of pass i-1 are
-// still running: the drain of one pass overlaps the start of the next.
-//
-//   * Tiles are plane-aligned (nxy a multiple of the tile's sites) and are
-//     dispatched plane by plane in the folded order z = 0, L3-1, 1, L3-2, ...,
-//     so that the periodic neighbours of a plane are dispatched within two
-//     planes of it.  A tile keeps its natural index (z * tiles per plane +
-//     position) for its partial sums, so the reduction is the same bit for
-//     bit.
-//   * A tile adds 1 to its plane's counter after its last write (block
-//     barrier, then a release add by one thread).  Every pass adds exactly
-//     tpp = nxy / tile sites to each plane, and a tile of pass i starts only
-//     after pass i-1 finished its own plane, so counter[z] >= i * tpp holds
-//     exactly when passes 0..i-1 are done with plane z.
-//   * Pass i >= 1 polls the three counters with acquire loads (three threads,
-//     bounded, short sleeps) and reads the fields with coherent loads
-//     (kLdPlain) after the block barrier.  If a poll runs out it falls back
-//     to griddepcontrol.wait -- the completion of pass i-1, which never
-//     depends on pass i -- and counts the fallback: the result is the same.
-//   * Pass 0 waits for the stream's earlier work with griddepcontrol.wait.
-//     No pass can deadlock: a dependent grid launches only when every block of
-//     the previous grid has started (each triggers before it waits).
-//   * The finalize kernel, which runs after the last pass has completed,
-//     zeroes the counters for the next queue.
-constexpr unsigned kPlaneSpinLimit = 1u << 16;  // polls (>= 64 ns sleep each) before the fallback
-
-__device__ __forceinline__ void red_release_add(unsigned* p, unsigned v) {
-  asm volatile("red.release.gpu.global.add.u32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
-}
-__device__ __forceinline__ unsigned ld_acquire(const unsigned* p) {
-  unsigned v;
-  asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
-  return v;
-}
-
-// First site (of the chain, natural order) and natural tile index of the tile
-// that block `tile` processes; z: its plane (plane-synchronised queues).
-struct TilePos {
-  int s, tile, z;
-};
-template <int LD, int TS>
-__device__ __forceinline__ TilePos tile_pos(const PassArgs& p, const ChainDev& ch, int b0, int tile) {
-  const int local = (tile - b0) * TS;
-  if constexpr (LD != kLdPlain) {
-    return TilePos{p.s_lo + local, tile, 0};
-  } else {
-    const int f = (int)fdiv((uint32_t)local, ch.dnxy);  // folded plane position
-    const int z = (f & 1) ? ch.L3 - 1 - (f >> 1) : (f >> 1);
-    const int s = z * ch.nxy + (local - f * ch.nxy);
-    return TilePos{s, b0 + s / TS, z};
-  }
-}
-
-// Wait for passes 0..plane_wait-1 on the planes z-1, z, z+1 (see above).
-template <int TS>
-__device__ __forceinline__ void plane_wait(const PassArgs& p, const ChainDev& ch, int z) {
-  bool late = false;
-  if (threadIdx.x < 3) {
-    int zz = z + (int)threadIdx.x - 1;
-    zz = zz < 0 ? zz + ch.L3 : (zz >= ch.L3 ? zz - ch.L3 : zz);
-    const unsigned* cnt = p.plane_cnt + ch.plane_off + zz;
-    const unsigned target = (unsigned)p.plane_wait * (unsigned)(ch.nxy / TS);
-    unsigned n = 0;
-    while (ld_acquire(cnt) < target) {
-      if (++n >= kPlaneSpinLimit) {
-        late = true;
-        break;
-      }
-      __nanosleep(64);
-    }
-  }
-  if (__syncthreads_or(late)) {
-    pdl_wait();
-    if (threadIdx.x == 0) atomicAdd(&p.st->plane_fallbacks, 1u);
-  }
-}
-
-// The tile's writes are done: count it on its plane.
-__device__ __forceinline__ void plane_signal(const PassArgs& p, const ChainDev& ch, int z) {
-  __syncthreads();
-  if (threadIdx.x == 0) red_release_add(p.plane_cnt + ch.plane_off + z, 1u);
+  const size_t i = ((size_t)(mu * 2 + p)) * ch.nh + s;
+  return NC ? LinkIO<R>::ld(ch.u, i) : LinkIO<R>::ld_cg(ch.u, i);
 }
 
 // f/staples.f:65-221: for each nu != mu (ascending),
 //   upper  = U_nu(x+mu) [U_mu(x+nu)^+ U_nu(x)^+]          (NN of DD)
 //   lower  = U_nu(x-nu+mu)^+ [U_mu(x-nu)^+ U_nu(x-nu)]    (DN of DN)
 //   V      = (V + upper) + lower
-template <typename R, int MU, int NU, int LD>
+template <typename R, int MU, int NU, bool NC>
 __device__ __forceinline__ void staple_add(const ChainDev& ch, int eo, const NbrOff& o, int s, su2<R>& V) {
   const int oe = 1 - eo;
   const int xpmu = s + o.p[MU], xpnu = s + o.p[NU], xmnu = s + o.m[NU];
   const int xmnupmu = xmnu + o.p[MU];
-  su2<R> up1 = dd(ldU<R, LD>(ch, MU, oe, xpnu), ldU<R, LD>(ch, NU, eo, s));
-  su2<R> up2 = nn(ldU<R, LD>(ch, NU, oe, xpmu), up1);
-  su2<R> bt1 = dn(ldU<R, LD>(ch, MU, oe, xmnu), ldU<R, LD>(ch, NU, oe, xmnu));
-  su2<R> bt2 = dn(ldU<R, LD>(ch, NU, eo, xmnupmu), bt1);
+  su2<R> up1 = dd(ldU<R, NC>(ch, MU, oe, xpnu), ldU<R, NC>(ch, NU, eo, s));
+  su2<R> up2 = nn(ldU<R, NC>(ch, NU, oe, xpmu), up1);
+  su2<R> bt1 = dn(ldU<R, NC>(ch, MU, oe, xmnu), ldU<R, NC>(ch, NU, oe, xmnu));
+  su2<R> bt2 = dn(ldU<R, NC>(ch, NU, eo, xmnupmu), bt1);
   V.a = (V.a + up2.a) + bt2.a;
   V.b = (V.b + up2.b) + bt2.b;
 }
 
-template <typename R, int MU, int LD = kLdNc>
+template <typename R, int MU, bool NC = true>
 __device__ __forceinline__ su2<R> staple(const ChainDev& ch, int eo, const NbrOff& o, int s) {
   su2<R> V{{(R)0, (R)0}, {(R)0, (R)0}};
   if (MU == 0) {
-    staple_add<R, 0, 1, LD>(ch, eo, o, s, V);
-    staple_add<R, 0, 2, LD>(ch, eo, o, s, V);
+    staple_add<R, 0, 1, NC>(ch, eo, o, s, V);
+    staple_add<R, 0, 2, NC>(ch, eo, o, s, V);
   } else if (MU == 1) {
-    staple_add<R, 1, 0, LD>(ch, eo, o, s, V);
-    staple_add<R, 1, 2, LD>(ch, eo, o, s, V);
+    staple_add<R, 1, 0, NC>(ch, eo, o, s, V);
+    staple_add<R, 1, 2, NC>(ch, eo, o, s, V);
   } else {
-    staple_add<R, 2, 0, LD>(ch, eo, o, s, V);
-    staple_add<R, 2, 1, LD>(ch, eo, o, s, V);
+    staple_add<R, 2, 0, NC>(ch, eo, o, s, V);
+    staple_add<R, 2, 1, NC>(ch, eo, o, s, V);
   }
   return V;
 }
 
 // f/a_force.f:54-110: F = sum_mu [U(x)(iA(x+mu))U(x)^+ + U(x-mu)^+(iA(x-mu))U(x-mu)],
 // components F3 = Im(.)_a, F2 = Re(.)_b, F1 = Im(.)_b
-template <typename R, int MU, int LD>
+template <typename R, int MU, bool NC>
 __device__ __forceinline__ void force_add(const ChainDev& ch, int eo, const NbrOff& o, int s, R& f1, R& f2,
                                           R& f3) {
   const int oe = 1 - eo, nh = ch.nh;
   const R* A = reinterpret_cast<const R*>(ch.a);
   const int xp = s + o.p[MU], xm = s + o.m[MU];
-  su2<R> ux = ldU<R, LD>(ch, MU, eo, s);
-  su2<R> ud = ldU<R, LD>(ch, MU, oe, xm);
-  su2<R> t1 = nn(ux, ad(ldA<R, LD>(A, nh, oe, 0, xp), ldA<R, LD>(A, nh, oe, 1, xp), ldA<R, LD>(A, nh, oe, 2, xp), ux));
-  su2<R> tb = dn(ud, an(ldA<R, LD>(A, nh, oe, 0, xm), ldA<R, LD>(A, nh, oe, 1, xm), ldA<R, LD>(A, nh, oe, 2, xm), ud));
+  su2<R> ux = ldU<R, NC>(ch, MU, eo, s);
+  su2<R> ud = ldU<R, NC>(ch, MU, oe, xm);
+  su2<R> t1 = nn(ux, ad(ldA<R, NC>(A, nh, oe, 0, xp), ldA<R, NC>(A, nh, oe, 1, xp), ldA<R, NC>(A, nh, oe, 2, xp), ux));
+  su2<R> tb = dn(ud, an(ldA<R, NC>(A, nh, oe, 0, xm), ldA<R, NC>(A, nh, oe, 1, xm), ldA<R, NC>(A, nh, oe, 2, xm), ud));
   f3 = f3 + (t1.a.im + tb.a.im);
   f2 = f2 + (t1.b.re + tb.b.re);
   f1 = f1 + (t1.b.im + tb.b.im);
 }
 
-template <typename R, int LD = kLdNc>
+template <typename R, bool NC = true>
 __device__ __forceinline__ void higgs_force(const ChainDev& ch, int eo, const NbrOff& o, int s, R& f1, R& f2,
                                             R& f3) {
   f1 = f2 = f3 = (R)0;
-  force_add<R, 0, LD>(ch, eo, o, s, f1, f2, f3);
-  force_add<R, 1, LD>(ch, eo, o, s, f1, f2, f3);
-  force_add<R, 2, LD>(ch, eo, o, s, f1, f2, f3);
+  force_add<R, 0, NC>(ch, eo, o, s, f1, f2, f3);
+  force_add<R, 1, NC>(ch, eo, o, s, f1, f2, f3);
+  force_add<R, 2, NC>(ch, eo, o, s, f1, f2, f3);
 }
 
 // Set up the uniform source of this pass (of hit `hit` of a multi-hit pass:
@@ -282,18 +168,16 @@ __device__ __forceinline__ bool setup_uniforms(const PassArgs& p, const ChainDev
 
 // ------------------------------------------------------------------ Higgs
 // One tile (BS * SPT consecutive sites of one chain, BS threads) of a Higgs
-// pass.  LD: the execution form (field loads above); the per-pass forms
-// (kLdNc, kLdPlain) trigger dependents and wait for the previous pass.
-template <typename R, int MODE, int LD, int SPT = 1, int BS = kBlock>
+// pass.  PDL: trigger dependents and wait for the previous kernel (per-pass
+// form only).
+template <typename R, int MODE, bool PDL, int SPT = 1, int BS = kBlock>
 __device__ __forceinline__ void higgs_tile(const PassArgs& p, int tile) {
-  constexpr bool PDL = LD != kLdCg;
   if (PDL && !p.trigger_late) pdl_trigger();
   // the chain table is written once at context creation: safe before pdl_wait
   const int c = p.nchains > 1 ? find_chain(p.blk_begin, p.nchains, tile) : 0;
   const ChainDev& ch = p.chains[c];
   // a tile is BS * SPT consecutive sites; thread t takes t, t + BS, ...
-  const TilePos tp = tile_pos<LD, BS * SPT>(p, ch, __ldg(p.blk_begin + c), tile);
-  const int s0 = tp.s + threadIdx.x;
+  const int s0 = p.s_lo + (tile - __ldg(p.blk_begin + c)) * BS * SPT + threadIdx.x;
   const int eo = p.eo, nh = ch.nh, s_hi = nh - p.s_lo;
   const Coord X0 = site_coord(eo, s0 < s_hi ? s0 : p.s_lo, ch.hx, ch.nxy, ch.dhx, ch.dnxy);
   unsigned acc[1] = {0u};
@@ -305,8 +189,7 @@ __device__ __forceinline__ void higgs_tile(const PassArgs& p, int tile) {
   const bool early = PDL && SPT == 1 && p.rng_early && s0 < s_hi;
   const bool ok0 = early ? setup_uniforms<R, NS>(p, ch, s0, layout, Un0) : false;
   if (PDL) {
-    if (LD == kLdPlain && p.plane_wait) plane_wait<BS * SPT>(p, ch, tp.z);
-    else pdl_wait();
+    pdl_wait();
     if (p.trigger_late) pdl_trigger();
   }
 #pragma unroll 1
@@ -318,7 +201,7 @@ __device__ __forceinline__ void higgs_tile(const PassArgs& p, int tile) {
     Uniforms<R, NS> Un = Un0;
     if (r == 0 && early ? ok0 : setup_uniforms<R, NS>(p, ch, s, layout, Un)) {
       R f[3];
-      higgs_force<R, LD>(ch, eo, no, s, f[0], f[1], f[2]);
+      higgs_force<R, PDL>(ch, eo, no, s, f[0], f[1], f[2]);
       R* A = reinterpret_cast<R*>(ch.a);
       R ao[3], an_[3];
 #pragma unroll
@@ -399,23 +282,20 @@ __device__ __forceinline__ void higgs_tile(const PassArgs& p, int tile) {
     }
   }
   // partials {accepted, sum rho, sum rho^2, sum a.F}
-  if (p.part) block_reduce_cs<1, 3, kNQ>(acc, q, p.part + (size_t)tp.tile * kNQ);
-  if (LD == kLdPlain) plane_signal(p, ch, tp.z);
+  if (p.part) block_reduce_cs<1, 3, kNQ>(acc, q, p.part + (size_t)tile * kNQ);
 }
 
 // ------------------------------------------------------------------ links
 // NHIT = 3 is f/agauge1.f: the staple is built once and the heatbath +
 // Metropolis hit is repeated on the updated link, each hit with its own
 // uniforms (f/agauge1.f:95-198).
-template <typename R, int MU, int OR, int LD, int NHIT = 1, int SPT = 1, int BS = kBlock>
+template <typename R, int MU, int OR, bool PDL, int NHIT = 1, int SPT = 1, int BS = kBlock>
 __device__ __forceinline__ void link_tile(const PassArgs& p, int tile) {
-  constexpr bool PDL = LD != kLdCg;
   if (PDL && !p.trigger_late) pdl_trigger();
   const int c = p.nchains > 1 ? find_chain(p.blk_begin, p.nchains, tile) : 0;
   const ChainDev& ch = p.chains[c];
   // a tile is BS * SPT consecutive sites; thread t takes t, t + BS, ...
-  const TilePos tp = tile_pos<LD, BS * SPT>(p, ch, __ldg(p.blk_begin + c), tile);
-  const int s0 = tp.s + threadIdx.x;
+  const int s0 = p.s_lo + (tile - __ldg(p.blk_begin + c)) * BS * SPT + threadIdx.x;
   const int eo = p.eo, oe = 1 - eo, nh = ch.nh, s_hi = nh - p.s_lo;
   const Coord X0 = site_coord(eo, s0 < s_hi ? s0 : p.s_lo, ch.hx, ch.nxy, ch.dhx, ch.dnxy);
   unsigned cnt[2] = {0u, 0u};
@@ -426,8 +306,7 @@ __device__ __forceinline__ void link_tile(const PassArgs& p, int tile) {
   const bool early = PDL && SPT == 1 && p.rng_early && s0 < s_hi;
   const bool ok0 = early ? setup_uniforms<R, OR ? 1 : 7>(p, ch, s0, OR ? kPlanar : kTriple, Un0) : false;
   if (PDL) {
-    if (LD == kLdPlain && p.plane_wait) plane_wait<BS * SPT>(p, ch, tp.z);
-    else pdl_wait();
+    pdl_wait();
     if (p.trigger_late) pdl_trigger();
   }
 #pragma unroll 1
@@ -438,17 +317,17 @@ __device__ __forceinline__ void link_tile(const PassArgs& p, int tile) {
     const NbrOff no = nbr_offsets(ch, X);
     Uniforms<R, OR ? 1 : 7> Un = Un0;
     if (r == 0 && early ? ok0 : setup_uniforms<R, OR ? 1 : 7>(p, ch, s, OR ? kPlanar : kTriple, Un)) {
-      const su2<R> V = staple<R, MU, LD>(ch, eo, no, s);
+      const su2<R> V = staple<R, MU, PDL>(ch, eo, no, s);
       const size_t li = ((size_t)(MU * 2 + eo)) * nh + s;
-      su2<R> uo = ld_link<R, LD>(ch.u, li);
+      su2<R> uo = PDL ? LinkIO<R>::ld(ch.u, li) : LinkIO<R>::ld_cg(ch.u, li);
       // f/agauge.f:71-84: normalised staple, 1/(beta |V|), 1/2 Re Tr(U Vhat)
       const R tn = M<R>::rsqrt(norm2(V));
       const su2<R> vh{{tn * V.a.re, tn * V.a.im}, {tn * V.b.re, tn * V.b.im}};
       // f/agauge.f:126-174 hopping term beta_a Re[(iA(x) U)(iA(x+mu) U^+)]_11 and accept
       const R* A = reinterpret_cast<const R*>(ch.a);
       const int xp = s + no.p[MU];
-      const R x1 = ldA<R, LD>(A, nh, eo, 0, s), x2 = ldA<R, LD>(A, nh, eo, 1, s), x3 = ldA<R, LD>(A, nh, eo, 2, s);
-      const R y1 = ldA<R, LD>(A, nh, oe, 0, xp), y2 = ldA<R, LD>(A, nh, oe, 1, xp), y3 = ldA<R, LD>(A, nh, oe, 2, xp);
+      const R x1 = ldA<R, PDL>(A, nh, eo, 0, s), x2 = ldA<R, PDL>(A, nh, eo, 1, s), x3 = ldA<R, PDL>(A, nh, eo, 2, s);
+      const R y1 = ldA<R, PDL>(A, nh, oe, 0, xp), y2 = ldA<R, PDL>(A, nh, oe, 1, xp), y3 = ldA<R, PDL>(A, nh, oe, 2, xp);
       const R beta_a = (R)ch.beta_a;
       bool changed = false;
 #pragma unroll 1
@@ -499,14 +378,13 @@ __device__ __forceinline__ void link_tile(const PassArgs& p, int tile) {
   }
   // partials {KP accepted, Metropolis accepted, sum plaquette} / {OR accepted}
   if (p.part) {
-    if constexpr (!OR) block_reduce_cs<2, 1, kNQ>(cnt, pl, p.part + (size_t)tp.tile * kNQ);
+    if constexpr (!OR) block_reduce_cs<2, 1, kNQ>(cnt, pl, p.part + (size_t)tile * kNQ);
     else {
       unsigned c1[1] = {cnt[0]};
       double d0[1] = {0.0};
-      block_reduce_cs<1, 0, kNQ>(c1, d0, p.part + (size_t)tp.tile * kNQ);
+      block_reduce_cs<1, 0, kNQ>(c1, d0, p.part + (size_t)tile * kNQ);
     }
   }
-  if (LD == kLdPlain) plane_signal(p, ch, tp.z);
 }
 
 // Tile shape: BS threads per block, SPT sites per thread (1, or 2 for the
@@ -518,22 +396,20 @@ constexpr int min_blocks_bs() {
   return OCC ? OCC / BS : (min_blocks<R>() * kBlock / BS > 0 ? min_blocks<R>() * kBlock / BS : 1);
 }
 
-// LD: kLdNc (the pass starts when the previous one has completed) or
-// kLdPlain (plane-synchronised queue)
-template <typename R, int MODE, int SPT, int BS, int OCC = 0, int LD = kLdNc>
+template <typename R, int MODE, int SPT, int BS, int OCC = 0>
 __global__ void __launch_bounds__(BS, min_blocks_bs<R, BS, OCC>()) higgs_kernel(PassArgs p) {
-  higgs_tile<R, MODE, LD, SPT, BS>(p, blockIdx.x);
+  higgs_tile<R, MODE, true, SPT, BS>(p, blockIdx.x);
 }
 
-template <typename R, int MU, int OR, int SPT, int BS, int OCC = 0, int LD = kLdNc>
+template <typename R, int MU, int OR, int SPT, int BS, int OCC = 0>
 __global__ void __launch_bounds__(BS, min_blocks_bs<R, BS, OCC>()) link_kernel(PassArgs p) {
-  link_tile<R, MU, OR, LD, 1, SPT, BS>(p, blockIdx.x);
+  link_tile<R, MU, OR, true, 1, SPT, BS>(p, blockIdx.x);
 }
 
 // f/agauge1.f (3 hits)
-template <typename R, int MU, int SPT, int BS, int OCC = 0, int LD = kLdNc>
+template <typename R, int MU, int SPT, int BS, int OCC = 0>
 __global__ void __launch_bounds__(BS, min_blocks_bs<R, BS, OCC>()) link3_kernel(PassArgs p) {
-  link_tile<R, MU, 0, LD, 3, SPT, BS>(p, blockIdx.x);
+  link_tile<R, MU, 0, true, 3, SPT, BS>(p, blockIdx.x);
 }
 
 // ------------------------------------------------------------------ finalize
@@ -667,9 +543,6 @@ constexpr int kFinWarps = 32;
 __global__ void __launch_bounds__(kFinWarps * 32) finalize_kernel(FinalizeArgs f) {
   pdl_trigger();
   pdl_wait();
-  // every pass of the queue has completed: reset the plane counters
-  if (f.plane_cnt && blockIdx.x == 0)
-    for (int i = threadIdx.x; i < f.nplanes; i += blockDim.x) f.plane_cnt[i] = 0u;
   const int nitems = f.nchains * f.nslots;
   for (int w = blockIdx.x * kFinWarps + (threadIdx.x >> 5); w < nitems; w += gridDim.x * kFinWarps)
     finalize_sum_warp(f, w);
@@ -702,6 +575,14 @@ __global__ void __launch_bounds__(kFinWarps * 32) finalize_kernel(FinalizeArgs f
 // with acquire loads and a bounded number of short sleeps.  On timeout the
 // block records the status bit and the kernel returns instead of spinning on.
 __device__ __forceinline__ void fence_acq_rel_gpu() { asm volatile("fence.acq_rel.gpu;" ::: "memory"); }
+__device__ __forceinline__ void red_release_add(unsigned* p, unsigned v) {
+  asm volatile("red.release.gpu.global.add.u32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
+}
+__device__ __forceinline__ unsigned ld_acquire(const unsigned* p) {
+  unsigned v;
+  asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+  return v;
+}
 
 __device__ __forceinline__ bool grid_sync(GridBar* bar, unsigned nblocks, unsigned& target, unsigned* status) {
   __shared__ int s_ok;
@@ -732,28 +613,28 @@ __device__ __forceinline__ void persistent_pass(const PersistArgs& a, const Pass
   const int nt = a.ntiles;
   switch (e.kind) {
     case kHiggsHB:
-      for (int t = blockIdx.x; t < nt; t += gridDim.x) higgs_tile<R, 0, kLdCg>(p, t);
+      for (int t = blockIdx.x; t < nt; t += gridDim.x) higgs_tile<R, 0, false>(p, t);
       break;
     case kHiggsOR:
-      for (int t = blockIdx.x; t < nt; t += gridDim.x) higgs_tile<R, 1, kLdCg>(p, t);
+      for (int t = blockIdx.x; t < nt; t += gridDim.x) higgs_tile<R, 1, false>(p, t);
       break;
     case kHiggsMetro:
-      for (int t = blockIdx.x; t < nt; t += gridDim.x) higgs_tile<R, 2, kLdCg>(p, t);
+      for (int t = blockIdx.x; t < nt; t += gridDim.x) higgs_tile<R, 2, false>(p, t);
       break;
     case kLinkHB:
-      if (e.mu == 0) for (int t = blockIdx.x; t < nt; t += gridDim.x) link_tile<R, 0, 0, kLdCg>(p, t);
-      else if (e.mu == 1) for (int t = blockIdx.x; t < nt; t += gridDim.x) link_tile<R, 1, 0, kLdCg>(p, t);
-      else for (int t = blockIdx.x; t < nt; t += gridDim.x) link_tile<R, 2, 0, kLdCg>(p, t);
+      if (e.mu == 0) for (int t = blockIdx.x; t < nt; t += gridDim.x) link_tile<R, 0, 0, false>(p, t);
+      else if (e.mu == 1) for (int t = blockIdx.x; t < nt; t += gridDim.x) link_tile<R, 1, 0, false>(p, t);
+      else for (int t = blockIdx.x; t < nt; t += gridDim.x) link_tile<R, 2, 0, false>(p, t);
       break;
     case kLinkHB3:
-      if (e.mu == 0) for (int t = blockIdx.x; t < nt; t += gridDim.x) link_tile<R, 0, 0, kLdCg, 3>(p, t);
-      else if (e.mu == 1) for (int t = blockIdx.x; t < nt; t += gridDim.x) link_tile<R, 1, 0, kLdCg, 3>(p, t);
-      else for (int t = blockIdx.x; t < nt; t += gridDim.x) link_tile<R, 2, 0, kLdCg, 3>(p, t);
+      if (e.mu == 0) for (int t = blockIdx.x; t < nt; t += gridDim.x) link_tile<R, 0, 0, false, 3>(p, t);
+      else if (e.mu == 1) for (int t = blockIdx.x; t < nt; t += gridDim.x) link_tile<R, 1, 0, false, 3>(p, t);
+      else for (int t = blockIdx.x; t < nt; t += gridDim.x) link_tile<R, 2, 0, false, 3>(p, t);
       break;
     default:
-      if (e.mu == 0) for (int t = blockIdx.x; t < nt; t += gridDim.x) link_tile<R, 0, 1, kLdCg>(p, t);
-      else if (e.mu == 1) for (int t = blockIdx.x; t < nt; t += gridDim.x) link_tile<R, 1, 1, kLdCg>(p, t);
-      else for (int t = blockIdx.x; t < nt; t += gridDim.x) link_tile<R, 2, 1, kLdCg>(p, t);
+      if (e.mu == 0) for (int t = blockIdx.x; t < nt; t += gridDim.x) link_tile<R, 0, 1, false>(p, t);
+      else if (e.mu == 1) for (int t = blockIdx.x; t < nt; t += gridDim.x) link_tile<R, 1, 1, false>(p, t);
+      else for (int t = blockIdx.x; t < nt; t += gridDim.x) link_tile<R, 2, 1, false>(p, t);
       break;
   }
 }
@@ -826,32 +707,26 @@ __global__ void debug_force_kernel(const ChainDev* chp, int eo, double* out) {
 // ------------------------------------------------------------------ launchers
 // The pass kernels and the finalize kernel are launched with programmatic
 // dependent launch (lce_common.cuh: launch_pdl / pdl_wait).
-template <typename R, int SPT, int BS, int OCC = 0, int LD = kLdNc>
+template <typename R, int SPT, int BS, int OCC = 0>
 void launch_higgs_t(int mode, const PassArgs& a, int nblocks, cudaStream_t s) {
-  void (*k)(PassArgs) = mode == 0 ? higgs_kernel<R, 0, SPT, BS, OCC, LD>
-                                  : (mode == 1 ? higgs_kernel<R, 1, SPT, BS, OCC, LD> : higgs_kernel<R, 2, SPT, BS, OCC, LD>);
+  void (*k)(PassArgs) = mode == 0 ? higgs_kernel<R, 0, SPT, BS, OCC>
+                                  : (mode == 1 ? higgs_kernel<R, 1, SPT, BS, OCC> : higgs_kernel<R, 2, SPT, BS, OCC>);
   (void)launch_pdl(k, nblocks, BS, 0, s, a);
 }
 
-template <typename R, int SPT, int BS, int OCC = 0, int LD = kLdNc>
+template <typename R, int SPT, int BS, int OCC = 0>
 void launch_link_t(int mode, int mu, const PassArgs& a, int nblocks, cudaStream_t s) {
   void (*k)(PassArgs);
   if (mode == 0)
-    k = mu == 0 ? link_kernel<R, 0, 0, SPT, BS, OCC, LD>
-                : (mu == 1 ? link_kernel<R, 1, 0, SPT, BS, OCC, LD> : link_kernel<R, 2, 0, SPT, BS, OCC, LD>);
+    k = mu == 0 ? link_kernel<R, 0, 0, SPT, BS, OCC>
+                : (mu == 1 ? link_kernel<R, 1, 0, SPT, BS, OCC> : link_kernel<R, 2, 0, SPT, BS, OCC>);
   else if (mode == 1)
-    k = mu == 0 ? link_kernel<R, 0, 1, SPT, BS, OCC, LD>
-                : (mu == 1 ? link_kernel<R, 1, 1, SPT, BS, OCC, LD> : link_kernel<R, 2, 1, SPT, BS, OCC, LD>);
+    k = mu == 0 ? link_kernel<R, 0, 1, SPT, BS, OCC>
+                : (mu == 1 ? link_kernel<R, 1, 1, SPT, BS, OCC> : link_kernel<R, 2, 1, SPT, BS, OCC>);
   else
-    k = mu == 0 ? link3_kernel<R, 0, SPT, BS, OCC, LD>
-                : (mu == 1 ? link3_kernel<R, 1, SPT, BS, OCC, LD> : link3_kernel<R, 2, SPT, BS, OCC, LD>);
+    k = mu == 0 ? link3_kernel<R, 0, SPT, BS, OCC>
+                : (mu == 1 ? link3_kernel<R, 1, SPT, BS, OCC> : link3_kernel<R, 2, SPT, BS, OCC>);
   (void)launch_pdl(k, nblocks, BS, 0, s, a);
-}
-
-// Plane-synchronised queues (a.plane_cnt set): FP32, tile shapes (128, 1),
-// (256, 1), (512, 1) and (256, 2) at the 64-register cap.
-bool plane_sync_shape(int bs, int spt, int occ) {
-  return occ == 0 && ((spt == 1 && (bs == 128 || bs == 256 || bs == 512)) || (spt == 2 && bs == 256));
 }
 
 // Tile shapes compiled: FP32 (BS, SPT) in {128, 256, 512} x {1} and
@@ -860,13 +735,6 @@ bool plane_sync_shape(int bs, int spt, int occ) {
 template <typename R>
 void launch_higgs(int mode, const PassArgs& a, int nblocks, cudaStream_t s) {
   if constexpr (sizeof(R) == 4) {
-    if (a.plane_cnt) {
-      if (a.spt == 2) launch_higgs_t<R, 2, 256, 0, kLdPlain>(mode, a, nblocks, s);
-      else if (a.bs == 128) launch_higgs_t<R, 1, 128, 0, kLdPlain>(mode, a, nblocks, s);
-      else if (a.bs == 512) launch_higgs_t<R, 1, 512, 0, kLdPlain>(mode, a, nblocks, s);
-      else launch_higgs_t<R, 1, 256, 0, kLdPlain>(mode, a, nblocks, s);
-      return;
-    }
     if (a.bs == 128 && a.occ == 1152) {
       launch_higgs_t<R, 1, 128, 1152>(mode, a, nblocks, s);
       return;
@@ -888,13 +756,6 @@ void launch_higgs(int mode, const PassArgs& a, int nblocks, cudaStream_t s) {
 template <typename R>
 void launch_link(int mode, int mu, const PassArgs& a, int nblocks, cudaStream_t s) {
   if constexpr (sizeof(R) == 4) {
-    if (a.plane_cnt) {
-      if (a.spt == 2) launch_link_t<R, 2, 256, 0, kLdPlain>(mode, mu, a, nblocks, s);
-      else if (a.bs == 128) launch_link_t<R, 1, 128, 0, kLdPlain>(mode, mu, a, nblocks, s);
-      else if (a.bs == 512) launch_link_t<R, 1, 512, 0, kLdPlain>(mode, mu, a, nblocks, s);
-      else launch_link_t<R, 1, 256, 0, kLdPlain>(mode, mu, a, nblocks, s);
-      return;
-    }
     if (a.bs == 128 && a.occ == 1152) {
       launch_link_t<R, 1, 128, 1152>(mode, mu, a, nblocks, s);
       return;

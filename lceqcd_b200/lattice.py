@@ -249,18 +249,6 @@ class _Context:
         self._ck(self.lib.lce_get_tile_shape(self.h, C.byref(bs), C.byref(spt), C.byref(reg)))
         return (bs.value, spt.value, reg.value) if registers else (bs.value, spt.value)
 
-    def set_plane_sync(self, on: bool):
-        """Chain the per-pass kernels by per-plane completion counters (True)
-        or by whole-pass completion (False); same results bit for bit."""
-        self._ck(self.lib.lce_set_plane_sync(self.h, 1 if on else 0))
-
-    def plane_sync(self):
-        """(switched on, used by the sweeps of the tile shape in use,
-        tiles that fell back to the whole-pass wait so far)."""
-        act, fb = C.c_int(), C.c_uint()
-        on = self._ck(self.lib.lce_get_plane_sync(self.h, C.byref(act), C.byref(fb)))
-        return bool(on), bool(act.value), fb.value
-
     def sweep_mode(self) -> str:
         m = self._ck(self.lib.lce_get_sweep_mode(self.h))
         return {v: k for k, v in SWEEP_MODES.items()}[m]
