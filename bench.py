@@ -561,11 +561,14 @@ def run_gpu(args):
         if rank == 0:
             passes = 4 + 6 * (1 + args.link_or)
             sweep_bytes = B_HIGGS * 4 + B_LINK * 6 * (1 + args.link_or)
-            print(json.dumps({"metric": METRIC, "value": value, "unit": UNIT, "L": list(L), "steps": args.steps,
-                              "ms_per_step": ms_max / args.steps, "sweep_mode": mode, "quick": True,
-                              "tile_shape": [tile_bs, tile_spt, tile_regs],
-                              "link_or": args.link_or, "passes": passes, "bytes_per_site": sweep_bytes,
-                              "frac_of_measured_hbm": value * sweep_bytes / 1e9 / peak}), flush=True)
+            line = {"metric": METRIC, "value": value, "unit": UNIT, "L": list(L), "steps": args.steps,
+                    "ms_per_step": ms_max / args.steps, "sweep_mode": mode, "quick": True,
+                    "tile_shape": [tile_bs, tile_spt, tile_regs],
+                    "link_or": args.link_or, "passes": passes, "bytes_per_site": sweep_bytes,
+                    "frac_of_measured_hbm": value * sweep_bytes / 1e9 / peak}
+            if args.pass_profile and mode != "persistent":
+                line["per_pass_us"] = [round(1e3 * x, 2) for x in kernel_profile(lat, reps=args.pass_profile)]
+            print(json.dumps(line), flush=True)
         lat.close()
         return
 
@@ -776,6 +779,9 @@ def main():
     ap.add_argument("--tile-threads", type=int, default=0, choices=[0, 128, 256, 512],
                     help="threads per block of the update kernels (default 0: the autotuner chooses with "
                          "--sweep-mode auto, else 256)")
+    ap.add_argument("--pass-profile", type=int, default=0, metavar="REPS",
+                    help="--quick runs: also print the per-pass durations inside the sweep graph (the last: "
+                         "the finalize kernel), averaged over REPS L2-flushed sweeps")
     ap.add_argument("--link-or", type=int, default=0, metavar="N",
                     help="--quick runs: N link overrelaxation hits per sweep after the heatbath")
     ap.add_argument("--quick-gauge-fix", type=int, default=0, metavar="ITERS",

@@ -65,6 +65,11 @@ struct lce_ctx {
   ChainDev* ch_d = nullptr;
   int* tiles_d[3] = {nullptr, nullptr, nullptr};
   int* blk_d = nullptr;   // = tiles_d[1]
+  // finalize reduction: per tile table, the prefix over chains of chunks of
+  // kChunkTiles tiles, and the chunk sums [chunk][kMaxSlots][kNQ]
+  std::vector<int> chunks[3];
+  int* chunks_begin_d[3] = {nullptr, nullptr, nullptr};
+  double* chunks_d = nullptr;
   CtxState* st_d = nullptr;
   ChainState* cst_d = nullptr;
   lce_meas* meas_d = nullptr;
@@ -290,6 +295,9 @@ void enq_begin(lce_ctx* c, const std::vector<unsigned char>& routines, int measf
   f.totals = c->totals_d;
   f.nchains = c->nchains;
   f.single = c->prec == LCE_PREC_F32;
+  f.chunk_begin = c->chunks_begin_d[ti];
+  f.chunks = c->chunks_d;
+  f.nchunks = c->chunks[ti].back();
   q.soff = 0;
   q.poff = 0;
   q.slot = 0;
@@ -406,6 +414,9 @@ int enqueue_persistent(lce_ctx* c, const std::vector<unsigned char>& routines, i
   f.totals = c->totals_d;
   f.nchains = c->nchains;
   f.single = c->prec == LCE_PREC_F32;
+  f.chunk_begin = c->chunks_begin_d[1];
+  f.chunks = c->chunks_d;
+  f.nchunks = c->chunks[1].back();
   unsigned long long soff = 0;
   unsigned int poff = 0;
   int slot = 0;
@@ -718,6 +729,19 @@ lce_ctx* create_impl(const lce_params* p, int n, const SlabInfo* slab = nullptr)
     if ((e = cudaMemcpy(c->tiles_d[t], c->tiles[t].data(), sizeof(int) * (n + 1), cudaMemcpyHostToDevice)) !=
         cudaSuccess)
       return bail(e, "cudaMemcpy(tiles)");
+    c->chunks[t].assign(1, 0);
+    for (int i = 0; i < n; ++i)
+      c->chunks[t].push_back(c->chunks[t].back() + ceil_div(c->tiles[t][i + 1] - c->tiles[t][i], kChunkTiles));
+    if ((e = cudaMalloc(&c->chunks_begin_d[t], sizeof(int) * (n + 1))) != cudaSuccess)
+      return bail(e, "cudaMalloc(chunk table)");
+    if ((e = cudaMemcpy(c->chunks_begin_d[t], c->chunks[t].data(), sizeof(int) * (n + 1), cudaMemcpyHostToDevice)) !=
+        cudaSuccess)
+      return bail(e, "cudaMemcpy(chunk table)");
+  }
+  {
+    // 128-site tiles (table 0) make the most chunks
+    const size_t nd = (size_t)c->chunks[0].back() * kMaxSlots * kNQ;
+    if ((e = cudaMalloc(&c->chunks_d, sizeof(double) * nd)) != cudaSuccess) return bail(e, "cudaMalloc(chunk sums)");
   }
   c->blk_d = c->tiles_d[1];
   if ((e = cudaMalloc(&c->st_d, sizeof(CtxState))) != cudaSuccess) return bail(e, "cudaMalloc(state)");
@@ -1418,7 +1442,8 @@ void lce_destroy(lce_ctx* c) {
   for (auto& kv : c->fa_exec) cudaGraphExecDestroy(kv.second);
   void* ptrs[] = {c->ch_d, c->tiles_d[0], c->tiles_d[1], c->tiles_d[2], c->st_d, c->cst_d, c->meas_d, c->part_d, c->totals_d,
                   c->scratch_d, c->fields_d, c->stream_d, c->staging_d, c->flush_d, c->bar_d,
-                  c->gsave_d, c->fa_d};
+                  c->gsave_d, c->fa_d, c->chunks_begin_d[0], c->chunks_begin_d[1], c->chunks_begin_d[2],
+                  c->chunks_d};
   for (void* q : ptrs)
     if (q) cudaFree(q);
   if (c->ev0) cudaEventDestroy(c->ev0);

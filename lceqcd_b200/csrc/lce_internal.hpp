@@ -29,6 +29,7 @@ template <typename R>
 constexpr int min_blocks() { return sizeof(R) == 4 ? 4 : 3; }
 constexpr int kNQ = 4;           // doubles of partial sums per block
 constexpr int kMaxSlots = 64;    // reduction slots per finalize
+constexpr int kChunkTiles = 128; // tiles per level-1 chunk of the finalize reduction
 
 // pass kinds (one kernel launch over one parity)
 enum PassKind : unsigned char {
@@ -147,6 +148,11 @@ struct FinalizeArgs {
   unsigned int npasses;           // advance of st->pass_ctr
   unsigned long long nstream;     // advance of st->stream_pos
   int single;                     // FP32 arithmetic for the ahiggs1 step update
+  // two-level reduction of the tile partials (lce_update.cu): chunks of 128
+  // tiles; chunk_begin = nchains + 1 prefix of chunks per chain
+  const int* chunk_begin;
+  double* chunks;                 // [chunk][kMaxSlots][kNQ]
+  int nchunks;
   unsigned char kinds[kMaxSlots];
 };
 

@@ -413,27 +413,79 @@ __global__ void __launch_bounds__(BS, min_blocks_bs<R, BS, OCC>()) link3_kernel(
 }
 
 // ------------------------------------------------------------------ finalize
-// Work item w = (chain c, slot i), one warp: sum the tile partials of chain c
-// in slot i into totals[c][i].  Lane l adds the tiles l, l + 32, ... in
-// order and the lanes are combined by a fixed shuffle tree, so the order of
-// the sum does not depend on which warp or block takes the item (the
-// per-pass and persistent forms give the same bits).
-__device__ __forceinline__ void finalize_sum_warp(const FinalizeArgs& f, int w) {
-  const int lane = threadIdx.x & 31;
-  const int c = w / f.nslots, i = w % f.nslots;
-  const int b0 = f.blk_begin[c], b1 = f.blk_begin[c + 1];
-  const double* part = f.part + (size_t)i * f.slot_stride;
-  double v[kNQ] = {0.0, 0.0, 0.0, 0.0};
-  for (int b = b0 + lane; b < b1; b += 32) {
-#pragma unroll
-    for (int q = 0; q < kNQ; ++q) v[q] += __ldcg(part + (size_t)b * kNQ + q);
-  }
+// The partial sums of a reduction slot (kNQ doubles per tile) are added in two
+// fixed levels, so the order of every FP64 addition depends only on the tile
+// table, never on which warp or block does the work (the per-pass and the
+// persistent forms give the same bits):
+//   level 1  chunk k of chain c = the chain's tiles [k*128, (k+1)*128); lane l
+//            adds the tiles l, l+32, l+64, l+96 of the chunk in order and the
+//            lanes are combined by a fixed shuffle tree;
+//   level 2  a chain of several chunks: lane l adds the chunk sums l, l+32,
+//            ... in order, same tree.  A one-chunk chain's level-1 sum is its
+//            total.
+// One (chunk, slot) or (chain, slot) item per warp; the loads of four tiles
+// (or chunk sums) are issued together before their in-order adds.
+__device__ __forceinline__ void warp_tree(double (&v)[kNQ]) {
 #pragma unroll
   for (int q = 0; q < kNQ; ++q) {
 #pragma unroll
     for (int o = 16; o > 0; o >>= 1) v[q] += __shfl_down_sync(0xffffffffu, v[q], o);
   }
-  if (lane == 0) {
+}
+
+// in-order sum over the strided elements e = e0 + lane, e0 + lane + 32, ...
+// (e < e1) of an array of kNQ-double records with record stride `stride`
+// (in double2), reading through L2
+__device__ __forceinline__ void strided_sum(const double2* base, size_t stride, int e0, int e1, double (&v)[kNQ]) {
+  static_assert(kNQ == 4, "a record is two double2");
+  const int lane = threadIdx.x & 31;
+  v[0] = v[1] = v[2] = v[3] = 0.0;
+  constexpr int kBatch = 4;
+  for (int b = e0 + lane; b < e1; b += 32 * kBatch) {
+    double2 x[kBatch][2];
+#pragma unroll
+    for (int j = 0; j < kBatch; ++j) {
+      const int e = b + 32 * j;
+      x[j][0] = e < e1 ? __ldcg(base + (size_t)e * stride) : make_double2(0.0, 0.0);
+      x[j][1] = e < e1 ? __ldcg(base + (size_t)e * stride + 1) : make_double2(0.0, 0.0);
+    }
+#pragma unroll
+    for (int j = 0; j < kBatch; ++j) {
+      if (b + 32 * j < e1) {
+        v[0] += x[j][0].x;
+        v[1] += x[j][0].y;
+        v[2] += x[j][1].x;
+        v[3] += x[j][1].y;
+      }
+    }
+  }
+  warp_tree(v);
+}
+
+// level 1, item w = (chunk g over all chains, slot i)
+__device__ __forceinline__ void finalize_chunk_warp(const FinalizeArgs& f, int w) {
+  const int g = w / f.nslots, i = w % f.nslots;
+  const int c = f.nchains > 1 ? find_chain(f.chunk_begin, f.nchains, g) : 0;
+  const int t0 = __ldg(f.blk_begin + c) + (g - __ldg(f.chunk_begin + c)) * kChunkTiles;
+  const int t1 = min(__ldg(f.blk_begin + c + 1), t0 + kChunkTiles);
+  double v[kNQ];
+  strided_sum(reinterpret_cast<const double2*>(f.part + (size_t)i * f.slot_stride), 2, t0, t1, v);
+  if ((threadIdx.x & 31) == 0) {
+    const bool one = __ldg(f.chunk_begin + c + 1) - __ldg(f.chunk_begin + c) == 1;
+    double* dst = one ? f.totals + ((size_t)c * kMaxSlots + i) * kNQ : f.chunks + ((size_t)g * kMaxSlots + i) * kNQ;
+#pragma unroll
+    for (int q = 0; q < kNQ; ++q) dst[q] = v[q];
+  }
+}
+
+// level 2, item w = (chain c, slot i); nothing to do for a one-chunk chain
+__device__ __forceinline__ void finalize_chain_warp(const FinalizeArgs& f, int w) {
+  const int c = w / f.nslots, i = w % f.nslots;
+  const int g0 = __ldg(f.chunk_begin + c), g1 = __ldg(f.chunk_begin + c + 1);
+  if (g1 - g0 <= 1) return;
+  double v[kNQ];
+  strided_sum(reinterpret_cast<const double2*>(f.chunks + (size_t)i * kNQ), kMaxSlots * kNQ / 2, g0, g1, v);
+  if ((threadIdx.x & 31) == 0) {
 #pragma unroll
     for (int q = 0; q < kNQ; ++q) f.totals[((size_t)c * kMaxSlots + i) * kNQ + q] = v[q];
   }
@@ -535,34 +587,37 @@ __device__ __forceinline__ void finalize_combine(const FinalizeArgs& f) {
   }
 }
 
-// kFinWarps warps per block, one (chain, slot) item per warp.  One block (a
-// single chain's slots): sum, then combine in the same block -- its own
-// global writes are visible to it after the barrier.  Several blocks (a
-// batch): the last block to finish, by an atomic ticket, combines.
+// kFinWarps warps per block, one level-1 item per warp.  One block: level 2
+// and the combine follow in the same block (its own global writes are
+// visible to it after the barrier).  Several blocks: the last block to finish
+// level 1, by an atomic ticket, does level 2 and the combine.
 constexpr int kFinWarps = 32;
 __global__ void __launch_bounds__(kFinWarps * 32) finalize_kernel(FinalizeArgs f) {
   pdl_trigger();
   pdl_wait();
-  const int nitems = f.nchains * f.nslots;
-  for (int w = blockIdx.x * kFinWarps + (threadIdx.x >> 5); w < nitems; w += gridDim.x * kFinWarps)
-    finalize_sum_warp(f, w);
-  if (gridDim.x == 1) {
+  const int warp = (int)(threadIdx.x >> 5);
+  const int n1 = f.nchunks * f.nslots;
+  for (int w = blockIdx.x * kFinWarps + warp; w < n1; w += gridDim.x * kFinWarps) finalize_chunk_warp(f, w);
+  if (gridDim.x > 1) {
+    __shared__ bool last;
+    __threadfence();
     __syncthreads();
-    finalize_combine(f);
-    return;
+    if (threadIdx.x == 0) {
+      unsigned int t = atomicAdd(&f.st->ticket, 1u);
+      last = (t == gridDim.x - 1);
+    }
+    __syncthreads();
+    if (!last) return;
+    __threadfence();
+  } else {
+    __syncthreads();
   }
-  __shared__ bool last;
-  __threadfence();
-  __syncthreads();
-  if (threadIdx.x == 0) {
-    unsigned int t = atomicAdd(&f.st->ticket, 1u);
-    last = (t == gridDim.x - 1);
+  if (f.nchunks > f.nchains) {
+    for (int w = warp; w < f.nchains * f.nslots; w += kFinWarps) finalize_chain_warp(f, w);
+    __syncthreads();
   }
-  __syncthreads();
-  if (!last) return;
-  __threadfence();
   finalize_combine(f);
-  if (threadIdx.x == 0) f.st->ticket = 0;
+  if (gridDim.x > 1 && threadIdx.x == 0) f.st->ticket = 0;
 }
 
 // ------------------------------------------------------------------ persistent sweep
@@ -657,9 +712,11 @@ __global__ void __launch_bounds__(kBlock, kPersistMinBlocks) sweep_persistent_ke
     if (!grid_sync(a.bar, gridDim.x, target, &a.base.st->status)) return;
   }
   {
-    const int nw = (int)(blockDim.x >> 5);
-    for (int w = blockIdx.x * nw + (int)(threadIdx.x >> 5); w < a.fin.nchains * a.fin.nslots; w += gridDim.x * nw)
-      finalize_sum_warp(a.fin, w);
+    const int nw = (int)(blockDim.x >> 5), w0 = blockIdx.x * nw + (int)(threadIdx.x >> 5);
+    for (int w = w0; w < a.fin.nchunks * a.fin.nslots; w += gridDim.x * nw) finalize_chunk_warp(a.fin, w);
+    if (!grid_sync(a.bar, gridDim.x, target, &a.base.st->status)) return;
+    if (a.fin.nchunks > a.fin.nchains)
+      for (int w = w0; w < a.fin.nchains * a.fin.nslots; w += gridDim.x * nw) finalize_chain_warp(a.fin, w);
   }
   if (!grid_sync(a.bar, gridDim.x, target, &a.base.st->status)) return;
   if (blockIdx.x == 0) {
@@ -775,7 +832,7 @@ void launch_link(int mode, int mu, const PassArgs& a, int nblocks, cudaStream_t 
 }
 
 void launch_finalize(const FinalizeArgs& f, cudaStream_t s) {
-  int grid = (f.nchains * f.nslots + kFinWarps - 1) / kFinWarps;
+  int grid = (f.nchunks * f.nslots + kFinWarps - 1) / kFinWarps;
   if (grid < 1) grid = 1;
   (void)launch_pdl(finalize_kernel, grid, kFinWarps * 32, 0, s, f);
 }
