@@ -166,6 +166,13 @@ int lce_synchronize(lce_ctx* ctx);
 /* ---- fields (COMMON /linkvar/ mirrors; f/confget.f / f/confsave.f boundary) ---- */
 int lce_upload(lce_ctx* ctx, int chain, int which, const float* u, const float* a, long ld);
 int lce_upload_f64(lce_ctx* ctx, int chain, int which, const double* u, const double* a, long ld);
+/* lce_upload without waiting (FP32 contexts): the host-to-device copy runs on
+ * a copy stream of the context and the update calls queued after it see the
+ * new fields.  The host buffers must stay unchanged until the next call that
+ * synchronises the context stream (lce_synchronize, lce_get_meas, lce_sweep
+ * with an lce_meas, lce_download); pinned buffers let the copy overlap the
+ * sweeps queued before it. */
+int lce_upload_async(lce_ctx* ctx, int chain, int which, const float* u, const float* a, long ld);
 int lce_download(lce_ctx* ctx, int chain, int which, float* u, float* a, long ld);
 int lce_download_f64(lce_ctx* ctx, int chain, int which, double* u, double* a, long ld);
 /* f/confget.f unitconf (:295-307): U = 1, A = (0, 0, a3) on every chain */

@@ -94,6 +94,7 @@ SIGNATURES = {
     "lce_set_stream": (I, [P, P]),
     "lce_synchronize": (I, [P]),
     "lce_upload": (I, [P, I, I, P, P, C.c_long]),
+    "lce_upload_async": (I, [P, I, I, P, P, C.c_long]),
     "lce_upload_f64": (I, [P, I, I, P, P, C.c_long]),
     "lce_download": (I, [P, I, I, P, P, C.c_long]),
     "lce_download_f64": (I, [P, I, I, P, P, C.c_long]),

@@ -84,6 +84,12 @@ struct lce_ctx {
   size_t stream_n = 0;
   void* staging_d = nullptr;
   size_t staging_bytes = 0;
+  // asynchronous upload (lce_upload_async): copy stream, its staging area
+  // (links then A of the largest chain) and the events that order the two
+  // streams around it
+  cudaStream_t copy = nullptr;
+  cudaEvent_t staged_ev = nullptr, free_ev = nullptr;
+  void* async_d = nullptr;
   void* flush_d = nullptr;
   size_t flush_bytes = 0;
   void* gsave_d = nullptr;  // G_prev during a warm-started gauge fixing
@@ -1456,7 +1462,7 @@ void lce_destroy(lce_ctx* c) {
   void* ptrs[] = {c->ch_d, c->tiles_d[0], c->tiles_d[1], c->tiles_d[2], c->st_d, c->cst_d, c->meas_d, c->part_d, c->totals_d,
                   c->scratch_d, c->fields_d, c->stream_d, c->staging_d, c->flush_d, c->bar_d,
                   c->gsave_d, c->fa_d, c->chunks_begin_d[0], c->chunks_begin_d[1], c->chunks_begin_d[2],
-                  c->chunks_d};
+                  c->chunks_d, c->async_d};
   for (void* q : ptrs)
     if (q) cudaFree(q);
   if (c->ev0) cudaEventDestroy(c->ev0);
@@ -1465,6 +1471,12 @@ void lce_destroy(lce_ctx* c) {
   if (c->fork_ev) cudaEventDestroy(c->fork_ev);
   if (c->join_ev) cudaEventDestroy(c->join_ev);
   if (c->side) cudaStreamDestroy(c->side);
+  if (c->copy) {
+    cudaStreamSynchronize(c->copy);
+    cudaStreamDestroy(c->copy);
+  }
+  if (c->staged_ev) cudaEventDestroy(c->staged_ev);
+  if (c->free_ev) cudaEventDestroy(c->free_ev);
   if (c->own) cudaStreamDestroy(c->own);
   delete c;
 }
@@ -1499,6 +1511,43 @@ int lce_upload(lce_ctx* c, int chain, int which, const float* u, const float* a,
   if (!c) return LCE_ERR_INVALID;
   return upload_t<float>(c, chain, which, u, a, ld);
 }
+// The host-to-device copies run on a copy stream into a staging area; the
+// context stream waits for them and copies the staging area into the fields
+// (links: one device copy; A: the layout kernel of lce_upload).  The copy
+// stream waits for the previous call's device copies before it overwrites the
+// staging area, so one upload can be in flight while the context stream runs
+// the sweeps of the previous one.
+int lce_upload_async(lce_ctx* c, int chain, int which, const float* u, const float* a, long ld) {
+  DeviceScope ds_(c ? c->device : -1);
+  if (!c) return LCE_ERR_INVALID;
+  if (c->prec != LCE_PREC_F32) return fail(c, LCE_ERR_UNSUPPORTED, "upload_async: FP32 contexts only (lce_upload)");
+  if (chain < 0 || chain >= c->nchains || (which != LCE_FIELDS && which != LCE_FIELDS_FIXED))
+    return fail(c, LCE_ERR_INVALID, "upload_async: bad chain or field selector");
+  const ChainDev& ch = c->ch[chain];
+  if (ld < ch.nh) return fail(c, LCE_ERR_INVALID, "upload_async: ld smaller than L1*L2*L3/2");
+  const size_t ulb = align256((size_t)6 * c->max_nh * 16);
+  if (!c->copy) {
+    CK(cudaStreamCreateWithFlags(&c->copy, cudaStreamNonBlocking));
+    CK(cudaEventCreateWithFlags(&c->staged_ev, cudaEventDisableTiming));
+    CK(cudaEventCreateWithFlags(&c->free_ev, cudaEventDisableTiming));
+    CK(cudaMalloc(&c->async_d, ulb + (size_t)6 * c->max_nh * sizeof(float)));
+    CK(cudaEventRecord(c->free_ev, c->stream));
+  }
+  const int nh = ch.nh;
+  char* su = static_cast<char*>(c->async_d);
+  char* sa = su + ulb;
+  CK(cudaStreamWaitEvent(c->copy, c->free_ev, 0));
+  if (u) CK(cudaMemcpy2DAsync(su, (size_t)nh * 16, u, (size_t)ld * 16, (size_t)nh * 16, 6, cudaMemcpyHostToDevice, c->copy));
+  if (a) CK(cudaMemcpy2DAsync(sa, (size_t)nh * 12, a, (size_t)ld * 12, (size_t)nh * 12, 2, cudaMemcpyHostToDevice, c->copy));
+  CK(cudaEventRecord(c->staged_ev, c->copy));
+  CK(cudaStreamWaitEvent(c->stream, c->staged_ev, 0));
+  if (u) CK(cudaMemcpyAsync(field_ptr(ch, which, true), su, (size_t)6 * nh * 16, cudaMemcpyDeviceToDevice, c->stream));
+  if (a) launch_higgs_in<float, float>(reinterpret_cast<const float*>(sa), field_ptr(ch, which, false), nh, c->stream);
+  CK(cudaGetLastError());
+  CK(cudaEventRecord(c->free_ev, c->stream));
+  return LCE_OK;
+}
+
 int lce_upload_f64(lce_ctx* c, int chain, int which, const double* u, const double* a, long ld) {
   DeviceScope ds_(c ? c->device : -1);
   if (!c) return LCE_ERR_INVALID;

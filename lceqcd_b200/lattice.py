@@ -124,11 +124,13 @@ class _Context:
             raise _lib.LceError(_lib.LCE_ERR_INVALID, "lce_create: " + self.lib.lce_last_error(None).decode())
         self.h = C.c_void_p(h)
         self.dtype = np.float64 if self.params[0].precision == "f64" else np.float32
+        self._inflight = []  # host arrays of lce_upload_async calls not yet known to be copied
 
     def close(self):
         if getattr(self, "h", None):
-            self.lib.lce_destroy(self.h)
+            self.lib.lce_destroy(self.h)  # synchronises the copy stream
             self.h = None
+            self._inflight = []
 
     def __del__(self):
         self.close()
@@ -151,6 +153,17 @@ class _Context:
         fn = self.lib.lce_upload_f64 if f64 else self.lib.lce_upload
         self._ck(fn(self.h, chain, which, None if uu is None else _ptr(uu), None if aa is None else _ptr(aa), nh))
 
+    def upload_async(self, u=None, a=None, which: int = 0, chain: int = 0):
+        """lce_upload_async: FP32 fields, returns before the copy ends.  The
+        arrays are kept referenced until the next synchronising call; pass
+        pinned arrays for a copy that overlaps the sweeps queued before it."""
+        nh = self.nh(chain)
+        uu = None if u is None else np.ascontiguousarray(u, np.float32).reshape(3, 2, nh, 4)
+        aa = None if a is None else np.ascontiguousarray(a, np.float32).reshape(2, nh, 3)
+        self._ck(self.lib.lce_upload_async(self.h, chain, which, None if uu is None else _ptr(uu),
+                                           None if aa is None else _ptr(aa), nh))
+        self._inflight.append((uu, aa))
+
     def download(self, which: int = 0, chain: int = 0, dtype=None):
         nh = self.nh(chain)
         dt = dtype or self.dtype
@@ -158,6 +171,7 @@ class _Context:
         a = np.zeros((2, nh, 3), dt)
         fn = self.lib.lce_download_f64 if dt == np.float64 else self.lib.lce_download
         self._ck(fn(self.h, chain, which, _ptr(u), _ptr(a), nh))
+        self._inflight = []
         return u, a
 
     def download_into(self, u: np.ndarray, a: np.ndarray, which: int = 0, chain: int = 0):
@@ -166,6 +180,7 @@ class _Context:
         assert u.dtype == a.dtype and u.size == 24 * nh and a.size == 6 * nh
         fn = self.lib.lce_download_f64 if u.dtype == np.float64 else self.lib.lce_download
         self._ck(fn(self.h, chain, which, _ptr(u), _ptr(a), nh))
+        self._inflight = []
 
     def extents(self, chain: int = 0):
         L = (C.c_int * 3)()
@@ -237,6 +252,7 @@ class _Context:
     def sweep(self, measflag: int = 1) -> dict:
         m = LceMeas()
         self._ck(self.lib.lce_sweep(self.h, measflag, C.byref(m)))
+        self._inflight = []
         return m.as_dict()
 
     def sweeps(self, n: int, measflag: int = 0):
@@ -256,6 +272,7 @@ class _Context:
     def meas1(self, chain: int = 0) -> dict:
         m = LceMeas()
         self._ck(self.lib.lce_get_meas(self.h, chain, C.byref(m)))
+        self._inflight = []
         return m.as_dict()
 
     def meas_batch(self) -> list:
@@ -265,6 +282,7 @@ class _Context:
 
     def synchronize(self):
         self._ck(self.lib.lce_synchronize(self.h))
+        self._inflight = []
 
     # ---- gauge fixing and measurements
     def landau_gauge(self, max_iters: int = 0, chain: int = 0):
