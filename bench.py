@@ -576,16 +576,13 @@ def run_gpu(args):
     # launch, one launch per step) when the autotuner chose it, else the link
     # pass kernel (68 B*V per launch, 6 of the 10 passes); per-pass kernel
     # durations come from events between the pass kernels of profiled sweeps
-    prof = kernel_profile(lat, reps=10)  # 10 passes, then the finalize kernel (none: fused)
-    # the last pass (link, eo 1, mu 3) also runs the finalize reduction in its
-    # last block: the link kernel's own duration is the mean of passes 4-8
-    link_ms = float(np.mean(prof[4:9]))
+    prof = kernel_profile(lat, reps=10)  # 10 passes, then the finalize kernel
+    link_ms = float(np.mean(prof[4:10]))
     # pass 0 also carries the graph's start and the cold L2 after the flush:
     # the Higgs kernel's own duration is the mean of passes 1-3
     higgs_ms = float(np.mean(prof[1:4]))
     first_ms = float(prof[0])
-    last_ms = float(prof[9])
-    fin_ms = last_ms - link_ms + float(prof[10])
+    fin_ms = float(prof[10])
     if mode == "persistent":
         dom_ms, dom_bytes = ms_max / args.steps, B_SWEEP * V
         dom_name = "sweep_persistent_kernel (whole sweep: 4 Higgs + 6 link passes, one cooperative launch)"
@@ -656,21 +653,17 @@ def run_gpu(args):
                      "pass_kernels": {"link_kernel_ms": link_ms, "link_kernel_frac": B_LINK * V / (link_ms / 1e3) / 1e9 / peak,
                                       "higgs_kernel_ms": higgs_ms,
                                       "higgs_kernel_frac": B_HIGGS * V / (higgs_ms / 1e3) / 1e9 / peak,
-                                      "finalize_ms": fin_ms,
+                                      "finalize_kernel_ms": fin_ms,
                                       "first_pass_ms": first_ms,
-                                      "last_pass_ms": last_ms,
                                       "per_pass_ms": [float(x) for x in prof],
-                                      "share_of_sweep": {"link_passes_4_8": 5 * link_ms / float(np.sum(prof)),
-                                                         "last_pass_with_finalize": (last_ms + float(prof[10]))
-                                                         / float(np.sum(prof)),
+                                      "share_of_sweep": {"link_passes": 6 * link_ms / float(np.sum(prof)),
                                                          "higgs_passes_1_3": 3 * higgs_ms / float(np.sum(prof)),
-                                                         "first_pass": first_ms / float(np.sum(prof))},
+                                                         "first_pass": first_ms / float(np.sum(prof)),
+                                                         "finalize": fin_ms / float(np.sum(prof))},
                                       "timing": "CUDA events hung off each pass of a sweep graph on a side stream "
                                                 "(the passes keep their programmatic overlap); a pass's time is "
                                                 "its completion minus the previous pass's (pass 0 from the graph "
-                                                "start, after an L2 flush).  The last pass runs the finalize "
-                                                "reduction in its last block (finalize_ms: its time beyond a link "
-                                                "pass's)"},
+                                                "start, after an L2 flush)"},
                      "sweep_frac": value / world * B_SWEEP / 1e9 / peak},
         "clocks": clocks,
     }

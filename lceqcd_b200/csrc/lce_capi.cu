@@ -272,7 +272,6 @@ struct Enq {
   unsigned long long soff = 0;
   unsigned int poff = 0;
   int slot = 0;
-  bool fused = false;  // the last pass ran the finalize reduction (single chain)
 };
 
 // index of the chain table for tiles of bs * spt sites (128, 256 or 512)
@@ -308,7 +307,6 @@ void enq_begin(lce_ctx* c, const std::vector<unsigned char>& routines, int measf
   q.soff = 0;
   q.poff = 0;
   q.slot = 0;
-  q.fused = false;
 }
 
 int enq_pass(lce_ctx* c, Enq& q, size_t i) {
@@ -340,22 +338,6 @@ int enq_pass(lce_ctx* c, Enq& q, size_t i) {
   // later passes follow pass kernels of this queue only
   a.rng_early = i > 0 ? 1 : 0;
   a.trigger_late = i == 0 ? 1 : 0;
-  if (reduce) {
-    q.f.kinds[q.slot] = (unsigned char)(ps.kind | (ps.end ? kKindEnd : 0));
-    ++q.slot;
-  }
-  if (c->nchains == 1) q.soff += (unsigned long long)nslots_of(ps.kind) * (c->stream_nh ? c->stream_nh : c->ch[0].nh);
-  q.poff += philox_passes(ps.kind);
-  // a single chain's last pass runs the finalize reduction in its last block
-  a.fin_fused = 0;
-  if (c->nchains == 1 && i + 1 == q.passes.size()) {
-    q.f.nslots = q.slot;
-    q.f.npasses = q.poff;
-    q.f.nstream = c->rng == LCE_RNG_STREAM ? q.soff : 0;
-    a.fin = q.f;
-    a.fin_fused = 1;
-    q.fused = true;
-  }
   if (ps.kind <= kHiggsMetro) {
     if (c->prec == LCE_PREC_F64) launch_higgs<double>(ps.kind, a, nblocks, c->stream);
     else launch_higgs<float>(ps.kind, a, nblocks, c->stream);
@@ -364,6 +346,12 @@ int enq_pass(lce_ctx* c, Enq& q, size_t i) {
     if (c->prec == LCE_PREC_F64) launch_link<double>(mode, ps.mu, a, nblocks, c->stream);
     else launch_link<float>(mode, ps.mu, a, nblocks, c->stream);
   }
+  if (reduce) {
+    q.f.kinds[q.slot] = (unsigned char)(ps.kind | (ps.end ? kKindEnd : 0));
+    ++q.slot;
+  }
+  if (c->nchains == 1) q.soff += (unsigned long long)nslots_of(ps.kind) * (c->stream_nh ? c->stream_nh : c->ch[0].nh);
+  q.poff += philox_passes(ps.kind);
   return LCE_OK;
 }
 
@@ -371,7 +359,7 @@ int enq_end(lce_ctx* c, Enq& q) {
   q.f.nslots = q.slot;
   q.f.npasses = q.poff;
   q.f.nstream = c->rng == LCE_RNG_STREAM ? q.soff : 0;
-  if (!q.fused) launch_finalize(q.f, c->stream);
+  launch_finalize(q.f, c->stream);
   CK(cudaGetLastError());
   return LCE_OK;
 }
@@ -421,7 +409,6 @@ int enqueue_persistent(lce_ctx* c, const std::vector<unsigned char>& routines, i
   b.stream_nh = c->stream_nh;
   b.rng_early = 0;
   b.trigger_late = 0;
-  b.fin_fused = 0;
   FinalizeArgs& f = a.fin;
   f.chains = c->ch_d;
   f.blk_begin = c->blk_d;

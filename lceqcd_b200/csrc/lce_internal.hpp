@@ -101,28 +101,6 @@ struct PlanEntry {
   unsigned char kind, eo, mu, slot;  // slot: reduction slot or kNoSlot
 };
 
-struct FinalizeArgs {
-  const ChainDev* chains;
-  const int* blk_begin;
-  CtxState* st;
-  ChainState* cst;
-  lce_meas* meas;         // [nchains]
-  const double* part;     // slot i at part + i * slot_stride
-  size_t slot_stride;
-  double* totals;         // [nchains][kMaxSlots][kNQ]
-  int nchains;
-  int nslots;
-  unsigned int npasses;           // advance of st->pass_ctr
-  unsigned long long nstream;     // advance of st->stream_pos
-  int single;                     // FP32 arithmetic for the ahiggs1 step update
-  // two-level reduction of the tile partials (lce_update.cu): chunks of 128
-  // tiles; chunk_begin = nchains + 1 prefix of chunks per chain
-  const int* chunk_begin;
-  double* chunks;                 // [chunk][kMaxSlots][kNQ]
-  int nchunks;
-  unsigned char kinds[kMaxSlots];
-};
-
 struct PassArgs {
   const ChainDev* chains;
   const int* blk_begin;   // nchains + 1 prefix of block counts
@@ -154,13 +132,29 @@ struct PassArgs {
   // kernel's wait (the first pass of a queue, so that no later pass can read
   // the counters while an earlier finalize still writes them).
   int rng_early, trigger_late;
-  // fin_fused: this is the last pass of a single-chain queue and its last
-  // block to finish (atomic ticket) runs the finalize reduction `fin`
-  // instead of a separate finalize kernel
-  int fin_fused;
-  FinalizeArgs fin;
 };
 
+struct FinalizeArgs {
+  const ChainDev* chains;
+  const int* blk_begin;
+  CtxState* st;
+  ChainState* cst;
+  lce_meas* meas;         // [nchains]
+  const double* part;     // slot i at part + i * slot_stride
+  size_t slot_stride;
+  double* totals;         // [nchains][kMaxSlots][kNQ]
+  int nchains;
+  int nslots;
+  unsigned int npasses;           // advance of st->pass_ctr
+  unsigned long long nstream;     // advance of st->stream_pos
+  int single;                     // FP32 arithmetic for the ahiggs1 step update
+  // two-level reduction of the tile partials (lce_update.cu): chunks of 128
+  // tiles; chunk_begin = nchains + 1 prefix of chunks per chain
+  const int* chunk_begin;
+  double* chunks;                 // [chunk][kMaxSlots][kNQ]
+  int nchunks;
+  unsigned char kinds[kMaxSlots];
+};
 
 struct PersistArgs {
   PassArgs base;          // per-pass fields (eo, part, offsets) are filled in the kernel

@@ -48,8 +48,6 @@ __device__ __forceinline__ int find_chain(const int* blk_begin, int n, int b) {
   return lo;
 }
 
-__device__ __noinline__ void fused_finalize(const PassArgs& p);
-
 // Field loads.  NC = true: the read-only (non-coherent) path, valid when no
 // earlier writer runs in the same kernel (the per-pass form).  NC = false:
 // L2 loads (ld.global.cg) for the persistent form, where fields written by
@@ -285,7 +283,6 @@ __device__ __forceinline__ void higgs_tile(const PassArgs& p, int tile) {
   }
   // partials {accepted, sum rho, sum rho^2, sum a.F}
   if (p.part) block_reduce_cs<1, 3, kNQ>(acc, q, p.part + (size_t)tile * kNQ);
-  if (PDL && p.fin_fused) fused_finalize(p);
 }
 
 // ------------------------------------------------------------------ links
@@ -388,7 +385,6 @@ __device__ __forceinline__ void link_tile(const PassArgs& p, int tile) {
       block_reduce_cs<1, 0, kNQ>(c1, d0, p.part + (size_t)tile * kNQ);
     }
   }
-  if (PDL && p.fin_fused) fused_finalize(p);
 }
 
 // Tile shape: BS threads per block, SPT sites per thread (1, or 2 for the
@@ -401,18 +397,18 @@ constexpr int min_blocks_bs() {
 }
 
 template <typename R, int MODE, int SPT, int BS, int OCC = 0>
-__global__ void __launch_bounds__(BS, min_blocks_bs<R, BS, OCC>()) higgs_kernel(const __grid_constant__ PassArgs p) {
+__global__ void __launch_bounds__(BS, min_blocks_bs<R, BS, OCC>()) higgs_kernel(PassArgs p) {
   higgs_tile<R, MODE, true, SPT, BS>(p, blockIdx.x);
 }
 
 template <typename R, int MU, int OR, int SPT, int BS, int OCC = 0>
-__global__ void __launch_bounds__(BS, min_blocks_bs<R, BS, OCC>()) link_kernel(const __grid_constant__ PassArgs p) {
+__global__ void __launch_bounds__(BS, min_blocks_bs<R, BS, OCC>()) link_kernel(PassArgs p) {
   link_tile<R, MU, OR, true, 1, SPT, BS>(p, blockIdx.x);
 }
 
 // f/agauge1.f (3 hits)
 template <typename R, int MU, int SPT, int BS, int OCC = 0>
-__global__ void __launch_bounds__(BS, min_blocks_bs<R, BS, OCC>()) link3_kernel(const __grid_constant__ PassArgs p) {
+__global__ void __launch_bounds__(BS, min_blocks_bs<R, BS, OCC>()) link3_kernel(PassArgs p) {
   link_tile<R, MU, 0, true, 3, SPT, BS>(p, blockIdx.x);
 }
 
@@ -624,33 +620,6 @@ __global__ void __launch_bounds__(kFinWarps * 32) finalize_kernel(FinalizeArgs f
   if (gridDim.x > 1 && threadIdx.x == 0) f.st->ticket = 0;
 }
 
-// The finalize reduction run by the last block of the last pass of a
-// single-chain queue (no finalize kernel, no kernel boundary after the last
-// pass).  Every block takes a ticket after its partials are written; the
-// block that takes the last one sees every block's writes (fence, ticket)
-// and every earlier pass's (they completed before this pass read its
-// fields), and runs levels 1 and 2 and the combine with its own warps, in
-// the same order as the finalize kernel.
-__device__ __noinline__ void fused_finalize(const PassArgs& p) {
-  const FinalizeArgs& f = p.fin;
-  __shared__ bool last;
-  __threadfence();
-  __syncthreads();
-  if (threadIdx.x == 0) last = atomicAdd(&f.st->ticket, 1u) == gridDim.x - 1;
-  __syncthreads();
-  if (!last) return;
-  __threadfence();
-  const int warp = (int)(threadIdx.x >> 5), nw = (int)(blockDim.x >> 5);
-  for (int w = warp; w < f.nchunks * f.nslots; w += nw) finalize_chunk_warp(f, w);
-  __syncthreads();
-  if (f.nchunks > f.nchains) {
-    for (int w = warp; w < f.nchains * f.nslots; w += nw) finalize_chain_warp(f, w);
-    __syncthreads();
-  }
-  finalize_combine(f);
-  if (threadIdx.x == 0) f.st->ticket = 0;
-}
-
 // ------------------------------------------------------------------ persistent sweep
 // Grid barrier for a cooperative launch (every block resident).  The arrival
 // counter only grows: barrier k of a launch waits for count >= base +
@@ -797,14 +766,14 @@ __global__ void debug_force_kernel(const ChainDev* chp, int eo, double* out) {
 // dependent launch (lce_common.cuh: launch_pdl / pdl_wait).
 template <typename R, int SPT, int BS, int OCC = 0>
 void launch_higgs_t(int mode, const PassArgs& a, int nblocks, cudaStream_t s) {
-  void (*k)(const PassArgs) = mode == 0 ? higgs_kernel<R, 0, SPT, BS, OCC>
+  void (*k)(PassArgs) = mode == 0 ? higgs_kernel<R, 0, SPT, BS, OCC>
                                   : (mode == 1 ? higgs_kernel<R, 1, SPT, BS, OCC> : higgs_kernel<R, 2, SPT, BS, OCC>);
   (void)launch_pdl(k, nblocks, BS, 0, s, a);
 }
 
 template <typename R, int SPT, int BS, int OCC = 0>
 void launch_link_t(int mode, int mu, const PassArgs& a, int nblocks, cudaStream_t s) {
-  void (*k)(const PassArgs);
+  void (*k)(PassArgs);
   if (mode == 0)
     k = mu == 0 ? link_kernel<R, 0, 0, SPT, BS, OCC>
                 : (mu == 1 ? link_kernel<R, 1, 0, SPT, BS, OCC> : link_kernel<R, 2, 0, SPT, BS, OCC>);
@@ -863,9 +832,7 @@ void launch_link(int mode, int mu, const PassArgs& a, int nblocks, cudaStream_t 
 }
 
 void launch_finalize(const FinalizeArgs& f, cudaStream_t s) {
-  // up to four level-1 items per warp before a second block (and the
-  // ticket) is worth it
-  int grid = (f.nchunks * f.nslots + 4 * kFinWarps - 1) / (4 * kFinWarps);
+  int grid = (f.nchunks * f.nslots + kFinWarps - 1) / kFinWarps;
   if (grid < 1) grid = 1;
   (void)launch_pdl(finalize_kernel, grid, kFinWarps * 32, 0, s, f);
 }
