@@ -624,9 +624,28 @@ def run_gpu(args):
         lat.sweep(1)
         lat.download_into(hu, ha)
         rt_ms += lat.timer_stop()
+    # Pipelined client: step k+1's input is uploaded (lce_upload_async, copy
+    # engine) while step k's sweep runs, then step k's measurements are read.
+    # Every step still copies its whole input from pinned host memory and
+    # reads its result back; one pair of CUDA events spans the Ke steps.
+    lat.upload_async(hu, ha)
+    lat.sweeps(1, 1)
+    lat.meas1()
+    barrier(world)
+    lat.synchronize()
+    lat.timer_start()
+    lat.upload_async(hu, ha)
+    for k in range(Ke):
+        lat.sweeps(1, 1)
+        if k + 1 < Ke:
+            lat.upload_async(hu, ha)
+        lat.meas1()
+    pipe_ms = lat.timer_stop()
     e2e_ms = max_over_ranks(e2e_ms, world)
     rt_ms = max_over_ranks(rt_ms, world)
-    e2e_val = world * V * Ke / (e2e_ms / 1e3)
+    pipe_ms = max_over_ranks(pipe_ms, world)
+    e2e_seq = world * V * Ke / (e2e_ms / 1e3)
+    e2e_val = world * V * Ke / (pipe_ms / 1e3)
     h2d = hu.nbytes + ha.nbytes
     d2h = 13 * 8  # lce_meas
 
@@ -639,7 +658,12 @@ def run_gpu(args):
         "parallelism": f"replicas x{world}" if world > 1 else "single GPU",
         "wall_s_timed_region": wall,
         "e2e": {"value": e2e_val, "unit": UNIT, "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
-                "note": "per step: lce_upload(pinned host fields) + lce_sweep(measflag=1, measurements read back)",
+                "note": "per step: lce_upload_async(pinned host fields), lce_sweeps(1, measflag=1), lce_get_meas "
+                        "(the step's measurements read back); step k+1's upload is queued before step k's "
+                        "result is read, so the copy engine overlaps the sweep; one event pair over all steps",
+                "sequential": {"value": e2e_seq,
+                               "note": "per step: lce_upload (returns when copied) + lce_sweep(measflag=1), "
+                                       "L2 flushed before each step outside its events"},
                 "with_field_download": {"value": world * V * Ke / (rt_ms / 1e3), "d2h_bytes_per_step": d2h + h2d}},
         "gpu_launches": launches,
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,

@@ -346,11 +346,13 @@ int lce_debug_force(lce_ctx* ctx, int eo, double* out);
 /* write a device buffer larger than L2 (126 MB) on the context stream */
 int lce_flush_l2(lce_ctx* ctx);
 /* one sweep (per-pass form, the tile shape in use) as a CUDA graph with a
- * timing event after every pass on a side stream, so the passes keep their
- * programmatic-dependent-launch overlap: ms[i] = completion of pass i minus
- * completion of pass i-1 (10 passes for the reference composition),
- * ms[npasses] = the finalize kernel's (when max_passes > npasses); returns
- * the pass count */
+ * timing event at its start and after every kernel, each on a side stream
+ * forked from the context stream, so the passes keep their
+ * programmatic-dependent-launch overlap and every difference carries the
+ * same fork latency: ms[i] = completion of pass i minus completion of pass
+ * i-1 (pass 0: minus the graph's start; 10 passes for the reference
+ * composition), ms[npasses] = the finalize kernel's (when max_passes >
+ * npasses); returns the pass count */
 int lce_profile_sweep(lce_ctx* ctx, int measflag, float* ms, int max_passes);
 /* events on the context stream */
 int lce_timer_start(lce_ctx* ctx);

@@ -2239,20 +2239,26 @@ int lce_profile_sweep(lce_ctx* c, int measflag, float* ms, int max_passes) {
   if (!*slot) {
     cudaGraph_t g;
     CK(cudaStreamBeginCapture(c->stream, cudaStreamCaptureModeThreadLocal));
-    cudaError_t e = cudaEventRecordWithFlags(c->prof_ev[0], c->stream, cudaEventRecordExternal);
+    // every timing event sits on the side stream, forked from the context
+    // stream at the start and after each kernel, so that the fork latency is
+    // the same in every difference
+    auto mark = [&](int k) {
+      cudaError_t x = cudaEventRecord(c->fork_ev, c->stream);
+      if (x == cudaSuccess) x = cudaStreamWaitEvent(c->side, c->fork_ev, 0);
+      if (x == cudaSuccess) x = cudaEventRecordWithFlags(c->prof_ev[k], c->side, cudaEventRecordExternal);
+      return x;
+    };
+    cudaError_t e = mark(0);
     Enq q;
     int rc = LCE_OK;
     if (e == cudaSuccess) {
       enq_begin(c, r, mf, true, c->tile_bs, c->tile_spt, c->tile_occ, q);
       for (int i = 0; i < np && rc == LCE_OK && e == cudaSuccess; ++i) {
         rc = enq_pass(c, q, i);
-        if (rc == LCE_OK) e = cudaEventRecord(c->fork_ev, c->stream);
-        if (e == cudaSuccess) e = cudaStreamWaitEvent(c->side, c->fork_ev, 0);
-        if (e == cudaSuccess) e = cudaEventRecordWithFlags(c->prof_ev[i + 1], c->side, cudaEventRecordExternal);
+        if (rc == LCE_OK) e = mark(i + 1);
       }
       if (rc == LCE_OK && e == cudaSuccess) rc = enq_end(c, q);
-      if (rc == LCE_OK && e == cudaSuccess)
-        e = cudaEventRecordWithFlags(c->prof_ev[np + 1], c->stream, cudaEventRecordExternal);
+      if (rc == LCE_OK && e == cudaSuccess) e = mark(np + 1);
     }
     // rejoin the side stream whatever happened, so that the capture can end
     const cudaError_t ej1 = cudaEventRecord(c->join_ev, c->side);

@@ -832,7 +832,9 @@ void launch_link(int mode, int mu, const PassArgs& a, int nblocks, cudaStream_t 
 }
 
 void launch_finalize(const FinalizeArgs& f, cudaStream_t s) {
-  int grid = (f.nchunks * f.nslots + kFinWarps - 1) / kFinWarps;
+  // up to four level-1 items per warp before a second block (and the
+  // ticket) is worth it
+  int grid = (f.nchunks * f.nslots + 4 * kFinWarps - 1) / (4 * kFinWarps);
   if (grid < 1) grid = 1;
   (void)launch_pdl(finalize_kernel, grid, kFinWarps * 32, 0, s, f);
 }
