@@ -624,22 +624,34 @@ def run_gpu(args):
         lat.sweep(1)
         lat.download_into(hu, ha)
         rt_ms += lat.timer_stop()
-    # Pipelined client: step k+1's input is uploaded (lce_upload_async, copy
-    # engine) while step k's sweep runs, then step k's measurements are read.
-    # Every step still copies its whole input from pinned host memory and
-    # reads its result back; one pair of CUDA events spans the Ke steps.
+    # Streaming client: the copy engine moves step k+2's input into a staging
+    # slot (lce_upload_stage) while step k sweeps and step k+1's staged input
+    # is applied behind it (lce_upload_apply), and step k's measurements are
+    # read after its sweep.  Every step still copies its whole input from
+    # pinned host memory and reads its result back; one pair of CUDA events
+    # spans the Ke steps.
+    hu2 = torch.empty(hu.shape, dtype=torch.float32, pin_memory=True).numpy()
+    ha2 = torch.empty(ha.shape, dtype=torch.float32, pin_memory=True).numpy()
+    hu2[...] = hu
+    ha2[...] = ha
+    bufs = [(hu, ha), (hu2, ha2)]  # the client refills one while the other is in flight
     lat.upload_async(hu, ha)
     lat.sweeps(1, 1)
     lat.meas1()
     barrier(world)
     lat.synchronize()
     lat.timer_start()
-    lat.upload_async(hu, ha)
+    lat.upload_stage(*bufs[0])
+    lat.upload_apply()
+    if Ke > 1:
+        lat.upload_stage(*bufs[1])
     for k in range(Ke):
         lat.sweeps(1, 1)
-        if k + 1 < Ke:
-            lat.upload_async(hu, ha)
         lat.meas1()
+        if k + 1 < Ke:
+            lat.upload_apply()
+        if k + 2 < Ke:
+            lat.upload_stage(*bufs[k % 2])
     pipe_ms = lat.timer_stop()
     e2e_ms = max_over_ranks(e2e_ms, world)
     rt_ms = max_over_ranks(rt_ms, world)
@@ -658,9 +670,9 @@ def run_gpu(args):
         "parallelism": f"replicas x{world}" if world > 1 else "single GPU",
         "wall_s_timed_region": wall,
         "e2e": {"value": e2e_val, "unit": UNIT, "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
-                "note": "per step: lce_upload_async(pinned host fields), lce_sweeps(1, measflag=1), lce_get_meas "
-                        "(the step's measurements read back); step k+1's upload is queued before step k's "
-                        "result is read, so the copy engine overlaps the sweep; one event pair over all steps",
+                "note": "streaming client, per step: lce_upload_stage(pinned host fields) two steps ahead, "
+                        "lce_upload_apply, lce_sweeps(1, measflag=1), lce_get_meas (the step's measurements "
+                        "read back); the copy engine overlaps the sweeps; one event pair over all steps",
                 "sequential": {"value": e2e_seq,
                                "note": "per step: lce_upload (returns when copied) + lce_sweep(measflag=1), "
                                        "L2 flushed before each step outside its events"},

@@ -166,12 +166,19 @@ int lce_synchronize(lce_ctx* ctx);
 /* ---- fields (COMMON /linkvar/ mirrors; f/confget.f / f/confsave.f boundary) ---- */
 int lce_upload(lce_ctx* ctx, int chain, int which, const float* u, const float* a, long ld);
 int lce_upload_f64(lce_ctx* ctx, int chain, int which, const double* u, const double* a, long ld);
-/* lce_upload without waiting (FP32 contexts): the host-to-device copy runs on
- * a copy stream of the context and the update calls queued after it see the
- * new fields.  The host buffers must stay unchanged until the next call that
- * synchronises the context stream (lce_synchronize, lce_get_meas, lce_sweep
- * with an lce_meas, lce_download); pinned buffers let the copy overlap the
- * sweeps queued before it. */
+/* lce_upload without waiting, FP32 contexts.  lce_upload_stage queues the
+ * host-to-device copy on a copy stream of the context, into one of two
+ * staging slots; lce_upload_apply makes the update calls queued after it see
+ * the oldest staged upload (a device copy on the context stream, after the
+ * staged copy).  At most two uploads are staged and not yet applied.  The host
+ * buffers must stay unchanged until the next call that synchronises the
+ * context stream after the apply (lce_synchronize, lce_get_meas, lce_sweep
+ * with an lce_meas, lce_download).  Pinned buffers let the copy overlap the
+ * work queued before it: a streaming client stages step k+2's input while
+ * step k sweeps and step k+1's is applied behind it.
+ * lce_upload_async = lce_upload_stage + lce_upload_apply (nothing staged). */
+int lce_upload_stage(lce_ctx* ctx, int chain, int which, const float* u, const float* a, long ld);
+int lce_upload_apply(lce_ctx* ctx);
 int lce_upload_async(lce_ctx* ctx, int chain, int which, const float* u, const float* a, long ld);
 int lce_download(lce_ctx* ctx, int chain, int which, float* u, float* a, long ld);
 int lce_download_f64(lce_ctx* ctx, int chain, int which, double* u, double* a, long ld);

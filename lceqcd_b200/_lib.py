@@ -95,6 +95,8 @@ SIGNATURES = {
     "lce_synchronize": (I, [P]),
     "lce_upload": (I, [P, I, I, P, P, C.c_long]),
     "lce_upload_async": (I, [P, I, I, P, P, C.c_long]),
+    "lce_upload_stage": (I, [P, I, I, P, P, C.c_long]),
+    "lce_upload_apply": (I, [P]),
     "lce_upload_f64": (I, [P, I, I, P, P, C.c_long]),
     "lce_download": (I, [P, I, I, P, P, C.c_long]),
     "lce_download_f64": (I, [P, I, I, P, P, C.c_long]),

@@ -14,6 +14,8 @@
 #include <cstddef>
 #include <cstdio>
 #include <cstring>
+#include <array>
+#include <deque>
 #include <map>
 #include <tuple>
 #include <string>
@@ -84,12 +86,16 @@ struct lce_ctx {
   size_t stream_n = 0;
   void* staging_d = nullptr;
   size_t staging_bytes = 0;
-  // asynchronous upload (lce_upload_async): copy stream, its staging area
-  // (links then A of the largest chain) and the events that order the two
-  // streams around it
+  // asynchronous uploads (lce_upload_stage / lce_upload_apply): copy stream,
+  // two staging slots (links then A of the largest chain, each), the events
+  // that order the two streams around each slot, and the staged uploads not
+  // yet applied (oldest first: slot, chain, field selector)
   cudaStream_t copy = nullptr;
-  cudaEvent_t staged_ev = nullptr, free_ev = nullptr;
+  cudaEvent_t staged_ev[2] = {nullptr, nullptr}, free_ev[2] = {nullptr, nullptr};
   void* async_d = nullptr;
+  size_t async_slot = 0;  // bytes per slot
+  int next_slot = 0;
+  std::deque<std::array<int, 3>> staged;
   void* flush_d = nullptr;
   size_t flush_bytes = 0;
   void* gsave_d = nullptr;  // G_prev during a warm-started gauge fixing
@@ -1462,8 +1468,10 @@ void lce_destroy(lce_ctx* c) {
     cudaStreamSynchronize(c->copy);
     cudaStreamDestroy(c->copy);
   }
-  if (c->staged_ev) cudaEventDestroy(c->staged_ev);
-  if (c->free_ev) cudaEventDestroy(c->free_ev);
+  for (int k = 0; k < 2; ++k) {
+    if (c->staged_ev[k]) cudaEventDestroy(c->staged_ev[k]);
+    if (c->free_ev[k]) cudaEventDestroy(c->free_ev[k]);
+  }
   if (c->own) cudaStreamDestroy(c->own);
   delete c;
 }
@@ -1498,41 +1506,72 @@ int lce_upload(lce_ctx* c, int chain, int which, const float* u, const float* a,
   if (!c) return LCE_ERR_INVALID;
   return upload_t<float>(c, chain, which, u, a, ld);
 }
-// The host-to-device copies run on a copy stream into a staging area; the
-// context stream waits for them and copies the staging area into the fields
-// (links: one device copy; A: the layout kernel of lce_upload).  The copy
-// stream waits for the previous call's device copies before it overwrites the
-// staging area, so one upload can be in flight while the context stream runs
-// the sweeps of the previous one.
-int lce_upload_async(lce_ctx* c, int chain, int which, const float* u, const float* a, long ld) {
+// Asynchronous uploads in two steps.  lce_upload_stage: the host-to-device
+// copies run on a copy stream into one of two staging slots (after the
+// previous upload through that slot has been applied).  lce_upload_apply: the
+// context stream waits for the oldest staged upload and copies it into the
+// fields (links: one device copy; A: the layout kernel of lce_upload).  With
+// two slots a client can stage the upload of step k+2 while step k+1's is
+// applied behind step k's sweeps, so the copy engine never waits for the
+// client.
+int lce_upload_stage(lce_ctx* c, int chain, int which, const float* u, const float* a, long ld) {
   DeviceScope ds_(c ? c->device : -1);
   if (!c) return LCE_ERR_INVALID;
-  if (c->prec != LCE_PREC_F32) return fail(c, LCE_ERR_UNSUPPORTED, "upload_async: FP32 contexts only (lce_upload)");
+  if (c->prec != LCE_PREC_F32) return fail(c, LCE_ERR_UNSUPPORTED, "upload_stage: FP32 contexts only (lce_upload)");
   if (chain < 0 || chain >= c->nchains || (which != LCE_FIELDS && which != LCE_FIELDS_FIXED))
-    return fail(c, LCE_ERR_INVALID, "upload_async: bad chain or field selector");
+    return fail(c, LCE_ERR_INVALID, "upload_stage: bad chain or field selector");
   const ChainDev& ch = c->ch[chain];
-  if (ld < ch.nh) return fail(c, LCE_ERR_INVALID, "upload_async: ld smaller than L1*L2*L3/2");
+  if (ld < ch.nh) return fail(c, LCE_ERR_INVALID, "upload_stage: ld smaller than L1*L2*L3/2");
+  if (c->staged.size() >= 2) return fail(c, LCE_ERR_INVALID, "upload_stage: two staged uploads not yet applied");
   const size_t ulb = align256((size_t)6 * c->max_nh * 16);
   if (!c->copy) {
     CK(cudaStreamCreateWithFlags(&c->copy, cudaStreamNonBlocking));
-    CK(cudaEventCreateWithFlags(&c->staged_ev, cudaEventDisableTiming));
-    CK(cudaEventCreateWithFlags(&c->free_ev, cudaEventDisableTiming));
-    CK(cudaMalloc(&c->async_d, ulb + (size_t)6 * c->max_nh * sizeof(float)));
-    CK(cudaEventRecord(c->free_ev, c->stream));
+    c->async_slot = ulb + align256((size_t)6 * c->max_nh * sizeof(float));
+    CK(cudaMalloc(&c->async_d, 2 * c->async_slot));
+    for (int k = 0; k < 2; ++k) {
+      CK(cudaEventCreateWithFlags(&c->staged_ev[k], cudaEventDisableTiming));
+      CK(cudaEventCreateWithFlags(&c->free_ev[k], cudaEventDisableTiming));
+      CK(cudaEventRecord(c->free_ev[k], c->stream));
+    }
   }
-  const int nh = ch.nh;
-  char* su = static_cast<char*>(c->async_d);
+  const int k = c->next_slot, nh = ch.nh;
+  char* su = static_cast<char*>(c->async_d) + (size_t)k * c->async_slot;
   char* sa = su + ulb;
-  CK(cudaStreamWaitEvent(c->copy, c->free_ev, 0));
+  CK(cudaStreamWaitEvent(c->copy, c->free_ev[k], 0));
   if (u) CK(cudaMemcpy2DAsync(su, (size_t)nh * 16, u, (size_t)ld * 16, (size_t)nh * 16, 6, cudaMemcpyHostToDevice, c->copy));
   if (a) CK(cudaMemcpy2DAsync(sa, (size_t)nh * 12, a, (size_t)ld * 12, (size_t)nh * 12, 2, cudaMemcpyHostToDevice, c->copy));
-  CK(cudaEventRecord(c->staged_ev, c->copy));
-  CK(cudaStreamWaitEvent(c->stream, c->staged_ev, 0));
-  if (u) CK(cudaMemcpyAsync(field_ptr(ch, which, true), su, (size_t)6 * nh * 16, cudaMemcpyDeviceToDevice, c->stream));
-  if (a) launch_higgs_in<float, float>(reinterpret_cast<const float*>(sa), field_ptr(ch, which, false), nh, c->stream);
-  CK(cudaGetLastError());
-  CK(cudaEventRecord(c->free_ev, c->stream));
+  CK(cudaEventRecord(c->staged_ev[k], c->copy));
+  c->staged.push_back({k, chain, which | (u ? 2 : 0) | (a ? 4 : 0)});
+  c->next_slot = 1 - k;
   return LCE_OK;
+}
+
+int lce_upload_apply(lce_ctx* c) {
+  DeviceScope ds_(c ? c->device : -1);
+  if (!c) return LCE_ERR_INVALID;
+  if (c->staged.empty()) return fail(c, LCE_ERR_INVALID, "upload_apply: no staged upload");
+  const std::array<int, 3> st = c->staged.front();
+  c->staged.pop_front();
+  const int k = st[0], which = st[2] & 1;
+  const ChainDev& ch = c->ch[st[1]];
+  const int nh = ch.nh;
+  char* su = static_cast<char*>(c->async_d) + (size_t)k * c->async_slot;
+  char* sa = su + align256((size_t)6 * c->max_nh * 16);
+  CK(cudaStreamWaitEvent(c->stream, c->staged_ev[k], 0));
+  if (st[2] & 2)
+    CK(cudaMemcpyAsync(field_ptr(ch, which, true), su, (size_t)6 * nh * 16, cudaMemcpyDeviceToDevice, c->stream));
+  if (st[2] & 4) launch_higgs_in<float, float>(reinterpret_cast<const float*>(sa), field_ptr(ch, which, false), nh, c->stream);
+  CK(cudaGetLastError());
+  CK(cudaEventRecord(c->free_ev[k], c->stream));
+  return LCE_OK;
+}
+
+int lce_upload_async(lce_ctx* c, int chain, int which, const float* u, const float* a, long ld) {
+  DeviceScope ds_(c ? c->device : -1);
+  if (!c) return LCE_ERR_INVALID;
+  if (!c->staged.empty()) return fail(c, LCE_ERR_INVALID, "upload_async: apply the staged uploads first");
+  if (int rc = lce_upload_stage(c, chain, which, u, a, ld)) return rc;
+  return lce_upload_apply(c);
 }
 
 int lce_upload_f64(lce_ctx* c, int chain, int which, const double* u, const double* a, long ld) {
@@ -2239,26 +2278,20 @@ int lce_profile_sweep(lce_ctx* c, int measflag, float* ms, int max_passes) {
   if (!*slot) {
     cudaGraph_t g;
     CK(cudaStreamBeginCapture(c->stream, cudaStreamCaptureModeThreadLocal));
-    // every timing event sits on the side stream, forked from the context
-    // stream at the start and after each kernel, so that the fork latency is
-    // the same in every difference
-    auto mark = [&](int k) {
-      cudaError_t x = cudaEventRecord(c->fork_ev, c->stream);
-      if (x == cudaSuccess) x = cudaStreamWaitEvent(c->side, c->fork_ev, 0);
-      if (x == cudaSuccess) x = cudaEventRecordWithFlags(c->prof_ev[k], c->side, cudaEventRecordExternal);
-      return x;
-    };
-    cudaError_t e = mark(0);
+    cudaError_t e = cudaEventRecordWithFlags(c->prof_ev[0], c->stream, cudaEventRecordExternal);
     Enq q;
     int rc = LCE_OK;
     if (e == cudaSuccess) {
       enq_begin(c, r, mf, true, c->tile_bs, c->tile_spt, c->tile_occ, q);
       for (int i = 0; i < np && rc == LCE_OK && e == cudaSuccess; ++i) {
         rc = enq_pass(c, q, i);
-        if (rc == LCE_OK) e = mark(i + 1);
+        if (rc == LCE_OK) e = cudaEventRecord(c->fork_ev, c->stream);
+        if (e == cudaSuccess) e = cudaStreamWaitEvent(c->side, c->fork_ev, 0);
+        if (e == cudaSuccess) e = cudaEventRecordWithFlags(c->prof_ev[i + 1], c->side, cudaEventRecordExternal);
       }
       if (rc == LCE_OK && e == cudaSuccess) rc = enq_end(c, q);
-      if (rc == LCE_OK && e == cudaSuccess) e = mark(np + 1);
+      if (rc == LCE_OK && e == cudaSuccess)
+        e = cudaEventRecordWithFlags(c->prof_ev[np + 1], c->stream, cudaEventRecordExternal);
     }
     // rejoin the side stream whatever happened, so that the capture can end
     const cudaError_t ej1 = cudaEventRecord(c->join_ev, c->side);

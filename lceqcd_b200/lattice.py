@@ -124,13 +124,18 @@ class _Context:
             raise _lib.LceError(_lib.LCE_ERR_INVALID, "lce_create: " + self.lib.lce_last_error(None).decode())
         self.h = C.c_void_p(h)
         self.dtype = np.float64 if self.params[0].precision == "f64" else np.float32
-        self._inflight = []  # host arrays of lce_upload_async calls not yet known to be copied
+        # host arrays of asynchronous uploads: applied ones not yet known to be
+        # copied (released by the next synchronising call), and staged ones
+        # (oldest first; moved to _inflight by upload_apply)
+        self._inflight = []
+        self._staged = []
 
     def close(self):
         if getattr(self, "h", None):
             self.lib.lce_destroy(self.h)  # synchronises the copy stream
             self.h = None
             self._inflight = []
+            self._staged = []
 
     def __del__(self):
         self.close()
@@ -153,16 +158,32 @@ class _Context:
         fn = self.lib.lce_upload_f64 if f64 else self.lib.lce_upload
         self._ck(fn(self.h, chain, which, None if uu is None else _ptr(uu), None if aa is None else _ptr(aa), nh))
 
-    def upload_async(self, u=None, a=None, which: int = 0, chain: int = 0):
-        """lce_upload_async: FP32 fields, returns before the copy ends.  The
-        arrays are kept referenced until the next synchronising call; pass
-        pinned arrays for a copy that overlaps the sweeps queued before it."""
+    def _async_args(self, u, a, chain, keep):
         nh = self.nh(chain)
         uu = None if u is None else np.ascontiguousarray(u, np.float32).reshape(3, 2, nh, 4)
         aa = None if a is None else np.ascontiguousarray(a, np.float32).reshape(2, nh, 3)
-        self._ck(self.lib.lce_upload_async(self.h, chain, which, None if uu is None else _ptr(uu),
-                                           None if aa is None else _ptr(aa), nh))
-        self._inflight.append((uu, aa))
+        keep.append((uu, aa))
+        return None if uu is None else _ptr(uu), None if aa is None else _ptr(aa), nh
+
+    def upload_async(self, u=None, a=None, which: int = 0, chain: int = 0):
+        """lce_upload_async: FP32 fields, returns before the copy ends.  The
+        arrays are kept referenced until the next synchronising call; pass
+        pinned arrays for a copy that overlaps the work queued before it."""
+        pu, pa, nh = self._async_args(u, a, chain, self._inflight)
+        self._ck(self.lib.lce_upload_async(self.h, chain, which, pu, pa, nh))
+
+    def upload_stage(self, u=None, a=None, which: int = 0, chain: int = 0):
+        """lce_upload_stage: queue the host-to-device copy into a staging slot."""
+        pu, pa, nh = self._async_args(u, a, chain, self._staged)
+        rc = self.lib.lce_upload_stage(self.h, chain, which, pu, pa, nh)
+        if rc < 0:
+            self._staged.pop()
+        self._ck(rc)
+
+    def upload_apply(self):
+        """lce_upload_apply: later update calls see the oldest staged upload."""
+        self._ck(self.lib.lce_upload_apply(self.h))
+        self._inflight.append(self._staged.pop(0))
 
     def download(self, which: int = 0, chain: int = 0, dtype=None):
         nh = self.nh(chain)

@@ -83,6 +83,49 @@ def test_pipelined_client_matches_sequential():
         assert m_seq == m_pipe
 
 
+def test_streaming_client_two_slots_matches_sequential():
+    """lce_upload_stage two steps ahead, lce_upload_apply behind each sweep:
+    every step sweeps its own configuration."""
+    cfgs = _configs(5)
+    seq = []
+    g = Lattice(L, **KW)
+    for u, a in cfgs:
+        g.upload(u, a)
+        seq.append(g.sweep(1))
+    g.close()
+    pins = [_pinned(u, a) for u, a in cfgs]
+    g = Lattice(L, **KW)
+    got = []
+    g.upload_stage(*pins[0])
+    g.upload_apply()
+    g.upload_stage(*pins[1])
+    for k in range(5):
+        g.sweeps(1, 1)
+        got.append(g.meas1())
+        if k + 1 < 5:
+            g.upload_apply()
+        if k + 2 < 5:
+            g.upload_stage(*pins[k + 2])
+    with pytest.raises(_lib.LceError):
+        g.upload_apply()  # nothing staged
+    g.close()
+    assert got == seq
+
+
+def test_upload_stage_refuses_a_third_pending_upload():
+    (u, a), = _configs(1)
+    g = Lattice(L, **KW)
+    p = _pinned(u, a)
+    g.upload_stage(*p)
+    g.upload_stage(*p)
+    with pytest.raises(_lib.LceError):
+        g.upload_stage(*p)
+    g.upload_apply()
+    g.upload_apply()
+    np.testing.assert_array_equal(g.download()[0], u)
+    g.close()
+
+
 def test_upload_async_fp64_context_unsupported():
     g = Lattice((8, 8, 8), beta=9.0, x=0.1, y=0.5, precision="f64", seed=2)
     u, a = g.download()
