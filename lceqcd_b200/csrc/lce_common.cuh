@@ -65,17 +65,22 @@ template <typename R>
 LCE_HD su2<R> dd(su2<R> u1, su2<R> u2) {
   return su2<R>{cj(u1.a) * cj(u2.a) - u1.b * cj(u2.b), -(cj(u1.a) * u2.b) - u1.b * u2.a};
 }
+// i a3 z for real a3: the product by the purely imaginary diagonal entry of
+// iA without its zero real part (equal to (0, a3) * z but for the sign of a
+// zero)
+template <typename R>
+LCE_HD cpx<R> imul(R a3, cpx<R> z) { return cpx<R>{-(a3 * z.im), a3 * z.re}; }
 // MULTALLAD:150-154   (iA) U^+
 template <typename R>
 LCE_HD su2<R> ad(R a1, R a2, R a3, su2<R> u) {
-  cpx<R> x = mk<R>(0, a3), y = mk<R>(a2, a1);
-  return su2<R>{x * cj(u.a) + y * cj(u.b), -(x * u.b) + y * u.a};
+  cpx<R> y = mk<R>(a2, a1);
+  return su2<R>{imul(a3, cj(u.a)) + y * cj(u.b), -imul(a3, u.b) + y * u.a};
 }
 // MULTALLAN:183-187   (iA) U
 template <typename R>
 LCE_HD su2<R> an(R a1, R a2, R a3, su2<R> u) {
-  cpx<R> x = mk<R>(0, a3), y = mk<R>(a2, a1);
-  return su2<R>{x * u.a - y * cj(u.b), x * u.b + y * cj(u.a)};
+  cpx<R> y = mk<R>(a2, a1);
+  return su2<R>{imul(a3, u.a) - y * cj(u.b), imul(a3, u.b) + y * cj(u.a)};
 }
 
 template <typename R>
@@ -226,14 +231,10 @@ LCE_HD int site_index(int x, int y, int z, int hx, int nxy) { return z * nxy + y
 LCE_HD void philox4x32_10(uint32_t c[4], uint32_t k0, uint32_t k1) {
 #pragma unroll
   for (int r = 0; r < 10; ++r) {
-#ifdef __CUDA_ARCH__
-    uint32_t hi0 = __umulhi(0xD2511F53u, c[0]), lo0 = 0xD2511F53u * c[0];
-    uint32_t hi1 = __umulhi(0xCD9E8D57u, c[2]), lo1 = 0xCD9E8D57u * c[2];
-#else
-    uint64_t p0 = (uint64_t)0xD2511F53u * c[0], p1 = (uint64_t)0xCD9E8D57u * c[2];
-    uint32_t hi0 = (uint32_t)(p0 >> 32), lo0 = (uint32_t)p0;
-    uint32_t hi1 = (uint32_t)(p1 >> 32), lo1 = (uint32_t)p1;
-#endif
+    // one 32x32 -> 64-bit multiply gives both halves
+    const uint64_t p0 = (uint64_t)0xD2511F53u * c[0], p1 = (uint64_t)0xCD9E8D57u * c[2];
+    const uint32_t hi0 = (uint32_t)(p0 >> 32), lo0 = (uint32_t)p0;
+    const uint32_t hi1 = (uint32_t)(p1 >> 32), lo1 = (uint32_t)p1;
     uint32_t n0 = hi1 ^ c[1] ^ k0, n2 = hi0 ^ c[3] ^ k1;
     c[0] = n0;
     c[1] = lo1;
@@ -244,7 +245,17 @@ LCE_HD void philox4x32_10(uint32_t c[4], uint32_t k0, uint32_t k1) {
   }
 }
 // (2k+1)/2^24 with k the top 23 bits: strictly inside (0,1), exact in FP32.
-LCE_HD float u01(uint32_t x) { return (float)((x >> 9) * 2u + 1u) * 5.9604644775390625e-8f; }
+// On the device it is built without an integer-to-float conversion: the bits
+// 0x3f800000 | k are the float 1 + k 2^-23, and subtracting 1 - 2^-24 (the
+// float below 1) leaves (2k+1) 2^-24 exactly (the operands are within a
+// factor 2 of each other, so the difference is exact -- Sterbenz's lemma).
+LCE_HD float u01(uint32_t x) {
+#ifdef __CUDA_ARCH__
+  return __uint_as_float(0x3f800000u | (x >> 9)) - 0.999999940395355224609375f;
+#else
+  return (float)((x >> 9) * 2u + 1u) * 5.9604644775390625e-8f;
+#endif
+}
 
 // Uniform slot layouts of one update pass in the reference's consumption
 // order: PLANAR puts slot k of site s at k*nh + s; TRIPLE interleaves slots
