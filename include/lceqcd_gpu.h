@@ -406,6 +406,12 @@ int lce_slabs_download_fixed_f64(lce_slabs* s, double* u, double* a, long ld);
  * goes back to the slab below, theta is the whole lattice's; same iterations
  * and (up to the order of the theta sum) the same u_f, a_f as undecomposed */
 int lce_slabs_landau_gauge(lce_slabs* s, double* theta, int* iters, int max_iters);
+/* the same fixing tracking the gauge transform G (lce_landau_gauge_from on
+ * the slabs), from G = 1 (LCE_GF_START_IDENTITY) or from the transform of
+ * the slabs' last tracked fixing applied to the current fields
+ * (LCE_GF_START_TRANSFORM, the previous measurement's warm start); same
+ * iterations and u_f, a_f as undecomposed */
+int lce_slabs_landau_gauge_from(lce_slabs* s, int start, double* theta, int* iters, int max_iters);
 /* lce_correlator / lce_polyakov / lce_scalarcorr of the whole lattice
  * (f/correlator.f, f/polyakov.f, f/scalarcorr.f): slice sums per slab,
  * correlated on the first slab's device */

@@ -1031,8 +1031,10 @@ int slab_rc(lce_ctx* c, int rc) {
 // device address of local plane z of a slab's field at local parity p: the
 // links U_mu (f = mu) or component k of the Higgs field (f = -1); fixed:
 // the gauge-fixed copies U_f, A_f
+// f: a link direction 0-2, 3 for the gauge transform G, -1 for the Higgs field
 char* slab_plane(lce_ctx* c, int f, int p, int z, int k, bool fixed = false) {
   const ChainDev& d = c->ch[0];
+  if (f == 3) return (char*)d.g + ((size_t)p * d.nh + (size_t)z * d.nxy) * link_bytes(c->prec);
   if (f >= 0)
     return (char*)(fixed ? d.uf : d.u) + (((size_t)(f * 2 + p)) * d.nh + (size_t)z * d.nxy) * link_bytes(c->prec);
   return (char*)(fixed ? d.af : d.a) + (((size_t)(p * 3 + k)) * d.nh + (size_t)z * d.nxy) * real_bytes(c->prec);
@@ -1191,7 +1193,7 @@ int slab_sweep(lce_slabs* S, int measflag, lce_meas* m) {
 // verdict copied to every slab's chain state, all ordered by events: no host
 // round trip inside a batch of iterations.
 template <typename R>
-int slab_gf_iterations(lce_slabs* S, int batch) {
+int slab_gf_iterations(lce_slabs* S, int batch, int track) {
   const int n = (int)S->slab.size(), nz = S->nz;
   lce_ctx* c0 = S->slab[0];
   const size_t off = offsetof(ChainState, gf_theta), len = offsetof(ChainState, gf_pad) - off;
@@ -1201,7 +1203,7 @@ int slab_gf_iterations(lce_slabs* S, int batch) {
       for (int k = 0; k < n; ++k) {
         lce_ctx* c = S->slab[k];
         DeviceScope ds_(c->device);
-        launch_gf_half<R>(c->ch_d, c->cst_d, pg ^ c->eo_flip, pg, c->scratch_d, c->ch[0].nh, c->s_lo, c->stream);
+        launch_gf_half<R>(c->ch_d, c->cst_d, pg ^ c->eo_flip, pg, c->scratch_d, c->ch[0].nh, c->s_lo, track, c->stream);
         SCK(cudaGetLastError());
         SCK(cudaEventRecord(S->ev_pass[k], c->stream));
       }
@@ -1240,17 +1242,45 @@ int slab_gf_iterations(lce_slabs* S, int batch) {
   return LCE_OK;
 }
 
-int slab_landau_gauge(lce_slabs* S, double* theta, int* iters, int max_iters) {
-  const int n = (int)S->slab.size();
+// start < 0: the reference's fixing from U (no transform kept); otherwise a
+// tracked fixing (G accumulated as in lce_landau_gauge_from) from G = 1
+// (LCE_GF_START_IDENTITY) or from the transform the slabs hold
+// (LCE_GF_START_TRANSFORM: the G planes next to every slab boundary are
+// exchanged into the halos, then U_f = G U G^+ and A_f = G A G^+ on every
+// plane of every slab -- a slab's halo planes get the values its neighbours
+// compute for them, so the start equals the undecomposed one bit for bit)
+int slab_landau_gauge(lce_slabs* S, double* theta, int* iters, int max_iters, int start = -1) {
+  const int n = (int)S->slab.size(), nz = S->nz;
   lce_ctx* c0 = S->slab[0];
   const int cap = max_iters > 0 ? max_iters : 1000000;
+  if (start == LCE_GF_START_TRANSFORM) {
+    for (int k = 0; k < n; ++k) {
+      lce_ctx* c = S->slab[k];
+      DeviceScope ds_(c->device);
+      SCK(cudaEventRecord(S->ev_pass[k], c->stream));
+    }
+    const PlaneCopy cp[4] = {{-1, nz, 0, 3, 0, false}, {-1, nz, 0, 3, 1, false},
+                             {+1, 1, nz + 1, 3, 0, false}, {+1, 1, nz + 1, 3, 1, false}};
+    if (int rc = slab_exchange(S, cp, 4)) return rc;
+  }
   for (int k = 0; k < n; ++k) {
     lce_ctx* c = S->slab[k];
     DeviceScope ds_(c->device);
     const ChainDev& ch = c->ch[0];
-    const size_t ub = (size_t)6 * ch.nh * link_bytes(c->prec), ab = (size_t)6 * ch.nh * real_bytes(c->prec);
-    SCK(cudaMemcpyAsync(ch.uf, ch.u, ub, cudaMemcpyDeviceToDevice, c->stream));
-    SCK(cudaMemcpyAsync(ch.af, ch.a, ab, cudaMemcpyDeviceToDevice, c->stream));
+    if (start == LCE_GF_START_TRANSFORM) {
+      if (c->prec == LCE_PREC_F64) launch_gauge_apply<double>(c->ch_d, ch.nh, c->stream);
+      else launch_gauge_apply<float>(c->ch_d, ch.nh, c->stream);
+      SCK(cudaGetLastError());
+    } else {
+      const size_t ub = (size_t)6 * ch.nh * link_bytes(c->prec), ab = (size_t)6 * ch.nh * real_bytes(c->prec);
+      SCK(cudaMemcpyAsync(ch.uf, ch.u, ub, cudaMemcpyDeviceToDevice, c->stream));
+      SCK(cudaMemcpyAsync(ch.af, ch.a, ab, cudaMemcpyDeviceToDevice, c->stream));
+      if (start == LCE_GF_START_IDENTITY) {
+        if (c->prec == LCE_PREC_F64) launch_transform_identity<double>(ch.g, ch.nh, c->stream);
+        else launch_transform_identity<float>(ch.g, ch.nh, c->stream);
+        SCK(cudaGetLastError());
+      }
+    }
     ChainState cs;
     SCK(cudaMemcpyAsync(&cs, c->cst_d, sizeof(cs), cudaMemcpyDeviceToHost, c->stream));
     SCK(cudaStreamSynchronize(c->stream));
@@ -1265,7 +1295,9 @@ int slab_landau_gauge(lce_slabs* S, double* theta, int* iters, int max_iters) {
   std::memset(&cs, 0, sizeof(cs));
   int batch = 8;
   while (true) {
-    const int rc = S->prec == LCE_PREC_F64 ? slab_gf_iterations<double>(S, batch) : slab_gf_iterations<float>(S, batch);
+    const int track = start >= 0 ? 1 : 0;
+    const int rc = S->prec == LCE_PREC_F64 ? slab_gf_iterations<double>(S, batch, track)
+                                           : slab_gf_iterations<float>(S, batch, track);
     if (rc) return rc;
     const int before = cs.gf_iters;
     {
@@ -2509,6 +2541,14 @@ int lce_slabs_landau_gauge(lce_slabs* h, double* theta, int* iters, int max_iter
   lce_slabs* S = h;
   if (!S) return LCE_ERR_INVALID;
   return slab_landau_gauge(S, theta, iters, max_iters);
+}
+
+int lce_slabs_landau_gauge_from(lce_slabs* h, int start, double* theta, int* iters, int max_iters) {
+  lce_slabs* S = h;
+  if (!S) return LCE_ERR_INVALID;
+  if (start != LCE_GF_START_IDENTITY && start != LCE_GF_START_TRANSFORM)
+    return slabs_fail(LCE_ERR_INVALID, "slabs_landau_gauge_from: start must be IDENTITY or TRANSFORM");
+  return slab_landau_gauge(S, theta, iters, max_iters, start);
 }
 
 int lce_slabs_correlator(lce_slabs* h, double* corr_a, double* corr_u, double* corr_3, double af[3]) {

@@ -349,10 +349,10 @@ void launch_gf_iteration(const ChainDev* ch, ChainState* cst, int track, double*
 }
 
 template <typename R>
-int launch_gf_half(const ChainDev* ch, ChainState* cst, int eo, int last, double* part, int nh, int s_lo,
+int launch_gf_half(const ChainDev* ch, ChainState* cst, int eo, int last, double* part, int nh, int s_lo, int track,
                    cudaStream_t s) {
   const int nb = ceil_div(nh - 2 * s_lo, kBlock);
-  (void)launch_pdl(gf_half_kernel<R>, nb, kBlock, 0, s, ch, (const ChainState*)cst, eo, part, 0, s_lo, last);
+  (void)launch_pdl(gf_half_kernel<R>, nb, kBlock, 0, s, ch, (const ChainState*)cst, eo, part, track, s_lo, last);
   return nb;
 }
 
@@ -398,8 +398,8 @@ void launch_sum_partials(const double* part, int nblocks, int nq, double* out, c
 
 template void launch_gf_iteration<float>(const ChainDev*, ChainState*, int, double*, int, cudaStream_t);
 template void launch_gf_iteration<double>(const ChainDev*, ChainState*, int, double*, int, cudaStream_t);
-template int launch_gf_half<float>(const ChainDev*, ChainState*, int, int, double*, int, int, cudaStream_t);
-template int launch_gf_half<double>(const ChainDev*, ChainState*, int, int, double*, int, int, cudaStream_t);
+template int launch_gf_half<float>(const ChainDev*, ChainState*, int, int, double*, int, int, int, cudaStream_t);
+template int launch_gf_half<double>(const ChainDev*, ChainState*, int, int, double*, int, int, int, cudaStream_t);
 template void launch_it_iteration<float>(const ChainDev*, ChainState*, int, int, double*, int, cudaStream_t);
 template void launch_it_iteration<double>(const ChainDev*, ChainState*, int, int, double*, int, cudaStream_t);
 template void launch_gf_theta<float>(const ChainDev*, double*, int, cudaStream_t);

@@ -206,10 +206,10 @@ void launch_gf_iteration(const ChainDev* ch, ChainState* cst, int track, double*
                          cudaStream_t s);
 // one overrelaxed half-step over sites [s_lo, nh - s_lo) of local parity eo
 // (a z-slab: s_lo = one plane); last: the second half-step, which writes the
-// theta partials into part and reunitarises; returns the number of blocks
-// (partials)
+// theta partials into part and reunitarises; track: also accumulate the
+// transform G; returns the number of blocks (partials)
 template <typename R>
-int launch_gf_half(const ChainDev* ch, ChainState* cst, int eo, int last, double* part, int nh, int s_lo,
+int launch_gf_half(const ChainDev* ch, ChainState* cst, int eo, int last, double* part, int nh, int s_lo, int track,
                    cudaStream_t s);
 // convergence test of a z-slab decomposed fixing from the slabs' theta sums
 void launch_gf_check_slabs(const ChainDev* ch, ChainState* cst, const double* sums, int nslabs, double nh,

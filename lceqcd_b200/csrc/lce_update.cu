@@ -497,19 +497,23 @@ __device__ __forceinline__ void finalize_chain_warp(const FinalizeArgs& f, int w
 // loads in flight at once (L2, the sums of other blocks), then the in-order
 // scan over the slots reads them from the lanes by shuffles -- one L2 round
 // trip per chain instead of one per slot.
-__device__ __forceinline__ void finalize_combine(const FinalizeArgs& f) {
+// SM: the totals of a single chain are in shared memory (stot) instead of
+// f.totals.
+template <bool SM = false>
+__device__ __forceinline__ void finalize_combine(const FinalizeArgs& f, const double* stot = nullptr) {
   static_assert(kMaxSlots <= 64, "two slots per lane");
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarps = (int)(blockDim.x >> 5);
   for (int c = warp; c < f.nchains; c += nwarps) {
     const ChainDev& ch = f.chains[c];
     const double V = 2.0 * ch.nh;
-    const double* base = f.totals + (size_t)c * kMaxSlots * kNQ;
+    const double* base = SM ? stot : f.totals + (size_t)c * kMaxSlots * kNQ;
     double t0[kNQ], t1[kNQ];
     bool bad = false;
 #pragma unroll
     for (int q = 0; q < kNQ; ++q) {
-      t0[q] = lane < f.nslots ? __ldcg(base + (size_t)lane * kNQ + q) : 0.0;
-      t1[q] = lane + 32 < f.nslots ? __ldcg(base + (size_t)(lane + 32) * kNQ + q) : 0.0;
+      const size_t i0 = (size_t)lane * kNQ + q, i1 = (size_t)(lane + 32) * kNQ + q;
+      t0[q] = lane < f.nslots ? (SM ? base[i0] : __ldcg(base + i0)) : 0.0;
+      t1[q] = lane + 32 < f.nslots ? (SM ? base[i1] : __ldcg(base + i1)) : 0.0;
       bad = bad || !isfinite(t0[q]) || !isfinite(t1[q]);
     }
     if (__any_sync(0xffffffffu, bad) && lane == 0) atomicOr(&f.st->status, kStatusNaN);
@@ -585,6 +589,83 @@ __device__ __forceinline__ void finalize_combine(const FinalizeArgs& f) {
     f.st->pass_ctr += f.npasses;
     f.st->stream_pos += f.nstream;
   }
+}
+
+// One block for a single chain of at most kSmallChunks chunks: warp w takes
+// the slots w, w + kFinSmallWarps, ... whole -- the loads of two chunks at a
+// time, level 1 of each chunk, level 2 across the chunks in registers (chunk
+// k's sum goes to lane k mod 32, added in chunk order), the same additions in
+// the same order as the two-level kernel below -- and the combine reads the
+// totals from shared memory: one global round trip per two chunks instead of
+// three for the whole reduction.
+constexpr int kFinSmallWarps = 16;
+constexpr int kSmallChunks = 8;
+__global__ void __launch_bounds__(kFinSmallWarps * 32) finalize_small_kernel(FinalizeArgs f) {
+  pdl_trigger();
+  pdl_wait();
+  __shared__ double s_tot[kMaxSlots * kNQ];
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const int b0 = __ldg(f.blk_begin), b1 = __ldg(f.blk_begin + 1);
+  const int nch = f.nchunks;
+  for (int i = warp; i < f.nslots; i += kFinSmallWarps) {
+    const double2* part = reinterpret_cast<const double2*>(f.part + (size_t)i * f.slot_stride);
+    double acc[kNQ] = {0.0, 0.0, 0.0, 0.0}, tot[kNQ] = {0.0, 0.0, 0.0, 0.0};
+    for (int k0 = 0; k0 < nch; k0 += 2) {
+      double2 x[2][4][2];
+#pragma unroll
+      for (int kk = 0; kk < 2; ++kk) {
+        const int t0 = b0 + (k0 + kk) * kChunkTiles, t1 = min(b1, t0 + kChunkTiles);
+#pragma unroll
+        for (int j = 0; j < 4; ++j) {
+          const int t = t0 + lane + 32 * j;
+          const bool ok = k0 + kk < nch && t < t1;
+          x[kk][j][0] = ok ? __ldcg(part + (size_t)t * 2) : make_double2(0.0, 0.0);
+          x[kk][j][1] = ok ? __ldcg(part + (size_t)t * 2 + 1) : make_double2(0.0, 0.0);
+        }
+      }
+#pragma unroll
+      for (int kk = 0; kk < 2; ++kk) {
+        const int k = k0 + kk;
+        if (k >= nch) break;
+        const int t0 = b0 + k * kChunkTiles, t1 = min(b1, t0 + kChunkTiles);
+        double v[kNQ] = {0.0, 0.0, 0.0, 0.0};
+#pragma unroll
+        for (int j = 0; j < 4; ++j) {
+          if (t0 + lane + 32 * j < t1) {
+            v[0] += x[kk][j][0].x;
+            v[1] += x[kk][j][0].y;
+            v[2] += x[kk][j][1].x;
+            v[3] += x[kk][j][1].y;
+          }
+        }
+        warp_tree(v);
+        if (nch == 1) {
+#pragma unroll
+          for (int q = 0; q < kNQ; ++q) tot[q] = v[q];
+        } else {
+#pragma unroll
+          for (int q = 0; q < kNQ; ++q) {
+            const double b = __shfl_sync(0xffffffffu, v[q], 0);
+            if (lane == (k & 31)) acc[q] += b;
+          }
+        }
+      }
+    }
+    if (nch > 1) {
+      warp_tree(acc);
+#pragma unroll
+      for (int q = 0; q < kNQ; ++q) tot[q] = acc[q];
+    }
+    if (lane == 0) {
+#pragma unroll
+      for (int q = 0; q < kNQ; ++q) {
+        s_tot[i * kNQ + q] = tot[q];
+        f.totals[(size_t)i * kNQ + q] = tot[q];
+      }
+    }
+  }
+  __syncthreads();
+  finalize_combine<true>(f, s_tot);
 }
 
 // kFinWarps warps per block, one level-1 item per warp.  One block: level 2
@@ -832,6 +913,10 @@ void launch_link(int mode, int mu, const PassArgs& a, int nblocks, cudaStream_t 
 }
 
 void launch_finalize(const FinalizeArgs& f, cudaStream_t s) {
+  if (f.nchains == 1 && f.nchunks <= kSmallChunks) {
+    (void)launch_pdl(finalize_small_kernel, 1, kFinSmallWarps * 32, 0, s, f);
+    return;
+  }
   // up to four level-1 items per warp before a second block (and the
   // ticket) is worth it
   int grid = (f.nchunks * f.nslots + 4 * kFinWarps - 1) / (4 * kFinWarps);

@@ -602,6 +602,14 @@ class SlabLattice:
         self._ck(self.lib.lce_slabs_landau_gauge(self.h, C.byref(th), C.byref(it), int(max_iters)))
         return th.value, it.value
 
+    def landau_gauge_from(self, start: str = "identity", max_iters: int = 0):
+        """Lattice.landau_gauge_from on the slabs (the transform G tracked;
+        start 'identity' or 'transform'); returns (theta, iterations)."""
+        th, it = C.c_double(), C.c_int()
+        code = {"identity": _lib.LCE_GF_START_IDENTITY, "transform": _lib.LCE_GF_START_TRANSFORM}[start]
+        self._ck(self.lib.lce_slabs_landau_gauge_from(self.h, code, C.byref(th), C.byref(it), int(max_iters)))
+        return th.value, it.value
+
     def correlator(self):
         L3 = self.params.L[2]
         ca, cu, c3, af = np.zeros(L3), np.zeros(L3), np.zeros(L3), np.zeros(3)

@@ -123,6 +123,32 @@ def _fixed(g, dt):
     return g.download(which=1, dtype=dt)  # LCE_FIELDS_FIXED
 
 
+@pytest.mark.parametrize("precision,limit_or", [("f64", 1e-10), ("f32", 1e-6)])
+@pytest.mark.parametrize("L,nslabs", [((8, 8, 8), 2), ((8, 6, 12), 3), ((6, 8, 16), 4)])
+def test_slabs_tracked_fixing_and_warm_start(precision, limit_or, L, nslabs):
+    """lce_landau_gauge_from on the slabs: the fixing from G = 1 tracking the
+    transform, three more sweeps, then the fixing from the previous
+    transform (G exchanged across the slab boundaries and applied on every
+    plane) -- the undecomposed run's iterations and u_f, a_f bit for bit."""
+    g, s, dt = _thermalised_pair(L, nslabs, precision, limit_or)
+    _, tg, ig = g.landau_gauge_from("identity")
+    ts, is_ = s.landau_gauge_from("identity")
+    assert is_ == ig and ig > 10 and abs(ts - tg) <= 1e-9 * tg
+    for x, y in zip(s.download(dtype=dt, fixed=True), _fixed(g, dt)):
+        np.testing.assert_array_equal(x, y)
+    for _ in range(3):
+        g.sweep(0)
+        s.sweep(0)
+    _, tg2, ig2 = g.landau_gauge_from("transform")
+    ts2, is2 = s.landau_gauge_from("transform")
+    assert is2 == ig2 and abs(ts2 - tg2) <= 1e-9 * tg2
+    for x, y in zip(s.download(dtype=dt, fixed=True), _fixed(g, dt)):
+        np.testing.assert_array_equal(x, y)
+    with pytest.raises(LceError):  # LCE_GF_START_NET: no network on slabs
+        s._ck(s.lib.lce_slabs_landau_gauge_from(s.h, 2, None, None, 0))
+    s.close()
+
+
 def test_slabs_landau_gauge_cap():
     """An iteration cap stops both runs at the same iteration with the
     reference's not-converged status and the same partly fixed u_f."""
