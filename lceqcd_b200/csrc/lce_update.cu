@@ -917,9 +917,10 @@ void launch_finalize(const FinalizeArgs& f, cudaStream_t s) {
     (void)launch_pdl(finalize_small_kernel, 1, kFinSmallWarps * 32, 0, s, f);
     return;
   }
-  // up to four level-1 items per warp before a second block (and the
-  // ticket) is worth it
-  int grid = (f.nchunks * f.nslots + 4 * kFinWarps - 1) / (4 * kFinWarps);
+  // one block for up to four level-1 items per warp (no ticket); beyond
+  // that one item per warp, all loads in flight at once
+  const int n1 = f.nchunks * f.nslots;
+  int grid = n1 <= 4 * kFinWarps ? 1 : (n1 + kFinWarps - 1) / kFinWarps;
   if (grid < 1) grid = 1;
   (void)launch_pdl(finalize_kernel, grid, kFinWarps * 32, 0, s, f);
 }
