@@ -412,6 +412,14 @@ int lce_slabs_landau_gauge(lce_slabs* s, double* theta, int* iters, int max_iter
  * (LCE_GF_START_TRANSFORM, the previous measurement's warm start); same
  * iterations and u_f, a_f as undecomposed */
 int lce_slabs_landau_gauge_from(lce_slabs* s, int start, double* theta, int* iters, int max_iters);
+/* lce_landau_gauge_fourier on the slabs (G tracked; start IDENTITY or
+ * TRANSFORM): the divergence, g and its application run on every slab's
+ * planes, the x transforms of a slab's lines too; the whole lattice's two
+ * transformed fields (16 bytes per site) live on the first slab's device,
+ * where the y and z transforms run.  Same iterations and u_f, a_f as
+ * undecomposed.  Extents: powers of two up to 1024. */
+int lce_slabs_landau_gauge_fourier(lce_slabs* s, int start, double step, double theta_switch, double* theta,
+                                   int* iters_fourier, int* iters_plain, int max_iters);
 /* lce_correlator / lce_polyakov / lce_scalarcorr of the whole lattice
  * (f/correlator.f, f/polyakov.f, f/scalarcorr.f): slice sums per slab,
  * correlated on the first slab's device */

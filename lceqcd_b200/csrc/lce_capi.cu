@@ -1005,6 +1005,7 @@ struct lce_slabs {
   std::vector<cudaEvent_t> ev_pass, ev_copy, ev_sum;
   cudaEvent_t ev_chk = nullptr;
   double* g_d = nullptr;  // slab 0's device: theta sums [n], slice sums [14 L3], correlators [7 L3 + 5]
+  void* fft_d = nullptr;  // slab 0's device: the whole lattice's two transformed fields (Fourier fixing)
   int L[3] = {0, 0, 0};
   int nz = 0, nxy = 0, prec = LCE_PREC_F32;
   double delta = 0.0;  // ahiggs1 step of the whole lattice (every slab holds a copy)
@@ -1031,9 +1032,14 @@ int slab_rc(lce_ctx* c, int rc) {
 // device address of local plane z of a slab's field at local parity p: the
 // links U_mu (f = mu) or component k of the Higgs field (f = -1); fixed:
 // the gauge-fixed copies U_f, A_f
-// f: a link direction 0-2, 3 for the gauge transform G, -1 for the Higgs field
+// f: a link direction 0-2, 3 for the gauge transform G, 4 for the Fourier
+// iteration's step transform g (FP64), -1 for the Higgs field
+size_t slab_elem_bytes(const lce_ctx* c, int f) {
+  return f == 4 ? 32 : (f >= 0 ? link_bytes(c->prec) : real_bytes(c->prec));
+}
 char* slab_plane(lce_ctx* c, int f, int p, int z, int k, bool fixed = false) {
   const ChainDev& d = c->ch[0];
+  if (f == 4) return (char*)fa_gstep_ptr(c->fa_d, fa_vcap(c)) + ((size_t)p * d.nh + (size_t)z * d.nxy) * 32;
   if (f == 3) return (char*)d.g + ((size_t)p * d.nh + (size_t)z * d.nxy) * link_bytes(c->prec);
   if (f >= 0)
     return (char*)(fixed ? d.uf : d.u) + (((size_t)(f * 2 + p)) * d.nh + (size_t)z * d.nxy) * link_bytes(c->prec);
@@ -1050,7 +1056,7 @@ struct PlaneCopy {
 
 int slab_copy_plane(lce_ctx* c, lce_ctx* cj, const PlaneCopy& q, size_t nxy) {
   const int ps = q.pg ^ cj->eo_flip, pd = q.pg ^ c->eo_flip;
-  const size_t bytes = nxy * (q.f >= 0 ? link_bytes(c->prec) : real_bytes(c->prec));
+  const size_t bytes = nxy * slab_elem_bytes(c, q.f);
   for (int comp = 0; comp < (q.f >= 0 ? 1 : 3); ++comp) {
     void* dst = slab_plane(c, q.f, pd, q.zd, comp, q.fixed);
     const void* src = slab_plane(cj, q.f, ps, q.zs, comp, q.fixed);
@@ -1242,17 +1248,94 @@ int slab_gf_iterations(lce_slabs* S, int batch, int track) {
   return LCE_OK;
 }
 
-// start < 0: the reference's fixing from U (no transform kept); otherwise a
-// tracked fixing (G accumulated as in lce_landau_gauge_from) from G = 1
-// (LCE_GF_START_IDENTITY) or from the transform the slabs hold
-// (LCE_GF_START_TRANSFORM: the G planes next to every slab boundary are
-// exchanged into the halos, then U_f = G U G^+ and A_f = G A G^+ on every
-// plane of every slab -- a slab's halo planes get the values its neighbours
-// compute for them, so the start equals the undecomposed one bit for bit)
-int slab_landau_gauge(lce_slabs* S, double* theta, int* iters, int max_iters, int start = -1) {
+// One batch of Fourier-accelerated iterations on the slabs (the stages of
+// launch_fa_slab_stage): (a) every slab: Delta and the x transforms of its
+// interior lines into the whole lattice's buffer on the first slab's
+// device, theta summed per slab and copied there; (b) the first slab: the
+// check (theta of the whole lattice, iteration count, done flag, step) and
+// the y and z transforms; (c) every slab: the chain state from the first,
+// the inverse x transforms and g at its interior sites; (d) g of the plane
+// above each slab into its upper halo; (e) every slab: g applied at its
+// interior sites (links, A_f, G); (f) the U_z links of the plane below each
+// slab into its lower halo.  Slabs write and read only the lines of their own
+// planes in the buffer; the transforms of (b) run between the two.
+template <typename R>
+int slab_fa_iterations(lce_slabs* S, int batch) {
   const int n = (int)S->slab.size(), nz = S->nz;
   lce_ctx* c0 = S->slab[0];
-  const int cap = max_iters > 0 ? max_iters : 1000000;
+  const int Lg[3] = {S->L[0], S->L[1], S->L[2]};
+  const double nh_all = (double)S->nxy * S->L[2];
+  const size_t off = offsetof(ChainState, gf_theta), len = sizeof(ChainState) - off;
+  for (int it = 0; it < batch; ++it) {
+    for (int k = 0; k < n; ++k) {
+      lce_ctx* c = S->slab[k];
+      DeviceScope ds_(c->device);
+      const int nb = launch_fa_slab_stage<R>(0, c->ch_d, c->ch[0], c->cst_d, S->fft_d, c->fa_d, fa_vcap(c),
+                                             c->scratch_d, Lg, 1, nz, k * nz, c->s_lo, c->stream);
+      const std::string fe = fa_take_error();
+      if (!fe.empty()) return slabs_fail(LCE_ERR_CUDA, "slabs Fourier fixing: " + fe);
+      launch_sum_partials(c->scratch_d, nb, 1, c->scratch_d + nb, c->stream);
+      SCK(cudaGetLastError());
+      if (c->device == c0->device)
+        SCK(cudaMemcpyAsync(S->g_d + k, c->scratch_d + nb, sizeof(double), cudaMemcpyDeviceToDevice, c->stream));
+      else
+        SCK(cudaMemcpyPeerAsync(S->g_d + k, c0->device, c->scratch_d + nb, c->device, sizeof(double), c->stream));
+      SCK(cudaEventRecord(S->ev_sum[k], c->stream));
+    }
+    {
+      DeviceScope ds_(c0->device);
+      for (int k = 1; k < n; ++k) SCK(cudaStreamWaitEvent(c0->stream, S->ev_sum[k], 0));
+      launch_gf_check_slabs(c0->ch_d, c0->cst_d, S->g_d, n, nh_all, c0->stream, 1);
+      launch_fa_slab_stage<R>(1, c0->ch_d, c0->ch[0], c0->cst_d, S->fft_d, c0->fa_d, fa_vcap(c0), nullptr, Lg, 1, nz,
+                              0, c0->s_lo, c0->stream);
+      const std::string fe = fa_take_error();
+      if (!fe.empty()) return slabs_fail(LCE_ERR_CUDA, "slabs Fourier fixing: " + fe);
+      SCK(cudaGetLastError());
+      SCK(cudaEventRecord(S->ev_chk, c0->stream));
+    }
+    for (int k = 0; k < n; ++k) {
+      lce_ctx* c = S->slab[k];
+      DeviceScope ds_(c->device);
+      if (k > 0) {
+        SCK(cudaStreamWaitEvent(c->stream, S->ev_chk, 0));
+        char* dst = (char*)c->cst_d + off;
+        const char* src = (const char*)c0->cst_d + off;
+        if (c->device == c0->device) SCK(cudaMemcpyAsync(dst, src, len, cudaMemcpyDeviceToDevice, c->stream));
+        else SCK(cudaMemcpyPeerAsync(dst, c->device, src, c0->device, len, c->stream));
+      }
+      launch_fa_slab_stage<R>(2, c->ch_d, c->ch[0], c->cst_d, S->fft_d, c->fa_d, fa_vcap(c), nullptr, Lg, 1, nz,
+                              k * nz, c->s_lo, c->stream);
+      const std::string fe = fa_take_error();
+      if (!fe.empty()) return slabs_fail(LCE_ERR_CUDA, "slabs Fourier fixing: " + fe);
+      SCK(cudaGetLastError());
+      SCK(cudaEventRecord(S->ev_pass[k], c->stream));
+    }
+    const PlaneCopy gcp[2] = {{+1, 1, nz + 1, 4, 0, false}, {+1, 1, nz + 1, 4, 1, false}};
+    if (int rc = slab_exchange(S, gcp, 2)) return rc;
+    for (int k = 0; k < n; ++k) {
+      lce_ctx* c = S->slab[k];
+      DeviceScope ds_(c->device);
+      launch_fa_slab_stage<R>(3, c->ch_d, c->ch[0], c->cst_d, S->fft_d, c->fa_d, fa_vcap(c), nullptr, Lg, 1, nz,
+                              k * nz, c->s_lo, c->stream);
+      SCK(cudaGetLastError());
+      SCK(cudaEventRecord(S->ev_pass[k], c->stream));
+    }
+    const PlaneCopy ucp[2] = {{-1, nz, 0, 2, 0, true}, {-1, nz, 0, 2, 1, true}};
+    if (int rc = slab_exchange(S, ucp, 2)) return rc;
+  }
+  return LCE_OK;
+}
+
+// The start of a gauge fixing on the slabs.  start < 0: the reference's
+// fixing from U (no transform kept); otherwise a tracked fixing (G
+// accumulated as in lce_landau_gauge_from) from G = 1 (LCE_GF_START_IDENTITY)
+// or from the transform the slabs hold (LCE_GF_START_TRANSFORM: the G planes
+// next to every slab boundary are exchanged into the halos, then U_f = G U
+// G^+ and A_f = G A G^+ on every plane of every slab -- a slab's halo planes
+// get the values its neighbours compute for them, so the start equals the
+// undecomposed one bit for bit)
+int slab_gf_start(lce_slabs* S, int start) {
+  const int n = (int)S->slab.size(), nz = S->nz;
   if (start == LCE_GF_START_TRANSFORM) {
     for (int k = 0; k < n; ++k) {
       lce_ctx* c = S->slab[k];
@@ -1281,6 +1364,15 @@ int slab_landau_gauge(lce_slabs* S, double* theta, int* iters, int max_iters, in
         SCK(cudaGetLastError());
       }
     }
+  }
+  return LCE_OK;
+}
+
+// every slab's chain state for a fixing: not done, no iterations, the cap;
+// limit and step: the Fourier iteration's stopping theta and step (< 0: kept)
+int slab_gf_state(lce_slabs* S, int cap, double limit = -1.0, double step = -1.0) {
+  for (lce_ctx* c : S->slab) {
+    DeviceScope ds_(c->device);
     ChainState cs;
     SCK(cudaMemcpyAsync(&cs, c->cst_d, sizeof(cs), cudaMemcpyDeviceToHost, c->stream));
     SCK(cudaStreamSynchronize(c->stream));
@@ -1288,16 +1380,27 @@ int slab_landau_gauge(lce_slabs* S, double* theta, int* iters, int max_iters, in
     cs.gf_iters = 0;
     cs.gf_cap = cap;
     cs.gf_theta = 1.0e4;
+    if (limit >= 0.0) cs.gf_limit = limit;
+    if (step >= 0.0) cs.gf_step = step;
     SCK(cudaMemcpyAsync(c->cst_d, &cs, sizeof(cs), cudaMemcpyHostToDevice, c->stream));
     SCK(cudaStreamSynchronize(c->stream));
   }
-  ChainState cs;
+  return LCE_OK;
+}
+
+// batches of iterations (overrelaxed, or Fourier-accelerated with fourier)
+// until the first slab's chain state says done; its final state in cs
+int slab_gf_run(lce_slabs* S, int track, bool fourier, ChainState& cs) {
+  lce_ctx* c0 = S->slab[0];
   std::memset(&cs, 0, sizeof(cs));
-  int batch = 8;
+  int batch = fourier ? 4 : 8;
   while (true) {
-    const int track = start >= 0 ? 1 : 0;
-    const int rc = S->prec == LCE_PREC_F64 ? slab_gf_iterations<double>(S, batch, track)
-                                           : slab_gf_iterations<float>(S, batch, track);
+    int rc;
+    if (fourier)
+      rc = S->prec == LCE_PREC_F64 ? slab_fa_iterations<double>(S, batch) : slab_fa_iterations<float>(S, batch);
+    else
+      rc = S->prec == LCE_PREC_F64 ? slab_gf_iterations<double>(S, batch, track)
+                                   : slab_gf_iterations<float>(S, batch, track);
     if (rc) return rc;
     const int before = cs.gf_iters;
     {
@@ -1309,16 +1412,74 @@ int slab_landau_gauge(lce_slabs* S, double* theta, int* iters, int max_iters, in
     if (cs.gf_iters <= before) return slabs_fail(LCE_ERR_CUDA, "slabs gauge fixing: a batch made no progress");
     if (batch < 64) batch *= 2;
   }
-  for (int k = 0; k < n; ++k) {
-    lce_ctx* c = S->slab[k];
+  for (lce_ctx* c : S->slab) {
     DeviceScope ds_(c->device);
     SCK(cudaStreamSynchronize(c->stream));
   }
+  return LCE_OK;
+}
+
+int slab_landau_gauge(lce_slabs* S, double* theta, int* iters, int max_iters, int start = -1) {
+  lce_ctx* c0 = S->slab[0];
+  const int cap = max_iters > 0 ? max_iters : 1000000;
+  if (int rc = slab_gf_start(S, start)) return rc;
+  if (int rc = slab_gf_state(S, cap)) return rc;
+  ChainState cs;
+  if (int rc = slab_gf_run(S, start >= 0 ? 1 : 0, false, cs)) return rc;
   if (theta) *theta = cs.gf_theta;
   if (iters) *iters = cs.gf_iters;
   if (!std::isfinite(cs.gf_theta)) return slabs_fail(LCE_ERR_NAN, "slabs gauge fixing: theta is not finite");
   if (cs.gf_theta > c0->ch[0].limit_or)
     return slabs_fail(LCE_ERR_GF_NOT_CONVERGED, "slabs gauge fixing: iteration cap reached");
+  return LCE_OK;
+}
+
+// lce_landau_gauge_fourier on the slabs: Fourier-accelerated iterations to
+// theta_switch, then the overrelaxed iteration to limit_or, tracking G
+int slab_fourier_fix(lce_slabs* S, int start, double step, double theta_switch, double* theta, int* iters_f,
+                     int* iters_p, int max_iters) {
+  lce_ctx* c0 = S->slab[0];
+  const double limit = c0->ch[0].limit_or;
+  if (!(step > 0.0)) step = 1.0;
+  if (!(theta_switch > 0.0)) theta_switch = limit;
+  for (int d = 0; d < 3; ++d) {
+    int lg = 0;
+    while ((1 << lg) < S->L[d]) ++lg;
+    if ((1 << lg) != S->L[d] || lg < 1 || S->L[d] > 1024)
+      return slabs_fail(LCE_ERR_UNSUPPORTED, "slabs Fourier fixing: extents must be powers of two up to 1024");
+  }
+  for (lce_ctx* c : S->slab) {
+    DeviceScope ds_(c->device);
+    if (int rc = fa_buffers(c)) return slab_rc(c, rc);
+  }
+  if (!S->fft_d) {
+    DeviceScope ds_(c0->device);
+    const size_t V = (size_t)S->L[0] * S->L[1] * S->L[2];
+    if (cudaMalloc(&S->fft_d, 2 * V * 2 * sizeof(float)) != cudaSuccess) {
+      S->fft_d = nullptr;
+      cudaGetLastError();
+      return slabs_fail(LCE_ERR_NOMEM, "slabs Fourier fixing: the whole lattice's transform buffer");
+    }
+  }
+  const int cap = max_iters > 0 ? max_iters : 1000000;
+  if (int rc = slab_gf_start(S, start)) return rc;
+  if (int rc = slab_gf_state(S, cap, theta_switch, step)) return rc;
+  ChainState cs;
+  if (int rc = slab_gf_run(S, 1, true, cs)) return rc;
+  if (iters_f) *iters_f = cs.gf_iters;
+  if (iters_p) *iters_p = 0;
+  if (theta) *theta = cs.gf_theta;
+  if (!std::isfinite(cs.gf_theta)) return slabs_fail(LCE_ERR_NAN, "slabs Fourier fixing: theta is not finite");
+  if (cs.gf_theta <= limit) return LCE_OK;
+  const int it_fa = cs.gf_iters;
+  if (it_fa >= cap) return slabs_fail(LCE_ERR_GF_NOT_CONVERGED, "slabs Fourier fixing: iteration cap reached");
+  // the overrelaxed iteration from theta_switch to limit_or
+  if (int rc = slab_gf_state(S, cap - it_fa)) return rc;
+  if (int rc = slab_gf_run(S, 1, false, cs)) return rc;
+  if (iters_p) *iters_p = cs.gf_iters;
+  if (theta) *theta = cs.gf_theta;
+  if (!std::isfinite(cs.gf_theta)) return slabs_fail(LCE_ERR_NAN, "slabs gauge fixing: theta is not finite");
+  if (cs.gf_theta > limit) return slabs_fail(LCE_ERR_GF_NOT_CONVERGED, "slabs gauge fixing: iteration cap reached");
   return LCE_OK;
 }
 
@@ -2474,6 +2635,7 @@ void lce_slabs_destroy(lce_slabs* h) {
   if (!S->slab.empty()) {
     DeviceScope ds_(S->slab[0]->device);
     if (S->g_d) cudaFree(S->g_d);
+    if (S->fft_d) cudaFree(S->fft_d);
     if (S->ev_chk) cudaEventDestroy(S->ev_chk);
   }
   for (size_t k = 0; k < S->slab.size(); ++k) {
@@ -2541,6 +2703,15 @@ int lce_slabs_landau_gauge(lce_slabs* h, double* theta, int* iters, int max_iter
   lce_slabs* S = h;
   if (!S) return LCE_ERR_INVALID;
   return slab_landau_gauge(S, theta, iters, max_iters);
+}
+
+int lce_slabs_landau_gauge_fourier(lce_slabs* h, int start, double step, double theta_switch, double* theta,
+                                   int* iters_fourier, int* iters_plain, int max_iters) {
+  lce_slabs* S = h;
+  if (!S) return LCE_ERR_INVALID;
+  if (start != LCE_GF_START_IDENTITY && start != LCE_GF_START_TRANSFORM)
+    return slabs_fail(LCE_ERR_INVALID, "slabs_landau_gauge_fourier: start must be IDENTITY or TRANSFORM");
+  return slab_fourier_fix(S, start, step, theta_switch, theta, iters_fourier, iters_plain, max_iters);
 }
 
 int lce_slabs_landau_gauge_from(lce_slabs* h, int start, double* theta, int* iters, int max_iters) {

@@ -58,6 +58,7 @@
 // reduction and g = exp(alpha X) per site.  The step is bounded by a trust
 // region (fa_alpha_kernel).
 #include <algorithm>
+#include <cstring>
 
 #include <string>
 
@@ -270,8 +271,13 @@ struct FaArgs {
   float* sdir;            // CG: direction s, [component][parity][site]
   double* cgpart;         // CG: per-block pairs of sums
   FaCg* cg;               // CG: state
-  int L[3], logL[3];
+  int L[3], logL[3];      // the transformed (whole) lattice
   int track;
+  // the planes the per-site kernels visit (a z-slab: its interior planes).
+  // zl0: first visited local plane, nzl: their number, zg0: the whole
+  // lattice's z of plane zl0, s_lo: first visited site of each parity.
+  // A whole lattice: 0, L3, 0, 0.
+  int zl0, nzl, zg0, s_lo;
 };
 
 __device__ __forceinline__ bool fa_done(const FaArgs& a) { return a.cst && a.cst->gf_done; }
@@ -298,7 +304,7 @@ __global__ void __launch_bounds__(kFaThreads) fa_div_kernel(FaArgs a) {
   FftC* tw = d + G::NLT * ld;
   if (fa_done(a)) return;
   const ChainDev& ch = *a.ch;
-  const int nlines = a.L[1] * a.L[2];
+  const int nlines = a.L[1] * a.nzl;
   const int l0 = blockIdx.x * NL;
   load_twiddles(tw, a.tw, n, -1);
   const double al = ch.alpha;
@@ -307,7 +313,9 @@ __global__ void __launch_bounds__(kFaThreads) fa_div_kernel(FaArgs a) {
     const int j = e >> LOGN, x = e & (n - 1), l = l0 + j;
     FftC v0{0, 0}, v1{0, 0};
     if (l < nlines) {
-      const int y = l & (a.L[1] - 1), z = l >> a.logL[1];
+      // z: the local plane (field arrays), zg: the whole lattice's (theta's
+      // odd sites)
+      const int y = l & (a.L[1] - 1), zi = l >> a.logL[1], z = zi + a.zl0, zg = zi + a.zg0;
       const int p = (x + y + z) & 1, op = 1 - p;
       const int s = site_index(x, y, z, ch.hx, ch.nxy);
       const int xm[3] = {site_index(wrap(x - 1, ch.L1), y, z, ch.hx, ch.nxy),
@@ -323,7 +331,7 @@ __global__ void __launch_bounds__(kFaThreads) fa_div_kernel(FaArgs a) {
         dbr += c * ((double)u.b.re - (double)w.b.re);
         dbi += c * ((double)u.b.im - (double)w.b.im);
       }
-      if (p == 1) q[0] += d3 * d3 + dbr * dbr + dbi * dbi;
+      if (((x + y + zg) & 1) == 1) q[0] += d3 * d3 + dbr * dbr + dbi * dbi;
       v0 = FftC{(FftR)dbr, (FftR)dbi};
       v1 = FftC{(FftR)d3, (FftR)0};
     }
@@ -335,10 +343,11 @@ __global__ void __launch_bounds__(kFaThreads) fa_div_kernel(FaArgs a) {
   fft2_lines<LOGN>(d, tw);
   const size_t V = (size_t)a.L[0] * a.L[1] * a.L[2];
   FftC* F = reinterpret_cast<FftC*>(a.fft);
+  const int lg0 = a.zg0 * a.L[1];  // the whole lattice's line of local line 0
   for (int e = threadIdx.x; e < NL * n; e += blockDim.x) {
     const int j = e >> LOGN, k = e & (n - 1), l = l0 + j;
     if (l >= nlines) continue;
-    const size_t gi = nat_index<0>(a, l, k);
+    const size_t gi = nat_index<0>(a, lg0 + l, k);
     F[gi] = d[j * ld + k];
     F[V + gi] = d[(NL + j) * ld + k];
   }
@@ -458,14 +467,15 @@ __global__ void __launch_bounds__(kFaThreads) fa_g_kernel(FaArgs a) {
   FftC* tw = d + G::NLT * ld;
   if (fa_done(a)) return;
   const ChainDev& ch = *a.ch;
-  const int nlines = a.L[1] * a.L[2];
+  const int nlines = a.L[1] * a.nzl;
   const int l0 = blockIdx.x * NL;
   const size_t V = (size_t)a.L[0] * a.L[1] * a.L[2];
   const FftC* F = reinterpret_cast<const FftC*>(a.fft);
+  const int lg0 = a.zg0 * a.L[1];
   load_twiddles(tw, a.tw, n, +1);
   for (int e = threadIdx.x; e < NL * n; e += blockDim.x) {
     const int j = e >> LOGN, k = e & (n - 1), l = l0 + j;
-    const size_t gi = l < nlines ? nat_index<0>(a, l, k) : 0;
+    const size_t gi = l < nlines ? nat_index<0>(a, lg0 + l, k) : 0;
     d[j * ld + k] = l < nlines ? F[gi] : FftC{0, 0};
     d[(NL + j) * ld + k] = l < nlines ? F[V + gi] : FftC{0, 0};
   }
@@ -474,7 +484,7 @@ __global__ void __launch_bounds__(kFaThreads) fa_g_kernel(FaArgs a) {
   for (int e = threadIdx.x; e < NL * n; e += blockDim.x) {
     const int j = e >> LOGN, x = e & (n - 1), l = l0 + j;
     if (l >= nlines) continue;
-    const int y = l & (a.L[1] - 1), z = l >> a.logL[1];
+    const int y = l & (a.L[1] - 1), z = (l >> a.logL[1]) + a.zl0;
     const int p = (x + y + z) & 1, s = site_index(x, y, z, ch.hx, ch.nxy);
     const double w3 = d[(NL + j) * ld + x].x, wbr = d[j * ld + x].x, wbi = d[j * ld + x].y;
     if (CG) {
@@ -541,8 +551,9 @@ __global__ void __launch_bounds__(kBlock) fa_apply_kernel(FaArgs a) {
   if (fa_done(a)) return;
   const ChainDev& ch = *a.ch;
   const int i = blockIdx.x * kBlock + threadIdx.x;
-  if (i >= 2 * ch.nh) return;
-  const int eo = i >= ch.nh ? 1 : 0, oe = 1 - eo, s = i - eo * ch.nh, nh = ch.nh;
+  const int nvis = ch.nh - 2 * a.s_lo;  // visited sites per parity
+  if (i >= 2 * nvis) return;
+  const int eo = i >= nvis ? 1 : 0, oe = 1 - eo, s = a.s_lo + i - eo * nvis, nh = ch.nh;
   const Coord X = site_coord(eo, s, ch.hx, ch.nxy, ch.dhx, ch.dnxy);
   const su2<double> gx = LinkIO<double>::ld_cg(a.gstep, (size_t)eo * nh + s);
   const int L[3] = {ch.L1, ch.L2, ch.L3};
@@ -697,6 +708,7 @@ size_t fa_off_cgpart(size_t vcap) { return (fa_off_sdir(vcap) + 3 * vcap * sizeo
 size_t fa_cgpart_n(size_t vcap) { return 3 * (vcap / 128 + 64); }  // doubles: triples for >= V/256 + 64 blocks
 }  // namespace
 size_t fa_buffer_bytes(size_t vcap) { return fa_off_cgpart(vcap) + fa_cgpart_n(vcap) * sizeof(double) + 256; }
+void* fa_gstep_ptr(void* buf, size_t vcap) { return reinterpret_cast<char*>(buf) + 2 * vcap * sizeof(FftC); }
 namespace {
 char* fa_at(void* buf, size_t off) { return reinterpret_cast<char*>(buf) + off; }
 void* fa_gstep(void* buf, size_t vcap) { return fa_at(buf, 2 * vcap * sizeof(FftC)); }
@@ -814,6 +826,10 @@ void launch_fa_iteration(const ChainDev* chd, const ChainDev& ch, ChainState* cs
   a.L[2] = ch.L3;
   for (int d = 0; d < 3; ++d) a.logL[d] = ilog2_exact(a.L[d]);
   a.track = track;
+  a.zl0 = 0;
+  a.nzl = ch.L3;
+  a.zg0 = 0;
+  a.s_lo = 0;
   a.cg = reinterpret_cast<FaCg*>(fa_at(buf, fa_off_cg(vcap)));
   a.prev = fa_at(buf, fa_off_prev(vcap));
   a.sdir = reinterpret_cast<float*>(fa_at(buf, fa_off_sdir(vcap)));
@@ -855,6 +871,79 @@ void launch_fa_iteration(const ChainDev* chd, const ChainDev& ch, ChainState* cs
   }
   if (with_apply) fa_apply_kernel<R><<<nbv, kBlock, 0, s>>>(a);
 }
+
+// One stage of a Fourier-accelerated iteration on a z-slab decomposed
+// lattice.  Each slab holds its own step transform and twiddle table (buf);
+// the whole lattice's two transformed fields are one buffer (fft) on the
+// first slab's device.  stage 0: Delta and the x transforms of the slab's
+// interior x-lines into fft, theta partials into part (returns their
+// number); stage 1: the y and z transforms of the whole of fft (on its
+// device; ch, cst: the first slab's); stage 2: the inverse x transforms of the
+// slab's lines and g at its interior sites; stage 3: g applied at its
+// interior sites, the transform G tracked.
+template <typename R>
+int launch_fa_slab_stage(int stage, const ChainDev* chd, const ChainDev& ch, ChainState* cst, void* fft, void* buf,
+                         size_t vcap, double* part, const int Lg[3], int zl0, int nzl, int zg0, int s_lo,
+                         cudaStream_t s) {
+  FaArgs a;
+  std::memset(&a, 0, sizeof(a));
+  a.ch = chd;
+  a.cst = cst;
+  a.gamma = 1.0;
+  a.fft = fft;
+  a.gstep = fa_gstep(buf, vcap);
+  a.part = part;
+  a.omega_out = nullptr;
+  a.tw = fa_table(buf, vcap);
+  for (int d = 0; d < 3; ++d) {
+    a.L[d] = Lg[d];
+    a.logL[d] = ilog2_exact(Lg[d]);
+  }
+  a.track = 1;
+  a.zl0 = zl0;
+  a.nzl = nzl;
+  a.zg0 = zg0;
+  a.s_lo = s_lo;
+  a.cg = reinterpret_cast<FaCg*>(fa_at(buf, fa_off_cg(vcap)));
+  a.prev = fa_at(buf, fa_off_prev(vcap));
+  a.sdir = reinterpret_cast<float*>(fa_at(buf, fa_off_sdir(vcap)));
+  a.cgpart = reinterpret_cast<double*>(fa_at(buf, fa_off_cgpart(vcap)));
+  const size_t V = (size_t)Lg[0] * Lg[1] * Lg[2];
+  const int nbd = fa_blocks((long)Lg[1] * nzl, a.logL[0], 2);
+  if (stage == 0) {
+#define LCE_FA_DIV(L) fa_div_launch<R, L>(a, nbd, s)
+    LCE_FA_SWITCH(a.logL[0], LCE_FA_DIV)
+#undef LCE_FA_DIV
+    return nbd;
+  }
+  if (stage == 1) {
+    const int nby = fa_blocks((long)V / Lg[1], a.logL[1], 1), nbz = fa_blocks((long)V / Lg[2], a.logL[2], 1);
+#define LCE_FA_Y(L) fa_fft_launch<1, -1, false, L>(a, nby, s)
+    LCE_FA_SWITCH(a.logL[1], LCE_FA_Y)
+#undef LCE_FA_Y
+#define LCE_FA_Z(L) fa_fft_launch<2, -1, true, L>(a, nbz, s)
+    LCE_FA_SWITCH(a.logL[2], LCE_FA_Z)
+#undef LCE_FA_Z
+#define LCE_FA_YI(L) fa_fft_launch<1, +1, false, L>(a, nby, s)
+    LCE_FA_SWITCH(a.logL[1], LCE_FA_YI)
+#undef LCE_FA_YI
+    return 0;
+  }
+  if (stage == 2) {
+#define LCE_FA_G(L) fa_g_launch<R, L>(a, nbd, s)
+    LCE_FA_SWITCH(a.logL[0], LCE_FA_G)
+#undef LCE_FA_G
+    return 0;
+  }
+  const int nbv = ceil_div(2L * (ch.nh - 2 * s_lo), kBlock);
+  fa_apply_kernel<R><<<nbv, kBlock, 0, s>>>(a);
+  return 0;
+}
+
+template int launch_fa_slab_stage<float>(int, const ChainDev*, const ChainDev&, ChainState*, void*, void*, size_t,
+                                         double*, const int*, int, int, int, int, cudaStream_t);
+template int launch_fa_slab_stage<double>(int, const ChainDev*, const ChainDev&, ChainState*, void*, void*, size_t,
+                                          double*, const int*, int, int, int, int, cudaStream_t);
 
 template void launch_fa_iteration<float>(const ChainDev*, const ChainDev&, ChainState*, double, void*, size_t,
                                          double*, double*, int, bool, bool, bool, cudaStream_t);

@@ -291,16 +291,21 @@ __global__ void __launch_bounds__(1024) gf_check_kernel(const ChainDev* chp, Cha
 // the same test for a lattice split into z-slabs: the slabs' theta sums (in
 // slab order) over the whole lattice's nh odd sites, counted into slab 0's
 // chain state, which the host copies to the other slabs
+// fa: the Fourier-accelerated iteration's check (stop at gf_limit, shorten
+// the step after an overshoot, as fa_check_kernel); else the overrelaxed
+// iteration's (stop at limit_or)
 __global__ void gf_check_slabs_kernel(const ChainDev* chp, ChainState* cst, const double* sums, int nslabs,
-                                      double nh) {
+                                      double nh, int fa) {
   if (cst->gf_done) return;
   double tot = 0.0;
   for (int j = 0; j < nslabs; ++j) tot += sums[j];
   const double theta = tot / nh;
   const int it = cst->gf_iters + 1;
+  if (fa && it > 1 && theta > 2.0 * cst->gf_theta) cst->gf_step = fmax(0.1, 0.7 * cst->gf_step);
   cst->gf_iters = it;
   cst->gf_theta = theta;
-  if (!(theta > chp->limit_or) || (cst->gf_cap > 0 && it >= cst->gf_cap)) cst->gf_done = 1;
+  const double limit = fa ? cst->gf_limit : chp->limit_or;
+  if (!(theta > limit) || (cst->gf_cap > 0 && it >= cst->gf_cap)) cst->gf_done = 1;
 }
 
 // theta of the current U_f without updating (odd sites)
@@ -357,8 +362,8 @@ int launch_gf_half(const ChainDev* ch, ChainState* cst, int eo, int last, double
 }
 
 void launch_gf_check_slabs(const ChainDev* ch, ChainState* cst, const double* sums, int nslabs, double nh,
-                           cudaStream_t s) {
-  gf_check_slabs_kernel<<<1, 1, 0, s>>>(ch, cst, sums, nslabs, nh);
+                           cudaStream_t s, int fa) {
+  gf_check_slabs_kernel<<<1, 1, 0, s>>>(ch, cst, sums, nslabs, nh, fa);
 }
 
 template <typename R>

@@ -213,7 +213,7 @@ int launch_gf_half(const ChainDev* ch, ChainState* cst, int eo, int last, double
                    cudaStream_t s);
 // convergence test of a z-slab decomposed fixing from the slabs' theta sums
 void launch_gf_check_slabs(const ChainDev* ch, ChainState* cst, const double* sums, int nslabs, double nh,
-                           cudaStream_t s);
+                           cudaStream_t s, int fa = 0);
 // one iteration of f/it_gauge_fixing.f (flags LCE_ITGF_*, step from cst->gf_step),
 // then the convergence check of the overrelaxed form
 template <typename R>
@@ -238,6 +238,17 @@ void launch_fa_iteration(const ChainDev* chd, const ChainDev& ch, ChainState* cs
                          bool cg, cudaStream_t s);
 // the conjugate-gradient form starts its next iteration from the gradient
 void fa_cg_reset(void* buf, size_t vcap, cudaStream_t s);
+// one stage of an iteration on a z-slab (lce_fourier.cu: 0 Delta and the x
+// transforms into the whole lattice's buffer fft, returns the number of theta
+// partials; 1 the y and z transforms of fft; 2 the inverse x transforms and
+// g; 3 g applied); Lg: the whole lattice; zl0, nzl, zg0, s_lo: the slab's
+// visited planes and sites
+template <typename R>
+int launch_fa_slab_stage(int stage, const ChainDev* chd, const ChainDev& ch, ChainState* cst, void* fft, void* buf,
+                         size_t vcap, double* part, const int Lg[3], int zl0, int nzl, int zg0, int s_lo,
+                         cudaStream_t s);
+// the step transform g of a buffer ([parity][site], FP64 first rows)
+void* fa_gstep_ptr(void* buf, size_t vcap);
 // the first launch set-up failure of this host thread's Fourier kernels
 // since the last call (kernel, line length, shared memory), or ""
 std::string fa_take_error();

@@ -149,6 +149,37 @@ def test_slabs_tracked_fixing_and_warm_start(precision, limit_or, L, nslabs):
     s.close()
 
 
+@pytest.mark.parametrize("precision,limit_or,switch", [("f64", 1e-10, 0.0), ("f32", 1e-6, 0.0),
+                                                       ("f64", 1e-10, 1e-4)])
+@pytest.mark.parametrize("L,nslabs", [((8, 8, 8), 2), ((8, 4, 16), 4), ((16, 8, 8), 2)])
+def test_slabs_fourier_fixing_reproduces_the_whole_lattice(precision, limit_or, switch, L, nslabs):
+    """The Fourier-accelerated fixing on the slabs (the per-site stages on
+    every slab, the y/z transforms of the whole lattice's buffer on the first
+    slab's device): from G = 1, then after three sweeps from the previous
+    transform; with a switch theta the plain iteration finishes.  The
+    undecomposed run's iteration counts and u_f, a_f bit for bit."""
+    g, s, dt = _thermalised_pair(L, nslabs, precision, limit_or)
+    for start in ("identity", "transform"):
+        tg, fg, pg = g.landau_gauge_fourier(start, theta_switch=switch)
+        ts, fs, ps = s.landau_gauge_fourier(start, theta_switch=switch)
+        assert (fs, ps) == (fg, pg) and fg > 2
+        assert (pg > 0) == (switch > 0)
+        assert tg <= limit_or and abs(ts - tg) <= 1e-9 * tg
+        for x, y in zip(s.download(dtype=dt, fixed=True), _fixed(g, dt)):
+            np.testing.assert_array_equal(x, y)
+        for _ in range(3):
+            g.sweep(0)
+            s.sweep(0)
+    s.close()
+
+
+def test_slabs_fourier_fixing_needs_powers_of_two():
+    s = SlabLattice((12, 8, 8), 2, precision="f64")
+    with pytest.raises(LceError):
+        s.landau_gauge_fourier()
+    s.close()
+
+
 def test_slabs_landau_gauge_cap():
     """An iteration cap stops both runs at the same iteration with the
     reference's not-converged status and the same partly fixed u_f."""
