@@ -812,7 +812,7 @@ def main():
                     help="sweep form (default: the library's autotuner chooses)")
     ap.add_argument("--tile-registers", type=int, default=0, choices=[0, 56],
                     help="register cap of the update kernels (56 needs --tile-threads 128)")
-    ap.add_argument("--tile-threads", type=int, default=0, choices=[0, 128, 256, 512],
+    ap.add_argument("--tile-threads", type=int, default=0, choices=[0, 128, 256, 448, 512],
                     help="threads per block of the update kernels (default 0: the autotuner chooses with "
                          "--sweep-mode auto, else 256)")
     ap.add_argument("--pass-profile", type=int, default=0, metavar="REPS",

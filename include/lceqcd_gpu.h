@@ -114,7 +114,8 @@ typedef struct lce_params {
                             one of the two files at build time */
   int tile_threads;      /* threads per block of the per-pass update kernels:
                             0 (default) = tuned with LCE_SWEEP_AUTO, else 256;
-                            or 128, 256, 512.  FP32 only: the FP64 validation
+                            or 128, 256, 448, 512 (448: one site per thread
+                            only).  FP32 only: the FP64 validation
                             path and z-slabs use 256.  Results do not depend on
                             it (per-site work and random numbers are the same;
                             FP64 sums are grouped per tile). */
@@ -420,6 +421,10 @@ int lce_slabs_landau_gauge_from(lce_slabs* s, int start, double* theta, int* ite
  * undecomposed.  Extents: powers of two up to 1024. */
 int lce_slabs_landau_gauge_fourier(lce_slabs* s, int start, double step, double theta_switch, double* theta,
                                    int* iters_fourier, int* iters_plain, int max_iters);
+/* lce_it_landau_gauge (f/it_gauge_fixing.f under f/landau_gauge.f) on the
+ * slabs: the same halo traffic as lce_slabs_landau_gauge; same iterations
+ * and u_f, a_f as undecomposed */
+int lce_slabs_it_landau_gauge(lce_slabs* s, double step, int flags, double* da1, int* iters, int max_iters);
 /* lce_correlator / lce_polyakov / lce_scalarcorr of the whole lattice
  * (f/correlator.f, f/polyakov.f, f/scalarcorr.f): slice sums per slab,
  * correlated on the first slab's device */

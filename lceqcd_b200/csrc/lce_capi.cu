@@ -58,19 +58,19 @@ struct lce_ctx {
   int agauge_hits = 1;  // 1: f/agauge.f, 3: f/agauge1.f in lce_sweep
   std::vector<lce_params> params;
   std::vector<ChainDev> ch;
-  // prefix over chains of the tiles of one pass, for tiles of 128, 256 and
-  // 512 sites (tile = threads per block x sites per thread); tiles of kBlock
-  // sites (blk) serve the persistent form and size the partial-sum slots
-  std::vector<int> tiles[3];
+  // prefix over chains of the tiles of one pass, for tiles of 128, 256, 512
+  // and 448 sites (kTileSites; tile = threads per block x sites per thread);
+  // tiles of kBlock sites (blk) serve the persistent form
+  std::vector<int> tiles[kTileTables];
   std::vector<int>& blk = tiles[1];
   int max_nh = 0, max_L3 = 0;
   ChainDev* ch_d = nullptr;
-  int* tiles_d[3] = {nullptr, nullptr, nullptr};
+  int* tiles_d[kTileTables] = {nullptr, nullptr, nullptr, nullptr};
   int* blk_d = nullptr;   // = tiles_d[1]
   // finalize reduction: per tile table, the prefix over chains of chunks of
   // kChunkTiles tiles, and the chunk sums [chunk][kMaxSlots][kNQ]
-  std::vector<int> chunks[3];
-  int* chunks_begin_d[3] = {nullptr, nullptr, nullptr};
+  std::vector<int> chunks[kTileTables];
+  int* chunks_begin_d[kTileTables] = {nullptr, nullptr, nullptr, nullptr};
   double* chunks_d = nullptr;
   CtxState* st_d = nullptr;
   ChainState* cst_d = nullptr;
@@ -194,8 +194,9 @@ bool valid_params(const lce_params& p, std::string& why) {
           "LCE_SWEEP_DIRECT";
     return false;
   }
-  if (p.tile_threads != 0 && p.tile_threads != 128 && p.tile_threads != 256 && p.tile_threads != 512) {
-    why = "tile_threads must be 0 (tuned), 128, 256 or 512";
+  if (p.tile_threads != 0 && p.tile_threads != 128 && p.tile_threads != 256 && p.tile_threads != 448 &&
+      p.tile_threads != 512) {
+    why = "tile_threads must be 0 (tuned), 128, 256, 448 or 512";
     return false;
   }
   if (p.tile_registers != 0 && !(p.tile_registers == 56 && p.tile_threads == 128 && p.precision == LCE_PREC_F32)) {
@@ -281,7 +282,10 @@ struct Enq {
 };
 
 // index of the chain table for tiles of bs * spt sites (128, 256 or 512)
-int tile_index(int bs, int spt) { return bs * spt == 128 ? 0 : (bs * spt == 256 ? 1 : 2); }
+int tile_index(int bs, int spt) {
+  const int t = bs * spt;
+  return t == 128 ? 0 : (t == 256 ? 1 : (t == 512 ? 2 : 3));
+}
 
 void enq_begin(lce_ctx* c, const std::vector<unsigned char>& routines, int measflag, bool fuse_renorm, int bs,
                int spt, int occ, Enq& q) {
@@ -717,7 +721,7 @@ lce_ctx* create_impl(const lce_params* p, int n, const SlabInfo* slab = nullptr)
     off += 2 * (align256((size_t)6 * d.nh * lb) + align256((size_t)6 * d.nh * rb)) + align256((size_t)2 * d.nh * lb);
     c->ch.push_back(d);
     const int nvis = slab ? d.nh - 2 * d.nxy : d.nh;  // sites a pass visits per parity
-    for (int t = 0; t < 3; ++t) c->tiles[t].push_back(c->tiles[t].back() + ceil_div(nvis, 128 << t));
+    for (int t = 0; t < kTileTables; ++t) c->tiles[t].push_back(c->tiles[t].back() + ceil_div(nvis, kTileSites[t]));
     c->max_nh = std::max(c->max_nh, d.nh);
     c->max_L3 = std::max(c->max_L3, d.L3);
   }
@@ -736,7 +740,7 @@ lce_ctx* create_impl(const lce_params* p, int n, const SlabInfo* slab = nullptr)
   if ((e = cudaMalloc(&c->ch_d, sizeof(ChainDev) * n)) != cudaSuccess) return bail(e, "cudaMalloc(chains)");
   if ((e = cudaMemcpy(c->ch_d, c->ch.data(), sizeof(ChainDev) * n, cudaMemcpyHostToDevice)) != cudaSuccess)
     return bail(e, "cudaMemcpy(chains)");
-  for (int t = 0; t < 3; ++t) {
+  for (int t = 0; t < kTileTables; ++t) {
     if ((e = cudaMalloc(&c->tiles_d[t], sizeof(int) * (n + 1))) != cudaSuccess) return bail(e, "cudaMalloc(tiles)");
     if ((e = cudaMemcpy(c->tiles_d[t], c->tiles[t].data(), sizeof(int) * (n + 1), cudaMemcpyHostToDevice)) !=
         cudaSuccess)
@@ -785,7 +789,7 @@ lce_ctx* create_impl(const lce_params* p, int n, const SlabInfo* slab = nullptr)
   c->tile_req = (c->prec == LCE_PREC_F32 && !slab) ? p[0].tile_threads : kBlock;
   c->tile_bs = c->tile_req ? c->tile_req : kBlock;
   c->tile_spt = c->mode == LCE_SWEEP_PASSES2 ? 2 : 1;
-  if (c->tile_spt == 2 && c->tile_bs == 512) c->tile_bs = kBlock;  // (512, 2) is not compiled
+  if (c->tile_spt == 2 && c->tile_bs > 256) c->tile_bs = kBlock;  // (448, 2), (512, 2) are not compiled
   const bool reg56 = !slab && p[0].tile_registers == 56;
   if (reg56) {
     c->tile_bs = 128;
@@ -793,7 +797,7 @@ lce_ctx* create_impl(const lce_params* p, int n, const SlabInfo* slab = nullptr)
     c->tile_occ = 1152;
   }
   if (c->mode == LCE_SWEEP_AUTO) {
-    const int bss[3] = {128, 256, 512};
+    const int bss[4] = {128, 256, 448, 512};
     for (int b : bss) {
       if (reg56) {
         c->tune.push_back(TuneForm{LCE_SWEEP_PASSES, 128, 1, 1152, {}});
@@ -802,7 +806,7 @@ lce_ctx* create_impl(const lce_params* p, int n, const SlabInfo* slab = nullptr)
       if (c->tile_req && b != c->tile_req) continue;
       if (c->prec == LCE_PREC_F64 && b != kBlock) continue;
       c->tune.push_back(TuneForm{LCE_SWEEP_PASSES, b, 1, 0, {}});
-      if (b != 512) c->tune.push_back(TuneForm{LCE_SWEEP_PASSES2, b, 2, 0, {}});
+      if (b <= 256) c->tune.push_back(TuneForm{LCE_SWEEP_PASSES2, b, 2, 0, {}});
     }
     // Not candidates, measured slower on the B200 at 64^3 and 128^3 (still
     // selectable): the 56-register 128-thread form (tile_registers = 56,
@@ -1198,8 +1202,10 @@ int slab_sweep(lce_slabs* S, int measflag, lce_meas* m) {
 // update) is summed per slab, combined on slab 0's device, and the count and
 // verdict copied to every slab's chain state, all ordered by events: no host
 // round trip inside a batch of iterations.
+// it_flags >= 0: the half-steps of f/it_gauge_fixing.f with these flags
+// (LCE_ITGF_*) instead of the overrelaxed ones
 template <typename R>
-int slab_gf_iterations(lce_slabs* S, int batch, int track) {
+int slab_gf_iterations(lce_slabs* S, int batch, int track, int it_flags = -1) {
   const int n = (int)S->slab.size(), nz = S->nz;
   lce_ctx* c0 = S->slab[0];
   const size_t off = offsetof(ChainState, gf_theta), len = offsetof(ChainState, gf_pad) - off;
@@ -1209,7 +1215,12 @@ int slab_gf_iterations(lce_slabs* S, int batch, int track) {
       for (int k = 0; k < n; ++k) {
         lce_ctx* c = S->slab[k];
         DeviceScope ds_(c->device);
-        launch_gf_half<R>(c->ch_d, c->cst_d, pg ^ c->eo_flip, pg, c->scratch_d, c->ch[0].nh, c->s_lo, track, c->stream);
+        if (it_flags >= 0)
+          launch_it_half<R>(c->ch_d, c->cst_d, pg ^ c->eo_flip, pg, c->scratch_d, c->ch[0].nh, c->s_lo, it_flags,
+                            c->stream);
+        else
+          launch_gf_half<R>(c->ch_d, c->cst_d, pg ^ c->eo_flip, pg, c->scratch_d, c->ch[0].nh, c->s_lo, track,
+                            c->stream);
         SCK(cudaGetLastError());
         SCK(cudaEventRecord(S->ev_pass[k], c->stream));
       }
@@ -1390,7 +1401,7 @@ int slab_gf_state(lce_slabs* S, int cap, double limit = -1.0, double step = -1.0
 
 // batches of iterations (overrelaxed, or Fourier-accelerated with fourier)
 // until the first slab's chain state says done; its final state in cs
-int slab_gf_run(lce_slabs* S, int track, bool fourier, ChainState& cs) {
+int slab_gf_run(lce_slabs* S, int track, bool fourier, ChainState& cs, int it_flags = -1) {
   lce_ctx* c0 = S->slab[0];
   std::memset(&cs, 0, sizeof(cs));
   int batch = fourier ? 4 : 8;
@@ -1399,8 +1410,8 @@ int slab_gf_run(lce_slabs* S, int track, bool fourier, ChainState& cs) {
     if (fourier)
       rc = S->prec == LCE_PREC_F64 ? slab_fa_iterations<double>(S, batch) : slab_fa_iterations<float>(S, batch);
     else
-      rc = S->prec == LCE_PREC_F64 ? slab_gf_iterations<double>(S, batch, track)
-                                   : slab_gf_iterations<float>(S, batch, track);
+      rc = S->prec == LCE_PREC_F64 ? slab_gf_iterations<double>(S, batch, track, it_flags)
+                                   : slab_gf_iterations<float>(S, batch, track, it_flags);
     if (rc) return rc;
     const int before = cs.gf_iters;
     {
@@ -1645,9 +1656,10 @@ void lce_destroy(lce_ctx* c) {
     if (kv.second) cudaGraphExecDestroy(kv.second);
   for (auto& kv : c->gf_exec) cudaGraphExecDestroy(kv.second);
   for (auto& kv : c->fa_exec) cudaGraphExecDestroy(kv.second);
-  void* ptrs[] = {c->ch_d, c->tiles_d[0], c->tiles_d[1], c->tiles_d[2], c->st_d, c->cst_d, c->meas_d, c->part_d, c->totals_d,
+  void* ptrs[] = {c->ch_d, c->tiles_d[0], c->tiles_d[1], c->tiles_d[2], c->tiles_d[3], c->st_d, c->cst_d, c->meas_d, c->part_d, c->totals_d,
                   c->scratch_d, c->fields_d, c->stream_d, c->staging_d, c->flush_d, c->bar_d,
                   c->gsave_d, c->fa_d, c->chunks_begin_d[0], c->chunks_begin_d[1], c->chunks_begin_d[2],
+                  c->chunks_begin_d[3],
                   c->chunks_d, c->async_d};
   for (void* q : ptrs)
     if (q) cudaFree(q);
@@ -1975,7 +1987,10 @@ int lce_get_tile_shape(lce_ctx* c, int* threads, int* sites_per_thread, int* reg
   if (threads) *threads = pers ? kBlock : c->tile_bs;
   if (sites_per_thread) *sites_per_thread = pers ? 1 : c->tile_spt;
   if (register_cap) {
-    const int occ = pers || !c->tile_occ ? (c->prec == LCE_PREC_F32 ? 4 : 3) * kBlock : c->tile_occ;
+    // resident threads per SM the cap is set for: min_blocks_bs of the kernels
+    const int bs = pers ? kBlock : c->tile_bs;
+    const int blocks = std::max(1, (c->prec == LCE_PREC_F32 ? 4 : 3) * kBlock / bs);
+    const int occ = pers || !c->tile_occ ? blocks * bs : c->tile_occ;
     *register_cap = std::min(255, (65536 / occ) & ~7);
   }
   return LCE_OK;
@@ -2703,6 +2718,23 @@ int lce_slabs_landau_gauge(lce_slabs* h, double* theta, int* iters, int max_iter
   lce_slabs* S = h;
   if (!S) return LCE_ERR_INVALID;
   return slab_landau_gauge(S, theta, iters, max_iters);
+}
+
+int lce_slabs_it_landau_gauge(lce_slabs* h, double step, int flags, double* da1, int* iters, int max_iters) {
+  lce_slabs* S = h;
+  if (!S || (flags & ~(LCE_ITGF_FIX_COMPONENT | LCE_ITGF_ASCEND | LCE_ITGF_TRACK))) return LCE_ERR_INVALID;
+  lce_ctx* c0 = S->slab[0];
+  const int cap = max_iters > 0 ? max_iters : 1000000;
+  if (int rc = slab_gf_start(S, (flags & LCE_ITGF_TRACK) ? LCE_GF_START_IDENTITY : -1)) return rc;
+  if (int rc = slab_gf_state(S, cap, -1.0, step > 0.0 ? step : c0->ch[0].alpha)) return rc;
+  ChainState cs;
+  if (int rc = slab_gf_run(S, 0, false, cs, flags)) return rc;
+  if (da1) *da1 = cs.gf_theta;
+  if (iters) *iters = cs.gf_iters;
+  if (!std::isfinite(cs.gf_theta)) return slabs_fail(LCE_ERR_NAN, "slabs gauge fixing: da1 is not finite");
+  if (cs.gf_theta > c0->ch[0].limit_or)
+    return slabs_fail(LCE_ERR_GF_NOT_CONVERGED, "slabs gauge fixing: iteration cap reached");
+  return LCE_OK;
 }
 
 int lce_slabs_landau_gauge_fourier(lce_slabs* h, int start, double step, double theta_switch, double* theta,

@@ -164,19 +164,21 @@ __global__ void __launch_bounds__(kBlock, sizeof(R) == 4 ? 4 : 1)
 // Omega in FP64.  The step comes from the chain state (gf_step); renorm
 // reunitarises the links on the second parity (u_f_renorm after the
 // iteration, as f/landau_gauge.f:56-57 does for the overrelaxed form).
+// s_lo and last as for gf_half_kernel (a z-slab's visited sites; the whole
+// lattice's second half-step, which sums |g|^2 and reunitarises).
 template <typename R>
 __global__ void __launch_bounds__(kBlock) it_half_kernel(const ChainDev* chp, const ChainState* cst, int eo,
-                                                         double* part, int flags, int renorm) {
+                                                         double* part, int flags, int renorm, int s_lo, int last) {
   pdl_trigger();
   const ChainDev& ch = *chp;
-  const int s = blockIdx.x * kBlock + threadIdx.x;
-  const int oe = 1 - eo, nh = ch.nh;
-  const Coord X = site_coord(eo, s < nh ? s : 0, ch.hx, ch.nxy, ch.dhx, ch.dnxy);
+  const int s = s_lo + blockIdx.x * kBlock + threadIdx.x;
+  const int oe = 1 - eo, nh = ch.nh, s_hi = nh - s_lo;
+  const Coord X = site_coord(eo, s < s_hi ? s : s_lo, ch.hx, ch.nxy, ch.dhx, ch.dnxy);
   const int xm[3] = {nbr_dn<0>(ch, X), nbr_dn<1>(ch, X), nbr_dn<2>(ch, X)};
   pdl_wait();
   if (cst->gf_done) return;
   double th[1] = {0.0};
-  if (s < nh) {
+  if (s < s_hi) {
     su2<R> um[3], ud[3];
     double g1a = 0, g1br = 0, g1bi = 0, g2a = 0, g2br = 0, g2bi = 0;
 #pragma unroll
@@ -200,7 +202,7 @@ __global__ void __launch_bounds__(kBlock) it_half_kernel(const ChainDev* chp, co
     const double ga = g1a - g2a;
     const double gbr = fix ? g1br - g2br : -g2br;
     const double gbi = fix ? g1bi - g2bi : g1a - g2bi;
-    if (eo == 1) th[0] = ga * ga + (gbr * gbr + gbi * gbi);
+    if (last) th[0] = ga * ga + (gbr * gbr + gbi * gbi);
     const double st = (flags & LCE_ITGF_ASCEND) ? -cst->gf_step : cst->gf_step;
     const double ha = st * ga, hbr = st * gbr, hbi = st * gbi;
     const double t1 = sqrt(ha * ha + hbr * hbr + hbi * hbi);
@@ -218,7 +220,7 @@ __global__ void __launch_bounds__(kBlock) it_half_kernel(const ChainDev* chp, co
     for (int mu = 0; mu < 3; ++mu) {
       su2<R> a = nn(o, um[mu]);
       su2<R> b = nd(ud[mu], o);
-      if (renorm && eo == 1) {
+      if (renorm && last) {
         a = unitarise64(a);
         b = unitarise64(b);
       }
@@ -230,7 +232,7 @@ __global__ void __launch_bounds__(kBlock) it_half_kernel(const ChainDev* chp, co
       LinkIO<R>::st(ch.g, gi, unitarise64(nn(o, LinkIO<R>::ld_cg(ch.g, gi))));
     }
   }
-  if (eo == 1) block_reduce_store<1>(th, part + blockIdx.x);
+  if (last) block_reduce_store<1>(th, part + blockIdx.x);
 }
 
 // U_f(x,mu) = G(x) U(x,mu) G(x+mu)^+ and A_f(x) -> G(x) A(x) G(x)^+, one
@@ -370,8 +372,8 @@ template <typename R>
 void launch_it_iteration(const ChainDev* ch, ChainState* cst, int flags, int renorm, double* part, int nh,
                          cudaStream_t s) {
   const int nb = ceil_div(nh, kBlock);
-  (void)launch_pdl(it_half_kernel<R>, nb, kBlock, 0, s, ch, (const ChainState*)cst, 0, part, flags, renorm);
-  (void)launch_pdl(it_half_kernel<R>, nb, kBlock, 0, s, ch, (const ChainState*)cst, 1, part, flags, renorm);
+  (void)launch_pdl(it_half_kernel<R>, nb, kBlock, 0, s, ch, (const ChainState*)cst, 0, part, flags, renorm, 0, 0);
+  (void)launch_pdl(it_half_kernel<R>, nb, kBlock, 0, s, ch, (const ChainState*)cst, 1, part, flags, renorm, 0, 1);
   (void)launch_pdl(gf_check_kernel, 1, 1024, 0, s, ch, cst, (const double*)part, nb);
 }
 
@@ -405,6 +407,16 @@ template void launch_gf_iteration<float>(const ChainDev*, ChainState*, int, doub
 template void launch_gf_iteration<double>(const ChainDev*, ChainState*, int, double*, int, cudaStream_t);
 template int launch_gf_half<float>(const ChainDev*, ChainState*, int, int, double*, int, int, int, cudaStream_t);
 template int launch_gf_half<double>(const ChainDev*, ChainState*, int, int, double*, int, int, int, cudaStream_t);
+template <typename R>
+int launch_it_half(const ChainDev* ch, ChainState* cst, int eo, int last, double* part, int nh, int s_lo, int flags,
+                   cudaStream_t s) {
+  const int nb = ceil_div(nh - 2 * s_lo, kBlock);
+  (void)launch_pdl(it_half_kernel<R>, nb, kBlock, 0, s, ch, (const ChainState*)cst, eo, part, flags, 1, s_lo, last);
+  return nb;
+}
+template int launch_it_half<float>(const ChainDev*, ChainState*, int, int, double*, int, int, int, cudaStream_t);
+template int launch_it_half<double>(const ChainDev*, ChainState*, int, int, double*, int, int, int, cudaStream_t);
+
 template void launch_it_iteration<float>(const ChainDev*, ChainState*, int, int, double*, int, cudaStream_t);
 template void launch_it_iteration<double>(const ChainDev*, ChainState*, int, int, double*, int, cudaStream_t);
 template void launch_gf_theta<float>(const ChainDev*, double*, int, cudaStream_t);

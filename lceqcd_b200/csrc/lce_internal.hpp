@@ -30,6 +30,11 @@ constexpr int min_blocks() { return sizeof(R) == 4 ? 4 : 3; }
 constexpr int kNQ = 4;           // doubles of partial sums per block
 constexpr int kMaxSlots = 64;    // reduction slots per finalize
 constexpr int kChunkTiles = 128; // tiles per level-1 chunk of the finalize reduction
+// the tile sizes (sites) of the per-pass kernels' tile tables: 448 = 14 warps,
+// two blocks per SM, balances a single-wave pass (a 64^3 parity: 293 blocks
+// on 148 SMs, at most 28 warps on an SM against 32 with 512)
+constexpr int kTileTables = 4;
+constexpr int kTileSites[kTileTables] = {128, 256, 512, 448};
 
 // pass kinds (one kernel launch over one parity)
 enum PassKind : unsigned char {
@@ -210,6 +215,12 @@ void launch_gf_iteration(const ChainDev* ch, ChainState* cst, int track, double*
 // transform G; returns the number of blocks (partials)
 template <typename R>
 int launch_gf_half(const ChainDev* ch, ChainState* cst, int eo, int last, double* part, int nh, int s_lo, int track,
+                   cudaStream_t s);
+// a half-step of f/it_gauge_fixing.f (reunitarising on the whole lattice's
+// second half-step) on a z-slab's visited sites; returns the number of
+// partials
+template <typename R>
+int launch_it_half(const ChainDev* ch, ChainState* cst, int eo, int last, double* part, int nh, int s_lo, int flags,
                    cudaStream_t s);
 // convergence test of a z-slab decomposed fixing from the slabs' theta sums
 void launch_gf_check_slabs(const ChainDev* ch, ChainState* cst, const double* sums, int nslabs, double nh,

@@ -868,8 +868,9 @@ void launch_link_t(int mode, int mu, const PassArgs& a, int nblocks, cudaStream_
 }
 
 // Tile shapes compiled: FP32 (BS, SPT) in {128, 256, 512} x {1} and
-// {128, 256} x {2} at the 64-register cap, and (128, 1) at 56 registers
-// (a.occ = 1152); the FP64 validation path only BS = 256.
+// {128, 256} x {2} at the 64-register cap, (448, 1) at two blocks per SM (72
+// registers), and (128, 1) at 56 registers (a.occ = 1152); the FP64
+// validation path only BS = 256.
 template <typename R>
 void launch_higgs(int mode, const PassArgs& a, int nblocks, cudaStream_t s) {
   if constexpr (sizeof(R) == 4) {
@@ -884,6 +885,10 @@ void launch_higgs(int mode, const PassArgs& a, int nblocks, cudaStream_t s) {
     }
     if (a.bs == 512) {
       launch_higgs_t<R, 1, 512>(mode, a, nblocks, s);
+      return;
+    }
+    if (a.bs == 448) {
+      launch_higgs_t<R, 1, 448>(mode, a, nblocks, s);
       return;
     }
   }
@@ -905,6 +910,10 @@ void launch_link(int mode, int mu, const PassArgs& a, int nblocks, cudaStream_t 
     }
     if (a.bs == 512) {
       launch_link_t<R, 1, 512>(mode, mu, a, nblocks, s);
+      return;
+    }
+    if (a.bs == 448) {
+      launch_link_t<R, 1, 448>(mode, mu, a, nblocks, s);
       return;
     }
   }

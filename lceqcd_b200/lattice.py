@@ -610,6 +610,17 @@ class SlabLattice:
         self._ck(self.lib.lce_slabs_landau_gauge_from(self.h, code, C.byref(th), C.byref(it), int(max_iters)))
         return th.value, it.value
 
+    def it_landau_gauge(self, step: float = 0.0, fix_component: bool = False, ascend: bool = False,
+                        track: bool = False, max_iters: int = 0):
+        """Lattice.it_landau_gauge (f/it_gauge_fixing.f) on the slabs.
+        Returns (da1, iterations)."""
+        flags = ((_lib.LCE_ITGF_FIX_COMPONENT if fix_component else 0) | (_lib.LCE_ITGF_ASCEND if ascend else 0) |
+                 (_lib.LCE_ITGF_TRACK if track else 0))
+        da1, it = C.c_double(), C.c_int()
+        self._ck(self.lib.lce_slabs_it_landau_gauge(self.h, float(step), flags, C.byref(da1), C.byref(it),
+                                                    int(max_iters)))
+        return da1.value, it.value
+
     def landau_gauge_fourier(self, start: str = "identity", step: float = 1.0, theta_switch: float = 0.0,
                              max_iters: int = 0):
         """Lattice.landau_gauge_fourier on the slabs.  Returns (theta,

@@ -458,7 +458,8 @@ def test_two_sites_per_thread_batch_and_three_way_autotune():
             np.testing.assert_array_equal(o[i][1], outs[0][i][1])
 
 
-SHAPES = [(256, "passes"), (128, "passes"), (512, "passes"), (128, "passes2"), (256, "passes2"), (256, "direct")]
+SHAPES = [(256, "passes"), (128, "passes"), (512, "passes"), (448, "passes"), (128, "passes2"), (256, "passes2"),
+          (256, "direct")]
 
 
 @pytest.mark.parametrize("L", [(16, 8, 12), (64, 32, 34)])
@@ -474,7 +475,7 @@ def test_tile_shapes_update_identically(L):
                     tile_registers=regs, n_link_or=1, n_higgs_metro=1)
         g.init_hot(8)
         ms = [g.sweep(1) for _ in range(3)]
-        assert g.tile_shape(registers=True) == (bs, 2 if mode == "passes2" else 1, regs or 64)
+        assert g.tile_shape(registers=True) == (bs, 2 if mode == "passes2" else 1, regs or (72 if bs == 448 else 64))
         res.append((g.download(), ms, g.rng_position()))
         g.close()
     for (u, a), ms, pos in res[1:]:

@@ -173,6 +173,21 @@ def test_slabs_fourier_fixing_reproduces_the_whole_lattice(precision, limit_or, 
     s.close()
 
 
+@pytest.mark.parametrize("precision,limit_or", [("f64", 1e-10), ("f32", 1e-6)])
+@pytest.mark.parametrize("L,nslabs", [((8, 8, 8), 2), ((6, 8, 12), 3)])
+@pytest.mark.parametrize("fix,asc,track", [(True, True, True), (True, False, False)])
+def test_slabs_iterative_fixing_reproduces_the_whole_lattice(precision, limit_or, L, nslabs, fix, asc, track):
+    """f/it_gauge_fixing.f under f/landau_gauge.f on the slabs: the same
+    iteration count, da1 to summation order, u_f, a_f bit for bit."""
+    g, s, dt = _thermalised_pair(L, nslabs, precision, limit_or)
+    dg, ig = g.it_landau_gauge(0.3, fix_component=fix, ascend=asc, track=track)
+    ds, is_ = s.it_landau_gauge(0.3, fix_component=fix, ascend=asc, track=track)
+    assert is_ == ig and ig > 10 and abs(ds - dg) <= 1e-9 * dg
+    for x, y in zip(s.download(dtype=dt, fixed=True), _fixed(g, dt)):
+        np.testing.assert_array_equal(x, y)
+    s.close()
+
+
 def test_slabs_fourier_fixing_needs_powers_of_two():
     s = SlabLattice((12, 8, 8), 2, precision="f64")
     with pytest.raises(LceError):
