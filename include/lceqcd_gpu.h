@@ -421,6 +421,13 @@ int lce_slabs_landau_gauge_from(lce_slabs* s, int start, double* theta, int* ite
  * undecomposed.  Extents: powers of two up to 1024. */
 int lce_slabs_landau_gauge_fourier(lce_slabs* s, int start, double step, double theta_switch, double* theta,
                                    int* iters_fourier, int* iters_plain, int max_iters);
+/* lce_landau_gauge_fourier_cg on the slabs: the stages of
+ * lce_slabs_landau_gauge_fourier with the conjugate-gradient direction (its
+ * halo plane exchanged), the momentum-space sums on the first slab's device
+ * and the line search summed per slab.  The step's sums are grouped per slab,
+ * so u_f, a_f agree with the undecomposed run to rounding, not bit for bit. */
+int lce_slabs_landau_gauge_fourier_cg(lce_slabs* s, int start, double theta_switch, double* theta,
+                                      int* iters_fourier, int* iters_plain, int max_iters);
 /* lce_it_landau_gauge (f/it_gauge_fixing.f under f/landau_gauge.f) on the
  * slabs: the same halo traffic as lce_slabs_landau_gauge; same iterations
  * and u_f, a_f as undecomposed */

@@ -134,6 +134,7 @@ SIGNATURES = {
     "lce_slabs_landau_gauge_from": (I, [P, I, P, P, I]),
     "lce_slabs_landau_gauge_fourier": (I, [P, I, D, D, P, P, P, I]),
     "lce_slabs_it_landau_gauge": (I, [P, D, I, P, P, I]),
+    "lce_slabs_landau_gauge_fourier_cg": (I, [P, I, D, P, P, P, I]),
     "lce_slabs_landau_gauge": (I, [P, P, P, I]),
     "lce_slabs_correlator": (I, [P, P, P, P, P]),
     "lce_slabs_polyakov": (I, [P, P, P, P]),

@@ -1010,6 +1010,8 @@ struct lce_slabs {
   cudaEvent_t ev_chk = nullptr;
   double* g_d = nullptr;  // slab 0's device: theta sums [n], slice sums [14 L3], correlators [7 L3 + 5]
   void* fft_d = nullptr;  // slab 0's device: the whole lattice's two transformed fields (Fourier fixing)
+  void* cg_d = nullptr;   // slab 0's device: the conjugate-gradient form's whole-lattice buffers (FaSlabCg)
+  FaSlabCg cgw{};
   int L[3] = {0, 0, 0};
   int nz = 0, nxy = 0, prec = LCE_PREC_F32;
   double delta = 0.0;  // ahiggs1 step of the whole lattice (every slab holds a copy)
@@ -1038,11 +1040,14 @@ int slab_rc(lce_ctx* c, int rc) {
 // the gauge-fixed copies U_f, A_f
 // f: a link direction 0-2, 3 for the gauge transform G, 4 for the Fourier
 // iteration's step transform g (FP64), -1 for the Higgs field
+// 5 for component k of the conjugate-gradient direction (FP32)
 size_t slab_elem_bytes(const lce_ctx* c, int f) {
-  return f == 4 ? 32 : (f >= 0 ? link_bytes(c->prec) : real_bytes(c->prec));
+  return f == 5 ? 4 : (f == 4 ? 32 : (f >= 0 ? link_bytes(c->prec) : real_bytes(c->prec)));
 }
+int slab_components(int f) { return f == 5 || f < 0 ? 3 : 1; }
 char* slab_plane(lce_ctx* c, int f, int p, int z, int k, bool fixed = false) {
   const ChainDev& d = c->ch[0];
+  if (f == 5) return (char*)fa_sdir_ptr(c->fa_d, fa_vcap(c)) + (((size_t)(k * 2 + p)) * d.nh + (size_t)z * d.nxy) * 4;
   if (f == 4) return (char*)fa_gstep_ptr(c->fa_d, fa_vcap(c)) + ((size_t)p * d.nh + (size_t)z * d.nxy) * 32;
   if (f == 3) return (char*)d.g + ((size_t)p * d.nh + (size_t)z * d.nxy) * link_bytes(c->prec);
   if (f >= 0)
@@ -1061,7 +1066,7 @@ struct PlaneCopy {
 int slab_copy_plane(lce_ctx* c, lce_ctx* cj, const PlaneCopy& q, size_t nxy) {
   const int ps = q.pg ^ cj->eo_flip, pd = q.pg ^ c->eo_flip;
   const size_t bytes = nxy * slab_elem_bytes(c, q.f);
-  for (int comp = 0; comp < (q.f >= 0 ? 1 : 3); ++comp) {
+  for (int comp = 0; comp < slab_components(q.f); ++comp) {
     void* dst = slab_plane(c, q.f, pd, q.zd, comp, q.fixed);
     const void* src = slab_plane(cj, q.f, ps, q.zs, comp, q.fixed);
     if (c->device == cj->device) SCK(cudaMemcpyAsync(dst, src, bytes, cudaMemcpyDeviceToDevice, c->stream));
@@ -1264,19 +1269,39 @@ int slab_gf_iterations(lce_slabs* S, int batch, int track, int it_flags = -1) {
 // interior lines into the whole lattice's buffer on the first slab's
 // device, theta summed per slab and copied there; (b) the first slab: the
 // check (theta of the whole lattice, iteration count, done flag, step) and
-// the y and z transforms; (c) every slab: the chain state from the first,
-// the inverse x transforms and g at its interior sites; (d) g of the plane
-// above each slab into its upper halo; (e) every slab: g applied at its
-// interior sites (links, A_f, G); (f) the U_z links of the plane below each
-// slab into its lower halo.  Slabs write and read only the lines of their own
-// planes in the buffer; the transforms of (b) run between the two.
+// the y and z transforms (cg: with the momentum-space sums and beta);
+// (c) every slab: the chain state (cg: and the CG state) from the first, the
+// inverse x transforms and g (cg: the direction) at its interior sites;
+// (d) g of the plane above each slab into its upper halo -- cg: the
+// direction's plane instead, then every slab's line derivatives summed per
+// slab and gathered on the first slab, the step there, the CG state back to
+// every slab and g = exp(alpha X) at every local site; (e) every slab: g
+// applied at its interior sites (links, A_f, G); (f) the U_z links of the
+// plane below each slab into its lower halo.  Slabs write and read only the
+// lines of their own planes in the buffer; the transforms of (b) run
+// between the two.
 template <typename R>
-int slab_fa_iterations(lce_slabs* S, int batch) {
+int slab_fa_iterations(lce_slabs* S, int batch, bool cg) {
   const int n = (int)S->slab.size(), nz = S->nz;
   lce_ctx* c0 = S->slab[0];
   const int Lg[3] = {S->L[0], S->L[1], S->L[2]};
   const double nh_all = (double)S->nxy * S->L[2];
   const size_t off = offsetof(ChainState, gf_theta), len = sizeof(ChainState) - off;
+  const FaSlabCg* cgw = cg ? &S->cgw : nullptr;
+  // the CG state of the first slab's device into every slab's buffer
+  auto cg_state_to_slabs = [&]() -> int {
+    for (int k = 0; k < n; ++k) {
+      lce_ctx* c = S->slab[k];
+      DeviceScope ds_(c->device);
+      if (k > 0) SCK(cudaStreamWaitEvent(c->stream, S->ev_chk, 0));
+      void* dst = fa_cg_state(c->fa_d, fa_vcap(c));
+      if (c->device == c0->device)
+        SCK(cudaMemcpyAsync(dst, S->cgw.cg, fa_cg_state_bytes(), cudaMemcpyDeviceToDevice, c->stream));
+      else
+        SCK(cudaMemcpyPeerAsync(dst, c->device, S->cgw.cg, c0->device, fa_cg_state_bytes(), c->stream));
+    }
+    return LCE_OK;
+  };
   for (int it = 0; it < batch; ++it) {
     for (int k = 0; k < n; ++k) {
       lce_ctx* c = S->slab[k];
@@ -1296,13 +1321,16 @@ int slab_fa_iterations(lce_slabs* S, int batch) {
     {
       DeviceScope ds_(c0->device);
       for (int k = 1; k < n; ++k) SCK(cudaStreamWaitEvent(c0->stream, S->ev_sum[k], 0));
-      launch_gf_check_slabs(c0->ch_d, c0->cst_d, S->g_d, n, nh_all, c0->stream, 1);
+      launch_gf_check_slabs(c0->ch_d, c0->cst_d, S->g_d, n, nh_all, c0->stream, cg ? 2 : 1);
       launch_fa_slab_stage<R>(1, c0->ch_d, c0->ch[0], c0->cst_d, S->fft_d, c0->fa_d, fa_vcap(c0), nullptr, Lg, 1, nz,
-                              0, c0->s_lo, c0->stream);
+                              0, c0->s_lo, c0->stream, cgw);
       const std::string fe = fa_take_error();
       if (!fe.empty()) return slabs_fail(LCE_ERR_CUDA, "slabs Fourier fixing: " + fe);
       SCK(cudaGetLastError());
       SCK(cudaEventRecord(S->ev_chk, c0->stream));
+    }
+    if (cg) {
+      if (int rc = cg_state_to_slabs()) return rc;
     }
     for (int k = 0; k < n; ++k) {
       lce_ctx* c = S->slab[k];
@@ -1315,14 +1343,50 @@ int slab_fa_iterations(lce_slabs* S, int batch) {
         else SCK(cudaMemcpyPeerAsync(dst, c->device, src, c0->device, len, c->stream));
       }
       launch_fa_slab_stage<R>(2, c->ch_d, c->ch[0], c->cst_d, S->fft_d, c->fa_d, fa_vcap(c), nullptr, Lg, 1, nz,
-                              k * nz, c->s_lo, c->stream);
+                              k * nz, c->s_lo, c->stream, cgw);
       const std::string fe = fa_take_error();
       if (!fe.empty()) return slabs_fail(LCE_ERR_CUDA, "slabs Fourier fixing: " + fe);
       SCK(cudaGetLastError());
       SCK(cudaEventRecord(S->ev_pass[k], c->stream));
     }
-    const PlaneCopy gcp[2] = {{+1, 1, nz + 1, 4, 0, false}, {+1, 1, nz + 1, 4, 1, false}};
-    if (int rc = slab_exchange(S, gcp, 2)) return rc;
+    if (cg) {
+      const PlaneCopy dcp[2] = {{+1, 1, nz + 1, 5, 0, false}, {+1, 1, nz + 1, 5, 1, false}};
+      if (int rc = slab_exchange(S, dcp, 2)) return rc;
+      for (int k = 0; k < n; ++k) {
+        lce_ctx* c = S->slab[k];
+        DeviceScope ds_(c->device);
+        const int nb = launch_fa_slab_stage<R>(4, c->ch_d, c->ch[0], c->cst_d, S->fft_d, c->fa_d, fa_vcap(c),
+                                               nullptr, Lg, 1, nz, k * nz, c->s_lo, c->stream, cgw);
+        // the slab's triple into its scratch, then to the first slab's device
+        launch_sum_partials(fa_cgpart_ptr(c->fa_d, fa_vcap(c)), nb, 3, c->scratch_d, c->stream);
+        SCK(cudaGetLastError());
+        double* dst = S->cgw.tri + 3 * (size_t)k;
+        if (c->device == c0->device)
+          SCK(cudaMemcpyAsync(dst, c->scratch_d, 3 * sizeof(double), cudaMemcpyDeviceToDevice, c->stream));
+        else
+          SCK(cudaMemcpyPeerAsync(dst, c0->device, c->scratch_d, c->device, 3 * sizeof(double), c->stream));
+        SCK(cudaEventRecord(S->ev_sum[k], c->stream));
+      }
+      {
+        DeviceScope ds_(c0->device);
+        for (int k = 1; k < n; ++k) SCK(cudaStreamWaitEvent(c0->stream, S->ev_sum[k], 0));
+        launch_fa_slab_stage<R>(5, c0->ch_d, c0->ch[0], c0->cst_d, S->fft_d, c0->fa_d, fa_vcap(c0), nullptr, Lg, 1,
+                                nz, 0, c0->s_lo, c0->stream, cgw);
+        SCK(cudaGetLastError());
+        SCK(cudaEventRecord(S->ev_chk, c0->stream));
+      }
+      if (int rc = cg_state_to_slabs()) return rc;
+      for (int k = 0; k < n; ++k) {
+        lce_ctx* c = S->slab[k];
+        DeviceScope ds_(c->device);
+        launch_fa_slab_stage<R>(6, c->ch_d, c->ch[0], c->cst_d, S->fft_d, c->fa_d, fa_vcap(c), nullptr, Lg, 1, nz,
+                                k * nz, c->s_lo, c->stream, cgw);
+        SCK(cudaGetLastError());
+      }
+    } else {
+      const PlaneCopy gcp[2] = {{+1, 1, nz + 1, 4, 0, false}, {+1, 1, nz + 1, 4, 1, false}};
+      if (int rc = slab_exchange(S, gcp, 2)) return rc;
+    }
     for (int k = 0; k < n; ++k) {
       lce_ctx* c = S->slab[k];
       DeviceScope ds_(c->device);
@@ -1401,14 +1465,15 @@ int slab_gf_state(lce_slabs* S, int cap, double limit = -1.0, double step = -1.0
 
 // batches of iterations (overrelaxed, or Fourier-accelerated with fourier)
 // until the first slab's chain state says done; its final state in cs
-int slab_gf_run(lce_slabs* S, int track, bool fourier, ChainState& cs, int it_flags = -1) {
+int slab_gf_run(lce_slabs* S, int track, bool fourier, ChainState& cs, int it_flags = -1, bool cg = false) {
   lce_ctx* c0 = S->slab[0];
   std::memset(&cs, 0, sizeof(cs));
   int batch = fourier ? 4 : 8;
   while (true) {
     int rc;
     if (fourier)
-      rc = S->prec == LCE_PREC_F64 ? slab_fa_iterations<double>(S, batch) : slab_fa_iterations<float>(S, batch);
+      rc = S->prec == LCE_PREC_F64 ? slab_fa_iterations<double>(S, batch, cg)
+                                   : slab_fa_iterations<float>(S, batch, cg);
     else
       rc = S->prec == LCE_PREC_F64 ? slab_gf_iterations<double>(S, batch, track, it_flags)
                                    : slab_gf_iterations<float>(S, batch, track, it_flags);
@@ -1448,7 +1513,7 @@ int slab_landau_gauge(lce_slabs* S, double* theta, int* iters, int max_iters, in
 // lce_landau_gauge_fourier on the slabs: Fourier-accelerated iterations to
 // theta_switch, then the overrelaxed iteration to limit_or, tracking G
 int slab_fourier_fix(lce_slabs* S, int start, double step, double theta_switch, double* theta, int* iters_f,
-                     int* iters_p, int max_iters) {
+                     int* iters_p, int max_iters, bool cg = false) {
   lce_ctx* c0 = S->slab[0];
   const double limit = c0->ch[0].limit_or;
   if (!(step > 0.0)) step = 1.0;
@@ -1472,11 +1537,38 @@ int slab_fourier_fix(lce_slabs* S, int start, double step, double theta_switch, 
       return slabs_fail(LCE_ERR_NOMEM, "slabs Fourier fixing: the whole lattice's transform buffer");
     }
   }
+  if (cg && !S->cg_d) {
+    // the CG state (256 bytes), F of this and the previous iteration, the z
+    // transform's per-block pairs and one line triple per slab
+    DeviceScope ds_(c0->device);
+    const size_t V = (size_t)S->L[0] * S->L[1] * S->L[2];
+    int lz = 0;
+    while ((1 << lz) < S->L[2]) ++lz;
+    const size_t nbz = (V / S->L[2] + (4096 >> lz) - 1) / (4096 >> lz);
+    const size_t prev_b = 4 * V * 2 * sizeof(float), pairs_n = 2 * 2 * nbz, tri_n = 3 * S->slab.size();
+    if (cudaMalloc(&S->cg_d, 256 + prev_b + (pairs_n + tri_n) * sizeof(double)) != cudaSuccess) {
+      S->cg_d = nullptr;
+      cudaGetLastError();
+      return slabs_fail(LCE_ERR_NOMEM, "slabs Fourier CG fixing: the whole lattice's CG buffers");
+    }
+    char* b = static_cast<char*>(S->cg_d);
+    S->cgw.cg = b;
+    S->cgw.prev = b + 256;
+    S->cgw.pairs = reinterpret_cast<double*>(b + 256 + prev_b);
+    S->cgw.tri = S->cgw.pairs + pairs_n;
+    S->cgw.nslabs = (int)S->slab.size();
+    S->cgw.nh_all = (double)S->nxy * S->L[2];
+  }
   const int cap = max_iters > 0 ? max_iters : 1000000;
   if (int rc = slab_gf_start(S, start)) return rc;
   if (int rc = slab_gf_state(S, cap, theta_switch, step)) return rc;
+  if (cg) {
+    DeviceScope ds_(c0->device);
+    fa_cg_reset_state(S->cgw.cg, c0->stream);
+    SCK(cudaGetLastError());
+  }
   ChainState cs;
-  if (int rc = slab_gf_run(S, 1, true, cs)) return rc;
+  if (int rc = slab_gf_run(S, 1, true, cs, -1, cg)) return rc;
   if (iters_f) *iters_f = cs.gf_iters;
   if (iters_p) *iters_p = 0;
   if (theta) *theta = cs.gf_theta;
@@ -2651,6 +2743,7 @@ void lce_slabs_destroy(lce_slabs* h) {
     DeviceScope ds_(S->slab[0]->device);
     if (S->g_d) cudaFree(S->g_d);
     if (S->fft_d) cudaFree(S->fft_d);
+    if (S->cg_d) cudaFree(S->cg_d);
     if (S->ev_chk) cudaEventDestroy(S->ev_chk);
   }
   for (size_t k = 0; k < S->slab.size(); ++k) {
@@ -2744,6 +2837,15 @@ int lce_slabs_landau_gauge_fourier(lce_slabs* h, int start, double step, double 
   if (start != LCE_GF_START_IDENTITY && start != LCE_GF_START_TRANSFORM)
     return slabs_fail(LCE_ERR_INVALID, "slabs_landau_gauge_fourier: start must be IDENTITY or TRANSFORM");
   return slab_fourier_fix(S, start, step, theta_switch, theta, iters_fourier, iters_plain, max_iters);
+}
+
+int lce_slabs_landau_gauge_fourier_cg(lce_slabs* h, int start, double theta_switch, double* theta,
+                                      int* iters_fourier, int* iters_plain, int max_iters) {
+  lce_slabs* S = h;
+  if (!S) return LCE_ERR_INVALID;
+  if (start != LCE_GF_START_IDENTITY && start != LCE_GF_START_TRANSFORM)
+    return slabs_fail(LCE_ERR_INVALID, "slabs_landau_gauge_fourier_cg: start must be IDENTITY or TRANSFORM");
+  return slab_fourier_fix(S, start, 1.0, theta_switch, theta, iters_fourier, iters_plain, max_iters, true);
 }
 
 int lce_slabs_landau_gauge_from(lce_slabs* h, int start, double* theta, int* iters, int max_iters) {

@@ -278,6 +278,9 @@ struct FaArgs {
   // lattice's z of plane zl0, s_lo: first visited site of each parity.
   // A whole lattice: 0, L3, 0, 0.
   int zl0, nzl, zg0, s_lo;
+  // CG: sites per parity of the whole lattice for the step's rms angle
+  // (0: the chain's)
+  double nh_all;
 };
 
 __device__ __forceinline__ bool fa_done(const FaArgs& a) { return a.cst && a.cst->gf_done; }
@@ -616,9 +619,10 @@ __global__ void __launch_bounds__(kBlock) fa_line_kernel(FaArgs a) {
   if (fa_done(a)) return;
   const ChainDev& ch = *a.ch;
   const int i = blockIdx.x * kBlock + threadIdx.x;
+  const int nvis = ch.nh - 2 * a.s_lo;  // visited sites per parity
   double v[3] = {0.0, 0.0, 0.0};
-  if (i < 2 * ch.nh) {
-    const int eo = i >= ch.nh ? 1 : 0, oe = 1 - eo, s = i - eo * ch.nh, nh = ch.nh;
+  if (i < 2 * nvis) {
+    const int eo = i >= nvis ? 1 : 0, oe = 1 - eo, s = a.s_lo + i - eo * nvis, nh = ch.nh;
     const size_t V2 = 2 * (size_t)nh;
     const Coord X = site_coord(eo, s, ch.hx, ch.nxy, ch.dhx, ch.dnxy);
     const su2<R> gx = fa_gen<R>(a.sdir, V2, (size_t)eo * nh + s);
@@ -663,7 +667,8 @@ __global__ void __launch_bounds__(1024) fa_alpha_kernel(FaArgs a, int nparts) {
   __syncthreads();
   if (threadIdx.x == 0) {
     FaCg* g = a.cg;
-    const double d1 = t[0], d2 = t[1], rms = sqrt(t[2] / (2.0 * a.ch->nh));
+    const double nh = a.nh_all > 0.0 ? a.nh_all : (double)a.ch->nh;
+    const double d1 = t[0], d2 = t[1], rms = sqrt(t[2] / (2.0 * nh));
     const double amax = rms > 0.0 ? fmin(10.0, 0.5 / rms) : 10.0;
     double al;
     if (d1 > 0.0 && d2 < 0.0) {
@@ -743,6 +748,11 @@ __global__ void fa_cg_reset_kernel(FaCg* g) {
 void fa_cg_reset(void* buf, size_t vcap, cudaStream_t s) {
   fa_cg_reset_kernel<<<1, 1, 0, s>>>(reinterpret_cast<FaCg*>(fa_at(buf, fa_off_cg(vcap))));
 }
+void* fa_cg_state(void* buf, size_t vcap) { return fa_at(buf, fa_off_cg(vcap)); }
+void fa_cg_reset_state(void* cg, cudaStream_t s) { fa_cg_reset_kernel<<<1, 1, 0, s>>>(reinterpret_cast<FaCg*>(cg)); }
+size_t fa_cg_state_bytes() { return sizeof(FaCg); }
+void* fa_sdir_ptr(void* buf, size_t vcap) { return fa_at(buf, fa_off_sdir(vcap)); }
+double* fa_cgpart_ptr(void* buf, size_t vcap) { return reinterpret_cast<double*>(fa_at(buf, fa_off_cgpart(vcap))); }
 
 // The first failed launch set-up of this host thread since the last
 // fa_take_error(): which kernel, its line length and the shared memory it
@@ -830,6 +840,7 @@ void launch_fa_iteration(const ChainDev* chd, const ChainDev& ch, ChainState* cs
   a.nzl = ch.L3;
   a.zg0 = 0;
   a.s_lo = 0;
+  a.nh_all = 0.0;
   a.cg = reinterpret_cast<FaCg*>(fa_at(buf, fa_off_cg(vcap)));
   a.prev = fa_at(buf, fa_off_prev(vcap));
   a.sdir = reinterpret_cast<float*>(fa_at(buf, fa_off_sdir(vcap)));
@@ -884,7 +895,7 @@ void launch_fa_iteration(const ChainDev* chd, const ChainDev& ch, ChainState* cs
 template <typename R>
 int launch_fa_slab_stage(int stage, const ChainDev* chd, const ChainDev& ch, ChainState* cst, void* fft, void* buf,
                          size_t vcap, double* part, const int Lg[3], int zl0, int nzl, int zg0, int s_lo,
-                         cudaStream_t s) {
+                         cudaStream_t s, const FaSlabCg* cgw) {
   FaArgs a;
   std::memset(&a, 0, sizeof(a));
   a.ch = chd;
@@ -908,6 +919,16 @@ int launch_fa_slab_stage(int stage, const ChainDev* chd, const ChainDev& ch, Cha
   a.prev = fa_at(buf, fa_off_prev(vcap));
   a.sdir = reinterpret_cast<float*>(fa_at(buf, fa_off_sdir(vcap)));
   a.cgpart = reinterpret_cast<double*>(fa_at(buf, fa_off_cgpart(vcap)));
+  a.nh_all = 0.0;
+  const bool cg = cgw != nullptr;
+  if (cg && (stage == 1 || stage == 5)) {
+    // the whole lattice's CG state, F of this and the previous iteration and
+    // the sums, on the first slab's device
+    a.cg = reinterpret_cast<FaCg*>(cgw->cg);
+    a.prev = cgw->prev;
+    a.cgpart = stage == 1 ? cgw->pairs : cgw->tri;
+    a.nh_all = cgw->nh_all;
+  }
   const size_t V = (size_t)Lg[0] * Lg[1] * Lg[2];
   const int nbd = fa_blocks((long)Lg[1] * nzl, a.logL[0], 2);
   if (stage == 0) {
@@ -921,29 +942,58 @@ int launch_fa_slab_stage(int stage, const ChainDev* chd, const ChainDev& ch, Cha
 #define LCE_FA_Y(L) fa_fft_launch<1, -1, false, L>(a, nby, s)
     LCE_FA_SWITCH(a.logL[1], LCE_FA_Y)
 #undef LCE_FA_Y
+    if (cg) {
+#define LCE_FA_ZC(L) fa_fft_launch<2, -1, true, L, true>(a, nbz, s)
+      LCE_FA_SWITCH(a.logL[2], LCE_FA_ZC)
+#undef LCE_FA_ZC
+      fa_beta_kernel<<<1, 1024, 0, s>>>(a, 2 * nbz);
+    } else {
 #define LCE_FA_Z(L) fa_fft_launch<2, -1, true, L>(a, nbz, s)
-    LCE_FA_SWITCH(a.logL[2], LCE_FA_Z)
+      LCE_FA_SWITCH(a.logL[2], LCE_FA_Z)
 #undef LCE_FA_Z
+    }
 #define LCE_FA_YI(L) fa_fft_launch<1, +1, false, L>(a, nby, s)
     LCE_FA_SWITCH(a.logL[1], LCE_FA_YI)
 #undef LCE_FA_YI
     return 0;
   }
   if (stage == 2) {
+    if (cg) {
+#define LCE_FA_GC(L) fa_g_launch<R, L, true>(a, nbd, s)
+      LCE_FA_SWITCH(a.logL[0], LCE_FA_GC)
+#undef LCE_FA_GC
+    } else {
 #define LCE_FA_G(L) fa_g_launch<R, L>(a, nbd, s)
-    LCE_FA_SWITCH(a.logL[0], LCE_FA_G)
+      LCE_FA_SWITCH(a.logL[0], LCE_FA_G)
 #undef LCE_FA_G
+    }
     return 0;
   }
   const int nbv = ceil_div(2L * (ch.nh - 2 * s_lo), kBlock);
+  if (stage == 4) {
+    // CG: the line derivatives at the slab's interior sites, one triple per
+    // block into the buffer's own per-block sums (fa_cgpart_ptr)
+    fa_line_kernel<R><<<nbv, kBlock, 0, s>>>(a);
+    return nbv;
+  }
+  if (stage == 5) {
+    // CG: the step from the slabs' sums (cgw->sums, one triple per slab)
+    fa_alpha_kernel<<<1, 1024, 0, s>>>(a, cgw->nslabs);
+    return 0;
+  }
+  if (stage == 6) {
+    // CG: g = exp(alpha X) at every local site (the halo planes included)
+    fa_gstep_kernel<<<ceil_div(2L * ch.nh, kBlock), kBlock, 0, s>>>(a);
+    return 0;
+  }
   fa_apply_kernel<R><<<nbv, kBlock, 0, s>>>(a);
   return 0;
 }
 
 template int launch_fa_slab_stage<float>(int, const ChainDev*, const ChainDev&, ChainState*, void*, void*, size_t,
-                                         double*, const int*, int, int, int, int, cudaStream_t);
+                                         double*, const int*, int, int, int, int, cudaStream_t, const FaSlabCg*);
 template int launch_fa_slab_stage<double>(int, const ChainDev*, const ChainDev&, ChainState*, void*, void*, size_t,
-                                          double*, const int*, int, int, int, int, cudaStream_t);
+                                          double*, const int*, int, int, int, int, cudaStream_t, const FaSlabCg*);
 
 template void launch_fa_iteration<float>(const ChainDev*, const ChainDev&, ChainState*, double, void*, size_t,
                                          double*, double*, int, bool, bool, bool, cudaStream_t);

@@ -293,8 +293,9 @@ __global__ void __launch_bounds__(1024) gf_check_kernel(const ChainDev* chp, Cha
 // the same test for a lattice split into z-slabs: the slabs' theta sums (in
 // slab order) over the whole lattice's nh odd sites, counted into slab 0's
 // chain state, which the host copies to the other slabs
-// fa: the Fourier-accelerated iteration's check (stop at gf_limit, shorten
-// the step after an overshoot, as fa_check_kernel); else the overrelaxed
+// fa: the Fourier-accelerated iteration's check (stop at gf_limit; fa = 1
+// also shortens the step after an overshoot, as fa_check_kernel, which the
+// conjugate-gradient form, fa = 2, does not); fa = 0: the overrelaxed
 // iteration's (stop at limit_or)
 __global__ void gf_check_slabs_kernel(const ChainDev* chp, ChainState* cst, const double* sums, int nslabs,
                                       double nh, int fa) {
@@ -303,7 +304,7 @@ __global__ void gf_check_slabs_kernel(const ChainDev* chp, ChainState* cst, cons
   for (int j = 0; j < nslabs; ++j) tot += sums[j];
   const double theta = tot / nh;
   const int it = cst->gf_iters + 1;
-  if (fa && it > 1 && theta > 2.0 * cst->gf_theta) cst->gf_step = fmax(0.1, 0.7 * cst->gf_step);
+  if (fa == 1 && it > 1 && theta > 2.0 * cst->gf_theta) cst->gf_step = fmax(0.1, 0.7 * cst->gf_step);
   cst->gf_iters = it;
   cst->gf_theta = theta;
   const double limit = fa ? cst->gf_limit : chp->limit_or;
@@ -400,6 +401,7 @@ void launch_gf_theta(const ChainDev* ch, double* part, int nh, cudaStream_t s) {
 void launch_sum_partials(const double* part, int nblocks, int nq, double* out, cudaStream_t s) {
   if (nq == 1) sum_partials_kernel<1><<<1, 1024, 0, s>>>(part, nblocks, out);
   else if (nq == 2) sum_partials_kernel<2><<<1, 1024, 0, s>>>(part, nblocks, out);
+  else if (nq == 3) sum_partials_kernel<3><<<1, 1024, 0, s>>>(part, nblocks, out);
   else sum_partials_kernel<4><<<1, 1024, 0, s>>>(part, nblocks, out);
 }
 

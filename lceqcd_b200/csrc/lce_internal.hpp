@@ -249,15 +249,37 @@ void launch_fa_iteration(const ChainDev* chd, const ChainDev& ch, ChainState* cs
                          bool cg, cudaStream_t s);
 // the conjugate-gradient form starts its next iteration from the gradient
 void fa_cg_reset(void* buf, size_t vcap, cudaStream_t s);
+// the conjugate-gradient form on z-slabs: the whole lattice's CG state, F of
+// this and the previous iteration ([2][2 fields][V] complex), the z
+// transform's per-block pairs and one line-search triple per slab, on the
+// first slab's device
+struct FaSlabCg {
+  void* cg;
+  void* prev;
+  double* pairs;
+  double* tri;
+  int nslabs;
+  double nh_all;
+};
 // one stage of an iteration on a z-slab (lce_fourier.cu: 0 Delta and the x
 // transforms into the whole lattice's buffer fft, returns the number of theta
 // partials; 1 the y and z transforms of fft; 2 the inverse x transforms and
-// g; 3 g applied); Lg: the whole lattice; zl0, nzl, zg0, s_lo: the slab's
-// visited planes and sites
+// g (CG: the direction); 3 g applied; CG: 4 the line derivatives (returns
+// the number of partial triples), 5 the step from the slabs' sums, 6 g from
+// the direction); Lg: the whole lattice; zl0, nzl, zg0, s_lo: the slab's
+// visited planes and sites; cg: the CG form's whole-lattice buffers, or NULL
 template <typename R>
 int launch_fa_slab_stage(int stage, const ChainDev* chd, const ChainDev& ch, ChainState* cst, void* fft, void* buf,
                          size_t vcap, double* part, const int Lg[3], int zl0, int nzl, int zg0, int s_lo,
-                         cudaStream_t s);
+                         cudaStream_t s, const FaSlabCg* cg = nullptr);
+// the CG state of a buffer, a reset of a state, its size; the direction
+// field of a buffer ([component][parity][site] FP32)
+void* fa_cg_state(void* buf, size_t vcap);
+void fa_cg_reset_state(void* cg, cudaStream_t s);
+size_t fa_cg_state_bytes();
+void* fa_sdir_ptr(void* buf, size_t vcap);
+// the per-block sums of a buffer (triples for up to vcap / 128 + 64 blocks)
+double* fa_cgpart_ptr(void* buf, size_t vcap);
 // the step transform g of a buffer ([parity][site], FP64 first rows)
 void* fa_gstep_ptr(void* buf, size_t vcap);
 // the first launch set-up failure of this host thread's Fourier kernels

@@ -621,6 +621,15 @@ class SlabLattice:
                                                     int(max_iters)))
         return da1.value, it.value
 
+    def landau_gauge_fourier_cg(self, start: str = "identity", theta_switch: float = 0.0, max_iters: int = 0):
+        """Lattice.landau_gauge_fourier_cg on the slabs.  Returns (theta,
+        fourier_iters, plain_iters)."""
+        th, itf, itp = C.c_double(), C.c_int(), C.c_int()
+        code = {"identity": _lib.LCE_GF_START_IDENTITY, "transform": _lib.LCE_GF_START_TRANSFORM}[start]
+        self._ck(self.lib.lce_slabs_landau_gauge_fourier_cg(self.h, code, float(theta_switch), C.byref(th),
+                                                            C.byref(itf), C.byref(itp), int(max_iters)))
+        return th.value, itf.value, itp.value
+
     def landau_gauge_fourier(self, start: str = "identity", step: float = 1.0, theta_switch: float = 0.0,
                              max_iters: int = 0):
         """Lattice.landau_gauge_fourier on the slabs.  Returns (theta,

@@ -188,6 +188,28 @@ def test_slabs_iterative_fixing_reproduces_the_whole_lattice(precision, limit_or
     s.close()
 
 
+@pytest.mark.parametrize("precision,limit_or", [("f64", 1e-10), ("f32", 1e-6)])
+@pytest.mark.parametrize("L,nslabs", [((8, 8, 8), 2), ((8, 4, 16), 4), ((16, 8, 8), 2)])
+def test_slabs_fourier_cg_fixing_matches_the_whole_lattice(precision, limit_or, L, nslabs):
+    """The conjugate-gradient form on the slabs, from G = 1 and after three
+    sweeps from the previous transform: the line search's sums are grouped
+    per slab, so the step differs from the undecomposed one in the last bits;
+    the same iteration counts and u_f, a_f equal to rounding."""
+    g, s, dt = _thermalised_pair(L, nslabs, precision, limit_or)
+    tol = 1e-9 if precision == "f64" else 2e-5
+    for start in ("identity", "transform"):
+        tg, fg, pg = g.landau_gauge_fourier_cg(start)
+        ts, fs, ps = s.landau_gauge_fourier_cg(start)
+        assert fs == fg and pg == ps == 0 and fg > 2
+        assert ts <= limit_or and tg <= limit_or
+        for x, y in zip(s.download(dtype=dt, fixed=True), _fixed(g, dt)):
+            assert np.max(np.abs(x.astype(np.float64) - y.astype(np.float64))) <= tol * max(1.0, np.max(np.abs(y)))
+        for _ in range(3):
+            g.sweep(0)
+            s.sweep(0)
+    s.close()
+
+
 def test_slabs_fourier_fixing_needs_powers_of_two():
     s = SlabLattice((12, 8, 8), 2, precision="f64")
     with pytest.raises(LceError):
