@@ -425,7 +425,9 @@ int lce_slabs_landau_gauge_fourier(lce_slabs* s, int start, double step, double 
  * lce_slabs_landau_gauge_fourier with the conjugate-gradient direction (its
  * halo plane exchanged), the momentum-space sums on the first slab's device
  * and the line search summed per slab.  The step's sums are grouped per slab,
- * so u_f, a_f agree with the undecomposed run to rounding, not bit for bit. */
+ * so the run takes steps equal to the undecomposed run's but for the last
+ * bits: the same iterations, u_f, a_f equal within what the stopping theta
+ * leaves free (~1e-8 at theta < 1e-10 in FP64), not bit for bit. */
 int lce_slabs_landau_gauge_fourier_cg(lce_slabs* s, int start, double theta_switch, double* theta,
                                       int* iters_fourier, int* iters_plain, int max_iters);
 /* lce_it_landau_gauge (f/it_gauge_fixing.f under f/landau_gauge.f) on the

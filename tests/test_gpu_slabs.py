@@ -193,10 +193,13 @@ def test_slabs_iterative_fixing_reproduces_the_whole_lattice(precision, limit_or
 def test_slabs_fourier_cg_fixing_matches_the_whole_lattice(precision, limit_or, L, nslabs):
     """The conjugate-gradient form on the slabs, from G = 1 and after three
     sweeps from the previous transform: the line search's sums are grouped
-    per slab, so the step differs from the undecomposed one in the last bits;
-    the same iteration counts and u_f, a_f equal to rounding."""
+    per slab, so the step differs from the undecomposed one in the last bits
+    and the two runs stop at different points inside theta < limit_or --
+    the same iteration counts, u_f, a_f equal within what the stopping
+    criterion leaves free (|dU| ~ sqrt(limit_or): 1e-6 in FP64 at 1e-10,
+    measured 1.8e-8; 2e-5 in FP32)."""
     g, s, dt = _thermalised_pair(L, nslabs, precision, limit_or)
-    tol = 1e-9 if precision == "f64" else 2e-5
+    tol = 1e-6 if precision == "f64" else 2e-5
     for start in ("identity", "transform"):
         tg, fg, pg = g.landau_gauge_fourier_cg(start)
         ts, fs, ps = s.landau_gauge_fourier_cg(start)
