@@ -473,6 +473,34 @@ def extras(args, peak):
         g.close()
     except Exception as e:
         out["slabs_256cubed_one_gpu"] = {"error": repr(e)[:300]}
+    # the Fourier-accelerated gauge fixing on z-slabs (one GPU): a 128^3
+    # configuration 30 sweeps from a hot start fixed from G = 1 to theta <
+    # 1e-10 undecomposed and in 2 slabs (per-site stages on every slab, the
+    # y/z transforms of the whole lattice's buffer on the first slab's device)
+    try:
+        from lceqcd_b200 import SlabLattice
+        L = (128, 128, 128)
+        kw = dict(COUP, precision="f32", seed=61, limit_or=1e-10)
+        g = Lattice(L, sweep_mode="passes", **kw)
+        g.init_hot(62)
+        g.sweeps(30, 0)
+        u, a = g.download()
+        s = SlabLattice(L, 2, **kw)
+        s.upload(u, a)
+        del u, a
+        res = {}
+        for name, fn in (("undecomposed", g.landau_gauge_fourier), ("2_slabs", s.landau_gauge_fourier)):
+            fn("identity", max_iters=5000)  # buffers, kernels' attributes
+            t0 = time.perf_counter()
+            th, itf, itp = fn("identity", max_iters=5000)
+            res[name] = {"s_per_fixing": time.perf_counter() - t0, "fourier_iters": itf, "plain_iters": itp,
+                         "theta": th}
+        res["note"] = "host wall clock around a synchronised fixing; both on one GPU"
+        out["slabs_fourier_fix_128cubed_one_gpu"] = res
+        s.close()
+        g.close()
+    except Exception as e:
+        out["slabs_fourier_fix_128cubed_one_gpu"] = {"error": repr(e)[:300]}
     # batched ensemble: 96 chains (32 each of 16^3, 32^3, 48^3) over the
     # coupling grid, against the same chains run one context at a time
     try:
