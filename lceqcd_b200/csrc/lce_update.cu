@@ -497,15 +497,18 @@ __device__ __forceinline__ void finalize_chain_warp(const FinalizeArgs& f, int w
 // loads in flight at once (L2, the sums of other blocks), then the in-order
 // scan over the slots reads them from the lanes by shuffles -- one L2 round
 // trip per chain instead of one per slot.
-// SM: the totals of a single chain are in shared memory (stot) instead of
-// f.totals.
+// SM: a single chain whose totals are in shared memory (stot) instead of
+// f.totals, with its volume, ahiggs1 step and RNG counters loaded at the
+// kernel's start (pre = {2 nh, delta}, ctr = {pass_ctr, stream_pos}): no
+// dependent global load is left for the combine.
 template <bool SM = false>
-__device__ __forceinline__ void finalize_combine(const FinalizeArgs& f, const double* stot = nullptr) {
+__device__ __forceinline__ void finalize_combine(const FinalizeArgs& f, const double* stot = nullptr,
+                                                 const double* pre = nullptr, const unsigned long long* ctr = nullptr) {
   static_assert(kMaxSlots <= 64, "two slots per lane");
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarps = (int)(blockDim.x >> 5);
   for (int c = warp; c < f.nchains; c += nwarps) {
-    const ChainDev& ch = f.chains[c];
-    const double V = 2.0 * ch.nh;
+    const double V = SM ? pre[0] : 2.0 * f.chains[c].nh;
+    double delta = SM ? pre[1] : 0.0;  // the ahiggs1 step as the combine leaves it (SM)
     const double* base = SM ? stot : f.totals + (size_t)c * kMaxSlots * kNQ;
     double t0[kNQ], t1[kNQ];
     bool bad = false;
@@ -538,18 +541,20 @@ __device__ __forceinline__ void finalize_combine(const FinalizeArgs& f, const do
             if (kind == kHiggsOR) m.acc_or = acc;
             if (kind == kHiggsMetro) {
               // f/ahiggs1.f:113-123 step adaptation, in the build's precision
+              const double d0 = SM ? delta : f.cst[c].delta;
               if (f.single) {
-                float a = (float)h[0] / (float)V, d = (float)f.cst[c].delta;
+                float a = (float)h[0] / (float)V, d = (float)d0;
                 if (fabsf(a - 0.5f) > 0.1f) d = (a > 0.5f) ? 1.1131241f * d : 0.8989669f * d;
                 m.acc_metro = a;
-                f.cst[c].delta = d;
+                delta = d;
               } else {
-                double d = f.cst[c].delta;
+                double d = d0;
                 if (fabs(acc - 0.5) > 0.1) d = (acc > 0.5) ? 1.1131241 * d : 0.8989669 * d;
                 m.acc_metro = acc;
-                f.cst[c].delta = d;
+                delta = d;
               }
-              m.delta = f.cst[c].delta;
+              f.cst[c].delta = delta;
+              m.delta = delta;
             }
           }
           h[0] = h[1] = h[2] = h[3] = 0;
@@ -582,12 +587,17 @@ __device__ __forceinline__ void finalize_combine(const FinalizeArgs& f, const do
         }
       }
     }
-    if (lane == 0) m.delta = f.cst[c].delta;
+    if (lane == 0) m.delta = SM ? delta : f.cst[c].delta;
   }
   __syncthreads();
   if (threadIdx.x == 0) {
-    f.st->pass_ctr += f.npasses;
-    f.st->stream_pos += f.nstream;
+    if (SM) {
+      f.st->pass_ctr = ctr[0] + f.npasses;
+      f.st->stream_pos = ctr[1] + f.nstream;
+    } else {
+      f.st->pass_ctr += f.npasses;
+      f.st->stream_pos += f.nstream;
+    }
   }
 }
 
@@ -604,7 +614,17 @@ __global__ void __launch_bounds__(kFinSmallWarps * 32) finalize_small_kernel(Fin
   pdl_trigger();
   pdl_wait();
   __shared__ double s_tot[kMaxSlots * kNQ];
+  __shared__ double s_pre[2];
+  __shared__ unsigned long long s_ctr[2];
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  // the combine's inputs other than the totals, loaded by the last warp (idle
+  // unless there are more slots than warps) while the others sum
+  if (warp == kFinSmallWarps - 1 && lane == 0) {
+    s_pre[0] = 2.0 * f.chains[0].nh;
+    s_pre[1] = f.cst[0].delta;
+    s_ctr[0] = f.st->pass_ctr;
+    s_ctr[1] = f.st->stream_pos;
+  }
   const int b0 = __ldg(f.blk_begin), b1 = __ldg(f.blk_begin + 1);
   const int nch = f.nchunks;
   for (int i = warp; i < f.nslots; i += kFinSmallWarps) {
@@ -665,7 +685,7 @@ __global__ void __launch_bounds__(kFinSmallWarps * 32) finalize_small_kernel(Fin
     }
   }
   __syncthreads();
-  finalize_combine<true>(f, s_tot);
+  finalize_combine<true>(f, s_tot, s_pre, s_ctr);
 }
 
 // kFinWarps warps per block, one level-1 item per warp.  One block: level 2
