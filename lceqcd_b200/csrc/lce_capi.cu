@@ -314,6 +314,7 @@ void enq_begin(lce_ctx* c, const std::vector<unsigned char>& routines, int measf
   f.chunk_begin = c->chunks_begin_d[ti];
   f.chunks = c->chunks_d;
   f.nchunks = c->chunks[ti].back();
+  f.ntiles0 = c->tiles[ti][1];
   q.soff = 0;
   q.poff = 0;
   q.slot = 0;
@@ -433,6 +434,7 @@ int enqueue_persistent(lce_ctx* c, const std::vector<unsigned char>& routines, i
   f.chunk_begin = c->chunks_begin_d[1];
   f.chunks = c->chunks_d;
   f.nchunks = c->chunks[1].back();
+  f.ntiles0 = c->tiles[1][1];
   unsigned long long soff = 0;
   unsigned int poff = 0;
   int slot = 0;

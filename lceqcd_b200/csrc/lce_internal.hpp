@@ -158,6 +158,7 @@ struct FinalizeArgs {
   const int* chunk_begin;
   double* chunks;                 // [chunk][kMaxSlots][kNQ]
   int nchunks;
+  int ntiles0;                    // tiles of chain 0 (= blk_begin[1]), for the single-chain kernel
   unsigned char kinds[kMaxSlots];
 };
 

@@ -625,7 +625,7 @@ __global__ void __launch_bounds__(kFinSmallWarps * 32) finalize_small_kernel(Fin
     s_ctr[0] = f.st->pass_ctr;
     s_ctr[1] = f.st->stream_pos;
   }
-  const int b0 = __ldg(f.blk_begin), b1 = __ldg(f.blk_begin + 1);
+  const int b0 = 0, b1 = f.ntiles0;  // chain 0's tiles, from the host (no load before the first batch)
   const int nch = f.nchunks;
   for (int i = warp; i < f.nslots; i += kFinSmallWarps) {
     const double2* part = reinterpret_cast<const double2*>(f.part + (size_t)i * f.slot_stride);
