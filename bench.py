@@ -435,8 +435,8 @@ def extras(args, peak):
                                              "per-site contractions, 3 per step",
                                      "judge_rule": "the warm start's judge takes, of the identity, the previous "
                                                    "transform and the network's start, the one with the highest "
-                                                   "gauge functional, not the lowest theta as the north star words "
-                                                   "it: the previous transform starts at a worse theta (~7 against "
+                                                   "gauge functional rather than the lowest theta: the previous "
+                                                   "transform starts at a worse theta (~7 against "
                                                    "~4.5 from G = 1) yet converges in 1.3-2x fewer iterations; the "
                                                    "plain iteration then runs to theta < limit_or from the start "
                                                    "taken"}

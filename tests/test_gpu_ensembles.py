@@ -2,8 +2,8 @@
 path: plaquette, <Tr A0^2>, Polyakov loop and the Tr A0^2 slice correlator
 agree within autocorrelation-corrected errors.  These are the secondary
 comparisons (many observables, forms and precisions), held to |z| < 3 so
-that the suite of them is not flaky; the north star's 2-sigma comparison of
-the production ensembles with the reference's CPU ensembles is
+that the suite of them is not flaky; the 2-sigma comparison of the
+production ensembles with the reference's CPU ensembles is
 tests/test_gpu_reference_ensembles.py.  The z-scores are printed."""
 import os
 

@@ -16,7 +16,7 @@ f/confget.f:295-307):
 each as R = 4 independent chains (Philox keys fixed below, different on the
 two sides), 300 thermalisation and 3000 measurement sweeps per chain.
 
-Compared, as the north star names them: the plaquette, <Tr A0^2>, the
+Compared: the plaquette, <Tr A0^2>, the
 Polyakov loop (root of f/polyakov.f's first output, the squared slice mean of
 cos(4|A0|)), and the correlator masses: the effective mass log(C(1)/C(2)) of
 the zero-momentum A0 and link correlators of f/correlator.f, every 10th
