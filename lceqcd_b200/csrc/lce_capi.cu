@@ -264,6 +264,46 @@ void expand(unsigned char kind, std::vector<Pass>& out) {
   }
 }
 
+}  // namespace
+
+// The finalize combine's routine groups.  A scan over the slots in order adds
+// each slot's totals to the accumulator of its class (Higgs: ahiggs1-3;
+// links: agauge, agauge1, link overrelaxation) and, at a slot flagged as the
+// end of a routine, normalises the accumulator and clears it.  Group g is
+// the set of slots such a scan adds before the g-th end (in slot order), so
+// that groups can be summed and normalised independently.  Flags: the last
+// Higgs group (a2, a4, akin are written by every Higgs group, the last
+// one's stay), the last group of each kind ({agauge, agauge1} share plaq and
+// acc_gauge), the ahiggs1 groups.
+void lce::fin_groups(FinalizeArgs& f) {
+  std::memset(f.gid, kNoGroup, sizeof(f.gid));
+  std::memset(f.gflags, 0, sizeof(f.gflags));
+  std::memset(f.gbeg, 0, sizeof(f.gbeg));
+  std::memset(f.gend, 0, sizeof(f.gend));
+  f.ngroups = 0;
+  f.nmetro = 0;
+  std::vector<int> members[2];
+  int last_higgs = -1, last_kind[6] = {-1, -1, -1, -1, -1, -1};
+  for (int i = 0; i < f.nslots; ++i) {
+    const int kind = f.kinds[i] & 0x7f, cls = kind <= kHiggsMetro ? 0 : 1;
+    members[cls].push_back(i);
+    if (!(f.kinds[i] & kKindEnd)) continue;
+    const int g = f.ngroups++;
+    for (int j : members[cls]) f.gid[j] = (unsigned char)g;
+    f.gbeg[g] = (unsigned char)members[cls].front();
+    f.gend[g] = (unsigned char)i;
+    members[cls].clear();
+    if (kind == kHiggsMetro) f.gflags[g] |= kGrpMetro, ++f.nmetro;
+    if (kind <= kHiggsMetro) last_higgs = g;
+    last_kind[kind == kLinkHB3 ? kLinkHB : kind] = g;
+  }
+  if (last_higgs >= 0) f.gflags[last_higgs] |= kGrpHiggsLast;
+  for (int k = 0; k < 6; ++k)
+    if (last_kind[k] >= 0) f.gflags[last_kind[k]] |= kGrpKindLast;
+}
+
+namespace {
+
 // Queue the passes of the given routines and one finalize kernel.
 // events: optional array receiving an event record after every pass.
 // The passes of a list of routines, queued one at a time: enq_begin plans
@@ -279,7 +319,13 @@ struct Enq {
   unsigned long long soff = 0;
   unsigned int poff = 0;
   int slot = 0;
+  int prev_slot = -1;  // reduction slot of the previous pass, or -1
+  bool rb = false;     // reduce-behind (the 448-thread FP32 kernels)
 };
+
+// reduce-behind blocks of a pass: enough warps for one level-1 item each, at
+// most kReduceBlocks blocks
+constexpr int kReduceBlocks = 64;
 
 // index of the chain table for tiles of bs * spt sites (128, 256 or 512)
 int tile_index(int bs, int spt) {
@@ -318,6 +364,8 @@ void enq_begin(lce_ctx* c, const std::vector<unsigned char>& routines, int measf
   q.soff = 0;
   q.poff = 0;
   q.slot = 0;
+  q.prev_slot = -1;
+  q.rb = bs == 448 && spt == 1 && c->prec == LCE_PREC_F32;
 }
 
 int enq_pass(lce_ctx* c, Enq& q, size_t i) {
@@ -349,14 +397,24 @@ int enq_pass(lce_ctx* c, Enq& q, size_t i) {
   // later passes follow pass kernels of this queue only
   a.rng_early = i > 0 ? 1 : 0;
   a.trigger_late = i == 0 ? 1 : 0;
+  // level 1 of the previous pass's slot in extra blocks of this launch
+  a.ntiles = nblocks;
+  int grid = nblocks;
+  if (q.rb && q.prev_slot >= 0) {
+    a.rb_slot = q.prev_slot;
+    a.rb_nitems = q.f.nchunks;
+    const int wpb = q.bs / 32;
+    grid += std::min(kReduceBlocks, (a.rb_nitems + wpb - 1) / wpb);
+  }
   if (ps.kind <= kHiggsMetro) {
-    if (c->prec == LCE_PREC_F64) launch_higgs<double>(ps.kind, a, nblocks, c->stream);
-    else launch_higgs<float>(ps.kind, a, nblocks, c->stream);
+    if (c->prec == LCE_PREC_F64) launch_higgs<double>(ps.kind, a, grid, c->stream);
+    else launch_higgs<float>(ps.kind, a, grid, c->stream);
   } else {
     const int mode = ps.kind == kLinkHB ? 0 : (ps.kind == kLinkOR ? 1 : 2);
-    if (c->prec == LCE_PREC_F64) launch_link<double>(mode, ps.mu, a, nblocks, c->stream);
-    else launch_link<float>(mode, ps.mu, a, nblocks, c->stream);
+    if (c->prec == LCE_PREC_F64) launch_link<double>(mode, ps.mu, a, grid, c->stream);
+    else launch_link<float>(mode, ps.mu, a, grid, c->stream);
   }
+  q.prev_slot = reduce ? q.slot : -1;
   if (reduce) {
     q.f.kinds[q.slot] = (unsigned char)(ps.kind | (ps.end ? kKindEnd : 0));
     ++q.slot;
@@ -370,6 +428,9 @@ int enq_end(lce_ctx* c, Enq& q) {
   q.f.nslots = q.slot;
   q.f.npasses = q.poff;
   q.f.nstream = c->rng == LCE_RNG_STREAM ? q.soff : 0;
+  // reduce-behind: every slot but the last pass's was summed by the pass after it
+  q.f.pre = !q.rb ? 0 : (q.prev_slot >= 0 ? q.slot - 1 : q.slot);
+  fin_groups(q.f);
   launch_finalize(q.f, c->stream);
   CK(cudaGetLastError());
   return LCE_OK;
@@ -456,6 +517,8 @@ int enqueue_persistent(lce_ctx* c, const std::vector<unsigned char>& routines, i
   f.nslots = slot;
   f.npasses = poff;
   f.nstream = c->rng == LCE_RNG_STREAM ? soff : 0;
+  f.pre = 0;
+  fin_groups(f);
   a.bar = c->bar_d;
   a.ntiles = c->blk.back();
   a.npasses = (int)passes.size();
@@ -824,6 +887,17 @@ lce_ctx* create_impl(const lce_params* p, int n, const SlabInfo* slab = nullptr)
     return bail(e, "cudaMalloc(partials)");
   if ((e = cudaMalloc(&c->totals_d, sizeof(double) * (size_t)n * kMaxSlots * kNQ)) != cudaSuccess)
     return bail(e, "cudaMalloc(totals)");
+  {
+    // the reduce-behind blocks' buffers (the 448-site tile table)
+    CtxState st{};
+    st.rb_part = c->part_d;
+    st.rb_slot_stride = c->slot_stride;
+    st.rb_chunk_begin = c->chunks_begin_d[tile_index(448, 1)];
+    st.rb_chunks = c->chunks_d;
+    st.rb_totals = c->totals_d;
+    if ((e = cudaMemcpy(c->st_d, &st, sizeof(st), cudaMemcpyHostToDevice)) != cudaSuccess)
+      return bail(e, "cudaMemcpy(state)");
+  }
   c->scratch_n = (size_t)2 * ceil_div(2L * c->max_nh, 256) + (size_t)32 * c->max_L3 + 64;
   if ((e = cudaMalloc(&c->scratch_d, sizeof(double) * c->scratch_n)) != cudaSuccess)
     return bail(e, "cudaMalloc(scratch)");

@@ -68,6 +68,14 @@ struct CtxState {
   unsigned long long stream_pos;  // validation-stream position
   unsigned int status;            // LCE_STATUS_* bits
   unsigned int ticket;            // last-block ticket of the finalize kernel
+  // the buffers of the reduce-behind blocks (lce_update.cu), set at context
+  // creation: tile partials (slot i at rb_part + i * rb_slot_stride), the
+  // chunk table of the 448-site tiles, chunk sums and totals
+  const double* rb_part;
+  unsigned long long rb_slot_stride;
+  const int* rb_chunk_begin;
+  double* rb_chunks;
+  double* rb_totals;
 };
 
 // per-chain mutable state
@@ -137,6 +145,13 @@ struct PassArgs {
   // kernel's wait (the first pass of a queue, so that no later pass can read
   // the counters while an earlier finalize still writes them).
   int rng_early, trigger_late;
+  // reduce-behind: blocks [ntiles, gridDim.x) of a per-pass launch sum the
+  // previous pass's tile partials (slot rb_slot; the buffers in *st) into
+  // level-1 chunk sums (lce_update.cu), the same additions in the same order
+  // as the finalize kernel's level 1, while this pass's tiles update sites;
+  // rb_nitems = 0: no previous slot.  (Three ints here: a larger argument
+  // block changed the register allocation of the 64-register kernels.)
+  int ntiles, rb_slot, rb_nitems;
 };
 
 struct FinalizeArgs {
@@ -159,8 +174,21 @@ struct FinalizeArgs {
   double* chunks;                 // [chunk][kMaxSlots][kNQ]
   int nchunks;
   int ntiles0;                    // tiles of chain 0 (= blk_begin[1]), for the single-chain kernel
+  // slots [0, pre) were summed to level-1 chunk sums by the pass after
+  // theirs (reduce-behind); the finalize does level 1 of [pre, nslots) only
+  int pre;
   unsigned char kinds[kMaxSlots];
+  // the combine's routine groups (fin_groups), numbered by their last slot:
+  // gid[i] = the group slot i belongs to (kNoGroup: none); gflags[g]:
+  // kGrpHiggsLast (the last Higgs group: a2, a4, akin), kGrpKindLast (the
+  // last group of its kind, or of {agauge, agauge1}: the kind's own
+  // fields), kGrpMetro (an ahiggs1 group)
+  // gbeg[g] / gend[g]: the first and the last slot of group g
+  int ngroups, nmetro;
+  unsigned char gid[kMaxSlots], gflags[kMaxSlots], gbeg[kMaxSlots], gend[kMaxSlots];
 };
+enum : unsigned char { kGrpHiggsLast = 1, kGrpKindLast = 2, kGrpMetro = 4, kNoGroup = 0xff };
+void fin_groups(FinalizeArgs& f);
 
 struct PersistArgs {
   PassArgs base;          // per-pass fields (eo, part, offsets) are filled in the kernel

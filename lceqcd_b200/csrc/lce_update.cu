@@ -387,31 +387,6 @@ __device__ __forceinline__ void link_tile(const PassArgs& p, int tile) {
   }
 }
 
-// Tile shape: BS threads per block, SPT sites per thread (1, or 2 for the
-// LCE_SWEEP_PASSES2 form), and OCC resident threads per SM the register cap
-// is set for: OCC = 0 keeps the cap of min_blocks<R>() blocks of kBlock
-// threads (64 registers in FP32); OCC = 1152 is nine blocks of 128 (56).
-template <typename R, int BS, int OCC>
-constexpr int min_blocks_bs() {
-  return OCC ? OCC / BS : (min_blocks<R>() * kBlock / BS > 0 ? min_blocks<R>() * kBlock / BS : 1);
-}
-
-template <typename R, int MODE, int SPT, int BS, int OCC = 0>
-__global__ void __launch_bounds__(BS, min_blocks_bs<R, BS, OCC>()) higgs_kernel(PassArgs p) {
-  higgs_tile<R, MODE, true, SPT, BS>(p, blockIdx.x);
-}
-
-template <typename R, int MU, int OR, int SPT, int BS, int OCC = 0>
-__global__ void __launch_bounds__(BS, min_blocks_bs<R, BS, OCC>()) link_kernel(PassArgs p) {
-  link_tile<R, MU, OR, true, 1, SPT, BS>(p, blockIdx.x);
-}
-
-// f/agauge1.f (3 hits)
-template <typename R, int MU, int SPT, int BS, int OCC = 0>
-__global__ void __launch_bounds__(BS, min_blocks_bs<R, BS, OCC>()) link3_kernel(PassArgs p) {
-  link_tile<R, MU, 0, true, 3, SPT, BS>(p, blockIdx.x);
-}
-
 // ------------------------------------------------------------------ finalize
 // The partial sums of a reduction slot (kNQ doubles per tile) are added in two
 // fixed levels, so the order of every FP64 addition depends only on the tile
@@ -424,7 +399,10 @@ __global__ void __launch_bounds__(BS, min_blocks_bs<R, BS, OCC>()) link3_kernel(
 //            ... in order, same tree.  A one-chunk chain's level-1 sum is its
 //            total.
 // One (chunk, slot) or (chain, slot) item per warp; the loads of four tiles
-// (or chunk sums) are issued together before their in-order adds.
+// (or chunk sums) are issued together before their in-order adds.  In the
+// per-pass form level 1 of a pass's slot is done by extra blocks of the next
+// pass (reduce-behind), so the finalize kernel is left with level 1 of the
+// last pass's slot, level 2 and the combine.
 __device__ __forceinline__ void warp_tree(double (&v)[kNQ]) {
 #pragma unroll
   for (int q = 0; q < kNQ; ++q) {
@@ -462,20 +440,77 @@ __device__ __forceinline__ void strided_sum(const double2* base, size_t stride, 
   warp_tree(v);
 }
 
-// level 1, item w = (chunk g over all chains, slot i)
-__device__ __forceinline__ void finalize_chunk_warp(const FinalizeArgs& f, int w) {
-  const int g = w / f.nslots, i = w % f.nslots;
-  const int c = f.nchains > 1 ? find_chain(f.chunk_begin, f.nchains, g) : 0;
-  const int t0 = __ldg(f.blk_begin + c) + (g - __ldg(f.chunk_begin + c)) * kChunkTiles;
-  const int t1 = min(__ldg(f.blk_begin + c + 1), t0 + kChunkTiles);
+// level 1 of slot i (partials at part_i), item g = chunk g over all chains:
+// the chunk's sum goes to the chain's total when the chain is one chunk,
+// else to chunks[g][i]
+__device__ __forceinline__ void level1_item(const double* part_i, const int* blk_begin, const int* chunk_begin,
+                                            int nchains, int g, int i, double* chunks, double* totals) {
+  const int c = nchains > 1 ? find_chain(chunk_begin, nchains, g) : 0;
+  const int t0 = __ldg(blk_begin + c) + (g - __ldg(chunk_begin + c)) * kChunkTiles;
+  const int t1 = min(__ldg(blk_begin + c + 1), t0 + kChunkTiles);
   double v[kNQ];
-  strided_sum(reinterpret_cast<const double2*>(f.part + (size_t)i * f.slot_stride), 2, t0, t1, v);
+  strided_sum(reinterpret_cast<const double2*>(part_i), 2, t0, t1, v);
   if ((threadIdx.x & 31) == 0) {
-    const bool one = __ldg(f.chunk_begin + c + 1) - __ldg(f.chunk_begin + c) == 1;
-    double* dst = one ? f.totals + ((size_t)c * kMaxSlots + i) * kNQ : f.chunks + ((size_t)g * kMaxSlots + i) * kNQ;
+    const bool one = __ldg(chunk_begin + c + 1) - __ldg(chunk_begin + c) == 1;
+    double* dst = one ? totals + ((size_t)c * kMaxSlots + i) * kNQ : chunks + ((size_t)g * kMaxSlots + i) * kNQ;
 #pragma unroll
     for (int q = 0; q < kNQ; ++q) dst[q] = v[q];
   }
+}
+
+// level 1, item w = (chunk g over all chains, slot pre + w % (nslots - pre))
+__device__ __forceinline__ void finalize_chunk_warp(const FinalizeArgs& f, int w) {
+  const int nrem = f.nslots - f.pre;
+  const int g = w / nrem, i = f.pre + w % nrem;
+  level1_item(f.part + (size_t)i * f.slot_stride, f.blk_begin, f.chunk_begin, f.nchains, g, i, f.chunks, f.totals);
+}
+
+// The reduce-behind blocks of a per-pass launch (blockIdx.x >= p.ntiles):
+// after the wait the previous pass has completed, and its slot's level-1
+// items are spread over these blocks' warps.
+__device__ __forceinline__ void reduce_behind(const PassArgs& p) {
+  pdl_trigger();
+  pdl_wait();
+  const int nw = (int)(blockDim.x >> 5);
+  const int nred = ((int)gridDim.x - p.ntiles) * nw;
+  const CtxState& st = *p.st;
+  const double* part = st.rb_part + (size_t)p.rb_slot * st.rb_slot_stride;
+  for (int g = ((int)blockIdx.x - p.ntiles) * nw + (int)(threadIdx.x >> 5); g < p.rb_nitems; g += nred)
+    level1_item(part, p.blk_begin, st.rb_chunk_begin, p.nchains, g, p.rb_slot, st.rb_chunks, st.rb_totals);
+}
+
+// Reduce-behind blocks are compiled into the 448-thread kernels only: the
+// 64-register kernels sit at their register cap, and the extra branch made
+// some of them spill (8 bytes, the 128-thread link passes 5% slower at 128^3).
+template <int BS>
+constexpr bool kReduceBehind = BS == 448;
+
+// Tile shape: BS threads per block, SPT sites per thread (1, or 2 for the
+// LCE_SWEEP_PASSES2 form), and OCC resident threads per SM the register cap
+// is set for: OCC = 0 keeps the cap of min_blocks<R>() blocks of kBlock
+// threads (64 registers in FP32); OCC = 1152 is nine blocks of 128 (56).
+template <typename R, int BS, int OCC>
+constexpr int min_blocks_bs() {
+  return OCC ? OCC / BS : (min_blocks<R>() * kBlock / BS > 0 ? min_blocks<R>() * kBlock / BS : 1);
+}
+
+template <typename R, int MODE, int SPT, int BS, int OCC = 0>
+__global__ void __launch_bounds__(BS, min_blocks_bs<R, BS, OCC>()) higgs_kernel(PassArgs p) {
+  if (kReduceBehind<BS> && p.rb_nitems && (int)blockIdx.x >= p.ntiles) reduce_behind(p);
+  else higgs_tile<R, MODE, true, SPT, BS>(p, blockIdx.x);
+}
+
+template <typename R, int MU, int OR, int SPT, int BS, int OCC = 0>
+__global__ void __launch_bounds__(BS, min_blocks_bs<R, BS, OCC>()) link_kernel(PassArgs p) {
+  if (kReduceBehind<BS> && p.rb_nitems && (int)blockIdx.x >= p.ntiles) reduce_behind(p);
+  else link_tile<R, MU, OR, true, 1, SPT, BS>(p, blockIdx.x);
+}
+
+// f/agauge1.f (3 hits)
+template <typename R, int MU, int SPT, int BS, int OCC = 0>
+__global__ void __launch_bounds__(BS, min_blocks_bs<R, BS, OCC>()) link3_kernel(PassArgs p) {
+  if (kReduceBehind<BS> && p.rb_nitems && (int)blockIdx.x >= p.ntiles) reduce_behind(p);
+  else link_tile<R, MU, 0, true, 3, SPT, BS>(p, blockIdx.x);
 }
 
 // level 2, item w = (chain c, slot i); nothing to do for a one-chunk chain
@@ -491,24 +526,41 @@ __device__ __forceinline__ void finalize_chain_warp(const FinalizeArgs& f, int w
   }
 }
 
-// Per chain, in slot order, the reference's normalisations; then advance the
-// RNG counters.  Run by one block after every finalize_sum has completed.
-// One warp per chain: each lane loads two slots' totals (kMaxSlots = 64), all
-// loads in flight at once (L2, the sums of other blocks), then the in-order
-// scan over the slots reads them from the lanes by shuffles -- one L2 round
-// trip per chain instead of one per slot.
+// The combine's slot tables in shared memory, copied by the finalize kernels
+// before their wait, while the previous pass still runs.
+struct FinTables {
+  unsigned char kinds[kMaxSlots], gid[kMaxSlots], gflags[kMaxSlots], gbeg[kMaxSlots], gend[kMaxSlots];
+};
+__device__ __forceinline__ void load_tables(const FinalizeArgs& f, FinTables& T) {
+  for (int i = threadIdx.x; i < kMaxSlots; i += blockDim.x) {
+    T.kinds[i] = f.kinds[i];
+    T.gid[i] = f.gid[i];
+    T.gflags[i] = f.gflags[i];
+    T.gbeg[i] = f.gbeg[i];
+    T.gend[i] = f.gend[i];
+  }
+}
+
+// Per chain the reference's normalisations of the slot totals, then the RNG
+// counters advance.  Run by one block after every total is complete, one
+// warp per chain.  The routine groups (fin_groups) are independent: lane j
+// sums the slots of groups j and j + 32 in slot order, and the divisions of
+// the normalisations (up to four per group) run one per lane, lane 4 g' + d
+// taking division d of group g = g' + 8 r, so that they overlap instead of
+// following one another.  The additions and divisions are those of a scan
+// over the slots in order, and each field is written by the last group that
+// sets it.  Only the ahiggs1 step adaptation runs as a chain over the
+// ahiggs1 groups in order.
 // SM: a single chain whose totals are in shared memory (stot) instead of
 // f.totals, with its volume, ahiggs1 step and RNG counters loaded at the
-// kernel's start (pre = {2 nh, delta}, ctr = {pass_ctr, stream_pos}): no
-// dependent global load is left for the combine.
+// kernel's start (pre = {2 nh, delta}, ctr = {pass_ctr, stream_pos}).
 template <bool SM = false>
-__device__ __forceinline__ void finalize_combine(const FinalizeArgs& f, const double* stot = nullptr,
+__device__ __forceinline__ void finalize_combine(const FinalizeArgs& f, const FinTables& T, const double* stot = nullptr,
                                                  const double* pre = nullptr, const unsigned long long* ctr = nullptr) {
-  static_assert(kMaxSlots <= 64, "two slots per lane");
+  static_assert(kMaxSlots <= 64, "two slots (groups) per lane");
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarps = (int)(blockDim.x >> 5);
   for (int c = warp; c < f.nchains; c += nwarps) {
     const double V = SM ? pre[0] : 2.0 * f.chains[c].nh;
-    double delta = SM ? pre[1] : 0.0;  // the ahiggs1 step as the combine leaves it (SM)
     const double* base = SM ? stot : f.totals + (size_t)c * kMaxSlots * kNQ;
     double t0[kNQ], t1[kNQ];
     bool bad = false;
@@ -521,73 +573,105 @@ __device__ __forceinline__ void finalize_combine(const FinalizeArgs& f, const do
     }
     if (__any_sync(0xffffffffu, bad) && lane == 0) atomicOr(&f.st->status, kStatusNaN);
     lce_meas& m = f.meas[c];
-    double h[kNQ] = {0, 0, 0, 0}, l[kNQ] = {0, 0, 0, 0};
-    for (int i = 0; i < f.nslots; ++i) {
-      double t[kNQ];
+    // the group sums: lane j, groups j (hs[0]) and j + 32 (hs[1])
+    double hs[2][kNQ] = {{0, 0, 0, 0}, {0, 0, 0, 0}};
+    if (SM) {
 #pragma unroll
-      for (int q = 0; q < kNQ; ++q) t[q] = __shfl_sync(0xffffffffu, i < 32 ? t0[q] : t1[q], i & 31);
-      const int kind = f.kinds[i] & 0x7f;
-      const bool end = (f.kinds[i] & kKindEnd) != 0;
-      if (kind <= kHiggsMetro) {
-        for (int q = 0; q < kNQ; ++q) h[q] += t[q];
-        if (end) {
-          if (lane == 0) {
-            // f/ahiggs2.f:142-147 (same in ahiggs1/3)
-            m.a2 = h[1] / V;
-            m.a4 = h[2] / V;
-            m.akin = h[3] / (6.0 * V);
-            const double acc = h[0] / V;
-            if (kind == kHiggsHB) m.acc_hb = acc;
-            if (kind == kHiggsOR) m.acc_or = acc;
-            if (kind == kHiggsMetro) {
-              // f/ahiggs1.f:113-123 step adaptation, in the build's precision
-              const double d0 = SM ? delta : f.cst[c].delta;
-              if (f.single) {
-                float a = (float)h[0] / (float)V, d = (float)d0;
-                if (fabsf(a - 0.5f) > 0.1f) d = (a > 0.5f) ? 1.1131241f * d : 0.8989669f * d;
-                m.acc_metro = a;
-                delta = d;
-              } else {
-                double d = d0;
-                if (fabs(acc - 0.5) > 0.1) d = (acc > 0.5) ? 1.1131241 * d : 0.8989669 * d;
-                m.acc_metro = acc;
-                delta = d;
-              }
-              f.cst[c].delta = delta;
-              m.delta = delta;
-            }
-          }
-          h[0] = h[1] = h[2] = h[3] = 0;
+      for (int s = 0; s < 2; ++s) {
+        const int g = lane + 32 * s;
+        if (g >= f.ngroups) continue;
+        for (int i = T.gbeg[g]; i <= T.gend[g]; ++i) {
+          if (T.gid[i] != g) continue;
+#pragma unroll
+          for (int q = 0; q < kNQ; ++q) hs[s][q] += stot[i * kNQ + q];
         }
-      } else if (kind == kLinkHB) {
-        for (int q = 0; q < kNQ; ++q) l[q] += t[q];
-        if (end) {
-          if (lane == 0) {
-            // f/agauge.f:195-200
-            m.plaq = l[2] / (12.0 * V);
-            m.acc_gauge = (l[0] / (3.0 * V)) * (l[1] / (12.0 * V));
-          }
-          l[0] = l[1] = l[2] = l[3] = 0;
-        }
-      } else if (kind == kLinkHB3) {
-        for (int q = 0; q < kNQ; ++q) l[q] += t[q];
-        if (end) {
-          if (lane == 0) {
-            // f/agauge1.f:227-232: the Metropolis count is divided by the 3 hits
-            m.plaq = l[2] / (12.0 * V);
-            m.acc_gauge = (l[0] / (3.0 * V)) * (l[1] / (12.0 * V) / 3.0);
-          }
-          l[0] = l[1] = l[2] = l[3] = 0;
-        }
-      } else if (kind == kLinkOR) {
-        for (int q = 0; q < kNQ; ++q) l[q] += t[q];
-        if (end) {
-          if (lane == 0) m.acc_link_or = l[0] / (3.0 * V);
-          l[0] = l[1] = l[2] = l[3] = 0;
+      }
+    } else {
+      // warp-uniform scan: slot i's totals by shuffle, added by its group's lane
+      for (int i = 0; i < f.nslots; ++i) {
+        const int g = T.gid[i];
+        double t[kNQ];
+#pragma unroll
+        for (int q = 0; q < kNQ; ++q) t[q] = __shfl_sync(0xffffffffu, i < 32 ? t0[q] : t1[q], i & 31);
+        if (g == kNoGroup || lane != (g & 31)) continue;
+#pragma unroll
+        for (int q = 0; q < kNQ; ++q) {
+          if (g < 32) hs[0][q] += t[q];
+          else hs[1][q] += t[q];
         }
       }
     }
-    if (lane == 0) m.delta = SM ? delta : f.cst[c].delta;
+    // the normalisations, one division per lane
+    for (int g0 = 0; g0 < f.ngroups; g0 += 8) {
+      const int g = g0 + (lane >> 2), d = lane & 3;
+      double h[kNQ];
+#pragma unroll
+      for (int q = 0; q < kNQ; ++q) {
+        const double x0 = __shfl_sync(0xffffffffu, hs[0][q], g & 31), x1 = __shfl_sync(0xffffffffu, hs[1][q], g & 31);
+        h[q] = g < 32 ? x0 : x1;
+      }
+      const int kind = g < f.ngroups ? (T.kinds[T.gend[g]] & 0x7f) : -1;
+      const unsigned fl = g < f.ngroups ? T.gflags[g] : 0u;
+      const bool higgs = kind >= 0 && kind <= kHiggsMetro, link = kind == kLinkHB || kind == kLinkHB3;
+      // f/ahiggs2.f:142-147 (same in ahiggs1/3): a2 = h1/V, a4 = h2/V, akin = h3/(6V), acc = h0/V;
+      // f/agauge.f:195-200: plaq = l2/(12V), acc = (l0/(3V)) (l1/(12V)); f/agauge1.f:227-232
+      // divides the Metropolis factor by the 3 hits; link overrelaxation: l0/(3V)
+      double num = 1.0, den = 1.0;
+      if (higgs) {
+        num = d == 0 ? h[1] : (d == 1 ? h[2] : (d == 2 ? h[3] : h[0]));
+        den = d == 2 ? 6.0 * V : V;
+      } else if (link) {
+        num = d == 0 ? h[2] : (d == 1 ? h[0] : h[1]);
+        den = d == 1 ? 3.0 * V : 12.0 * V;
+      } else if (kind == kLinkOR) {
+        num = h[0];
+        den = 3.0 * V;
+      }
+      double r = num / den;
+      if (kind == kLinkHB3 && d == 2) r = r / 3.0;
+      const double r2 = __shfl_down_sync(0xffffffffu, r, 1);  // division d + 1 of the same group
+      if (higgs) {
+        if (fl & kGrpHiggsLast) {
+          if (d == 0) m.a2 = r;
+          if (d == 1) m.a4 = r;
+          if (d == 2) m.akin = r;
+        }
+        if ((fl & kGrpKindLast) && d == 3) {
+          if (kind == kHiggsHB) m.acc_hb = r;
+          if (kind == kHiggsOR) m.acc_or = r;
+        }
+      } else if (link) {
+        if (fl & kGrpKindLast) {
+          if (d == 0) m.plaq = r;
+          if (d == 1) m.acc_gauge = r * r2;
+        }
+      } else if (kind == kLinkOR) {
+        if ((fl & kGrpKindLast) && d == 0) m.acc_link_or = r;
+      }
+    }
+    // f/ahiggs1.f:113-123 step adaptation after each ahiggs1 group, in order,
+    // in the build's precision
+    double delta = SM ? pre[1] : f.cst[c].delta;
+    if (f.nmetro) {
+      for (int g = 0; g < f.ngroups; ++g) {
+        if (!(T.gflags[g] & kGrpMetro)) continue;
+        const double h0 = __shfl_sync(0xffffffffu, g < 32 ? hs[0][0] : hs[1][0], g & 31);
+        if (f.single) {
+          float a = (float)h0 / (float)V, dl = (float)delta;
+          if (fabsf(a - 0.5f) > 0.1f) dl = (a > 0.5f) ? 1.1131241f * dl : 0.8989669f * dl;
+          if (lane == 0 && (T.gflags[g] & kGrpKindLast)) m.acc_metro = a;
+          delta = dl;
+        } else {
+          const double a = h0 / V;
+          double dl = delta;
+          if (fabs(a - 0.5) > 0.1) dl = (a > 0.5) ? 1.1131241 * dl : 0.8989669 * dl;
+          if (lane == 0 && (T.gflags[g] & kGrpKindLast)) m.acc_metro = a;
+          delta = dl;
+        }
+      }
+      if (lane == 0) f.cst[c].delta = delta;
+    }
+    if (lane == 0) m.delta = delta;
   }
   __syncthreads();
   if (threadIdx.x == 0) {
@@ -601,91 +685,80 @@ __device__ __forceinline__ void finalize_combine(const FinalizeArgs& f, const do
   }
 }
 
-// One block for a single chain of at most kSmallChunks chunks: warp w takes
-// the slots w, w + kFinSmallWarps, ... whole -- the loads of two chunks at a
-// time, level 1 of each chunk, level 2 across the chunks in registers (chunk
-// k's sum goes to lane k mod 32, added in chunk order), the same additions in
-// the same order as the two-level kernel below -- and the combine reads the
-// totals from shared memory: one global round trip per two chunks instead of
-// three for the whole reduction.
+// One block for a single chain of at most kSmallChunks chunks, everything
+// after the wait in one global round trip: warp w < (nslots - pre) * nch
+// sums chunk w % nch of slot pre + w / nch (level 1, to shared memory) while
+// the block loads the chunk sums of the slots [0, pre) that the passes
+// summed behind; level 2 per slot (lane k holds chunk k, the fixed tree) and
+// the combine then read shared memory.  Same additions, same order as the
+// two-level kernel below.
 constexpr int kFinSmallWarps = 16;
 constexpr int kSmallChunks = 8;
 __global__ void __launch_bounds__(kFinSmallWarps * 32) finalize_small_kernel(FinalizeArgs f) {
-  pdl_trigger();
-  pdl_wait();
   __shared__ double s_tot[kMaxSlots * kNQ];
+  __shared__ double s_ck[kMaxSlots * kSmallChunks * kNQ];  // [slot][chunk][q]
   __shared__ double s_pre[2];
   __shared__ unsigned long long s_ctr[2];
+  __shared__ FinTables T;
+  pdl_trigger();
+  // before the wait: the slot tables, and the combine's inputs other than the
+  // totals -- the volume, and the ahiggs1 step and the RNG counters, which
+  // only an earlier queue's finalize writes (it completed before this
+  // queue's first pass went past its wait)
+  load_tables(f, T);
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-  // the combine's inputs other than the totals, loaded by the last warp (idle
-  // unless there are more slots than warps) while the others sum
-  if (warp == kFinSmallWarps - 1 && lane == 0) {
+  if (threadIdx.x == kFinSmallWarps * 32 - 1) {
     s_pre[0] = 2.0 * f.chains[0].nh;
     s_pre[1] = f.cst[0].delta;
     s_ctr[0] = f.st->pass_ctr;
     s_ctr[1] = f.st->stream_pos;
   }
-  const int b0 = 0, b1 = f.ntiles0;  // chain 0's tiles, from the host (no load before the first batch)
-  const int nch = f.nchunks;
-  for (int i = warp; i < f.nslots; i += kFinSmallWarps) {
-    const double2* part = reinterpret_cast<const double2*>(f.part + (size_t)i * f.slot_stride);
-    double acc[kNQ] = {0.0, 0.0, 0.0, 0.0}, tot[kNQ] = {0.0, 0.0, 0.0, 0.0};
-    for (int k0 = 0; k0 < nch; k0 += 2) {
-      double2 x[2][4][2];
+  pdl_wait();
+  const int nch = f.nchunks, b1 = f.ntiles0;  // chain 0's chunks and tiles, from the host
+  // chunk sums summed behind: one chunk -> the total, else chunks[k][i]
+  // (the slots [0, pre) of one chunk are pre * kNQ consecutive doubles)
+  if ((int)threadIdx.x < f.pre * kNQ) {
+    const int i = threadIdx.x / kNQ, q = threadIdx.x % kNQ;
 #pragma unroll
-      for (int kk = 0; kk < 2; ++kk) {
-        const int t0 = b0 + (k0 + kk) * kChunkTiles, t1 = min(b1, t0 + kChunkTiles);
-#pragma unroll
-        for (int j = 0; j < 4; ++j) {
-          const int t = t0 + lane + 32 * j;
-          const bool ok = k0 + kk < nch && t < t1;
-          x[kk][j][0] = ok ? __ldcg(part + (size_t)t * 2) : make_double2(0.0, 0.0);
-          x[kk][j][1] = ok ? __ldcg(part + (size_t)t * 2 + 1) : make_double2(0.0, 0.0);
-        }
-      }
-#pragma unroll
-      for (int kk = 0; kk < 2; ++kk) {
-        const int k = k0 + kk;
-        if (k >= nch) break;
-        const int t0 = b0 + k * kChunkTiles, t1 = min(b1, t0 + kChunkTiles);
-        double v[kNQ] = {0.0, 0.0, 0.0, 0.0};
-#pragma unroll
-        for (int j = 0; j < 4; ++j) {
-          if (t0 + lane + 32 * j < t1) {
-            v[0] += x[kk][j][0].x;
-            v[1] += x[kk][j][0].y;
-            v[2] += x[kk][j][1].x;
-            v[3] += x[kk][j][1].y;
-          }
-        }
-        warp_tree(v);
-        if (nch == 1) {
-#pragma unroll
-          for (int q = 0; q < kNQ; ++q) tot[q] = v[q];
-        } else {
-#pragma unroll
-          for (int q = 0; q < kNQ; ++q) {
-            const double b = __shfl_sync(0xffffffffu, v[q], 0);
-            if (lane == (k & 31)) acc[q] += b;
-          }
-        }
-      }
+    for (int k = 0; k < kSmallChunks; ++k) {
+      if (k < nch)
+        s_ck[(i * kSmallChunks + k) * kNQ + q] =
+            nch == 1 ? __ldcg(f.totals + threadIdx.x) : __ldcg(f.chunks + (size_t)k * kMaxSlots * kNQ + threadIdx.x);
     }
-    if (nch > 1) {
-      warp_tree(acc);
+  }
+  // level 1 of the remaining slots
+  for (int w = warp; w < (f.nslots - f.pre) * nch; w += kFinSmallWarps) {
+    const int i = f.pre + w / nch, k = w % nch;
+    const int t0 = k * kChunkTiles, t1 = min(b1, t0 + kChunkTiles);
+    double v[kNQ];
+    strided_sum(reinterpret_cast<const double2*>(f.part + (size_t)i * f.slot_stride), 2, t0, t1, v);
+    if (lane == 0) {
 #pragma unroll
-      for (int q = 0; q < kNQ; ++q) tot[q] = acc[q];
+      for (int q = 0; q < kNQ; ++q) s_ck[(i * kSmallChunks + k) * kNQ + q] = v[q];
+    }
+  }
+  __syncthreads();
+  // level 2: lane k adds chunk k to zero, then the tree (a one-chunk chain's
+  // level-1 sum is its total)
+  for (int i = warp; i < f.nslots; i += kFinSmallWarps) {
+    double v[kNQ];
+#pragma unroll
+    for (int q = 0; q < kNQ; ++q) v[q] = nch == 1 || lane < nch ? s_ck[(i * kSmallChunks + (nch == 1 ? 0 : lane)) * kNQ + q] : 0.0;
+    if (nch > 1) {
+#pragma unroll
+      for (int q = 0; q < kNQ; ++q) v[q] = 0.0 + v[q];
+      warp_tree(v);
     }
     if (lane == 0) {
 #pragma unroll
       for (int q = 0; q < kNQ; ++q) {
-        s_tot[i * kNQ + q] = tot[q];
-        f.totals[(size_t)i * kNQ + q] = tot[q];
+        s_tot[i * kNQ + q] = v[q];
+        f.totals[(size_t)i * kNQ + q] = v[q];
       }
     }
   }
   __syncthreads();
-  finalize_combine<true>(f, s_tot, s_pre, s_ctr);
+  finalize_combine<true>(f, T, s_tot, s_pre, s_ctr);
 }
 
 // kFinWarps warps per block, one level-1 item per warp.  One block: level 2
@@ -694,10 +767,12 @@ __global__ void __launch_bounds__(kFinSmallWarps * 32) finalize_small_kernel(Fin
 // level 1, by an atomic ticket, does level 2 and the combine.
 constexpr int kFinWarps = 32;
 __global__ void __launch_bounds__(kFinWarps * 32) finalize_kernel(FinalizeArgs f) {
+  __shared__ FinTables T;
   pdl_trigger();
+  load_tables(f, T);
   pdl_wait();
   const int warp = (int)(threadIdx.x >> 5);
-  const int n1 = f.nchunks * f.nslots;
+  const int n1 = f.nchunks * (f.nslots - f.pre);
   for (int w = blockIdx.x * kFinWarps + warp; w < n1; w += gridDim.x * kFinWarps) finalize_chunk_warp(f, w);
   if (gridDim.x > 1) {
     __shared__ bool last;
@@ -717,7 +792,7 @@ __global__ void __launch_bounds__(kFinWarps * 32) finalize_kernel(FinalizeArgs f
     for (int w = warp; w < f.nchains * f.nslots; w += kFinWarps) finalize_chain_warp(f, w);
     __syncthreads();
   }
-  finalize_combine(f);
+  finalize_combine(f, T);
   if (gridDim.x > 1 && threadIdx.x == 0) f.st->ticket = 0;
 }
 
@@ -821,7 +896,10 @@ __global__ void __launch_bounds__(kBlock, kPersistMinBlocks) sweep_persistent_ke
   }
   if (!grid_sync(a.bar, gridDim.x, target, &a.base.st->status)) return;
   if (blockIdx.x == 0) {
-    finalize_combine(a.fin);
+    __shared__ FinTables T;
+    load_tables(a.fin, T);
+    __syncthreads();
+    finalize_combine(a.fin, T);
     // every block has passed the last barrier: record where the count stands
     if (threadIdx.x == 0) *(volatile unsigned*)&a.bar->base = target;
   }
