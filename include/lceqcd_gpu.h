@@ -100,7 +100,9 @@ typedef struct lce_params {
   unsigned long long seed;  /* Philox key */
   int device;            /* CUDA device ordinal */
   int n_link_or;         /* link overrelaxation hits per lce_sweep (0: reference composition) */
-  int n_higgs_metro;     /* ahiggs1 calls per lce_sweep (0: reference composition) */
+  int n_higgs_metro;     /* ahiggs1 calls per lce_sweep (0: reference composition); the calls of
+                            one sweep share the step in force at its start, and the step is
+                            adapted after each call's acceptance, in order, at the sweep's end */
   double delta0;         /* initial ahiggs1 step */
   int gf_angle;          /* gauge-fixing rotation angle: LCE_GF_ACOS (the
                             reference, f/or_gauge_fixing1.f:174) or LCE_GF_ATAN2 */

@@ -504,6 +504,70 @@ def test_tile_shapes_batch_of_uneven_volumes():
             np.testing.assert_array_equal(o[i][1], outs[0][i][1])
 
 
+MEAS_KEYS = ("plaq", "akin", "a2", "a4", "acc_gauge", "acc_hb", "acc_or", "acc_metro", "acc_link_or")
+
+
+@pytest.mark.parametrize("L", [(64, 64, 64), (96, 64, 48)])
+def test_reduce_behind_multichunk(L):
+    """The 448-thread kernels sum each pass's tile partials in extra blocks of
+    the next pass (reduce-behind), and the finalize combines routine groups
+    in parallel lanes.  At these volumes a slot spans 3 chunks of 128 tiles
+    (448 threads), 2 (512), 8 or 9 (128: the single-chain and the multi-block
+    finalize kernels), and the persistent form sums everything in its own
+    kernel.  Two ahiggs1 calls and a link-overrelaxation hit per sweep make
+    five routine groups (the step adaptation runs as a chain over two of
+    them); measflag 0 sweeps leave slots for the ahiggs1 passes only.  Every
+    form updates every site identically and advances the RNG and the ahiggs1
+    step identically; the measurements agree to the FP64 rounding of their
+    different tile groupings."""
+    res = []
+    for bs, mode in ((448, "passes"), (128, "passes"), (512, "passes"), (256, "persistent")):
+        g = Lattice(L, beta=9.0, x=0.1, y=0.45, seed=31, sweep_mode=mode, tile_threads=bs if mode == "passes" else 0,
+                    n_link_or=1, n_higgs_metro=2, delta0=2.0)
+        g.init_hot(12)
+        ms = []
+        for mf in (1, 0, 1, 1, 0, 1):
+            g.sweeps(1, mf)
+            if mf:
+                ms.append(g.meas1())
+        assert g.sweep_mode() == mode
+        res.append((g.download(), ms, g.rng_position()))
+        g.close()
+    (u0, a0), ms0, pos0 = res[0]
+    for (u, a), ms, pos in res[1:]:
+        np.testing.assert_array_equal(u, u0)
+        np.testing.assert_array_equal(a, a0)
+        assert pos == pos0
+        for m0, m1 in zip(ms0, ms):
+            assert m0["delta"] == m1["delta"]
+            for k in MEAS_KEYS:
+                assert abs(m0[k] - m1[k]) <= 1e-12 * max(1.0, abs(m0[k])), k
+    # the step moved: the acceptance of the two ahiggs1 calls was adapted to
+    assert ms0[-1]["delta"] != 2.0
+
+
+def test_reduce_behind_batch_of_multichunk_chains():
+    """A batch whose chains span several chunks each: the reduce-behind
+    blocks take the level-1 items of every chain, the multi-block finalize
+    the rest.  448-thread tiles against 128-thread tiles."""
+    specs = [Params(L=(64, 64, 64), beta=6.0, x=0.1, y=0.1, seed=5, n_link_or=1, n_higgs_metro=1),
+             Params(L=(80, 64, 40), beta=16.0, x=0.08, y=0.5, seed=6, imode=1, n_link_or=1, n_higgs_metro=1),
+             Params(L=(8, 12, 6), beta=9.0, x=0.1, y=0.3, seed=7, n_link_or=1, n_higgs_metro=1)]
+    outs = []
+    for bs in (448, 128):
+        ens = Ensemble([Params(**{**s.__dict__, "sweep_mode": "passes", "tile_threads": bs}) for s in specs])
+        ens.init_hot(3)
+        ens.sweeps(3, 1)
+        outs.append(([ens.download(chain=i) for i in range(3)], ens.meas_batch()))
+        ens.close()
+    for i in range(3):
+        np.testing.assert_array_equal(outs[1][0][i][0], outs[0][0][i][0])
+        np.testing.assert_array_equal(outs[1][0][i][1], outs[0][0][i][1])
+    for m0, m1 in zip(outs[0][1], outs[1][1]):
+        for k in MEAS_KEYS:
+            assert abs(m0[k] - m1[k]) <= 1e-12 * max(1.0, abs(m0[k])), k
+
+
 def test_autotune_chooses_form_and_tile_shape():
     """LCE_SWEEP_AUTO times every candidate (per-pass forms at each tile
     shape, and the persistent form) on real sweeps and keeps one; with
