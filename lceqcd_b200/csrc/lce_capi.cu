@@ -320,7 +320,7 @@ struct Enq {
   unsigned int poff = 0;
   int slot = 0;
   int prev_slot = -1;  // reduction slot of the previous pass, or -1
-  bool rb = false;     // reduce-behind (the 448-thread FP32 kernels)
+  bool rb = false;     // reduce-behind (the one-site-per-thread kernels)
 };
 
 // reduce-behind blocks of a pass: enough warps for one level-1 item each, at
@@ -365,7 +365,7 @@ void enq_begin(lce_ctx* c, const std::vector<unsigned char>& routines, int measf
   q.poff = 0;
   q.slot = 0;
   q.prev_slot = -1;
-  q.rb = bs == 448 && spt == 1 && c->prec == LCE_PREC_F32;
+  q.rb = spt == 1;
 }
 
 int enq_pass(lce_ctx* c, Enq& q, size_t i) {
@@ -401,7 +401,7 @@ int enq_pass(lce_ctx* c, Enq& q, size_t i) {
   a.ntiles = nblocks;
   int grid = nblocks;
   if (q.rb && q.prev_slot >= 0) {
-    a.rb_slot = q.prev_slot;
+    a.rb_slot = q.prev_slot | (tile_index(q.bs, q.spt) << 8);
     a.rb_nitems = q.f.nchunks;
     const int wpb = q.bs / 32;
     grid += std::min(kReduceBlocks, (a.rb_nitems + wpb - 1) / wpb);
@@ -888,11 +888,12 @@ lce_ctx* create_impl(const lce_params* p, int n, const SlabInfo* slab = nullptr)
   if ((e = cudaMalloc(&c->totals_d, sizeof(double) * (size_t)n * kMaxSlots * kNQ)) != cudaSuccess)
     return bail(e, "cudaMalloc(totals)");
   {
-    // the reduce-behind blocks' buffers (the 448-site tile table)
+    // the reduce-behind blocks' buffers
+    static_assert(sizeof(CtxState::rb_chunk_begin) / sizeof(int*) == kTileTables, "one chunk table per tile table");
     CtxState st{};
     st.rb_part = c->part_d;
     st.rb_slot_stride = c->slot_stride;
-    st.rb_chunk_begin = c->chunks_begin_d[tile_index(448, 1)];
+    for (int t = 0; t < kTileTables; ++t) st.rb_chunk_begin[t] = c->chunks_begin_d[t];
     st.rb_chunks = c->chunks_d;
     st.rb_totals = c->totals_d;
     if ((e = cudaMemcpy(c->st_d, &st, sizeof(st), cudaMemcpyHostToDevice)) != cudaSuccess)

@@ -33,7 +33,7 @@ constexpr int kChunkTiles = 128; // tiles per level-1 chunk of the finalize redu
 // the tile sizes (sites) of the per-pass kernels' tile tables: 448 = 14 warps,
 // two blocks per SM, balances a single-wave pass (a 64^3 parity: 293 blocks
 // on 148 SMs, at most 28 warps on an SM against 32 with 512)
-constexpr int kTileTables = 4;
+constexpr int kTileTables = 4;  // (CtxState::rb_chunk_begin has one entry per table)
 constexpr int kTileSites[kTileTables] = {128, 256, 512, 448};
 
 // pass kinds (one kernel launch over one parity)
@@ -70,10 +70,10 @@ struct CtxState {
   unsigned int ticket;            // last-block ticket of the finalize kernel
   // the buffers of the reduce-behind blocks (lce_update.cu), set at context
   // creation: tile partials (slot i at rb_part + i * rb_slot_stride), the
-  // chunk table of the 448-site tiles, chunk sums and totals
+  // chunk table of each tile table, chunk sums and totals
   const double* rb_part;
   unsigned long long rb_slot_stride;
-  const int* rb_chunk_begin;
+  const int* rb_chunk_begin[4];
   double* rb_chunks;
   double* rb_totals;
 };
@@ -146,11 +146,12 @@ struct PassArgs {
   // the counters while an earlier finalize still writes them).
   int rng_early, trigger_late;
   // reduce-behind: blocks [ntiles, gridDim.x) of a per-pass launch sum the
-  // previous pass's tile partials (slot rb_slot; the buffers in *st) into
-  // level-1 chunk sums (lce_update.cu), the same additions in the same order
-  // as the finalize kernel's level 1, while this pass's tiles update sites;
-  // rb_nitems = 0: no previous slot.  (Three ints here: a larger argument
-  // block changed the register allocation of the 64-register kernels.)
+  // previous pass's tile partials (slot rb_slot & 0xff, tile table rb_slot >>
+  // 8; the buffers in *st) into level-1 chunk sums (lce_update.cu), the same
+  // additions in the same order as the finalize kernel's level 1, while this
+  // pass's tiles update sites; rb_nitems = 0: no previous slot.  (Three ints
+  // here: a larger argument block changed the register allocation of the
+  // 64-register kernels.)
   int ntiles, rb_slot, rb_nitems;
 };
 

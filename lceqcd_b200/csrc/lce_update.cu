@@ -474,16 +474,18 @@ __device__ __forceinline__ void reduce_behind(const PassArgs& p) {
   const int nw = (int)(blockDim.x >> 5);
   const int nred = ((int)gridDim.x - p.ntiles) * nw;
   const CtxState& st = *p.st;
-  const double* part = st.rb_part + (size_t)p.rb_slot * st.rb_slot_stride;
+  const int slot = p.rb_slot & 0xff;
+  const double* part = st.rb_part + (size_t)slot * st.rb_slot_stride;
+  const int* chunk_begin = st.rb_chunk_begin[p.rb_slot >> 8];
   for (int g = ((int)blockIdx.x - p.ntiles) * nw + (int)(threadIdx.x >> 5); g < p.rb_nitems; g += nred)
-    level1_item(part, p.blk_begin, st.rb_chunk_begin, p.nchains, g, p.rb_slot, st.rb_chunks, st.rb_totals);
+    level1_item(part, p.blk_begin, chunk_begin, p.nchains, g, slot, st.rb_chunks, st.rb_totals);
 }
 
-// Reduce-behind blocks are compiled into the 448-thread kernels only: the
-// 64-register kernels sit at their register cap, and the extra branch made
-// some of them spill (8 bytes, the 128-thread link passes 5% slower at 128^3).
-template <int BS>
-constexpr bool kReduceBehind = BS == 448;
+// Reduce-behind blocks are compiled into the one-site-per-thread kernels:
+// in the two-sites form, at its 64-register cap, the extra branch made the
+// link kernels spill (56-76 bytes).
+template <int SPT>
+constexpr bool kReduceBehind = SPT == 1;
 
 // Tile shape: BS threads per block, SPT sites per thread (1, or 2 for the
 // LCE_SWEEP_PASSES2 form), and OCC resident threads per SM the register cap
@@ -496,20 +498,20 @@ constexpr int min_blocks_bs() {
 
 template <typename R, int MODE, int SPT, int BS, int OCC = 0>
 __global__ void __launch_bounds__(BS, min_blocks_bs<R, BS, OCC>()) higgs_kernel(PassArgs p) {
-  if (kReduceBehind<BS> && p.rb_nitems && (int)blockIdx.x >= p.ntiles) reduce_behind(p);
+  if (kReduceBehind<SPT> && p.rb_nitems && (int)blockIdx.x >= p.ntiles) reduce_behind(p);
   else higgs_tile<R, MODE, true, SPT, BS>(p, blockIdx.x);
 }
 
 template <typename R, int MU, int OR, int SPT, int BS, int OCC = 0>
 __global__ void __launch_bounds__(BS, min_blocks_bs<R, BS, OCC>()) link_kernel(PassArgs p) {
-  if (kReduceBehind<BS> && p.rb_nitems && (int)blockIdx.x >= p.ntiles) reduce_behind(p);
+  if (kReduceBehind<SPT> && p.rb_nitems && (int)blockIdx.x >= p.ntiles) reduce_behind(p);
   else link_tile<R, MU, OR, true, 1, SPT, BS>(p, blockIdx.x);
 }
 
 // f/agauge1.f (3 hits)
 template <typename R, int MU, int SPT, int BS, int OCC = 0>
 __global__ void __launch_bounds__(BS, min_blocks_bs<R, BS, OCC>()) link3_kernel(PassArgs p) {
-  if (kReduceBehind<BS> && p.rb_nitems && (int)blockIdx.x >= p.ntiles) reduce_behind(p);
+  if (kReduceBehind<SPT> && p.rb_nitems && (int)blockIdx.x >= p.ntiles) reduce_behind(p);
   else link_tile<R, MU, 0, true, 3, SPT, BS>(p, blockIdx.x);
 }
 
