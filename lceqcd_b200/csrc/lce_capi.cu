@@ -1282,7 +1282,7 @@ int slab_sweep(lce_slabs* S, int measflag, lce_meas* m) {
 // slab k's halo (the next half-step's U_f(x - z, z)).  Nothing else crosses
 // a slab boundary.  Theta (the whole lattice's odd sites, before their
 // update) is summed per slab, combined on slab 0's device, and the count and
-// verdict copied to every slab's chain state, all ordered by events: no host
+// stop decision copied to every slab's chain state, all ordered by events: no host
 // round trip inside a batch of iterations.
 // it_flags >= 0: the half-steps of f/it_gauge_fixing.f with these flags
 // (LCE_ITGF_*) instead of the overrelaxed ones
