@@ -385,7 +385,7 @@ __global__ void __launch_bounds__(1024) fa_check_kernel(const ChainDev* chp, Cha
 // CG (with SCALE): the block's sums of |F|^2 / p_c^2 and Re(F^* F_prev) / p_c^2
 // into cgpart, and F kept as the next F_prev
 template <int AX, int SIGN, bool SCALE, int LOGN, bool CG = false>
-__global__ void __launch_bounds__(kFaThreads, SCALE && LOGN <= 8 ? 4 : 1) fa_fft_kernel(FaArgs a) {
+__global__ void __launch_bounds__(kFaThreads, LOGN <= 8 ? 4 : 1) fa_fft_kernel(FaArgs a) {
   using G = FaLines<LOGN>;
   constexpr int n = G::n, ld = G::ld, NL = G::NLT, LNL = kFaBlockLog - LOGN;
   extern __shared__ __align__(16) FftC fa_sm[];
@@ -423,25 +423,34 @@ __global__ void __launch_bounds__(kFaThreads, SCALE && LOGN <= 8 ? 4 : 1) fa_fft
   fft2_lines<LOGN>(d, tw);
   if (CG) {
     // two buffers: a read-modify-write of one stalled every element on its
-    // own load (5x the kernel's time at 128^3)
+    // own load (5x the kernel's time at 128^3).  One pass: the sums with the
+    // weight 1/(4 p^2) = (1/p^2) / 4 (exact), then the element scaled by
+    // gamma / (4 V p^2) = gv (1/p^2) -- one FP64 division per element
     const int par = a.cg->parity;
     FftC* Pn = reinterpret_cast<FftC*>(a.prev) + ((size_t)par * 2 + blockIdx.y) * V;
     const FftC* Po = reinterpret_cast<const FftC*>(a.prev) + ((size_t)(par ^ 1) * 2 + blockIdx.y) * V;
+    const double gv = (a.cst ? a.cst->gf_step : a.gamma) / (4.0 * (double)V);
     double v[2] = {0.0, 0.0};
     for (int e = threadIdx.x; e < NL * n; e += blockDim.x) {
       const int j = e & (NL - 1), k = e >> LNL, l = l0 + j;
+      const int q = j * ld + k;
       if (l >= nlines) continue;
       const size_t gi = nat_index<AX>(a, l, k);
-      const FftC f = d[j * ld + k], pv = __ldg(Po + gi);
+      const FftC f = d[q], pv = __ldg(Po + gi);
       Pn[gi] = f;
-      if ((l | k) == 0) continue;
-      const double m0 = 1.0 / (4.0 * (sxy[j] + sz2[k]));
+      if ((l | k) == 0) {
+        d[q] = FftC{0, 0};
+        continue;
+      }
+      const double r = 1.0 / (sxy[j] + sz2[k]), m0 = 0.25 * r, m = gv * r;
       v[0] += m0 * ((double)f.x * f.x + (double)f.y * f.y);
       v[1] += m0 * ((double)f.x * pv.x + (double)f.y * pv.y);
+      d[q] = FftC{(FftR)(f.x * m), (FftR)(f.y * m)};
     }
     block_reduce_store<2>(v, a.cgpart + 2 * ((size_t)blockIdx.y * gridDim.x + blockIdx.x));
-  }
-  if (SCALE) {
+    __syncthreads();
+    fft2_lines<LOGN>(d, twi);
+  } else if (SCALE) {
     const double gv = (a.cst ? a.cst->gf_step : a.gamma) / (4.0 * (double)V);
     for (int e = threadIdx.x; e < NL * n; e += blockDim.x) {
       const int j = e >> LOGN, kz = e & (n - 1), l = l0 + j;
