@@ -111,7 +111,7 @@ struct lce_ctx {
   std::vector<cudaEvent_t> prof_ev;
   // instantiated sweep graphs by (form, threads per block, sites per thread,
   // register-cap occupancy, measflag)
-  std::map<std::tuple<int, int, int, int, int>, cudaGraphExec_t> sweep_graphs;
+  std::map<std::tuple<int, int, int, int, int, int>, cudaGraphExec_t> sweep_graphs;
   GridBar* bar_d = nullptr;
   int persist_grid = 0;
   int sweep_mode = LCE_SWEEP_AUTO;   // requested
@@ -529,21 +529,29 @@ int enqueue_persistent(lce_ctx* c, const std::vector<unsigned char>& routines, i
 
 constexpr size_t kTuneSamples = 3;
 
-// The instantiated graph of one sweep in the given form (built once per
-// form and measflag).  The persistent form falls back to the per-pass form
-// under LCE_SWEEP_AUTO if it cannot be captured on this device.
-int sweep_graph(lce_ctx* c, int form, int bs, int spt, int occ, int mf, cudaGraphExec_t* out) {
+// Runs of sweeps (lce_sweeps) replay a graph of kSweepsPerGraph sweeps: inside
+// one graph a sweep's first pass launches programmatically behind the
+// previous sweep's finalize (and waits for it before reading the RNG
+// counters), instead of after a graph boundary.
+constexpr int kSweepsPerGraph = 8;
+
+// The instantiated graph of nrep sweeps in the given form (built once per
+// form, measflag and nrep).  The persistent form falls back to the per-pass
+// form under LCE_SWEEP_AUTO if it cannot be captured on this device.
+int sweep_graph(lce_ctx* c, int form, int bs, int spt, int occ, int mf, cudaGraphExec_t* out, int nrep = 1) {
   if (form == LCE_SWEEP_PERSISTENT) bs = kBlock, spt = 1, occ = 0;
-  cudaGraphExec_t* slot = &c->sweep_graphs[std::make_tuple(form, bs, spt, occ, mf)];
+  cudaGraphExec_t* slot = &c->sweep_graphs[std::make_tuple(form, bs, spt, occ, mf, nrep)];
   if (!*slot) {
     cudaGraph_t g;
     CK(cudaStreamBeginCapture(c->stream, cudaStreamCaptureModeThreadLocal));
-    int rc;
-    if (form == LCE_SWEEP_PERSISTENT)
-      rc = c->prec == LCE_PREC_F64 ? enqueue_persistent<double>(c, sweep_routines(c), mf, true)
-                                   : enqueue_persistent<float>(c, sweep_routines(c), mf, true);
-    else
-      rc = enqueue(c, sweep_routines(c), mf, true, nullptr, bs, spt, occ);
+    int rc = LCE_OK;
+    for (int r = 0; r < nrep && rc == LCE_OK; ++r) {
+      if (form == LCE_SWEEP_PERSISTENT)
+        rc = c->prec == LCE_PREC_F64 ? enqueue_persistent<double>(c, sweep_routines(c), mf, true)
+                                     : enqueue_persistent<float>(c, sweep_routines(c), mf, true);
+      else
+        rc = enqueue(c, sweep_routines(c), mf, true, nullptr, bs, spt, occ);
+    }
     const cudaError_t ec = cudaStreamEndCapture(c->stream, &g);
     cudaError_t ei = cudaSuccess;
     if (ec == cudaSuccess) {
@@ -559,7 +567,7 @@ int sweep_graph(lce_ctx* c, int form, int bs, int spt, int occ, int mf, cudaGrap
         c->err = std::string("persistent sweep unavailable: ") + cudaGetErrorString(e);
         c->mode = LCE_SWEEP_PASSES;
         c->tune.clear();
-        return sweep_graph(c, LCE_SWEEP_PASSES, c->tile_bs, c->tile_spt, c->tile_occ, mf, out);
+        return sweep_graph(c, LCE_SWEEP_PASSES, c->tile_bs, c->tile_spt, c->tile_occ, mf, out, nrep);
       }
       return cuda_fail(c, e, "sweep graph capture");
     }
@@ -2140,10 +2148,17 @@ int lce_sweeps(lce_ctx* c, int nsweeps, int measflag) {
         if (int rc = enqueue(c, r, mf, true)) return rc;
       return LCE_OK;
     }
-    cudaGraphExec_t ex;
-    int rc = sweep_graph(c, c->mode, c->tile_bs, c->tile_spt, c->tile_occ, mf, &ex);
-    if (rc) return rc;
-    for (int i = done; i < nsweeps; ++i) CK(cudaGraphLaunch(ex, c->stream));
+    int i = done;
+    if (nsweeps - i >= kSweepsPerGraph) {
+      cudaGraphExec_t exm;
+      if (int rc = sweep_graph(c, c->mode, c->tile_bs, c->tile_spt, c->tile_occ, mf, &exm, kSweepsPerGraph)) return rc;
+      for (; nsweeps - i >= kSweepsPerGraph; i += kSweepsPerGraph) CK(cudaGraphLaunch(exm, c->stream));
+    }
+    if (i < nsweeps) {
+      cudaGraphExec_t ex;
+      if (int rc = sweep_graph(c, c->mode, c->tile_bs, c->tile_spt, c->tile_occ, mf, &ex)) return rc;
+      for (; i < nsweeps; ++i) CK(cudaGraphLaunch(ex, c->stream));
+    }
   }
   return LCE_OK;
 }
@@ -2651,7 +2666,7 @@ int lce_profile_sweep(lce_ctx* c, int measflag, float* ms, int max_passes) {
     CK(cudaEventCreate(&e));
     c->prof_ev.push_back(e);
   }
-  cudaGraphExec_t* slot = &c->sweep_graphs[std::make_tuple(-1, c->tile_bs, c->tile_spt, c->tile_occ, mf)];
+  cudaGraphExec_t* slot = &c->sweep_graphs[std::make_tuple(-1, c->tile_bs, c->tile_spt, c->tile_occ, mf, 1)];
   if (!*slot) {
     cudaGraph_t g;
     CK(cudaStreamBeginCapture(c->stream, cudaStreamCaptureModeThreadLocal));
