@@ -234,9 +234,11 @@ int lce_renorm(lce_ctx* ctx);
  * [link OR x n_link_or], reunitarisation fused into the link writers; one
  * CUDA graph per measflag.  m (chain 0) may be NULL: no synchronisation. */
 int lce_sweep(lce_ctx* ctx, int measflag, lce_meas* m);
-/* nsweeps graph replays without synchronisation (with LCE_SWEEP_AUTO the first
- * sweeps of a context rotate through the forms and tile shapes under CUDA
- * events -- every one of them a real sweep -- and the fastest is kept) */
+/* nsweeps sweeps as graph replays without synchronisation (graphs of 8 sweeps
+ * while nsweeps allows, whose sweeps chain by programmatic launch, then
+ * one-sweep graphs; with LCE_SWEEP_AUTO the first sweeps of a context rotate
+ * through the forms and tile shapes under CUDA events -- every one of them a
+ * real sweep -- and the fastest is kept) */
 int lce_sweeps(lce_ctx* ctx, int nsweeps, int measflag);
 /* the form lce_sweeps uses now (LCE_SWEEP_AUTO while still undecided) */
 int lce_get_sweep_mode(lce_ctx* ctx);
