@@ -71,7 +71,7 @@ extern "C" {
  * cooperative persistent kernel per sweep that loops over the (chain, tile)
  * work list of every pass with a grid barrier in between.  AUTO times the
  * forms -- and, for FP32 contexts, the tile shapes of the per-pass forms
- * (128, 256 or 512 threads per block, see lce_params.tile_threads) -- on the
+ * (128, 256, 448 or 512 threads per block, see lce_params.tile_threads) -- on the
  * first sweeps and keeps the fastest (lce_get_sweep_mode, lce_get_tile_shape). */
 #define LCE_SWEEP_AUTO 0
 #define LCE_SWEEP_PASSES 1
