@@ -568,6 +568,32 @@ def test_reduce_behind_batch_of_multichunk_chains():
             assert abs(m0[k] - m1[k]) <= 1e-12 * max(1.0, abs(m0[k])), k
 
 
+@pytest.mark.parametrize("mode", ["passes", "persistent"])
+def test_multi_sweep_graph_equals_single_sweeps(mode):
+    """lce_sweeps(n) replays graphs of 8 sweeps chained by programmatic
+    launch: 19 sweeps that way (two 8-sweep graphs and three single ones)
+    give the same fields, RNG position and last measurements as 19 single
+    lce_sweep calls, with ahiggs1 (its step adapted after every sweep) and a
+    link-overrelaxation hit in the composition."""
+    res = []
+    for many in (True, False):
+        g = Lattice((16, 16, 16), beta=9.0, x=0.1, y=0.45, seed=17, sweep_mode=mode, n_link_or=1, n_higgs_metro=1,
+                    delta0=3.0)
+        g.init_hot(4)
+        if many:
+            g.sweeps(19, 1)
+        else:
+            for _ in range(19):
+                g.sweep(1)
+        res.append((g.download(), g.meas1(), g.rng_position()))
+        g.close()
+    (u0, a0), m0, r0 = res[0]
+    (u1, a1), m1, r1 = res[1]
+    np.testing.assert_array_equal(u0, u1)
+    np.testing.assert_array_equal(a0, a1)
+    assert r0 == r1 and m0 == m1
+
+
 def test_autotune_chooses_form_and_tile_shape():
     """LCE_SWEEP_AUTO times every candidate (per-pass forms at each tile
     shape, and the persistent form) on real sweeps and keeps one; with
