@@ -317,14 +317,16 @@ inline cudaError_t launch_pdl(void (*kern)(KArgs...), dim3 grid, dim3 block, siz
 // ------------------------------------------------------------------ reductions
 // Block partials of NC event counts (reduced as 32-bit integers) and ND FP64
 // sums; out[0..NC) = counts, out[NC..NC+ND) = sums, out[NC+ND..NQ) = 0.
-template <int NC, int ND, int NQ>
+// REUSE: the block calls it more than once (the persistent form's tile loop),
+// so the shared slots are first waited free.
+template <int NC, int ND, int NQ, bool REUSE = true>
 __device__ __forceinline__ void block_reduce_cs(const unsigned (&cnt)[NC > 0 ? NC : 1], double (&v)[ND > 0 ? ND : 1],
                                                 double* out) {
   static_assert(NC + ND <= NQ, "too many partials");
   __shared__ unsigned redc[32][NC > 0 ? NC : 1];
   __shared__ double redd[32][ND > 0 ? ND : 1];
   const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
-  __syncthreads();  // a previous call's readers are done with the shared slots
+  if (REUSE) __syncthreads();  // a previous call's readers are done with the shared slots
   unsigned cw[NC > 0 ? NC : 1];
 #pragma unroll
   for (int q = 0; q < NC; ++q) cw[q] = __reduce_add_sync(0xffffffffu, cnt[q]);

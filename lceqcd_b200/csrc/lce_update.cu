@@ -282,7 +282,7 @@ __device__ __forceinline__ void higgs_tile(const PassArgs& p, int tile) {
     }
   }
   // partials {accepted, sum rho, sum rho^2, sum a.F}
-  if (p.part) block_reduce_cs<1, 3, kNQ>(acc, q, p.part + (size_t)tile * kNQ);
+  if (p.part) block_reduce_cs<1, 3, kNQ, !PDL>(acc, q, p.part + (size_t)tile * kNQ);
 }
 
 // ------------------------------------------------------------------ links
@@ -378,11 +378,11 @@ __device__ __forceinline__ void link_tile(const PassArgs& p, int tile) {
   }
   // partials {KP accepted, Metropolis accepted, sum plaquette} / {OR accepted}
   if (p.part) {
-    if constexpr (!OR) block_reduce_cs<2, 1, kNQ>(cnt, pl, p.part + (size_t)tile * kNQ);
+    if constexpr (!OR) block_reduce_cs<2, 1, kNQ, !PDL>(cnt, pl, p.part + (size_t)tile * kNQ);
     else {
       unsigned c1[1] = {cnt[0]};
       double d0[1] = {0.0};
-      block_reduce_cs<1, 0, kNQ>(c1, d0, p.part + (size_t)tile * kNQ);
+      block_reduce_cs<1, 0, kNQ, !PDL>(c1, d0, p.part + (size_t)tile * kNQ);
     }
   }
 }
