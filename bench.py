@@ -311,6 +311,30 @@ def extras(args, peak):
             lat.close()
         except Exception as e:  # a secondary number must not take the headline down
             out[key] = {"error": repr(e)[:300]}
+    # a production run of the headline workload: sweeps back to back through
+    # lce_sweeps (graphs of 8 sweeps), measurements on every sweep as in the
+    # reference's main loop, one event pair around 160 sweeps, no L2 flush
+    try:
+        lat = Lattice(L_MAIN, **COUP, precision="f32", seed=1000)
+        lat.init_hot(2000)
+        settle(lat)
+        lat.sweeps(16, 1)
+        res = {}
+        for mf in (1, 0):
+            lat.synchronize()
+            lat.timer_start()
+            lat.sweeps(160, mf)
+            ms = lat.timer_stop() / 160
+            res["measured" if mf else "unmeasured"] = {"us_per_sweep": 1e3 * ms,
+                                                       "site_updates_per_s": vol(L_MAIN) / (ms / 1e3)}
+        out["production_64cubed"] = {**res, "sweep_mode": lat.sweep_mode(),
+                                     "tile_shape": list(lat.tile_shape(registers=True)),
+                                     "timing": "CUDA events around 160 back-to-back sweeps (lce_sweeps), no L2 "
+                                               "flush; measured: measflag 1 on every sweep (f/main.f's production "
+                                               "loop), unmeasured: measflag 0 (its thermalisation loop)"}
+        lat.close()
+    except Exception as e:
+        out["production_64cubed"] = {"error": repr(e)[:300]}
     # Landau gauge fixing of thermalised 128^3 configurations (10 sweeps
     # apart) to theta < 1e-10: the reference's method (overrelaxation from
     # G = 1), the same iteration from the previous configuration's converged
