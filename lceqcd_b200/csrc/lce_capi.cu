@@ -321,6 +321,11 @@ struct Enq {
   int slot = 0;
   int prev_slot = -1;  // reduction slot of the previous pass, or -1
   bool rb = false;     // reduce-behind (the one-site-per-thread kernels)
+  // graphs of several sweeps (sweep_graph): the previous sweep's finalize,
+  // run by an extra block of this queue's first pass; defer_out: leave this
+  // queue's finalize in f for the next queue instead of launching it
+  const FinalizeArgs* defer_in = nullptr;
+  bool defer_out = false;
 };
 
 // reduce-behind blocks of a pass: enough warps for one level-1 item each, at
@@ -333,8 +338,10 @@ int tile_index(int bs, int spt) {
   return t == 128 ? 0 : (t == 256 ? 1 : (t == 512 ? 2 : 3));
 }
 
+// poff0, soff0: the queue's RNG offsets from the counters' values (nonzero
+// for the later sweeps of a graph of several sweeps)
 void enq_begin(lce_ctx* c, const std::vector<unsigned char>& routines, int measflag, bool fuse_renorm, int bs,
-               int spt, int occ, Enq& q) {
+               int spt, int occ, Enq& q, unsigned int poff0 = 0, unsigned long long soff0 = 0) {
   const int ti = tile_index(bs, spt);
   q.blk = &c->tiles[ti];
   q.blk_d = c->tiles_d[ti];
@@ -361,8 +368,8 @@ void enq_begin(lce_ctx* c, const std::vector<unsigned char>& routines, int measf
   f.chunks = c->chunks_d;
   f.nchunks = c->chunks[ti].back();
   f.ntiles0 = c->tiles[ti][1];
-  q.soff = 0;
-  q.poff = 0;
+  q.soff = soff0;
+  q.poff = poff0;
   q.slot = 0;
   q.prev_slot = -1;
   q.rb = spt == 1;
@@ -406,7 +413,12 @@ int enq_pass(lce_ctx* c, Enq& q, size_t i) {
     const int wpb = q.bs / 32;
     grid += std::min(kReduceBlocks, (a.rb_nitems + wpb - 1) / wpb);
   }
-  if (ps.kind <= kHiggsMetro) {
+  if (i == 0 && q.defer_in) {
+    // the previous sweep's finalize in one extra block (sweep_graph checked
+    // that this pass is ahiggs2 with one site per thread and no reduce-behind)
+    if (c->prec == LCE_PREC_F64) launch_higgs_fin<double>(a, *q.defer_in, grid + 1, c->stream);
+    else launch_higgs_fin<float>(a, *q.defer_in, grid + 1, c->stream);
+  } else if (ps.kind <= kHiggsMetro) {
     if (c->prec == LCE_PREC_F64) launch_higgs<double>(ps.kind, a, grid, c->stream);
     else launch_higgs<float>(ps.kind, a, grid, c->stream);
   } else {
@@ -431,6 +443,13 @@ int enq_end(lce_ctx* c, Enq& q) {
   // reduce-behind: every slot but the last pass's was summed by the pass after it
   q.f.pre = !q.rb ? 0 : (q.prev_slot >= 0 ? q.slot - 1 : q.slot);
   fin_groups(q.f);
+  if (q.defer_out) {
+    // run by the next queue's first pass; inside a graph of sweeps the
+    // counters advance at its last finalize only
+    q.f.npasses = 0;
+    q.f.nstream = 0;
+    return LCE_OK;
+  }
   launch_finalize(q.f, c->stream);
   CK(cudaGetLastError());
   return LCE_OK;
@@ -529,6 +548,43 @@ int enqueue_persistent(lce_ctx* c, const std::vector<unsigned char>& routines, i
 
 constexpr size_t kTuneSamples = 3;
 
+// Graphs of several sweeps defer each sweep's finalize (but the last) into an
+// extra block of the next sweep's first pass (higgs_fin_kernel): a single
+// chain of at most 8 chunks (the single-chain finalize), the per-pass form
+// with one site per thread and a tile shape that kernel is compiled for.
+bool sweeps_defer_finalize(const lce_ctx* c, int form, int bs, int spt, int occ) {
+  if (form != LCE_SWEEP_PASSES || spt != 1 || occ != 0 || c->nchains != 1) return false;
+  if (c->chunks[tile_index(bs, spt)].back() > 8) return false;
+  return c->prec == LCE_PREC_F64 ? bs == 256 : (bs == 128 || bs == 256 || bs == 448 || bs == 512);
+}
+
+// nrep sweeps with deferred finalizes: sweep r's passes take the RNG offsets
+// r x (one sweep's advance) from the counters, which only the last sweep's
+// finalize advances (by nrep sweeps' worth)
+int enqueue_sweeps_deferred(lce_ctx* c, int nrep, int mf, int bs) {
+  const std::vector<unsigned char> r = sweep_routines(c);
+  std::vector<Pass> passes;
+  for (unsigned char k : r) expand(k, passes);
+  unsigned int per = 0;
+  unsigned long long nst = 0;
+  for (const Pass& ps : passes) {
+    per += philox_passes(ps.kind);
+    nst += (unsigned long long)nslots_of(ps.kind) * (c->stream_nh ? c->stream_nh : c->ch[0].nh);
+  }
+  FinalizeArgs prev;
+  for (int k = 0; k < nrep; ++k) {
+    Enq q;
+    q.defer_in = k > 0 ? &prev : nullptr;
+    q.defer_out = k < nrep - 1;
+    enq_begin(c, r, mf, true, bs, 1, 0, q, per * (unsigned)k, nst * (unsigned long long)k);
+    for (size_t i = 0; i < q.passes.size(); ++i)
+      if (int rc = enq_pass(c, q, i)) return rc;
+    if (int rc = enq_end(c, q)) return rc;
+    if (q.defer_out) prev = q.f;
+  }
+  return LCE_OK;
+}
+
 // Runs of sweeps (lce_sweeps) replay a graph of kSweepsPerGraph sweeps: inside
 // one graph a sweep's first pass launches programmatically behind the
 // previous sweep's finalize (and waits for it before reading the RNG
@@ -545,13 +601,15 @@ int sweep_graph(lce_ctx* c, int form, int bs, int spt, int occ, int mf, cudaGrap
     cudaGraph_t g;
     CK(cudaStreamBeginCapture(c->stream, cudaStreamCaptureModeThreadLocal));
     int rc = LCE_OK;
-    for (int r = 0; r < nrep && rc == LCE_OK; ++r) {
-      if (form == LCE_SWEEP_PERSISTENT)
-        rc = c->prec == LCE_PREC_F64 ? enqueue_persistent<double>(c, sweep_routines(c), mf, true)
-                                     : enqueue_persistent<float>(c, sweep_routines(c), mf, true);
-      else
-        rc = enqueue(c, sweep_routines(c), mf, true, nullptr, bs, spt, occ);
-    }
+    if (nrep > 1 && sweeps_defer_finalize(c, form, bs, spt, occ)) rc = enqueue_sweeps_deferred(c, nrep, mf, bs);
+    else
+      for (int r = 0; r < nrep && rc == LCE_OK; ++r) {
+        if (form == LCE_SWEEP_PERSISTENT)
+          rc = c->prec == LCE_PREC_F64 ? enqueue_persistent<double>(c, sweep_routines(c), mf, true)
+                                       : enqueue_persistent<float>(c, sweep_routines(c), mf, true);
+        else
+          rc = enqueue(c, sweep_routines(c), mf, true, nullptr, bs, spt, occ);
+      }
     const cudaError_t ec = cudaStreamEndCapture(c->stream, &g);
     cudaError_t ei = cudaSuccess;
     if (ec == cudaSuccess) {

@@ -212,6 +212,10 @@ void launch_higgs(int mode, const PassArgs& a, int nblocks, cudaStream_t s);
 template <typename R>
 void launch_link(int mode, int mu, const PassArgs& a, int nblocks, cudaStream_t s);
 void launch_finalize(const FinalizeArgs& f, cudaStream_t s);
+// a sweep's first pass (ahiggs2, eo 0) with one extra block running the
+// previous sweep's single-chain finalize fp (graphs of several sweeps)
+template <typename R>
+void launch_higgs_fin(const PassArgs& a, const FinalizeArgs& fp, int nblocks, cudaStream_t s);
 template <typename R>
 void launch_renorm(void* u, size_t nlinks, cudaStream_t s);
 template <typename R>

@@ -676,7 +676,7 @@ __device__ __forceinline__ void finalize_combine(const FinalizeArgs& f, const Fi
     if (lane == 0) m.delta = delta;
   }
   __syncthreads();
-  if (threadIdx.x == 0) {
+  if (threadIdx.x == 0 && (f.npasses || f.nstream)) {
     if (SM) {
       f.st->pass_ctr = ctr[0] + f.npasses;
       f.st->stream_pos = ctr[1] + f.nstream;
@@ -696,26 +696,32 @@ __device__ __forceinline__ void finalize_combine(const FinalizeArgs& f, const Fi
 // two-level kernel below.
 constexpr int kFinSmallWarps = 16;
 constexpr int kSmallChunks = 8;
-__global__ void __launch_bounds__(kFinSmallWarps * 32) finalize_small_kernel(FinalizeArgs f) {
-  __shared__ double s_tot[kMaxSlots * kNQ];
-  __shared__ double s_ck[kMaxSlots * kSmallChunks * kNQ];  // [slot][chunk][q]
-  __shared__ double s_pre[2];
-  __shared__ unsigned long long s_ctr[2];
-  __shared__ FinTables T;
-  pdl_trigger();
-  // before the wait: the slot tables, and the combine's inputs other than the
-  // totals -- the volume, and the ahiggs1 step and the RNG counters, which
-  // only an earlier queue's finalize writes (it completed before this
-  // queue's first pass went past its wait)
-  load_tables(f, T);
-  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-  if (threadIdx.x == kFinSmallWarps * 32 - 1) {
-    s_pre[0] = 2.0 * f.chains[0].nh;
-    s_pre[1] = f.cst[0].delta;
-    s_ctr[0] = f.st->pass_ctr;
-    s_ctr[1] = f.st->stream_pos;
+struct SmallFinSmem {
+  double tot[kMaxSlots * kNQ];
+  double ck[kMaxSlots * kSmallChunks * kNQ];  // [slot][chunk][q]
+  double pre[2];
+  unsigned long long ctr[2];
+  FinTables T;
+};
+// The single-chain finalize, run by one block of any number of warps: the
+// finalize_small_kernel block, or the block a sweep's first pass carries for
+// the previous sweep (DEFERRED: called after the caller's wait; the RNG
+// counters are then left alone when f.npasses and f.nstream are 0).
+template <bool DEFERRED>
+__device__ __forceinline__ void finalize_small_body(const FinalizeArgs& f, SmallFinSmem& S) {
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarps = (int)(blockDim.x >> 5);
+  // the slot tables, and the combine's inputs other than the totals -- the
+  // volume, and the ahiggs1 step and the RNG counters, which only an earlier
+  // finalize writes (before the wait in the finalize kernel: that finalize
+  // completed before this queue's first pass went past its wait)
+  load_tables(f, S.T);
+  if ((int)threadIdx.x == (int)blockDim.x - 1) {
+    S.pre[0] = 2.0 * f.chains[0].nh;
+    S.pre[1] = f.cst[0].delta;
+    S.ctr[0] = f.st->pass_ctr;
+    S.ctr[1] = f.st->stream_pos;
   }
-  pdl_wait();
+  if (!DEFERRED) pdl_wait();
   const int nch = f.nchunks, b1 = f.ntiles0;  // chain 0's chunks and tiles, from the host
   // chunk sums summed behind: one chunk -> the total, else chunks[k][i]
   // (the slots [0, pre) of one chunk are pre * kNQ consecutive doubles)
@@ -724,28 +730,29 @@ __global__ void __launch_bounds__(kFinSmallWarps * 32) finalize_small_kernel(Fin
 #pragma unroll
     for (int k = 0; k < kSmallChunks; ++k) {
       if (k < nch)
-        s_ck[(i * kSmallChunks + k) * kNQ + q] =
+        S.ck[(i * kSmallChunks + k) * kNQ + q] =
             nch == 1 ? __ldcg(f.totals + threadIdx.x) : __ldcg(f.chunks + (size_t)k * kMaxSlots * kNQ + threadIdx.x);
     }
   }
   // level 1 of the remaining slots
-  for (int w = warp; w < (f.nslots - f.pre) * nch; w += kFinSmallWarps) {
+  for (int w = warp; w < (f.nslots - f.pre) * nch; w += nwarps) {
     const int i = f.pre + w / nch, k = w % nch;
     const int t0 = k * kChunkTiles, t1 = min(b1, t0 + kChunkTiles);
     double v[kNQ];
     strided_sum(reinterpret_cast<const double2*>(f.part + (size_t)i * f.slot_stride), 2, t0, t1, v);
     if (lane == 0) {
 #pragma unroll
-      for (int q = 0; q < kNQ; ++q) s_ck[(i * kSmallChunks + k) * kNQ + q] = v[q];
+      for (int q = 0; q < kNQ; ++q) S.ck[(i * kSmallChunks + k) * kNQ + q] = v[q];
     }
   }
   __syncthreads();
   // level 2: lane k adds chunk k to zero, then the tree (a one-chunk chain's
   // level-1 sum is its total)
-  for (int i = warp; i < f.nslots; i += kFinSmallWarps) {
+  for (int i = warp; i < f.nslots; i += nwarps) {
     double v[kNQ];
 #pragma unroll
-    for (int q = 0; q < kNQ; ++q) v[q] = nch == 1 || lane < nch ? s_ck[(i * kSmallChunks + (nch == 1 ? 0 : lane)) * kNQ + q] : 0.0;
+    for (int q = 0; q < kNQ; ++q)
+      v[q] = nch == 1 || lane < nch ? S.ck[(i * kSmallChunks + (nch == 1 ? 0 : lane)) * kNQ + q] : 0.0;
     if (nch > 1) {
 #pragma unroll
       for (int q = 0; q < kNQ; ++q) v[q] = 0.0 + v[q];
@@ -754,13 +761,40 @@ __global__ void __launch_bounds__(kFinSmallWarps * 32) finalize_small_kernel(Fin
     if (lane == 0) {
 #pragma unroll
       for (int q = 0; q < kNQ; ++q) {
-        s_tot[i * kNQ + q] = v[q];
+        S.tot[i * kNQ + q] = v[q];
         f.totals[(size_t)i * kNQ + q] = v[q];
       }
     }
   }
   __syncthreads();
-  finalize_combine<true>(f, T, s_tot, s_pre, s_ctr);
+  finalize_combine<true>(f, S.T, S.tot, S.pre, S.ctr);
+}
+
+__global__ void __launch_bounds__(kFinSmallWarps * 32) finalize_small_kernel(FinalizeArgs f) {
+  __shared__ SmallFinSmem S;
+  pdl_trigger();
+  finalize_small_body<false>(f, S);
+}
+
+// The first pass (ahiggs2, eo 0) of a sweep inside a graph of several
+// sweeps, with one extra block that runs the previous sweep's finalize (fp):
+// its inputs -- the other slots' chunk sums and the last pass's partials --
+// are not overwritten before this pass completes (the next pass's
+// reduce-behind blocks write slot 0's chunk sums), and the RNG counters are
+// not advanced inside such a graph (each sweep's passes take fixed offsets
+// from its start; the graph's last finalize advances them), so the finalize
+// runs beside this pass's tiles instead of between the sweeps.
+template <typename R, int BS>
+__global__ void __launch_bounds__(BS, min_blocks_bs<R, BS, 0>())
+    higgs_fin_kernel(PassArgs p, const __grid_constant__ FinalizeArgs fp) {
+  if ((int)blockIdx.x >= p.ntiles) {
+    __shared__ SmallFinSmem S;
+    pdl_wait();
+    pdl_trigger();
+    finalize_small_body<true>(fp, S);
+  } else {
+    higgs_tile<R, 0, true, 1, BS>(p, blockIdx.x);
+  }
 }
 
 // kFinWarps warps per block, one level-1 item per warp.  One block: level 2
@@ -1020,6 +1054,29 @@ void launch_link(int mode, int mu, const PassArgs& a, int nblocks, cudaStream_t 
   if (a.spt == 2) launch_link_t<R, 2, 256>(mode, mu, a, nblocks, s);
   else launch_link_t<R, 1, 256>(mode, mu, a, nblocks, s);
 }
+
+// the first pass of a sweep carrying the previous sweep's finalize (one site
+// per thread, 128 (64 registers), 256, 448 or 512 threads in FP32; 256 in FP64)
+template <typename R>
+void launch_higgs_fin(const PassArgs& a, const FinalizeArgs& fp, int nblocks, cudaStream_t s) {
+  if constexpr (sizeof(R) == 4) {
+    if (a.bs == 128) {
+      (void)launch_pdl(higgs_fin_kernel<R, 128>, nblocks, 128, 0, s, a, fp);
+      return;
+    }
+    if (a.bs == 448) {
+      (void)launch_pdl(higgs_fin_kernel<R, 448>, nblocks, 448, 0, s, a, fp);
+      return;
+    }
+    if (a.bs == 512) {
+      (void)launch_pdl(higgs_fin_kernel<R, 512>, nblocks, 512, 0, s, a, fp);
+      return;
+    }
+  }
+  (void)launch_pdl(higgs_fin_kernel<R, 256>, nblocks, 256, 0, s, a, fp);
+}
+template void launch_higgs_fin<float>(const PassArgs&, const FinalizeArgs&, int, cudaStream_t);
+template void launch_higgs_fin<double>(const PassArgs&, const FinalizeArgs&, int, cudaStream_t);
 
 void launch_finalize(const FinalizeArgs& f, cudaStream_t s) {
   if (f.nchains == 1 && f.nchunks <= kSmallChunks) {

@@ -568,18 +568,29 @@ def test_reduce_behind_batch_of_multichunk_chains():
             assert abs(m0[k] - m1[k]) <= 1e-12 * max(1.0, abs(m0[k])), k
 
 
-@pytest.mark.parametrize("mode", ["passes", "persistent"])
-def test_multi_sweep_graph_equals_single_sweeps(mode):
+@pytest.mark.parametrize("case", ["passes", "persistent", "passes_448_64cubed", "f64_stream"])
+def test_multi_sweep_graph_equals_single_sweeps(case):
     """lce_sweeps(n) replays graphs of 8 sweeps chained by programmatic
-    launch: 19 sweeps that way (two 8-sweep graphs and three single ones)
-    give the same fields, RNG position and last measurements as 19 single
-    lce_sweep calls, with ahiggs1 (its step adapted after every sweep) and a
-    link-overrelaxation hit in the composition."""
+    launch; in the per-pass form each sweep's finalize but the last runs in
+    an extra block of the next sweep's first pass, and the sweeps take fixed
+    RNG offsets that only the graph's last finalize advances.  19 sweeps that
+    way (two 8-sweep graphs and three single ones) give the same fields, RNG
+    position (Philox counter or validation-stream position) and last
+    measurements as 19 single lce_sweep calls, with ahiggs1 (its step adapted
+    after every sweep) and a link-overrelaxation hit in the composition."""
+    L, kw = (16, 16, 16), dict(sweep_mode="passes")
+    if case == "persistent":
+        kw = dict(sweep_mode="persistent")
+    elif case == "passes_448_64cubed":
+        L, kw = (64, 64, 64), dict(sweep_mode="passes", tile_threads=448)
+    elif case == "f64_stream":
+        L, kw = (8, 8, 8), dict(sweep_mode="passes", precision="f64", rng="stream")
     res = []
     for many in (True, False):
-        g = Lattice((16, 16, 16), beta=9.0, x=0.1, y=0.45, seed=17, sweep_mode=mode, n_link_or=1, n_higgs_metro=1,
-                    delta0=3.0)
+        g = Lattice(L, beta=9.0, x=0.1, y=0.45, seed=17, n_link_or=1, n_higgs_metro=1, delta0=3.0, **kw)
         g.init_hot(4)
+        if case == "f64_stream":
+            g.set_rng_stream(np.random.default_rng(5).random(40 * 19 * L[0] * L[1] * L[2]))
         if many:
             g.sweeps(19, 1)
         else:
