@@ -277,6 +277,7 @@ __device__ __forceinline__ void higgs_tile(const PassArgs& p, int tile) {
         q[0] += (double)rho_o;
         q[1] += (double)rho_o * (double)rho_o;
         if (MODE == 2) q[2] += (double)sf_o;
+        else if constexpr (sizeof(R) == 4) q[2] += (double)(ao[0] * f[0] + ao[1] * f[1] + ao[2] * f[2]);
         else q[2] += (double)ao[0] * f[0] + (double)ao[1] * f[1] + (double)ao[2] * f[2];
       }
     }
