@@ -626,7 +626,7 @@ def test_autotune_chooses_form_and_tile_shape():
         if mode == "persistent":
             assert (bs, spt) == (256, 1)
         else:
-            assert bs in ((128, 256, 512) if req == 0 else (req,)) and spt == (2 if mode == "passes2" else 1)
+            assert bs in ((128, 256, 448, 512) if req == 0 else (req,)) and spt == (2 if mode == "passes2" else 1)
         u, a = g.download()
         g.close()
         np.testing.assert_array_equal(u, u_ref)
