@@ -605,6 +605,35 @@ def test_multi_sweep_graph_equals_single_sweeps(case):
     assert r0 == r1 and m0 == m1
 
 
+@pytest.mark.parametrize("case", ["single_128cubed", "batch"])
+def test_multi_sweep_graph_multichunk_and_batch(case):
+    """Graphs of sweeps where each sweep keeps its own finalize kernel (the
+    multi-block one): a chain of more than 8 chunks (128^3, 128-thread tiles:
+    64 chunks) and a batch of chains.  19 sweeps through lce_sweeps equal 19
+    single sweeps bit for bit."""
+    if case == "single_128cubed":
+        specs = [Params(L=(128, 128, 128), beta=12.0, x=0.09, y=0.3, seed=5, n_higgs_metro=1, delta0=2.0)]
+    else:
+        specs = [Params(L=(32, 32, 32), beta=6.0, x=0.1, y=0.1, seed=5, n_link_or=1, n_higgs_metro=1),
+                 Params(L=(8, 12, 6), beta=16.0, x=0.08, y=0.5, seed=6, imode=1, n_link_or=1, n_higgs_metro=1),
+                 Params(L=(48, 16, 16), beta=9.0, x=0.1, y=0.3, seed=7, n_link_or=1, n_higgs_metro=1)]
+    res = []
+    for many in (True, False):
+        ens = Ensemble([Params(**{**s.__dict__, "sweep_mode": "passes", "tile_threads": 128}) for s in specs])
+        ens.init_hot(3)
+        if many:
+            ens.sweeps(19, 1)
+        else:
+            for _ in range(19):
+                ens.sweep(1)
+        res.append(([ens.download(chain=i) for i in range(len(specs))], ens.meas_batch(), ens.rng_position()))
+        ens.close()
+    for i in range(len(specs)):
+        np.testing.assert_array_equal(res[0][0][i][0], res[1][0][i][0])
+        np.testing.assert_array_equal(res[0][0][i][1], res[1][0][i][1])
+    assert res[0][1] == res[1][1] and res[0][2] == res[1][2]
+
+
 def test_autotune_chooses_form_and_tile_shape():
     """LCE_SWEEP_AUTO times every candidate (per-pass forms at each tile
     shape, and the persistent form) on real sweeps and keeps one; with
